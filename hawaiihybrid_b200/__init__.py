@@ -1,0 +1,17 @@
+"""B200-native trajectory hot path of HAWAIIHYBRID (classical-trajectory CIA spectra).
+
+The numerical work runs in libhh_cuda.so (hand-written sm_100a CUDA, C ABI in
+include/hh_cuda.h); `hawaii` mirrors the reference's host interface on top of it.
+"""
+from . import _lib
+from ._lib import HHError
+from .hawaii import (ATOM, LINEAR_MOLECULE, PAIR_STATE_ALL, PAIR_STATE_BOUND,
+                     PAIR_STATE_FREE_AND_METASTABLE, PRECISION_FP64, PRECISION_MIXED,
+                     SYSTEM_CO2_AR, SYSTEM_HE_AR, CalcParams, CFnc, MoleculeSystem, SFnc,
+                     analytic_full_partition_function_by_V, calculate_correlation_and_save,
+                     calculate_m0, correlation_from_initial_conditions, correlation_iteration,
+                     idct_cf_to_sf, init_ms, read_correlation_function, read_spectral_function,
+                     sample_initial_conditions, write_correlation_function,
+                     write_spectral_function)
+
+__all__ = [n for n in dir() if not n.startswith("_")]

@@ -1,0 +1,122 @@
+"""ctypes binding of libhh_cuda.so (C ABI declared in include/hh_cuda.h).
+
+There is no CPU fallback: if the library is missing or no CUDA device is
+visible, every call raises HHError.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+PKG = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(PKG, "lib", "libhh_cuda.so")
+
+HH_OK = 0
+HH_E_NOT_INITIALIZED = -1
+HH_E_INVALID_ARGUMENT = -2
+HH_E_CUDA = -3
+HH_E_UNSUPPORTED_SYSTEM = -4
+HH_E_OUT_OF_MEMORY = -5
+HH_E_NOT_POWER_OF_TWO = -6
+HH_E_SAMPLER = -7
+HH_E_NO_DEVICE = -8
+
+HH_MONOMER_ATOM = 0
+HH_MONOMER_LINEAR_MOLECULE = 4
+HH_PAIR_STATE_FREE_AND_METASTABLE = 1
+HH_PAIR_STATE_BOUND = 2
+HH_PAIR_STATE_ALL = 3
+HH_SYSTEM_HE_AR = 1
+HH_SYSTEM_CO2_AR = 2
+HH_PRECISION_FP64 = 0
+HH_PRECISION_MIXED = 1
+
+# entry points declared in include/hh_cuda.h
+EXPORTS = (
+    "hh_cuda_init", "hh_cuda_seed", "hh_cuda_sample", "hh_cuda_correlation",
+    "hh_cuda_correlation_ic", "hh_cuda_m0", "hh_cuda_idct_cf_to_sf", "hh_cuda_strerror",
+    "hh_cuda_mt_stream", "hh_cuda_debug_inject", "hh_cuda_shutdown",
+)
+
+
+class HHError(RuntimeError):
+    def __init__(self, code: int, msg: str):
+        super().__init__(f"{msg} (code {code})")
+        self.code = code
+
+
+class SystemDesc(C.Structure):
+    _fields_ = [
+        ("system_id", C.c_int), ("mu", C.c_double),
+        ("monomer1_type", C.c_int), ("monomer2_type", C.c_int),
+        ("II1", C.c_double * 3), ("II2", C.c_double * 3),
+    ]
+
+
+class CalcParamsC(C.Structure):
+    _fields_ = [
+        ("pair_state", C.c_int),
+        ("sampler_Rmin", C.c_double), ("sampler_Rmax", C.c_double), ("pesmin", C.c_double),
+        ("sampling_time", C.c_double), ("MaxTrajectoryLength", C.c_size_t), ("Rcut", C.c_double),
+        ("cvode_tolerance", C.c_double), ("partial_partition_function_ratio", C.c_double),
+        ("mixed_tolerance", C.c_double), ("max_steps", C.c_long),
+    ]
+
+
+class Stats(C.Structure):
+    _fields_ = [
+        ("n_candidates", C.c_uint64), ("n_accepted", C.c_uint64), ("n_steps", C.c_uint64),
+        ("n_rejected_steps", C.c_uint64), ("n_rhs", C.c_uint64), ("n_samples", C.c_uint64),
+        ("n_dense", C.c_uint64), ("n_failed", C.c_uint64), ("status", C.c_uint64 * 8),
+        ("sample_ms", C.c_double), ("traj_ms", C.c_double), ("total_ms", C.c_double),
+    ]
+
+    def as_dict(self) -> dict:
+        d = {f: getattr(self, f) for f, _ in self._fields_ if f != "status"}
+        d["status"] = list(self.status)[:6]
+        return d
+
+
+_dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
+_u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
+_lib = None
+
+
+def load(path: str | None = None):
+    """Load libhh_cuda.so; raises HHError when it is not built."""
+    global _lib
+    if _lib is not None:
+        return _lib
+    path = path or LIB_PATH
+    if not os.path.exists(path):
+        raise HHError(HH_E_CUDA, f"CUDA library not built: {path} (run __graft_entry__.build())")
+    L = C.CDLL(path)
+    L.hh_cuda_init.argtypes = [C.c_int, C.POINTER(SystemDesc)]
+    L.hh_cuda_seed.argtypes = [C.c_uint32]
+    L.hh_cuda_sample.argtypes = [C.POINTER(CalcParamsC), C.c_double, C.c_uint32, C.c_uint64, _dp,
+                                 C.POINTER(C.c_uint64)]
+    L.hh_cuda_correlation.argtypes = [C.POINTER(CalcParamsC), C.c_double, C.c_uint32, C.c_uint64,
+                                      C.c_int, _dp, C.POINTER(C.c_double), C.POINTER(Stats)]
+    L.hh_cuda_correlation_ic.argtypes = [C.POINTER(CalcParamsC), _dp, C.c_uint64, C.c_int, _dp,
+                                         C.POINTER(Stats)]
+    L.hh_cuda_m0.argtypes = [C.POINTER(CalcParamsC), _dp, C.c_int, C.c_uint64, C.c_uint64, C.c_int,
+                             _dp, _dp]
+    L.hh_cuda_idct_cf_to_sf.argtypes = [_dp, C.c_size_t, C.c_double, _dp, _dp]
+    L.hh_cuda_strerror.restype = C.c_char_p
+    L.hh_cuda_strerror.argtypes = [C.c_int]
+    L.hh_cuda_mt_stream.argtypes = [C.c_uint32, C.c_uint64, _u32p]
+    L.hh_cuda_debug_inject.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int]
+    L.hh_cuda_shutdown.restype = None
+    for name in EXPORTS:
+        if name not in ("hh_cuda_strerror", "hh_cuda_shutdown"):
+            getattr(L, name).restype = C.c_int
+    _lib = L
+    return L
+
+
+def check(code: int) -> None:
+    if code != HH_OK:
+        msg = load().hh_cuda_strerror(code).decode()
+        raise HHError(code, msg)

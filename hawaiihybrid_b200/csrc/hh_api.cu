@@ -1,0 +1,644 @@
+// C ABI of libhh_cuda.so (include/hh_cuda.h): device context, buffers, the
+// sampler rounds, the trajectory launch with its failure-compensation pass, the
+// zeroth-moment integral and the CF->SF transform.
+#include <cuda_runtime.h>
+#include <stdint.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <vector>
+
+#include "../../include/hh_cuda.h"
+#include "hh_co2ar_tables.h"
+#include "hh_consts.h"
+#include "hh_fft.cuh"
+#include "hh_internal.h"
+#include "hh_m0.cuh"
+#include "hh_traj.cuh"
+
+namespace {
+
+using namespace hh;
+
+char g_errmsg[512] = "";
+
+#define CK(call)                                                                     \
+  do {                                                                               \
+    cudaError_t e_ = (call);                                                         \
+    if (e_ != cudaSuccess) {                                                         \
+      snprintf(g_errmsg, sizeof g_errmsg, "%s:%d %s: %s", __FILE__, __LINE__, #call, \
+               cudaGetErrorString(e_));                                              \
+      return HH_E_CUDA;                                                              \
+    }                                                                                \
+  } while (0)
+
+template <typename T> struct DevBuf {
+  T *p = nullptr;
+  size_t cap = 0;
+  cudaError_t ensure(size_t n) {
+    if (n <= cap) return cudaSuccess;
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+    size_t want = std::max(n, cap * 3 / 2);
+    cudaError_t e = cudaMalloc(&p, want * sizeof(T));
+    if (e == cudaSuccess) cap = want;
+    return e;
+  }
+  void release() {
+    if (p) cudaFree(p);
+    p = nullptr;
+    cap = 0;
+  }
+};
+
+struct Ctx {
+  bool init = false;
+  int device = -1;
+  int sys = 0;
+  double mu = 0.0, II = 0.0;
+  int QP = 0, D = 0;
+  cudaStream_t st = nullptr;
+  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  int num_sms = 0;
+  Co2arTablesGlobal *d_tab = nullptr;
+  // MT19937 stream
+  uint32_t *d_mt = nullptr;
+  DevBuf<uint32_t> words[2];
+  int cur = 0;
+  long long wbase = 0, wvalid = 0, wpos = 0;
+  double p_accept = 0.25;
+  // sampler scratch
+  DevBuf<unsigned char> accept, consumed;
+  DevBuf<double> qp_cand, energy, qp0;
+  DevBuf<unsigned int> block_counts;
+  DevBuf<long long> cand_idx;
+  DevBuf<unsigned long long> scal;  // [0] first_irregular, [1] total
+  // trajectories
+  DevBuf<double> crln;
+  DevBuf<unsigned long long> counters;
+  DevBuf<unsigned int> status_hist, queue;
+  DevBuf<int> fail_flag, fail_list, fail_count, items;
+  // M0
+  DevBuf<double> m0_partials, m0_out;
+  // FFT
+  DevBuf<double> f_cf, f_nu, f_sf;
+  DevBuf<double2> f_a, f_b;
+};
+
+Ctx g;
+int g_inject_item = -1, g_inject_k = -1, g_inject_status = 0;
+
+void build_tables(Co2arTablesGlobal *t) {
+  memcpy(t->pes, hh_co2ar_pes, sizeof(t->pes));
+  memcpy(t->dipx, hh_co2ar_dipx, sizeof(t->dipx));
+  memcpy(t->dipz, hh_co2ar_dipz, sizeof(t->dipz));
+  for (int i = 0; i < CO2AR_NINT; ++i) {
+    t->rbound[i] = (i < CO2AR_NINT - 1) ? hh_co2ar_rbound[i] : 1e300;
+    t->rlo[i] = hh_co2ar_rlo[i];
+    int fp = 0, fd = 0;
+    for (int l = 0; l < CO2AR_NL; ++l) {
+      const double *rp = hh_co2ar_pes[i][l];
+      const double *rx = hh_co2ar_dipx[i][l];
+      const double *rz = hh_co2ar_dipz[i][l];
+      for (int k = 4; k < 8; ++k) {
+        if (rp[k] != 0.0) fp |= 1;
+        if (rx[k] != 0.0 || rz[k] != 0.0) fd |= 1;
+      }
+      if (rp[8] != 0.0) fp |= 2;
+      if (rx[8] != 0.0 || rz[8] != 0.0) fd |= 2;
+    }
+    t->fpes[i] = fp;
+    t->fdip[i] = fd;
+  }
+}
+
+int check_params(const hh_calc_params *p) {
+  if (!p) return HH_E_INVALID_ARGUMENT;
+  if (!(p->sampler_Rmin > 0) || !(p->sampler_Rmax > p->sampler_Rmin)) return HH_E_INVALID_ARGUMENT;
+  if (!(p->sampling_time > 0) || p->MaxTrajectoryLength < 2) return HH_E_INVALID_ARGUMENT;
+  if (!(p->Rcut > 0) || !(p->cvode_tolerance > 0)) return HH_E_INVALID_ARGUMENT;
+  if (p->pair_state < 1 || p->pair_state > 3) return HH_E_INVALID_ARGUMENT;
+  if (p->MaxTrajectoryLength > (size_t)INT32_MAX) return HH_E_INVALID_ARGUMENT;
+  return HH_OK;
+}
+
+// make words [wpos, need_end) resident in words[cur]
+int ensure_words(long long need_end) {
+  if (g.wbase <= g.wpos && g.wbase + g.wvalid >= need_end) return HH_OK;
+  long long end_old = g.wbase + g.wvalid;
+  long long left = std::max(0LL, end_old - g.wpos);
+  long long gen = need_end - (g.wpos + left);
+  long long nblk = (gen + MT_N - 1) / MT_N + 1;
+  int nxt = 1 - g.cur;
+  CK(g.words[nxt].ensure((size_t)(left + nblk * MT_N)));
+  if (left) {
+    CK(cudaMemcpyAsync(g.words[nxt].p, g.words[g.cur].p + (g.wpos - g.wbase),
+                       (size_t)left * sizeof(uint32_t), cudaMemcpyDeviceToDevice, g.st));
+  }
+  CK(launch_mt_generate(g.d_mt, g.words[nxt].p + left, nblk, g.st));
+  g.cur = nxt;
+  g.wbase = g.wpos;
+  g.wvalid = left + nblk * MT_N;
+  return HH_OK;
+}
+
+int reseed(uint32_t seed) {
+  CK(launch_mt_seed(seed, g.d_mt, g.st));
+  g.wbase = g.wvalid = g.wpos = 0;
+  return HH_OK;
+}
+
+// draw n accepted phase points into d_out (device), in the reference's order
+int sample_into(const hh_calc_params *p, double T, uint64_t n, double *d_out, uint64_t *ncand_out) {
+  uint64_t got = 0, ncand_total = 0;
+  CK(g.cand_idx.ensure(std::max<uint64_t>(n, 1)));
+  CK(g.scal.ensure(4));
+  while (got < n) {
+    long long remaining = (long long)(n - got);
+    double pe = std::max(g.p_accept, 0.01);
+    long long ncand = (long long)(remaining / pe * 1.15) + 4096;
+    ncand = std::min(std::max(ncand, 65536LL), 1LL << 23);
+    int rc = ensure_words(g.wpos + ncand * g.D + 4096);
+    if (rc) return rc;
+    CK(g.accept.ensure(ncand));
+    CK(g.consumed.ensure(ncand));
+    CK(g.qp_cand.ensure((size_t)ncand * g.QP));
+    CK(g.energy.ensure(ncand));
+    CK(g.block_counts.ensure((ncand + 1023) / 1024 + 1));
+    CK(cudaMemsetAsync(g.scal.p, 0xff, sizeof(unsigned long long), g.st));
+    CK(launch_candidates(g.sys, g.mu, g.II, T, p->sampler_Rmin, p->sampler_Rmax, p->pesmin,
+                         p->pair_state, g.d_tab, g.words[g.cur].p, g.wvalid, g.wpos - g.wbase, g.D,
+                         ncand, g.accept.p, g.consumed.p, g.qp_cand.p, g.energy.p, g.scal.p,
+                         g.st));
+    unsigned long long first_irr = 0;
+    CK(cudaMemcpyAsync(&first_irr, g.scal.p, sizeof first_irr, cudaMemcpyDeviceToHost, g.st));
+    CK(cudaStreamSynchronize(g.st));
+    long long limit = (first_irr == ~0ULL) ? ncand - 1 : (long long)first_irr;
+    CK(launch_compact(g.accept.p, g.qp_cand.p, ncand, limit, g.QP, (long long)got, (long long)n,
+                      d_out, g.cand_idx.p, g.block_counts.p, g.scal.p + 1, g.st));
+    unsigned long long total = 0;
+    CK(cudaMemcpyAsync(&total, g.scal.p + 1, sizeof total, cudaMemcpyDeviceToHost, g.st));
+    CK(cudaStreamSynchronize(g.st));
+    long long take = std::min<long long>((long long)total, remaining);
+    long long E;
+    if (take == remaining && take > 0) {
+      long long last = 0;
+      CK(cudaMemcpy(&last, g.cand_idx.p + got + take - 1, sizeof last, cudaMemcpyDeviceToHost));
+      E = last;
+    } else {
+      E = limit;
+    }
+    int usedE = g.D;
+    if (first_irr != ~0ULL && E == (long long)first_irr) {
+      unsigned char cE = 0;
+      CK(cudaMemcpy(&cE, g.consumed.p + E, 1, cudaMemcpyDeviceToHost));
+      if (cE == 0) {
+        snprintf(g_errmsg, sizeof g_errmsg, "sampler ran past the generated stream");
+        return HH_E_SAMPLER;
+      }
+      usedE = cE;
+    }
+    g.wpos += E * g.D + usedE;
+    ncand_total += (uint64_t)(E + 1);
+    got += (uint64_t)take;
+    if (got < n && ncand_total > 20000000000ULL) {
+      snprintf(g_errmsg, sizeof g_errmsg,
+               "sampler: %llu of %llu phase points accepted after %llu candidates (acceptance too low)",
+               (unsigned long long)got, (unsigned long long)n, (unsigned long long)ncand_total);
+      return HH_E_SAMPLER;
+    }
+    g.p_accept = std::max(1.0, (double)total) / double(limit + 1);
+  }
+  if (ncand_out) *ncand_out = ncand_total;
+  return HH_OK;
+}
+
+template <int SYS, typename PHYS, typename STG, bool COMP>
+int launch_traj(const TrajParams &P, const TrajIO &io, int *grid_out) {
+  auto kern = traj_kernel<SYS, PHYS, STG, COMP>;
+  size_t smem = (SYS == SYS_CO2AR) ? sizeof(Co2arTables<PHYS>) : 0;
+  if (smem > 48 * 1024) CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem));
+  int grid = std::max(1, per_sm) * g.num_sms;
+  long long need = (io.n_items + 127) / 128;
+  if (need < grid) grid = (int)std::max(1LL, need);
+  kern<<<grid, 128, smem, g.st>>>(P, io, g.d_tab);
+  CK(cudaGetLastError());
+  if (grid_out) *grid_out = grid;
+  return HH_OK;
+}
+
+int run_traj_dispatch(int precision, const TrajParams &P, const TrajIO &io) {
+  if (g.sys == SYS_HEAR) {
+    if (precision == HH_PRECISION_MIXED) return launch_traj<SYS_HEAR, float, float, true>(P, io, nullptr);
+    return launch_traj<SYS_HEAR, double, double, false>(P, io, nullptr);
+  }
+  if (precision == HH_PRECISION_MIXED) return launch_traj<SYS_CO2AR, float, float, true>(P, io, nullptr);
+  return launch_traj<SYS_CO2AR, double, double, false>(P, io, nullptr);
+}
+
+// integrate both branches of n trajectories whose phase points are in d_ic
+int run_trajectories(const hh_calc_params *p, const double *d_ic, uint64_t n, int precision,
+                     double *crln_host, hh_stats *stats) {
+  const size_t N = p->MaxTrajectoryLength;
+  TrajParams P;
+  P.mu = g.mu;
+  P.II = g.II;
+  P.dt = p->sampling_time;
+  P.N = (int)N;
+  P.Rcut = p->Rcut;
+  double tol = (precision == HH_PRECISION_MIXED)
+                   ? (p->mixed_tolerance > 0 ? p->mixed_tolerance : 1e-8)
+                   : p->cvode_tolerance;
+  P.rtol = P.atol = tol;
+  P.max_steps = p->max_steps > 0 ? p->max_steps : 50000;
+  P.max_total_steps = 4000000;
+  P.weight = p->partial_partition_function_ratio * 0.5 * HH_ALU * HH_ALU * HH_ALU;
+  P.inject_item = g_inject_item;
+  P.inject_k = g_inject_k;
+  P.inject_status = g_inject_status;
+  CK(g.crln.ensure(N));
+  CK(g.counters.ensure(16));
+  CK(g.status_hist.ensure(2 * HH_ST_COUNT));
+  CK(g.queue.ensure(1));
+  CK(g.fail_flag.ensure(std::max<uint64_t>(n, 1)));
+  CK(g.fail_list.ensure(std::max<uint64_t>(n, 1)));
+  CK(g.fail_count.ensure(1));
+  CK(cudaMemsetAsync(g.crln.p, 0, N * sizeof(double), g.st));
+  CK(cudaMemsetAsync(g.counters.p, 0, 16 * sizeof(unsigned long long), g.st));
+  CK(cudaMemsetAsync(g.status_hist.p, 0, 2 * HH_ST_COUNT * sizeof(unsigned int), g.st));
+  CK(cudaMemsetAsync(g.queue.p, 0, sizeof(unsigned int), g.st));
+  CK(cudaMemsetAsync(g.fail_flag.p, 0, n * sizeof(int), g.st));
+  CK(cudaMemsetAsync(g.fail_count.p, 0, sizeof(int), g.st));
+  TrajIO io;
+  io.ic = d_ic;
+  io.items = nullptr;
+  io.n_items = (int)(2 * n);
+  io.queue = g.queue.p;
+  io.crln = g.crln.p;
+  io.counters = g.counters.p;
+  io.status_hist = g.status_hist.p;
+  io.fail_flag = g.fail_flag.p;
+  io.fail_list = g.fail_list.p;
+  io.fail_count = g.fail_count.p;
+  CK(cudaEventRecord(g.ev[2], g.st));
+  int rc = run_traj_dispatch(precision, P, io);
+  if (rc) return rc;
+  int nfail = 0;
+  CK(cudaMemcpyAsync(&nfail, g.fail_count.p, sizeof nfail, cudaMemcpyDeviceToHost, g.st));
+  CK(cudaStreamSynchronize(g.st));
+  if (nfail > 0) {
+    // the reference drops a trajectory whose correlation_eval returns 1 while
+    // still counting it; both branches are replayed with the opposite weight
+    std::vector<int> fl(nfail), it(2 * (size_t)nfail);
+    CK(cudaMemcpy(fl.data(), g.fail_list.p, nfail * sizeof(int), cudaMemcpyDeviceToHost));
+    for (int i = 0; i < nfail; ++i) {
+      it[2 * i] = 2 * fl[i];
+      it[2 * i + 1] = 2 * fl[i] + 1;
+    }
+    CK(g.items.ensure(it.size()));
+    CK(cudaMemcpyAsync(g.items.p, it.data(), it.size() * sizeof(int), cudaMemcpyHostToDevice, g.st));
+    CK(cudaMemsetAsync(g.queue.p, 0, sizeof(unsigned int), g.st));
+    TrajParams P2 = P;
+    P2.weight = -P.weight;
+    TrajIO io2 = io;
+    io2.items = g.items.p;
+    io2.n_items = (int)it.size();
+    io2.fail_flag = nullptr;
+    io2.counters = g.counters.p + 8;           // replay work is not counted twice
+    io2.status_hist = g.status_hist.p + HH_ST_COUNT;
+    rc = run_traj_dispatch(precision, P2, io2);
+    if (rc) return rc;
+  }
+  CK(cudaEventRecord(g.ev[3], g.st));
+  CK(cudaMemcpyAsync(crln_host, g.crln.p, N * sizeof(double), cudaMemcpyDeviceToHost, g.st));
+  unsigned long long cnt[8];
+  unsigned int hist[HH_ST_COUNT];
+  CK(cudaMemcpyAsync(cnt, g.counters.p, sizeof cnt, cudaMemcpyDeviceToHost, g.st));
+  CK(cudaMemcpyAsync(hist, g.status_hist.p, sizeof hist, cudaMemcpyDeviceToHost, g.st));
+  CK(cudaStreamSynchronize(g.st));
+  if (stats) {
+    stats->n_steps = cnt[0];
+    stats->n_rejected_steps = cnt[1];
+    stats->n_rhs = cnt[2];
+    stats->n_samples = cnt[3];
+    stats->n_dense = cnt[4];
+    stats->n_failed = (uint64_t)nfail;
+    for (int i = 0; i < 8; ++i) stats->status[i] = (i < HH_ST_COUNT) ? hist[i] : 0;
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, g.ev[2], g.ev[3]));
+    stats->traj_ms = ms;
+  }
+  return HH_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char *hh_cuda_strerror(int code) {
+  switch (code) {
+    case HH_OK: return "ok";
+    case HH_E_NOT_INITIALIZED: return "hh_cuda_init has not been called";
+    case HH_E_INVALID_ARGUMENT: return "invalid argument";
+    case HH_E_CUDA: return g_errmsg[0] ? g_errmsg : "CUDA error";
+    case HH_E_UNSUPPORTED_SYSTEM: return "unsupported system";
+    case HH_E_OUT_OF_MEMORY: return "out of device memory";
+    case HH_E_NOT_POWER_OF_TWO: return "length of the input array should be a power of 2";
+    case HH_E_SAMPLER: return g_errmsg[0] ? g_errmsg : "sampler error";
+    case HH_E_NO_DEVICE: return "no CUDA device";
+    default: return "unknown error";
+  }
+}
+
+int hh_cuda_init(int device, const hh_system_desc *sys) {
+  if (!sys) return HH_E_INVALID_ARGUMENT;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) {
+    cudaGetLastError();
+    return HH_E_NO_DEVICE;
+  }
+  if (device < 0 || device >= ndev) return HH_E_INVALID_ARGUMENT;
+  int sid = sys->system_id;
+  if (sid == HH_SYSTEM_HE_AR) {
+    if (sys->monomer1_type != HH_MONOMER_ATOM || sys->monomer2_type != HH_MONOMER_ATOM)
+      return HH_E_UNSUPPORTED_SYSTEM;
+  } else if (sid == HH_SYSTEM_CO2_AR) {
+    if (sys->monomer1_type != HH_MONOMER_LINEAR_MOLECULE || sys->monomer2_type != HH_MONOMER_ATOM)
+      return HH_E_UNSUPPORTED_SYSTEM;
+    if (!(sys->II1[0] > 0) || sys->II1[0] != sys->II1[1]) return HH_E_INVALID_ARGUMENT;
+  } else {
+    return HH_E_UNSUPPORTED_SYSTEM;
+  }
+  if (!(sys->mu > 0)) return HH_E_INVALID_ARGUMENT;
+  if (g.init && g.device != device) hh_cuda_shutdown();
+  CK(cudaSetDevice(device));
+  if (!g.init) {
+    CK(cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking));
+    for (auto &e : g.ev) CK(cudaEventCreate(&e));
+    CK(cudaDeviceGetAttribute(&g.num_sms, cudaDevAttrMultiProcessorCount, device));
+    CK(cudaMalloc(&g.d_tab, sizeof(Co2arTablesGlobal)));
+    CK(cudaMalloc(&g.d_mt, MT_N * sizeof(uint32_t)));
+    static Co2arTablesGlobal host_tab;
+    build_tables(&host_tab);
+    CK(cudaMemcpy(g.d_tab, &host_tab, sizeof host_tab, cudaMemcpyHostToDevice));
+    g.device = device;
+    g.init = true;
+    int rc = reseed(0);
+    if (rc) return rc;
+  }
+  g.sys = (sid == HH_SYSTEM_HE_AR) ? SYS_HEAR : SYS_CO2AR;
+  g.mu = sys->mu;
+  g.II = (sid == HH_SYSTEM_CO2_AR) ? sys->II1[0] : 0.0;
+  g.QP = (sid == HH_SYSTEM_HE_AR) ? 6 : 10;
+  g.D = (sid == HH_SYSTEM_HE_AR) ? 10 : 16;
+  g.p_accept = 0.25;
+  return HH_OK;
+}
+
+int hh_cuda_seed(uint32_t seed) {
+  if (!g.init) return HH_E_NOT_INITIALIZED;
+  CK(cudaSetDevice(g.device));
+  int rc = reseed(seed);
+  if (rc) return rc;
+  CK(cudaStreamSynchronize(g.st));
+  return HH_OK;
+}
+
+int hh_cuda_sample(const hh_calc_params *p, double T, uint32_t seed, uint64_t n, double *qp_out,
+                   uint64_t *n_candidates) {
+  if (!g.init) return HH_E_NOT_INITIALIZED;
+  int rc = check_params(p);
+  if (rc) return rc;
+  if (!(T > 0) || (n > 0 && !qp_out)) return HH_E_INVALID_ARGUMENT;
+  CK(cudaSetDevice(g.device));
+  if (seed > 0) {
+    rc = reseed(seed);
+    if (rc) return rc;
+  }
+  if (n == 0) return HH_OK;
+  CK(g.qp0.ensure(n * g.QP));
+  rc = sample_into(p, T, n, g.qp0.p, n_candidates);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(qp_out, g.qp0.p, n * g.QP * sizeof(double), cudaMemcpyDeviceToHost, g.st));
+  CK(cudaStreamSynchronize(g.st));
+  return HH_OK;
+}
+
+int hh_cuda_correlation(const hh_calc_params *p, double T, uint32_t seed, uint64_t n_accept,
+                        int precision_mode, double *crln_sum, double *ntraj, hh_stats *stats) {
+  if (!g.init) return HH_E_NOT_INITIALIZED;
+  int rc = check_params(p);
+  if (rc) return rc;
+  if (!(T > 0) || !crln_sum || n_accept == 0 || n_accept > (uint64_t)(INT32_MAX / 2))
+    return HH_E_INVALID_ARGUMENT;
+  if (precision_mode != HH_PRECISION_FP64 && precision_mode != HH_PRECISION_MIXED)
+    return HH_E_INVALID_ARGUMENT;
+  CK(cudaSetDevice(g.device));
+  if (seed > 0) {
+    rc = reseed(seed);
+    if (rc) return rc;
+  }
+  hh_stats local;
+  memset(&local, 0, sizeof local);
+  CK(g.qp0.ensure(n_accept * g.QP));
+  CK(cudaEventRecord(g.ev[0], g.st));
+  uint64_t ncand = 0;
+  rc = sample_into(p, T, n_accept, g.qp0.p, &ncand);
+  if (rc) return rc;
+  CK(cudaEventRecord(g.ev[1], g.st));
+  rc = run_trajectories(p, g.qp0.p, n_accept, precision_mode, crln_sum, &local);
+  if (rc) return rc;
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, g.ev[0], g.ev[1]));
+  local.sample_ms = ms;
+  CK(cudaEventElapsedTime(&ms, g.ev[0], g.ev[3]));
+  local.total_ms = ms;
+  local.n_candidates = ncand;
+  local.n_accepted = n_accept;
+  if (ntraj) *ntraj = (double)n_accept;
+  if (stats) *stats = local;
+  return HH_OK;
+}
+
+int hh_cuda_correlation_ic(const hh_calc_params *p, const double *qp0, uint64_t n,
+                           int precision_mode, double *crln_sum, hh_stats *stats) {
+  if (!g.init) return HH_E_NOT_INITIALIZED;
+  int rc = check_params(p);
+  if (rc) return rc;
+  if (!qp0 || !crln_sum || n == 0 || n > (uint64_t)(INT32_MAX / 2)) return HH_E_INVALID_ARGUMENT;
+  if (precision_mode != HH_PRECISION_FP64 && precision_mode != HH_PRECISION_MIXED)
+    return HH_E_INVALID_ARGUMENT;
+  CK(cudaSetDevice(g.device));
+  hh_stats local;
+  memset(&local, 0, sizeof local);
+  CK(g.qp0.ensure(n * g.QP));
+  CK(cudaEventRecord(g.ev[0], g.st));
+  CK(cudaMemcpyAsync(g.qp0.p, qp0, n * g.QP * sizeof(double), cudaMemcpyHostToDevice, g.st));
+  CK(cudaEventRecord(g.ev[1], g.st));
+  rc = run_trajectories(p, g.qp0.p, n, precision_mode, crln_sum, &local);
+  if (rc) return rc;
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, g.ev[0], g.ev[3]));
+  local.total_ms = ms;
+  local.n_accepted = n;
+  if (stats) *stats = local;
+  return HH_OK;
+}
+
+int hh_cuda_m0(const hh_calc_params *p, const double *T, int nT, uint64_t n_samples,
+               uint64_t seed, int precision_mode, double *m, double *err) {
+  if (!g.init) return HH_E_NOT_INITIALIZED;
+  if (!p || !T || nT < 1 || !m || n_samples == 0) return HH_E_INVALID_ARGUMENT;
+  if (!(p->sampler_Rmin > 0) || !(p->sampler_Rmax > p->sampler_Rmin)) return HH_E_INVALID_ARGUMENT;
+  if (p->pair_state < 1 || p->pair_state > 3) return HH_E_INVALID_ARGUMENT;
+  if (precision_mode != HH_PRECISION_FP64 && precision_mode != HH_PRECISION_MIXED)
+    return HH_E_INVALID_ARGUMENT;
+  for (int t = 0; t < nT; ++t)
+    if (!(T[t] > 0)) return HH_E_INVALID_ARGUMENT;
+  CK(cudaSetDevice(g.device));
+  const int block = 256;
+  const int grid = g.num_sms * 4;
+  CK(g.m0_partials.ensure((size_t)grid * M0_MAXT * 2));
+  CK(g.m0_out.ensure(M0_MAXT * 2));
+  const double scale = HH_ZEROCOEFF * 4.0 * HH_PI * (p->sampler_Rmax - p->sampler_Rmin);
+  for (int t0 = 0; t0 < nT; t0 += M0_MAXT) {
+    M0Args a;
+    memset(&a, 0, sizeof a);
+    a.sys = g.sys;
+    a.Rmin = p->sampler_Rmin;
+    a.Rmax = p->sampler_Rmax;
+    a.pair_state = p->pair_state;
+    a.nT = std::min(M0_MAXT, nT - t0);
+    for (int t = 0; t < a.nT; ++t) a.invkT[t] = HH_HKT / T[t0 + t];
+    a.n_samples = n_samples;
+    a.offset = 0;
+    a.seed = seed;
+    if (g.sys == SYS_HEAR) {
+      if (precision_mode == HH_PRECISION_MIXED)
+        m0_kernel<SYS_HEAR, float, true><<<grid, block, 0, g.st>>>(a, g.d_tab, g.m0_partials.p);
+      else
+        m0_kernel<SYS_HEAR, double, false><<<grid, block, 0, g.st>>>(a, g.d_tab, g.m0_partials.p);
+    } else {
+      if (precision_mode == HH_PRECISION_MIXED)
+        m0_kernel<SYS_CO2AR, float, true><<<grid, block, sizeof(Co2arTables<float>), g.st>>>(
+            a, g.d_tab, g.m0_partials.p);
+      else
+        m0_kernel<SYS_CO2AR, double, false><<<grid, block, sizeof(Co2arTables<double>), g.st>>>(
+            a, g.d_tab, g.m0_partials.p);
+    }
+    CK(cudaGetLastError());
+    m0_finalize_kernel<<<1, 32, 0, g.st>>>(g.m0_partials.p, grid, g.m0_out.p);
+    CK(cudaGetLastError());
+    double out[M0_MAXT * 2];
+    CK(cudaMemcpyAsync(out, g.m0_out.p, sizeof out, cudaMemcpyDeviceToHost, g.st));
+    CK(cudaStreamSynchronize(g.st));
+    for (int t = 0; t < a.nT; ++t) {
+      double mean = out[2 * t] / double(n_samples);
+      double var = out[2 * t + 1] / double(n_samples) - mean * mean;
+      m[t0 + t] = scale * mean;
+      if (err) err[t0 + t] = scale * sqrt(std::max(var, 0.0) / double(n_samples));
+    }
+  }
+  return HH_OK;
+}
+
+int hh_cuda_idct_cf_to_sf(double *cf, size_t N, double dt, double *nu, double *sf) {
+  if (!g.init) return HH_E_NOT_INITIALIZED;
+  if (!cf || !nu || !sf || !(dt > 0)) return HH_E_INVALID_ARGUMENT;
+  if (N == 0 || (N & (N - 1))) return HH_E_NOT_POWER_OF_TWO;
+  for (size_t i = 0; i < N; ++i)
+    if (cf[i] != cf[i]) return HH_E_INVALID_ARGUMENT;  // the reference exits on NaN input
+  CK(cudaSetDevice(g.device));
+  long long L = 2 * (long long)N;
+  CK(g.f_cf.ensure(N));
+  CK(g.f_nu.ensure(N));
+  CK(g.f_sf.ensure(N));
+  CK(g.f_a.ensure(L));
+  CK(g.f_b.ensure(L));
+  CK(cudaMemcpyAsync(g.f_cf.p, cf, N * sizeof(double), cudaMemcpyHostToDevice, g.st));
+  int tb = 256;
+  idct_pack_kernel<<<(unsigned)((L + tb - 1) / tb), tb, 0, g.st>>>(g.f_cf.p, (long long)N, dt, g.f_a.p);
+  idct_pack2_kernel<<<(unsigned)((N + tb - 1) / tb), tb, 0, g.st>>>(g.f_cf.p, (long long)N, g.f_a.p);
+  double2 *x = g.f_a.p, *y = g.f_b.p;
+  for (long long s = 1; s < L; s *= 2) {
+    stockham_pass_kernel<<<(unsigned)((L / 2 + tb - 1) / tb), tb, 0, g.st>>>(x, y, L, s);
+    std::swap(x, y);
+  }
+  idct_finish_kernel<<<(unsigned)((N + tb - 1) / tb), tb, 0, g.st>>>(x, (long long)N, dt, g.f_nu.p,
+                                                                      g.f_sf.p);
+  CK(cudaGetLastError());
+  CK(cudaMemcpyAsync(nu, g.f_nu.p, N * sizeof(double), cudaMemcpyDeviceToHost, g.st));
+  CK(cudaMemcpyAsync(sf, g.f_sf.p, N * sizeof(double), cudaMemcpyDeviceToHost, g.st));
+  CK(cudaMemcpyAsync(cf, g.f_cf.p, N * sizeof(double), cudaMemcpyDeviceToHost, g.st));
+  CK(cudaStreamSynchronize(g.st));
+  return HH_OK;
+}
+
+int hh_cuda_mt_stream(uint32_t seed, uint64_t n, uint32_t *out) {
+  if (!g.init) return HH_E_NOT_INITIALIZED;
+  if (!out && n) return HH_E_INVALID_ARGUMENT;
+  CK(cudaSetDevice(g.device));
+  int rc = reseed(seed);
+  if (rc) return rc;
+  rc = ensure_words((long long)n);
+  if (rc) return rc;
+  CK(cudaMemcpyAsync(out, g.words[g.cur].p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, g.st));
+  CK(cudaStreamSynchronize(g.st));
+  return reseed(seed);
+}
+
+int hh_cuda_debug_inject(int traj, int dir, int k, int status) {
+  if (status < 0 || status >= HH_ST_COUNT || dir < 0 || dir > 1) return HH_E_INVALID_ARGUMENT;
+  if (traj < 0) {
+    g_inject_item = g_inject_k = -1;
+    g_inject_status = 0;
+    return HH_OK;
+  }
+  g_inject_item = 2 * traj + dir;
+  g_inject_k = k;
+  g_inject_status = status;
+  return HH_OK;
+}
+
+void hh_cuda_shutdown(void) {
+  if (!g.init) return;
+  cudaSetDevice(g.device);
+  cudaStreamSynchronize(g.st);
+  g.words[0].release();
+  g.words[1].release();
+  g.accept.release();
+  g.consumed.release();
+  g.qp_cand.release();
+  g.energy.release();
+  g.qp0.release();
+  g.block_counts.release();
+  g.cand_idx.release();
+  g.scal.release();
+  g.crln.release();
+  g.counters.release();
+  g.status_hist.release();
+  g.queue.release();
+  g.fail_flag.release();
+  g.fail_list.release();
+  g.fail_count.release();
+  g.items.release();
+  g.m0_partials.release();
+  g.m0_out.release();
+  g.f_cf.release();
+  g.f_nu.release();
+  g.f_sf.release();
+  g.f_a.release();
+  g.f_b.release();
+  if (g.d_tab) cudaFree(g.d_tab);
+  if (g.d_mt) cudaFree(g.d_mt);
+  for (auto &e : g.ev)
+    if (e) cudaEventDestroy(e);
+  if (g.st) cudaStreamDestroy(g.st);
+  g = Ctx();
+}
+
+}  // extern "C"

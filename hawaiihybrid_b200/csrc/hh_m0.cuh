@@ -1,0 +1,180 @@
+// Zeroth spectral moment by plain Monte Carlo over phase space, all
+// temperatures in one launch.
+//
+// The reference integrates jac * |mu(q)|^2 * exp(-H/kT) over phase space with
+// VEGAS (src/hep_hawaii.cpp:148-201) and scales by ZeroCoeff / pf_analytic
+// (src/driver.c:3425-3431).  With R uniform on [Rmin, Rmax], isotropic angles
+// and momenta drawn from exp(-K/kT) (the p_generator distribution), the
+// momentum integral cancels pf_analytic except for its configurational part:
+//   M0(T) = ZeroCoeff * 4 pi (Rmax - Rmin) * < R^2 |mu|^2 exp(-V/kT) 1[filter] >
+// where the free+metastable filter keeps H = K + V >= 0 (bound: H <= 0).
+// Only K enters, and K = kT * kappa with kappa half a chi^2 variable of 3
+// (atom-atom) or 5 (linear-atom) degrees of freedom; it is drawn with
+// Box-Muller sums, so one phase-space sample serves every temperature.
+//
+// Random numbers: Philox4x32-10, counter (i_lo, i_hi, block, 0), key = seed,
+// uniforms ((w >> 8) + 0.5) * 2^-24, which are exact in FP32 and FP64, so the
+// FP32 and FP64 integrands see the same sample.
+//
+// Sums: per thread FP64 compensated sums of w and plain sums of w^2 per
+// temperature, a fixed-order block reduction, then one fixed-order pass over
+// the block partials.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "hh_consts.h"
+#include "hh_physics.cuh"
+#include "hh_traj.cuh"
+
+namespace hh {
+
+constexpr int M0_MAXT = 16;  // temperatures per launch chunk
+
+struct M0Args {
+  int sys;
+  double Rmin, Rmax;
+  int pair_state;
+  int nT;
+  double invkT[M0_MAXT];   // Hartree^-1
+  uint64_t n_samples, offset, seed;
+};
+
+__device__ __forceinline__ void philox4x32_10(uint32_t c0, uint32_t c1, uint32_t c2, uint32_t c3,
+                                              uint32_t k0, uint32_t k1, uint32_t out[4]) {
+#pragma unroll
+  for (int r = 0; r < 10; ++r) {
+    uint32_t lo0 = 0xD2511F53u * c0, hi0 = __umulhi(0xD2511F53u, c0);
+    uint32_t lo1 = 0xCD9E8D57u * c2, hi1 = __umulhi(0xCD9E8D57u, c2);
+    uint32_t n0 = hi1 ^ c1 ^ k0, n2 = hi0 ^ c3 ^ k1;
+    c0 = n0;
+    c1 = lo1;
+    c2 = n2;
+    c3 = lo0;
+    k0 += 0x9E3779B9u;
+    k1 += 0xBB67AE85u;
+  }
+  out[0] = c0;
+  out[1] = c1;
+  out[2] = c2;
+  out[3] = c3;
+}
+
+template <typename T> __device__ __forceinline__ T u24(uint32_t w) {
+  return (T(w >> 8) + T(0.5)) * T(1.0 / 16777216.0);
+}
+
+template <int SYS, typename PHYS, bool COMP>
+__global__ void __launch_bounds__(256) m0_kernel(M0Args a, const Co2arTablesGlobal *gtab,
+                                                 double *partials) {
+  extern __shared__ unsigned char smem_raw[];
+  Co2arTables<PHYS> *tb = reinterpret_cast<Co2arTables<PHYS> *>(smem_raw);
+  if (SYS == SYS_CO2AR) load_tables<PHYS>(tb, gtab);
+  __syncthreads();
+  double s[M0_MAXT], c[M0_MAXT], q[M0_MAXT];
+  PHYS ikT[M0_MAXT];
+#pragma unroll
+  for (int t = 0; t < M0_MAXT; ++t) {
+    s[t] = c[t] = q[t] = 0.0;
+    ikT[t] = PHYS(a.invkT[t]);
+  }
+  const PHYS Rmin = PHYS(a.Rmin), dR = PHYS(a.Rmax - a.Rmin);
+  const PHYS twopi = PHYS(2.0 * HH_PI);
+  const uint32_t k0 = (uint32_t)a.seed, k1 = (uint32_t)(a.seed >> 32);
+  const uint64_t stride = (uint64_t)gridDim.x * blockDim.x;
+  for (uint64_t i = blockIdx.x * (uint64_t)blockDim.x + threadIdx.x; i < a.n_samples; i += stride) {
+    uint64_t id = a.offset + i;
+    uint32_t w[12];
+    philox4x32_10((uint32_t)id, (uint32_t)(id >> 32), 0u, 0u, k0, k1, w);
+    philox4x32_10((uint32_t)id, (uint32_t)(id >> 32), 1u, 0u, k0, k1, w + 4);
+    philox4x32_10((uint32_t)id, (uint32_t)(id >> 32), 2u, 0u, k0, k1, w + 8);
+    PHYS R = Rmin + dR * u24<PHYS>(w[0]);
+    PHYS zc = cos(twopi * u24<PHYS>(w[8]));
+    PHYS V, mu2, kappa;
+    if (SYS == SYS_HEAR) {
+      PHYS dV;
+      hear_V_dV<PHYS>(R, V, dV);
+      PHYS d = hear_dip<PHYS>(R);
+      mu2 = d * d;
+      kappa = -log(u24<PHYS>(w[5])) - log(u24<PHYS>(w[7])) * zc * zc;
+    } else {
+      // x = cos(angle between r^ and u^) from the sampled lab angles
+      PHYS Phi = twopi * u24<PHYS>(w[1]);
+      PHYS cT = PHYS(2) * u24<PHYS>(w[2]) - PHYS(1);
+      PHYS ph = twopi * u24<PHYS>(w[3]);
+      PHYS ct = PHYS(2) * u24<PHYS>(w[4]) - PHYS(1);
+      PHYS sT = sqrt((PHYS(1) - cT) * (PHYS(1) + cT));
+      PHYS st = sqrt((PHYS(1) - ct) * (PHYS(1) + ct));
+      PHYS x = sT * st * cos(Phi - ph) + cT * ct;
+      PHYS VR, Vx;
+      co2ar_pes<PHYS, COMP>(tb->pes, tb->fpes, tb->rbound, tb->rlo, R, x, V, VR, Vx, true);
+      PHYS dz, ax;
+      co2ar_dip<PHYS, COMP>(tb->dipx, tb->dipz, tb->fdip, tb->rbound, tb->rlo, R, x, dz, ax);
+      mu2 = dz * dz + ax * ax * (PHYS(1) - x) * (PHYS(1) + x);
+      kappa = -log(u24<PHYS>(w[5])) - log(u24<PHYS>(w[6])) - log(u24<PHYS>(w[7])) * zc * zc;
+    }
+    PHYS base = R * R * mu2;
+#pragma unroll
+    for (int t = 0; t < M0_MAXT; ++t) {
+      if (t < a.nT) {
+        PHYS H = kappa / ikT[t] + V;
+        bool keep = true;
+        if (a.pair_state == 1) keep = (H >= PHYS(0));
+        else if (a.pair_state == 2) keep = (H <= PHYS(0));
+        double wv = keep ? double(base * exp(-V * ikT[t])) : 0.0;
+        // compensated accumulation of w, plain accumulation of w^2
+        double y = wv - c[t];
+        double tt = s[t] + y;
+        c[t] = (tt - s[t]) - y;
+        s[t] = tt;
+        q[t] += wv * wv;
+      }
+    }
+  }
+  // block reduction in a fixed order
+  __shared__ double red[2][M0_MAXT][8];
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+  for (int t = 0; t < M0_MAXT; ++t) {
+    double v = s[t] - c[t], vq = q[t];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) {
+      v += __shfl_down_sync(0xffffffffu, v, o);
+      vq += __shfl_down_sync(0xffffffffu, vq, o);
+    }
+    if (lane == 0) {
+      red[0][t][warp] = v;
+      red[1][t][warp] = vq;
+    }
+  }
+  __syncthreads();
+  if (threadIdx.x < M0_MAXT) {
+    int t = threadIdx.x;
+    double v = 0.0, vq = 0.0;
+    for (int wi = 0; wi < (int)(blockDim.x >> 5); ++wi) {
+      v += red[0][t][wi];
+      vq += red[1][t][wi];
+    }
+    partials[((size_t)blockIdx.x * M0_MAXT + t) * 2 + 0] = v;
+    partials[((size_t)blockIdx.x * M0_MAXT + t) * 2 + 1] = vq;
+  }
+}
+
+// fixed-order compensated sum of the block partials
+__global__ void m0_finalize_kernel(const double *partials, int n_blocks, double *out) {
+  int t = threadIdx.x;
+  if (t >= M0_MAXT) return;
+  double s = 0.0, c = 0.0, q = 0.0;
+  for (int b = 0; b < n_blocks; ++b) {
+    double y = partials[((size_t)b * M0_MAXT + t) * 2] - c;
+    double tt = s + y;
+    c = (tt - s) - y;
+    s = tt;
+    q += partials[((size_t)b * M0_MAXT + t) * 2 + 1];
+  }
+  out[t * 2] = s;
+  out[t * 2 + 1] = q;
+}
+
+}  // namespace hh

@@ -1,0 +1,45 @@
+// Sampler translation unit of libhh_cuda.so (built with -fmad=false).
+#include "hh_internal.h"
+#include "hh_sampler.cuh"
+
+namespace hh {
+
+cudaError_t launch_mt_seed(uint32_t seed, uint32_t *state, cudaStream_t st) {
+  mt_seed_kernel<<<(MT_N + 255) / 256, 256, 0, st>>>(seed, state);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_mt_generate(uint32_t *state, uint32_t *out, long long n_blocks, cudaStream_t st) {
+  if (n_blocks <= 0) return cudaSuccess;
+  mt_generate_kernel<<<1, 256, 0, st>>>(state, out, n_blocks);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_candidates(int sys, double mu, double II, double T, double Rmin, double Rmax,
+                              double pesmin, int pair_state, const Co2arTablesGlobal *gtab,
+                              const uint32_t *words, long long n_words, long long word_base, int D,
+                              long long n_cand, unsigned char *accept, unsigned char *consumed,
+                              double *qp, double *energy, unsigned long long *first_irregular,
+                              cudaStream_t st) {
+  SamplerArgs a{sys, mu, II, T, Rmin, Rmax, pesmin, pair_state};
+  size_t smem = (sys == SYS_CO2AR) ? sizeof(Co2arTables<double>) : 0;
+  long long blocks = (n_cand + 255) / 256;
+  candidate_kernel<<<(unsigned)blocks, 256, smem, st>>>(a, gtab, words, n_words, word_base, D,
+                                                         n_cand, accept, consumed, qp, energy,
+                                                         first_irregular);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_compact(const unsigned char *accept, const double *qp_cand, long long n,
+                           long long limit, int QP, long long out_base, long long out_cap,
+                           double *qp_out, long long *cand_index_out, unsigned int *block_counts,
+                           unsigned long long *total, cudaStream_t st) {
+  long long blocks = (n + 1023) / 1024;
+  count_kernel<<<(unsigned)blocks, 1024, 0, st>>>(accept, n, limit, block_counts);
+  scan_kernel<<<1, 1024, 0, st>>>(block_counts, (int)blocks, total);
+  scatter_kernel<<<(unsigned)blocks, 1024, 0, st>>>(accept, qp_cand, n, limit, block_counts, QP,
+                                                     out_base, out_cap, qp_out, cand_index_out, 0);
+  return cudaGetLastError();
+}
+
+}  // namespace hh

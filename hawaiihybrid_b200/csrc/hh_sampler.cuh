@@ -1,0 +1,286 @@
+// Initial-condition sampler on the GPU.
+//
+// The reference draws every candidate phase point from one MT19937 stream
+// (thirdparty/mtwist.c, seeded by mt_seed32 in init_ms, src/hawaii.c:157-163)
+// and consumes a fixed number of words per candidate (src/hawaii.c:1206-1421):
+//   q_generator: R, Phi, Theta (+ phi1, theta1 for a linear monomer)
+//   p_generator: 3 (+2) Box-Muller normals, 2 words each
+//   reject:      1 word
+// i.e. D = 10 (atom-atom) or 16 (linear-atom) words.  A Box-Muller draw only
+// retries when its first word is exactly 0 (log(0) = -inf).
+//
+// GPU mapping:
+//  1. mt_generate: one CTA advances the MT state 624 words at a time with a
+//     three-phase parallel refresh and writes the tempered words to HBM;
+//  2. candidates: one thread per candidate c reads the words [c*D, (c+1)*D),
+//     restates q_generator/p_generator/Hamiltonian/reject/pair-state filter in
+//     FP64 with the reference's operation order, and flags acceptance;
+//  3. count/scan/scatter: accepted candidates are compacted in candidate order,
+//     which is the order the reference's while-loop accepts them.
+// A zero word at a Box-Muller position shifts every later candidate's window:
+// the candidate kernel reports the first such candidate and the host restarts
+// the following round right after it.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "hh_consts.h"
+#include "hh_internal.h"
+#include "hh_physics.cuh"
+#include "hh_traj.cuh"
+
+namespace hh {
+
+__device__ __forceinline__ uint32_t mt_twist(uint32_t a, uint32_t b, uint32_t c) {
+  uint32_t y = (a & 0x80000000u) | (b & 0x7fffffffu);
+  return c ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+}
+
+__device__ __forceinline__ uint32_t mt_temper(uint32_t y) {
+  y ^= y >> 11;
+  y ^= (y << 7) & 0x9d2c5680u;
+  y ^= (y << 15) & 0xefc60000u;
+  y ^= y >> 18;
+  return y;
+}
+
+// state[0..623] <- Knuth-69069 seeding (mts_seed32, thirdparty/mtwist.c:372-400):
+// mt[0] = seed, mt[i] = 69069 * mt[i-1] (mod 2^32), i.e. 69069^i * seed
+__global__ void mt_seed_kernel(uint32_t seed, uint32_t *state) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  if (i >= MT_N) return;
+  if (seed == 0) seed = 4357u;
+  uint32_t p = 1u, b = 69069u;
+  for (int e = i; e; e >>= 1) {
+    if (e & 1) p *= b;
+    b *= b;
+  }
+  state[i] = p * seed;
+}
+
+// Advance the generator by n_blocks refreshes, writing 624 tempered words per
+// refresh to out.  One CTA of 256 threads; the state lives in shared memory.
+__global__ void __launch_bounds__(256) mt_generate_kernel(uint32_t *state, uint32_t *out,
+                                                          long long n_blocks) {
+  __shared__ uint32_t mt[MT_N];
+  for (int i = threadIdx.x; i < MT_N; i += blockDim.x) mt[i] = state[i];
+  __syncthreads();
+  const int tid = threadIdx.x;
+  for (long long b = 0; b < n_blocks; ++b) {
+    uint32_t v;
+    // phase A: i in [0, 227) depends on old words only
+    if (tid < MT_N - MT_M) v = mt_twist(mt[tid], mt[tid + 1], mt[tid + MT_M]);
+    __syncthreads();
+    if (tid < MT_N - MT_M) mt[tid] = v;
+    __syncthreads();
+    // phase B: i in [227, 454) uses new words i-227 from phase A
+    {
+      int i = tid + (MT_N - MT_M);
+      if (tid < MT_N - MT_M) v = mt_twist(mt[i], mt[i + 1], mt[i - (MT_N - MT_M)]);
+      __syncthreads();
+      if (tid < MT_N - MT_M) mt[i] = v;
+      __syncthreads();
+    }
+    // phase C: i in [454, 624); the last word wraps to the new mt[0]
+    {
+      int i = tid + 2 * (MT_N - MT_M);
+      if (i < MT_N) v = mt_twist(mt[i], mt[(i + 1) % MT_N], mt[i - (MT_N - MT_M)]);
+      __syncthreads();
+      if (i < MT_N) mt[i] = v;
+      __syncthreads();
+    }
+    uint32_t *o = out + b * MT_N;
+    for (int i = tid; i < MT_N; i += blockDim.x) o[i] = mt_temper(mt[i]);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < MT_N; i += blockDim.x) state[i] = mt[i];
+}
+
+struct SamplerArgs {
+  int sys;
+  double mu, II;
+  double T;
+  double Rmin, Rmax, pesmin;
+  int pair_state;  // 1 free+metastable, 2 bound, 3 all
+};
+
+// reference operation order is kept; FP contraction is disabled for this code
+// by building with -fmad=false on the sampler translation unit
+__device__ __forceinline__ double mt_d(const uint32_t *w, long long &pos) {
+  return double(w[pos++]) * (1.0 / 4294967296.0);
+}
+
+__device__ __forceinline__ double bm_normal(const uint32_t *w, long long &pos, long long limit,
+                                            int &retries, bool &overrun) {
+  for (;;) {
+    if (pos + 2 > limit) { overrun = true; return 0.0; }
+    double U = mt_d(w, pos);
+    double V = mt_d(w, pos);
+    double logU = log(U);
+    if (isnan(logU) || isinf(logU)) { ++retries; continue; }
+    return 1.0 * sqrt(-2 * logU) * cos(2.0 * HH_PI * V);
+  }
+}
+
+// kinetic energy (src/hawaii.c:1041-1137) and potential for one phase point
+__device__ __forceinline__ double kinetic(const SamplerArgs &a, const double *qp) {
+  double mu = a.mu;
+  double pPhi = qp[1], Theta = qp[2], pTheta = qp[3], R = qp[4], pR = qp[5];
+  double sT = sin(Theta);
+  double K = pR * pR / (2.0 * mu) + pTheta * pTheta / (2.0 * mu * R * R) +
+             pPhi * pPhi / (2.0 * mu * R * R * sT * sT);
+  if (a.sys == SYS_CO2AR) {
+    double I = a.II, pphi = qp[7], th = qp[8], pth = qp[9];
+    double s = sin(th);
+    K += pth * pth / (2.0 * I) + pphi * pphi / (2.0 * I * s * s);
+  }
+  return K;
+}
+
+__device__ __forceinline__ double potential(const SamplerArgs &a, const Co2arTables<double> *tb,
+                                            const double *qp) {
+  if (a.sys == SYS_HEAR) {
+    double V, dV;
+    hear_V_dV<double>(qp[4], V, dV);
+    return V;
+  }
+  double y[12];
+  qp_to_state<SYS_CO2AR>(qp, y);
+  double R = sqrt(y[0] * y[0] + y[1] * y[1] + y[2] * y[2]);
+  double x = (y[0] * y[6] + y[1] * y[7] + y[2] * y[8]) / R;
+  double V, VR, Vx;
+  co2ar_pes<double, false>(tb->pes, tb->fpes, tb->rbound, tb->rlo, R, x, V, VR, Vx, true);
+  return V;
+}
+
+// one thread per candidate; words of candidate c start at word_base + c*D
+__global__ void __launch_bounds__(256) candidate_kernel(
+    SamplerArgs a, const Co2arTablesGlobal *gtab, const uint32_t *words, long long n_words,
+    long long word_base, int D, long long n_cand, unsigned char *accept, unsigned char *consumed,
+    double *qp_out, double *energy_out, unsigned long long *first_irregular) {
+  extern __shared__ unsigned char smem_raw[];
+  Co2arTables<double> *tb = reinterpret_cast<Co2arTables<double> *>(smem_raw);
+  if (a.sys == SYS_CO2AR) load_tables<double>(tb, gtab);
+  __syncthreads();
+  long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (c >= n_cand) return;
+  long long pos = word_base + c * D;
+  const long long limit = n_words;
+  int retries = 0;
+  bool overrun = false;
+  const int QP = (a.sys == SYS_HEAR) ? 6 : 10;
+  double qp[10];
+  double RMIN = a.Rmin, RMAX = a.Rmax, T = a.T;
+  // q_generator (src/hawaii.c:1232-1290)
+  double R3 = mt_d(words, pos) * (RMAX * RMAX * RMAX - RMIN * RMIN * RMIN) + RMIN * RMIN * RMIN;
+  qp[4] = pow(R3, 1.0 / 3.0);
+  qp[0] = mt_d(words, pos) * 2.0 * HH_PI;
+  qp[2] = acos(2.0 * mt_d(words, pos) - 1.0);
+  if (a.sys == SYS_CO2AR) {
+    qp[6] = mt_d(words, pos) * 2.0 * HH_PI;
+    qp[8] = acos(2.0 * mt_d(words, pos) - 1.0);
+  }
+  // p_generator (src/hawaii.c:1292-1380)
+  double sqrt_MUKT = sqrt(a.mu / HH_HKT * T);
+  double sinTheta = sin(qp[2]);
+  double x0 = bm_normal(words, pos, limit, retries, overrun);
+  double x1 = bm_normal(words, pos, limit, retries, overrun);
+  double x2 = bm_normal(words, pos, limit, retries, overrun);
+  qp[1] = sqrt_MUKT * qp[4] * sinTheta * x0;
+  qp[3] = sqrt_MUKT * qp[4] * x1;
+  qp[5] = sqrt_MUKT * x2;
+  if (a.sys == SYS_CO2AR) {
+    double sqrt_IIKT = sqrt(a.II / HH_HKT * T);
+    double sin_theta = sin(qp[8]);
+    double m0 = bm_normal(words, pos, limit, retries, overrun);
+    double m1 = bm_normal(words, pos, limit, retries, overrun);
+    qp[7] = sqrt_IIKT * sin_theta * m1;
+    qp[9] = sqrt_IIKT * m0;
+  }
+  if (pos + 1 > limit) overrun = true;
+  bool acc = false;
+  double E = 0.0;
+  if (!overrun) {
+    // Hamiltonian, then reject() (src/hawaii.c:1382-1421), then the filter (2981-2994)
+    double kin = kinetic(a, qp);
+    double pot = potential(a, tb, qp);
+    E = kin + pot;
+    double u = mt_d(words, pos);
+    double Mval = exp(-a.pesmin * HH_HKT / T);
+    double M = 1.5 * Mval;
+    double proposal = exp(-kin * HH_HKT / T);
+    double desired = exp(-(kin + pot) * HH_HKT / T);
+    double weight = desired / proposal / M;
+    acc = !(weight < u);
+    if (a.pair_state == 1 && E < 0.0) acc = false;
+    if (a.pair_state == 2 && E > 0.0) acc = false;
+  }
+  if (retries || overrun) atomicMin(first_irregular, (unsigned long long)c);
+  accept[c] = acc ? 1 : 0;
+  consumed[c] = overrun ? 0 : (unsigned char)(pos - (word_base + c * D));
+  for (int i = 0; i < QP; ++i) qp_out[c * QP + i] = qp[i];
+  energy_out[c] = E;
+}
+
+// ---- ordered compaction of accepted candidates ----
+__global__ void __launch_bounds__(1024) count_kernel(const unsigned char *accept, long long n,
+                                                     long long limit, unsigned int *block_counts) {
+  long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  int v = (c < n && c <= limit) ? accept[c] : 0;
+  int cnt = __syncthreads_count(v);
+  if (threadIdx.x == 0) block_counts[blockIdx.x] = cnt;
+}
+
+// exclusive scan of block counts in one CTA (n_blocks is small)
+__global__ void __launch_bounds__(1024) scan_kernel(unsigned int *counts, int n_blocks,
+                                                    unsigned long long *total) {
+  __shared__ unsigned int partial[1024];
+  __shared__ unsigned long long carry;
+  if (threadIdx.x == 0) carry = 0;
+  __syncthreads();
+  for (int base = 0; base < n_blocks; base += 1024) {
+    int i = base + threadIdx.x;
+    unsigned int v = (i < n_blocks) ? counts[i] : 0u;
+    partial[threadIdx.x] = v;
+    __syncthreads();
+    for (int off = 1; off < 1024; off <<= 1) {
+      unsigned int t = (threadIdx.x >= off) ? partial[threadIdx.x - off] : 0u;
+      __syncthreads();
+      partial[threadIdx.x] += t;
+      __syncthreads();
+    }
+    if (i < n_blocks) counts[i] = (unsigned int)(carry + partial[threadIdx.x] - v);
+    __syncthreads();
+    if (threadIdx.x == 1023) carry += partial[1023];
+    __syncthreads();
+  }
+  if (threadIdx.x == 0) *total = carry;
+}
+
+__global__ void __launch_bounds__(1024) scatter_kernel(const unsigned char *accept,
+                                                       const double *qp_cand, long long n,
+                                                       long long limit, const unsigned int *offsets,
+                                                       int QP, long long out_base, long long out_cap,
+                                                       double *qp_out, long long *cand_index_out,
+                                                       long long cand_base) {
+  __shared__ unsigned int warp_tot[32];
+  long long c = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  int v = (c < n && c <= limit) ? accept[c] : 0;
+  unsigned int ballot = __ballot_sync(0xffffffffu, v);
+  int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  unsigned int before = __popc(ballot & ((1u << lane) - 1u));
+  if (lane == 0) warp_tot[warp] = __popc(ballot);
+  __syncthreads();
+  unsigned int woff = 0;
+  for (int w = 0; w < warp; ++w) woff += warp_tot[w];
+  if (v) {
+    long long dst = out_base + offsets[blockIdx.x] + woff + before;
+    if (dst < out_cap) {
+      for (int i = 0; i < QP; ++i) qp_out[dst * QP + i] = qp_cand[c * QP + i];
+      if (cand_index_out) cand_index_out[dst] = cand_base + c;
+    }
+  }
+}
+
+}  // namespace hh

@@ -1,0 +1,339 @@
+"""Host-side mirror of HAWAIIHYBRID's trajectory-path interface over libhh_cuda.so.
+
+Names, argument meaning and units follow the reference's C API
+(src/hawaii.h): MonomerType / PairState values, CalcParams fields,
+init_ms, calculate_correlation_and_save, idct_cf_to_sf, the CF/SF text
+formats and analytic_full_partition_function_by_V.  Every numerical step runs
+in the CUDA library; this module only marshals arguments, loops over
+iterations and writes files.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import dataclasses
+import math
+import os
+import time
+from typing import Optional, Sequence
+
+import numpy as np
+
+from . import _lib
+from ._lib import HHError, check
+
+# ---- constants (src/constants.h:8-53) ----
+ALU = 5.29177210903e-11
+Boltzmann = 1.380649e-23
+Hartree = 4.3597447222071e-18
+HTOCM = 2.1947463136320e5
+HkT = Hartree / Boltzmann
+ZeroCoeff = 0.00361479637 / (4.0 * math.pi)
+RAMTOAMU = 1822.888485332
+m_He = 4.00260325413 * RAMTOAMU
+m_Ar = 39.9623831237 * RAMTOAMU
+m_C = 12.0 * RAMTOAMU
+m_O = 15.994914619598 * RAMTOAMU
+l_CO2 = 4.398
+II_CO2 = m_O / 2.0 * l_CO2 * l_CO2
+
+# ---- MonomerType (src/hawaii.h:183-190) ----
+ATOM = 0
+LINEAR_MOLECULE = 4
+
+# ---- PairState (src/hawaii.h:290-300) ----
+PAIR_STATE_NONE = 0
+PAIR_STATE_FREE_AND_METASTABLE = 1
+PAIR_STATE_BOUND = 2
+PAIR_STATE_ALL = 3
+
+# ---- surfaces available on the device ----
+SYSTEM_HE_AR = _lib.HH_SYSTEM_HE_AR
+SYSTEM_CO2_AR = _lib.HH_SYSTEM_CO2_AR
+
+PRECISION_FP64 = _lib.HH_PRECISION_FP64
+PRECISION_MIXED = _lib.HH_PRECISION_MIXED
+
+
+@dataclasses.dataclass
+class CalcParams:
+    """Subset of the reference's CalcParams (src/hawaii.h:313-365) used by the path."""
+    ps: int = PAIR_STATE_FREE_AND_METASTABLE
+    sampler_Rmin: float = 4.0
+    sampler_Rmax: float = 40.0
+    pesmin: float = 0.0
+    sampling_time: float = 200.0
+    MaxTrajectoryLength: int = 65536
+    cvode_tolerance: float = 1e-12
+    niterations: int = 1
+    total_trajectories: int = 0
+    cf_filename: Optional[str] = None
+    Rcut: float = 40.0
+    partial_partition_function_ratio: float = 0.0
+    # device-path knobs (no reference counterpart)
+    mixed_tolerance: float = 1e-8
+    max_steps: int = 50000
+
+    def to_c(self) -> _lib.CalcParamsC:
+        return _lib.CalcParamsC(
+            int(self.ps), float(self.sampler_Rmin), float(self.sampler_Rmax), float(self.pesmin),
+            float(self.sampling_time), int(self.MaxTrajectoryLength), float(self.Rcut),
+            float(self.cvode_tolerance), float(self.partial_partition_function_ratio),
+            float(self.mixed_tolerance), int(self.max_steps))
+
+
+@dataclasses.dataclass
+class MoleculeSystem:
+    """The pair being simulated (src/hawaii.h:267-284) bound to a device surface."""
+    system_id: int
+    mu: float
+    m1_type: int
+    m2_type: int
+    II1: tuple = (0.0, 0.0, 0.0)
+    II2: tuple = (0.0, 0.0, 0.0)
+    seed: int = 0
+    device: int = 0
+
+    @property
+    def QP_SIZE(self) -> int:
+        return 6 + (self.m1_type % 100) + (self.m2_type % 100)
+
+    @property
+    def Q_SIZE(self) -> int:
+        return self.QP_SIZE // 2
+
+    def desc(self) -> _lib.SystemDesc:
+        return _lib.SystemDesc(self.system_id, self.mu, self.m1_type, self.m2_type,
+                               (C.c_double * 3)(*self.II1), (C.c_double * 3)(*self.II2))
+
+
+def init_ms(mu: float, t1: int, t2: int, II1: Optional[Sequence[float]], II2: Optional[Sequence[float]],
+            seed: int, system_id: Optional[int] = None, device: int = 0) -> MoleculeSystem:
+    """init_ms (src/hawaii.c:173-270): bind the pair to the device and seed the sampler stream.
+
+    system_id names the device surface (the role of the plugin .so in the reference);
+    it defaults from the monomer types (ATOM+ATOM -> He-Ar, LINEAR+ATOM -> CO2-Ar)."""
+    if mu <= 0:
+        raise ValueError(f"invalid reduced mass ({mu:.5e}) -- must be positive")
+    if system_id is None:
+        if t1 == ATOM and t2 == ATOM:
+            system_id = SYSTEM_HE_AR
+        elif t1 == LINEAR_MOLECULE and t2 == ATOM:
+            system_id = SYSTEM_CO2_AR
+        else:
+            raise HHError(_lib.HH_E_UNSUPPORTED_SYSTEM, "no device surface for these monomers")
+    ms = MoleculeSystem(system_id, mu, t1, t2, tuple(II1 or (0, 0, 0)) + (0.0,) * (3 - len(II1 or (0, 0, 0))),
+                        tuple(II2 or (0, 0, 0)) + (0.0,) * (3 - len(II2 or (0, 0, 0))), seed, device)
+    L = _lib.load()
+    check(L.hh_cuda_init(device, C.byref(ms.desc())))
+    check(L.hh_cuda_seed(seed))
+    return ms
+
+
+@dataclasses.dataclass
+class CFnc:
+    t: np.ndarray
+    data: np.ndarray
+    ntraj: float = 0.0
+    Temperature: float = 0.0
+    normalized: bool = False
+
+    @property
+    def len(self) -> int:
+        return int(self.data.size)
+
+
+@dataclasses.dataclass
+class SFnc:
+    nu: np.ndarray
+    data: np.ndarray
+    ntraj: float = 0.0
+    Temperature: float = 0.0
+    normalized: bool = False
+
+    @property
+    def len(self) -> int:
+        return int(self.data.size)
+
+
+def _bind(ms: MoleculeSystem):
+    L = _lib.load()
+    check(L.hh_cuda_init(ms.device, C.byref(ms.desc())))
+    return L
+
+
+def sample_initial_conditions(ms: MoleculeSystem, params: CalcParams, Temperature: float, n: int,
+                              seed: int = 0) -> tuple[np.ndarray, int]:
+    """q_generator + p_generator + reject + pair-state filter for n accepted points."""
+    L = _bind(ms)
+    out = np.empty(n * ms.QP_SIZE, dtype=np.float64)
+    nc = C.c_uint64()
+    pc = params.to_c()
+    check(L.hh_cuda_sample(C.byref(pc), Temperature, seed, n, out, C.byref(nc)))
+    return out.reshape(n, ms.QP_SIZE), int(nc.value)
+
+
+def correlation_iteration(ms: MoleculeSystem, params: CalcParams, Temperature: float, n: int,
+                          precision: int = PRECISION_FP64, seed: int = 0):
+    """One accumulation pass of calculate_correlation_and_save: returns
+    (sum_i ppf * crln_i, n, stats)."""
+    L = _bind(ms)
+    crln = np.zeros(params.MaxTrajectoryLength, dtype=np.float64)
+    ntraj = C.c_double()
+    st = _lib.Stats()
+    pc = params.to_c()
+    check(L.hh_cuda_correlation(C.byref(pc), Temperature, seed, n, precision, crln,
+                                C.byref(ntraj), C.byref(st)))
+    return crln, ntraj.value, st
+
+
+def correlation_from_initial_conditions(ms: MoleculeSystem, params: CalcParams, qp0: np.ndarray,
+                                        precision: int = PRECISION_FP64):
+    """correlation_eval + accumulation over caller-supplied phase points."""
+    L = _bind(ms)
+    qp0 = np.ascontiguousarray(qp0, dtype=np.float64).reshape(-1, ms.QP_SIZE)
+    crln = np.zeros(params.MaxTrajectoryLength, dtype=np.float64)
+    st = _lib.Stats()
+    pc = params.to_c()
+    check(L.hh_cuda_correlation_ic(C.byref(pc), qp0.ravel(), qp0.shape[0], precision, crln,
+                                   C.byref(st)))
+    return crln, st
+
+
+def calculate_correlation_and_save(ms: MoleculeSystem, params: CalcParams, Temperature: float,
+                                   precision: int = PRECISION_FP64, log=print) -> CFnc:
+    """calculate_correlation_and_save (src/hawaii.c:2795-3119): niterations passes of
+    total_trajectories/niterations trajectories, the CF file rewritten after each
+    pass, the result normalised by ntraj."""
+    if params.partial_partition_function_ratio <= 0:
+        raise ValueError("partial_partition_function_ratio must be provided (> 0)")
+    if params.total_trajectories <= 0 or params.niterations < 1:
+        raise ValueError("total_trajectories and niterations must be positive")
+    N = params.MaxTrajectoryLength
+    total = CFnc(t=np.linspace(0.0, params.sampling_time * (N - 1), N), data=np.zeros(N),
+                 ntraj=0.0, Temperature=Temperature, normalized=False)
+    per_iter = params.total_trajectories // params.niterations
+    fp = open(params.cf_filename, "w") if params.cf_filename else None
+    try:
+        for it in range(params.niterations):
+            crln, ntraj, st = correlation_iteration(ms, params, Temperature, per_iter, precision)
+            total.data += crln
+            total.ntraj += ntraj
+            if log:
+                log(f"ITERATION {it + 1}/{params.niterations}: accumulated {int(total.ntraj)} trajectories."
+                    + (f" Saving the temporary result to '{params.cf_filename}'" if fp else ""))
+                m0 = total.data[0] / total.ntraj * ZeroCoeff / ALU ** 3
+                log(f"M0 ESTIMATE FROM CF: {m0:.5e}")
+            if fp:
+                write_correlation_function_ext(fp, total)
+    finally:
+        if fp:
+            fp.close()
+    total.data = total.data / total.ntraj
+    total.normalized = True
+    return total
+
+
+def idct_cf_to_sf(cf: CFnc) -> SFnc:
+    """idct_cf_to_sf (src/hawaii.c:5569-5601).  Like the reference, the Connes
+    apodization is applied to cf.data in place."""
+    L = _lib.load()
+    data = np.ascontiguousarray(cf.data, dtype=np.float64)
+    if data is not cf.data:
+        cf.data = data
+    N = data.size
+    dt = float(cf.t[1] - cf.t[0])
+    nu = np.empty(N)
+    sf = np.empty(N)
+    check(L.hh_cuda_idct_cf_to_sf(data, N, dt, nu, sf))
+    return SFnc(nu=nu, data=sf, ntraj=cf.ntraj, Temperature=cf.Temperature, normalized=cf.normalized)
+
+
+def calculate_m0(ms: MoleculeSystem, params: CalcParams, temperatures: Sequence[float], n_samples: int,
+                 seed: int = 1, precision: int = PRECISION_FP64) -> tuple[np.ndarray, np.ndarray]:
+    """Zeroth moment M0(T) for every temperature from one batch of phase-space samples
+    (the quantity the reference prints as "T = ... => M0", src/driver.c:3425-3431)."""
+    L = _bind(ms)
+    T = np.ascontiguousarray(temperatures, dtype=np.float64)
+    m = np.empty(T.size)
+    e = np.empty(T.size)
+    pc = params.to_c()
+    check(L.hh_cuda_m0(C.byref(pc), T, T.size, n_samples, seed, precision, m, e))
+    return m, e
+
+
+def analytic_full_partition_function_by_V(ms: MoleculeSystem, Temperature: float) -> float:
+    """src/hawaii.c:5071-5090 (ATOM-ATOM and LINEAR_MOLECULE-ATOM)."""
+    if ms.m1_type == ATOM and ms.m2_type == ATOM:
+        return (2.0 * math.pi * ms.mu * Temperature / HkT) ** 1.5
+    if ms.m1_type == LINEAR_MOLECULE and ms.m2_type == ATOM:
+        return 4.0 * math.pi * (2.0 * math.pi * Temperature / HkT) ** 2.5 * ms.mu ** 1.5 * ms.II1[0]
+    raise NotImplementedError("analytic_full_partition_function_by_V")
+
+
+# ---- CF / SF text files (src/hawaii.c:4150-4284, 4502-4597) ----
+def _header(fp, kind: str, T: float, ntraj: float, n: int) -> None:
+    fp.write("# HAWAII HYBRID v0.1\n")
+    fp.write("# Saved on " + time.strftime("%Y-%m-%d %H:%M:%S") + "\n")
+    fp.write(f"# TEMPERATURE: {T:.2f}\n")
+    fp.write(f"# AVERAGE OVER {ntraj:.2f} TRAJECTORIES\n")
+    fp.write(f"# {kind}: {n}\n")
+
+
+def write_correlation_function_ext(fp, cf: CFnc) -> int:
+    """Rewrite an open CF file (truncate, write, flush, fsync)."""
+    fp.seek(0)
+    fp.truncate(0)
+    if not cf.normalized and cf.ntraj <= 0:
+        raise ValueError(f"cannot normalize correlation function: trajectories count is {cf.ntraj:.2f}")
+    _header(fp, "MAXIMUM TRAJECTORY LENGTH", cf.Temperature, cf.ntraj, cf.len)
+    data = cf.data if cf.normalized else cf.data / cf.ntraj
+    fp.writelines(f"{t:.2f} {v:.10e}\n" for t, v in zip(cf.t, data))
+    fp.flush()
+    os.fsync(fp.fileno())
+    return fp.tell()
+
+
+def write_correlation_function(filename: str, cf: CFnc) -> int:
+    with open(filename, "w") as fp:
+        return write_correlation_function_ext(fp, cf)
+
+
+def write_spectral_function(filename: str, sf: SFnc) -> int:
+    with open(filename, "w") as fp:
+        _header(fp, "SPECTRAL FUNCTION LENGTH", sf.Temperature, sf.ntraj, sf.len)
+        data = sf.data if sf.normalized else sf.data / sf.ntraj
+        fp.writelines(f"{n:.10f}   {v:.10e}\n" for n, v in zip(sf.nu, data))
+        fp.flush()
+        os.fsync(fp.fileno())
+        return fp.tell()
+
+
+def _read_table(filename: str):
+    T = None
+    ntraj = None
+    rows = []
+    with open(filename) as fh:
+        for line in fh:
+            if line.startswith("#"):
+                if line.startswith("# TEMPERATURE:"):
+                    T = float(line.split(":")[1])
+                elif line.startswith("# AVERAGE OVER"):
+                    ntraj = float(line.split()[3])
+                continue
+            if line.strip():
+                a, b = line.split()
+                rows.append((float(a), float(b)))
+    if T is None or ntraj is None:
+        raise ValueError(f"incomplete header in '{filename}'")
+    arr = np.array(rows, dtype=np.float64).reshape(-1, 2)
+    return T, ntraj, arr
+
+
+def read_correlation_function(filename: str) -> CFnc:
+    T, ntraj, a = _read_table(filename)
+    return CFnc(t=a[:, 0].copy(), data=a[:, 1].copy(), ntraj=ntraj, Temperature=T, normalized=True)
+
+
+def read_spectral_function(filename: str) -> SFnc:
+    T, ntraj, a = _read_table(filename)
+    return SFnc(nu=a[:, 0].copy(), data=a[:, 1].copy(), ntraj=ntraj, Temperature=T, normalized=True)

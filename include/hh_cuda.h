@@ -1,0 +1,157 @@
+/*
+ * hh_cuda.h -- C ABI of the B200 trajectory library (libhh_cuda.so).
+ *
+ * Drop-in boundary for HAWAIIHYBRID's trajectory hot path.  The host keeps the
+ * reference's C driver, .conf parsing, plugin loading and CF/SF writers; the
+ * per-trajectory loop, the zeroth-moment integral and the CF->SF transform call
+ * into this library instead.  Plain C types only; every function returns
+ * HH_OK (0) or a negative HH_E_* code; output buffers are caller-owned host
+ * memory; device memory is owned by the library.  Calls are synchronous and
+ * must come from one host thread.
+ *
+ * Replaced reference interfaces (file:line in the reference tree):
+ *   hh_cuda_init             setup_pes/setup_dipole plugin binding (src/driver.c:3097-3181)
+ *                            + init_ms (src/hawaii.c:173-270)
+ *   hh_cuda_seed             mt_seed32 in init_ms (src/hawaii.c:157-163)
+ *   hh_cuda_sample           q_generator/p_generator/reject + pair-state filter
+ *                            (src/hawaii.c:1232-1421, 2976-2994)
+ *   hh_cuda_correlation      the accumulation loop of calculate_correlation_and_save
+ *                            (src/hawaii.c:2970-3012) with correlation_eval
+ *                            (src/hawaii.c:2116-2347) per trajectory
+ *   hh_cuda_correlation_ic   correlation_eval over caller-supplied phase points
+ *                            (src/hawaii.c:2116-2347, accumulation 3008)
+ *   hh_cuda_m0               c_mpi_perform_integration(..., INTEGRAND_M0, ...)
+ *                            (src/hep_hawaii.h:16, src/hep_hawaii.cpp:148-201) and
+ *                            the M0 scaling of src/driver.c:3425-3431
+ *   hh_cuda_idct_cf_to_sf    SFnc idct_cf_to_sf(CFnc) (src/hawaii.h:648,
+ *                            src/hawaii.c:5569-5601)
+ */
+#ifndef HH_CUDA_H_
+#define HH_CUDA_H_
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* error codes */
+#define HH_OK 0
+#define HH_E_NOT_INITIALIZED (-1)
+#define HH_E_INVALID_ARGUMENT (-2)
+#define HH_E_CUDA (-3)
+#define HH_E_UNSUPPORTED_SYSTEM (-4)
+#define HH_E_OUT_OF_MEMORY (-5)
+#define HH_E_NOT_POWER_OF_TWO (-6)
+#define HH_E_SAMPLER (-7)
+#define HH_E_NO_DEVICE (-8)
+
+/* MonomerType values of the reference (src/hawaii.h:183-190) */
+#define HH_MONOMER_ATOM 0
+#define HH_MONOMER_LINEAR_MOLECULE 4
+
+/* PairState of the reference (src/hawaii.h:290-300) */
+#define HH_PAIR_STATE_FREE_AND_METASTABLE 1
+#define HH_PAIR_STATE_BOUND 2
+#define HH_PAIR_STATE_ALL 3
+
+/* device surfaces; a plugin .so names its surface by exporting
+ * int hh_cuda_system_id(void) next to pes_lab/dpes_lab/dipole_lab */
+#define HH_SYSTEM_HE_AR 1
+#define HH_SYSTEM_CO2_AR 2
+
+/* precision modes */
+#define HH_PRECISION_FP64 0  /* FP64 surfaces and stages: the plain drop-in path */
+#define HH_PRECISION_MIXED 1 /* FP32 surfaces (compensated sums) and stages, FP64 state */
+
+typedef struct {
+    int system_id;          /* HH_SYSTEM_* */
+    double mu;              /* pair reduced mass, a.u. (pair_reduced_mass) */
+    int monomer1_type;      /* HH_MONOMER_* */
+    int monomer2_type;
+    double II1[3];          /* inertia of monomer 1, a.u. (II = {...}) */
+    double II2[3];
+} hh_system_desc;
+
+typedef struct {
+    int pair_state;                 /* HH_PAIR_STATE_* (PAIR_STATE) */
+    double sampler_Rmin;            /* bohr */
+    double sampler_Rmax;            /* bohr */
+    double pesmin;                  /* Hartree */
+    double sampling_time;           /* a.t.u. */
+    size_t MaxTrajectoryLength;
+    double Rcut;                    /* bohr */
+    double cvode_tolerance;         /* rtol = atol of the FP64 path */
+    double partial_partition_function_ratio;
+    double mixed_tolerance;         /* rtol = atol of the mixed path; 0 selects 1e-8 */
+    long max_steps;                 /* internal steps between two samples; 0 selects 50000 */
+} hh_calc_params;
+
+typedef struct {
+    uint64_t n_candidates;          /* sampler candidates drawn */
+    uint64_t n_accepted;
+    uint64_t n_steps;               /* accepted integrator steps (all half-trajectories) */
+    uint64_t n_rejected_steps;
+    uint64_t n_rhs;                 /* right-hand-side evaluations */
+    uint64_t n_samples;             /* dipole samples */
+    uint64_t n_dense;               /* steps that needed dense output */
+    uint64_t n_failed;              /* trajectories dropped like the reference's `return 1` */
+    uint64_t status[8];             /* per half-trajectory: OK, MAXSTEPS, H_UNDERFLOW,
+                                       NAN_DIPOLE, OVERFLOW, JUMP */
+    double sample_ms;               /* device time of the sampler (CUDA events) */
+    double traj_ms;                 /* device time of the trajectory kernel(s) */
+    double total_ms;                /* device time of the whole call */
+} hh_stats;
+
+/* Select the device and the surface; uploads coefficient tables.  Re-callable. */
+int hh_cuda_init(int device, const hh_system_desc *sys);
+
+/* Reseed the sampler stream exactly like mt_seed32(seed) in init_ms. */
+int hh_cuda_seed(uint32_t seed);
+
+/* Draw n accepted initial phase points (reference layout, QP_SIZE doubles each)
+ * from the stream; seed > 0 reseeds first, seed == 0 continues the stream. */
+int hh_cuda_sample(const hh_calc_params *p, double T, uint32_t seed, uint64_t n,
+                   double *qp_out, uint64_t *n_candidates);
+
+/* One CORRELATION_SINGLE iteration: sample n_accept phase points (seed as in
+ * hh_cuda_sample), integrate both branches of every trajectory and return
+ * crln_sum[k] = sum_i ppf * crln_i[k] (length MaxTrajectoryLength) and the
+ * trajectory count to add to ntraj. */
+int hh_cuda_correlation(const hh_calc_params *p, double T, uint32_t seed, uint64_t n_accept,
+                        int precision_mode, double *crln_sum, double *ntraj, hh_stats *stats);
+
+/* Same, for caller-supplied initial phase points qp0[n][QP_SIZE]. */
+int hh_cuda_correlation_ic(const hh_calc_params *p, const double *qp0, uint64_t n,
+                           int precision_mode, double *crln_sum, hh_stats *stats);
+
+/* M0 at nT temperatures from n_samples phase-space points (Philox stream
+ * `seed`), all temperatures in one launch: m[t] (same units as the reference's
+ * "T = ... => M0") and its one-sigma statistical error err[t]. */
+int hh_cuda_m0(const hh_calc_params *p, const double *T, int nT, uint64_t n_samples,
+               uint64_t seed, int precision_mode, double *m, double *err);
+
+/* CF -> SF: apodizes cf in place (as the reference does), N a power of two. */
+int hh_cuda_idct_cf_to_sf(double *cf, size_t N, double dt, double *nu, double *sf);
+
+const char *hh_cuda_strerror(int code);
+
+/* Test and diagnostic entry points (no counterpart in the reference):
+ * hh_cuda_mt_stream writes the first n words of the MT19937 stream of `seed`
+ * as the sampler consumes them (the stream is left reseeded with `seed`);
+ * hh_cuda_debug_inject makes branch `dir` (0 forward, 1 backward) of
+ * trajectory `traj` of the next correlation calls end with status `status`
+ * (1..5) at sample k, as if its integrator or dipole had failed there; traj < 0
+ * switches injection off. */
+int hh_cuda_mt_stream(uint32_t seed, uint64_t n, uint32_t *out);
+int hh_cuda_debug_inject(int traj, int dir, int k, int status);
+
+/* Release all device memory of the library. */
+void hh_cuda_shutdown(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* HH_CUDA_H_ */

@@ -1,0 +1,997 @@
+/*
+ * CPU oracle for the HAWAIIHYBRID trajectory hot path -- TEST INFRASTRUCTURE ONLY.
+ * See hh_oracle.h for what it restates and how it is pinned.  Only tests/, the
+ * smoke check and bench.py's CPU-baseline leg load it.  Build flags keep
+ * floating-point contraction off so that its arithmetic order is the one written.
+ */
+#define _GNU_SOURCE
+#include "hh_oracle.h"
+
+#include <math.h>
+#include <pthread.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include "../hawaiihybrid_b200/csrc/hh_co2ar_tables.h"
+#include "../hawaiihybrid_b200/csrc/hh_dop853_tableau.h"
+
+/* ---- constants (src/constants.h:8-53, CODATA 2022) ---- */
+#define ALU 5.29177210903e-11
+#define Boltzmann 1.380649e-23
+#define Hartree 4.3597447222071e-18
+#define HTOCM 2.1947463136320e5
+#define ATU 2.4188843265857e-17
+#define LightSpeed_cm 2.99792458e10
+#define ADIPMOMU 8.4783536255e-30
+#define EPSILON0 8.8541878128e-12
+#define HkT (Hartree / Boltzmann)
+#define ZeroCoeff (0.00361479637 / (4.0 * M_PI))
+
+/* ======================================================================== */
+/* MT19937 as configured by mtwist (thirdparty/mtwist.c:372-400, 640-796,   */
+/* thirdparty/mtwist.h:624-634): Knuth-69069 seeding of the 624 words, an   */
+/* immediate refresh, words consumed in generation order, standard tempering,*/
+/* double = word * 2^-32.                                                    */
+/* ======================================================================== */
+static void mt_refresh(hho_mt *s) {
+    uint32_t *m = s->mt;
+    for (int i = 0; i < 624; ++i) {
+        uint32_t y = (m[i] & 0x80000000u) | (m[(i + 1) % 624] & 0x7fffffffu);
+        m[i] = m[(i + 397) % 624] ^ (y >> 1) ^ ((y & 1u) ? 0x9908b0dfu : 0u);
+    }
+    s->idx = 0;
+}
+
+void hho_mt_seed(hho_mt *s, uint32_t seed) {
+    if (seed == 0) seed = 4357u;
+    s->mt[0] = seed;
+    for (int i = 1; i < 624; ++i) s->mt[i] = 69069u * s->mt[i - 1];
+    mt_refresh(s);
+}
+
+uint32_t hho_mt_u32(hho_mt *s) {
+    if (s->idx >= 624) mt_refresh(s);
+    uint32_t y = s->mt[s->idx++];
+    y ^= y >> 11;
+    y ^= (y << 7) & 0x9d2c5680u;
+    y ^= (y << 15) & 0xefc60000u;
+    y ^= y >> 18;
+    return y;
+}
+
+double hho_mt_drand(hho_mt *s) { return (double)hho_mt_u32(s) * (1.0 / 4294967296.0); }
+
+void hho_mt_stream(uint32_t seed, size_t n, uint32_t *out) {
+    hho_mt s;
+    hho_mt_seed(&s, seed);
+    for (size_t i = 0; i < n; ++i) out[i] = hho_mt_u32(&s);
+}
+
+/* ======================================================================== */
+/* Philox4x32-10 (Salmon, Moraes, Dror, Shaw, SC'11)                         */
+/* ======================================================================== */
+void hho_philox4x32_10(const uint32_t ctr[4], const uint32_t key[2], uint32_t out[4]) {
+    uint32_t c0 = ctr[0], c1 = ctr[1], c2 = ctr[2], c3 = ctr[3];
+    uint32_t k0 = key[0], k1 = key[1];
+    for (int r = 0; r < 10; ++r) {
+        uint64_t p0 = (uint64_t)0xD2511F53u * c0;
+        uint64_t p1 = (uint64_t)0xCD9E8D57u * c2;
+        uint32_t n0 = (uint32_t)(p1 >> 32) ^ c1 ^ k0;
+        uint32_t n1 = (uint32_t)p1;
+        uint32_t n2 = (uint32_t)(p0 >> 32) ^ c3 ^ k1;
+        uint32_t n3 = (uint32_t)p0;
+        c0 = n0; c1 = n1; c2 = n2; c3 = n3;
+        k0 += 0x9E3779B9u;
+        k1 += 0xBB67AE85u;
+    }
+    out[0] = c0; out[1] = c1; out[2] = c2; out[3] = c3;
+}
+
+/* ======================================================================== */
+/* He-Ar (PES-IDS/HeAr.h:33-107).  V is an exponential repulsion plus       */
+/* damped dispersion -C_2n f_2n(bR)/R^2n, n = 3..8, with the damping          */
+/* f_2n(x) = 1 - exp(-x) sum_{k<=2n} x^k/k!; the constants are the          */
+/* reference's.  dV/dR is the analytic derivative of the same form.          */
+/* ======================================================================== */
+static const double HEAR_A = 0.2303058634e2;
+static const double HEAR_G1 = 0.163051044e1;   /* exp(-G1 R - G2 R^2) */
+static const double HEAR_G2 = 0.4680016e-1;
+static const double HEAR_B = 0.16274792500000e1;
+static const double HEAR_C[6] = {0.940835513e1, 0.165523018e3, 0.379715796e4,
+                                 0.1165179999e6, 0.466258000e7, 0.236861000e9};
+
+double hho_hear_V(double R) {
+    double x = HEAR_B * R, ex = exp(-x);
+    double term = 1.0, S = 1.0;          /* S = sum_{k<=m} x^k/k! */
+    double V = HEAR_A * exp(-HEAR_G1 * R - HEAR_G2 * R * R);
+    double R2 = R * R, Rp = R2 * R2;     /* R^4 -> multiplied up to R^2n */
+    int m = 0;
+    for (int n = 3; n <= 8; ++n) {
+        while (m < 2 * n) { ++m; term *= x / m; S += term; }
+        Rp *= R2;
+        V -= HEAR_C[n - 3] * (1.0 - ex * S) / Rp;
+    }
+    return V;
+}
+
+double hho_hear_dV(double R) {
+    double x = HEAR_B * R, ex = exp(-x);
+    double term = 1.0, S = 1.0;
+    double dV = HEAR_A * exp(-HEAR_G1 * R - HEAR_G2 * R * R) * (-HEAR_G1 - 2.0 * HEAR_G2 * R);
+    double R2 = R * R, Rp = R2 * R2;
+    int m = 0;
+    for (int n = 3; n <= 8; ++n) {
+        while (m < 2 * n) { ++m; term *= x / m; S += term; }
+        Rp *= R2;
+        double f = 1.0 - ex * S;
+        double fp = HEAR_B * ex * term;  /* d f/dR = b e^-x x^2n/(2n)! */
+        dV -= HEAR_C[n - 3] * (fp / Rp - 2.0 * n * f / (Rp * R));
+    }
+    return dV;
+}
+
+double hho_hear_dip(double R) {
+    return exp(0.47293181 - 0.40100613 * R - 0.10292726 * R * R) - 148.55391 * pow(R, -7);
+}
+
+/* ======================================================================== */
+/* CO2-Ar molecular-frame surfaces from the generated tables                 */
+/* (PES-IDS/ai_pes_co2ar.c:27-459, PES-IDS/ai_ids_co2ar.cpp:21-491).         */
+/* ======================================================================== */
+static int co2ar_interval(double R) {
+    int i = 0;
+    while (i < HH_CO2AR_NINT - 1 && !(R < hh_co2ar_rbound[i])) ++i;
+    return i;
+}
+
+/* radial function c(R) and c'(R) of one table row */
+static void co2ar_radial(const double *row, double R, double rlo, double *c, double *dc) {
+    double t = R - rlo;
+    double v = ((row[3] * t + row[2]) * t + row[1]) * t + row[0];
+    double d = (3.0 * row[3] * t + 2.0 * row[2]) * t + row[1];
+    double iR = 1.0 / R;
+    double iR4 = iR * iR * iR * iR;
+    double iR5 = iR4 * iR, iR6 = iR5 * iR, iR7 = iR6 * iR;
+    v += row[4] * iR4 + row[5] * iR5 + row[6] * iR6 + row[7] * iR7;
+    d -= (4.0 * row[4] * iR4 + 5.0 * row[5] * iR5 + 6.0 * row[6] * iR6 + 7.0 * row[7] * iR7) * iR;
+    if (row[8] != 0.0) {
+        double e = row[8] * exp(row[9] * R);
+        v += e;
+        d += row[9] * e;
+    }
+    *c = v;
+    if (dc) *dc = d;
+}
+
+/* P_l(x), l = 0..10 (gsl_sf_legendre_Pl_array), and P_l'(x) */
+static void legendre_P(double x, double P[11], double dP[11]) {
+    P[0] = 1.0; P[1] = x;
+    for (int l = 1; l < 10; ++l) P[l + 1] = ((2 * l + 1) * x * P[l] - l * P[l - 1]) / (l + 1);
+    if (dP) {
+        dP[0] = 0.0; dP[1] = 1.0;
+        for (int l = 1; l < 10; ++l) dP[l + 1] = dP[l - 1] + (2 * l + 1) * P[l];
+    }
+}
+
+double hho_co2ar_V_mol(double R, double theta) {
+    double P[11];
+    legendre_P(cos(theta), P, NULL);
+    int i = co2ar_interval(R);
+    double V = 0.0;
+    for (int li = 0; li < HH_CO2AR_NL; ++li) {
+        double c;
+        co2ar_radial(hh_co2ar_pes[i][li], R, hh_co2ar_rlo[i], &c, NULL);
+        V += P[2 * li] * c;
+    }
+    return V / HTOCM;
+}
+
+void hho_co2ar_dV_mol(double R, double theta, double *dR, double *dtheta) {
+    double P[11], dP[11];
+    double x = cos(theta), s = sin(theta);
+    legendre_P(x, P, dP);
+    int i = co2ar_interval(R);
+    double vR = 0.0, vx = 0.0;
+    for (int li = 0; li < HH_CO2AR_NL; ++li) {
+        double c, dc;
+        co2ar_radial(hh_co2ar_pes[i][li], R, hh_co2ar_rlo[i], &c, &dc);
+        vR += P[2 * li] * dc;
+        vx += dP[2 * li] * c;
+    }
+    *dR = vR / HTOCM;
+    *dtheta = -s * vx / HTOCM;
+}
+
+/* body-frame dipole (d_x, 0, d_z): d_x = sum_l P_l^1 a_l(R) with the
+ * Condon-Shortley phase (GSL csphase = -1), d_z = sum_l P_l b_l(R) */
+void hho_co2ar_dip_mol(double R, double theta, double d[3]) {
+    double x = cos(theta);
+    double P[11];
+    legendre_P(x, P, NULL);
+    /* associated P_l^1 by the upward recurrence from P_1^1 = -sqrt(1-x^2) */
+    double P1[11];
+    P1[0] = 0.0;
+    P1[1] = -sqrt((1.0 - x) * (1.0 + x));
+    P1[2] = 3.0 * x * P1[1];
+    for (int l = 2; l < 10; ++l) P1[l + 1] = ((2 * l + 1) * x * P1[l] - (l + 1) * P1[l - 1]) / l;
+    int i = co2ar_interval(R);
+    double dx = 0.0, dz = 0.0;
+    for (int li = 0; li < HH_CO2AR_NL; ++li) {
+        double a, b;
+        co2ar_radial(hh_co2ar_dipx[i][li], R, hh_co2ar_rlo[i], &a, NULL);
+        co2ar_radial(hh_co2ar_dipz[i][li], R, hh_co2ar_rlo[i], &b, NULL);
+        dx += P1[2 * li] * a;
+        dz += P[2 * li] * b;
+    }
+    d[0] = dx; d[1] = 0.0; d[2] = dz;
+}
+
+/* rotations with the reference's sign conventions (src/angles_handler.cpp:45-104) */
+static void Sz(double a, double m[3][3]) {
+    double s = sin(a), c = cos(a);
+    double r[3][3] = {{c, s, 0}, {-s, c, 0}, {0, 0, 1}};
+    memcpy(m, r, sizeof r);
+}
+static void Sz_dot(double a, double m[3][3]) {
+    double s = sin(a), c = cos(a);
+    double r[3][3] = {{-s, c, 0}, {-c, -s, 0}, {0, 0, 0}};
+    memcpy(m, r, sizeof r);
+}
+static void Sx(double a, double m[3][3]) {
+    double s = sin(a), c = cos(a);
+    double r[3][3] = {{1, 0, 0}, {0, c, s}, {0, -s, c}};
+    memcpy(m, r, sizeof r);
+}
+static void Sx_dot(double a, double m[3][3]) {
+    double s = sin(a), c = cos(a);
+    double r[3][3] = {{0, 0, 0}, {0, -s, c}, {0, -c, -s}};
+    memcpy(m, r, sizeof r);
+}
+static void mv(double m[3][3], const double v[3], double o[3]) {
+    double t[3];
+    for (int i = 0; i < 3; ++i) t[i] = m[i][0] * v[0] + m[i][1] * v[1] + m[i][2] * v[2];
+    memcpy(o, t, sizeof t);
+}
+static void mtv(double m[3][3], const double v[3], double o[3]) {
+    double t[3];
+    for (int i = 0; i < 3; ++i) t[i] = m[0][i] * v[0] + m[1][i] * v[1] + m[2][i] * v[2];
+    memcpy(o, t, sizeof t);
+}
+
+/* linear_molecule_atom_lab_to_mol (src/angles_handler.cpp:106-138):
+ * qlab (PHI THETA R PHI1 THETA1) -> qmol (R PHIEM THETAEM PSIEM THETAM) */
+void hho_co2ar_lab_to_mol(const double *qlab, double *qmol) {
+    qmol[0] = qlab[2];
+    qmol[1] = qlab[0] + M_PI / 2.0;
+    qmol[2] = qlab[1];
+    double Mz[3][3], Mx[3][3];
+    Sz(qmol[1], Mz);
+    Sx(qmol[2], Mx);
+    double u[3] = {cos(qlab[3]) * sin(qlab[4]), sin(qlab[3]) * sin(qlab[4]), cos(qlab[4])};
+    double dd[3];
+    mv(Mz, u, dd);
+    mv(Mx, dd, dd);
+    qmol[4] = acos(dd[2]);
+    double st = sqrt(1 - dd[2] * dd[2]);
+    qmol[3] = atan2(dd[1] / st, dd[0] / st);
+}
+
+/* linear_molecule_atom_Jacobi_mol_by_lab (src/angles_handler.cpp:140-193):
+ * jac[i*5 + j] = d qmol_j / d qlab_i */
+void hho_co2ar_jacobian(const double *q, double *jac) {
+    double qmol[5];
+    hho_co2ar_lab_to_mol(q, qmol);
+    memset(jac, 0, 25 * sizeof(double));
+    jac[2 * 5 + 0] = 1.0;
+    jac[0 * 5 + 1] = 1.0;
+    jac[1 * 5 + 2] = 1.0;
+    double Mz[3][3], Mx[3][3], Mzd[3][3], Mxd[3][3];
+    Sz(qmol[1], Mz); Sx(qmol[2], Mx);
+    Sz_dot(qmol[1], Mzd); Sx_dot(qmol[2], Mxd);
+    double sphi = sin(q[3]), cphi = cos(q[3]), sth = sin(q[4]), cth = cos(q[4]);
+    double u[3] = {cphi * sth, sphi * sth, cth};
+    double u_phi[3] = {-sphi * sth, cphi * sth, 0.0};
+    double u_th[3] = {cphi * cth, sphi * cth, -sth};
+    double sin_thetam = sin(qmol[4]);
+    double spsi = sin(qmol[3]), cpsi = cos(qmol[3]);
+    double d[3];
+    /* row r <- derivative of dd along lab coordinate r:
+     * d(thetam) = -d(dd_z)/sin(thetam), d(psiem) = (d(dd_y) cos psi - d(dd_x) sin psi)/sin(thetam) */
+    mv(Mz, u_phi, d); mv(Mx, d, d);
+    jac[3 * 5 + 4] = -d[2] / sin_thetam;
+    jac[3 * 5 + 3] = (d[1] * cpsi - d[0] * spsi) / sin_thetam;
+    mv(Mz, u_th, d); mv(Mx, d, d);
+    jac[4 * 5 + 4] = -d[2] / sin_thetam;
+    jac[4 * 5 + 3] = (d[1] * cpsi - d[0] * spsi) / sin_thetam;
+    mv(Mzd, u, d); mv(Mx, d, d);
+    jac[0 * 5 + 4] = -d[2] / sin_thetam;
+    jac[0 * 5 + 3] = (d[1] * cpsi - d[0] * spsi) / sin_thetam;
+    mv(Mz, u, d); mv(Mxd, d, d);
+    jac[1 * 5 + 4] = -d[2] / sin_thetam;
+    jac[1 * 5 + 3] = (d[1] * cpsi - d[0] * spsi) / sin_thetam;
+}
+
+/* dpes_lab (PES-IDS/ai_pes_co2ar_lib.cpp:11-30): dV/dq_lab = J (dV/dR, 0, 0, 0, dV/dthetam) */
+static void co2ar_dpes_lab(const double *q, double *dVdq) {
+    double qmol[5], jac[25];
+    hho_co2ar_lab_to_mol(q, qmol);
+    double dR, dth;
+    hho_co2ar_dV_mol(qmol[0], qmol[4], &dR, &dth);
+    hho_co2ar_jacobian(q, jac);
+    for (int i = 0; i < 5; ++i) dVdq[i] = jac[i * 5 + 0] * dR + jac[i * 5 + 4] * dth;
+}
+
+/* dipole_lab (PES-IDS/ai_ids_co2ar_lib.cpp:12-37) */
+static void co2ar_dipole_lab(const double *q, double out[3]) {
+    double qmol[5];
+    hho_co2ar_lab_to_mol(q, qmol);
+    double dm[3];
+    hho_co2ar_dip_mol(qmol[0], qmol[4], dm);
+    double Mphi[3][3], Mth[3][3], Mpsi[3][3];
+    Sz(qmol[1], Mphi); Sx(qmol[2], Mth); Sz(qmol[3], Mpsi);
+    double t[3];
+    mtv(Mpsi, dm, t);
+    mtv(Mth, t, t);
+    mtv(Mphi, t, out);
+}
+
+int hho_qp_size(const hho_system *sys) { return sys->system == HHO_SYS_HEAR ? 6 : 10; }
+
+double hho_pes(const hho_system *sys, const double *q) {
+    if (sys->system == HHO_SYS_HEAR) return hho_hear_V(q[2]);
+    double qmol[5];
+    hho_co2ar_lab_to_mol(q, qmol);
+    return hho_co2ar_V_mol(qmol[0], qmol[4]);
+}
+
+void hho_dpes(const hho_system *sys, const double *q, double *dVdq) {
+    if (sys->system == HHO_SYS_HEAR) {
+        dVdq[0] = 0.0; dVdq[1] = 0.0; dVdq[2] = hho_hear_dV(q[2]);
+        return;
+    }
+    co2ar_dpes_lab(q, dVdq);
+}
+
+void hho_dipole(const hho_system *sys, const double *q, double d[3]) {
+    if (sys->system == HHO_SYS_HEAR) {
+        double Phi = q[0], Theta = q[1], dl = hho_hear_dip(q[2]);
+        d[0] = dl * sin(Theta) * cos(Phi);
+        d[1] = dl * sin(Theta) * sin(Phi);
+        d[2] = dl * cos(Theta);
+        return;
+    }
+    co2ar_dipole_lab(q, d);
+}
+
+/* ======================================================================== */
+/* Hamilton's equations (src/hawaii.c:474-616), kinetic energy (1041-1137)   */
+/* phase point: PHI PPHI THETA PTHETA R PR [phi1 pphi1 theta1 ptheta1]        */
+/* ======================================================================== */
+static void extract_q(const hho_system *sys, const double *qp, double *q) {
+    int n = hho_qp_size(sys);
+    for (int k = 0; k < n; k += 2) q[k / 2] = qp[k];
+}
+
+void hho_rhs(const hho_system *sys, const double *y, double *yd) {
+    double q[5], dV[5];
+    extract_q(sys, y, q);
+    hho_dpes(sys, q, dV);
+    double mu = sys->mu;
+    double pPhi = y[1], Theta = y[2], pTheta = y[3], R = y[4], pR = y[5];
+    double R2 = R * R, R3 = R2 * R;
+    double sT = sin(Theta), cT = cos(Theta);
+    double sT2 = sT * sT, sT3 = sT2 * sT;
+    yd[4] = pR / mu;
+    yd[5] = pTheta * pTheta / (mu * R3) + pPhi * pPhi / (mu * R3 * sT2) - dV[2];
+    yd[0] = pPhi / (mu * R2 * sT2);
+    yd[1] = -dV[0];
+    yd[2] = pTheta / (mu * R2);
+    yd[3] = pPhi * pPhi * cT / (mu * R2 * sT3) - dV[1];
+    if (sys->system == HHO_SYS_CO2AR) {
+        double I = sys->II;
+        double pphi = y[7], th = y[8], pth = y[9];
+        double s = sin(th), c = cos(th);
+        yd[6] = pphi / I / s / s;
+        yd[7] = -dV[3];
+        yd[8] = pth / I;
+        yd[9] = pphi * pphi * c / I / s / s / s - dV[4];
+    }
+}
+
+double hho_kinetic(const hho_system *sys, const double *qp) {
+    double mu = sys->mu;
+    double pPhi = qp[1], Theta = qp[2], pTheta = qp[3], R = qp[4], pR = qp[5];
+    double sT = sin(Theta);
+    double K = pR * pR / (2.0 * mu) + pTheta * pTheta / (2.0 * mu * R * R) +
+               pPhi * pPhi / (2.0 * mu * R * R * sT * sT);
+    if (sys->system == HHO_SYS_CO2AR) {
+        double I = sys->II, pphi = qp[7], th = qp[8], pth = qp[9];
+        double s = sin(th);
+        K += pth * pth / (2.0 * I) + pphi * pphi / (2.0 * I * s * s);
+    }
+    return K;
+}
+
+double hho_hamiltonian(const hho_system *sys, const double *qp) {
+    double q[5];
+    extract_q(sys, qp, q);
+    double V = hho_pes(sys, q);
+    return hho_kinetic(sys, qp) + V;
+}
+
+void hho_qp_to_cart(const hho_system *sys, const double *qp, double *cart) {
+    double Phi = qp[0], pPhi = qp[1], Th = qp[2], pTh = qp[3], R = qp[4], pR = qp[5];
+    double sT = sin(Th), cT = cos(Th), sP = sin(Phi), cP = cos(Phi);
+    double Rh[3] = {sT * cP, sT * sP, cT};
+    double Th_h[3] = {cT * cP, cT * sP, -sT};
+    double Ph_h[3] = {-sP, cP, 0.0};
+    for (int i = 0; i < 3; ++i) {
+        cart[i] = R * Rh[i];
+        cart[3 + i] = pR * Rh[i] + pTh / R * Th_h[i] + pPhi / (R * sT) * Ph_h[i];
+    }
+    if (sys->system == HHO_SYS_CO2AR) {
+        double ph = qp[6], pph = qp[7], th = qp[8], pth = qp[9];
+        double s = sin(th), c = cos(th), sp = sin(ph), cp = cos(ph);
+        double u[3] = {s * cp, s * sp, c};
+        double th_h[3] = {c * cp, c * sp, -s};
+        double ph_h[3] = {-sp, cp, 0.0};
+        for (int i = 0; i < 3; ++i) {
+            cart[6 + i] = u[i];
+            cart[9 + i] = pth * ph_h[i] - pph / s * th_h[i];  /* j = u x p_u (j_monomer, hawaii.c:398-431) */
+        }
+    }
+}
+
+/* ======================================================================== */
+/* Sampler (src/hawaii.c:1206-1421) and pair-state filter (2976-2994)        */
+/* ======================================================================== */
+static double generate_normal(hho_mt *s, int *draws) {
+    for (;;) {
+        double U = hho_mt_drand(s);
+        double V = hho_mt_drand(s);
+        *draws += 2;
+        double logU = log(U);
+        if (isnan(logU) || isinf(logU)) continue;
+        return 1.0 * sqrt(-2 * logU) * cos(2.0 * M_PI * V);
+    }
+}
+
+int hho_candidate(hho_mt *s, const hho_system *sys, const hho_params *p, double T,
+                  double *qp, double *energy, int *draws) {
+    *draws = 0;
+    double RMIN = p->Rmin, RMAX = p->Rmax;
+    /* q_generator */
+    double R3 = hho_mt_drand(s) * (RMAX * RMAX * RMAX - RMIN * RMIN * RMIN) + RMIN * RMIN * RMIN;
+    qp[4] = pow(R3, 1.0 / 3.0);
+    qp[0] = hho_mt_drand(s) * 2.0 * M_PI;
+    qp[2] = acos(2.0 * hho_mt_drand(s) - 1.0);
+    *draws += 3;
+    if (sys->system == HHO_SYS_CO2AR) {
+        qp[6] = hho_mt_drand(s) * 2.0 * M_PI;
+        qp[8] = acos(2.0 * hho_mt_drand(s) - 1.0);
+        *draws += 2;
+    }
+    /* p_generator */
+    double sqrt_MUKT = sqrt(sys->mu / HkT * T);
+    double sinTheta = sin(qp[2]);
+    double x[3];
+    for (int i = 0; i < 3; ++i) x[i] = generate_normal(s, draws);
+    qp[1] = sqrt_MUKT * qp[4] * sinTheta * x[0];
+    qp[3] = sqrt_MUKT * qp[4] * x[1];
+    qp[5] = sqrt_MUKT * x[2];
+    if (sys->system == HHO_SYS_CO2AR) {
+        double sqrt_IIKT = sqrt(sys->II / HkT * T);
+        double sin_theta = sin(qp[8]);
+        double x0 = generate_normal(s, draws);
+        double x1 = generate_normal(s, draws);
+        qp[7] = sqrt_IIKT * sin_theta * x1;
+        qp[9] = sqrt_IIKT * x0;
+    }
+    /* Hamiltonian, then reject() */
+    double E = hho_hamiltonian(sys, qp);
+    double u = hho_mt_drand(s);
+    *draws += 1;
+    double Mval = exp(-p->pesmin * HkT / T);
+    double M = 1.5 * Mval;
+    double kin = hho_kinetic(sys, qp);
+    double q[5];
+    extract_q(sys, qp, q);
+    double pot = hho_pes(sys, q);
+    double proposal = exp(-kin * HkT / T);
+    double desired = exp(-(kin + pot) * HkT / T);
+    double weight = desired / proposal / M;
+    *energy = E;
+    if (weight < u) return 0;
+    if (p->pair_state == HHO_PS_FREE_AND_METASTABLE && E < 0.0) return 0;
+    if (p->pair_state == HHO_PS_BOUND && E > 0.0) return 0;
+    return 1;
+}
+
+long hho_sample(uint32_t seed, const hho_system *sys, const hho_params *p, double T,
+                size_t n, double *qp_out) {
+    hho_mt s;
+    hho_mt_seed(&s, seed);
+    int QP = hho_qp_size(sys);
+    long cand = 0;
+    size_t got = 0;
+    double qp[10], E;
+    int draws;
+    while (got < n) {
+        ++cand;
+        if (hho_candidate(&s, sys, p, T, qp, &E, &draws)) {
+            memcpy(qp_out + got * QP, qp, QP * sizeof(double));
+            ++got;
+        }
+    }
+    return cand;
+}
+
+/* ======================================================================== */
+/* DOP853 with dense output (Hairer-Norsett-Wanner); step control and        */
+/* initial step as in the standard published algorithm.                      */
+/* ======================================================================== */
+#define NMAX 10
+
+typedef struct {
+    const hho_system *sys;
+    int n;
+    double rtol, atol;
+    long nrhs;
+} integ;
+
+static void f_eval(integ *I, const double *y, double *f) {
+    hho_rhs(I->sys, y, f);
+    I->nrhs++;
+}
+
+static double rms(const double *v, int n) {
+    double s = 0.0;
+    for (int i = 0; i < n; ++i) s += v[i] * v[i];
+    return sqrt(s / n);
+}
+
+static double initial_step(integ *I, const double *y0, const double *f0, double span) {
+    int n = I->n;
+    double sc[NMAX], tmp[NMAX], y1[NMAX], f1[NMAX];
+    for (int i = 0; i < n; ++i) sc[i] = I->atol + fabs(y0[i]) * I->rtol;
+    for (int i = 0; i < n; ++i) tmp[i] = y0[i] / sc[i];
+    double d0 = rms(tmp, n);
+    for (int i = 0; i < n; ++i) tmp[i] = f0[i] / sc[i];
+    double d1 = rms(tmp, n);
+    double h0 = (d0 < 1e-5 || d1 < 1e-5) ? 1e-6 : 0.01 * d0 / d1;
+    if (h0 > span) h0 = span;
+    for (int i = 0; i < n; ++i) y1[i] = y0[i] + h0 * f0[i];
+    f_eval(I, y1, f1);
+    for (int i = 0; i < n; ++i) tmp[i] = (f1[i] - f0[i]) / sc[i];
+    double d2 = rms(tmp, n) / h0;
+    double h1;
+    if (d1 <= 1e-15 && d2 <= 1e-15) h1 = fmax(1e-6, h0 * 1e-3);
+    else h1 = pow(0.01 / fmax(d1, d2), 1.0 / 8.0);
+    return fmin(fmin(100 * h0, h1), span);
+}
+
+/* one adaptive step from (t, y, f): on success y_new/f_new/K filled, *h is the
+ * step taken and *h_next the proposal.  returns 0 or HHO_ST_H_UNDERFLOW */
+static int dop853_step(integ *I, double t, const double *y, const double *f, double *h_io,
+                       double *h_taken, double K[16][NMAX], double *y_new, long *nrej) {
+    int n = I->n;
+    double h = *h_io;
+    int rejected = 0;
+    for (;;) {
+        double min_step = 10.0 * fabs(nextafter(t, INFINITY) - t);
+        if (h < min_step) return HHO_ST_H_UNDERFLOW;
+        double ys[NMAX];
+        memcpy(K[0], f, n * sizeof(double));
+        for (int s = 1; s < 12; ++s) {
+            for (int i = 0; i < n; ++i) {
+                double acc = 0.0;
+                for (int j = 0; j < s; ++j) acc += hh_dop853_a[s][j] * K[j][i];
+                ys[i] = y[i] + h * acc;
+            }
+            f_eval(I, ys, K[s]);
+        }
+        for (int i = 0; i < n; ++i) {
+            double acc = 0.0;
+            for (int j = 0; j < 12; ++j) acc += hh_dop853_a[12][j] * K[j][i];
+            y_new[i] = y[i] + h * acc;
+        }
+        f_eval(I, y_new, K[12]);
+        double e5 = 0.0, e3 = 0.0;
+        for (int i = 0; i < n; ++i) {
+            double sc = I->atol + fmax(fabs(y[i]), fabs(y_new[i])) * I->rtol;
+            double a5 = 0.0, a3 = 0.0;
+            for (int j = 0; j < 13; ++j) {
+                a5 += hh_dop853_e5[j] * K[j][i];
+                a3 += hh_dop853_e3[j] * K[j][i];
+            }
+            a5 /= sc; a3 /= sc;
+            e5 += a5 * a5; e3 += a3 * a3;
+        }
+        double err;
+        if (e5 == 0.0 && e3 == 0.0) err = 0.0;
+        else err = fabs(h) * e5 / sqrt((e5 + 0.01 * e3) * n);
+        if (err < 1.0) {
+            double fac = (err == 0.0) ? 10.0 : fmin(10.0, 0.9 * pow(err, -1.0 / 8.0));
+            if (rejected) fac = fmin(1.0, fac);
+            *h_taken = h;
+            *h_io = h * fac;
+            return 0;
+        }
+        h *= fmax(0.2, 0.9 * pow(err, -1.0 / 8.0));
+        rejected = 1;
+        (*nrej)++;
+    }
+}
+
+/* dense output coefficients F[7][n] for the step (y_old, h) -> y_new */
+static void dop853_dense(integ *I, const double *y_old, const double *y_new, double h,
+                         double K[16][NMAX], double F[7][NMAX]) {
+    int n = I->n;
+    double ys[NMAX];
+    for (int s = 13; s < 16; ++s) {
+        for (int i = 0; i < n; ++i) {
+            double acc = 0.0;
+            for (int j = 0; j < s; ++j) acc += hh_dop853_a[s][j] * K[j][i];
+            ys[i] = y_old[i] + h * acc;
+        }
+        f_eval(I, ys, K[s]);
+    }
+    for (int i = 0; i < n; ++i) {
+        double dy = y_new[i] - y_old[i];
+        F[0][i] = dy;
+        F[1][i] = h * K[0][i] - dy;
+        F[2][i] = 2 * dy - h * (K[12][i] + K[0][i]);
+        for (int r = 0; r < 4; ++r) {
+            double acc = 0.0;
+            for (int j = 0; j < 16; ++j) acc += hh_dop853_d[r][j] * K[j][i];
+            F[3 + r][i] = h * acc;
+        }
+    }
+}
+
+static void dense_eval(int n, const double *y_old, double F[7][NMAX], double x, double *y) {
+    for (int i = 0; i < n; ++i) {
+        double v = 0.0;
+        for (int r = 6; r >= 0; --r) {
+            v += F[r][i];
+            v *= ((6 - r) % 2 == 0) ? x : (1.0 - x);
+        }
+        y[i] = y_old[i] + v;
+    }
+}
+
+/* one direction of correlation_eval: samples k = 1..N-1 of mu0 . mu(t_k) */
+static int half_traj(const hho_system *sys, const hho_params *p, const double *y0,
+                     const double mu0[3], double *corr, hho_traj_stats *st, int *hard) {
+    integ I = {sys, hho_qp_size(sys), p->rtol, p->atol, 0};
+    int n = I.n;
+    double y[NMAX], f[NMAX], y_new[NMAX], K[16][NMAX], F[7][NMAX], ys[NMAX];
+    memcpy(y, y0, n * sizeof(double));
+    f_eval(&I, y, f);
+    double dt = p->sampling_time;
+    double span = dt * (double)(p->N - 1);
+    double h = initial_step(&I, y, f, span);
+    double t = 0.0;
+    size_t k = 1;
+    long since = 0;
+    double prev = 0.0, curr = 0.0;
+    int status = HHO_OK;
+    *hard = 0;
+    while (k < p->N) {
+        double ht;
+        int rc = dop853_step(&I, t, y, f, &h, &ht, K, y_new, &st->nrej);
+        if (rc) { status = rc; break; }
+        st->nsteps++;
+        double t_new = t + ht;
+        int dense = 0;
+        while (k < p->N && (double)k * dt <= t_new) {
+            if (!dense) { dop853_dense(&I, y, y_new, ht, K, F); dense = 1; }
+            double x = ((double)k * dt - t) / ht;
+            dense_eval(n, y, F, x, ys);
+            double q[5], d[3];
+            extract_q(sys, ys, q);
+            hho_dipole(sys, q, d);
+            st->nsamples++;
+            if (isnan(d[0]) || isnan(d[1]) || isnan(d[2])) { status = HHO_ST_NAN_DIPOLE; *hard = 1; goto done; }
+            prev = curr;
+            curr = mu0[0] * d[0] + mu0[1] * d[1] + mu0[2] * d[2];
+            if (fabs(curr) > 1e100) { status = HHO_ST_OVERFLOW; *hard = 1; goto done; }
+            if (k > 1) {
+                double ratio = fabs(curr / prev);
+                if (ratio > 1e10) { status = HHO_ST_JUMP; *hard = 1; goto done; }
+            }
+            corr[k] = curr;
+            ++k;
+            since = 0;
+            if (ys[4] > p->Rcut) goto done;
+        }
+        t = t_new;
+        memcpy(y, y_new, n * sizeof(double));
+        memcpy(f, K[12], n * sizeof(double));
+        if (++since > p->max_steps) { status = HHO_ST_MAXSTEPS; break; }
+    }
+done:
+    st->nrhs += I.nrhs;
+    return status;
+}
+
+int hho_correlation_eval(const hho_system *sys, const hho_params *p, const double *qp0,
+                         double *crln, hho_traj_stats *st) {
+    int n = hho_qp_size(sys);
+    size_t N = p->N;
+    double *fw = calloc(N, sizeof(double)), *bw = calloc(N, sizeof(double));
+    memset(crln, 0, N * sizeof(double));
+    memset(st, 0, sizeof *st);
+    double q[5], mu0[3];
+    extract_q(sys, qp0, q);
+    hho_dipole(sys, q, mu0);
+    fw[0] = bw[0] = mu0[0] * mu0[0] + mu0[1] * mu0[1] + mu0[2] * mu0[2];
+    int hard = 0;
+    st->status_fwd = half_traj(sys, p, qp0, mu0, fw, st, &hard);
+    if (!hard) {
+        double y[NMAX];
+        memcpy(y, qp0, n * sizeof(double));
+        for (int i = 1; i < n; i += 2) y[i] = -y[i];   /* invert_momenta (hawaii.c:1171-1188) */
+        st->status_bwd = half_traj(sys, p, y, mu0, bw, st, &hard);
+    }
+    if (hard) {
+        st->failed = 1;      /* reference returns 1: crln stays zero */
+    } else {
+        for (size_t i = 0; i < N; ++i) crln[i] = 0.5 * (fw[i] + bw[i]) * ALU * ALU * ALU;
+    }
+    free(fw); free(bw);
+    return st->failed;
+}
+
+int hho_correlation_parts(const hho_system *sys, const hho_params *p, const double *qp0,
+                          double *fw, double *bw, hho_traj_stats *st) {
+    int n = hho_qp_size(sys);
+    size_t N = p->N;
+    memset(fw, 0, N * sizeof(double));
+    memset(bw, 0, N * sizeof(double));
+    memset(st, 0, sizeof *st);
+    double q[5], mu0[3];
+    extract_q(sys, qp0, q);
+    hho_dipole(sys, q, mu0);
+    fw[0] = bw[0] = mu0[0] * mu0[0] + mu0[1] * mu0[1] + mu0[2] * mu0[2];
+    int hard = 0;
+    st->status_fwd = half_traj(sys, p, qp0, mu0, fw, st, &hard);
+    double y[NMAX];
+    memcpy(y, qp0, n * sizeof(double));
+    for (int i = 1; i < n; i += 2) y[i] = -y[i];
+    int hard2 = 0;
+    st->status_bwd = half_traj(sys, p, y, mu0, bw, st, &hard2);
+    st->failed = hard || hard2;
+    return st->failed;
+}
+
+int hho_propagate(const hho_system *sys, const hho_params *p, const double *qp0,
+                  double t_end, double *qp_out, long *nsteps) {
+    integ I = {sys, hho_qp_size(sys), p->rtol, p->atol, 0};
+    int n = I.n;
+    double y[NMAX], f[NMAX], y_new[NMAX], K[16][NMAX], F[7][NMAX];
+    memcpy(y, qp0, n * sizeof(double));
+    f_eval(&I, y, f);
+    double dt = p->sampling_time;
+    double h = initial_step(&I, y, f, dt * (double)(p->N - 1));
+    double t = 0.0;
+    long ns = 0, nrej = 0;
+    for (;;) {
+        double ht;
+        int rc = dop853_step(&I, t, y, f, &h, &ht, K, y_new, &nrej);
+        if (rc) return rc;
+        ++ns;
+        if (t + ht >= t_end) {
+            dop853_dense(&I, y, y_new, ht, K, F);
+            dense_eval(n, y, F, (t_end - t) / ht, qp_out);
+            break;
+        }
+        t += ht;
+        memcpy(y, y_new, n * sizeof(double));
+        memcpy(f, K[12], n * sizeof(double));
+    }
+    if (nsteps) *nsteps = ns;
+    return 0;
+}
+
+typedef struct {
+    const hho_system *sys;
+    const hho_params *p;
+    const double *qp0;
+    size_t begin, end;
+    double *sum;
+    hho_traj_stats *stats;
+} corr_job;
+
+static void *corr_worker(void *arg) {
+    corr_job *J = arg;
+    int n = hho_qp_size(J->sys);
+    size_t N = J->p->N;
+    double *crln = malloc(N * sizeof(double));
+    for (size_t i = J->begin; i < J->end; ++i) {
+        hho_traj_stats st;
+        hho_correlation_eval(J->sys, J->p, J->qp0 + i * n, crln, &st);
+        for (size_t k = 0; k < N; ++k) J->sum[k] += J->p->ppf_ratio * crln[k];
+        if (J->stats) J->stats[i] = st;
+    }
+    free(crln);
+    return NULL;
+}
+
+int hho_correlation_sum(const hho_system *sys, const hho_params *p, const double *qp0,
+                        size_t n, int nthreads, double *crln_sum, hho_traj_stats *stats) {
+    if (nthreads < 1) nthreads = 1;
+    size_t N = p->N;
+    pthread_t th[256];
+    corr_job jobs[256];
+    if (nthreads > 256) nthreads = 256;
+    for (int w = 0; w < nthreads; ++w) {
+        jobs[w] = (corr_job){sys, p, qp0, n * w / nthreads, n * (w + 1) / nthreads,
+                             calloc(N, sizeof(double)), stats};
+        pthread_create(&th[w], NULL, corr_worker, &jobs[w]);
+    }
+    memset(crln_sum, 0, N * sizeof(double));
+    for (int w = 0; w < nthreads; ++w) {
+        pthread_join(th[w], NULL);
+        for (size_t k = 0; k < N; ++k) crln_sum[k] += jobs[w].sum[k];
+        free(jobs[w].sum);
+    }
+    return 0;
+}
+
+/* ======================================================================== */
+/* CF -> SF (src/hawaii.c:5401-5410, 5478-5553, 5569-5601)                   */
+/* ======================================================================== */
+static void fft_backward(double *re, double *im, size_t L) {
+    /* iterative radix-2, unnormalised exp(+i...) */
+    for (size_t i = 1, j = 0; i < L; ++i) {
+        size_t bit = L >> 1;
+        for (; j & bit; bit >>= 1) j ^= bit;
+        j ^= bit;
+        if (i < j) {
+            double t = re[i]; re[i] = re[j]; re[j] = t;
+            t = im[i]; im[i] = im[j]; im[j] = t;
+        }
+    }
+    for (size_t len = 2; len <= L; len <<= 1) {
+        size_t half = len / 2;
+        for (size_t k = 0; k < half; ++k) {
+            double ang = 2.0 * M_PI * (double)k / (double)len;
+            double wr = cos(ang), wi = sin(ang);
+            for (size_t i = k; i < L; i += len) {
+                size_t j = i + half;
+                double xr = re[j] * wr - im[j] * wi;
+                double xi = re[j] * wi + im[j] * wr;
+                re[j] = re[i] - xr; im[j] = im[i] - xi;
+                re[i] += xr; im[i] += xi;
+            }
+        }
+    }
+}
+
+int hho_idct_cf_to_sf(double *cf, size_t N, double dt, double *nu, double *sf) {
+    if (N == 0 || (N & (N - 1))) return -1;
+    double Xscale = 1.0 / LightSpeed_cm / ATU / 2.0 / M_PI;
+    double Yscale = ATU * ADIPMOMU * ADIPMOMU / (4.0 * M_PI * EPSILON0);
+    double tmax_a = dt * (double)N;
+    for (size_t i = 0; i < N; ++i) {
+        double tc = dt * (double)i;
+        double f = (1.0 - (tc / tmax_a) * (tc / tmax_a)) * (1.0 - (tc / tmax_a) * (tc / tmax_a));
+        cf[i] *= f;
+    }
+    size_t L = 2 * N;
+    double *re = calloc(L, sizeof(double)), *im = calloc(L, sizeof(double));
+    for (size_t k = 0; k < N; ++k) {
+        double a = M_PI * (double)k / (2.0 * N);
+        re[k] = cf[k] * cos(a) / (2.0 * N);
+        im[k] = cf[k] * sin(a) / (2.0 * N);
+    }
+    for (size_t k = N + 1; k < L; ++k) {
+        size_t i = L - k;
+        double a = M_PI * (double)k / (2.0 * N);
+        re[k] = -cf[i] * cos(a) / (2.0 * N);
+        im[k] = -cf[i] * sin(a) / (2.0 * N);
+    }
+    fft_backward(re, im, L);
+    double tmax = (double)N * dt;
+    for (size_t i = 0; i < N; ++i) {
+        nu[i] = (double)i * M_PI / tmax * Xscale;
+        sf[i] = re[i] * tmax / M_PI * Yscale;
+    }
+    free(re); free(im);
+    return 0;
+}
+
+/* ======================================================================== */
+/* Zeroth moment by plain Monte Carlo (the M0 integrand of                  */
+/* src/hep_hawaii.cpp:148-201 sampled with R uniform on [Rmin, Rmax],       */
+/* isotropic angles and Gaussian momenta):                                   */
+/*   M0(T) = ZeroCoeff * 4 pi (Rmax - Rmin) < R^2 |mu|^2 exp(-V/kT) 1[filter] >*/
+/* Only the kinetic energy K = kT * kappa of the momenta enters; kappa is    */
+/* half a chi^2 with 3 (atom-atom) or 5 (linear-atom) degrees of freedom,    */
+/* drawn by Box-Muller sums.                                                 */
+/* ======================================================================== */
+static inline double u24(uint32_t w) { return ((double)(w >> 8) + 0.5) * (1.0 / 16777216.0); }
+
+typedef struct {
+    const hho_system *sys;
+    const hho_params *p;
+    const double *T;
+    int nT;
+    uint64_t begin, end, seed;
+    double *wsum, *wsq;
+} m0_job;
+
+static void *m0_worker(void *arg) {
+    m0_job *J = arg;
+    int nT = J->nT;
+    double invkT[64];
+    for (int t = 0; t < nT; ++t) invkT[t] = HkT / J->T[t];
+    uint32_t key[2] = {(uint32_t)J->seed, (uint32_t)(J->seed >> 32)};
+    double Rmin = J->p->Rmin, dR = J->p->Rmax - J->p->Rmin;
+    for (uint64_t i = J->begin; i < J->end; ++i) {
+        uint32_t w[12];
+        for (uint32_t c = 0; c < 3; ++c) {
+            uint32_t ctr[4] = {(uint32_t)i, (uint32_t)(i >> 32), c, 0u};
+            hho_philox4x32_10(ctr, key, w + 4 * c);
+        }
+        double R = Rmin + dR * u24(w[0]);
+        double Phi = 2.0 * M_PI * u24(w[1]);
+        double cT = 2.0 * u24(w[2]) - 1.0;
+        double q[5] = {Phi, acos(cT), R, 0.0, 0.0};
+        double kappa;
+        double zc = cos(2.0 * M_PI * u24(w[8]));
+        if (J->sys->system == HHO_SYS_CO2AR) {
+            q[3] = 2.0 * M_PI * u24(w[3]);
+            q[4] = acos(2.0 * u24(w[4]) - 1.0);
+            kappa = -log(u24(w[5])) - log(u24(w[6])) - log(u24(w[7])) * zc * zc;
+        } else {
+            kappa = -log(u24(w[5])) - log(u24(w[7])) * zc * zc;
+        }
+        double V = hho_pes(J->sys, q);
+        double d[3];
+        hho_dipole(J->sys, q, d);
+        double base = R * R * (d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+        for (int t = 0; t < nT; ++t) {
+            double H = kappa / invkT[t] + V;
+            int keep = 1;
+            if (J->p->pair_state == HHO_PS_FREE_AND_METASTABLE) keep = (H >= 0.0);
+            else if (J->p->pair_state == HHO_PS_BOUND) keep = (H <= 0.0);
+            double wv = keep ? base * exp(-V * invkT[t]) : 0.0;
+            J->wsum[t] += wv;
+            J->wsq[t] += wv * wv;
+        }
+    }
+    return NULL;
+}
+
+int hho_m0(const hho_system *sys, const hho_params *p, const double *T, int nT,
+           uint64_t n_samples, uint64_t seed, uint64_t offset, int nthreads,
+           double *wsum, double *wsq) {
+    if (nT > 64 || nT < 1) return -1;
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 256) nthreads = 256;
+    pthread_t th[256];
+    m0_job jobs[256];
+    for (int w = 0; w < nthreads; ++w) {
+        jobs[w] = (m0_job){sys, p, T, nT, offset + n_samples * w / nthreads,
+                           offset + n_samples * (w + 1) / nthreads, seed,
+                           calloc(nT, sizeof(double)), calloc(nT, sizeof(double))};
+        pthread_create(&th[w], NULL, m0_worker, &jobs[w]);
+    }
+    for (int t = 0; t < nT; ++t) wsum[t] = wsq[t] = 0.0;
+    for (int w = 0; w < nthreads; ++w) {
+        pthread_join(th[w], NULL);
+        for (int t = 0; t < nT; ++t) { wsum[t] += jobs[w].wsum[t]; wsq[t] += jobs[w].wsq[t]; }
+        free(jobs[w].wsum); free(jobs[w].wsq);
+    }
+    return 0;
+}
+
+double hho_m0_scale(const hho_params *p) { return ZeroCoeff * 4.0 * M_PI * (p->Rmax - p->Rmin); }
+
+/* analytic_full_partition_function_by_V (src/hawaii.c:5071-5090) */
+double hho_analytic_pf(const hho_system *sys, double T) {
+    if (sys->system == HHO_SYS_HEAR) return pow(2.0 * M_PI * sys->mu * T / HkT, 1.5);
+    return 4.0 * M_PI * pow(2.0 * M_PI * T / HkT, 2.5) * pow(sys->mu, 1.5) * sys->II;
+}

@@ -1,0 +1,144 @@
+"""GPU parity against the CPU oracle, through the C ABI (libhh_cuda.so)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests.helpers import lib_params, lib_system, oracle_params, oracle_system, rel_to_c0
+
+pytestmark = pytest.mark.gpu
+
+
+@pytest.fixture(scope="module")
+def lib():
+    from hawaiihybrid_b200 import _lib
+    return _lib.load()
+
+
+def test_mt_stream_bit_exact(lib):
+    lib_system("hear")
+    for seed in (42, 7, 1):
+        n = 200_000
+        out = np.empty(n, dtype=np.uint32)
+        assert lib.hh_cuda_mt_stream(seed, n, out) == 0
+        assert np.array_equal(out, O.mt_stream(seed, n))
+    assert abs(out[:1].astype(np.float64)[0] * 2.0 ** -32 - O.mt_stream(1, 1)[0] * 2.0 ** -32) == 0
+
+
+@pytest.mark.parametrize("name,seed,T,n", [("hear", 42, 300.0, 3000), ("co2ar", 7, 300.0, 3000),
+                                           ("hear", 5, 100.0, 1000), ("co2ar", 11, 150.0, 1000)])
+def test_sampler_matches_oracle(name, seed, T, n):
+    import hawaiihybrid_b200 as hh
+    ms = lib_system(name, seed)
+    p = lib_params(name, 64, 100.0)
+    qp, cand = hh.sample_initial_conditions(ms, p, T, n, seed=seed)
+    qp_ref, cand_ref = O.sample(seed, oracle_system(name), oracle_params(name, 64, 100.0), T, n)
+    assert cand == cand_ref
+    # same candidates accepted in the same order; values agree to libm rounding
+    np.testing.assert_allclose(qp, qp_ref, rtol=1e-13, atol=1e-300)
+
+
+def test_sampler_stream_continues(lib):
+    """seed == 0 continues the stream, as consecutive iterations of the reference do."""
+    import hawaiihybrid_b200 as hh
+    ms = lib_system("co2ar", 3)
+    p = lib_params("co2ar", 64, 100.0)
+    a, _ = hh.sample_initial_conditions(ms, p, 300.0, 500, seed=3)
+    b, _ = hh.sample_initial_conditions(ms, p, 300.0, 700, seed=0)
+    ref, _ = O.sample(3, oracle_system("co2ar"), oracle_params("co2ar", 64, 100.0), 300.0, 1200)
+    np.testing.assert_allclose(np.vstack([a, b]), ref, rtol=1e-13, atol=1e-300)
+
+
+@pytest.mark.parametrize("name,N,dt,n", [("hear", 2048, 200.0, 256), ("co2ar", 4096, 100.0, 128)])
+def test_fp64_correlation_matches_oracle(name, N, dt, n):
+    import hawaiihybrid_b200 as hh
+    ms = lib_system(name)
+    qp, _ = O.sample(42, oracle_system(name), oracle_params(name, N, dt), 300.0, n)
+    crln, st = hh.correlation_from_initial_conditions(ms, lib_params(name, N, dt), qp)
+    ref = O.correlation_sum(oracle_system(name), oracle_params(name, N, dt), qp)
+    assert st.n_failed == 0
+    # same integrator family at rtol 1e-12 in two coordinate systems
+    assert rel_to_c0(crln, ref) < 1e-7
+
+
+@pytest.mark.parametrize("name,dt", [("hear", 200.0), ("co2ar", 100.0)])
+def test_single_trajectory_early_times(name, dt):
+    """Per-trajectory C_i(t_k) over the first 1000 a.u. against the oracle, 1e-9 of C_i(0)."""
+    import hawaiihybrid_b200 as hh
+    ms = lib_system(name)
+    qp, _ = O.sample(9, oracle_system(name), oracle_params(name, 64, dt), 300.0, 16)
+    kmax = int(1000.0 / dt) + 1
+    for i in range(qp.shape[0]):
+        crln, _ = hh.correlation_from_initial_conditions(ms, lib_params(name, 64, dt), qp[i:i + 1])
+        ref, st = O.correlation_eval(oracle_system(name), oracle_params(name, 64, dt), qp[i])
+        assert np.max(np.abs(crln[:kmax] - ref[:kmax])) <= 1e-9 * abs(ref[0])
+
+
+@pytest.mark.parametrize("name,N,dt,n", [("hear", 4096, 200.0, 2048), ("co2ar", 4096, 100.0, 2048)])
+def test_mixed_matches_fp64(name, N, dt, n):
+    import hawaiihybrid_b200 as hh
+    ms = lib_system(name)
+    p = lib_params(name, N, dt)
+    c64, _, s64 = hh.correlation_iteration(ms, p, 300.0, n, hh.PRECISION_FP64, seed=5)
+    c32, _, s32 = hh.correlation_iteration(ms, p, 300.0, n, hh.PRECISION_MIXED, seed=5)
+    assert rel_to_c0(c32, c64) <= 1e-4
+    assert abs(c32[0] - c64[0]) / abs(c64[0]) <= 1e-4   # M0 from C(0)
+
+
+@pytest.mark.parametrize("name", ["hear", "co2ar"])
+def test_m0_matches_oracle(name):
+    import hawaiihybrid_b200 as hh
+    ms = lib_system(name)
+    p = lib_params(name, 64, 100.0)
+    T = np.linspace(150.0, 400.0, 16)
+    n = 400_000
+    m64, e64 = hh.calculate_m0(ms, p, T, n, seed=99, precision=hh.PRECISION_FP64)
+    m32, e32 = hh.calculate_m0(ms, p, T, n, seed=99, precision=hh.PRECISION_MIXED)
+    ws, wq = O.m0(oracle_system(name), oracle_params(name, 64, 100.0), T, n, 99)
+    mref = O.m0_scale(oracle_params(name, 64, 100.0)) * ws / n
+    np.testing.assert_allclose(m64, mref, rtol=1e-10)
+    np.testing.assert_allclose(m32, m64, rtol=1e-4)
+
+
+def test_idct_golden():
+    import os
+    import hawaiihybrid_b200 as hh
+    lib_system("hear")
+    g = np.load(os.path.join(os.path.dirname(__file__), "golden", "cf_sf_he_ar_1000.npz"))
+    N = g["cf"].size
+    cf = hh.CFnc(t=g["dt"] * np.arange(N), data=g["cf"].copy(), ntraj=float(g["ntraj"]),
+                 Temperature=float(g["temperature"]), normalized=True)
+    sf = hh.idct_cf_to_sf(cf)
+    peak = np.max(np.abs(g["sf"]))
+    assert np.max(np.abs(sf.data - g["sf"])) / peak < 1e-6
+    m = np.abs(g["sf"]) >= 1e-6 * peak
+    assert np.max(np.abs(sf.data[m] - g["sf"][m]) / np.abs(g["sf"][m])) < 1e-6
+    np.testing.assert_allclose(sf.nu[::64][1:], g["sf_nu_every64"][1:], rtol=1e-9)
+
+
+@pytest.mark.parametrize("status,hard", [(3, True), (5, True), (1, False)])
+def test_failure_semantics(lib, status, hard):
+    """A branch ending in a hard failure drops the whole trajectory (still counted);
+    an integrator failure keeps the samples taken before it (src/hawaii.c:2172-2243, 3001)."""
+    import hawaiihybrid_b200 as hh
+    name, N, dt = "hear", 512, 200.0
+    ms = lib_system(name)
+    qp, _ = O.sample(21, oracle_system(name), oracle_params(name, N, dt), 300.0, 32)
+    traj, k_fail = 5, 3
+    assert lib.hh_cuda_debug_inject(traj, 0, k_fail, status) == 0
+    try:
+        crln, st = hh.correlation_from_initial_conditions(ms, lib_params(name, N, dt), qp)
+    finally:
+        lib.hh_cuda_debug_inject(-1, 0, 0, 0)
+    keep = [i for i in range(qp.shape[0]) if i != traj]
+    ref = O.correlation_sum(oracle_system(name), oracle_params(name, N, dt), qp[keep])
+    if not hard:
+        # forward branch of `traj` truncated before sample k_fail, backward branch intact
+        full, _ = O.correlation_eval(oracle_system(name), oracle_params(name, N, dt), qp[traj])
+        fw_bw = O.correlation_parts(oracle_system(name), oracle_params(name, N, dt), qp[traj])
+        fw, bw = fw_bw
+        fw[k_fail:] = 0.0
+        ref = ref + 0.5 * (fw + bw) * (5.29177210903e-11) ** 3
+    assert st.n_failed == (1 if hard else 0)
+    assert rel_to_c0(crln, ref) < 1e-7
