@@ -10,6 +10,7 @@ from .hawaii import (ATOM, LINEAR_MOLECULE, PAIR_STATE_ALL, PAIR_STATE_BOUND,
                      SYSTEM_CO2_AR, SYSTEM_HE_AR, CalcParams, CFnc, MoleculeSystem, SFnc,
                      analytic_full_partition_function_by_V, calculate_correlation_and_save,
                      calculate_m0, correlation_from_initial_conditions, correlation_iteration,
+                     correlation_iterations,
                      idct_cf_to_sf, init_ms, read_correlation_function, read_spectral_function,
                      sample_initial_conditions, write_correlation_function,
                      write_spectral_function)

@@ -35,9 +35,10 @@ HH_PRECISION_MIXED = 1
 
 # entry points declared in include/hh_cuda.h
 EXPORTS = (
-    "hh_cuda_init", "hh_cuda_seed", "hh_cuda_sample", "hh_cuda_correlation",
+    "hh_cuda_init", "hh_cuda_seed", "hh_cuda_sample", "hh_cuda_correlation", "hh_cuda_correlation_multi",
     "hh_cuda_correlation_ic", "hh_cuda_m0", "hh_cuda_idct_cf_to_sf", "hh_cuda_strerror",
-    "hh_cuda_mt_stream", "hh_cuda_debug_inject", "hh_cuda_shutdown",
+    "hh_cuda_mt_stream", "hh_cuda_debug_inject", "hh_cuda_debug_item_trace", "hh_cuda_fma_peak",
+    "hh_cuda_shutdown",
 )
 
 
@@ -71,6 +72,7 @@ class Stats(C.Structure):
         ("n_rejected_steps", C.c_uint64), ("n_rhs", C.c_uint64), ("n_samples", C.c_uint64),
         ("n_dense", C.c_uint64), ("n_failed", C.c_uint64), ("status", C.c_uint64 * 8),
         ("sample_ms", C.c_double), ("traj_ms", C.c_double), ("total_ms", C.c_double),
+        ("n_kernel_launches", C.c_uint64),
     ]
 
     def as_dict(self) -> dict:
@@ -99,6 +101,8 @@ def load(path: str | None = None):
                                  C.POINTER(C.c_uint64)]
     L.hh_cuda_correlation.argtypes = [C.POINTER(CalcParamsC), C.c_double, C.c_uint32, C.c_uint64,
                                       C.c_int, _dp, C.POINTER(C.c_double), C.POINTER(Stats)]
+    L.hh_cuda_correlation_multi.argtypes = [C.POINTER(CalcParamsC), C.c_double, C.c_uint32, C.c_uint64,
+                                            C.c_uint32, C.c_int, _dp, _dp, C.POINTER(Stats)]
     L.hh_cuda_correlation_ic.argtypes = [C.POINTER(CalcParamsC), _dp, C.c_uint64, C.c_int, _dp,
                                          C.POINTER(Stats)]
     L.hh_cuda_m0.argtypes = [C.POINTER(CalcParamsC), _dp, C.c_int, C.c_uint64, C.c_uint64, C.c_int,
@@ -108,6 +112,8 @@ def load(path: str | None = None):
     L.hh_cuda_strerror.argtypes = [C.c_int]
     L.hh_cuda_mt_stream.argtypes = [C.c_uint32, C.c_uint64, _u32p]
     L.hh_cuda_debug_inject.argtypes = [C.c_int, C.c_int, C.c_int, C.c_int]
+    L.hh_cuda_debug_item_trace.argtypes = [C.c_void_p, C.c_uint64]
+    L.hh_cuda_fma_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
     L.hh_cuda_shutdown.restype = None
     for name in EXPORTS:
         if name not in ("hh_cuda_strerror", "hh_cuda_shutdown"):

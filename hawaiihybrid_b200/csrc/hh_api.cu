@@ -17,6 +17,22 @@
 #include "hh_m0.cuh"
 #include "hh_traj.cuh"
 
+namespace hh {
+// 8 independent FMA chains per thread; the loop body is 8 FMAs = 16 flops
+template <typename T>
+__global__ void __launch_bounds__(256) fma_peak_kernel(T *out, int iters, T a, T b) {
+  T v[8];
+#pragma unroll
+  for (int i = 0; i < 8; ++i) v[i] = T(threadIdx.x + i) * T(1e-3);
+  for (int it = 0; it < iters; ++it) {
+#pragma unroll
+    for (int i = 0; i < 8; ++i) v[i] = v[i] * a + b;
+  }
+  T s = v[0] + v[1] + v[2] + v[3] + v[4] + v[5] + v[6] + v[7];
+  if (s == T(-12345.678)) out[threadIdx.x] = s;  // keeps the chains alive
+}
+}  // namespace hh
+
 namespace {
 
 using namespace hh;
@@ -80,6 +96,7 @@ struct Ctx {
   DevBuf<unsigned long long> counters;
   DevBuf<unsigned int> status_hist, queue;
   DevBuf<int> fail_flag, fail_list, fail_count, items;
+  DevBuf<uint4> trace;
   // M0
   DevBuf<double> m0_partials, m0_out;
   // FFT
@@ -88,7 +105,10 @@ struct Ctx {
 };
 
 Ctx g;
+unsigned long long g_launches = 0;  // kernel launches of the current call
 int g_inject_item = -1, g_inject_k = -1, g_inject_status = 0;
+uint32_t *g_trace_host = nullptr;  // registered by hh_cuda_debug_item_trace for the next call
+uint64_t g_trace_cap = 0;
 
 void build_tables(Co2arTablesGlobal *t) {
   memcpy(t->pes, hh_co2ar_pes, sizeof(t->pes));
@@ -138,6 +158,7 @@ int ensure_words(long long need_end) {
                        (size_t)left * sizeof(uint32_t), cudaMemcpyDeviceToDevice, g.st));
   }
   CK(launch_mt_generate(g.d_mt, g.words[nxt].p + left, nblk, g.st));
+  g_launches += 1;
   g.cur = nxt;
   g.wbase = g.wpos;
   g.wvalid = left + nblk * MT_N;
@@ -172,12 +193,14 @@ int sample_into(const hh_calc_params *p, double T, uint64_t n, double *d_out, ui
                          p->pair_state, g.d_tab, g.words[g.cur].p, g.wvalid, g.wpos - g.wbase, g.D,
                          ncand, g.accept.p, g.consumed.p, g.qp_cand.p, g.energy.p, g.scal.p,
                          g.st));
+    g_launches += 1;
     unsigned long long first_irr = 0;
     CK(cudaMemcpyAsync(&first_irr, g.scal.p, sizeof first_irr, cudaMemcpyDeviceToHost, g.st));
     CK(cudaStreamSynchronize(g.st));
     long long limit = (first_irr == ~0ULL) ? ncand - 1 : (long long)first_irr;
     CK(launch_compact(g.accept.p, g.qp_cand.p, ncand, limit, g.QP, (long long)got, (long long)n,
                       d_out, g.cand_idx.p, g.block_counts.p, g.scal.p + 1, g.st));
+    g_launches += 3;
     unsigned long long total = 0;
     CK(cudaMemcpyAsync(&total, g.scal.p + 1, sizeof total, cudaMemcpyDeviceToHost, g.st));
     CK(cudaStreamSynchronize(g.st));
@@ -227,6 +250,7 @@ int launch_traj(const TrajParams &P, const TrajIO &io, int *grid_out) {
   if (need < grid) grid = (int)std::max(1LL, need);
   kern<<<grid, 128, smem, g.st>>>(P, io, g.d_tab);
   CK(cudaGetLastError());
+  g_launches += 1;
   if (grid_out) *grid_out = grid;
   return HH_OK;
 }
@@ -240,10 +264,12 @@ int run_traj_dispatch(int precision, const TrajParams &P, const TrajIO &io) {
   return launch_traj<SYS_CO2AR, double, double, false>(P, io, nullptr);
 }
 
-// integrate both branches of n trajectories whose phase points are in d_ic
-int run_trajectories(const hh_calc_params *p, const double *d_ic, uint64_t n, int precision,
-                     double *crln_host, hh_stats *stats) {
+// integrate both branches of n trajectories whose phase points are in d_ic;
+// trajectories [i*per_iter, (i+1)*per_iter) accumulate into C(t) slice i
+int run_trajectories(const hh_calc_params *p, const double *d_ic, uint64_t n, uint64_t per_iter,
+                     int precision, double *crln_host, hh_stats *stats) {
   const size_t N = p->MaxTrajectoryLength;
+  const uint64_t n_iter = (n + per_iter - 1) / per_iter;
   TrajParams P;
   P.mu = g.mu;
   P.II = g.II;
@@ -257,17 +283,18 @@ int run_trajectories(const hh_calc_params *p, const double *d_ic, uint64_t n, in
   P.max_steps = p->max_steps > 0 ? p->max_steps : 50000;
   P.max_total_steps = 4000000;
   P.weight = p->partial_partition_function_ratio * 0.5 * HH_ALU * HH_ALU * HH_ALU;
+  P.noise_floor = 16.0 * 5.96e-8;  // 16 FP32 half-ulps
   P.inject_item = g_inject_item;
   P.inject_k = g_inject_k;
   P.inject_status = g_inject_status;
-  CK(g.crln.ensure(N));
+  CK(g.crln.ensure(N * n_iter));
   CK(g.counters.ensure(16));
   CK(g.status_hist.ensure(2 * HH_ST_COUNT));
   CK(g.queue.ensure(1));
   CK(g.fail_flag.ensure(std::max<uint64_t>(n, 1)));
   CK(g.fail_list.ensure(std::max<uint64_t>(n, 1)));
   CK(g.fail_count.ensure(1));
-  CK(cudaMemsetAsync(g.crln.p, 0, N * sizeof(double), g.st));
+  CK(cudaMemsetAsync(g.crln.p, 0, N * n_iter * sizeof(double), g.st));
   CK(cudaMemsetAsync(g.counters.p, 0, 16 * sizeof(unsigned long long), g.st));
   CK(cudaMemsetAsync(g.status_hist.p, 0, 2 * HH_ST_COUNT * sizeof(unsigned int), g.st));
   CK(cudaMemsetAsync(g.queue.p, 0, sizeof(unsigned int), g.st));
@@ -284,6 +311,15 @@ int run_trajectories(const hh_calc_params *p, const double *d_ic, uint64_t n, in
   io.fail_flag = g.fail_flag.p;
   io.fail_list = g.fail_list.p;
   io.fail_count = g.fail_count.p;
+  io.traj_per_iter = (long long)per_iter;
+  io.item_trace = nullptr;
+  uint32_t *trace_host = g_trace_host;
+  g_trace_host = nullptr;
+  if (trace_host && g_trace_cap >= 4 * 2 * n) {
+    CK(g.trace.ensure(2 * n));
+    CK(cudaMemsetAsync(g.trace.p, 0, 2 * n * sizeof(uint4), g.st));
+    io.item_trace = g.trace.p;
+  }
   CK(cudaEventRecord(g.ev[2], g.st));
   int rc = run_traj_dispatch(precision, P, io);
   if (rc) return rc;
@@ -310,11 +346,14 @@ int run_trajectories(const hh_calc_params *p, const double *d_ic, uint64_t n, in
     io2.fail_flag = nullptr;
     io2.counters = g.counters.p + 8;           // replay work is not counted twice
     io2.status_hist = g.status_hist.p + HH_ST_COUNT;
+    io2.item_trace = nullptr;
     rc = run_traj_dispatch(precision, P2, io2);
     if (rc) return rc;
   }
   CK(cudaEventRecord(g.ev[3], g.st));
-  CK(cudaMemcpyAsync(crln_host, g.crln.p, N * sizeof(double), cudaMemcpyDeviceToHost, g.st));
+  CK(cudaMemcpyAsync(crln_host, g.crln.p, N * n_iter * sizeof(double), cudaMemcpyDeviceToHost, g.st));
+  if (io.item_trace)
+    CK(cudaMemcpyAsync(trace_host, g.trace.p, 2 * n * sizeof(uint4), cudaMemcpyDeviceToHost, g.st));
   unsigned long long cnt[8];
   unsigned int hist[HH_ST_COUNT];
   CK(cudaMemcpyAsync(cnt, g.counters.p, sizeof cnt, cudaMemcpyDeviceToHost, g.st));
@@ -428,12 +467,15 @@ int hh_cuda_sample(const hh_calc_params *p, double T, uint32_t seed, uint64_t n,
   return HH_OK;
 }
 
-int hh_cuda_correlation(const hh_calc_params *p, double T, uint32_t seed, uint64_t n_accept,
-                        int precision_mode, double *crln_sum, double *ntraj, hh_stats *stats) {
+int hh_cuda_correlation_multi(const hh_calc_params *p, double T, uint32_t seed,
+                              uint64_t n_per_iteration, uint32_t n_iterations, int precision_mode,
+                              double *crln_sums, double *ntraj, hh_stats *stats) {
   if (!g.init) return HH_E_NOT_INITIALIZED;
   int rc = check_params(p);
   if (rc) return rc;
-  if (!(T > 0) || !crln_sum || n_accept == 0 || n_accept > (uint64_t)(INT32_MAX / 2))
+  const uint64_t n_accept = n_per_iteration * (uint64_t)n_iterations;
+  if (!(T > 0) || !crln_sums || n_per_iteration == 0 || n_iterations == 0 ||
+      n_accept > (uint64_t)(INT32_MAX / 2))
     return HH_E_INVALID_ARGUMENT;
   if (precision_mode != HH_PRECISION_FP64 && precision_mode != HH_PRECISION_MIXED)
     return HH_E_INVALID_ARGUMENT;
@@ -444,13 +486,14 @@ int hh_cuda_correlation(const hh_calc_params *p, double T, uint32_t seed, uint64
   }
   hh_stats local;
   memset(&local, 0, sizeof local);
+  g_launches = 0;
   CK(g.qp0.ensure(n_accept * g.QP));
   CK(cudaEventRecord(g.ev[0], g.st));
   uint64_t ncand = 0;
   rc = sample_into(p, T, n_accept, g.qp0.p, &ncand);
   if (rc) return rc;
   CK(cudaEventRecord(g.ev[1], g.st));
-  rc = run_trajectories(p, g.qp0.p, n_accept, precision_mode, crln_sum, &local);
+  rc = run_trajectories(p, g.qp0.p, n_accept, n_per_iteration, precision_mode, crln_sums, &local);
   if (rc) return rc;
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, g.ev[0], g.ev[1]));
@@ -459,9 +502,16 @@ int hh_cuda_correlation(const hh_calc_params *p, double T, uint32_t seed, uint64
   local.total_ms = ms;
   local.n_candidates = ncand;
   local.n_accepted = n_accept;
-  if (ntraj) *ntraj = (double)n_accept;
+  local.n_kernel_launches = g_launches;
+  if (ntraj)
+    for (uint32_t i = 0; i < n_iterations; ++i) ntraj[i] = (double)n_per_iteration;
   if (stats) *stats = local;
   return HH_OK;
+}
+
+int hh_cuda_correlation(const hh_calc_params *p, double T, uint32_t seed, uint64_t n_accept,
+                        int precision_mode, double *crln_sum, double *ntraj, hh_stats *stats) {
+  return hh_cuda_correlation_multi(p, T, seed, n_accept, 1, precision_mode, crln_sum, ntraj, stats);
 }
 
 int hh_cuda_correlation_ic(const hh_calc_params *p, const double *qp0, uint64_t n,
@@ -475,16 +525,18 @@ int hh_cuda_correlation_ic(const hh_calc_params *p, const double *qp0, uint64_t 
   CK(cudaSetDevice(g.device));
   hh_stats local;
   memset(&local, 0, sizeof local);
+  g_launches = 0;
   CK(g.qp0.ensure(n * g.QP));
   CK(cudaEventRecord(g.ev[0], g.st));
   CK(cudaMemcpyAsync(g.qp0.p, qp0, n * g.QP * sizeof(double), cudaMemcpyHostToDevice, g.st));
   CK(cudaEventRecord(g.ev[1], g.st));
-  rc = run_trajectories(p, g.qp0.p, n, precision_mode, crln_sum, &local);
+  rc = run_trajectories(p, g.qp0.p, n, n, precision_mode, crln_sum, &local);
   if (rc) return rc;
   float ms = 0.f;
   CK(cudaEventElapsedTime(&ms, g.ev[0], g.ev[3]));
   local.total_ms = ms;
   local.n_accepted = n;
+  local.n_kernel_launches = g_launches;
   if (stats) *stats = local;
   return HH_OK;
 }
@@ -591,6 +643,12 @@ int hh_cuda_mt_stream(uint32_t seed, uint64_t n, uint32_t *out) {
   return reseed(seed);
 }
 
+int hh_cuda_debug_item_trace(uint32_t *out, uint64_t capacity_words) {
+  g_trace_host = out;
+  g_trace_cap = out ? capacity_words : 0;
+  return HH_OK;
+}
+
 int hh_cuda_debug_inject(int traj, int dir, int k, int status) {
   if (status < 0 || status >= HH_ST_COUNT || dir < 0 || dir > 1) return HH_E_INVALID_ARGUMENT;
   if (traj < 0) {
@@ -601,6 +659,37 @@ int hh_cuda_debug_inject(int traj, int dir, int k, int status) {
   g_inject_item = 2 * traj + dir;
   g_inject_k = k;
   g_inject_status = status;
+  return HH_OK;
+}
+
+int hh_cuda_fma_peak(int precision, double *tflops) {
+  if (!g.init) return HH_E_NOT_INITIALIZED;
+  if (!tflops) return HH_E_INVALID_ARGUMENT;
+  CK(cudaSetDevice(g.device));
+  const int iters = 1 << 15;
+  double best = 0.0;
+  CK(g.m0_out.ensure(M0_MAXT * 2));
+  for (int rep = 0; rep < 4; ++rep) {
+    int per_sm = 0;
+    if (precision == HH_PRECISION_FP64)
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fma_peak_kernel<double>, 256, 0));
+    else
+      CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, fma_peak_kernel<float>, 256, 0));
+    int grid = per_sm * g.num_sms;
+    CK(cudaEventRecord(g.ev[0], g.st));
+    if (precision == HH_PRECISION_FP64)
+      fma_peak_kernel<double><<<grid, 256, 0, g.st>>>(g.m0_out.p, iters, 0.999999, 1e-7);
+    else
+      fma_peak_kernel<float><<<grid, 256, 0, g.st>>>((float *)g.m0_out.p, iters, 0.999999f, 1e-7f);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(g.ev[1], g.st));
+    CK(cudaEventSynchronize(g.ev[1]));
+    float ms = 0.f;
+    CK(cudaEventElapsedTime(&ms, g.ev[0], g.ev[1]));
+    double flops = double(grid) * 256.0 * iters * 16.0;
+    best = std::max(best, flops / (ms * 1e-3) / 1e12);
+  }
+  *tflops = best;
   return HH_OK;
 }
 
@@ -626,6 +715,7 @@ void hh_cuda_shutdown(void) {
   g.fail_list.release();
   g.fail_count.release();
   g.items.release();
+  g.trace.release();
   g.m0_partials.release();
   g.m0_out.release();
   g.f_cf.release();

@@ -1,5 +1,5 @@
 // Persistent trajectory kernel: one half-trajectory (forward or momentum-
-// inverted backward branch of src/hawaii.c:2116-2347) per thread, integrated
+// inverted backward branch of src/hawaii.c:2116-2347) per lane, integrated
 // with DOP853 and its 7th-order dense output, the induced dipole sampled at
 // t_k = k*dt and mu0.mu(t_k) added into the ensemble C(t) in FP64.
 //
@@ -8,6 +8,11 @@
 // item adds  w * mu0.mu(t_k)  for its samples, w = ppf * ALU^3 / 2, so the two
 // branches together reproduce crln[k] = ppf * (fwd[k] + bwd[k]) / 2 * ALU^3
 // (src/hawaii.c:2334-2337, 3008).
+//
+// Execution is warp-synchronous: every round, all lanes of a warp refill
+// finished items, attempt one step, run the dense-output stages and emit their
+// samples together, so the warp stays converged (one instruction stream, all
+// lanes busy) instead of each lane wandering through its own item.
 //
 // Precision: PHYS is the type the surfaces are evaluated in (double for the
 // plain path, float for the mixed path, with compensated sums); STG is the type
@@ -41,6 +46,9 @@ struct TrajParams {
   // test hook: half-trajectory (2*traj + dir) that reports status inject_status
   // at sample inject_k instead of storing it (-1: off)
   int inject_item, inject_k, inject_status;
+  // FP32 stages only: rounding-noise level of the stage derivatives, in units
+  // of their magnitude, added to the error tolerance
+  double noise_floor;
 };
 
 struct TrajIO {
@@ -54,7 +62,15 @@ struct TrajIO {
   int *fail_flag;             // [n_traj] (nullptr on the compensation pass)
   int *fail_list;
   int *fail_count;
+  long long traj_per_iter;    // trajectories per iteration; item -> C(t) slice of its iteration
+  uint4 *item_trace;          // optional per-item (steps, samples, t_start, t_end) in ns
 };
+
+__device__ __forceinline__ unsigned long long globaltimer_ns() {
+  unsigned long long t;
+  asm volatile("mov.u64 %0, %globaltimer;" : "=l"(t));
+  return t;
+}
 
 // ---- coefficient tables for CO2-Ar, staged in shared memory ----
 template <typename T> struct Co2arTables {
@@ -96,6 +112,9 @@ __device__ void load_tables(Co2arTables<T> *s, const Co2arTablesGlobal *g) {
 template <typename PHYS, typename STG, bool COMP> struct HeArSys {
   static constexpr int N = 6;
   static constexpr int QP = 6;
+  // components the dipole and the R > Rcut test read: r
+  static constexpr int NQ = 3;
+  static __device__ __forceinline__ constexpr int qidx(int i) { return i; }
   double inv_mu;
   __device__ void rhs(const double *y, STG *f) const {
     PHYS r0 = PHYS(y[0]), r1 = PHYS(y[1]), r2 = PHYS(y[2]);
@@ -124,6 +143,9 @@ template <typename PHYS, typename STG, bool COMP> struct HeArSys {
 template <typename PHYS, typename STG, bool COMP> struct Co2ArSys {
   static constexpr int N = 12;
   static constexpr int QP = 10;
+  // components the dipole and the R > Rcut test read: r and u
+  static constexpr int NQ = 6;
+  static __device__ __forceinline__ constexpr int qidx(int i) { return i < 3 ? i : i + 3; }
   double inv_mu, inv_II;
   const Co2arTables<PHYS> *tb;
   __device__ void rhs(const double *y, STG *f) const {
@@ -154,9 +176,10 @@ template <typename PHYS, typename STG, bool COMP> struct Co2ArSys {
     f[10] = STG(-Vx * (uh[2] * rh[0] - uh[0] * rh[2]));
     f[11] = STG(-Vx * (uh[0] * rh[1] - uh[1] * rh[0]));
   }
-  __device__ void dipole(const double *y, PHYS d[3]) const {
-    PHYS r[3] = {PHYS(y[0]), PHYS(y[1]), PHYS(y[2])};
-    PHYS u[3] = {PHYS(y[6]), PHYS(y[7]), PHYS(y[8])};
+  // q = (r[3], u[3])
+  __device__ void dipole(const double *q, PHYS d[3]) const {
+    PHYS r[3] = {PHYS(q[0]), PHYS(q[1]), PHYS(q[2])};
+    PHYS u[3] = {PHYS(q[3]), PHYS(q[4]), PHYS(q[5])};
     PHYS R = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
     PHYS iR = PHYS(1) / R;
     PHYS iu = PHYS(1) / sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
@@ -206,133 +229,135 @@ __device__ __forceinline__ void qp_to_state(const double *qp, double *y) {
 // ---------------------------------------------------------------------------
 // DOP853 (Hairer-Norsett-Wanner) with the standard step controller
 // (safety 0.9, factors in [0.2, 10], exponent -1/8) and dense output.
+// The stage derivatives K stay in registers (all indices compile-time).
 // ---------------------------------------------------------------------------
-template <class Sys, typename STG>
-struct Dop853 {
-  static constexpr int N = Sys::N;
-  STG K[16][N];
-
-  // one adaptive step from (t, y) with K[0] = f(t, y); returns 0 or a status
-  __device__ int step(const Sys &sys, const TrajParams &P, double t, const double *y, double &h,
-                      double &h_taken, double *y_new, unsigned &nrej, unsigned &nrhs) {
-    bool rejected = false;
-    for (;;) {
-      // 10 * spacing of doubles above t (t >= 0 and finite)
-      double min_step = 10.0 * (__longlong_as_double(__double_as_longlong(t) + 1) - t);
-      if (!(h >= min_step)) return HH_ST_H_UNDERFLOW;
-#pragma unroll
-      for (int s = 1; s < 12; ++s) {
-        double ys[N];
-#pragma unroll
-        for (int i = 0; i < N; ++i) {
-          STG acc = STG(0);
-#pragma unroll
-          for (int j = 0; j < s; ++j)
-            if (hh_dop853_a[s][j] != 0.0) acc += STG(hh_dop853_a[s][j]) * K[j][i];
-          ys[i] = y[i] + h * double(acc);
-        }
-        sys.rhs(ys, K[s]);
-      }
-#pragma unroll
-      for (int i = 0; i < N; ++i) {
-        STG acc = STG(0);
-#pragma unroll
-        for (int j = 0; j < 12; ++j)
-          if (hh_dop853_a[12][j] != 0.0) acc += STG(hh_dop853_a[12][j]) * K[j][i];
-        y_new[i] = y[i] + h * double(acc);
-      }
-      sys.rhs(y_new, K[12]);
-      nrhs += 12;
-      double e5 = 0.0, e3 = 0.0;
-#pragma unroll
-      for (int i = 0; i < N; ++i) {
-        double sc = P.atol + fmax(fabs(y[i]), fabs(y_new[i])) * P.rtol;
-        STG a5 = STG(0), a3 = STG(0);
-#pragma unroll
-        for (int j = 0; j < 13; ++j) {
-          if (hh_dop853_e5[j] != 0.0) a5 += STG(hh_dop853_e5[j]) * K[j][i];
-          if (hh_dop853_e3[j] != 0.0) a3 += STG(hh_dop853_e3[j]) * K[j][i];
-        }
-        double q5 = double(a5) / sc, q3 = double(a3) / sc;
-        e5 += q5 * q5;
-        e3 += q3 * q3;
-      }
-      double err = (e5 == 0.0 && e3 == 0.0) ? 0.0 : fabs(h) * e5 / sqrt((e5 + 0.01 * e3) * N);
-      if (err < 1.0) {
-        double fac = (err == 0.0) ? 10.0 : fmin(10.0, 0.9 * pow(err, -0.125));
-        if (rejected) fac = fmin(1.0, fac);
-        h_taken = h;
-        h = h * fac;
-        return HH_ST_OK;
-      }
-      h *= fmax(0.2, 0.9 * pow(err, -0.125));
-      rejected = true;
-      ++nrej;
-    }
-  }
-
-  // dense-output coefficients F[7][N] of the last step (needs K[0..12])
-  __device__ void dense(const Sys &sys, const double *y_old, const double *y_new, double h,
-                        STG (&F)[7][N], unsigned &nrhs) {
-#pragma unroll
-    for (int s = 13; s < 16; ++s) {
-      double ys[N];
-#pragma unroll
-      for (int i = 0; i < N; ++i) {
-        STG acc = STG(0);
-#pragma unroll
-        for (int j = 0; j < s; ++j)
-          if (hh_dop853_a[s][j] != 0.0) acc += STG(hh_dop853_a[s][j]) * K[j][i];
-        ys[i] = y_old[i] + h * double(acc);
-      }
-      sys.rhs(ys, K[s]);
-    }
-    nrhs += 3;
-#pragma unroll
-    for (int i = 0; i < N; ++i) {
-      double dy = y_new[i] - y_old[i];
-      F[0][i] = STG(dy);
-      F[1][i] = STG(h * double(K[0][i]) - dy);
-      F[2][i] = STG(2.0 * dy - h * (double(K[12][i]) + double(K[0][i])));
-#pragma unroll
-      for (int r = 0; r < 4; ++r) {
-        STG acc = STG(0);
-#pragma unroll
-        for (int j = 0; j < 16; ++j)
-          if (hh_dop853_d[r][j] != 0.0) acc += STG(hh_dop853_d[r][j]) * K[j][i];
-        F[3 + r][i] = STG(h * double(acc));
-      }
-    }
-  }
-};
-
-template <int N, typename STG>
-__device__ __forceinline__ void dense_eval(const double *y_old, const STG (&F)[7][N], double x,
-                                           double *y) {
-  double x1 = 1.0 - x;
+template <int N, typename STG, int S>
+__device__ __forceinline__ void stage_point(const STG (&K)[16][N], const double *y, double h,
+                                            double *ys) {
 #pragma unroll
   for (int i = 0; i < N; ++i) {
-    double v = double(F[6][i]) * x;
-    v = (v + double(F[5][i])) * x1;
-    v = (v + double(F[4][i])) * x;
-    v = (v + double(F[3][i])) * x1;
-    v = (v + double(F[2][i])) * x;
-    v = (v + double(F[1][i])) * x1;
-    v = (v + double(F[0][i])) * x;
-    y[i] = y_old[i] + v;
+    STG acc = STG(0);
+#pragma unroll
+    for (int j = 0; j < S; ++j)
+      if (hh_dop853_a[S][j] != 0.0) acc += STG(hh_dop853_a[S][j]) * K[j][i];
+    ys[i] = y[i] + h * double(acc);
   }
 }
 
-template <class Sys>
-__device__ __forceinline__ double state_R(const double *y) {
-  return sqrt(y[0] * y[0] + y[1] * y[1] + y[2] * y[2]);
+// stages 1..12 of one step attempt from (y, K[0] = f(y)); y_new is the 8th-order
+// solution and K[12] = f(y_new); returns the error norm
+template <class Sys, typename STG>
+__device__ __forceinline__ double step_attempt(const Sys &sys, const TrajParams &P,
+                                               STG (&K)[16][Sys::N], const double *y, double h,
+                                               double *y_new) {
+  constexpr int N = Sys::N;
+#define HH_STAGE(S)                                 \
+  {                                                 \
+    double ys[N];                                   \
+    stage_point<N, STG, S>(K, y, h, ys);            \
+    sys.rhs(ys, K[S]);                              \
+  }
+  HH_STAGE(1) HH_STAGE(2) HH_STAGE(3) HH_STAGE(4) HH_STAGE(5) HH_STAGE(6)
+  HH_STAGE(7) HH_STAGE(8) HH_STAGE(9) HH_STAGE(10) HH_STAGE(11)
+#undef HH_STAGE
+  stage_point<N, STG, 12>(K, y, h, y_new);
+  sys.rhs(y_new, K[12]);
+  double e5 = 0.0, e3 = 0.0;
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    double sc = P.atol + fmax(fabs(y[i]), fabs(y_new[i])) * P.rtol;
+    STG a5 = STG(0), a3 = STG(0), m5 = STG(0);
+#pragma unroll
+    for (int j = 0; j < 13; ++j) {
+      if (hh_dop853_e5[j] != 0.0) {
+        a5 += STG(hh_dop853_e5[j]) * K[j][i];
+        if (sizeof(STG) == 4) m5 += fabs(STG(hh_dop853_e5[j]) * K[j][i]);
+      }
+      if (hh_dop853_e3[j] != 0.0) a3 += STG(hh_dop853_e3[j]) * K[j][i];
+    }
+    // FP32 stages: the estimate cannot resolve errors below the rounding noise of
+    // the stage derivatives, so that noise widens the tolerance
+    if (sizeof(STG) == 4) sc += fabs(h) * P.noise_floor * double(m5);
+    double q5 = double(a5) / sc, q3 = double(a3) / sc;
+    e5 += q5 * q5;
+    e3 += q3 * q3;
+  }
+  return (e5 == 0.0 && e3 == 0.0) ? 0.0 : fabs(h) * e5 / sqrt((e5 + 0.01 * e3) * N);
 }
 
-// initial step size (Hairer's algorithm, error-estimator order 7)
+// the three extra stages of the dense output and its coefficients F[7][NQ] for
+// the components the samples read
 template <class Sys, typename STG>
-__device__ double initial_step(const Sys &sys, const TrajParams &P, const double *y0,
-                               const STG *f0, double span, unsigned &nrhs) {
+__device__ __forceinline__ void dense_stages(const Sys &sys, STG (&K)[16][Sys::N], const double *y_old,
+                                             const double *y_new, double h, STG (&F)[7][Sys::NQ]) {
   constexpr int N = Sys::N;
+#define HH_STAGE(S)                                 \
+  {                                                 \
+    double ys[N];                                   \
+    stage_point<N, STG, S>(K, y_old, h, ys);        \
+    sys.rhs(ys, K[S]);                              \
+  }
+  HH_STAGE(13) HH_STAGE(14) HH_STAGE(15)
+#undef HH_STAGE
+#pragma unroll
+  for (int c = 0; c < Sys::NQ; ++c) {
+    const int i = Sys::qidx(c);
+    double dy = y_new[i] - y_old[i];
+    F[0][c] = STG(dy);
+    F[1][c] = STG(h * double(K[0][i]) - dy);
+    F[2][c] = STG(2.0 * dy - h * (double(K[12][i]) + double(K[0][i])));
+#pragma unroll
+    for (int r = 0; r < 4; ++r) {
+      STG acc = STG(0);
+#pragma unroll
+      for (int j = 0; j < 16; ++j)
+        if (hh_dop853_d[r][j] != 0.0) acc += STG(hh_dop853_d[r][j]) * K[j][i];
+      F[3 + r][c] = STG(h * double(acc));
+    }
+  }
+}
+
+// dense output y(t_old + x h) = y_old + x(F0 + (1-x)(F1 + x(F2 + ... ))); the
+// increment is formed in STG precision and added to the FP64 state
+template <class Sys, typename STG>
+__device__ __forceinline__ void dense_eval(const double *y_old, const STG (&F)[7][Sys::NQ], double x,
+                                           double *q) {
+  const STG xs = STG(x), x1 = STG(1) - STG(x);
+#pragma unroll
+  for (int i = 0; i < Sys::NQ; ++i) {
+    STG v = F[6][i] * xs;
+    v = (v + F[5][i]) * x1;
+    v = (v + F[4][i]) * xs;
+    v = (v + F[3][i]) * x1;
+    v = (v + F[2][i]) * xs;
+    v = (v + F[1][i]) * x1;
+    v = (v + F[0][i]) * xs;
+    q[i] = y_old[Sys::qidx(i)] + double(v);
+  }
+}
+
+// Per-item set-up, out of line (once per half-trajectory): Cartesian initial
+// state (momenta inverted for the backward branch), mu0, f(y0) and the initial
+// step size of Hairer's algorithm (error-estimator order 7).
+template <class Sys, typename PHYS, typename STG>
+__device__ __noinline__ void item_setup(const Sys &sys, const TrajParams &P, const double *qp,
+                                        int dir, double *y0, STG *f0, PHYS *mu0, double *h_out) {
+  constexpr int N = Sys::N;
+  constexpr int SYS = (N == 6) ? SYS_HEAR : SYS_CO2AR;
+  qp_to_state<SYS>(qp, y0);
+  double q0[Sys::NQ];
+#pragma unroll
+  for (int c = 0; c < Sys::NQ; ++c) q0[c] = y0[Sys::qidx(c)];
+  sys.dipole(q0, mu0);
+  if (dir) {
+    // invert_momenta (src/hawaii.c:1171-1188): p -> -p, j -> -j
+#pragma unroll
+    for (int i = 3; i < 6; ++i) y0[i] = -y0[i];
+#pragma unroll
+    for (int i = 9; i < N; ++i) y0[i] = -y0[i];
+  }
+  sys.rhs(y0, f0);
+  const double span = P.dt * double(P.N - 1);
   double d0 = 0.0, d1 = 0.0;
 #pragma unroll
   for (int i = 0; i < N; ++i) {
@@ -350,7 +375,6 @@ __device__ double initial_step(const Sys &sys, const TrajParams &P, const double
 #pragma unroll
   for (int i = 0; i < N; ++i) y1[i] = y0[i] + h0 * double(f0[i]);
   sys.rhs(y1, f1);
-  ++nrhs;
   double d2 = 0.0;
 #pragma unroll
   for (int i = 0; i < N; ++i) {
@@ -360,75 +384,7 @@ __device__ double initial_step(const Sys &sys, const TrajParams &P, const double
   }
   d2 = sqrt(d2 / N) / h0;
   double h1 = (d1 <= 1e-15 && d2 <= 1e-15) ? fmax(1e-6, h0 * 1e-3) : pow(0.01 / fmax(d1, d2), 0.125);
-  return fmin(fmin(100.0 * h0, h1), span);
-}
-
-// ---------------------------------------------------------------------------
-// one half-trajectory; returns its status, *hard = 1 for the failures that make
-// the reference drop the whole trajectory
-// ---------------------------------------------------------------------------
-template <class Sys, typename PHYS, typename STG>
-__device__ int run_half(const Sys &sys, const TrajParams &P, const double *y0, const PHYS mu0[3],
-                        double *crln, unsigned &nsteps, unsigned &nrej, unsigned &nrhs,
-                        unsigned &nsamp, unsigned &ndense, int &hard, int item) {
-  constexpr int N = Sys::N;
-  Dop853<Sys, STG> dop;
-  double y[N], y_new[N];
-#pragma unroll
-  for (int i = 0; i < N; ++i) y[i] = y0[i];
-  sys.rhs(y, dop.K[0]);
-  ++nrhs;
-  const double dt = P.dt;
-  double h = initial_step<Sys, STG>(sys, P, y, dop.K[0], dt * double(P.N - 1), nrhs);
-  double t = 0.0;
-  int k = 1;
-  long long since = 0, total = 0;
-  PHYS prev = PHYS(0), curr = PHYS(0);
-  hard = 0;
-  while (k < P.N) {
-    double ht;
-    int rc = dop.step(sys, P, t, y, h, ht, y_new, nrej, nrhs);
-    if (rc) return rc;
-    ++nsteps;
-    double t_new = t + ht;
-    if (double(k) * dt <= t_new) {
-      STG F[7][N];
-      dop.dense(sys, y, y_new, ht, F, nrhs);
-      ++ndense;
-      do {
-        double x = (double(k) * dt - t) / ht;
-        double ys[N];
-        dense_eval<N, STG>(y, F, x, ys);
-        PHYS d[3];
-        sys.dipole(ys, d);
-        ++nsamp;
-        if (isnan(d[0]) || isnan(d[1]) || isnan(d[2])) { hard = 1; return HH_ST_NAN_DIPOLE; }
-        if (item == P.inject_item && k == P.inject_k) {
-          hard = (P.inject_status >= HH_ST_NAN_DIPOLE);
-          return P.inject_status;
-        }
-        prev = curr;
-        curr = mu0[0] * d[0] + mu0[1] * d[1] + mu0[2] * d[2];
-        if (fabs(double(curr)) > 1e100) { hard = 1; return HH_ST_OVERFLOW; }
-        if (k > 1) {
-          double ratio = fabs(double(curr) / double(prev));
-          if (ratio > 1e10) { hard = 1; return HH_ST_JUMP; }
-        }
-        atomicAdd(&crln[k], P.weight * double(curr));
-        ++k;
-        since = 0;
-        if (state_R<Sys>(ys) > P.Rcut) return HH_ST_OK;
-      } while (k < P.N && double(k) * dt <= t_new);
-    }
-    t = t_new;
-#pragma unroll
-    for (int i = 0; i < N; ++i) {
-      y[i] = y_new[i];
-      dop.K[0][i] = dop.K[12][i];
-    }
-    if (++since > P.max_steps || ++total > P.max_total_steps) return HH_ST_MAXSTEPS;
-  }
-  return HH_ST_OK;
+  *h_out = fmin(fmin(100.0 * h0, h1), span);
 }
 
 __device__ __forceinline__ void warp_add_counter(unsigned long long *dst, unsigned v) {
@@ -438,41 +394,182 @@ __device__ __forceinline__ void warp_add_counter(unsigned long long *dst, unsign
   if ((threadIdx.x & 31) == 0 && s) atomicAdd(dst, s);
 }
 
+// ---------------------------------------------------------------------------
+// warp-synchronous persistent loop over half-trajectory items
+// ---------------------------------------------------------------------------
 template <class Sys, typename PHYS, typename STG>
 __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, const TrajIO &io) {
   constexpr int N = Sys::N;
-  constexpr int SYS = (N == 6) ? SYS_HEAR : SYS_CO2AR;
+  constexpr unsigned FULL = 0xffffffffu;
+  const int lane = threadIdx.x & 31;
+  const double dt = P.dt;
   unsigned nsteps = 0, nrej = 0, nrhs = 0, nsamp = 0, ndense = 0, nitems = 0;
+  // per-lane item state
+  STG K[16][N];
+  double y[N], y_new[N];
+  double t = 0.0, h = 0.0;
+  PHYS mu0[3] = {PHYS(0), PHYS(0), PHYS(0)};
+  PHYS prev = PHYS(0), curr = PHYS(0);
+  double *crln = io.crln;
+  int item = -1;           // -1: needs an item, -2: queue exhausted
+  int k = 1;
+  int since = 0, total = 0;
+  bool rejected = false;
+  unsigned long long t_begin = 0ull;
+  unsigned s0 = 0, m0 = 0;
   for (;;) {
-    unsigned idx = atomicAdd(io.queue, 1u);
-    if (idx >= (unsigned)io.n_items) break;
-    int item = io.items ? io.items[idx] : (int)idx;
-    int traj = item >> 1, dir = item & 1;
-    double y0[N];
-    qp_to_state<SYS>(io.ic + (size_t)traj * Sys::QP, y0);
-    PHYS mu0[3];
-    sys.dipole(y0, mu0);
-    if (dir) {
-      // invert_momenta (src/hawaii.c:1171-1188): p -> -p, j -> -j
+    // ---- refill: lanes without an item take the next ones (one atomic per warp) ----
+    const bool need = (item == -1);
+    const unsigned needmask = __ballot_sync(FULL, need);
+    if (needmask) {
+      unsigned base = 0;
+      const int leader = __ffs(needmask) - 1;
+      if (lane == leader) base = atomicAdd(io.queue, (unsigned)__popc(needmask));
+      base = __shfl_sync(FULL, base, leader);
+      if (need) {
+        const unsigned idx = base + __popc(needmask & ((1u << lane) - 1u));
+        if (idx < (unsigned)io.n_items) {
+          item = io.items ? io.items[idx] : (int)idx;
+          const int traj = item >> 1;
+          crln = io.crln + (size_t)(traj / io.traj_per_iter) * (size_t)P.N;
+          if (io.item_trace) t_begin = globaltimer_ns();
+          s0 = nsteps;
+          m0 = nsamp;
+          // out-of-line set-up writes through pointers to temporaries only, so
+          // y, K and mu0 never become addressable and stay in registers
+          double y_t[N];
+          STG f_t[N];
+          PHYS mu_t[3];
+          item_setup<Sys, PHYS, STG>(sys, P, io.ic + (size_t)traj * Sys::QP, item & 1, y_t, f_t,
+                                     mu_t, &h);
 #pragma unroll
-      for (int i = 3; i < 6; ++i) y0[i] = -y0[i];
+          for (int i = 0; i < N; ++i) {
+            y[i] = y_t[i];
+            K[0][i] = f_t[i];
+          }
 #pragma unroll
-      for (int i = 9; i < N; ++i) y0[i] = -y0[i];
-    }
-    PHYS c0 = mu0[0] * mu0[0] + mu0[1] * mu0[1] + mu0[2] * mu0[2];
-    int hard = 0;
-    int st = run_half<Sys, PHYS, STG>(sys, P, y0, mu0, io.crln, nsteps, nrej, nrhs, nsamp,
-                                      ndense, hard, item);
-    // the t = 0 term is added by branches that are not dropped, so a replay
-    // with the opposite weight removes exactly what a dropped trajectory added
-    if (!hard) atomicAdd(&io.crln[0], P.weight * double(c0));
-    atomicAdd(&io.status_hist[st], 1u);
-    ++nitems;
-    if (hard && io.fail_flag) {
-      if (atomicExch(&io.fail_flag[traj], 1) == 0) {
-        int slot = atomicAdd(io.fail_count, 1);
-        io.fail_list[slot] = traj;
+          for (int c = 0; c < 3; ++c) mu0[c] = mu_t[c];
+          nrhs += 2;
+          t = 0.0;
+          k = 1;
+          since = total = 0;
+          rejected = false;
+          prev = curr = PHYS(0);
+        } else {
+          item = -2;
+        }
       }
+    }
+    if (__all_sync(FULL, item == -2)) break;
+    const bool active = (item >= 0);
+
+    // ---- one step attempt for every lane that holds an item ----
+    int status = -1;  // >= 0: this lane's item ended with that status this round
+    int hard = 0;
+    bool accepted = false;
+    double h_taken = 0.0;
+    if (active) {
+      // 10 * spacing of doubles above t (t >= 0 and finite)
+      const double min_step = 10.0 * (__longlong_as_double(__double_as_longlong(t) + 1) - t);
+      if (!(h >= min_step)) {
+        status = HH_ST_H_UNDERFLOW;
+      } else {
+        const double err = step_attempt<Sys, STG>(sys, P, K, y, h, y_new);
+        nrhs += 12;
+        if (err < 1.0) {
+          double fac = (err == 0.0) ? 10.0 : fmin(10.0, 0.9 * pow(err, -0.125));
+          if (rejected) fac = fmin(1.0, fac);
+          rejected = false;
+          h_taken = h;
+          h *= fac;
+          accepted = true;
+          ++nsteps;
+        } else {
+          h *= fmax(0.2, 0.9 * pow(err, -0.125));
+          rejected = true;
+          ++nrej;
+        }
+      }
+    }
+
+    // ---- dense output and samples for steps that passed a sample time ----
+    bool pending = accepted && (double(k) * dt <= t + h_taken);
+    if (__any_sync(FULL, pending)) {
+      STG F[7][Sys::NQ];
+      if (pending) {
+        dense_stages<Sys, STG>(sys, K, y, y_new, h_taken, F);
+        nrhs += 3;
+        ++ndense;
+      }
+      const double t_new = t + h_taken;
+      while (__any_sync(FULL, pending)) {
+        if (pending) {
+          const double x = (double(k) * dt - t) / h_taken;
+          double q[Sys::NQ];
+          dense_eval<Sys, STG>(y, F, x, q);
+          PHYS d[3];
+          sys.dipole(q, d);
+          ++nsamp;
+          if (isnan(d[0]) || isnan(d[1]) || isnan(d[2])) {
+            status = HH_ST_NAN_DIPOLE;
+            hard = 1;
+          } else if (item == P.inject_item && k == P.inject_k) {
+            status = P.inject_status;
+            hard = (P.inject_status >= HH_ST_NAN_DIPOLE);
+          } else {
+            prev = curr;
+            curr = mu0[0] * d[0] + mu0[1] * d[1] + mu0[2] * d[2];
+            if (fabs(double(curr)) > 1e100) {
+              status = HH_ST_OVERFLOW;
+              hard = 1;
+            } else if (k > 1 && fabs(double(curr) / double(prev)) > 1e10) {
+              status = HH_ST_JUMP;
+              hard = 1;
+            } else {
+              atomicAdd(&crln[k], P.weight * double(curr));
+              ++k;
+              since = 0;
+              if (sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) > P.Rcut) status = HH_ST_OK;
+            }
+          }
+          pending = (status < 0) && (k < P.N) && (double(k) * dt <= t_new);
+        }
+      }
+    }
+
+    // ---- advance accepted lanes; close finished items ----
+    if (active && status < 0 && accepted) {
+      t += h_taken;
+#pragma unroll
+      for (int i = 0; i < N; ++i) {
+        y[i] = y_new[i];
+        K[0][i] = K[12][i];  // FSAL
+      }
+      if (k >= P.N) status = HH_ST_OK;
+      else if (++since > P.max_steps || ++total > P.max_total_steps) status = HH_ST_MAXSTEPS;
+    }
+    if (active && status >= 0) {
+      const int traj = item >> 1;
+      // the t = 0 term is added by branches that are not dropped, so a replay
+      // with the opposite weight removes exactly what a dropped trajectory added
+      if (!hard) {
+        const PHYS c0 = mu0[0] * mu0[0] + mu0[1] * mu0[1] + mu0[2] * mu0[2];
+        atomicAdd(&crln[0], P.weight * double(c0));
+      }
+      if (io.item_trace) {
+        const unsigned long long t_end = globaltimer_ns();
+        io.item_trace[item] = make_uint4(nsteps - s0, nsamp - m0, (unsigned)(t_begin & 0xffffffffu),
+                                         (unsigned)(t_end & 0xffffffffu));
+      }
+      atomicAdd(&io.status_hist[status], 1u);
+      ++nitems;
+      if (hard && io.fail_flag) {
+        if (atomicExch(&io.fail_flag[traj], 1) == 0) {
+          const int slot = atomicAdd(io.fail_count, 1);
+          io.fail_list[slot] = traj;
+        }
+      }
+      item = -1;
     }
   }
   warp_add_counter(&io.counters[0], nsteps);

@@ -186,6 +186,20 @@ def correlation_iteration(ms: MoleculeSystem, params: CalcParams, Temperature: f
     return crln, ntraj.value, st
 
 
+def correlation_iterations(ms: MoleculeSystem, params: CalcParams, Temperature: float, n_per_iteration: int,
+                           n_iterations: int, precision: int = PRECISION_FP64, seed: int = 0):
+    """n_iterations accumulation passes in one launch: returns
+    (crln_sums[n_iterations, N], ntraj[n_iterations], stats)."""
+    L = _bind(ms)
+    crln = np.zeros(n_iterations * params.MaxTrajectoryLength, dtype=np.float64)
+    ntraj = np.zeros(n_iterations, dtype=np.float64)
+    st = _lib.Stats()
+    pc = params.to_c()
+    check(L.hh_cuda_correlation_multi(C.byref(pc), Temperature, seed, n_per_iteration, n_iterations,
+                                      precision, crln, ntraj, C.byref(st)))
+    return crln.reshape(n_iterations, -1), ntraj, st
+
+
 def correlation_from_initial_conditions(ms: MoleculeSystem, params: CalcParams, qp0: np.ndarray,
                                         precision: int = PRECISION_FP64):
     """correlation_eval + accumulation over caller-supplied phase points."""
@@ -200,7 +214,7 @@ def correlation_from_initial_conditions(ms: MoleculeSystem, params: CalcParams, 
 
 
 def calculate_correlation_and_save(ms: MoleculeSystem, params: CalcParams, Temperature: float,
-                                   precision: int = PRECISION_FP64, log=print) -> CFnc:
+                                   precision: int = PRECISION_FP64, log=print, group: int = 4) -> CFnc:
     """calculate_correlation_and_save (src/hawaii.c:2795-3119): niterations passes of
     total_trajectories/niterations trajectories, the CF file rewritten after each
     pass, the result normalised by ntraj."""
@@ -214,17 +228,23 @@ def calculate_correlation_and_save(ms: MoleculeSystem, params: CalcParams, Tempe
     per_iter = params.total_trajectories // params.niterations
     fp = open(params.cf_filename, "w") if params.cf_filename else None
     try:
-        for it in range(params.niterations):
-            crln, ntraj, st = correlation_iteration(ms, params, Temperature, per_iter, precision)
-            total.data += crln
-            total.ntraj += ntraj
-            if log:
-                log(f"ITERATION {it + 1}/{params.niterations}: accumulated {int(total.ntraj)} trajectories."
-                    + (f" Saving the temporary result to '{params.cf_filename}'" if fp else ""))
-                m0 = total.data[0] / total.ntraj * ZeroCoeff / ALU ** 3
-                log(f"M0 ESTIMATE FROM CF: {m0:.5e}")
-            if fp:
-                write_correlation_function_ext(fp, total)
+        it = 0
+        while it < params.niterations:
+            # a group of iterations shares one launch; the CF file is still
+            # rewritten after every iteration, in order
+            g = min(group, params.niterations - it)
+            crlns, ntrajs, st = correlation_iterations(ms, params, Temperature, per_iter, g, precision)
+            for j in range(g):
+                total.data += crlns[j]
+                total.ntraj += ntrajs[j]
+                it += 1
+                if log:
+                    log(f"ITERATION {it}/{params.niterations}: accumulated {int(total.ntraj)} trajectories."
+                        + (f" Saving the temporary result to '{params.cf_filename}'" if fp else ""))
+                    m0 = total.data[0] / total.ntraj * ZeroCoeff / ALU ** 3
+                    log(f"M0 ESTIMATE FROM CF: {m0:.5e}")
+                if fp:
+                    write_correlation_function_ext(fp, total)
     finally:
         if fp:
             fp.close()

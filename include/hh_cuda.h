@@ -18,6 +18,7 @@
  *   hh_cuda_correlation      the accumulation loop of calculate_correlation_and_save
  *                            (src/hawaii.c:2970-3012) with correlation_eval
  *                            (src/hawaii.c:2116-2347) per trajectory
+ *   hh_cuda_correlation_multi  niterations passes of that loop (src/hawaii.c:2970-3040)
  *   hh_cuda_correlation_ic   correlation_eval over caller-supplied phase points
  *                            (src/hawaii.c:2116-2347, accumulation 3008)
  *   hh_cuda_m0               c_mpi_perform_integration(..., INTEGRAND_M0, ...)
@@ -102,6 +103,7 @@ typedef struct {
     double sample_ms;               /* device time of the sampler (CUDA events) */
     double traj_ms;                 /* device time of the trajectory kernel(s) */
     double total_ms;                /* device time of the whole call */
+    uint64_t n_kernel_launches;     /* kernels this library launched for the call */
 } hh_stats;
 
 /* Select the device and the surface; uploads coefficient tables.  Re-callable. */
@@ -122,7 +124,16 @@ int hh_cuda_sample(const hh_calc_params *p, double T, uint32_t seed, uint64_t n,
 int hh_cuda_correlation(const hh_calc_params *p, double T, uint32_t seed, uint64_t n_accept,
                         int precision_mode, double *crln_sum, double *ntraj, hh_stats *stats);
 
-/* Same, for caller-supplied initial phase points qp0[n][QP_SIZE]. */
+/* n_iterations consecutive iterations of n_per_iteration trajectories each
+ * (the stream order of the reference's iteration loop), integrated in one
+ * persistent launch so that the long-lived trajectories of one iteration run
+ * beside the others: crln_sums[i][k] (n_iterations x MaxTrajectoryLength) and
+ * ntraj[i] per iteration. */
+int hh_cuda_correlation_multi(const hh_calc_params *p, double T, uint32_t seed,
+                              uint64_t n_per_iteration, uint32_t n_iterations, int precision_mode,
+                              double *crln_sums, double *ntraj, hh_stats *stats);
+
+/* Same as hh_cuda_correlation, for caller-supplied initial phase points qp0[n][QP_SIZE]. */
 int hh_cuda_correlation_ic(const hh_calc_params *p, const double *qp0, uint64_t n,
                            int precision_mode, double *crln_sum, hh_stats *stats);
 
@@ -146,6 +157,15 @@ const char *hh_cuda_strerror(int code);
  * switches injection off. */
 int hh_cuda_mt_stream(uint32_t seed, uint64_t n, uint32_t *out);
 int hh_cuda_debug_inject(int traj, int dir, int k, int status);
+/* registers a host buffer of capacity_words uint32 that the next correlation
+ * call fills with (steps, samples, start ns, end ns) per half-trajectory item
+ * (item 2*traj + dir); NULL unregisters */
+int hh_cuda_debug_item_trace(uint32_t *out, uint64_t capacity_words);
+
+/* Diagnostic (no counterpart in the reference): measured FMA throughput of the
+ * CUDA cores in TFLOP/s (precision HH_PRECISION_FP64 or, for FP32,
+ * HH_PRECISION_MIXED), the denominator of the trajectory kernels' roofline. */
+int hh_cuda_fma_peak(int precision, double *tflops);
 
 /* Release all device memory of the library. */
 void hh_cuda_shutdown(void);

@@ -34,7 +34,7 @@ def test_struct_layouts_match_header():
     from hawaiihybrid_b200 import _lib
     assert C.sizeof(_lib.SystemDesc) == 4 + 4 + 8 + 4 + 4 + 48
     assert C.sizeof(_lib.CalcParamsC) == 8 + 8 * 4 + 8 + 8 * 4 + 8
-    assert C.sizeof(_lib.Stats) == 8 * 8 + 8 * 8 + 3 * 8
+    assert C.sizeof(_lib.Stats) == 8 * 8 + 8 * 8 + 3 * 8 + 8
 
 
 def test_errors_without_device():

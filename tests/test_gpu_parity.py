@@ -75,15 +75,21 @@ def test_single_trajectory_early_times(name, dt):
         assert np.max(np.abs(crln[:kmax] - ref[:kmax])) <= 1e-9 * abs(ref[0])
 
 
-@pytest.mark.parametrize("name,N,dt,n", [("hear", 4096, 200.0, 2048), ("co2ar", 4096, 100.0, 2048)])
-def test_mixed_matches_fp64(name, N, dt, n):
+@pytest.mark.parametrize("name,N,dt,n,window", [("hear", 4096, 200.0, 2048, 4096),
+                                                  ("co2ar", 4096, 100.0, 2048, 1001)])
+def test_mixed_matches_fp64(name, N, dt, n, window):
+    """The mixed path against the FP64 path on the same initial conditions: M0 (from C(0))
+    and C(t) within 1e-4 of C(0).  He-Ar is compared over the whole window; for CO2-Ar the
+    comparison covers t <= 1e5 a.u. (the collision window), because later samples are
+    dominated by long-lived chaotic complexes whose pointwise C(t) is not reproducible even
+    between two FP64 runs at rtol 1e-12 and 1e-13."""
     import hawaiihybrid_b200 as hh
     ms = lib_system(name)
     p = lib_params(name, N, dt)
     c64, _, s64 = hh.correlation_iteration(ms, p, 300.0, n, hh.PRECISION_FP64, seed=5)
     c32, _, s32 = hh.correlation_iteration(ms, p, 300.0, n, hh.PRECISION_MIXED, seed=5)
-    assert rel_to_c0(c32, c64) <= 1e-4
-    assert abs(c32[0] - c64[0]) / abs(c64[0]) <= 1e-4   # M0 from C(0)
+    assert rel_to_c0(c32[:window], c64[:window]) <= 1e-4
+    assert abs(c32[0] - c64[0]) / abs(c64[0]) <= 1e-6   # M0 from C(0)
 
 
 @pytest.mark.parametrize("name", ["hear", "co2ar"])
@@ -142,3 +148,16 @@ def test_failure_semantics(lib, status, hard):
         ref = ref + 0.5 * (fw + bw) * (5.29177210903e-11) ** 3
     assert st.n_failed == (1 if hard else 0)
     assert rel_to_c0(crln, ref) < 1e-7
+
+
+def test_multi_iteration_matches_consecutive_calls(lib):
+    """Iterations in one launch equal consecutive single-iteration calls on the same stream."""
+    import hawaiihybrid_b200 as hh
+    ms = lib_system("co2ar", 13)
+    p = lib_params("co2ar", 1024, 100.0)
+    c_multi, nt, st = hh.correlation_iterations(ms, p, 300.0, 300, 3, hh.PRECISION_FP64, seed=13)
+    singles = [hh.correlation_iteration(ms, p, 300.0, 300, hh.PRECISION_FP64, seed=(13 if i == 0 else 0))[0]
+               for i in range(3)]
+    for i in range(3):
+        assert rel_to_c0(c_multi[i], singles[i]) < 1e-12
+    assert list(nt) == [300.0, 300.0, 300.0]
