@@ -241,7 +241,7 @@ int sample_into(const hh_calc_params *p, double T, uint64_t n, double *d_out, ui
 template <int SYS, typename PHYS, typename STG, bool COMP>
 int launch_traj(const TrajParams &P, const TrajIO &io, int *grid_out) {
   auto kern = traj_kernel<SYS, PHYS, STG, COMP>;
-  size_t smem = (SYS == SYS_CO2AR) ? sizeof(Co2arTables<PHYS>) : 0;
+  size_t smem = traj_smem_bytes<SYS, PHYS, STG>();
   if (smem > 48 * 1024) CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, 128, smem));

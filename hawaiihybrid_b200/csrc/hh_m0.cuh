@@ -94,8 +94,9 @@ __global__ void __launch_bounds__(256) m0_kernel(M0Args a, const Co2arTablesGlob
     PHYS V, mu2, kappa;
     if (SYS == SYS_HEAR) {
       PHYS dV;
-      hear_V_dV<PHYS>(R, V, dV);
-      PHYS d = hear_dip<PHYS>(R);
+      PHYS iR = PHYS(1) / R;
+      hear_V_dV<PHYS>(R, iR, V, dV);
+      PHYS d = hear_dip<PHYS>(R, iR);
       mu2 = d * d;
       kappa = -log(u24<PHYS>(w[5])) - log(u24<PHYS>(w[7])) * zc * zc;
     } else {
@@ -108,9 +109,10 @@ __global__ void __launch_bounds__(256) m0_kernel(M0Args a, const Co2arTablesGlob
       PHYS st = sqrt((PHYS(1) - ct) * (PHYS(1) + ct));
       PHYS x = sT * st * cos(Phi - ph) + cT * ct;
       PHYS VR, Vx;
-      co2ar_pes<PHYS, COMP>(tb->pes, tb->fpes, tb->rbound, tb->rlo, R, x, V, VR, Vx, true);
+      PHYS iR = PHYS(1) / R;
+      co2ar_pes<PHYS, COMP>(tb->pes, tb->fpes, tb->rbound, tb->rlo, R, iR, x, V, VR, Vx, true);
       PHYS dz, ax;
-      co2ar_dip<PHYS, COMP>(tb->dipx, tb->dipz, tb->fdip, tb->rbound, tb->rlo, R, x, dz, ax);
+      co2ar_dip<PHYS, COMP>(tb->dipx, tb->dipz, tb->fdip, tb->rbound, tb->rlo, R, iR, x, dz, ax);
       mu2 = dz * dz + ax * ax * (PHYS(1) - x) * (PHYS(1) + x);
       kappa = -log(u24<PHYS>(w[5])) - log(u24<PHYS>(w[6])) - log(u24<PHYS>(w[7])) * zc * zc;
     }

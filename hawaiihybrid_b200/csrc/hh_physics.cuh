@@ -29,7 +29,7 @@ namespace hh {
 // f_2n(x) = 1 - exp(-x) sum_{k<=2n} x^k/k!.
 // ----------------------------------------------------------------------------
 template <typename T>
-__device__ __forceinline__ void hear_V_dV(T R, T &V, T &dV) {
+__device__ __forceinline__ void hear_V_dV(T R, T iR, T &V, T &dV) {
   const T A = T(0.2303058634e2), G1 = T(0.163051044e1), G2 = T(0.4680016e-1);
   const T B = T(0.16274792500000e1);
   const T C[6] = {T(0.940835513e1), T(0.165523018e3), T(0.379715796e4),
@@ -46,7 +46,6 @@ __device__ __forceinline__ void hear_V_dV(T R, T &V, T &dV) {
     term *= x * T(1.0 / double(m));
     S += term;
   }
-  T iR = T(1) / R;
   T iR2 = iR * iR;
   T iRp = iR2 * iR2;  // R^-4, multiplied up to R^-2n
 #pragma unroll
@@ -64,8 +63,7 @@ __device__ __forceinline__ void hear_V_dV(T R, T &V, T &dV) {
 }
 
 template <typename T>
-__device__ __forceinline__ T hear_dip(T R) {
-  T iR = T(1) / R;
+__device__ __forceinline__ T hear_dip(T R, T iR) {
   T iR2 = iR * iR;
   T iR7 = iR2 * iR2 * iR2 * iR;
   return exp(T(0.47293181) - T(0.40100613) * R - T(0.10292726) * R * R) - T(148.55391) * iR7;
@@ -130,6 +128,10 @@ __device__ __forceinline__ T radial_value(const T *row, T R, T t, T iR, int flag
   return c;
 }
 
+// 1/sqrt: hardware estimate refined to ~1 ulp in FP32, CUDA's rsqrt in FP64
+__device__ __forceinline__ float inv_sqrt(float x) { return rsqrtf(x); }
+__device__ __forceinline__ double inv_sqrt(double x) { return rsqrt(x); }
+
 // compensated (Kahan-Babuska) accumulation, used by the FP32 surfaces
 template <typename T> struct Acc {
   T s, c;
@@ -164,12 +166,12 @@ __device__ __forceinline__ void legendre10(T x, T P[11], T dP[11]) {
 // V (Hartree) and its partial derivatives V_R, V_x at (R, x)
 template <typename T, bool COMP>
 __device__ __forceinline__ void co2ar_pes(const T *tab, const int *flags, const T *rbound,
-                                          const T *rlo, T R, T x, T &V, T &VR, T &Vx, bool want_V) {
+                                          const T *rlo, T R, T iR, T x, T &V, T &VR, T &Vx,
+                                          bool want_V) {
   int i = co2ar_interval<T>(R, rbound);
   T P[11], dP[11];
   legendre10(x, P, dP);
   T t = R - rlo[i];
-  T iR = T(1) / R;
   int fl = flags[i];
   Acc<T> aV, aR, ax;
   const T *base = tab + i * CO2AR_NL * CO2AR_ROW;
@@ -190,13 +192,12 @@ __device__ __forceinline__ void co2ar_pes(const T *tab, const int *flags, const 
 // body-frame dipole sums: dz = sum b_l P_l(x), ax = sum a_l P_l'(x)
 template <typename T, bool COMP>
 __device__ __forceinline__ void co2ar_dip(const T *tabx, const T *tabz, const int *flags,
-                                          const T *rbound, const T *rlo, T R, T x, T &dz,
+                                          const T *rbound, const T *rlo, T R, T iR, T x, T &dz,
                                           T &ax) {
   int i = co2ar_interval<T>(R, rbound);
   T P[11], dP[11];
   legendre10(x, P, dP);
   T t = R - rlo[i];
-  T iR = T(1) / R;
   int fl = flags[i];
   Acc<T> az, aa;
   const T *bx = tabx + i * CO2AR_NL * CO2AR_ROW;

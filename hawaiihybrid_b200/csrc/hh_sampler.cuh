@@ -142,7 +142,7 @@ __device__ __forceinline__ double potential(const SamplerArgs &a, const Co2arTab
                                             const double *qp) {
   if (a.sys == SYS_HEAR) {
     double V, dV;
-    hear_V_dV<double>(qp[4], V, dV);
+    hear_V_dV<double>(qp[4], 1.0 / qp[4], V, dV);
     return V;
   }
   double y[12];
@@ -150,7 +150,7 @@ __device__ __forceinline__ double potential(const SamplerArgs &a, const Co2arTab
   double R = sqrt(y[0] * y[0] + y[1] * y[1] + y[2] * y[2]);
   double x = (y[0] * y[6] + y[1] * y[7] + y[2] * y[8]) / R;
   double V, VR, Vx;
-  co2ar_pes<double, false>(tb->pes, tb->fpes, tb->rbound, tb->rlo, R, x, V, VR, Vx, true);
+  co2ar_pes<double, false>(tb->pes, tb->fpes, tb->rbound, tb->rlo, R, 1.0 / R, x, V, VR, Vx, true);
   return V;
 }
 

@@ -119,21 +119,24 @@ template <typename PHYS, typename STG, bool COMP> struct HeArSys {
   __device__ void rhs(const double *y, STG *f) const {
     PHYS r0 = PHYS(y[0]), r1 = PHYS(y[1]), r2 = PHYS(y[2]);
     PHYS R2 = r0 * r0 + r1 * r1 + r2 * r2;
-    PHYS R = sqrt(R2);
+    PHYS iR = inv_sqrt(R2);
+    PHYS R = R2 * iR;
     PHYS V, dV;
-    hear_V_dV<PHYS>(R, V, dV);
-    PHYS g = dV / R;
-    f[0] = STG(y[3] * inv_mu);
-    f[1] = STG(y[4] * inv_mu);
-    f[2] = STG(y[5] * inv_mu);
+    hear_V_dV<PHYS>(R, iR, V, dV);
+    PHYS g = dV * iR;
+    // dr/dt = p/mu in the stage precision
+    f[0] = STG(STG(y[3]) * STG(inv_mu));
+    f[1] = STG(STG(y[4]) * STG(inv_mu));
+    f[2] = STG(STG(y[5]) * STG(inv_mu));
     f[3] = STG(-g * r0);
     f[4] = STG(-g * r1);
     f[5] = STG(-g * r2);
   }
   __device__ void dipole(const double *y, PHYS d[3]) const {
     PHYS r0 = PHYS(y[0]), r1 = PHYS(y[1]), r2 = PHYS(y[2]);
-    PHYS R = sqrt(r0 * r0 + r1 * r1 + r2 * r2);
-    PHYS s = hear_dip<PHYS>(R) / R;
+    PHYS R2 = r0 * r0 + r1 * r1 + r2 * r2;
+    PHYS iR = inv_sqrt(R2);
+    PHYS s = hear_dip<PHYS>(R2 * iR, iR) * iR;
     d[0] = s * r0;
     d[1] = s * r1;
     d[2] = s * r2;
@@ -151,26 +154,31 @@ template <typename PHYS, typename STG, bool COMP> struct Co2ArSys {
   __device__ void rhs(const double *y, STG *f) const {
     PHYS r[3] = {PHYS(y[0]), PHYS(y[1]), PHYS(y[2])};
     PHYS u[3] = {PHYS(y[6]), PHYS(y[7]), PHYS(y[8])};
-    PHYS R = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
-    PHYS iR = PHYS(1) / R;
-    PHYS iu = PHYS(1) / sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    PHYS R2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+    PHYS iR = inv_sqrt(R2);
+    PHYS R = R2 * iR;
+    PHYS iu = inv_sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
     PHYS rh[3] = {r[0] * iR, r[1] * iR, r[2] * iR};
     PHYS uh[3] = {u[0] * iu, u[1] * iu, u[2] * iu};
     PHYS x = rh[0] * uh[0] + rh[1] * uh[1] + rh[2] * uh[2];
     PHYS V, VR, Vx;
-    co2ar_pes<PHYS, COMP>(tb->pes, tb->fpes, tb->rbound, tb->rlo, R, x, V, VR, Vx, false);
+    co2ar_pes<PHYS, COMP>(tb->pes, tb->fpes, tb->rbound, tb->rlo, R, iR, x, V, VR, Vx, false);
     PHYS a = VR - Vx * x * iR;  // dV/dr = a r^ + (Vx/R) u^
     PHYS b = Vx * iR;
-    f[0] = STG(y[3] * inv_mu);
-    f[1] = STG(y[4] * inv_mu);
-    f[2] = STG(y[5] * inv_mu);
+    // kinematics in the stage precision: dr/dt = p/mu, du/dt = (j x u)/I
+    const STG p0 = STG(y[3]), p1 = STG(y[4]), p2 = STG(y[5]);
+    const STG u0 = STG(y[6]), u1 = STG(y[7]), u2 = STG(y[8]);
+    const STG j0 = STG(y[9]), j1 = STG(y[10]), j2 = STG(y[11]);
+    const STG im = STG(inv_mu), iI = STG(inv_II);
+    f[0] = p0 * im;
+    f[1] = p1 * im;
+    f[2] = p2 * im;
     f[3] = STG(-(a * rh[0] + b * uh[0]));
     f[4] = STG(-(a * rh[1] + b * uh[1]));
     f[5] = STG(-(a * rh[2] + b * uh[2]));
-    // du/dt = (j x u)/I, evaluated in FP64 (kinematic part)
-    f[6] = STG((y[10] * y[8] - y[11] * y[7]) * inv_II);
-    f[7] = STG((y[11] * y[6] - y[9] * y[8]) * inv_II);
-    f[8] = STG((y[9] * y[7] - y[10] * y[6]) * inv_II);
+    f[6] = (j1 * u2 - j2 * u1) * iI;
+    f[7] = (j2 * u0 - j0 * u2) * iI;
+    f[8] = (j0 * u1 - j1 * u0) * iI;
     // dj/dt = -Vx (u^ x r^)
     f[9] = STG(-Vx * (uh[1] * rh[2] - uh[2] * rh[1]));
     f[10] = STG(-Vx * (uh[2] * rh[0] - uh[0] * rh[2]));
@@ -180,14 +188,14 @@ template <typename PHYS, typename STG, bool COMP> struct Co2ArSys {
   __device__ void dipole(const double *q, PHYS d[3]) const {
     PHYS r[3] = {PHYS(q[0]), PHYS(q[1]), PHYS(q[2])};
     PHYS u[3] = {PHYS(q[3]), PHYS(q[4]), PHYS(q[5])};
-    PHYS R = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
-    PHYS iR = PHYS(1) / R;
-    PHYS iu = PHYS(1) / sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    PHYS R2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+    PHYS iR = inv_sqrt(R2);
+    PHYS iu = inv_sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
     PHYS rh[3] = {r[0] * iR, r[1] * iR, r[2] * iR};
     PHYS uh[3] = {u[0] * iu, u[1] * iu, u[2] * iu};
     PHYS x = rh[0] * uh[0] + rh[1] * uh[1] + rh[2] * uh[2];
     PHYS dz, ax;
-    co2ar_dip<PHYS, COMP>(tb->dipx, tb->dipz, tb->fdip, tb->rbound, tb->rlo, R, x, dz, ax);
+    co2ar_dip<PHYS, COMP>(tb->dipx, tb->dipz, tb->fdip, tb->rbound, tb->rlo, R2 * iR, iR, x, dz, ax);
 #pragma unroll
     for (int c = 0; c < 3; ++c) d[c] = dz * rh[c] - ax * (uh[c] - x * rh[c]);
   }
@@ -262,10 +270,11 @@ __device__ __forceinline__ double step_attempt(const Sys &sys, const TrajParams 
 #undef HH_STAGE
   stage_point<N, STG, 12>(K, y, h, y_new);
   sys.rhs(y_new, K[12]);
-  double e5 = 0.0, e3 = 0.0;
+  // error norm in the stage precision (FP32 stages have no FP64 error to resolve)
+  STG e5 = STG(0), e3 = STG(0);
 #pragma unroll
   for (int i = 0; i < N; ++i) {
-    double sc = P.atol + fmax(fabs(y[i]), fabs(y_new[i])) * P.rtol;
+    STG sc = STG(P.atol) + STG(fmax(fabs(y[i]), fabs(y_new[i]))) * STG(P.rtol);
     STG a5 = STG(0), a3 = STG(0), m5 = STG(0);
 #pragma unroll
     for (int j = 0; j < 13; ++j) {
@@ -277,12 +286,19 @@ __device__ __forceinline__ double step_attempt(const Sys &sys, const TrajParams 
     }
     // FP32 stages: the estimate cannot resolve errors below the rounding noise of
     // the stage derivatives, so that noise widens the tolerance
-    if (sizeof(STG) == 4) sc += fabs(h) * P.noise_floor * double(m5);
-    double q5 = double(a5) / sc, q3 = double(a3) / sc;
+    if (sizeof(STG) == 4) sc += STG(fabs(h)) * STG(P.noise_floor) * m5;
+    const STG isc = STG(1) / sc;
+    const STG q5 = a5 * isc, q3 = a3 * isc;
     e5 += q5 * q5;
     e3 += q3 * q3;
   }
-  return (e5 == 0.0 && e3 == 0.0) ? 0.0 : fabs(h) * e5 / sqrt((e5 + 0.01 * e3) * N);
+  if (e5 == STG(0) && e3 == STG(0)) return 0.0;
+  return fabs(h) * double(e5) / sqrt(double(e5 + STG(0.01) * e3) * N);
+}
+
+// err^(-1/8) for the step controller
+__device__ __forceinline__ double inv_eighth_root(double err) {
+  return 1.0 / sqrt(sqrt(sqrt(err)));
 }
 
 // the three extra stages of the dense output and its coefficients F[7][NQ] for
@@ -387,6 +403,25 @@ __device__ __noinline__ void item_setup(const Sys &sys, const TrajParams &P, con
   *h_out = fmin(fmin(100.0 * h0, h1), span);
 }
 
+// per-warp pool of dense-output contexts for the pooled sample evaluation
+constexpr int SAMPLE_CHUNK = 64;
+template <typename STG, typename PHYS, int NQ> struct WarpSamples {
+  STG F[7][NQ][32];
+  double qold[NQ][32];
+  double t0[32];
+  double inv_h[32];
+  double *crln[32];
+  PHYS mu0[3][32];
+  PHYS prev[32];   // the owner's last stored sample before this round
+  PHYS tail[32];   // the owner's last sample of the previous chunk
+  PHYS last[32];   // the owner's last stored sample
+  PHYS res[SAMPLE_CHUNK];
+  int kst[32];
+  int off[32];
+  int item[32];
+  unsigned cut[32];  // (end << 3) | reason; end = index past the last stored sample
+};
+
 __device__ __forceinline__ void warp_add_counter(unsigned long long *dst, unsigned v) {
   unsigned long long s = v;
 #pragma unroll
@@ -398,10 +433,12 @@ __device__ __forceinline__ void warp_add_counter(unsigned long long *dst, unsign
 // warp-synchronous persistent loop over half-trajectory items
 // ---------------------------------------------------------------------------
 template <class Sys, typename PHYS, typename STG>
-__device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, const TrajIO &io) {
+__device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, const TrajIO &io,
+                                          WarpSamples<STG, PHYS, Sys::NQ> *ws_block) {
   constexpr int N = Sys::N;
   constexpr unsigned FULL = 0xffffffffu;
   const int lane = threadIdx.x & 31;
+  WarpSamples<STG, PHYS, Sys::NQ> *ws = ws_block + (threadIdx.x >> 5);
   const double dt = P.dt;
   unsigned nsteps = 0, nrej = 0, nrhs = 0, nsamp = 0, ndense = 0, nitems = 0;
   // per-lane item state
@@ -477,7 +514,7 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
         const double err = step_attempt<Sys, STG>(sys, P, K, y, h, y_new);
         nrhs += 12;
         if (err < 1.0) {
-          double fac = (err == 0.0) ? 10.0 : fmin(10.0, 0.9 * pow(err, -0.125));
+          double fac = (err == 0.0) ? 10.0 : fmin(10.0, 0.9 * inv_eighth_root(err));
           if (rejected) fac = fmin(1.0, fac);
           rejected = false;
           h_taken = h;
@@ -485,7 +522,7 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
           accepted = true;
           ++nsteps;
         } else {
-          h *= fmax(0.2, 0.9 * pow(err, -0.125));
+          h *= fmax(0.2, 0.9 * inv_eighth_root(err));
           rejected = true;
           ++nrej;
         }
@@ -493,48 +530,160 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
     }
 
     // ---- dense output and samples for steps that passed a sample time ----
+    // The steps of the 32 lanes pass very different numbers of sample times
+    // (none inside a collision, dozens in free flight), so the samples are
+    // pooled: each lane publishes its dense-output context to shared memory,
+    // and all lanes evaluate the pooled (owner, k) jobs in chunks.  A sample
+    // the reference would not have stored (after an R > Rcut exit or a
+    // failure) is cut off per owner with an atomicMin on (end, reason).
     bool pending = accepted && (double(k) * dt <= t + h_taken);
     if (__any_sync(FULL, pending)) {
-      STG F[7][Sys::NQ];
+      int cnt = 0;
       if (pending) {
+        STG F[7][Sys::NQ];
         dense_stages<Sys, STG>(sys, K, y, y_new, h_taken, F);
         nrhs += 3;
         ++ndense;
+        const double t_new = t + h_taken;
+        int kl = (int)fmin(floor(t_new / dt), double(P.N - 1));
+        while (kl + 1 <= P.N - 1 && double(kl + 1) * dt <= t_new) ++kl;
+        while (kl > k && double(kl) * dt > t_new) --kl;
+        cnt = kl - k + 1;
+#pragma unroll
+        for (int r = 0; r < 7; ++r)
+#pragma unroll
+          for (int c = 0; c < Sys::NQ; ++c) ws->F[r][c][lane] = F[r][c];
+#pragma unroll
+        for (int c = 0; c < Sys::NQ; ++c) ws->qold[c][lane] = y[Sys::qidx(c)];
+#pragma unroll
+        for (int c = 0; c < 3; ++c) ws->mu0[c][lane] = mu0[c];
+        ws->t0[lane] = t;
+        ws->inv_h[lane] = 1.0 / h_taken;
+        ws->prev[lane] = curr;
+        ws->crln[lane] = crln;
+        ws->kst[lane] = k;
+        ws->item[lane] = item;
+        ws->cut[lane] = 0xffffffffu;
       }
-      const double t_new = t + h_taken;
-      while (__any_sync(FULL, pending)) {
-        if (pending) {
-          const double x = (double(k) * dt - t) / h_taken;
-          double q[Sys::NQ];
-          dense_eval<Sys, STG>(y, F, x, q);
-          PHYS d[3];
-          sys.dipole(q, d);
-          ++nsamp;
-          if (isnan(d[0]) || isnan(d[1]) || isnan(d[2])) {
-            status = HH_ST_NAN_DIPOLE;
-            hard = 1;
-          } else if (item == P.inject_item && k == P.inject_k) {
-            status = P.inject_status;
-            hard = (P.inject_status >= HH_ST_NAN_DIPOLE);
-          } else {
-            prev = curr;
-            curr = mu0[0] * d[0] + mu0[1] * d[1] + mu0[2] * d[2];
-            if (fabs(double(curr)) > 1e100) {
-              status = HH_ST_OVERFLOW;
-              hard = 1;
-            } else if (k > 1 && fabs(double(curr) / double(prev)) > 1e10) {
-              status = HH_ST_JUMP;
-              hard = 1;
-            } else {
-              atomicAdd(&crln[k], P.weight * double(curr));
-              ++k;
-              since = 0;
-              if (sqrt(q[0] * q[0] + q[1] * q[1] + q[2] * q[2]) > P.Rcut) status = HH_ST_OK;
+      int incl = cnt;
+#pragma unroll
+      for (int o = 1; o < 32; o <<= 1) {
+        const int v = __shfl_up_sync(FULL, incl, o);
+        if (lane >= o) incl += v;
+      }
+      const int my_off = incl - cnt;
+      const int pooled = __shfl_sync(FULL, incl, 31);
+      ws->off[lane] = my_off;
+      __syncwarp();
+      for (int base = 0; base < pooled; base += SAMPLE_CHUNK) {
+        const int m = min(SAMPLE_CHUNK, pooled - base);
+        // (1) evaluate: each lane takes jobs jj = lane, lane + 32
+        int own[SAMPLE_CHUNK / 32];
+        int kks[SAMPLE_CHUNK / 32];
+        bool nan_[SAMPLE_CHUNK / 32], out_[SAMPLE_CHUNK / 32];
+#pragma unroll
+        for (int u = 0; u < SAMPLE_CHUNK / 32; ++u) {
+          const int jj = lane + 32 * u;
+          own[u] = -1;
+          if (jj < m) {
+            const int j = base + jj;
+            int o = 0;  // owner: the largest lane whose offset is <= j
+#pragma unroll
+            for (int step = 16; step > 0; step >>= 1)
+              if (o + step <= 31 && ws->off[o + step] <= j) o += step;
+            const int kk = ws->kst[o] + (j - ws->off[o]);
+            const double x = (double(kk) * dt - ws->t0[o]) * ws->inv_h[o];
+            const STG xs = STG(x), x1 = STG(1) - STG(x);
+            double q[Sys::NQ];
+#pragma unroll
+            for (int c = 0; c < Sys::NQ; ++c) {
+              STG v = ws->F[6][c][o] * xs;
+              v = (v + ws->F[5][c][o]) * x1;
+              v = (v + ws->F[4][c][o]) * xs;
+              v = (v + ws->F[3][c][o]) * x1;
+              v = (v + ws->F[2][c][o]) * xs;
+              v = (v + ws->F[1][c][o]) * x1;
+              v = (v + ws->F[0][c][o]) * xs;
+              q[c] = ws->qold[c][o] + double(v);
             }
+            PHYS d[3];
+            sys.dipole(q, d);
+            ++nsamp;
+            own[u] = o;
+            kks[u] = kk;
+            nan_[u] = isnan(d[0]) || isnan(d[1]) || isnan(d[2]);
+            out_[u] = q[0] * q[0] + q[1] * q[1] + q[2] * q[2] > P.Rcut * P.Rcut;
+            ws->res[jj] = ws->mu0[0][o] * d[0] + ws->mu0[1][o] * d[1] + ws->mu0[2][o] * d[2];
           }
-          pending = (status < 0) && (k < P.N) && (double(k) * dt <= t_new);
+        }
+        __syncwarp();
+        // (2) the reference's per-sample tests (src/hawaii.c:2183-2243), in its order
+#pragma unroll
+        for (int u = 0; u < SAMPLE_CHUNK / 32; ++u) {
+          const int o = own[u];
+          if (o >= 0) {
+            const int jj = lane + 32 * u;
+            const int j = base + jj;
+            const PHYS val = ws->res[jj];
+            unsigned code = 0xffffffffu;
+            if (nan_[u]) code = (unsigned(j) << 3) | 1u;
+            else if (ws->item[o] == P.inject_item && kks[u] == P.inject_k) code = (unsigned(j) << 3) | 4u;
+            else if (fabs(double(val)) > 1e100) code = (unsigned(j) << 3) | 2u;
+            else {
+              const PHYS pv = (j == ws->off[o]) ? ws->prev[o] : (jj == 0 ? ws->tail[o] : ws->res[jj - 1]);
+              if (kks[u] > 1 && fabs(double(val) / double(pv)) > 1e10) code = (unsigned(j) << 3) | 3u;
+              else if (out_[u]) code = (unsigned(j + 1) << 3);  // stored, then the branch ends
+            }
+            if (code != 0xffffffffu) atomicMin(&ws->cut[o], code);
+          }
+        }
+        __syncwarp();
+        // (3) commit the samples before each owner's cut
+#pragma unroll
+        for (int u = 0; u < SAMPLE_CHUNK / 32; ++u) {
+          const int o = own[u];
+          if (o >= 0) {
+            const int jj = lane + 32 * u;
+            const int j = base + jj;
+            const PHYS val = ws->res[jj];
+            const unsigned cut = ws->cut[o];
+            const int end_o = (o == 31) ? pooled : ws->off[o + 1];
+            const int stop = (cut == 0xffffffffu) ? end_o : min(end_o, int(cut >> 3));
+            const int chunk_end = min(end_o, base + m);
+            if (j < stop) {
+              atomicAdd(&ws->crln[o][kks[u]], P.weight * double(val));
+              // the owner's last stored sample so far (a cut found in a later
+              // chunk lies past every sample of this one)
+              if (j == min(stop, chunk_end) - 1) ws->last[o] = val;
+            }
+            if (j == chunk_end - 1) ws->tail[o] = val;
+          }
+        }
+        __syncwarp();
+      }
+      if (pending) {
+        const unsigned cut = ws->cut[lane];
+        const int stop = (cut == 0xffffffffu) ? my_off + cnt : min(my_off + cnt, int(cut >> 3));
+        const int committed = stop - my_off;
+        if (committed > 0) {
+          k += committed;
+          curr = ws->last[lane];
+          since = 0;
+        }
+        if (cut != 0xffffffffu) {
+          switch (cut & 7u) {
+            case 0: status = HH_ST_OK; break;  // R > Rcut
+            case 1: status = HH_ST_NAN_DIPOLE; hard = 1; break;
+            case 2: status = HH_ST_OVERFLOW; hard = 1; break;
+            case 3: status = HH_ST_JUMP; hard = 1; break;
+            default:
+              status = P.inject_status;
+              hard = (P.inject_status >= HH_ST_NAN_DIPOLE);
+              break;
+          }
         }
       }
+      __syncwarp();
     }
 
     // ---- advance accepted lanes; close finished items ----
@@ -580,23 +729,37 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
   warp_add_counter(&io.counters[5], nitems);
 }
 
+template <typename PHYS> __host__ __device__ constexpr size_t smem_tables_bytes() {
+  return (sizeof(Co2arTables<PHYS>) + 15) / 16 * 16;
+}
+
+// dynamic shared memory of traj_kernel: coefficient tables (CO2-Ar) + 4 warp pools
+template <int SYS, typename PHYS, typename STG> constexpr size_t traj_smem_bytes() {
+  return (SYS == SYS_CO2AR ? smem_tables_bytes<PHYS>() : 0) +
+         4 * sizeof(WarpSamples<STG, PHYS, (SYS == SYS_HEAR ? 3 : 6)>);
+}
+
 template <int SYS, typename PHYS, typename STG, bool COMP>
 __global__ void __launch_bounds__(128) traj_kernel(TrajParams P, TrajIO io,
                                                    const Co2arTablesGlobal *gtab) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
   if (SYS == SYS_HEAR) {
-    HeArSys<PHYS, STG, COMP> sys;
+    using Sys = HeArSys<PHYS, STG, COMP>;
+    Sys sys;
     sys.inv_mu = 1.0 / P.mu;
-    traj_body<HeArSys<PHYS, STG, COMP>, PHYS, STG>(sys, P, io);
+    auto *ws = reinterpret_cast<WarpSamples<STG, PHYS, Sys::NQ> *>(smem_raw);
+    traj_body<Sys, PHYS, STG>(sys, P, io, ws);
   } else {
-    extern __shared__ unsigned char smem_raw[];
+    using Sys = Co2ArSys<PHYS, STG, COMP>;
     Co2arTables<PHYS> *tb = reinterpret_cast<Co2arTables<PHYS> *>(smem_raw);
     load_tables<PHYS>(tb, gtab);
     __syncthreads();
-    Co2ArSys<PHYS, STG, COMP> sys;
+    Sys sys;
     sys.inv_mu = 1.0 / P.mu;
     sys.inv_II = 1.0 / P.II;
     sys.tb = tb;
-    traj_body<Co2ArSys<PHYS, STG, COMP>, PHYS, STG>(sys, P, io);
+    auto *ws = reinterpret_cast<WarpSamples<STG, PHYS, Sys::NQ> *>(smem_raw + smem_tables_bytes<PHYS>());
+    traj_body<Sys, PHYS, STG>(sys, P, io, ws);
   }
 }
 
