@@ -374,6 +374,37 @@ int run_trajectories(const hh_calc_params *p, const double *d_ic, uint64_t n, ui
   return HH_OK;
 }
 
+// ---------------------------------------------------------------------------
+// Scratch of hh_cuda_m0_noalloc: a fixed array compiled into the library, so
+// that M0 can run in a process that must not allocate device memory once its
+// run has started.  Layout: block partials [M0_NOALLOC_MAX_BLOCKS][M0_MAXT][2]
+// (sum of w, sum of w^2), then results [HH_M0_NOALLOC_MAX_T][2].  One copy per
+// device; calls whose GPU work overlaps share it and race.
+constexpr int M0_NOALLOC_MAX_BLOCKS = 1024;
+constexpr size_t M0_NOALLOC_PARTIALS = (size_t)M0_NOALLOC_MAX_BLOCKS * M0_MAXT * 2;
+constexpr size_t M0_NOALLOC_WORDS = M0_NOALLOC_PARTIALS + 2 * (size_t)HH_M0_NOALLOC_MAX_T;
+static_assert(HH_M0_NOALLOC_MAX_T % M0_MAXT == 0, "result slots come in whole temperature chunks");
+static_assert(M0_NOALLOC_WORDS * sizeof(double) == HH_M0_NOALLOC_SCRATCH_BYTES,
+              "header size of the allocation-free M0 scratch");
+static __device__ __align__(256) double g_m0_noalloc_scratch[M0_NOALLOC_WORDS];
+
+constexpr int NOALLOC_MAX_DEVICES = 64;
+double *g_m0_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};  // device address per device, set on first use
+
+// Device address of the scratch on the current device `dev`.  The first call
+// per device asks the runtime for it; with lazy module loading that is also
+// when the driver places the array in device memory.
+int m0_noalloc_scratch(int dev, double **out) {
+  if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return HH_E_INVALID_ARGUMENT;
+  if (!g_m0_noalloc_ptr[dev]) {
+    void *ptr = nullptr;
+    CK(cudaGetSymbolAddress(&ptr, g_m0_noalloc_scratch));
+    g_m0_noalloc_ptr[dev] = static_cast<double *>(ptr);
+  }
+  *out = g_m0_noalloc_ptr[dev];
+  return HH_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -389,6 +420,9 @@ const char *hh_cuda_strerror(int code) {
     case HH_E_NOT_POWER_OF_TWO: return "length of the input array should be a power of 2";
     case HH_E_SAMPLER: return g_errmsg[0] ? g_errmsg : "sampler error";
     case HH_E_NO_DEVICE: return "no CUDA device";
+    case HH_E_SCRATCH_LIMIT:
+      return "request exceeds the fixed scratch of an allocation-free entry point "
+             "(hh_cuda_m0_noalloc: nT > HH_M0_NOALLOC_MAX_T)";
     default: return "unknown error";
   }
 }
@@ -690,6 +724,73 @@ int hh_cuda_fma_peak(int precision, double *tflops) {
     best = std::max(best, flops / (ms * 1e-3) / 1e12);
   }
   *tflops = best;
+  return HH_OK;
+}
+
+// Allocation-free M0: the samples, kernels and result of hh_cuda_m0, with the
+// block partials and results kept in g_m0_noalloc_scratch instead of buffers
+// that grow on demand.  Every partial a launch reads was written by that
+// launch, so only the result slots are cleared; a failed launch then cannot
+// hand back an earlier call's numbers.
+int hh_cuda_m0_noalloc(const hh_calc_params *p, const double *T, int nT, uint64_t n_samples,
+                       uint64_t seed, int precision_mode, double *m, double *err) {
+  if (!g.init) return HH_E_NOT_INITIALIZED;
+  if (!p || !T || nT < 1 || !m || n_samples == 0) return HH_E_INVALID_ARGUMENT;
+  if (nT > HH_M0_NOALLOC_MAX_T) return HH_E_SCRATCH_LIMIT;
+  if (!(p->sampler_Rmin > 0) || !(p->sampler_Rmax > p->sampler_Rmin)) return HH_E_INVALID_ARGUMENT;
+  if (p->pair_state < 1 || p->pair_state > 3) return HH_E_INVALID_ARGUMENT;
+  if (precision_mode != HH_PRECISION_FP64 && precision_mode != HH_PRECISION_MIXED)
+    return HH_E_INVALID_ARGUMENT;
+  for (int t = 0; t < nT; ++t)
+    if (!(T[t] > 0)) return HH_E_INVALID_ARGUMENT;
+  CK(cudaSetDevice(g.device));
+  double *scratch = nullptr;
+  int rc = m0_noalloc_scratch(g.device, &scratch);
+  if (rc) return rc;
+  double *partials = scratch, *res = scratch + M0_NOALLOC_PARTIALS;
+  const int block = 256;
+  const int grid = std::min(g.num_sms * 4, M0_NOALLOC_MAX_BLOCKS);
+  const int n_chunks = (nT + M0_MAXT - 1) / M0_MAXT;
+  CK(cudaMemsetAsync(res, 0, sizeof(double) * 2 * M0_MAXT * n_chunks, g.st));
+  for (int c = 0; c < n_chunks; ++c) {
+    const int t0 = c * M0_MAXT;
+    M0Args a;
+    memset(&a, 0, sizeof a);
+    a.sys = g.sys;
+    a.Rmin = p->sampler_Rmin;
+    a.Rmax = p->sampler_Rmax;
+    a.pair_state = p->pair_state;
+    a.nT = std::min(M0_MAXT, nT - t0);
+    for (int t = 0; t < a.nT; ++t) a.invkT[t] = HH_HKT / T[t0 + t];
+    a.n_samples = n_samples;
+    a.offset = 0;
+    a.seed = seed;
+    const bool mixed = precision_mode == HH_PRECISION_MIXED;
+    if (g.sys == SYS_HEAR) {
+      if (mixed) m0_kernel<SYS_HEAR, float, true><<<grid, block, 0, g.st>>>(a, g.d_tab, partials);
+      else m0_kernel<SYS_HEAR, double, false><<<grid, block, 0, g.st>>>(a, g.d_tab, partials);
+    } else {
+      if (mixed)
+        m0_kernel<SYS_CO2AR, float, true><<<grid, block, sizeof(Co2arTables<float>), g.st>>>(
+            a, g.d_tab, partials);
+      else
+        m0_kernel<SYS_CO2AR, double, false><<<grid, block, sizeof(Co2arTables<double>), g.st>>>(
+            a, g.d_tab, partials);
+    }
+    CK(cudaGetLastError());
+    m0_finalize_kernel<<<1, 32, 0, g.st>>>(partials, grid, res + 2 * (size_t)t0);
+    CK(cudaGetLastError());
+  }
+  double out[2 * HH_M0_NOALLOC_MAX_T];
+  CK(cudaMemcpyAsync(out, res, sizeof(double) * 2 * nT, cudaMemcpyDeviceToHost, g.st));
+  CK(cudaStreamSynchronize(g.st));
+  const double scale = HH_ZEROCOEFF * 4.0 * HH_PI * (p->sampler_Rmax - p->sampler_Rmin);
+  for (int t = 0; t < nT; ++t) {
+    double mean = out[2 * t] / double(n_samples);
+    double var = out[2 * t + 1] / double(n_samples) - mean * mean;
+    m[t] = scale * mean;
+    if (err) err[t] = scale * sqrt(std::max(var, 0.0) / double(n_samples));
+  }
   return HH_OK;
 }
 

@@ -143,6 +143,30 @@ int hh_cuda_correlation_ic(const hh_calc_params *p, const double *qp0, uint64_t 
 int hh_cuda_m0(const hh_calc_params *p, const double *T, int nT, uint64_t n_samples,
                uint64_t seed, int precision_mode, double *m, double *err);
 
+/* Allocation-free M0 (no counterpart in the reference).
+ *
+ * Same arguments, samples and results as hh_cuda_m0, but the call allocates no
+ * device memory: its block partials and results live in one fixed array
+ * compiled into the library (HH_M0_NOALLOC_SCRATCH_BYTES per device).  It is
+ * meant for hosts that must not allocate once their run has started: a job that
+ * shares the GPU with an allocator holding most of HBM in its pool (a PyTorch
+ * caching allocator, a process under an MPS memory limit), where a cudaMalloc
+ * in the middle of a temperature scan can fail, and a host that overlaps this
+ * call with work on other streams, which the cudaFree of a growing buffer would
+ * stall until the whole device drains.
+ *
+ * Limits: nT <= HH_M0_NOALLOC_MAX_T, else HH_E_SCRATCH_LIMIT and nothing runs.
+ * hh_cuda_init must have been called (it allocates the surface tables once).
+ * The first call on a device looks up the array's device address; with lazy
+ * module loading that is when the driver places the array, so make that first
+ * call during set-up, before any stream capture.  There is one array per device:
+ * calls whose GPU work overlaps (e.g. from two host threads) race on it. */
+#define HH_E_SCRATCH_LIMIT (-9)
+#define HH_M0_NOALLOC_MAX_T 256
+#define HH_M0_NOALLOC_SCRATCH_BYTES (8 * (1024 * 16 * 2 + 2 * HH_M0_NOALLOC_MAX_T))
+int hh_cuda_m0_noalloc(const hh_calc_params *p, const double *T, int nT, uint64_t n_samples,
+                       uint64_t seed, int precision_mode, double *m, double *err);
+
 /* CF -> SF: apodizes cf in place (as the reference does), N a power of two. */
 int hh_cuda_idct_cf_to_sf(double *cf, size_t N, double dt, double *nu, double *sf);
 
