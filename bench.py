@@ -269,12 +269,15 @@ def main():
     peak = achieved / frac if frac > 0 else None
     wp = flops.work("co2ar", st_p, mixed=False)
     frac_p = wp["fp64"] / (p64.value * 1e12) / (st_p["traj_ms"] / 1e3)
+    # DRAM bytes per trajectory from one ncu capture of a single-iteration launch,
+    # scaled to the timed launch's n * steps trajectories (initial conditions and
+    # C(t) slices both grow with the trajectories a launch processes)
     traffic = None
     if os.path.exists(PROFILE_TRAFFIC):
         try:
             tr = json.load(open(PROFILE_TRAFFIC))
-            traffic = tr.get("traj_kernel_mixed_bytes_per_launch")
-        except (ValueError, OSError):
+            traffic = tr["traj_kernel_mixed_bytes_per_trajectory"] * n * args.steps
+        except (ValueError, OSError, KeyError, TypeError):
             traffic = None
     roof = {"bound": "fp32+fp64 CUDA-core FMA (no tensor or HBM bound: ~1e-3 B/flop)",
             "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": frac, "traffic": traffic,

@@ -143,6 +143,20 @@ template <typename PHYS, typename STG, bool COMP> struct HeArSys {
   }
 };
 
+// V_R and V_x of the CO2-Ar surface, called out of line.  A DOP853 step with
+// its dense output evaluates the right-hand side 15 times; inlined, the surface
+// code is repeated at each of those sites and the loop no longer fits the
+// instruction cache.  One shared copy costs a call per evaluation instead.
+template <typename T> struct PesGrad {
+  T VR, Vx;
+};
+template <typename T, bool COMP>
+__device__ __noinline__ PesGrad<T> co2ar_pes_grad(const Co2arTables<T> *tb, T R, T iR, T x) {
+  T V, VR, Vx;
+  co2ar_pes<T, COMP>(tb->pes, tb->fpes, tb->rbound, tb->rlo, R, iR, x, V, VR, Vx, false);
+  return {VR, Vx};
+}
+
 template <typename PHYS, typename STG, bool COMP> struct Co2ArSys {
   static constexpr int N = 12;
   static constexpr int QP = 10;
@@ -161,8 +175,8 @@ template <typename PHYS, typename STG, bool COMP> struct Co2ArSys {
     PHYS rh[3] = {r[0] * iR, r[1] * iR, r[2] * iR};
     PHYS uh[3] = {u[0] * iu, u[1] * iu, u[2] * iu};
     PHYS x = rh[0] * uh[0] + rh[1] * uh[1] + rh[2] * uh[2];
-    PHYS V, VR, Vx;
-    co2ar_pes<PHYS, COMP>(tb->pes, tb->fpes, tb->rbound, tb->rlo, R, iR, x, V, VR, Vx, false);
+    const PesGrad<PHYS> g = co2ar_pes_grad<PHYS, COMP>(tb, R, iR, x);
+    const PHYS VR = g.VR, Vx = g.Vx;
     PHYS a = VR - Vx * x * iR;  // dV/dr = a r^ + (Vx/R) u^
     PHYS b = Vx * iR;
     // kinematics in the stage precision: dr/dt = p/mu, du/dt = (j x u)/I
