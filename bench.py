@@ -9,7 +9,7 @@ reduced into C(t).  The sampled initial conditions are generated on the
 device, so the inputs are resident in HBM when a step starts.
 
   value   trajectories/s of the batched mixed-precision path (FP32 surfaces
-          with compensated sums, FP32 stages, FP64 state and C(t)), whole job
+          and stages, FP64 state and C(t)), whole job
   plain   the same for the FP64 drop-in path, same initial conditions
   e2e     the mixed path timed around the public call (hh_cuda_correlation via
           the Python mirror) with its host buffers

@@ -47,7 +47,10 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
     objs = []
     for src, flags in UNITS:
         obj = os.path.join(LIBDIR, src.replace(".cu", ".o"))
-        cmd = [NVCC, *ARCH, *COMMON, *flags, *(extra or []), "-dc", "-o", obj, os.path.join(CSRC, src)]
+        # whole-program compilation per unit (no relocatable device code: the units
+        # share no device functions), so ptxas allocates the registers of the
+        # out-of-line device functions within their callers' limits
+        cmd = [NVCC, *ARCH, *COMMON, *flags, *(extra or []), "-c", "-o", obj, os.path.join(CSRC, src)]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.run(cmd, check=True)

@@ -132,7 +132,7 @@ __device__ __forceinline__ T radial_value(const T *row, T R, T t, T iR, int flag
 __device__ __forceinline__ float inv_sqrt(float x) { return rsqrtf(x); }
 __device__ __forceinline__ double inv_sqrt(double x) { return rsqrt(x); }
 
-// compensated (Kahan-Babuska) accumulation, used by the FP32 surfaces
+// compensated (Kahan-Babuska) accumulation, used by the FP32 M0 integrand
 template <typename T> struct Acc {
   T s, c;
   __device__ __forceinline__ Acc() : s(0), c(0) {}

@@ -15,9 +15,9 @@
 // lanes busy) instead of each lane wandering through its own item.
 //
 // Precision: PHYS is the type the surfaces are evaluated in (double for the
-// plain path, float for the mixed path, with compensated sums); STG is the type
-// of the stage derivatives and increments.  Integrator state, time, step size
-// and the C(t) accumulation are FP64 in both paths.
+// plain path, float for the mixed path); STG is the type of the stage points,
+// stage derivatives and dense-output increments.  Integrator state, time, step
+// size and the C(t) accumulation are FP64 in both paths.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -116,7 +116,8 @@ template <typename PHYS, typename STG, bool COMP> struct HeArSys {
   static constexpr int NQ = 3;
   static __device__ __forceinline__ constexpr int qidx(int i) { return i; }
   double inv_mu;
-  __device__ void rhs(const double *y, STG *f) const {
+  // y in FP64 (the state) or in the stage precision (stage points)
+  template <typename YT> __device__ void rhs(const YT *y, STG *f) const {
     PHYS r0 = PHYS(y[0]), r1 = PHYS(y[1]), r2 = PHYS(y[2]);
     PHYS R2 = r0 * r0 + r1 * r1 + r2 * r2;
     PHYS iR = inv_sqrt(R2);
@@ -157,6 +158,19 @@ __device__ __noinline__ PesGrad<T> co2ar_pes_grad(const Co2arTables<T> *tb, T R,
   return {VR, Vx};
 }
 
+// Body-frame dipole sums (d_z, a_x) of CO2-Ar, out of line for the same reason:
+// the sample loop evaluates two pooled samples per lane and the item set-up one
+// more, and each inlined copy repeats the whole dipole surface.
+template <typename T> struct DipSums {
+  T dz, ax;
+};
+template <typename T, bool COMP>
+__device__ __noinline__ DipSums<T> co2ar_dip_sums(const Co2arTables<T> *tb, T R, T iR, T x) {
+  T dz, ax;
+  co2ar_dip<T, COMP>(tb->dipx, tb->dipz, tb->fdip, tb->rbound, tb->rlo, R, iR, x, dz, ax);
+  return {dz, ax};
+}
+
 template <typename PHYS, typename STG, bool COMP> struct Co2ArSys {
   static constexpr int N = 12;
   static constexpr int QP = 10;
@@ -165,7 +179,8 @@ template <typename PHYS, typename STG, bool COMP> struct Co2ArSys {
   static __device__ __forceinline__ constexpr int qidx(int i) { return i < 3 ? i : i + 3; }
   double inv_mu, inv_II;
   const Co2arTables<PHYS> *tb;
-  __device__ void rhs(const double *y, STG *f) const {
+  // y in FP64 (the state) or in the stage precision (stage points)
+  template <typename YT> __device__ void rhs(const YT *y, STG *f) const {
     PHYS r[3] = {PHYS(y[0]), PHYS(y[1]), PHYS(y[2])};
     PHYS u[3] = {PHYS(y[6]), PHYS(y[7]), PHYS(y[8])};
     PHYS R2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
@@ -208,8 +223,8 @@ template <typename PHYS, typename STG, bool COMP> struct Co2ArSys {
     PHYS rh[3] = {r[0] * iR, r[1] * iR, r[2] * iR};
     PHYS uh[3] = {u[0] * iu, u[1] * iu, u[2] * iu};
     PHYS x = rh[0] * uh[0] + rh[1] * uh[1] + rh[2] * uh[2];
-    PHYS dz, ax;
-    co2ar_dip<PHYS, COMP>(tb->dipx, tb->dipz, tb->fdip, tb->rbound, tb->rlo, R2 * iR, iR, x, dz, ax);
+    const DipSums<PHYS> ds = co2ar_dip_sums<PHYS, COMP>(tb, R2 * iR, iR, x);
+    const PHYS dz = ds.dz, ax = ds.ax;
 #pragma unroll
     for (int c = 0; c < 3; ++c) d[c] = dz * rh[c] - ax * (uh[c] - x * rh[c]);
   }
@@ -252,17 +267,34 @@ __device__ __forceinline__ void qp_to_state(const double *qp, double *y) {
 // DOP853 (Hairer-Norsett-Wanner) with the standard step controller
 // (safety 0.9, factors in [0.2, 10], exponent -1/8) and dense output.
 // The stage derivatives K stay in registers (all indices compile-time).
+// Intermediate stage points are formed in the stage precision from a copy of
+// the state in that precision: the right-hand side reads them in that precision
+// anyway, and an FP32 stage point carries one rounding more than the FP32
+// conversion of an FP64 one.  The 8th-order solution is formed in FP64.
 // ---------------------------------------------------------------------------
 template <int N, typename STG, int S>
-__device__ __forceinline__ void stage_point(const STG (&K)[16][N], const double *y, double h,
-                                            double *ys) {
+__device__ __forceinline__ void stage_point(const STG (&K)[16][N], const STG *ys0, STG hs,
+                                            STG *ys) {
 #pragma unroll
   for (int i = 0; i < N; ++i) {
     STG acc = STG(0);
 #pragma unroll
     for (int j = 0; j < S; ++j)
       if (hh_dop853_a[S][j] != 0.0) acc += STG(hh_dop853_a[S][j]) * K[j][i];
-    ys[i] = y[i] + h * double(acc);
+    ys[i] = ys0[i] + hs * acc;
+  }
+}
+
+template <int N, typename STG>
+__device__ __forceinline__ void solution_point(const STG (&K)[16][N], const double *y, double h,
+                                               double *y_new) {
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    STG acc = STG(0);
+#pragma unroll
+    for (int j = 0; j < 12; ++j)
+      if (hh_dop853_a[12][j] != 0.0) acc += STG(hh_dop853_a[12][j]) * K[j][i];
+    y_new[i] = y[i] + h * double(acc);
   }
 }
 
@@ -273,16 +305,20 @@ __device__ __forceinline__ double step_attempt(const Sys &sys, const TrajParams 
                                                STG (&K)[16][Sys::N], const double *y, double h,
                                                double *y_new) {
   constexpr int N = Sys::N;
+  STG ys0[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) ys0[i] = STG(y[i]);
+  const STG hs = STG(h);
 #define HH_STAGE(S)                                 \
   {                                                 \
-    double ys[N];                                   \
-    stage_point<N, STG, S>(K, y, h, ys);            \
+    STG ys[N];                                      \
+    stage_point<N, STG, S>(K, ys0, hs, ys);         \
     sys.rhs(ys, K[S]);                              \
   }
   HH_STAGE(1) HH_STAGE(2) HH_STAGE(3) HH_STAGE(4) HH_STAGE(5) HH_STAGE(6)
   HH_STAGE(7) HH_STAGE(8) HH_STAGE(9) HH_STAGE(10) HH_STAGE(11)
 #undef HH_STAGE
-  stage_point<N, STG, 12>(K, y, h, y_new);
+  solution_point<N, STG>(K, y, h, y_new);
   sys.rhs(y_new, K[12]);
   // error norm in the stage precision (FP32 stages have no FP64 error to resolve)
   STG e5 = STG(0), e3 = STG(0);
@@ -321,10 +357,14 @@ template <class Sys, typename STG>
 __device__ __forceinline__ void dense_stages(const Sys &sys, STG (&K)[16][Sys::N], const double *y_old,
                                              const double *y_new, double h, STG (&F)[7][Sys::NQ]) {
   constexpr int N = Sys::N;
+  STG ys0[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) ys0[i] = STG(y_old[i]);
+  const STG hs = STG(h);
 #define HH_STAGE(S)                                 \
   {                                                 \
-    double ys[N];                                   \
-    stage_point<N, STG, S>(K, y_old, h, ys);        \
+    STG ys[N];                                      \
+    stage_point<N, STG, S>(K, ys0, hs, ys);         \
     sys.rhs(ys, K[S]);                              \
   }
   HH_STAGE(13) HH_STAGE(14) HH_STAGE(15)
@@ -747,15 +787,21 @@ template <typename PHYS> __host__ __device__ constexpr size_t smem_tables_bytes(
   return (sizeof(Co2arTables<PHYS>) + 15) / 16 * 16;
 }
 
-// dynamic shared memory of traj_kernel: coefficient tables (CO2-Ar) + 4 warp pools
+// block shape of traj_kernel: warps per block, and the blocks per SM that the
+// register allocation must allow
+constexpr int TRAJ_WARPS = 4;
+constexpr int TRAJ_THREADS = TRAJ_WARPS * 32;
+constexpr int TRAJ_MIN_BLOCKS = 1;
+
+// dynamic shared memory of traj_kernel: coefficient tables (CO2-Ar) + one pool per warp
 template <int SYS, typename PHYS, typename STG> constexpr size_t traj_smem_bytes() {
   return (SYS == SYS_CO2AR ? smem_tables_bytes<PHYS>() : 0) +
-         4 * sizeof(WarpSamples<STG, PHYS, (SYS == SYS_HEAR ? 3 : 6)>);
+         TRAJ_WARPS * sizeof(WarpSamples<STG, PHYS, (SYS == SYS_HEAR ? 3 : 6)>);
 }
 
 template <int SYS, typename PHYS, typename STG, bool COMP>
-__global__ void __launch_bounds__(128) traj_kernel(TrajParams P, TrajIO io,
-                                                   const Co2arTablesGlobal *gtab) {
+__global__ void __launch_bounds__(TRAJ_THREADS, TRAJ_MIN_BLOCKS)
+    traj_kernel(TrajParams P, TrajIO io, const Co2arTablesGlobal *gtab) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   if (SYS == SYS_HEAR) {
     using Sys = HeArSys<PHYS, STG, COMP>;

@@ -64,7 +64,7 @@ extern "C" {
 
 /* precision modes */
 #define HH_PRECISION_FP64 0  /* FP64 surfaces and stages: the plain drop-in path */
-#define HH_PRECISION_MIXED 1 /* FP32 surfaces (compensated sums) and stages, FP64 state */
+#define HH_PRECISION_MIXED 1 /* FP32 surfaces and stages, FP64 state */
 
 typedef struct {
     int system_id;          /* HH_SYSTEM_* */
