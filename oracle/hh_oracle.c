@@ -13,6 +13,7 @@
 #include <string.h>
 
 #include "../hawaiihybrid_b200/csrc/hh_co2ar_tables.h"
+#include "../hawaiihybrid_b200/csrc/hh_n2ar_tables.h"
 #include "../hawaiihybrid_b200/csrc/hh_dop853_tableau.h"
 
 /* ---- constants (src/constants.h:8-53, CODATA 2022) ---- */
@@ -335,10 +336,267 @@ static void co2ar_dipole_lab(const double *q, double out[3]) {
     mtv(Mphi, t, out);
 }
 
+/* ======================================================================== */
+/* N2-Ar PIP-NN surfaces.  PES: PES-IDS/ai_pes_n2_ar_pip_nn.cpp:8-146 with   */
+/* PES-IDS/mlp.hpp:178-256 (forward, backward) and the lab chain rule of     */
+/* examples/correlation_n2_ar.cpp:18-50.  Dipole: PES-IDS/ai_ids_n2_ar_pip_nn */
+/* .cpp:11-128 with PES-IDS/QModel.hpp:144-257.  PIP bases and weights are   */
+/* the tables of hh_n2ar_tables.h.                                           */
+/* ======================================================================== */
+#define L_N2 2.07856749                     /* src/constants.h:80 */
+#define N2AR_EN_INF 0.0384490895371528      /* ai_pes_n2_ar_pip_nn.cpp:130 */
+
+/* quintic switch 10r^3 - 15r^4 + 6r^5 on [xi, xf] (ai_pes_n2_ar_pip_nn.cpp:14-41) */
+static double n2ar_sw(double x, double xi, double xf) {
+    if (x < xi) return 0.0;
+    if (x < xf) {
+        double r = (x - xi) / (xf - xi), r3 = r * r * r, r4 = r3 * r, r5 = r4 * r;
+        return 10.0 * r3 - 15.0 * r4 + 6.0 * r5;
+    }
+    return 1.0;
+}
+static double n2ar_dsw(double x, double xi, double xf) {
+    if (x < xi || !(x < xf)) return 0.0;
+    double t = (x - xi) / (xf - xi), t2 = t * t, t3 = t2 * t, t4 = t3 * t;
+    return (30.0 * t2 - 60.0 * t3 + 30.0 * t4) / (xf - xi);
+}
+static double silu(double x) { return x / (1.0 + exp(-x)); }
+static double dsilu(double x) {
+    double e = exp(-x), d = 1.0 + e;
+    return 1.0 / d + x * e / d / d;
+}
+
+/* PIPs p[17] of y[3] and (jac != NULL) jac[k * 17 + i] = d p_i / d y_k, from
+ * the monomial table (c_basis_2_1_4_purify.cc; the Jacobian is differentiated
+ * here, c_jac_2_1_4_purify.cc is the reference's own) */
+void hho_n2ar_pes_pip(const double *y, double *p, double *jac) {
+    memset(p, 0, HH_N2AR_PES_NPIP * sizeof(double));
+    if (jac) memset(jac, 0, 3 * HH_N2AR_PES_NPIP * sizeof(double));
+    for (int m = 0; m < HH_N2AR_PES_NMONO; ++m) {
+        const signed char *v = hh_n2ar_pes_var[m];
+        int deg = 0;
+        while (deg < 4 && v[deg] >= 0) ++deg;
+        double prod = 1.0;
+        for (int j = 0; j < deg; ++j) prod *= y[v[j]];
+        p[hh_n2ar_pes_poly[m]] += prod;
+        if (!jac) continue;
+        for (int j = 0; j < deg; ++j) {  /* d(monomial)/dy[v[j]] */
+            double dp = 1.0;
+            for (int i = 0; i < deg; ++i)
+                if (i != j) dp *= y[v[i]];
+            jac[v[j] * HH_N2AR_PES_NPIP + hh_n2ar_pes_poly[m]] += dp;
+        }
+    }
+}
+
+/* PIPs p[308] of y[10] of the dipole model (the three bases in model order) */
+void hho_n2ar_dip_pip(const double *y, double *p) {
+    memset(p, 0, HH_N2AR_DIP_NPIP * sizeof(double));
+    for (int m = 0; m < HH_N2AR_DIP_NMONO; ++m) {
+        double prod = 1.0;
+        for (int j = 0; j < 3 && hh_n2ar_dip_var[m][j] >= 0; ++j) prod *= y[hh_n2ar_dip_var[m][j]];
+        p[hh_n2ar_dip_poly[m]] += prod;
+    }
+}
+
+/* PES energy (cm^-1, before the en_inf shift) from the distances
+ * d[0] = |N1-N2|, d[1] = |N1-Ar|, d[2] = |N2-Ar|; dEdd (optional) receives dE/dd */
+double hho_n2ar_energy_cm(const double d[3], double dEdd[3]) {
+    double y[3], dy[3];
+    y[0] = exp(-d[0] / 2.0);
+    dy[0] = -0.5 * y[0];
+    for (int k = 1; k < 3; ++k) {
+        double s = n2ar_sw(d[k], 6.0, 20.0), ds = n2ar_dsw(d[k], 6.0, 20.0);
+        double e = exp(-d[k] / 2.0), d6 = pow(d[k], 6), d7 = d6 * d[k];
+        y[k] = (1.0 - s) * e + s * 1e4 / d6;
+        dy[k] = -ds * e - (1.0 - s) * e / 2.0 + ds * 1e4 / d6 - s * 6e4 / d7;
+    }
+    double p[HH_N2AR_PES_NPIP], J[3][HH_N2AR_PES_NPIP];
+    hho_n2ar_pes_pip(y, p, &J[0][0]);
+    double ptr[HH_N2AR_PES_NPIP];
+    for (int i = 0; i < HH_N2AR_PES_NPIP; ++i) ptr[i] = (p[i] - hh_n2ar_pes_xmean[i]) / hh_n2ar_pes_xscale[i];
+    double out = hh_n2ar_pes_b1[0], g[HH_N2AR_PES_HIDDEN];
+    for (int j = 0; j < HH_N2AR_PES_HIDDEN; ++j) {
+        double h = hh_n2ar_pes_b0[j];
+        for (int i = 0; i < HH_N2AR_PES_NPIP; ++i) h += ptr[i] * hh_n2ar_pes_w0[i][j];
+        out += silu(h) * hh_n2ar_pes_w1[j];
+        g[j] = dsilu(h) * hh_n2ar_pes_w1[j];
+    }
+    const double ymean = hh_n2ar_pes_y[0], yscale = hh_n2ar_pes_y[1];
+    if (dEdd) {
+        double dEdp[HH_N2AR_PES_NPIP];
+        for (int i = 0; i < HH_N2AR_PES_NPIP; ++i) {
+            double a = 0.0;
+            for (int j = 0; j < HH_N2AR_PES_HIDDEN; ++j) a += hh_n2ar_pes_w0[i][j] * g[j];
+            dEdp[i] = a / hh_n2ar_pes_xscale[i];
+        }
+        for (int k = 0; k < 3; ++k) {
+            double a = 0.0;
+            for (int i = 0; i < HH_N2AR_PES_NPIP; ++i) a += J[k][i] * dEdp[i];
+            dEdd[k] = a * dy[k] * yscale;
+        }
+    }
+    return yscale * out + ymean;
+}
+
+/* lab_to_xyz (ai_pes_n2_ar_pip_nn.cpp:103-121): N1, N2, Ar */
+static void n2ar_lab_xyz(const double *q, double x[9]) {
+    double Phi = q[0], Theta = q[1], R = q[2], ph = q[3], th = q[4];
+    double h = L_N2 / 2.0;
+    double u[3] = {cos(ph) * sin(th), sin(ph) * sin(th), cos(th)};
+    for (int i = 0; i < 3; ++i) { x[i] = h * u[i]; x[3 + i] = -h * u[i]; }
+    x[6] = R * cos(Phi) * sin(Theta);
+    x[7] = R * sin(Phi) * sin(Theta);
+    x[8] = R * cos(Theta);
+}
+
+static double n2ar_xyz_energy(const double x[9], double dx[9]) {
+    static const int pi_[3] = {0, 0, 1}, pj_[3] = {1, 2, 2};
+    double d[3], e[3][3];
+    for (int k = 0; k < 3; ++k) {
+        double s = 0.0;
+        for (int c = 0; c < 3; ++c) {
+            e[k][c] = x[3 * pi_[k] + c] - x[3 * pj_[k] + c];
+            s += e[k][c] * e[k][c];
+        }
+        d[k] = sqrt(s);
+    }
+    double g[3];
+    double E = hho_n2ar_energy_cm(d, dx ? g : NULL);
+    if (dx) {
+        memset(dx, 0, 9 * sizeof(double));
+        for (int k = 0; k < 3; ++k)
+            for (int c = 0; c < 3; ++c) {
+                dx[3 * pi_[k] + c] += g[k] * e[k][c] / d[k];
+                dx[3 * pj_[k] + c] -= g[k] * e[k][c] / d[k];
+            }
+    }
+    return E;
+}
+
+double hho_n2ar_V_lab(const double *q) {
+    double x[9];
+    n2ar_lab_xyz(q, x);
+    return (n2ar_xyz_energy(x, NULL) - N2AR_EN_INF) / HTOCM;
+}
+
+/* dpes (examples/correlation_n2_ar.cpp:18-50) */
+static void n2ar_dpes_lab(const double *q, double *dV) {
+    double x[9], c[9];
+    n2ar_lab_xyz(q, x);
+    n2ar_xyz_energy(x, c);
+    double Phi = q[0], Theta = q[1], R = q[2];
+    double sP = sin(Phi), cP = cos(Phi), sT = sin(Theta), cT = cos(Theta);
+    dV[0] = R * (-sP * sT * c[6] + cP * sT * c[7]) / HTOCM;
+    dV[1] = R * (cP * cT * c[6] + sP * cT * c[7] - sT * c[8]) / HTOCM;
+    dV[2] = (cP * sT * c[6] + sP * sT * c[7] + cT * c[8]) / HTOCM;
+    double sp = sin(q[3]), cp = cos(q[3]), st = sin(q[4]), ct = cos(q[4]);
+    dV[3] = L_N2 / 2.0 * (-sp * st * c[0] + cp * st * c[1] + sp * st * c[3] - cp * st * c[4]) / HTOCM;
+    dV[4] = L_N2 / 2.0 * (cp * ct * c[0] + sp * ct * c[1] - st * c[2] - cp * ct * c[3] - sp * ct * c[4] +
+                          st * c[5]) / HTOCM;
+}
+
+/* one charge model: charges q[5] of N1, N2, N1', N2', Ar from the 10 site
+ * distances (pairs i < j in site order), y = exp(-d / a0); p == NULL gives the
+ * model's charges at infinite separation (all PIPs zero, QModel::forward_inf) */
+static void n2ar_charges(int model, const double *dist, double a0, double q[5]) {
+    const double *xm = model ? &hh_n2ar_dip_long_xmean[0] : &hh_n2ar_dip_short_xmean[0];
+    const double *xs = model ? &hh_n2ar_dip_long_xscale[0] : &hh_n2ar_dip_short_xscale[0];
+    double p[HH_N2AR_DIP_NPIP] = {0};
+    if (dist) {
+        double y[10];
+        for (int k = 0; k < 10; ++k) y[k] = exp(-dist[k] / a0);
+        hho_n2ar_dip_pip(y, p);
+    }
+    double ptr[HH_N2AR_DIP_NPIP];
+    for (int i = 0; i < HH_N2AR_DIP_NPIP; ++i) ptr[i] = (p[i] - xm[i]) / xs[i];
+    /* sub-networks: PIPs [0,119) -> q0,q1; [119,238) -> q2,q3; [238,308) -> q4 */
+    const double *w0[3], *b0[3], *w1[3], *b1[3];
+    if (model) {
+        w0[0] = &hh_n2ar_dip_long_w0_0[0][0]; b0[0] = hh_n2ar_dip_long_b0_0; w1[0] = &hh_n2ar_dip_long_w1_0[0][0]; b1[0] = hh_n2ar_dip_long_b1_0;
+        w0[1] = &hh_n2ar_dip_long_w0_1[0][0]; b0[1] = hh_n2ar_dip_long_b0_1; w1[1] = &hh_n2ar_dip_long_w1_1[0][0]; b1[1] = hh_n2ar_dip_long_b1_1;
+        w0[2] = &hh_n2ar_dip_long_w0_2[0][0]; b0[2] = hh_n2ar_dip_long_b0_2; w1[2] = &hh_n2ar_dip_long_w1_2[0][0]; b1[2] = hh_n2ar_dip_long_b1_2;
+    } else {
+        w0[0] = &hh_n2ar_dip_short_w0_0[0][0]; b0[0] = hh_n2ar_dip_short_b0_0; w1[0] = &hh_n2ar_dip_short_w1_0[0][0]; b1[0] = hh_n2ar_dip_short_b1_0;
+        w0[1] = &hh_n2ar_dip_short_w0_1[0][0]; b0[1] = hh_n2ar_dip_short_b0_1; w1[1] = &hh_n2ar_dip_short_w1_1[0][0]; b1[1] = hh_n2ar_dip_short_b1_1;
+        w0[2] = &hh_n2ar_dip_short_w0_2[0][0]; b0[2] = hh_n2ar_dip_short_b0_2; w1[2] = &hh_n2ar_dip_short_w1_2[0][0]; b1[2] = hh_n2ar_dip_short_b1_2;
+    }
+    const int nin[3] = {HH_N2AR_DIP_NPIP0, HH_N2AR_DIP_NPIP1, HH_N2AR_DIP_NPIP2};
+    const int nhid[3] = {16, 16, 8}, nout[3] = {2, 2, 1};
+    int off = 0, qo = 0;
+    for (int s = 0; s < 3; ++s) {
+        double h[16];
+        for (int j = 0; j < nhid[s]; ++j) {
+            double a = b0[s][j];
+            for (int i = 0; i < nin[s]; ++i) a += ptr[off + i] * w0[s][i * nhid[s] + j];
+            h[j] = silu(a);
+        }
+        for (int o = 0; o < nout[s]; ++o) {
+            double a = b1[s][o];
+            for (int j = 0; j < nhid[s]; ++j) a += h[j] * w1[s][j * nout[s] + o];
+            q[qo++] = a;
+        }
+        off += nin[s];
+    }
+}
+
+/* dipole_bf (ai_ids_n2_ar_pip_nn.cpp:83-127): body-frame dipole at (R, Theta) */
+void hho_n2ar_dip_mol(double R, double Theta, double dm[3]) {
+    double h = L_N2 / 2.0, s = sin(Theta), c = cos(Theta);
+    double x[5][3] = {{h * s, 0.0, h * c}, {-h * s, 0.0, -h * c}, {h * c, 0.0, -h * s},
+                      {-h * c, 0.0, h * s}, {0.0, 0.0, R}};
+    double dist[10];
+    int k = 0;
+    for (int i = 0; i < 5; ++i)
+        for (int j = i + 1; j < 5; ++j) {
+            double a = x[i][0] - x[j][0], b = x[i][1] - x[j][1], e = x[i][2] - x[j][2];
+            dist[k++] = sqrt(a * a + b * b + e * e);
+        }
+    double out[2][3];
+    const double a0[2] = {2.0, 6.0};
+    for (int m = 0; m < 2; ++m) {
+        double q[5], qi[5];
+        n2ar_charges(m, dist, a0[m], q);
+        n2ar_charges(m, NULL, a0[m], qi);
+        for (int cc = 0; cc < 3; ++cc) {
+            out[m][cc] = 0.0;
+            for (int i = 0; i < 5; ++i) out[m][cc] += (q[i] - qi[i]) * x[i][cc];
+        }
+    }
+    /* R of the N-site centre to Ar (the centre is the origin here) */
+    double cx = 0.25 * (x[0][0] + x[1][0] + x[2][0] + x[3][0]);
+    double cy = 0.25 * (x[0][1] + x[1][1] + x[2][1] + x[3][1]);
+    double cz = 0.25 * (x[0][2] + x[1][2] + x[2][2] + x[3][2]);
+    double Rc = sqrt((cx - x[4][0]) * (cx - x[4][0]) + (cy - x[4][1]) * (cy - x[4][1]) +
+                     (cz - x[4][2]) * (cz - x[4][2]));
+    double sw = n2ar_sw(Rc, 9.5, 12.5);
+    for (int cc = 0; cc < 3; ++cc) dm[cc] = (1.0 - sw) * out[0][cc] + sw * out[1][cc];
+}
+
+/* dipole_lab (examples/correlation_n2_ar.cpp:52-76) */
+static void n2ar_dipole_lab(const double *q, double out[3]) {
+    double qmol[5];
+    hho_co2ar_lab_to_mol(q, qmol);
+    double dm[3];
+    hho_n2ar_dip_mol(qmol[0], qmol[4], dm);
+    double Mphi[3][3], Mth[3][3], Mpsi[3][3];
+    Sz(qmol[1], Mphi); Sx(qmol[2], Mth); Sz(qmol[3], Mpsi);
+    double t[3];
+    mtv(Mpsi, dm, t);
+    mtv(Mth, t, t);
+    mtv(Mphi, t, out);
+}
+
+/* systems with a linear monomer (phase point of 10, inertia II) */
+static int is_linear(const hho_system *sys) {
+    return sys->system == HHO_SYS_CO2AR || sys->system == HHO_SYS_N2AR;
+}
+
 int hho_qp_size(const hho_system *sys) { return sys->system == HHO_SYS_HEAR ? 6 : 10; }
 
 double hho_pes(const hho_system *sys, const double *q) {
     if (sys->system == HHO_SYS_HEAR) return hho_hear_V(q[2]);
+    if (sys->system == HHO_SYS_N2AR) return hho_n2ar_V_lab(q);
     double qmol[5];
     hho_co2ar_lab_to_mol(q, qmol);
     return hho_co2ar_V_mol(qmol[0], qmol[4]);
@@ -347,6 +605,10 @@ double hho_pes(const hho_system *sys, const double *q) {
 void hho_dpes(const hho_system *sys, const double *q, double *dVdq) {
     if (sys->system == HHO_SYS_HEAR) {
         dVdq[0] = 0.0; dVdq[1] = 0.0; dVdq[2] = hho_hear_dV(q[2]);
+        return;
+    }
+    if (sys->system == HHO_SYS_N2AR) {
+        n2ar_dpes_lab(q, dVdq);
         return;
     }
     co2ar_dpes_lab(q, dVdq);
@@ -358,6 +620,10 @@ void hho_dipole(const hho_system *sys, const double *q, double d[3]) {
         d[0] = dl * sin(Theta) * cos(Phi);
         d[1] = dl * sin(Theta) * sin(Phi);
         d[2] = dl * cos(Theta);
+        return;
+    }
+    if (sys->system == HHO_SYS_N2AR) {
+        n2ar_dipole_lab(q, d);
         return;
     }
     co2ar_dipole_lab(q, d);
@@ -387,7 +653,7 @@ void hho_rhs(const hho_system *sys, const double *y, double *yd) {
     yd[1] = -dV[0];
     yd[2] = pTheta / (mu * R2);
     yd[3] = pPhi * pPhi * cT / (mu * R2 * sT3) - dV[1];
-    if (sys->system == HHO_SYS_CO2AR) {
+    if (is_linear(sys)) {
         double I = sys->II;
         double pphi = y[7], th = y[8], pth = y[9];
         double s = sin(th), c = cos(th);
@@ -404,7 +670,7 @@ double hho_kinetic(const hho_system *sys, const double *qp) {
     double sT = sin(Theta);
     double K = pR * pR / (2.0 * mu) + pTheta * pTheta / (2.0 * mu * R * R) +
                pPhi * pPhi / (2.0 * mu * R * R * sT * sT);
-    if (sys->system == HHO_SYS_CO2AR) {
+    if (is_linear(sys)) {
         double I = sys->II, pphi = qp[7], th = qp[8], pth = qp[9];
         double s = sin(th);
         K += pth * pth / (2.0 * I) + pphi * pphi / (2.0 * I * s * s);
@@ -429,7 +695,7 @@ void hho_qp_to_cart(const hho_system *sys, const double *qp, double *cart) {
         cart[i] = R * Rh[i];
         cart[3 + i] = pR * Rh[i] + pTh / R * Th_h[i] + pPhi / (R * sT) * Ph_h[i];
     }
-    if (sys->system == HHO_SYS_CO2AR) {
+    if (is_linear(sys)) {
         double ph = qp[6], pph = qp[7], th = qp[8], pth = qp[9];
         double s = sin(th), c = cos(th), sp = sin(ph), cp = cos(ph);
         double u[3] = {s * cp, s * sp, c};
@@ -466,7 +732,7 @@ int hho_candidate(hho_mt *s, const hho_system *sys, const hho_params *p, double 
     qp[0] = hho_mt_drand(s) * 2.0 * M_PI;
     qp[2] = acos(2.0 * hho_mt_drand(s) - 1.0);
     *draws += 3;
-    if (sys->system == HHO_SYS_CO2AR) {
+    if (is_linear(sys)) {
         qp[6] = hho_mt_drand(s) * 2.0 * M_PI;
         qp[8] = acos(2.0 * hho_mt_drand(s) - 1.0);
         *draws += 2;
@@ -479,7 +745,7 @@ int hho_candidate(hho_mt *s, const hho_system *sys, const hho_params *p, double 
     qp[1] = sqrt_MUKT * qp[4] * sinTheta * x[0];
     qp[3] = sqrt_MUKT * qp[4] * x[1];
     qp[5] = sqrt_MUKT * x[2];
-    if (sys->system == HHO_SYS_CO2AR) {
+    if (is_linear(sys)) {
         double sqrt_IIKT = sqrt(sys->II / HkT * T);
         double sin_theta = sin(qp[8]);
         double x0 = generate_normal(s, draws);
@@ -941,7 +1207,7 @@ static void *m0_worker(void *arg) {
         double q[5] = {Phi, acos(cT), R, 0.0, 0.0};
         double kappa;
         double zc = cos(2.0 * M_PI * u24(w[8]));
-        if (J->sys->system == HHO_SYS_CO2AR) {
+        if (is_linear(J->sys)) {
             q[3] = 2.0 * M_PI * u24(w[3]);
             q[4] = acos(2.0 * u24(w[4]) - 1.0);
             kappa = -log(u24(w[5])) - log(u24(w[6])) - log(u24(w[7])) * zc * zc;

@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-enum { HHO_SYS_HEAR = 0, HHO_SYS_CO2AR = 1 };
+enum { HHO_SYS_HEAR = 0, HHO_SYS_CO2AR = 1, HHO_SYS_N2AR = 2 };
 enum { HHO_PS_FREE_AND_METASTABLE = 1, HHO_PS_BOUND = 2, HHO_PS_ALL = 3 };
 
 /* per-half-trajectory status codes (same numbering as the CUDA library) */
@@ -43,7 +43,7 @@ enum {
 typedef struct {
     int system;      /* HHO_SYS_* */
     double mu;       /* reduced mass, a.u. */
-    double II;       /* moment of inertia of the linear monomer, a.u. (CO2-Ar) */
+    double II;       /* moment of inertia of the linear monomer, a.u. (CO2-Ar, N2-Ar) */
 } hho_system;
 
 typedef struct {
@@ -85,6 +85,13 @@ void hho_co2ar_dV_mol(double R, double theta, double *dR, double *dtheta);
 void hho_co2ar_dip_mol(double R, double theta, double d[3]);
 void hho_co2ar_lab_to_mol(const double *qlab, double *qmol);
 void hho_co2ar_jacobian(const double *qlab, double *jac25);
+/* N2-Ar PIP-NN: energy in cm^-1 (before the en_inf shift) from the distances
+ * |N1-N2|, |N1-Ar|, |N2-Ar| with dE/dd; lab-frame V in Hartree; body-frame dipole */
+double hho_n2ar_energy_cm(const double d[3], double dEdd[3]);
+void hho_n2ar_pes_pip(const double *y, double *p, double *jac);
+void hho_n2ar_dip_pip(const double *y, double *p);
+double hho_n2ar_V_lab(const double *q);
+void hho_n2ar_dip_mol(double R, double Theta, double dm[3]);
 double hho_pes(const hho_system *sys, const double *q);
 void hho_dpes(const hho_system *sys, const double *q, double *dVdq);
 void hho_dipole(const hho_system *sys, const double *q, double d[3]);

@@ -13,7 +13,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 
-SYS_HEAR, SYS_CO2AR = 0, 1
+SYS_HEAR, SYS_CO2AR, SYS_N2AR = 0, 1, 2
 PS_FREE_AND_METASTABLE, PS_BOUND, PS_ALL = 1, 2, 3
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
@@ -93,6 +93,18 @@ def lib():
         L.hho_m0_scale.argtypes = [C.POINTER(Params)]
         L.hho_analytic_pf.restype = C.c_double
         L.hho_analytic_pf.argtypes = [C.POINTER(System), C.c_double]
+        L.hho_n2ar_energy_cm.argtypes = [_dp, _dp]
+        L.hho_n2ar_energy_cm.restype = C.c_double
+        L.hho_n2ar_V_lab.argtypes = [_dp]
+        L.hho_n2ar_V_lab.restype = C.c_double
+        L.hho_n2ar_dip_mol.argtypes = [C.c_double, C.c_double, _dp]
+        L.hho_n2ar_pes_pip.argtypes = [_dp, _dp, _dp]
+        L.hho_n2ar_dip_pip.argtypes = [_dp, _dp]
+        L.hho_pes.argtypes = [C.POINTER(System), _dp]
+        L.hho_pes.restype = C.c_double
+        L.hho_dpes.argtypes = [C.POINTER(System), _dp, _dp]
+        L.hho_dipole.argtypes = [C.POINTER(System), _dp, _dp]
+        L.hho_rhs.argtypes = [C.POINTER(System), _dp, _dp]
         _lib = L
     return _lib
 
@@ -187,6 +199,54 @@ def qp_to_cart(sysd, qp):
     return out
 
 
+def pes(sysd, q):
+    return lib().hho_pes(C.byref(sysd), np.ascontiguousarray(q, dtype=np.float64))
+
+
+def dpes(sysd, q):
+    out = np.zeros(5)
+    lib().hho_dpes(C.byref(sysd), np.ascontiguousarray(q, dtype=np.float64), out)
+    return out
+
+
+def dipole(sysd, q):
+    out = np.zeros(3)
+    lib().hho_dipole(C.byref(sysd), np.ascontiguousarray(q, dtype=np.float64), out)
+    return out
+
+
+def rhs(sysd, y):
+    y = np.ascontiguousarray(y, dtype=np.float64)
+    out = np.zeros(y.size)
+    lib().hho_rhs(C.byref(sysd), y, out)
+    return out
+
+
+def n2ar_energy_cm(d):
+    g = np.zeros(3)
+    e = lib().hho_n2ar_energy_cm(np.ascontiguousarray(d, dtype=np.float64), g)
+    return e, g
+
+
+def n2ar_dip_mol(R, theta):
+    out = np.zeros(3)
+    lib().hho_n2ar_dip_mol(R, theta, out)
+    return out
+
+
+def n2ar_pes_pip(y):
+    p = np.zeros(17)
+    jac = np.zeros(51)
+    lib().hho_n2ar_pes_pip(np.ascontiguousarray(y, dtype=np.float64), p, jac)
+    return p, jac.reshape(3, 17)
+
+
+def n2ar_dip_pip(y):
+    p = np.zeros(308)
+    lib().hho_n2ar_dip_pip(np.ascontiguousarray(y, dtype=np.float64), p)
+    return p
+
+
 # ---- reference pieces compiled from the reference sources (oracle/_ref) ----
 _ref = {}
 
@@ -214,5 +274,9 @@ def ref(name):
             L.dpes_co2ar.argtypes = [C.c_double, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         elif name == "co2ar_ids":
             L.ref_co2ar_dip_mol.argtypes = [C.c_double, C.c_double, _dp]
+        elif name == "n2ar_pip":
+            L.ref_n2ar_pes_pip.argtypes = [_dp, _dp]
+            L.ref_n2ar_pes_jac.argtypes = [_dp, _dp]
+            L.ref_n2ar_dip_pip.argtypes = [_dp, _dp]
         _ref[name] = L
     return _ref[name]
