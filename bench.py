@@ -49,7 +49,7 @@ def parse():
     ap.add_argument("--impl", default="b200", choices=["b200", "reference"])
     ap.add_argument("--trajectories", type=int, default=WORKLOAD["n_traj"])
     ap.add_argument("--samples", type=int, default=WORKLOAD["N"])
-    ap.add_argument("--mixed-tol", type=float, default=1e-7)
+    ap.add_argument("--mixed-tol", type=float, default=3e-8)
     ap.add_argument("--plain-steps", type=int, default=2)
     ap.add_argument("--no-accuracy", action="store_true")
     ap.add_argument("--no-cpu-baseline", action="store_true")
