@@ -32,6 +32,7 @@ HH_PAIR_STATE_BOUND = 2
 HH_PAIR_STATE_ALL = 3
 HH_SYSTEM_HE_AR = 1
 HH_SYSTEM_CO2_AR = 2
+HH_SYSTEM_N2_AR = 3
 HH_PRECISION_FP64 = 0
 HH_PRECISION_MIXED = 1
 

@@ -22,12 +22,15 @@ UNITS = [
     ("hh_api.cu", []),
     ("hh_sampler.cu", ["-fmad=false"]),
 ]
+# host-only units (the host compiler sees the generated tables as plain arrays)
+HOST_UNITS = ["hh_n2ar_host.cpp"]
+CXX = os.environ.get("CXX", "g++")
 
 
 def _sources():
     out = []
     for f in sorted(os.listdir(CSRC)):
-        if f.endswith((".cu", ".cuh", ".h")):
+        if f.endswith((".cu", ".cuh", ".h", ".cpp")):
             out.append(os.path.join(CSRC, f))
     out.append(os.path.join(os.path.dirname(PKG), "include", "hh_cuda.h"))
     return out
@@ -51,6 +54,13 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
         # share no device functions), so ptxas allocates the registers of the
         # out-of-line device functions within their callers' limits
         cmd = [NVCC, *ARCH, *COMMON, *flags, *(extra or []), "-c", "-o", obj, os.path.join(CSRC, src)]
+        if verbose:
+            print(" ".join(cmd), file=sys.stderr)
+        subprocess.run(cmd, check=True)
+        objs.append(obj)
+    for src in HOST_UNITS:
+        obj = os.path.join(LIBDIR, src.replace(".cpp", ".o"))
+        cmd = [CXX, "-O2", "-std=c++17", "-fPIC", "-c", "-o", obj, os.path.join(CSRC, src)]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         subprocess.run(cmd, check=True)

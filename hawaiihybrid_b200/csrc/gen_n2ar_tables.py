@@ -129,23 +129,62 @@ def main():
         emit_array(fh, "double", "hh_n2ar_pes_b0", z["0.bias"])
         emit_array(fh, "double", "hh_n2ar_pes_w1", z["2.weight"][:, 0])
         emit_array(fh, "double", "hh_n2ar_pes_b1", z["2.bias"])
-        # ---- dipole charge models ----
-        for tag, f in zip(("short", "long"), DIP_NPZ):
-            z = np.load(os.path.join(npz_dir, f))
-            fh.write(f"\n/* dipole charge model `{tag}` ({f}): sub-network s maps its PIP block\n"
-                     " * through SiLU(ptr W0 + b0) W1 + b1 to its charges */\n")
-            emit_array(fh, "double", f"hh_n2ar_dip_{tag}_xmean", z["xscaler.mean"])
-            emit_array(fh, "double", f"hh_n2ar_dip_{tag}_xscale", z["xscaler.scale"])
-            for s in range(3):
-                a = [int(x) for x in z[f"architecture.{s}"]]
-                if a[0] != sizes[s]:
-                    raise ValueError(f"{f}: sub-network {s} reads {a[0]} PIPs, basis has {sizes[s]}")
-                fh.write(f"#define HH_N2AR_DIP_{tag.upper()}_ARCH{s} {{{a[0]}, {a[1]}, {a[2]}}}\n")
-                emit_array(fh, "double", f"hh_n2ar_dip_{tag}_w0_{s}", z[f"blocks.{s}.0.weight"])
-                emit_array(fh, "double", f"hh_n2ar_dip_{tag}_b0_{s}", z[f"blocks.{s}.0.bias"])
-                emit_array(fh, "double", f"hh_n2ar_dip_{tag}_w1_{s}", z[f"blocks.{s}.2.weight"])
-                emit_array(fh, "double", f"hh_n2ar_dip_{tag}_b1_{s}", z[f"blocks.{s}.2.bias"])
-
+        # ---- dipole charge models, flattened: sub-network s of model m has its
+        # first-layer rows at w0[m][W0OFF[s] ...] ([nin][nhid] row-major), its
+        # hidden units at b0[m][B0OFF[s] ...], its output layer at w1[m][W1OFF[s] ...]
+        # ([nhid][nout] row-major) and its charges at b1/qinf[m][QOFF[s] ...] ----
+        archs = []
+        zs = [np.load(os.path.join(npz_dir, f)) for f in DIP_NPZ]
+        for s_ in range(3):
+            a = [int(x) for x in zs[0][f"architecture.{s_}"]]
+            for z in zs:
+                if [int(x) for x in z[f"architecture.{s_}"]] != a:
+                    raise ValueError("the two dipole models differ in architecture")
+            if a[0] != sizes[s_]:
+                raise ValueError(f"sub-network {s_} reads {a[0]} PIPs, basis has {sizes[s_]}")
+            archs.append(a)
+        w0off, b0off, w1off, qoff = [0], [0], [0], [0]
+        for a in archs:
+            w0off.append(w0off[-1] + a[0] * a[1])
+            b0off.append(b0off[-1] + a[1])
+            w1off.append(w1off[-1] + a[1] * a[2])
+            qoff.append(qoff[-1] + a[2])
+        fh.write("\n/* dipole charge models [0] = short range (a0 = 2), [1] = long range (a0 = 6)\n"
+                 " * (PES-IDS/npz/n2-ar-dipoleq-effquad-{short,long}.npz); sub-network s maps PIPs\n"
+                 " * [PIPOFF[s], PIPOFF[s+1]) through SiLU(ptr W0 + b0) W1 + b1 to charges\n"
+                 " * [QOFF[s], QOFF[s+1]) of the sites N1, N2, N1', N2', Ar */\n")
+        fh.write(f"#define HH_N2AR_DIP_NW0 {w0off[-1]}\n#define HH_N2AR_DIP_NB0 {b0off[-1]}\n"
+                 f"#define HH_N2AR_DIP_NW1 {w1off[-1]}\n#define HH_N2AR_DIP_NQ {qoff[-1]}\n")
+        pipoff = [0, sizes[0], sizes[0] + sizes[1], off]
+        emit_array(fh, "int", "hh_n2ar_dip_arch", np.array(archs))
+        emit_array(fh, "int", "hh_n2ar_dip_pipoff", pipoff)
+        emit_array(fh, "int", "hh_n2ar_dip_w0off", w0off)
+        emit_array(fh, "int", "hh_n2ar_dip_b0off", b0off)
+        emit_array(fh, "int", "hh_n2ar_dip_w1off", w1off)
+        emit_array(fh, "int", "hh_n2ar_dip_qoff", qoff)
+        # CSR over the monomial table (monomials are grouped by PIP)
+        polys = p
+        if np.any(np.diff(polys) < 0):
+            raise ValueError("dipole monomials are not grouped by PIP")
+        start = np.searchsorted(polys, np.arange(off + 1), side="left")
+        emit_array(fh, "short", "hh_n2ar_dip_start", start)
+        W0 = np.zeros((2, w0off[-1])); B0 = np.zeros((2, b0off[-1]))
+        W1 = np.zeros((2, w1off[-1])); B1 = np.zeros((2, qoff[-1]))
+        XM = np.zeros((2, off)); XS = np.zeros((2, off))
+        for m, z in enumerate(zs):
+            XM[m] = z["xscaler.mean"]
+            XS[m] = z["xscaler.scale"]
+            for s_ in range(3):
+                W0[m, w0off[s_]:w0off[s_ + 1]] = z[f"blocks.{s_}.0.weight"].ravel(order="C")
+                B0[m, b0off[s_]:b0off[s_ + 1]] = z[f"blocks.{s_}.0.bias"]
+                W1[m, w1off[s_]:w1off[s_ + 1]] = z[f"blocks.{s_}.2.weight"].ravel(order="C")
+                B1[m, qoff[s_]:qoff[s_ + 1]] = z[f"blocks.{s_}.2.bias"]
+        emit_array(fh, "double", "hh_n2ar_dip_xmean", XM)
+        emit_array(fh, "double", "hh_n2ar_dip_xscale", XS)
+        emit_array(fh, "double", "hh_n2ar_dip_w0", W0)
+        emit_array(fh, "double", "hh_n2ar_dip_b0", B0)
+        emit_array(fh, "double", "hh_n2ar_dip_w1", W1)
+        emit_array(fh, "double", "hh_n2ar_dip_b1", B1)
 
 if __name__ == "__main__":
     main()

@@ -79,6 +79,7 @@ struct Ctx {
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
   int num_sms = 0;
   Co2arTablesGlobal *d_tab = nullptr;
+  N2arDipFold *d_n2ar_fold = nullptr;  // N2-Ar dipole models, folded (hh_n2ar_fold.h)
   // MT19937 stream
   uint32_t *d_mt = nullptr;
   DevBuf<uint32_t> words[2];
@@ -260,6 +261,12 @@ int run_traj_dispatch(int precision, const TrajParams &P, const TrajIO &io) {
     if (precision == HH_PRECISION_MIXED) return launch_traj<SYS_HEAR, float, float, false>(P, io, nullptr);
     return launch_traj<SYS_HEAR, double, double, false>(P, io, nullptr);
   }
+  if (g.sys == SYS_N2AR) {
+    TrajIO io2 = io;
+    io2.dipnet = g.d_n2ar_fold;
+    if (precision == HH_PRECISION_MIXED) return launch_traj<SYS_N2AR, float, float, false>(P, io2, nullptr);
+    return launch_traj<SYS_N2AR, double, double, false>(P, io2, nullptr);
+  }
   // plain FP32 sums: compensation does not reduce the FP32 error of the surfaces,
   // which comes from the radial rows, and cost 12 % of the kernel's time
   if (precision == HH_PRECISION_MIXED) return launch_traj<SYS_CO2AR, float, float, false>(P, io, nullptr);
@@ -315,6 +322,7 @@ int run_trajectories(const hh_calc_params *p, const double *d_ic, uint64_t n, ui
   io.fail_count = g.fail_count.p;
   io.traj_per_iter = (long long)per_iter;
   io.item_trace = nullptr;
+  io.dipnet = nullptr;
   uint32_t *trace_host = g_trace_host;
   g_trace_host = nullptr;
   if (trace_host && g_trace_cap >= 4 * 2 * n) {
@@ -373,6 +381,35 @@ int run_trajectories(const hh_calc_params *p, const double *d_ic, uint64_t n, ui
     CK(cudaEventElapsedTime(&ms, g.ev[2], g.ev[3]));
     stats->traj_ms = ms;
   }
+  return HH_OK;
+}
+
+// launches the M0 kernel of the bound system over `grid` blocks; allocates nothing
+int launch_m0(const M0Args &a, int grid, bool mixed, double *partials) {
+  const int block = 256;
+  if (g.sys == SYS_HEAR) {
+    if (mixed) m0_kernel<SYS_HEAR, float, true><<<grid, block, 0, g.st>>>(a, g.d_tab, nullptr, partials);
+    else m0_kernel<SYS_HEAR, double, false><<<grid, block, 0, g.st>>>(a, g.d_tab, nullptr, partials);
+  } else if (g.sys == SYS_N2AR) {
+    const size_t smem = sizeof(N2arDipFold);
+    if (mixed) {
+      auto k = m0_kernel<SYS_N2AR, float, true>;
+      CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k<<<grid, block, smem, g.st>>>(a, g.d_tab, g.d_n2ar_fold, partials);
+    } else {
+      auto k = m0_kernel<SYS_N2AR, double, false>;
+      CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+      k<<<grid, block, smem, g.st>>>(a, g.d_tab, g.d_n2ar_fold, partials);
+    }
+  } else {
+    if (mixed)
+      m0_kernel<SYS_CO2AR, float, true><<<grid, block, sizeof(Co2arTables<float>), g.st>>>(
+          a, g.d_tab, nullptr, partials);
+    else
+      m0_kernel<SYS_CO2AR, double, false><<<grid, block, sizeof(Co2arTables<double>), g.st>>>(
+          a, g.d_tab, nullptr, partials);
+  }
+  CK(cudaGetLastError());
   return HH_OK;
 }
 
@@ -441,7 +478,7 @@ int hh_cuda_init(int device, const hh_system_desc *sys) {
   if (sid == HH_SYSTEM_HE_AR) {
     if (sys->monomer1_type != HH_MONOMER_ATOM || sys->monomer2_type != HH_MONOMER_ATOM)
       return HH_E_UNSUPPORTED_SYSTEM;
-  } else if (sid == HH_SYSTEM_CO2_AR) {
+  } else if (sid == HH_SYSTEM_CO2_AR || sid == HH_SYSTEM_N2_AR) {
     if (sys->monomer1_type != HH_MONOMER_LINEAR_MOLECULE || sys->monomer2_type != HH_MONOMER_ATOM)
       return HH_E_UNSUPPORTED_SYSTEM;
     if (!(sys->II1[0] > 0) || sys->II1[0] != sys->II1[1]) return HH_E_INVALID_ARGUMENT;
@@ -465,9 +502,15 @@ int hh_cuda_init(int device, const hh_system_desc *sys) {
     int rc = reseed(0);
     if (rc) return rc;
   }
-  g.sys = (sid == HH_SYSTEM_HE_AR) ? SYS_HEAR : SYS_CO2AR;
+  if (sid == HH_SYSTEM_N2_AR && !g.d_n2ar_fold) {
+    static N2arDipFold host_fold;
+    if (n2ar_build_fold(&host_fold) != 0) return HH_E_UNSUPPORTED_SYSTEM;
+    CK(cudaMalloc(&g.d_n2ar_fold, sizeof(N2arDipFold)));
+    CK(cudaMemcpy(g.d_n2ar_fold, &host_fold, sizeof host_fold, cudaMemcpyHostToDevice));
+  }
+  g.sys = (sid == HH_SYSTEM_HE_AR) ? SYS_HEAR : (sid == HH_SYSTEM_N2_AR) ? SYS_N2AR : SYS_CO2AR;
   g.mu = sys->mu;
-  g.II = (sid == HH_SYSTEM_CO2_AR) ? sys->II1[0] : 0.0;
+  g.II = (sid == HH_SYSTEM_HE_AR) ? 0.0 : sys->II1[0];
   g.QP = (sid == HH_SYSTEM_HE_AR) ? 6 : 10;
   g.D = (sid == HH_SYSTEM_HE_AR) ? 10 : 16;
   g.p_accept = 0.25;
@@ -605,20 +648,8 @@ int hh_cuda_m0(const hh_calc_params *p, const double *T, int nT, uint64_t n_samp
     a.n_samples = n_samples;
     a.offset = 0;
     a.seed = seed;
-    if (g.sys == SYS_HEAR) {
-      if (precision_mode == HH_PRECISION_MIXED)
-        m0_kernel<SYS_HEAR, float, true><<<grid, block, 0, g.st>>>(a, g.d_tab, g.m0_partials.p);
-      else
-        m0_kernel<SYS_HEAR, double, false><<<grid, block, 0, g.st>>>(a, g.d_tab, g.m0_partials.p);
-    } else {
-      if (precision_mode == HH_PRECISION_MIXED)
-        m0_kernel<SYS_CO2AR, float, true><<<grid, block, sizeof(Co2arTables<float>), g.st>>>(
-            a, g.d_tab, g.m0_partials.p);
-      else
-        m0_kernel<SYS_CO2AR, double, false><<<grid, block, sizeof(Co2arTables<double>), g.st>>>(
-            a, g.d_tab, g.m0_partials.p);
-    }
-    CK(cudaGetLastError());
+    int rc = launch_m0(a, grid, precision_mode == HH_PRECISION_MIXED, g.m0_partials.p);
+    if (rc) return rc;
     m0_finalize_kernel<<<1, 32, 0, g.st>>>(g.m0_partials.p, grid, g.m0_out.p);
     CK(cudaGetLastError());
     double out[M0_MAXT * 2];
@@ -767,19 +798,8 @@ int hh_cuda_m0_noalloc(const hh_calc_params *p, const double *T, int nT, uint64_
     a.n_samples = n_samples;
     a.offset = 0;
     a.seed = seed;
-    const bool mixed = precision_mode == HH_PRECISION_MIXED;
-    if (g.sys == SYS_HEAR) {
-      if (mixed) m0_kernel<SYS_HEAR, float, true><<<grid, block, 0, g.st>>>(a, g.d_tab, partials);
-      else m0_kernel<SYS_HEAR, double, false><<<grid, block, 0, g.st>>>(a, g.d_tab, partials);
-    } else {
-      if (mixed)
-        m0_kernel<SYS_CO2AR, float, true><<<grid, block, sizeof(Co2arTables<float>), g.st>>>(
-            a, g.d_tab, partials);
-      else
-        m0_kernel<SYS_CO2AR, double, false><<<grid, block, sizeof(Co2arTables<double>), g.st>>>(
-            a, g.d_tab, partials);
-    }
-    CK(cudaGetLastError());
+    rc = launch_m0(a, grid, precision_mode == HH_PRECISION_MIXED, partials);
+    if (rc) return rc;
     m0_finalize_kernel<<<1, 32, 0, g.st>>>(partials, grid, res + 2 * (size_t)t0);
     CK(cudaGetLastError());
   }
@@ -827,6 +847,7 @@ void hh_cuda_shutdown(void) {
   g.f_a.release();
   g.f_b.release();
   if (g.d_tab) cudaFree(g.d_tab);
+  if (g.d_n2ar_fold) cudaFree(g.d_n2ar_fold);
   if (g.d_mt) cudaFree(g.d_mt);
   for (auto &e : g.ev)
     if (e) cudaEventDestroy(e);

@@ -67,10 +67,12 @@ template <typename T> __device__ __forceinline__ T u24(uint32_t w) {
 
 template <int SYS, typename PHYS, bool COMP>
 __global__ void __launch_bounds__(256) m0_kernel(M0Args a, const Co2arTablesGlobal *gtab,
-                                                 double *partials) {
+                                                 const void *dipnet, double *partials) {
   extern __shared__ unsigned char smem_raw[];
   Co2arTables<PHYS> *tb = reinterpret_cast<Co2arTables<PHYS> *>(smem_raw);
+  N2arDipFold *fold = reinterpret_cast<N2arDipFold *>(smem_raw);
   if (SYS == SYS_CO2AR) load_tables<PHYS>(tb, gtab);
+  if (SYS == SYS_N2AR) load_words(fold, dipnet, sizeof(N2arDipFold));
   __syncthreads();
   double s[M0_MAXT], c[M0_MAXT], q[M0_MAXT];
   PHYS ikT[M0_MAXT];
@@ -99,6 +101,20 @@ __global__ void __launch_bounds__(256) m0_kernel(M0Args a, const Co2arTablesGlob
       PHYS d = hear_dip<PHYS>(R, iR);
       mu2 = d * d;
       kappa = -log(u24<PHYS>(w[5])) - log(u24<PHYS>(w[7])) * zc * zc;
+    } else if (SYS == SYS_N2AR) {
+      PHYS Phi = twopi * u24<PHYS>(w[1]);
+      PHYS cT = PHYS(2) * u24<PHYS>(w[2]) - PHYS(1);
+      PHYS ph = twopi * u24<PHYS>(w[3]);
+      PHYS ct = PHYS(2) * u24<PHYS>(w[4]) - PHYS(1);
+      PHYS sT = sqrt((PHYS(1) - cT) * (PHYS(1) + cT));
+      PHYS st = sqrt((PHYS(1) - ct) * (PHYS(1) + ct));
+      PHYS x = sT * st * cos(Phi - ph) + cT * ct;
+      // N1-Ar and N2-Ar distances with the N2 axis at angle acos(x) to r^
+      const PHYS h = PHYS(N2AR_L / 2.0), base = R * R + h * h, t = PHYS(2) * h * R * x;
+      V = n2ar_pes_energy<PHYS>(sqrt(base - t), sqrt(base + t));
+      const N2arDipBody<double> b = n2ar_dip_body(fold, double(R), double(x));
+      mu2 = PHYS(b.dx * b.dx + b.dz * b.dz);
+      kappa = -log(u24<PHYS>(w[5])) - log(u24<PHYS>(w[6])) - log(u24<PHYS>(w[7])) * zc * zc;
     } else {
       // x = cos(angle between r^ and u^) from the sampled lab angles
       PHYS Phi = twopi * u24<PHYS>(w[1]);

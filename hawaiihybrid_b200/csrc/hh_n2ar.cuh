@@ -1,0 +1,224 @@
+// N2-Ar PIP-NN surfaces on the device.
+//
+// PES (PES-IDS/ai_pes_n2_ar_pip_nn.cpp:8-146, PES-IDS/mlp.hpp:178-256): the
+// three site distances |N1-N2| (fixed, rigid rotor), d1 = |N1-Ar|, d2 = |N2-Ar|
+// map to y = exp(-d/2), switched to 1e4/d^6 on [6, 20] bohr for the N-Ar pairs,
+// then to 17 permutationally invariant polynomials (PIPs), a standard scaler, a
+// 17-32-1 SiLU network and an inverse scaler (cm^-1).  The kernels need dE/dd1
+// and dE/dd2 (the network's backward pass); the sampler and M0 need E.  The
+// network is unrolled over the constexpr tables of hh_n2ar_tables.h, so every
+// weight is a compile-time constant operand, and the function is called out of
+// line (one copy per kernel).
+//
+// Dipole (PES-IDS/ai_ids_n2_ar_pip_nn.cpp:11-128, PES-IDS/QModel.hpp:144-257):
+// five sites N1, N2 = -N1, N1', N2' = -N1' (the effective-quadrupole sites,
+// perpendicular to the N2 axis) and Ar; charges from 308 PIPs of y = exp(-d/a0)
+// of the 10 site distances through three SiLU sub-networks, minus the charges
+// at infinite separation; the dipole is sum q_i x_i, blended between the short-
+// (a0 = 2) and long-range (a0 = 6) models on R in [9.5, 12.5] bohr.  The kernels
+// evaluate the exact refolding of hh_n2ar_fold.h in FP64 on both precision
+// paths: the charges relative to infinity are small differences of O(0.1)
+// network outputs, which FP32 resolves only to about 5e-4 of the dipole.
+#pragma once
+
+#include <cuda_runtime.h>
+
+#include "hh_consts.h"
+#include "hh_n2ar_fold.h"
+#include "hh_n2ar_tables.h"
+
+namespace hh {
+
+constexpr double N2AR_L = 2.07856749;                 // src/constants.h:80
+constexpr double N2AR_EN_INF = 0.0384490895371528;    // ai_pes_n2_ar_pip_nn.cpp:130, cm^-1
+
+template <typename T> __device__ __forceinline__ T n2ar_silu(T x) { return x / (T(1) + exp(-x)); }
+
+// quintic switch 10r^3 - 15r^4 + 6r^5 on [xi, xf] and its derivative
+template <typename T> __device__ __forceinline__ T n2ar_switch(T x, T xi, T xf) {
+  if (x < xi) return T(0);
+  if (x < xf) {
+    const T r = (x - xi) / (xf - xi), r3 = r * r * r, r4 = r3 * r, r5 = r4 * r;
+    return T(10) * r3 - T(15) * r4 + T(6) * r5;
+  }
+  return T(1);
+}
+
+// y(d) of an N-Ar pair and dy/dd (ai_pes_n2_ar_pip_nn.cpp:43-101)
+template <typename T> __device__ __forceinline__ void n2ar_pair_y(T d, T &y, T &dy) {
+  const T xi = T(6), xf = T(20);
+  const T e = exp(-d / T(2));
+  if (d < xi) {
+    y = e;
+    dy = -e / T(2);
+    return;
+  }
+  const T d2 = d * d, d6 = d2 * d2 * d2, d7 = d6 * d;
+  if (d < xf) {
+    const T w = xf - xi, r = (d - xi) / w, r2 = r * r, r3 = r2 * r, r4 = r3 * r, r5 = r4 * r;
+    const T s = T(10) * r3 - T(15) * r4 + T(6) * r5;
+    const T ds = (T(30) * r2 - T(60) * r3 + T(30) * r4) / w;
+    y = (T(1) - s) * e + s * T(1e4) / d6;
+    dy = -ds * e - (T(1) - s) * e / T(2) + ds * T(1e4) / d6 - s * T(6e4) / d7;
+  } else {
+    y = T(1e4) / d6;
+    dy = -T(6e4) / d7;
+  }
+}
+
+// PES network: E (cm^-1, before the en_inf shift) and, with GRAD, dE/dy1 and
+// dE/dy2 (mlp.hpp:178-256: forward, then backward through the hidden layer and
+// the PIP Jacobian).  y0 = exp(-|N1-N2|/2) is fixed by the rigid rotor.
+template <typename T, bool GRAD>
+__device__ __forceinline__ T n2ar_pes_net(T y1, T y2, T *gy) {
+  constexpr int NP = HH_N2AR_PES_NPIP, NH = HH_N2AR_PES_HIDDEN;
+  const T y[3] = {exp(-T(N2AR_L) / T(2)), y1, y2};
+  T p[NP], j1[NP], j2[NP];
+#pragma unroll
+  for (int i = 0; i < NP; ++i) p[i] = j1[i] = j2[i] = T(0);
+#pragma unroll
+  for (int m = 0; m < HH_N2AR_PES_NMONO; ++m) {
+    const int pi = hh_n2ar_pes_poly[m];
+    T prod = T(1);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (hh_n2ar_pes_var[m][k] >= 0) prod *= y[hh_n2ar_pes_var[m][k]];
+    p[pi] += prod;
+    if (GRAD) {
+#pragma unroll
+      for (int k = 0; k < 4; ++k) {
+        const int vk = hh_n2ar_pes_var[m][k];
+        if (vk == 1 || vk == 2) {
+          T d = T(1);
+#pragma unroll
+          for (int i = 0; i < 4; ++i)
+            if (i != k && hh_n2ar_pes_var[m][i] >= 0) d *= y[hh_n2ar_pes_var[m][i]];
+          if (vk == 1) j1[pi] += d;
+          else j2[pi] += d;
+        }
+      }
+    }
+  }
+  T ptr[NP];
+#pragma unroll
+  for (int i = 0; i < NP; ++i) ptr[i] = (p[i] - T(hh_n2ar_pes_xmean[i])) * T(1.0 / hh_n2ar_pes_xscale[i]);
+  T out = T(hh_n2ar_pes_b1[0]);
+  T g[NH];
+#pragma unroll
+  for (int j = 0; j < NH; ++j) {
+    T h = T(hh_n2ar_pes_b0[j]);
+#pragma unroll
+    for (int i = 0; i < NP; ++i) h += ptr[i] * T(hh_n2ar_pes_w0[i][j]);
+    const T e = exp(-h), r = T(1) / (T(1) + e);
+    out += h * r * T(hh_n2ar_pes_w1[j]);
+    if (GRAD) g[j] = r * (T(1) + h * e * r) * T(hh_n2ar_pes_w1[j]);  // SiLU'(h) W1
+  }
+  if (GRAD) {
+    T a1 = T(0), a2 = T(0);
+#pragma unroll
+    for (int i = 0; i < NP; ++i) {
+      T a = T(0);
+#pragma unroll
+      for (int j = 0; j < NH; ++j) a += T(hh_n2ar_pes_w0[i][j]) * g[j];
+      a *= T(1.0 / hh_n2ar_pes_xscale[i]);
+      a1 += j1[i] * a;
+      a2 += j2[i] * a;
+    }
+    gy[0] = a1 * T(hh_n2ar_pes_y[1]);
+    gy[1] = a2 * T(hh_n2ar_pes_y[1]);
+  }
+  return T(hh_n2ar_pes_y[1]) * out + T(hh_n2ar_pes_y[0]);
+}
+
+template <typename T> struct N2arGrad {
+  T g1, g2;  // dV/dd1, dV/dd2 in Hartree/bohr
+};
+
+// dV/dd1, dV/dd2 (Hartree/bohr) for d1 = |N1-Ar|, d2 = |N2-Ar|; out of line
+template <typename T> __device__ __noinline__ N2arGrad<T> n2ar_pes_grad(T d1, T d2) {
+  T y1, dy1, y2, dy2, gy[2];
+  n2ar_pair_y(d1, y1, dy1);
+  n2ar_pair_y(d2, y2, dy2);
+  n2ar_pes_net<T, true>(y1, y2, gy);
+  const T s = T(1.0 / HH_HTOCM);
+  return {gy[0] * dy1 * s, gy[1] * dy2 * s};
+}
+
+// V (Hartree) for d1 = |N1-Ar|, d2 = |N2-Ar| (pes_xyz, ai_pes_n2_ar_pip_nn.cpp:127-132)
+template <typename T> __device__ __noinline__ T n2ar_pes_energy(T d1, T d2) {
+  T y1, dy1, y2, dy2;
+  n2ar_pair_y(d1, y1, dy1);
+  n2ar_pair_y(d2, y2, dy2);
+  const T e = n2ar_pes_net<T, false>(y1, y2, nullptr);
+  return (e - T(N2AR_EN_INF)) * T(1.0 / HH_HTOCM);
+}
+
+template <typename T> struct N2arDipBody {
+  T dx, dz;  // body-frame dipole: Ar on +z, the N2 axis in the xz plane at angle T
+};
+
+// body-frame dipole (FP64) at R (bohr) and c = cos T from the folded charge models
+// F (shared memory in the kernels); dipole_bf and dipole_xyz of
+// ai_ids_n2_ar_pip_nn.cpp:83-127.  Out of line.
+static __device__ __noinline__ N2arDipBody<double> n2ar_dip_body(const N2arDipFold *F, double R,
+                                                              double c) {
+  const double h = N2AR_L / 2.0;
+  const double s = sqrt(fmax(0.0, (1.0 - c) * (1.0 + c)));
+  const double base = h * h + R * R, hc = 2.0 * h * c * R, hs = 2.0 * h * s * R;
+  // the varying distances N1-Ar, N2-Ar, N1'-Ar, N2'-Ar
+  const double dv[4] = {sqrt(base - hc), sqrt(base + hc), sqrt(base + hs), sqrt(base - hs)};
+  const double sw = n2ar_switch(R, 9.5, 12.5);
+  N2arDipBody<double> out = {0.0, 0.0};
+#pragma unroll 1
+  for (int m = 0; m < 2; ++m) {
+    const double wm = (m == 0) ? 1.0 - sw : sw;
+    if (wm == 0.0) continue;
+    const double ia0 = (m == 0) ? 0.5 : 1.0 / 6.0;
+    double v[4], z[N2AR_NZ];
+#pragma unroll
+    for (int i = 0; i < 4; ++i) v[i] = exp(-dv[i] * ia0);
+    int k = 0;
+#pragma unroll
+    for (int i = 0; i < 4; ++i) z[k++] = v[i];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = i; j < 4; ++j) z[k++] = v[i] * v[j];
+#pragma unroll
+    for (int i = 0; i < 4; ++i)
+#pragma unroll
+      for (int j = i; j < 4; ++j)
+#pragma unroll
+        for (int l = j; l < 4; ++l) z[k++] = v[i] * v[j] * v[l];
+    double dh[N2AR_NH];
+#pragma unroll
+    for (int j = 0; j < N2AR_NH; ++j) dh[j] = 0.0;
+    const double2 *W = reinterpret_cast<const double2 *>(&F->w[m][0][0]);
+#pragma unroll 2
+    for (int kk = 0; kk < N2AR_NZ; ++kk) {
+      const double zk = z[kk];
+#pragma unroll
+      for (int j = 0; j < N2AR_NH / 2; ++j) {
+        const double2 w2 = W[kk * (N2AR_NH / 2) + j];
+        dh[2 * j] += zk * w2.x;
+        dh[2 * j + 1] += zk * w2.y;
+      }
+    }
+    double A = 0.0, B = 0.0, Q = 0.0;
+#pragma unroll
+    for (int j = 0; j < N2AR_NH; ++j) {
+      const double a = F->h0[m][j], d = dh[j];
+      const double sd = 1.0 / (1.0 + exp(-(a + d)));
+      const double ds = d * sd + a * sd * (1.0 - F->s0[m][j]) * (-expm1(-d));
+      const double t = ds * F->wo[m][j];
+      if (j < 16) A += t;
+      else if (j < 32) B += t;
+      else Q += t;
+    }
+    out.dx += wm * (h * s * A + h * c * B);
+    out.dz += wm * (h * c * A - h * s * B + R * Q);
+  }
+  return out;
+}
+
+}  // namespace hh

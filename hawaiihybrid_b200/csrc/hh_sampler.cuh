@@ -130,7 +130,7 @@ __device__ __forceinline__ double kinetic(const SamplerArgs &a, const double *qp
   double sT = sin(Theta);
   double K = pR * pR / (2.0 * mu) + pTheta * pTheta / (2.0 * mu * R * R) +
              pPhi * pPhi / (2.0 * mu * R * R * sT * sT);
-  if (a.sys == SYS_CO2AR) {
+  if (a.sys != SYS_HEAR) {
     double I = a.II, pphi = qp[7], th = qp[8], pth = qp[9];
     double s = sin(th);
     K += pth * pth / (2.0 * I) + pphi * pphi / (2.0 * I * s * s);
@@ -147,6 +147,17 @@ __device__ __forceinline__ double potential(const SamplerArgs &a, const Co2arTab
   }
   double y[12];
   qp_to_state<SYS_CO2AR>(qp, y);
+  if (a.sys == SYS_N2AR) {
+    // N1 = +L/2 u^, N2 = -L/2 u^ (lab_to_xyz, ai_pes_n2_ar_pip_nn.cpp:103-121)
+    const double h = N2AR_L / 2.0;
+    double d1 = 0.0, d2 = 0.0;
+    for (int c = 0; c < 3; ++c) {
+      const double e1 = y[c] - h * y[6 + c], e2 = y[c] + h * y[6 + c];
+      d1 += e1 * e1;
+      d2 += e2 * e2;
+    }
+    return n2ar_pes_energy<double>(sqrt(d1), sqrt(d2));
+  }
   double R = sqrt(y[0] * y[0] + y[1] * y[1] + y[2] * y[2]);
   double x = (y[0] * y[6] + y[1] * y[7] + y[2] * y[8]) / R;
   double V, VR, Vx;
@@ -177,7 +188,7 @@ __global__ void __launch_bounds__(256) candidate_kernel(
   qp[4] = pow(R3, 1.0 / 3.0);
   qp[0] = mt_d(words, pos) * 2.0 * HH_PI;
   qp[2] = acos(2.0 * mt_d(words, pos) - 1.0);
-  if (a.sys == SYS_CO2AR) {
+  if (a.sys != SYS_HEAR) {
     qp[6] = mt_d(words, pos) * 2.0 * HH_PI;
     qp[8] = acos(2.0 * mt_d(words, pos) - 1.0);
   }
@@ -190,7 +201,7 @@ __global__ void __launch_bounds__(256) candidate_kernel(
   qp[1] = sqrt_MUKT * qp[4] * sinTheta * x0;
   qp[3] = sqrt_MUKT * qp[4] * x1;
   qp[5] = sqrt_MUKT * x2;
-  if (a.sys == SYS_CO2AR) {
+  if (a.sys != SYS_HEAR) {
     double sqrt_IIKT = sqrt(a.II / HH_HKT * T);
     double sin_theta = sin(qp[8]);
     double m0 = bm_normal(words, pos, limit, retries, overrun);

@@ -28,11 +28,12 @@
 
 #include "hh_consts.h"
 #include "hh_dop853_tableau.h"
+#include "hh_n2ar.cuh"
 #include "hh_physics.cuh"
 
 namespace hh {
 
-enum { SYS_HEAR = 1, SYS_CO2AR = 2 };
+enum { SYS_HEAR = 1, SYS_CO2AR = 2, SYS_N2AR = 3 };
 
 struct TrajParams {
   double mu, II;
@@ -64,6 +65,7 @@ struct TrajIO {
   int *fail_count;
   long long traj_per_iter;    // trajectories per iteration; item -> C(t) slice of its iteration
   uint4 *item_trace;          // optional per-item (steps, samples, t_start, t_end) in ns
+  const void *dipnet;         // N2-Ar: the folded dipole models (N2arDipFold), global memory
 };
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
@@ -230,6 +232,76 @@ template <typename PHYS, typename STG, bool COMP> struct Co2ArSys {
   }
 };
 
+// N2-Ar: rigid N2 (sites at +-L/2 u^) and Ar, PIP-NN surfaces of hh_n2ar.cuh.
+// With a = (L/2) u^, d1 = |r - a| and d2 = |r + a| (N1-Ar, N2-Ar):
+//   dV/dr = g1 (r - a)/d1 + g2 (r + a)/d2,  dV/du^ = (L/2)(-g1 (r - a)/d1 + g2 (r + a)/d2)
+//   dp/dt = -dV/dr,  dj/dt = -u^ x dV/du^,  du/dt = (j x u)/I.
+// Dipole: mu = d_z r^ + d_x (u^ - x r^)/|u^ - x r^| with the body-frame (d_x, d_z) at
+// (R, x = r^.u^): the Euler-angle rotation of the reference (examples/correlation_n2_ar.cpp:52-76)
+// maps body z to r^ and body x to the in-plane normal to r^ on the N1 side.
+template <typename PHYS, typename STG, bool COMP> struct N2ArSys {
+  static constexpr int N = 12;
+  static constexpr int QP = 10;
+  static constexpr int NQ = 6;
+  static __device__ __forceinline__ constexpr int qidx(int i) { return i < 3 ? i : i + 3; }
+  double inv_mu, inv_II;
+  const N2arDipFold *fold;  // shared-memory copy
+  template <typename YT> __device__ void rhs(const YT *y, STG *f) const {
+    const PHYS r[3] = {PHYS(y[0]), PHYS(y[1]), PHYS(y[2])};
+    const PHYS u[3] = {PHYS(y[6]), PHYS(y[7]), PHYS(y[8])};
+    const PHYS iu = inv_sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    const PHYS h = PHYS(N2AR_L / 2.0);
+    const PHYS uh[3] = {u[0] * iu, u[1] * iu, u[2] * iu};
+    PHYS e1[3], e2[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      e1[c] = r[c] - h * uh[c];
+      e2[c] = r[c] + h * uh[c];
+    }
+    const PHYS i1 = inv_sqrt(e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2]);
+    const PHYS i2 = inv_sqrt(e2[0] * e2[0] + e2[1] * e2[1] + e2[2] * e2[2]);
+    const N2arGrad<PHYS> g = n2ar_pes_grad<PHYS>(PHYS(1) / i1, PHYS(1) / i2);
+    const PHYS a1 = g.g1 * i1, a2 = g.g2 * i2;
+    PHYS Gr[3], Gu[3];
+#pragma unroll
+    for (int c = 0; c < 3; ++c) {
+      Gr[c] = a1 * e1[c] + a2 * e2[c];
+      Gu[c] = h * (a2 * e2[c] - a1 * e1[c]);
+    }
+    const STG p0 = STG(y[3]), p1 = STG(y[4]), p2 = STG(y[5]);
+    const STG u0 = STG(y[6]), u1 = STG(y[7]), u2 = STG(y[8]);
+    const STG j0 = STG(y[9]), j1 = STG(y[10]), j2 = STG(y[11]);
+    const STG im = STG(inv_mu), iI = STG(inv_II);
+    f[0] = p0 * im;
+    f[1] = p1 * im;
+    f[2] = p2 * im;
+    f[3] = STG(-Gr[0]);
+    f[4] = STG(-Gr[1]);
+    f[5] = STG(-Gr[2]);
+    f[6] = (j1 * u2 - j2 * u1) * iI;
+    f[7] = (j2 * u0 - j0 * u2) * iI;
+    f[8] = (j0 * u1 - j1 * u0) * iI;
+    f[9] = STG(-(uh[1] * Gu[2] - uh[2] * Gu[1]));
+    f[10] = STG(-(uh[2] * Gu[0] - uh[0] * Gu[2]));
+    f[11] = STG(-(uh[0] * Gu[1] - uh[1] * Gu[0]));
+  }
+  // q = (r[3], u[3]); the dipole is FP64 on both precision paths (hh_n2ar.cuh)
+  __device__ void dipole(const double *q, PHYS d[3]) const {
+    const double R2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
+    const double iR = rsqrt(R2);
+    const double iu = rsqrt(q[3] * q[3] + q[4] * q[4] + q[5] * q[5]);
+    const double rh[3] = {q[0] * iR, q[1] * iR, q[2] * iR};
+    const double uh[3] = {q[3] * iu, q[4] * iu, q[5] * iu};
+    const double x = rh[0] * uh[0] + rh[1] * uh[1] + rh[2] * uh[2];
+    const N2arDipBody<double> b = n2ar_dip_body(fold, R2 * iR, x);
+    const double e[3] = {uh[0] - x * rh[0], uh[1] - x * rh[1], uh[2] - x * rh[2]};
+    const double en2 = e[0] * e[0] + e[1] * e[1] + e[2] * e[2];
+    const double ie = en2 > 0.0 ? rsqrt(en2) : 0.0;
+#pragma unroll
+    for (int c = 0; c < 3; ++c) d[c] = PHYS(b.dz * rh[c] + b.dx * e[c] * ie);
+  }
+};
+
 // spherical phase point (reference layout, src/hawaii.h:210-284) -> Cartesian
 template <int SYS>
 __device__ __forceinline__ void qp_to_state(const double *qp, double *y) {
@@ -246,7 +318,7 @@ __device__ __forceinline__ void qp_to_state(const double *qp, double *y) {
     y[i] = R * Rh[i];
     y[3 + i] = pR * Rh[i] + a * Thh[i] + b * Phh[i];
   }
-  if (SYS == SYS_CO2AR) {
+  if (SYS != SYS_HEAR) {
     double ph = qp[6], pph = qp[7], th = qp[8], pth = qp[9];
     double s, c, sp, cp;
     sincos(th, &s, &c);
@@ -787,6 +859,13 @@ template <typename PHYS> __host__ __device__ constexpr size_t smem_tables_bytes(
   return (sizeof(Co2arTables<PHYS>) + 15) / 16 * 16;
 }
 
+// block-wide copy of `bytes` (a multiple of 8) from global to shared memory
+__device__ __forceinline__ void load_words(void *dst, const void *src, size_t bytes) {
+  const double *s = static_cast<const double *>(src);
+  double *d = static_cast<double *>(dst);
+  for (size_t i = threadIdx.x; i < bytes / 8; i += blockDim.x) d[i] = s[i];
+}
+
 // block shape of traj_kernel: warps per block, and the blocks per SM that the
 // register allocation must allow
 constexpr int TRAJ_WARPS = 4;
@@ -795,7 +874,7 @@ constexpr int TRAJ_MIN_BLOCKS = 1;
 
 // dynamic shared memory of traj_kernel: coefficient tables (CO2-Ar) + one pool per warp
 template <int SYS, typename PHYS, typename STG> constexpr size_t traj_smem_bytes() {
-  return (SYS == SYS_CO2AR ? smem_tables_bytes<PHYS>() : 0) +
+  return (SYS == SYS_CO2AR ? smem_tables_bytes<PHYS>() : SYS == SYS_N2AR ? sizeof(N2arDipFold) : 0) +
          TRAJ_WARPS * sizeof(WarpSamples<STG, PHYS, (SYS == SYS_HEAR ? 3 : 6)>);
 }
 
@@ -808,6 +887,17 @@ __global__ void __launch_bounds__(TRAJ_THREADS, TRAJ_MIN_BLOCKS)
     Sys sys;
     sys.inv_mu = 1.0 / P.mu;
     auto *ws = reinterpret_cast<WarpSamples<STG, PHYS, Sys::NQ> *>(smem_raw);
+    traj_body<Sys, PHYS, STG>(sys, P, io, ws);
+  } else if (SYS == SYS_N2AR) {
+    using Sys = N2ArSys<PHYS, STG, COMP>;
+    Sys sys;
+    sys.inv_mu = 1.0 / P.mu;
+    sys.inv_II = 1.0 / P.II;
+    N2arDipFold *fold = reinterpret_cast<N2arDipFold *>(smem_raw);
+    load_words(fold, io.dipnet, sizeof(N2arDipFold));
+    __syncthreads();
+    sys.fold = fold;
+    auto *ws = reinterpret_cast<WarpSamples<STG, PHYS, Sys::NQ> *>(smem_raw + sizeof(N2arDipFold));
     traj_body<Sys, PHYS, STG>(sys, P, io, ws);
   } else {
     using Sys = Co2ArSys<PHYS, STG, COMP>;

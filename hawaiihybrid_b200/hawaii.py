@@ -49,6 +49,7 @@ PAIR_STATE_ALL = 3
 # ---- surfaces available on the device ----
 SYSTEM_HE_AR = _lib.HH_SYSTEM_HE_AR
 SYSTEM_CO2_AR = _lib.HH_SYSTEM_CO2_AR
+SYSTEM_N2_AR = _lib.HH_SYSTEM_N2_AR
 
 PRECISION_FP64 = _lib.HH_PRECISION_FP64
 PRECISION_MIXED = _lib.HH_PRECISION_MIXED

@@ -61,6 +61,7 @@ extern "C" {
  * int hh_cuda_system_id(void) next to pes_lab/dpes_lab/dipole_lab */
 #define HH_SYSTEM_HE_AR 1
 #define HH_SYSTEM_CO2_AR 2
+#define HH_SYSTEM_N2_AR 3   /* PIP-NN surfaces of PES-IDS/ai_pes_n2_ar_pip_nn.cpp, ai_ids_n2_ar_pip_nn.cpp */
 
 /* precision modes */
 #define HH_PRECISION_FP64 0  /* FP64 surfaces and stages: the plain drop-in path */

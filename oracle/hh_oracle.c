@@ -496,12 +496,11 @@ static void n2ar_dpes_lab(const double *q, double *dV) {
                           st * c[5]) / HTOCM;
 }
 
-/* one charge model: charges q[5] of N1, N2, N1', N2', Ar from the 10 site
- * distances (pairs i < j in site order), y = exp(-d / a0); p == NULL gives the
- * model's charges at infinite separation (all PIPs zero, QModel::forward_inf) */
+/* one charge model (0 short, 1 long range): charges q[5] of N1, N2, N1', N2', Ar
+ * from the 10 site distances (pairs i < j in site order), y = exp(-d / a0);
+ * dist == NULL gives the model's charges at infinite separation (all PIPs
+ * zero, QModel::forward_inf) */
 static void n2ar_charges(int model, const double *dist, double a0, double q[5]) {
-    const double *xm = model ? &hh_n2ar_dip_long_xmean[0] : &hh_n2ar_dip_short_xmean[0];
-    const double *xs = model ? &hh_n2ar_dip_long_xscale[0] : &hh_n2ar_dip_short_xscale[0];
     double p[HH_N2AR_DIP_NPIP] = {0};
     if (dist) {
         double y[10];
@@ -509,34 +508,26 @@ static void n2ar_charges(int model, const double *dist, double a0, double q[5]) 
         hho_n2ar_dip_pip(y, p);
     }
     double ptr[HH_N2AR_DIP_NPIP];
-    for (int i = 0; i < HH_N2AR_DIP_NPIP; ++i) ptr[i] = (p[i] - xm[i]) / xs[i];
-    /* sub-networks: PIPs [0,119) -> q0,q1; [119,238) -> q2,q3; [238,308) -> q4 */
-    const double *w0[3], *b0[3], *w1[3], *b1[3];
-    if (model) {
-        w0[0] = &hh_n2ar_dip_long_w0_0[0][0]; b0[0] = hh_n2ar_dip_long_b0_0; w1[0] = &hh_n2ar_dip_long_w1_0[0][0]; b1[0] = hh_n2ar_dip_long_b1_0;
-        w0[1] = &hh_n2ar_dip_long_w0_1[0][0]; b0[1] = hh_n2ar_dip_long_b0_1; w1[1] = &hh_n2ar_dip_long_w1_1[0][0]; b1[1] = hh_n2ar_dip_long_b1_1;
-        w0[2] = &hh_n2ar_dip_long_w0_2[0][0]; b0[2] = hh_n2ar_dip_long_b0_2; w1[2] = &hh_n2ar_dip_long_w1_2[0][0]; b1[2] = hh_n2ar_dip_long_b1_2;
-    } else {
-        w0[0] = &hh_n2ar_dip_short_w0_0[0][0]; b0[0] = hh_n2ar_dip_short_b0_0; w1[0] = &hh_n2ar_dip_short_w1_0[0][0]; b1[0] = hh_n2ar_dip_short_b1_0;
-        w0[1] = &hh_n2ar_dip_short_w0_1[0][0]; b0[1] = hh_n2ar_dip_short_b0_1; w1[1] = &hh_n2ar_dip_short_w1_1[0][0]; b1[1] = hh_n2ar_dip_short_b1_1;
-        w0[2] = &hh_n2ar_dip_short_w0_2[0][0]; b0[2] = hh_n2ar_dip_short_b0_2; w1[2] = &hh_n2ar_dip_short_w1_2[0][0]; b1[2] = hh_n2ar_dip_short_b1_2;
-    }
-    const int nin[3] = {HH_N2AR_DIP_NPIP0, HH_N2AR_DIP_NPIP1, HH_N2AR_DIP_NPIP2};
-    const int nhid[3] = {16, 16, 8}, nout[3] = {2, 2, 1};
-    int off = 0, qo = 0;
+    for (int i = 0; i < HH_N2AR_DIP_NPIP; ++i)
+        ptr[i] = (p[i] - hh_n2ar_dip_xmean[model][i]) / hh_n2ar_dip_xscale[model][i];
     for (int s = 0; s < 3; ++s) {
+        const int nin = hh_n2ar_dip_arch[s][0], nhid = hh_n2ar_dip_arch[s][1], nout = hh_n2ar_dip_arch[s][2];
+        const double *w0 = &hh_n2ar_dip_w0[model][hh_n2ar_dip_w0off[s]];
+        const double *b0 = &hh_n2ar_dip_b0[model][hh_n2ar_dip_b0off[s]];
+        const double *w1 = &hh_n2ar_dip_w1[model][hh_n2ar_dip_w1off[s]];
+        const double *b1 = &hh_n2ar_dip_b1[model][hh_n2ar_dip_qoff[s]];
+        const double *x = ptr + hh_n2ar_dip_pipoff[s];
         double h[16];
-        for (int j = 0; j < nhid[s]; ++j) {
-            double a = b0[s][j];
-            for (int i = 0; i < nin[s]; ++i) a += ptr[off + i] * w0[s][i * nhid[s] + j];
+        for (int j = 0; j < nhid; ++j) {
+            double a = b0[j];
+            for (int i = 0; i < nin; ++i) a += x[i] * w0[i * nhid + j];
             h[j] = silu(a);
         }
-        for (int o = 0; o < nout[s]; ++o) {
-            double a = b1[s][o];
-            for (int j = 0; j < nhid[s]; ++j) a += h[j] * w1[s][j * nout[s] + o];
-            q[qo++] = a;
+        for (int o = 0; o < nout; ++o) {
+            double a = b1[o];
+            for (int j = 0; j < nhid; ++j) a += h[j] * w1[j * nout + o];
+            q[hh_n2ar_dip_qoff[s] + o] = a;
         }
-        off += nin[s];
     }
 }
 

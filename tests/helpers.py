@@ -8,24 +8,38 @@ MU_CO2AR = 3.817083069753919e+04
 II_CO2 = 2.819827114123505e+05
 PESMIN_HEAR = -9.424412560638486e-05
 PESMIN_CO2AR = -8.913727688689150e-04
+# N2-Ar (constants.h:43-50,80,98; examples/correlation_n2_ar.cpp:214-234)
+MU_N2AR = 30016.287464295514
+II_N2 = 55141.90310147907
+PESMIN_N2AR = -97.3 / 2.1947463136320e5
+RMIN_N2AR = 4.51
 
 
 def oracle_system(name):
     if name == "hear":
         return O.System(O.SYS_HEAR, MU_HEAR, 0.0)
+    if name == "n2ar":
+        return O.System(O.SYS_N2AR, MU_N2AR, II_N2)
     return O.System(O.SYS_CO2AR, MU_CO2AR, II_CO2)
 
 
-def oracle_params(name, N, dt, tol=1e-12, ps=O.PS_FREE_AND_METASTABLE, Rmin=4.0, Rmax=40.0, Rcut=40.0,
+def _pesmin(name):
+    return {"hear": PESMIN_HEAR, "co2ar": PESMIN_CO2AR, "n2ar": PESMIN_N2AR}[name]
+
+
+def _rmin(name, Rmin):
+    return RMIN_N2AR if (name == "n2ar" and Rmin is None) else (4.0 if Rmin is None else Rmin)
+
+
+def oracle_params(name, N, dt, tol=1e-12, ps=O.PS_FREE_AND_METASTABLE, Rmin=None, Rmax=40.0, Rcut=40.0,
                   ppf=1.0):
-    pesmin = PESMIN_HEAR if name == "hear" else PESMIN_CO2AR
-    return O.Params(ps, Rmin, Rmax, pesmin, dt, N, Rcut, tol, tol, ppf, 50000)
+    return O.Params(ps, _rmin(name, Rmin), Rmax, _pesmin(name), dt, N, Rcut, tol, tol, ppf, 50000)
 
 
-def lib_params(name, N, dt, tol=1e-12, ps=1, Rmin=4.0, Rmax=40.0, Rcut=40.0, ppf=1.0, mixed_tol=1e-8):
+def lib_params(name, N, dt, tol=1e-12, ps=1, Rmin=None, Rmax=40.0, Rcut=40.0, ppf=1.0, mixed_tol=1e-8):
     from hawaiihybrid_b200 import hawaii as H
-    pesmin = PESMIN_HEAR if name == "hear" else PESMIN_CO2AR
-    return H.CalcParams(ps=ps, sampler_Rmin=Rmin, sampler_Rmax=Rmax, pesmin=pesmin, sampling_time=dt,
+    return H.CalcParams(ps=ps, sampler_Rmin=_rmin(name, Rmin), sampler_Rmax=Rmax, pesmin=_pesmin(name),
+                        sampling_time=dt,
                         MaxTrajectoryLength=N, cvode_tolerance=tol, Rcut=Rcut,
                         partial_partition_function_ratio=ppf, mixed_tolerance=mixed_tol)
 
@@ -34,6 +48,9 @@ def lib_system(name, seed=1):
     import hawaiihybrid_b200 as hh
     if name == "hear":
         return hh.init_ms(MU_HEAR, hh.ATOM, hh.ATOM, None, None, seed)
+    if name == "n2ar":
+        return hh.init_ms(MU_N2AR, hh.LINEAR_MOLECULE, hh.ATOM, (II_N2, II_N2), None, seed,
+                          system_id=hh.SYSTEM_N2_AR)
     return hh.init_ms(MU_CO2AR, hh.LINEAR_MOLECULE, hh.ATOM, (II_CO2, II_CO2), None, seed)
 
 
