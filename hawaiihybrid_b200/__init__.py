@@ -7,8 +7,9 @@ from . import _lib
 from ._lib import HHError
 from .hawaii import (ATOM, LINEAR_MOLECULE, PAIR_STATE_ALL, PAIR_STATE_BOUND,
                      PAIR_STATE_FREE_AND_METASTABLE, PRECISION_FP64, PRECISION_MIXED,
-                     SYSTEM_CO2_AR, SYSTEM_HE_AR, SYSTEM_N2_AR, CalcParams, CFnc, MoleculeSystem, SFnc,
-                     analytic_full_partition_function_by_V, calculate_correlation_and_save,
+                     SYSTEM_CO2_AR, SYSTEM_HE_AR, SYSTEM_N2_AR, CalcParams, CFnc, CFncArray, MoleculeSystem,
+                     SFnc, analytic_full_partition_function_by_V, calculate_correlation_and_save,
+                     calculate_correlation_array_and_save, correlation_array_iteration,
                      calculate_m0, correlation_from_initial_conditions, correlation_iteration,
                      correlation_iterations,
                      idct_cf_to_sf, init_ms, read_correlation_function, read_spectral_function,

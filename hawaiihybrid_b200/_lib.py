@@ -41,7 +41,7 @@ EXPORTS = (
     "hh_cuda_init", "hh_cuda_seed", "hh_cuda_sample", "hh_cuda_correlation", "hh_cuda_correlation_multi",
     "hh_cuda_correlation_ic", "hh_cuda_m0", "hh_cuda_idct_cf_to_sf", "hh_cuda_strerror",
     "hh_cuda_mt_stream", "hh_cuda_debug_inject", "hh_cuda_debug_item_trace", "hh_cuda_fma_peak",
-    "hh_cuda_shutdown", "hh_cuda_m0_noalloc",
+    "hh_cuda_shutdown", "hh_cuda_m0_noalloc", "hh_cuda_correlation_array",
 )
 
 
@@ -111,6 +111,9 @@ def load(path: str | None = None):
     L.hh_cuda_m0.argtypes = [C.POINTER(CalcParamsC), _dp, C.c_int, C.c_uint64, C.c_uint64, C.c_int,
                              _dp, _dp]
     L.hh_cuda_m0_noalloc.argtypes = L.hh_cuda_m0.argtypes
+    L.hh_cuda_correlation_array.argtypes = [C.POINTER(CalcParamsC), C.c_double, _dp, _dp, C.c_int, C.c_uint32,
+                                            C.c_uint64, C.c_int, _dp, _dp, C.POINTER(C.c_double),
+                                            C.POINTER(Stats)]
     L.hh_cuda_idct_cf_to_sf.argtypes = [_dp, C.c_size_t, C.c_double, _dp, _dp]
     L.hh_cuda_strerror.restype = C.c_char_p
     L.hh_cuda_strerror.argtypes = [C.c_int]

@@ -80,6 +80,8 @@ struct Ctx {
   int num_sms = 0;
   Co2arTablesGlobal *d_tab = nullptr;
   N2arDipFold *d_n2ar_fold = nullptr;  // N2-Ar dipole models, folded (hh_n2ar_fold.h)
+  N2arPesNet<double> *d_n2ar_pes_d = nullptr;  // N2-Ar PES network, FP64 and FP32
+  N2arPesNet<float> *d_n2ar_pes_f = nullptr;
   // MT19937 stream
   uint32_t *d_mt = nullptr;
   DevBuf<uint32_t> words[2];
@@ -98,6 +100,8 @@ struct Ctx {
   DevBuf<unsigned int> status_hist, queue;
   DevBuf<int> fail_flag, fail_list, fail_count, items;
   DevBuf<uint4> trace;
+  // CORRELATION_ARRAY weights [n][n_sat]: with ratios (C(t)) and without (nstar)
+  DevBuf<double> sat_w, sat_wraw;
   // M0
   DevBuf<double> m0_partials, m0_out;
   // FFT
@@ -264,7 +268,11 @@ int run_traj_dispatch(int precision, const TrajParams &P, const TrajIO &io) {
   if (g.sys == SYS_N2AR) {
     TrajIO io2 = io;
     io2.dipnet = g.d_n2ar_fold;
-    if (precision == HH_PRECISION_MIXED) return launch_traj<SYS_N2AR, float, float, false>(P, io2, nullptr);
+    if (precision == HH_PRECISION_MIXED) {
+      io2.pesnet = g.d_n2ar_pes_f;
+      return launch_traj<SYS_N2AR, float, float, false>(P, io2, nullptr);
+    }
+    io2.pesnet = g.d_n2ar_pes_d;
     return launch_traj<SYS_N2AR, double, double, false>(P, io2, nullptr);
   }
   // plain FP32 sums: compensation does not reduce the FP32 error of the surfaces,
@@ -276,9 +284,11 @@ int run_traj_dispatch(int precision, const TrajParams &P, const TrajIO &io) {
 // integrate both branches of n trajectories whose phase points are in d_ic;
 // trajectories [i*per_iter, (i+1)*per_iter) accumulate into C(t) slice i
 int run_trajectories(const hh_calc_params *p, const double *d_ic, uint64_t n, uint64_t per_iter,
-                     int precision, double *crln_host, hh_stats *stats) {
+                     int precision, double *crln_host, hh_stats *stats, const double *d_satw = nullptr,
+                     int n_sat = 0) {
   const size_t N = p->MaxTrajectoryLength;
-  const uint64_t n_iter = (n + per_iter - 1) / per_iter;
+  // C(t) slices: one per iteration, or one per satellite temperature
+  const uint64_t n_iter = (n_sat > 0) ? (uint64_t)n_sat : (n + per_iter - 1) / per_iter;
   TrajParams P;
   P.mu = g.mu;
   P.II = g.II;
@@ -323,6 +333,9 @@ int run_trajectories(const hh_calc_params *p, const double *d_ic, uint64_t n, ui
   io.traj_per_iter = (long long)per_iter;
   io.item_trace = nullptr;
   io.dipnet = nullptr;
+  io.pesnet = nullptr;
+  io.sat_w = d_satw;
+  io.n_sat = n_sat;
   uint32_t *trace_host = g_trace_host;
   g_trace_host = nullptr;
   if (trace_host && g_trace_cap >= 4 * 2 * n) {
@@ -507,6 +520,13 @@ int hh_cuda_init(int device, const hh_system_desc *sys) {
     if (n2ar_build_fold(&host_fold) != 0) return HH_E_UNSUPPORTED_SYSTEM;
     CK(cudaMalloc(&g.d_n2ar_fold, sizeof(N2arDipFold)));
     CK(cudaMemcpy(g.d_n2ar_fold, &host_fold, sizeof host_fold, cudaMemcpyHostToDevice));
+    static N2arPesNet<double> pes_d;
+    static N2arPesNet<float> pes_f;
+    n2ar_build_pes(&pes_d, &pes_f);
+    CK(cudaMalloc(&g.d_n2ar_pes_d, sizeof pes_d));
+    CK(cudaMalloc(&g.d_n2ar_pes_f, sizeof pes_f));
+    CK(cudaMemcpy(g.d_n2ar_pes_d, &pes_d, sizeof pes_d, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(g.d_n2ar_pes_f, &pes_f, sizeof pes_f, cudaMemcpyHostToDevice));
   }
   g.sys = (sid == HH_SYSTEM_HE_AR) ? SYS_HEAR : (sid == HH_SYSTEM_N2_AR) ? SYS_N2AR : SYS_CO2AR;
   g.mu = sys->mu;
@@ -584,6 +604,64 @@ int hh_cuda_correlation_multi(const hh_calc_params *p, double T, uint32_t seed,
   local.n_kernel_launches = g_launches;
   if (ntraj)
     for (uint32_t i = 0; i < n_iterations; ++i) ntraj[i] = (double)n_per_iteration;
+  if (stats) *stats = local;
+  return HH_OK;
+}
+
+int hh_cuda_correlation_array(const hh_calc_params *p, double base_T, const double *sat_T,
+                              const double *ppf_ratios, int n_sat, uint32_t seed, uint64_t n_accept,
+                              int precision_mode, double *crln_sums, double *nstar, double *ntraj,
+                              hh_stats *stats) {
+  if (!g.init) return HH_E_NOT_INITIALIZED;
+  int rc = check_params(p);
+  if (rc) return rc;
+  if (!(base_T > 0) || !sat_T || !ppf_ratios || !crln_sums || !nstar || n_sat < 1 || n_sat > SAT_MAX ||
+      n_accept == 0 || n_accept > (uint64_t)(INT32_MAX / 2))
+    return HH_E_INVALID_ARGUMENT;
+  for (int s = 0; s < n_sat; ++s)
+    if (!(sat_T[s] > 0)) return HH_E_INVALID_ARGUMENT;
+  // the reference has no weights for PAIR_STATE_ALL (hawaii.c:2652)
+  if (p->pair_state != HH_PAIR_STATE_FREE_AND_METASTABLE && p->pair_state != HH_PAIR_STATE_BOUND)
+    return HH_E_INVALID_ARGUMENT;
+  if (precision_mode != HH_PRECISION_FP64 && precision_mode != HH_PRECISION_MIXED)
+    return HH_E_INVALID_ARGUMENT;
+  CK(cudaSetDevice(g.device));
+  if (seed > 0) {
+    rc = reseed(seed);
+    if (rc) return rc;
+  }
+  hh_stats local;
+  memset(&local, 0, sizeof local);
+  g_launches = 0;
+  CK(g.qp0.ensure(n_accept * g.QP));
+  CK(g.sat_w.ensure(n_accept * n_sat));
+  CK(g.sat_wraw.ensure(n_accept * n_sat));
+  CK(cudaEventRecord(g.ev[0], g.st));
+  uint64_t ncand = 0;
+  rc = sample_into(p, base_T, n_accept, g.qp0.p, &ncand);
+  if (rc) return rc;
+  CK(launch_sat_weights(g.sys, g.mu, g.II, p->pesmin, p->pair_state, g.d_tab, g.qp0.p, (long long)n_accept,
+                        base_T, sat_T, ppf_ratios, n_sat, g.sat_w.p, g.sat_wraw.p, g.st));
+  g_launches += 1;
+  CK(cudaEventRecord(g.ev[1], g.st));
+  hh_calc_params p1 = *p;
+  p1.partial_partition_function_ratio = 1.0;  // the ratios are in the weights
+  rc = run_trajectories(&p1, g.qp0.p, n_accept, n_accept, precision_mode, crln_sums, &local, g.sat_w.p, n_sat);
+  if (rc) return rc;
+  std::vector<double> wraw(n_accept * (size_t)n_sat);
+  CK(cudaMemcpy(wraw.data(), g.sat_wraw.p, wraw.size() * sizeof(double), cudaMemcpyDeviceToHost));
+  for (int s = 0; s < n_sat; ++s) nstar[s] = 0.0;
+  for (uint64_t i = 0; i < n_accept; ++i)
+    for (int s = 0; s < n_sat; ++s) nstar[s] += wraw[i * n_sat + s];
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, g.ev[0], g.ev[1]));
+  local.sample_ms = ms;
+  CK(cudaEventElapsedTime(&ms, g.ev[0], g.ev[3]));
+  local.total_ms = ms;
+  local.n_candidates = ncand;
+  local.n_accepted = n_accept;
+  local.n_kernel_launches = g_launches;
+  if (ntraj) *ntraj = (double)n_accept;
   if (stats) *stats = local;
   return HH_OK;
 }
@@ -839,6 +917,8 @@ void hh_cuda_shutdown(void) {
   g.fail_count.release();
   g.items.release();
   g.trace.release();
+  g.sat_w.release();
+  g.sat_wraw.release();
   g.m0_partials.release();
   g.m0_out.release();
   g.f_cf.release();
@@ -848,6 +928,8 @@ void hh_cuda_shutdown(void) {
   g.f_b.release();
   if (g.d_tab) cudaFree(g.d_tab);
   if (g.d_n2ar_fold) cudaFree(g.d_n2ar_fold);
+  if (g.d_n2ar_pes_d) cudaFree(g.d_n2ar_pes_d);
+  if (g.d_n2ar_pes_f) cudaFree(g.d_n2ar_pes_f);
   if (g.d_mt) cudaFree(g.d_mt);
   for (auto &e : g.ev)
     if (e) cudaEventDestroy(e);

@@ -134,14 +134,67 @@ template <typename T> struct N2arGrad {
   T g1, g2;  // dV/dd1, dV/dd2 in Hartree/bohr
 };
 
-// dV/dd1, dV/dd2 (Hartree/bohr) for d1 = |N1-Ar|, d2 = |N2-Ar|; out of line
-template <typename T> __device__ __noinline__ N2arGrad<T> n2ar_pes_grad(T d1, T d2) {
-  T y1, dy1, y2, dy2, gy[2];
+// dV/dd1, dV/dd2 (Hartree/bohr) for d1 = |N1-Ar|, d2 = |N2-Ar|, out of line.  The
+// PIPs and their Jacobian are unrolled over the monomial table; the network is a
+// runtime loop over the 32 hidden units (forward and backward in one pass) with
+// the weights of `net` (shared memory in the kernels), so the code stays small.
+template <typename T>
+__device__ __noinline__ N2arGrad<T> n2ar_pes_grad(const N2arPesNet<T> *net, T d1, T d2) {
+  constexpr int NP = N2AR_PES_NP;
+  T y1, dy1, y2, dy2;
   n2ar_pair_y(d1, y1, dy1);
   n2ar_pair_y(d2, y2, dy2);
-  n2ar_pes_net<T, true>(y1, y2, gy);
-  const T s = T(1.0 / HH_HTOCM);
-  return {gy[0] * dy1 * s, gy[1] * dy2 * s};
+  const T y[3] = {exp(-T(N2AR_L) / T(2)), y1, y2};
+  T p[NP], j1[NP], j2[NP];
+#pragma unroll
+  for (int i = 0; i < NP; ++i) p[i] = j1[i] = j2[i] = T(0);
+#pragma unroll
+  for (int m = 0; m < HH_N2AR_PES_NMONO; ++m) {
+    const int pi = hh_n2ar_pes_poly[m];
+    T prod = T(1);
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      if (hh_n2ar_pes_var[m][k] >= 0) prod *= y[hh_n2ar_pes_var[m][k]];
+    p[pi] += prod;
+#pragma unroll
+    for (int k = 0; k < 4; ++k) {
+      const int vk = hh_n2ar_pes_var[m][k];
+      if (vk == 1 || vk == 2) {
+        T d = T(1);
+#pragma unroll
+        for (int i = 0; i < 4; ++i)
+          if (i != k && hh_n2ar_pes_var[m][i] >= 0) d *= y[hh_n2ar_pes_var[m][i]];
+        if (vk == 1) j1[pi] += d;
+        else j2[pi] += d;
+      }
+    }
+  }
+  T ptr[NP], a[NP];
+#pragma unroll
+  for (int i = 0; i < NP; ++i) {
+    ptr[i] = (p[i] - net->xmean[i]) * net->ixscale[i];
+    a[i] = T(0);
+  }
+#pragma unroll 1
+  for (int j = 0; j < N2AR_PES_NH; ++j) {
+    const T *w = net->w0t[j];
+    T h = net->b0[j];
+#pragma unroll
+    for (int i = 0; i < NP; ++i) h += ptr[i] * w[i];
+    const T e = exp(-h), r = T(1) / (T(1) + e);
+    const T g = r * (T(1) + h * e * r) * net->w1[j];  // SiLU'(h) W1
+#pragma unroll
+    for (int i = 0; i < NP; ++i) a[i] += w[i] * g;
+  }
+  T a1 = T(0), a2 = T(0);
+#pragma unroll
+  for (int i = 0; i < NP; ++i) {
+    const T ai = a[i] * net->ixscale[i];
+    a1 += j1[i] * ai;
+    a2 += j2[i] * ai;
+  }
+  const T s = net->yscale * T(1.0 / HH_HTOCM);
+  return {a1 * dy1 * s, a2 * dy2 * s};
 }
 
 // V (Hartree) for d1 = |N1-Ar|, d2 = |N2-Ar| (pes_xyz, ai_pes_n2_ar_pip_nn.cpp:127-132)

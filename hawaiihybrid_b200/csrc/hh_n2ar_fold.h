@@ -51,3 +51,19 @@ inline N2arMonomial n2ar_monomial(int k) {
 // builds the fold from the generated tables (hh_n2ar_host.cpp); returns 0 on
 // success, -1 when a PIP monomial has no Ar pair (the basis is not purified)
 int n2ar_build_fold(N2arDipFold *out);
+
+// The PES network in the layout of the trajectory kernels' compact loop: one
+// row of 20 (17 used) first-layer weights per hidden unit, so the loop over the
+// 32 hidden units reads each row with vector loads from shared memory.
+constexpr int N2AR_PES_NP = 17;
+constexpr int N2AR_PES_NH = 32;
+constexpr int N2AR_PES_ROW = 20;
+template <typename T> struct N2arPesNet {
+  T w0t[N2AR_PES_NH][N2AR_PES_ROW];  // w0t[j][i] = W0[i][j]
+  T b0[N2AR_PES_NH];
+  T w1[N2AR_PES_NH];
+  T xmean[N2AR_PES_ROW];
+  T ixscale[N2AR_PES_ROW];           // 1 / xscale
+  T ymean, yscale, b1, pad;
+};
+void n2ar_build_pes(N2arPesNet<double> *d, N2arPesNet<float> *f);

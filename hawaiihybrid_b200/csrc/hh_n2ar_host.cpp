@@ -32,6 +32,26 @@ int monomial_index(int deg, const int *v) {
 double logistic(double x) { return 1.0 / (1.0 + std::exp(-x)); }
 }  // namespace
 
+void n2ar_build_pes(N2arPesNet<double> *d, N2arPesNet<float> *f) {
+  std::memset(d, 0, sizeof *d);
+  std::memset(f, 0, sizeof *f);
+  for (int j = 0; j < N2AR_PES_NH; ++j) {
+    for (int i = 0; i < N2AR_PES_NP; ++i) d->w0t[j][i] = hh_n2ar_pes_w0[i][j];
+    d->b0[j] = hh_n2ar_pes_b0[j];
+    d->w1[j] = hh_n2ar_pes_w1[j];
+  }
+  for (int i = 0; i < N2AR_PES_NP; ++i) {
+    d->xmean[i] = hh_n2ar_pes_xmean[i];
+    d->ixscale[i] = 1.0 / hh_n2ar_pes_xscale[i];
+  }
+  d->ymean = hh_n2ar_pes_y[0];
+  d->yscale = hh_n2ar_pes_y[1];
+  d->b1 = hh_n2ar_pes_b1[0];
+  const double *src = reinterpret_cast<const double *>(d);
+  float *dst = reinterpret_cast<float *>(f);
+  for (size_t k = 0; k < sizeof *d / sizeof(double); ++k) dst[k] = (float)src[k];
+}
+
 int n2ar_build_fold(N2arDipFold *out) {
   std::memset(out, 0, sizeof *out);
   static double M[HH_N2AR_DIP_NPIP][N2AR_NZ];

@@ -30,6 +30,25 @@ cudaError_t launch_candidates(int sys, double mu, double II, double T, double Rm
   return cudaGetLastError();
 }
 
+cudaError_t launch_sat_weights(int sys, double mu, double II, double pesmin, int pair_state,
+                               const Co2arTablesGlobal *gtab, const double *qp, long long n, double T0,
+                               const double *Ts, const double *ratio, int n_sat, double *w, double *wraw,
+                               cudaStream_t st) {
+  if (n_sat < 1 || n_sat > SAT_MAX) return cudaErrorInvalidValue;
+  SamplerArgs a{sys, mu, II, T0, 0.0, 0.0, pesmin, pair_state};
+  SatArgs s;
+  s.n_sat = n_sat;
+  s.T0 = T0;
+  for (int k = 0; k < n_sat; ++k) {
+    s.Ts[k] = Ts[k];
+    s.ratio[k] = ratio[k];
+  }
+  size_t smem = (sys == SYS_CO2AR) ? sizeof(Co2arTables<double>) : 0;
+  long long blocks = (n + 255) / 256;
+  sat_weight_kernel<<<(unsigned)blocks, 256, smem, st>>>(a, s, gtab, qp, n, w, wraw);
+  return cudaGetLastError();
+}
+
 cudaError_t launch_compact(const unsigned char *accept, const double *qp_cand, long long n,
                            long long limit, int QP, long long out_base, long long out_cap,
                            double *qp_out, long long *cand_index_out, unsigned int *block_counts,

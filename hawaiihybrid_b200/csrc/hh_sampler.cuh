@@ -234,6 +234,46 @@ __global__ void __launch_bounds__(256) candidate_kernel(
   energy_out[c] = E;
 }
 
+// ---- CORRELATION_ARRAY reweighting (src/hawaii.c:2640-2676) ----
+// One thread per trajectory: its energy at the base temperature T0 (the same
+// Hamiltonian the sampler's filter used) and, per satellite temperature Ts,
+//   weight = exp(-E HkT / T0 / Ts (T0 - Ts)) / WTT,
+// with WTT = exp(-pesmin HkT / T0 / Ts (T0 - Ts)) for bound pairs below T0 and 1
+// otherwise, and weight = 0 for free pairs above T0.  w[i][s] = weight * ratio_s
+// feeds C(t); wraw[i][s] = weight feeds nstar.
+struct SatArgs {
+  int n_sat;
+  double T0;
+  double Ts[SAT_MAX];
+  double ratio[SAT_MAX];
+};
+
+__global__ void __launch_bounds__(256) sat_weight_kernel(SamplerArgs a, SatArgs s,
+                                                         const Co2arTablesGlobal *gtab,
+                                                         const double *qp, long long n, double *w,
+                                                         double *wraw) {
+  extern __shared__ unsigned char smem_raw[];
+  Co2arTables<double> *tb = reinterpret_cast<Co2arTables<double> *>(smem_raw);
+  if (a.sys == SYS_CO2AR) load_tables<double>(tb, gtab);
+  __syncthreads();
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const int QP = (a.sys == SYS_HEAR) ? 6 : 10;
+  double q[10];
+  for (int c = 0; c < QP; ++c) q[c] = qp[i * QP + c];
+  const double E = kinetic(a, q) + potential(a, tb, q);
+  const double T0 = s.T0;
+  for (int k = 0; k < s.n_sat; ++k) {
+    const double T = s.Ts[k];
+    double WTT = 1.0;
+    if (a.pair_state == 2 && T < T0) WTT = exp(-a.pesmin * HH_HKT / T0 / T * (T0 - T));
+    double weight = exp(-E * HH_HKT / T0 / T * (T0 - T)) / WTT;
+    if (a.pair_state == 1 && T > T0) weight = 0.0;
+    w[i * s.n_sat + k] = weight * s.ratio[k];
+    wraw[i * s.n_sat + k] = weight;
+  }
+}
+
 // ---- ordered compaction of accepted candidates ----
 __global__ void __launch_bounds__(1024) count_kernel(const unsigned char *accept, long long n,
                                                      long long limit, unsigned int *block_counts) {

@@ -66,6 +66,9 @@ struct TrajIO {
   long long traj_per_iter;    // trajectories per iteration; item -> C(t) slice of its iteration
   uint4 *item_trace;          // optional per-item (steps, samples, t_start, t_end) in ns
   const void *dipnet;         // N2-Ar: the folded dipole models (N2arDipFold), global memory
+  const void *pesnet;         // N2-Ar: the PES network (N2arPesNet) in the surface precision
+  const double *sat_w;        // CORRELATION_ARRAY: [n_traj][n_sat] weights (nullptr: one C(t))
+  int n_sat;                  // satellite temperatures; their C(t) are consecutive N-slices
 };
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
@@ -245,7 +248,8 @@ template <typename PHYS, typename STG, bool COMP> struct N2ArSys {
   static constexpr int NQ = 6;
   static __device__ __forceinline__ constexpr int qidx(int i) { return i < 3 ? i : i + 3; }
   double inv_mu, inv_II;
-  const N2arDipFold *fold;  // shared-memory copy
+  const N2arDipFold *fold;      // shared-memory copies
+  const N2arPesNet<PHYS> *pes;
   template <typename YT> __device__ void rhs(const YT *y, STG *f) const {
     const PHYS r[3] = {PHYS(y[0]), PHYS(y[1]), PHYS(y[2])};
     const PHYS u[3] = {PHYS(y[6]), PHYS(y[7]), PHYS(y[8])};
@@ -260,7 +264,7 @@ template <typename PHYS, typename STG, bool COMP> struct N2ArSys {
     }
     const PHYS i1 = inv_sqrt(e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2]);
     const PHYS i2 = inv_sqrt(e2[0] * e2[0] + e2[1] * e2[1] + e2[2] * e2[2]);
-    const N2arGrad<PHYS> g = n2ar_pes_grad<PHYS>(PHYS(1) / i1, PHYS(1) / i2);
+    const N2arGrad<PHYS> g = n2ar_pes_grad<PHYS>(pes, PHYS(1) / i1, PHYS(1) / i2);
     const PHYS a1 = g.g1 * i1, a2 = g.g2 * i2;
     PHYS Gr[3], Gu[3];
 #pragma unroll
@@ -537,6 +541,7 @@ template <typename STG, typename PHYS, int NQ> struct WarpSamples {
   double t0[32];
   double inv_h[32];
   double *crln[32];
+  const double *satw[32];
   PHYS mu0[3][32];
   PHYS prev[32];   // the owner's last stored sample before this round
   PHYS tail[32];   // the owner's last sample of the previous chunk
@@ -574,6 +579,7 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
   PHYS mu0[3] = {PHYS(0), PHYS(0), PHYS(0)};
   PHYS prev = PHYS(0), curr = PHYS(0);
   double *crln = io.crln;
+  const double *satw = nullptr;  // this trajectory's satellite weights
   int item = -1;           // -1: needs an item, -2: queue exhausted
   int k = 1;
   int since = 0, total = 0;
@@ -595,6 +601,7 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
           item = io.items ? io.items[idx] : (int)idx;
           const int traj = item >> 1;
           crln = io.crln + (size_t)(traj / io.traj_per_iter) * (size_t)P.N;
+          satw = io.sat_w ? io.sat_w + (size_t)traj * io.n_sat : nullptr;
           if (io.item_trace) t_begin = globaltimer_ns();
           s0 = nsteps;
           m0 = nsamp;
@@ -687,6 +694,7 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
         ws->inv_h[lane] = 1.0 / h_taken;
         ws->prev[lane] = curr;
         ws->crln[lane] = crln;
+        ws->satw[lane] = satw;
         ws->kst[lane] = k;
         ws->item[lane] = item;
         ws->cut[lane] = 0xffffffffu;
@@ -777,7 +785,13 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
             const int stop = (cut == 0xffffffffu) ? end_o : min(end_o, int(cut >> 3));
             const int chunk_end = min(end_o, base + m);
             if (j < stop) {
-              atomicAdd(&ws->crln[o][kks[u]], P.weight * double(val));
+              if (io.n_sat == 0) {
+                atomicAdd(&ws->crln[o][kks[u]], P.weight * double(val));
+              } else {
+                const double *w = ws->satw[o];
+                for (int s = 0; s < io.n_sat; ++s)
+                  atomicAdd(&ws->crln[o][(size_t)s * P.N + kks[u]], P.weight * w[s] * double(val));
+              }
               // the owner's last stored sample so far (a cut found in a later
               // chunk lies past every sample of this one)
               if (j == min(stop, chunk_end) - 1) ws->last[o] = val;
@@ -829,7 +843,12 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
       // with the opposite weight removes exactly what a dropped trajectory added
       if (!hard) {
         const PHYS c0 = mu0[0] * mu0[0] + mu0[1] * mu0[1] + mu0[2] * mu0[2];
-        atomicAdd(&crln[0], P.weight * double(c0));
+        if (io.n_sat == 0) {
+          atomicAdd(&crln[0], P.weight * double(c0));
+        } else {
+          for (int s = 0; s < io.n_sat; ++s)
+            atomicAdd(&crln[(size_t)s * P.N], P.weight * satw[s] * double(c0));
+        }
       }
       if (io.item_trace) {
         const unsigned long long t_end = globaltimer_ns();
@@ -874,7 +893,9 @@ constexpr int TRAJ_MIN_BLOCKS = 1;
 
 // dynamic shared memory of traj_kernel: coefficient tables (CO2-Ar) + one pool per warp
 template <int SYS, typename PHYS, typename STG> constexpr size_t traj_smem_bytes() {
-  return (SYS == SYS_CO2AR ? smem_tables_bytes<PHYS>() : SYS == SYS_N2AR ? sizeof(N2arDipFold) : 0) +
+  return (SYS == SYS_CO2AR   ? smem_tables_bytes<PHYS>()
+          : SYS == SYS_N2AR ? sizeof(N2arDipFold) + sizeof(N2arPesNet<PHYS>)
+                            : 0) +
          TRAJ_WARPS * sizeof(WarpSamples<STG, PHYS, (SYS == SYS_HEAR ? 3 : 6)>);
 }
 
@@ -894,10 +915,14 @@ __global__ void __launch_bounds__(TRAJ_THREADS, TRAJ_MIN_BLOCKS)
     sys.inv_mu = 1.0 / P.mu;
     sys.inv_II = 1.0 / P.II;
     N2arDipFold *fold = reinterpret_cast<N2arDipFold *>(smem_raw);
+    N2arPesNet<PHYS> *pes = reinterpret_cast<N2arPesNet<PHYS> *>(smem_raw + sizeof(N2arDipFold));
     load_words(fold, io.dipnet, sizeof(N2arDipFold));
+    load_words(pes, io.pesnet, sizeof(N2arPesNet<PHYS>));
     __syncthreads();
     sys.fold = fold;
-    auto *ws = reinterpret_cast<WarpSamples<STG, PHYS, Sys::NQ> *>(smem_raw + sizeof(N2arDipFold));
+    sys.pes = pes;
+    auto *ws = reinterpret_cast<WarpSamples<STG, PHYS, Sys::NQ> *>(smem_raw + sizeof(N2arDipFold) +
+                                                                   sizeof(N2arPesNet<PHYS>));
     traj_body<Sys, PHYS, STG>(sys, P, io, ws);
   } else {
     using Sys = Co2ArSys<PHYS, STG, COMP>;

@@ -70,6 +70,10 @@ class CalcParams:
     cf_filename: Optional[str] = None
     Rcut: float = 40.0
     partial_partition_function_ratio: float = 0.0
+    # CORRELATION_ARRAY (src/hawaii.h:313-365: num_satellite_temperatures, ...)
+    satellite_temperatures: Sequence[float] = ()
+    partial_partition_function_ratios: Sequence[float] = ()
+    cf_filenames: Sequence[str] = ()
     # device-path knobs (no reference counterpart)
     mixed_tolerance: float = 1e-8
     max_steps: int = 50000
@@ -212,6 +216,73 @@ def correlation_from_initial_conditions(ms: MoleculeSystem, params: CalcParams, 
     check(L.hh_cuda_correlation_ic(C.byref(pc), qp0.ravel(), qp0.shape[0], precision, crln,
                                    C.byref(st)))
     return crln, st
+
+
+def correlation_array_iteration(ms: MoleculeSystem, params: CalcParams, base_temperature: float, n: int,
+                                precision: int = PRECISION_FP64, seed: int = 0):
+    """One accumulation pass of calculate_correlation_array_and_save: returns
+    (data[n_sat, N] = sum_i w_is * ratio_s * crln_i, nstar[n_sat], ntraj, stats)."""
+    L = _bind(ms)
+    Ts = np.ascontiguousarray(params.satellite_temperatures, dtype=np.float64)
+    ratios = np.ascontiguousarray(params.partial_partition_function_ratios, dtype=np.float64)
+    if Ts.size < 1 or ratios.size != Ts.size:
+        raise ValueError("satellite_temperatures and partial_partition_function_ratios must have the same, "
+                         "nonzero length")
+    N = params.MaxTrajectoryLength
+    data = np.zeros(Ts.size * N, dtype=np.float64)
+    nstar = np.zeros(Ts.size, dtype=np.float64)
+    ntraj = C.c_double()
+    st = _lib.Stats()
+    pc = params.to_c()
+    check(L.hh_cuda_correlation_array(C.byref(pc), base_temperature, Ts, ratios, Ts.size, seed, n, precision,
+                                      data, nstar, C.byref(ntraj), C.byref(st)))
+    return data.reshape(Ts.size, N), nstar, ntraj.value, st
+
+
+@dataclasses.dataclass
+class CFncArray:
+    """CFncArray (src/hawaii.h): one unnormalised C(t) per satellite temperature."""
+    t: np.ndarray
+    data: np.ndarray        # [n_sat, N]
+    nstar: np.ndarray       # per satellite: sum of the trajectory weights
+    ntraj: float
+    satellite_temperatures: tuple
+
+
+def calculate_correlation_array_and_save(ms: MoleculeSystem, params: CalcParams, base_temperature: float,
+                                         precision: int = PRECISION_FP64, log=print) -> CFncArray:
+    """calculate_correlation_array_and_save (src/hawaii.c:2361-2793): trajectories sampled
+    at base_temperature, each added to the C(t) of every satellite temperature with the
+    reference's Boltzmann reweighting; after every pass each satellite's CF file is
+    rewritten, unnormalised, with ntraj = nstar (hawaii.c:2758-2771)."""
+    if params.total_trajectories <= 0 or params.niterations < 1:
+        raise ValueError("total_trajectories and niterations must be positive")
+    if params.ps not in (PAIR_STATE_FREE_AND_METASTABLE, PAIR_STATE_BOUND):
+        raise ValueError("CORRELATION_ARRAY supports the FREE_AND_METASTABLE and BOUND pair states")
+    Ts = tuple(float(x) for x in params.satellite_temperatures)
+    N = params.MaxTrajectoryLength
+    total = CFncArray(t=np.linspace(0.0, params.sampling_time * (N - 1), N), data=np.zeros((len(Ts), N)),
+                      nstar=np.zeros(len(Ts)), ntraj=0.0, satellite_temperatures=Ts)
+    if params.cf_filenames and len(params.cf_filenames) != len(Ts):
+        raise ValueError("one cf_filename per satellite temperature")
+    per_iter = params.total_trajectories // params.niterations
+    for it in range(params.niterations):
+        data, nstar, ntraj, _ = correlation_array_iteration(ms, params, base_temperature, per_iter, precision)
+        total.data += data
+        total.nstar += nstar
+        total.ntraj += ntraj
+        if log:
+            log(f"ITERATION {it + 1}/{params.niterations}: accumulated {int(total.ntraj)} trajectories. "
+                "Saving the temporary results")
+            for s, T in enumerate(Ts):
+                if total.nstar[s] > 0:
+                    m0 = total.data[s][0] / total.nstar[s] * ZeroCoeff / ALU ** 3
+                    log(f"T = {T:.2f}: NSTAR = {total.nstar[s]:.2f}, M0 ESTIMATE FROM CF: {m0:.5e}")
+        for s, fname in enumerate(params.cf_filenames):
+            with open(fname, "w") as fp:
+                write_correlation_function_ext(fp, CFnc(t=total.t, data=total.data[s], ntraj=total.nstar[s],
+                                                        Temperature=Ts[s], normalized=False))
+    return total
 
 
 def calculate_correlation_and_save(ms: MoleculeSystem, params: CalcParams, Temperature: float,

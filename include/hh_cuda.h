@@ -19,6 +19,8 @@
  *                            (src/hawaii.c:2970-3012) with correlation_eval
  *                            (src/hawaii.c:2116-2347) per trajectory
  *   hh_cuda_correlation_multi  niterations passes of that loop (src/hawaii.c:2970-3040)
+ *   hh_cuda_correlation_array  calculate_correlation_array_and_save's accumulation loop
+ *                            (src/hawaii.c:2361-2793; reweighting 2640-2676)
  *   hh_cuda_correlation_ic   correlation_eval over caller-supplied phase points
  *                            (src/hawaii.c:2116-2347, accumulation 3008)
  *   hh_cuda_m0               c_mpi_perform_integration(..., INTEGRAND_M0, ...)
@@ -133,6 +135,17 @@ int hh_cuda_correlation(const hh_calc_params *p, double T, uint32_t seed, uint64
 int hh_cuda_correlation_multi(const hh_calc_params *p, double T, uint32_t seed,
                               uint64_t n_per_iteration, uint32_t n_iterations, int precision_mode,
                               double *crln_sums, double *ntraj, hh_stats *stats);
+
+/* CORRELATION_ARRAY: n_accept trajectories sampled at base_T, each added to the
+ * C(t) of every satellite temperature sat_T[s] with the reference's reweighting
+ * w = exp(-E HkT / base_T / T (base_T - T)) / WTT (0 for free pairs above base_T)
+ * times ppf_ratios[s]: crln_sums[s][k] (n_sat x MaxTrajectoryLength),
+ * nstar[s] = sum of the weights, *ntraj = n_accept.  n_sat <= 64; the pair state
+ * must be FREE_AND_METASTABLE or BOUND. */
+int hh_cuda_correlation_array(const hh_calc_params *p, double base_T, const double *sat_T,
+                              const double *ppf_ratios, int n_sat, uint32_t seed, uint64_t n_accept,
+                              int precision_mode, double *crln_sums, double *nstar, double *ntraj,
+                              hh_stats *stats);
 
 /* Same as hh_cuda_correlation, for caller-supplied initial phase points qp0[n][QP_SIZE]. */
 int hh_cuda_correlation_ic(const hh_calc_params *p, const double *qp0, uint64_t n,

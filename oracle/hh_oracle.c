@@ -1058,6 +1058,8 @@ typedef struct {
     size_t begin, end;
     double *sum;
     hho_traj_stats *stats;
+    const double *w;   /* CORRELATION_ARRAY: [n][n_sat] weights, or NULL */
+    int n_sat;
 } corr_job;
 
 static void *corr_worker(void *arg) {
@@ -1068,7 +1070,12 @@ static void *corr_worker(void *arg) {
     for (size_t i = J->begin; i < J->end; ++i) {
         hho_traj_stats st;
         hho_correlation_eval(J->sys, J->p, J->qp0 + i * n, crln, &st);
-        for (size_t k = 0; k < N; ++k) J->sum[k] += J->p->ppf_ratio * crln[k];
+        if (J->w) {
+            for (int s = 0; s < J->n_sat; ++s)
+                for (size_t k = 0; k < N; ++k) J->sum[s * N + k] += J->w[i * J->n_sat + s] * crln[k];
+        } else {
+            for (size_t k = 0; k < N; ++k) J->sum[k] += J->p->ppf_ratio * crln[k];
+        }
         if (J->stats) J->stats[i] = st;
     }
     free(crln);
@@ -1084,7 +1091,7 @@ int hho_correlation_sum(const hho_system *sys, const hho_params *p, const double
     if (nthreads > 256) nthreads = 256;
     for (int w = 0; w < nthreads; ++w) {
         jobs[w] = (corr_job){sys, p, qp0, n * w / nthreads, n * (w + 1) / nthreads,
-                             calloc(N, sizeof(double)), stats};
+                             calloc(N, sizeof(double)), stats, NULL, 0};
         pthread_create(&th[w], NULL, corr_worker, &jobs[w]);
     }
     memset(crln_sum, 0, N * sizeof(double));
@@ -1251,4 +1258,41 @@ double hho_m0_scale(const hho_params *p) { return ZeroCoeff * 4.0 * M_PI * (p->R
 double hho_analytic_pf(const hho_system *sys, double T) {
     if (sys->system == HHO_SYS_HEAR) return pow(2.0 * M_PI * sys->mu * T / HkT, 1.5);
     return 4.0 * M_PI * pow(2.0 * M_PI * T / HkT, 2.5) * pow(sys->mu, 1.5) * sys->II;
+}
+
+/* ======================================================================== */
+/* CORRELATION_ARRAY (src/hawaii.c:2361-2793): trajectories sampled at the   */
+/* base temperature T0 are reweighted to satellite temperatures Ts           */
+/* (accumulation at hawaii.c:2640-2676)                                      */
+/* ======================================================================== */
+void hho_array_weights(int pair_state, double pesmin, double T0, const double *Ts, int n_sat,
+                       double E, double *w) {
+    for (int s = 0; s < n_sat; ++s) {
+        double T = Ts[s], WTT = 1.0;
+        if (pair_state == HHO_PS_BOUND && T < T0) WTT = exp(-pesmin * HkT / T0 / T * (T0 - T));
+        double weight = exp(-E * HkT / T0 / T * (T0 - T)) / WTT;
+        if (pair_state == HHO_PS_FREE_AND_METASTABLE && T > T0) weight = 0.0;
+        w[s] = weight;
+    }
+}
+
+int hho_correlation_sum_array(const hho_system *sys, const hho_params *p, const double *qp0, size_t n,
+                              int nthreads, const double *w, int n_sat, double *out) {
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 256) nthreads = 256;
+    size_t N = p->N;
+    pthread_t th[256];
+    corr_job jobs[256];
+    for (int t = 0; t < nthreads; ++t) {
+        jobs[t] = (corr_job){sys, p, qp0, n * t / nthreads, n * (t + 1) / nthreads,
+                             calloc(N * n_sat, sizeof(double)), NULL, w, n_sat};
+        pthread_create(&th[t], NULL, corr_worker, &jobs[t]);
+    }
+    memset(out, 0, N * n_sat * sizeof(double));
+    for (int t = 0; t < nthreads; ++t) {
+        pthread_join(th[t], NULL);
+        for (size_t k = 0; k < N * n_sat; ++k) out[k] += jobs[t].sum[k];
+        free(jobs[t].sum);
+    }
+    return 0;
 }

@@ -124,6 +124,14 @@ int hho_propagate(const hho_system *sys, const hho_params *p, const double *qp0,
 int hho_correlation_sum(const hho_system *sys, const hho_params *p, const double *qp0,
                         size_t n, int nthreads, double *crln_sum, hho_traj_stats *stats);
 
+/* ---- CORRELATION_ARRAY (hawaii.c:2361-2793) ---- */
+/* reweighting of one trajectory of energy E sampled at T0 to Ts[0..n_sat) (hawaii.c:2640-2664) */
+void hho_array_weights(int pair_state, double pesmin, double T0, const double *Ts, int n_sat,
+                       double E, double *w);
+/* out[s][N] = sum_i w[i][s] * crln_i (w carries the partial partition function ratios) */
+int hho_correlation_sum_array(const hho_system *sys, const hho_params *p, const double *qp0, size_t n,
+                              int nthreads, const double *w, int n_sat, double *out);
+
 /* ---- CF -> SF (hawaii.c:5401-5601); apodizes cf in place like the reference ---- */
 int hho_idct_cf_to_sf(double *cf, size_t N, double dt, double *nu, double *sf);
 

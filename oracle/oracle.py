@@ -100,11 +100,9 @@ def lib():
         L.hho_n2ar_dip_mol.argtypes = [C.c_double, C.c_double, _dp]
         L.hho_n2ar_pes_pip.argtypes = [_dp, _dp, _dp]
         L.hho_n2ar_dip_pip.argtypes = [_dp, _dp]
-        L.hho_pes.argtypes = [C.POINTER(System), _dp]
-        L.hho_pes.restype = C.c_double
-        L.hho_dpes.argtypes = [C.POINTER(System), _dp, _dp]
-        L.hho_dipole.argtypes = [C.POINTER(System), _dp, _dp]
-        L.hho_rhs.argtypes = [C.POINTER(System), _dp, _dp]
+        L.hho_array_weights.argtypes = [C.c_int, C.c_double, C.c_double, _dp, C.c_int, C.c_double, _dp]
+        L.hho_correlation_sum_array.argtypes = [C.POINTER(System), C.POINTER(Params), _dp, C.c_size_t, C.c_int,
+                                                _dp, C.c_int, _dp]
         _lib = L
     return _lib
 
@@ -220,6 +218,29 @@ def rhs(sysd, y):
     out = np.zeros(y.size)
     lib().hho_rhs(C.byref(sysd), y, out)
     return out
+
+
+def hamiltonian(sysd, qp):
+    return lib().hho_hamiltonian(C.byref(sysd), np.ascontiguousarray(qp, dtype=np.float64))
+
+
+def array_weights(pair_state, pesmin, T0, Ts, E):
+    """CORRELATION_ARRAY reweighting of one trajectory of energy E (hawaii.c:2640-2664)."""
+    Ts = np.ascontiguousarray(Ts, dtype=np.float64)
+    w = np.zeros(Ts.size)
+    lib().hho_array_weights(pair_state, pesmin, T0, Ts, Ts.size, E, w)
+    return w
+
+
+def correlation_sum_array(sysd, params, qp0, w, nthreads=None):
+    """out[s] = sum_i w[i, s] * crln_i (w carries the partial partition function ratios)."""
+    qp0 = np.ascontiguousarray(qp0, dtype=np.float64)
+    w = np.ascontiguousarray(w, dtype=np.float64)
+    n_sat = w.shape[1]
+    out = np.zeros(n_sat * params.N)
+    lib().hho_correlation_sum_array(C.byref(sysd), C.byref(params), qp0.ravel(), qp0.shape[0],
+                                    nthreads or os.cpu_count(), w.ravel(), n_sat, out)
+    return out.reshape(n_sat, params.N)
 
 
 def n2ar_energy_cm(d):
