@@ -77,6 +77,11 @@ struct Ctx {
   int QP = 0, D = 0;
   cudaStream_t st = nullptr;
   cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // side stream that generates the MT19937 words of the next call while this
+  // call's trajectories run
+  cudaStream_t st2 = nullptr;
+  cudaEvent_t ev_sampled = nullptr, ev_pregen = nullptr;
+  bool pregen_pending = false;
   int num_sms = 0;
   Co2arTablesGlobal *d_tab = nullptr;
   N2arDipFold *d_n2ar_fold = nullptr;  // N2-Ar dipole models, folded (hh_n2ar_fold.h)
@@ -170,7 +175,50 @@ int ensure_words(long long need_end) {
   return HH_OK;
 }
 
+// the main stream waits for words generated ahead on the side stream (they and
+// the generator state are read or rewritten next)
+int join_pregen() {
+  if (g.pregen_pending) {
+    CK(cudaStreamWaitEvent(g.st, g.ev_pregen, 0));
+    g.pregen_pending = false;
+  }
+  return HH_OK;
+}
+
+// After a call's sampling: generate, on the side stream, the next n words of the
+// stream, the ones the next call of the same size will consume.  They are the
+// words ensure_words would produce later; generating them now overlaps the
+// sequential MT19937 refresh with this call's trajectories.
+int pregen_words(long long n) {
+  n = std::min(n, 1LL << 26);
+  if (n <= 0 || g.pregen_pending) return HH_OK;
+  const long long need_end = g.wpos + n;
+  if (g.wbase <= g.wpos && g.wbase + g.wvalid >= need_end) return HH_OK;
+  const long long end_old = g.wbase + g.wvalid;
+  const long long left = std::max(0LL, end_old - g.wpos);
+  const long long gen = need_end - (g.wpos + left);
+  const long long nblk = (gen + MT_N - 1) / MT_N + 1;
+  const int nxt = 1 - g.cur;
+  CK(g.words[nxt].ensure((size_t)(left + nblk * MT_N)));
+  CK(cudaEventRecord(g.ev_sampled, g.st));
+  CK(cudaStreamWaitEvent(g.st2, g.ev_sampled, 0));
+  if (left) {
+    CK(cudaMemcpyAsync(g.words[nxt].p, g.words[g.cur].p + (g.wpos - g.wbase),
+                       (size_t)left * sizeof(uint32_t), cudaMemcpyDeviceToDevice, g.st2));
+  }
+  CK(launch_mt_generate(g.d_mt, g.words[nxt].p + left, nblk, g.st2));
+  g_launches += 1;
+  CK(cudaEventRecord(g.ev_pregen, g.st2));
+  g.pregen_pending = true;
+  g.cur = nxt;
+  g.wbase = g.wpos;
+  g.wvalid = left + nblk * MT_N;
+  return HH_OK;
+}
+
 int reseed(uint32_t seed) {
+  int rc = join_pregen();
+  if (rc) return rc;
   CK(launch_mt_seed(seed, g.d_mt, g.st));
   g.wbase = g.wvalid = g.wpos = 0;
   return HH_OK;
@@ -179,6 +227,8 @@ int reseed(uint32_t seed) {
 // draw n accepted phase points into d_out (device), in the reference's order
 int sample_into(const hh_calc_params *p, double T, uint64_t n, double *d_out, uint64_t *ncand_out) {
   uint64_t got = 0, ncand_total = 0;
+  int jrc = join_pregen();
+  if (jrc) return jrc;
   CK(g.cand_idx.ensure(std::max<uint64_t>(n, 1)));
   CK(g.scal.ensure(4));
   while (got < n) {
@@ -503,6 +553,9 @@ int hh_cuda_init(int device, const hh_system_desc *sys) {
   CK(cudaSetDevice(device));
   if (!g.init) {
     CK(cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithFlags(&g.st2, cudaStreamNonBlocking));
+    CK(cudaEventCreateWithFlags(&g.ev_sampled, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&g.ev_pregen, cudaEventDisableTiming));
     for (auto &e : g.ev) CK(cudaEventCreate(&e));
     CK(cudaDeviceGetAttribute(&g.num_sms, cudaDevAttrMultiProcessorCount, device));
     CK(cudaMalloc(&g.d_tab, sizeof(Co2arTablesGlobal)));
@@ -589,9 +642,12 @@ int hh_cuda_correlation_multi(const hh_calc_params *p, double T, uint32_t seed,
   CK(g.qp0.ensure(n_accept * g.QP));
   CK(cudaEventRecord(g.ev[0], g.st));
   uint64_t ncand = 0;
+  const long long wpos0 = g.wpos;
   rc = sample_into(p, T, n_accept, g.qp0.p, &ncand);
   if (rc) return rc;
   CK(cudaEventRecord(g.ev[1], g.st));
+  rc = pregen_words(g.wpos - wpos0);
+  if (rc) return rc;
   rc = run_trajectories(p, g.qp0.p, n_accept, n_per_iteration, precision_mode, crln_sums, &local);
   if (rc) return rc;
   float ms = 0.f;
@@ -638,7 +694,10 @@ int hh_cuda_correlation_array(const hh_calc_params *p, double base_T, const doub
   CK(g.sat_wraw.ensure(n_accept * n_sat));
   CK(cudaEventRecord(g.ev[0], g.st));
   uint64_t ncand = 0;
+  const long long wpos0 = g.wpos;
   rc = sample_into(p, base_T, n_accept, g.qp0.p, &ncand);
+  if (rc) return rc;
+  rc = pregen_words(g.wpos - wpos0);
   if (rc) return rc;
   CK(launch_sat_weights(g.sys, g.mu, g.II, p->pesmin, p->pair_state, g.d_tab, g.qp0.p, (long long)n_accept,
                         base_T, sat_T, ppf_ratios, n_sat, g.sat_w.p, g.sat_wraw.p, g.st));
@@ -898,6 +957,7 @@ void hh_cuda_shutdown(void) {
   if (!g.init) return;
   cudaSetDevice(g.device);
   cudaStreamSynchronize(g.st);
+  if (g.st2) cudaStreamSynchronize(g.st2);
   g.words[0].release();
   g.words[1].release();
   g.accept.release();
@@ -934,6 +994,9 @@ void hh_cuda_shutdown(void) {
   for (auto &e : g.ev)
     if (e) cudaEventDestroy(e);
   if (g.st) cudaStreamDestroy(g.st);
+  if (g.st2) cudaStreamDestroy(g.st2);
+  if (g.ev_sampled) cudaEventDestroy(g.ev_sampled);
+  if (g.ev_pregen) cudaEventDestroy(g.ev_pregen);
   g = Ctx();
 }
 
