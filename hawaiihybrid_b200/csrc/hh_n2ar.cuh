@@ -260,9 +260,10 @@ static __device__ __noinline__ N2arDipBody<double> n2ar_dip_body(const N2arDipFo
     double A = 0.0, B = 0.0, Q = 0.0;
 #pragma unroll
     for (int j = 0; j < N2AR_NH; ++j) {
-      const double a = F->h0[m][j], d = dh[j];
-      const double sd = 1.0 / (1.0 + exp(-(a + d)));
-      const double ds = d * sd + a * sd * (1.0 - F->s0[m][j]) * (-expm1(-d));
+      const double d = dh[j], u = expm1(-d);
+      const double e0 = F->e0[m][j];
+      const double sd = 1.0 / (1.0 + (e0 + e0 * u));
+      const double ds = sd * (d - F->c1[m][j] * u);
       const double t = ds * F->wo[m][j];
       if (j < 16) A += t;
       else if (j < 32) B += t;

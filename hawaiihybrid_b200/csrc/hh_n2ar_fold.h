@@ -12,8 +12,9 @@
 //   h(p) - h(0) = sum_k z_k w[k]          (the scaler mean cancels exactly)
 // and the charges relative to infinite separation (QModel::forward_inf) are
 //   q - q_inf = W1^T (SiLU(h0 + dh) - SiLU(h0))   (the output bias cancels),
-// with SiLU(a + d) - SiLU(a) = d s(a+d) + a s(a+d)(1 - s(a))(-expm1(-d)), s the
-// logistic function.  The dipole needs q_N1 - q_N2 and q_N1' - q_N2', so the
+// with SiLU(a + d) - SiLU(a) = s(a+d) (d - a (1 - s(a)) u), u = expm1(-d), s the
+// logistic function, and s(a+d) = 1 / (1 + e^-a (1 + u)): one expm1 and one
+// division per hidden unit.  The dipole needs q_N1 - q_N2 and q_N1' - q_N2', so the
 // output weights are stored differenced.  Every step avoids the cancellations of
 // the reference's q - q_inf, which cost FP32 about 5e-4 of the dipole.
 #pragma once
@@ -24,7 +25,8 @@ constexpr int N2AR_NH = 40;    // hidden units of the three sub-networks (16 + 1
 struct N2arDipFold {
   double w[2][N2AR_NZ][N2AR_NH];  // model m: dh_j = sum_k z_k w[m][k][j]
   double h0[2][N2AR_NH];          // pre-activations at all-zero PIPs
-  double s0[2][N2AR_NH];          // logistic(h0)
+  double e0[2][N2AR_NH];          // exp(-h0)
+  double c1[2][N2AR_NH];          // h0 (1 - logistic(h0))
   double wo[2][N2AR_NH];          // [0,16): W1[:,0]-W1[:,1] of sub-network 0 (q_N1 - q_N2);
                                   // [16,32): the same for sub-network 1 (q_N1' - q_N2');
                                   // [32,40): W1[:,0] of sub-network 2 (q_Ar)

@@ -87,7 +87,8 @@ int n2ar_build_fold(N2arDipFold *out) {
         for (int i = 0; i < nin; ++i)
           b += (0.0 - hh_n2ar_dip_xmean[m][p0 + i]) / hh_n2ar_dip_xscale[m][p0 + i] * W0[i * nh + j];
         out->h0[m][h0 + j] = b;
-        out->s0[m][h0 + j] = logistic(b);
+        out->e0[m][h0 + j] = std::exp(-b);
+        out->c1[m][h0 + j] = b * (1.0 - logistic(b));
         for (int k = 0; k < N2AR_NZ; ++k) {
           double a = 0.0;
           for (int i = 0; i < nin; ++i) a += M[p0 + i][k] / hh_n2ar_dip_xscale[m][p0 + i] * W0[i * nh + j];
