@@ -768,7 +768,6 @@ int hh_cuda_m0(const hh_calc_params *p, const double *T, int nT, uint64_t n_samp
   for (int t = 0; t < nT; ++t)
     if (!(T[t] > 0)) return HH_E_INVALID_ARGUMENT;
   CK(cudaSetDevice(g.device));
-  const int block = 256;
   const int grid = g.num_sms * 4;
   CK(g.m0_partials.ensure((size_t)grid * M0_MAXT * 2));
   CK(g.m0_out.ensure(M0_MAXT * 2));
@@ -918,7 +917,6 @@ int hh_cuda_m0_noalloc(const hh_calc_params *p, const double *T, int nT, uint64_
   int rc = m0_noalloc_scratch(g.device, &scratch);
   if (rc) return rc;
   double *partials = scratch, *res = scratch + M0_NOALLOC_PARTIALS;
-  const int block = 256;
   const int grid = std::min(g.num_sms * 4, M0_NOALLOC_MAX_BLOCKS);
   const int n_chunks = (nT + M0_MAXT - 1) / M0_MAXT;
   CK(cudaMemsetAsync(res, 0, sizeof(double) * 2 * M0_MAXT * n_chunks, g.st));
