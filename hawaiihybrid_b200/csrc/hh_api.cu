@@ -109,9 +109,13 @@ struct Ctx {
   DevBuf<double> sat_w, sat_wraw;
   // M0
   DevBuf<double> m0_partials, m0_out;
-  // FFT
+  // FFT, and the CUDA graph of its kernel sequence for the current (N, dt, buffers)
   DevBuf<double> f_cf, f_nu, f_sf;
   DevBuf<double2> f_a, f_b;
+  cudaGraphExec_t idct_exec = nullptr;
+  size_t idct_N = 0;
+  double idct_dt = 0.0;
+  const void *idct_bufs[5] = {nullptr, nullptr, nullptr, nullptr, nullptr};
 };
 
 Ctx g;
@@ -801,6 +805,21 @@ int hh_cuda_m0(const hh_calc_params *p, const double *T, int nT, uint64_t n_samp
   return HH_OK;
 }
 
+// the transform's kernels on g.st: pack, log2(2N) Stockham passes, finish
+void idct_enqueue(size_t N, double dt) {
+  const long long L = 2 * (long long)N;
+  const int tb = 256;
+  idct_pack_kernel<<<(unsigned)((L + tb - 1) / tb), tb, 0, g.st>>>(g.f_cf.p, (long long)N, dt, g.f_a.p);
+  idct_pack2_kernel<<<(unsigned)((N + tb - 1) / tb), tb, 0, g.st>>>(g.f_cf.p, (long long)N, g.f_a.p);
+  double2 *x = g.f_a.p, *y = g.f_b.p;
+  for (long long s = 1; s < L; s *= 2) {
+    stockham_pass_kernel<<<(unsigned)((L / 2 + tb - 1) / tb), tb, 0, g.st>>>(x, y, L, s);
+    std::swap(x, y);
+  }
+  idct_finish_kernel<<<(unsigned)((N + tb - 1) / tb), tb, 0, g.st>>>(x, (long long)N, dt, g.f_nu.p,
+                                                                      g.f_sf.p);
+}
+
 int hh_cuda_idct_cf_to_sf(double *cf, size_t N, double dt, double *nu, double *sf) {
   if (!g.init) return HH_E_NOT_INITIALIZED;
   if (!cf || !nu || !sf || !(dt > 0)) return HH_E_INVALID_ARGUMENT;
@@ -814,18 +833,28 @@ int hh_cuda_idct_cf_to_sf(double *cf, size_t N, double dt, double *nu, double *s
   CK(g.f_sf.ensure(N));
   CK(g.f_a.ensure(L));
   CK(g.f_b.ensure(L));
-  CK(cudaMemcpyAsync(g.f_cf.p, cf, N * sizeof(double), cudaMemcpyHostToDevice, g.st));
-  int tb = 256;
-  idct_pack_kernel<<<(unsigned)((L + tb - 1) / tb), tb, 0, g.st>>>(g.f_cf.p, (long long)N, dt, g.f_a.p);
-  idct_pack2_kernel<<<(unsigned)((N + tb - 1) / tb), tb, 0, g.st>>>(g.f_cf.p, (long long)N, g.f_a.p);
-  double2 *x = g.f_a.p, *y = g.f_b.p;
-  for (long long s = 1; s < L; s *= 2) {
-    stockham_pass_kernel<<<(unsigned)((L / 2 + tb - 1) / tb), tb, 0, g.st>>>(x, y, L, s);
-    std::swap(x, y);
+  // the ~log2(2N) + 3 small kernels are launch-bound: they are captured once per
+  // (N, dt, buffers) into a CUDA graph and replayed
+  const void *bufs[5] = {g.f_cf.p, g.f_nu.p, g.f_sf.p, g.f_a.p, g.f_b.p};
+  bool same = g.idct_exec && g.idct_N == N && g.idct_dt == dt;
+  for (int i = 0; i < 5; ++i) same = same && (g.idct_bufs[i] == bufs[i]);
+  if (!same) {
+    if (g.idct_exec) cudaGraphExecDestroy(g.idct_exec);
+    g.idct_exec = nullptr;
+    cudaGraph_t graph = nullptr;
+    CK(cudaStreamBeginCapture(g.st, cudaStreamCaptureModeThreadLocal));
+    idct_enqueue(N, dt);
+    CK(cudaStreamEndCapture(g.st, &graph));
+    const cudaError_t e = cudaGraphInstantiate(&g.idct_exec, graph, 0);
+    cudaGraphDestroy(graph);
+    CK(e);
+    g.idct_N = N;
+    g.idct_dt = dt;
+    for (int i = 0; i < 5; ++i) g.idct_bufs[i] = bufs[i];
   }
-  idct_finish_kernel<<<(unsigned)((N + tb - 1) / tb), tb, 0, g.st>>>(x, (long long)N, dt, g.f_nu.p,
-                                                                      g.f_sf.p);
-  CK(cudaGetLastError());
+  (void)L;
+  CK(cudaMemcpyAsync(g.f_cf.p, cf, N * sizeof(double), cudaMemcpyHostToDevice, g.st));
+  CK(cudaGraphLaunch(g.idct_exec, g.st));
   CK(cudaMemcpyAsync(nu, g.f_nu.p, N * sizeof(double), cudaMemcpyDeviceToHost, g.st));
   CK(cudaMemcpyAsync(sf, g.f_sf.p, N * sizeof(double), cudaMemcpyDeviceToHost, g.st));
   CK(cudaMemcpyAsync(cf, g.f_cf.p, N * sizeof(double), cudaMemcpyDeviceToHost, g.st));
@@ -984,6 +1013,7 @@ void hh_cuda_shutdown(void) {
   g.f_sf.release();
   g.f_a.release();
   g.f_b.release();
+  if (g.idct_exec) cudaGraphExecDestroy(g.idct_exec);
   if (g.d_tab) cudaFree(g.d_tab);
   if (g.d_n2ar_fold) cudaFree(g.d_n2ar_fold);
   if (g.d_n2ar_pes_d) cudaFree(g.d_n2ar_pes_d);

@@ -123,6 +123,23 @@ def test_idct_golden():
     np.testing.assert_allclose(sf.nu[::64][1:], g["sf_nu_every64"][1:], rtol=1e-9)
 
 
+def test_idct_graph_replay_and_recapture():
+    """The CF->SF kernels run as a captured CUDA graph: repeated calls replay it, a new
+    length or time step captures a new one; every result matches the oracle."""
+    import hawaiihybrid_b200 as hh
+    lib_system("hear")
+    rng = np.random.default_rng(4)
+    for N, dt in ((4096, 200.0), (4096, 200.0), (1024, 200.0), (4096, 100.0), (4096, 200.0)):
+        data = np.exp(-np.arange(N) / (0.1 * N)) * (1 + 0.01 * rng.standard_normal(N))
+        cf = hh.CFnc(t=dt * np.arange(N), data=data.copy(), ntraj=1.0, Temperature=300.0, normalized=True)
+        sf = hh.idct_cf_to_sf(cf)
+        nu_ref, sf_ref, cf_ref = O.idct_cf_to_sf(data, dt)
+        peak = np.max(np.abs(sf_ref))
+        assert np.max(np.abs(sf.data - sf_ref)) <= 1e-12 * peak
+        np.testing.assert_allclose(sf.nu, nu_ref, rtol=1e-12)
+        np.testing.assert_allclose(cf.data, cf_ref, rtol=0, atol=1e-15)
+
+
 @pytest.mark.parametrize("status,hard", [(3, True), (5, True), (1, False)])
 def test_failure_semantics(lib, status, hard):
     """A branch ending in a hard failure drops the whole trajectory (still counted);
