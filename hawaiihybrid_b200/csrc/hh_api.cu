@@ -151,7 +151,7 @@ void build_tables(Co2arTablesGlobal *t) {
 int check_params(const hh_calc_params *p) {
   if (!p) return HH_E_INVALID_ARGUMENT;
   if (!(p->sampler_Rmin > 0) || !(p->sampler_Rmax > p->sampler_Rmin)) return HH_E_INVALID_ARGUMENT;
-  if (!(p->sampling_time > 0) || p->MaxTrajectoryLength < 2) return HH_E_INVALID_ARGUMENT;
+  if (!(p->sampling_time > 0) || p->MaxTrajectoryLength < 1) return HH_E_INVALID_ARGUMENT;
   if (!(p->Rcut > 0) || !(p->cvode_tolerance > 0)) return HH_E_INVALID_ARGUMENT;
   if (p->pair_state < 1 || p->pair_state > 3) return HH_E_INVALID_ARGUMENT;
   if (p->MaxTrajectoryLength > (size_t)INT32_MAX) return HH_E_INVALID_ARGUMENT;
@@ -303,6 +303,7 @@ int launch_traj(const TrajParams &P, const TrajIO &io, int *grid_out) {
   size_t smem = traj_smem_bytes<SYS, PHYS, STG>();
   if (smem > 48 * 1024) CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
+  constexpr int TRAJ_THREADS = traj_threads<PHYS>();
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TRAJ_THREADS, smem));
   int grid = std::max(1, per_sm) * g.num_sms;
   long long need = (io.n_items + TRAJ_THREADS - 1) / TRAJ_THREADS;

@@ -503,7 +503,9 @@ __device__ __noinline__ void item_setup(const Sys &sys, const TrajParams &P, con
     for (int i = 9; i < N; ++i) y0[i] = -y0[i];
   }
   sys.rhs(y0, f0);
-  const double span = P.dt * double(P.N - 1);
+  // the sampled window bounds the first step (one sample interval when N = 1,
+  // where only the t = 0 term is kept)
+  const double span = P.dt * double(P.N > 1 ? P.N - 1 : 1);
   double d0 = 0.0, d1 = 0.0;
 #pragma unroll
   for (int i = 0; i < N; ++i) {
@@ -885,10 +887,13 @@ __device__ __forceinline__ void load_words(void *dst, const void *src, size_t by
   for (size_t i = threadIdx.x; i < bytes / 8; i += blockDim.x) d[i] = s[i];
 }
 
-// block shape of traj_kernel: warps per block, and the blocks per SM that the
-// register allocation must allow
-constexpr int TRAJ_WARPS = 4;
-constexpr int TRAJ_THREADS = TRAJ_WARPS * 32;
+// block shape of traj_kernel, measured per precision path on the CO2-Ar
+// workload: both use every register (255), so 8 warps run per SM either way.
+// The FP64 kernels run 10 % faster as one block of 8 warps (one copy of the
+// surface tables per SM); the FP32-stage kernels are 1 % faster as two blocks of
+// 4.  TRAJ_MIN_BLOCKS is the blocks per SM the register allocation must allow.
+template <typename PHYS> constexpr int traj_warps() { return sizeof(PHYS) == 8 ? 8 : 4; }
+template <typename PHYS> constexpr int traj_threads() { return 32 * traj_warps<PHYS>(); }
 constexpr int TRAJ_MIN_BLOCKS = 1;
 
 // dynamic shared memory of traj_kernel: coefficient tables (CO2-Ar) + one pool per warp
@@ -896,11 +901,11 @@ template <int SYS, typename PHYS, typename STG> constexpr size_t traj_smem_bytes
   return (SYS == SYS_CO2AR   ? smem_tables_bytes<PHYS>()
           : SYS == SYS_N2AR ? sizeof(N2arDipFold) + sizeof(N2arPesNet<PHYS>)
                             : 0) +
-         TRAJ_WARPS * sizeof(WarpSamples<STG, PHYS, (SYS == SYS_HEAR ? 3 : 6)>);
+         traj_warps<PHYS>() * sizeof(WarpSamples<STG, PHYS, (SYS == SYS_HEAR ? 3 : 6)>);
 }
 
 template <int SYS, typename PHYS, typename STG, bool COMP>
-__global__ void __launch_bounds__(TRAJ_THREADS, TRAJ_MIN_BLOCKS)
+__global__ void __launch_bounds__(traj_threads<PHYS>(), TRAJ_MIN_BLOCKS)
     traj_kernel(TrajParams P, TrajIO io, const Co2arTablesGlobal *gtab) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   if (SYS == SYS_HEAR) {
