@@ -15,6 +15,8 @@
 #include "../hawaiihybrid_b200/csrc/hh_co2ar_tables.h"
 #include "../hawaiihybrid_b200/csrc/hh_n2ar_tables.h"
 #include "../hawaiihybrid_b200/csrc/hh_dop853_tableau.h"
+#include "../hawaiihybrid_b200/csrc/hh_ch4co2_tables.h"
+#include "../hawaiihybrid_b200/csrc/hh_ch4co2_standin.h"
 
 /* ---- constants (src/constants.h:8-53, CODATA 2022) ---- */
 #define ALU 5.29177210903e-11
@@ -337,6 +339,206 @@ static void co2ar_dipole_lab(const double *q, double out[3]) {
 }
 
 /* ======================================================================== */
+/* CH4-CO2 (ROTOR + LINEAR).  Lab coordinates q (PHI THETA R PHI1 THETA1 PSI1 */
+/* PHI2 THETA2), src/angles_handler.cpp:357-365.                             */
+/* ======================================================================== */
+/* Sy_filler_non_standard (src/angles_handler.cpp:91-97) and its derivative */
+static void Sy_ns(double a, double m[3][3]) {
+    double s = sin(a), c = cos(a);
+    double r[3][3] = {{c, 0, s}, {0, 1, 0}, {-s, 0, c}};
+    memcpy(m, r, sizeof r);
+}
+static void mm(double a[3][3], double b[3][3], double o[3][3]) {
+    double t[3][3];
+    for (int i = 0; i < 3; ++i)
+        for (int j = 0; j < 3; ++j) t[i][j] = a[i][0] * b[0][j] + a[i][1] * b[1][j] + a[i][2] * b[2][j];
+    memcpy(o, t, sizeof t);
+}
+
+/* unit vectors of the intermolecular axis and of the CO2 axis in the lab frame:
+ * Sz(PHI)^T Sy_ns(THETA)^T z = (-sin THETA cos PHI, -sin THETA sin PHI, cos THETA)
+ * (src/angles_handler.cpp:396, 408) */
+static void ch4co2_axis(double Phi, double Th, double u[3]) {
+    u[0] = -sin(Th) * cos(Phi);
+    u[1] = -sin(Th) * sin(Phi);
+    u[2] = cos(Th);
+}
+
+/* S1 = Spsi1 Sx(theta1) Sz(phi1): lab -> CH4 body frame (src/angles_handler.cpp:384-394) */
+static void ch4co2_S1(double phi, double th, double psi, double S1[3][3]) {
+    double A[3][3], B[3][3], C[3][3];
+    Sz(psi, A); Sx(th, B); Sz(phi, C);
+    mm(A, B, S1);
+    mm(S1, C, S1);
+}
+
+/* CH4_linear_molecule_lab_to_kal (src/angles_handler.cpp:357-419):
+ * qkal = (R, PHI1K, THETA1K, PHI2K, THETA2K), the directions of the intermolecular
+ * axis and of the CO2 axis in the CH4 body frame */
+void hho_ch4co2_lab_to_kal(const double *qlab, double *qkal) {
+    qkal[0] = qlab[2];
+    double SPhi[3][3], STheta[3][3], S1[3][3], Sphi2[3][3], Stheta2[3][3];
+    Sz(qlab[0], SPhi); Sy_ns(qlab[1], STheta);
+    ch4co2_S1(qlab[3], qlab[4], qlab[5], S1);
+    Sz(qlab[6], Sphi2); Sy_ns(qlab[7], Stheta2);
+    double z[3] = {0, 0, 1}, dd[3];
+    mtv(STheta, z, dd); mtv(SPhi, dd, dd); mv(S1, dd, dd);
+    double c1 = dd[2], s1 = sqrt(1 - c1 * c1);
+    qkal[2] = acos(c1);
+    qkal[1] = atan2(dd[1] / s1, dd[0] / s1);
+    mtv(Stheta2, z, dd); mtv(Sphi2, dd, dd); mv(S1, dd, dd);
+    double c2 = dd[2], s2 = sqrt(1.0 - dd[2] * dd[2]);
+    qkal[4] = acos(c2);
+    qkal[3] = atan2(dd[1] / s2, dd[0] / s2);
+}
+
+/* GSL_SF_LEGENDRE_NONE with the Condon-Shortley phase, index l(l+1)/2 + m */
+static void legendre_lm(int lmax, double x, double *P) {
+    double s = sqrt((1.0 - x) * (1.0 + x));
+    double pmm = 1.0;
+    for (int m = 0; m <= lmax; ++m) {
+        if (m > 0) pmm *= -(2.0 * m - 1.0) * s;
+        P[m * (m + 1) / 2 + m] = pmm;
+        if (m + 1 <= lmax) {
+            double p1 = x * (2.0 * m + 1.0) * pmm, p0 = pmm;
+            P[(m + 1) * (m + 2) / 2 + m] = p1;
+            for (int l = m + 2; l <= lmax; ++l) {
+                double pl = ((2.0 * l - 1.0) * x * p1 - (double)(l + m - 1) * p0) / (double)(l - m);
+                P[l * (l + 1) / 2 + m] = pl;
+                p0 = p1;
+                p1 = pl;
+            }
+        }
+    }
+}
+
+/* radial function b at R (piece tables of hh_ch4co2_tables.h) */
+static double ch4co2_rad(int b, double R) {
+    int s = 0;
+    while (s < HH_CH4CO2_NSEG - 1 && R >= hh_ch4co2_seg_hi[s]) ++s;
+    const double *c = hh_ch4co2_rad[b][s];
+    double x = R - hh_ch4co2_centre[s];
+    double v = c[0] + x * (c[1] + x * (c[2] + x * c[3]));
+    return (s == HH_CH4CO2_NSEG - 1) ? v * pow(R, -6) : v;
+}
+
+/* dipole_vector (PES-IDS/ai_ids_ch4_co2.cpp:672-1067): sum over the 320 basis
+ * functions of rad_b(R) times the real part of their angular functions, here in
+ * the expanded form of hh_ch4co2_tables.h; Legendre functions of cos(theta) and
+ * cos(k phi), sin(k phi) from the angles, as the reference computes them */
+void hho_ch4co2_dipole_kal(const double *qkal, double d[3]) {
+    double R = qkal[0];
+    double P1[(HH_CH4CO2_L1MAX + 1) * (HH_CH4CO2_L1MAX + 2) / 2];
+    double P2[(HH_CH4CO2_L2MAX + 1) * (HH_CH4CO2_L2MAX + 2) / 2];
+    legendre_lm(HH_CH4CO2_L1MAX, cos(qkal[2]), P1);
+    legendre_lm(HH_CH4CO2_L2MAX, cos(qkal[4]), P2);
+    double t1[2][HH_CH4CO2_L1MAX + 1], t2[2][HH_CH4CO2_L2MAX + 1];
+    for (int k = 0; k <= HH_CH4CO2_L1MAX; ++k) { t1[0][k] = cos(k * qkal[1]); t1[1][k] = sin(k * qkal[1]); }
+    for (int k = 0; k <= HH_CH4CO2_L2MAX; ++k) { t2[0][k] = cos(k * qkal[3]); t2[1][k] = sin(k * qkal[3]); }
+    double rad[HH_CH4CO2_NB];
+    for (int b = 0; b < HH_CH4CO2_NB; ++b) rad[b] = ch4co2_rad(b, R);
+    double acc[HH_CH4CO2_NB][3];
+    memset(acc, 0, sizeof acc);
+    for (int t = 0; t < HH_CH4CO2_NTERM; ++t) {
+        const short *ix = hh_ch4co2_tidx[t];
+        int i1 = ix[2] >> 1, c1 = ix[2] & 1, i2 = ix[3] >> 1, c2 = ix[3] & 1;
+        int l1 = (int)((sqrt(8.0 * i1 + 1.0) - 1.0) / 2.0), l2 = (int)((sqrt(8.0 * i2 + 1.0) - 1.0) / 2.0);
+        int m1 = i1 - l1 * (l1 + 1) / 2, m2 = i2 - l2 * (l2 + 1) / 2;
+        double y1 = P1[i1] * (m1 ? t1[c1][m1] : 1.0);
+        double y2 = P2[i2] * (m2 ? t2[c2][m2] : 1.0);
+        acc[ix[0]][ix[1]] += hh_ch4co2_tcoef[t] * y1 * y2;
+    }
+    d[0] = d[1] = d[2] = 0.0;
+    for (int b = 0; b < HH_CH4CO2_NB; ++b)
+        for (int c = 0; c < 3; ++c) d[c] += acc[b][c] * rad[b];
+}
+
+/* dipole_lab (PES-IDS/ai_ids_ch4_co2_lib.cpp:8-33): S1^T times the body-frame dipole */
+static void ch4co2_dipole_lab(const double *q, double out[3]) {
+    double qkal[5], dk[3], S1[3][3];
+    hho_ch4co2_lab_to_kal(q, qkal);
+    hho_ch4co2_dipole_kal(qkal, dk);
+    ch4co2_S1(q[3], q[4], q[5], S1);
+    mtv(S1, dk, out);
+}
+
+/* the stand-in surface (hh_ch4co2_standin.h) from the lab-frame site positions;
+ * with grad != NULL also dV/dq (8 lab coordinates) */
+static double ch4co2_V(const double *q, double *grad) {
+    double A[2][2], B[2][2];
+    hh_ch4co2_lj_pairs(A, B);
+    double rh[3], u2[3], S1[3][3];
+    ch4co2_axis(q[0], q[1], rh);
+    ch4co2_axis(q[6], q[7], u2);
+    ch4co2_S1(q[3], q[4], q[5], S1);
+    const double R = q[2], a = HH_CH4CO2_RCH / sqrt(3.0);
+    double x1[5][3], hb[5][3], x2[3][3];
+    for (int s = 0; s < 5; ++s) {
+        for (int i = 0; i < 3; ++i) hb[s][i] = s ? a * hh_ch4co2_hsign[s - 1][i] : 0.0;
+        mtv(S1, hb[s], x1[s]);
+    }
+    for (int i = 0; i < 3; ++i) {
+        x2[0][i] = R * rh[i];
+        x2[1][i] = R * rh[i] + HH_CH4CO2_RCO * u2[i];
+        x2[2][i] = R * rh[i] - HH_CH4CO2_RCO * u2[i];
+    }
+    double V = 0.0, g1[5][3], g2[3][3];
+    memset(g1, 0, sizeof g1);
+    memset(g2, 0, sizeof g2);
+    for (int s = 0; s < 5; ++s)
+        for (int t = 0; t < 3; ++t) {
+            double dx[3] = {x2[t][0] - x1[s][0], x2[t][1] - x1[s][1], x2[t][2] - x1[s][2]};
+            double i2 = 1.0 / (dx[0] * dx[0] + dx[1] * dx[1] + dx[2] * dx[2]);
+            double i6 = i2 * i2 * i2;
+            double Ap = A[s ? 1 : 0][t ? 1 : 0], Bp = B[s ? 1 : 0][t ? 1 : 0];
+            V += i6 * (Ap * i6 - Bp);
+            double f = -(12.0 * Ap * i6 - 6.0 * Bp) * i6 * i2;  /* (dV/dd) / d */
+            for (int i = 0; i < 3; ++i) {
+                g2[t][i] += f * dx[i];
+                g1[s][i] -= f * dx[i];
+            }
+        }
+    if (grad) {
+        double Gr[3], Gu[3];
+        for (int i = 0; i < 3; ++i) {
+            Gr[i] = g2[0][i] + g2[1][i] + g2[2][i];
+            Gu[i] = HH_CH4CO2_RCO * (g2[1][i] - g2[2][i]);
+        }
+        double sT = sin(q[1]), cT = cos(q[1]), sP = sin(q[0]), cP = cos(q[0]);
+        double r_Phi[3] = {sT * sP, -sT * cP, 0.0}, r_Th[3] = {-cT * cP, -cT * sP, -sT};
+        double s2 = sin(q[7]), c2 = cos(q[7]), sp2 = sin(q[6]), cp2 = cos(q[6]);
+        double u_phi[3] = {s2 * sp2, -s2 * cp2, 0.0}, u_th[3] = {-c2 * cp2, -c2 * sp2, -s2};
+        grad[0] = grad[1] = grad[2] = grad[6] = grad[7] = 0.0;
+        for (int i = 0; i < 3; ++i) {
+            grad[0] += Gr[i] * R * r_Phi[i];
+            grad[1] += Gr[i] * R * r_Th[i];
+            grad[2] += Gr[i] * rh[i];
+            grad[6] += Gu[i] * u_phi[i];
+            grad[7] += Gu[i] * u_th[i];
+        }
+        /* dS1/d(angle) = Spsi Sx Sz_dot(phi), Spsi Sx_dot Sz, Sz_dot(psi) Sx Sz */
+        double Zp[3][3], Xt[3][3], Zs[3][3], Zpd[3][3], Xtd[3][3], Zsd[3][3], D[3][3][3];
+        Sz(q[3], Zp); Sx(q[4], Xt); Sz(q[5], Zs);
+        Sz_dot(q[3], Zpd); Sx_dot(q[4], Xtd); Sz_dot(q[5], Zsd);
+        mm(Zs, Xt, D[0]); mm(D[0], Zpd, D[0]);
+        mm(Zs, Xtd, D[1]); mm(D[1], Zp, D[1]);
+        mm(Zsd, Xt, D[2]); mm(D[2], Zp, D[2]);
+        for (int k = 0; k < 3; ++k) {
+            double acc = 0.0;
+            for (int s = 1; s < 5; ++s) {
+                double dx[3];
+                mtv(D[k], hb[s], dx);
+                acc += g1[s][0] * dx[0] + g1[s][1] * dx[1] + g1[s][2] * dx[2];
+            }
+            grad[3 + k] = acc;
+        }
+    }
+    return V;
+}
+
+double hho_ch4co2_V_lab(const double *q) { return ch4co2_V(q, NULL); }
+
+/* ======================================================================== */
 /* N2-Ar PIP-NN surfaces.  PES: PES-IDS/ai_pes_n2_ar_pip_nn.cpp:8-146 with   */
 /* PES-IDS/mlp.hpp:178-256 (forward, backward) and the lab chain rule of     */
 /* examples/correlation_n2_ar.cpp:18-50.  Dipole: PES-IDS/ai_ids_n2_ar_pip_nn */
@@ -583,11 +785,14 @@ static int is_linear(const hho_system *sys) {
     return sys->system == HHO_SYS_CO2AR || sys->system == HHO_SYS_N2AR;
 }
 
-int hho_qp_size(const hho_system *sys) { return sys->system == HHO_SYS_HEAR ? 6 : 10; }
+int hho_qp_size(const hho_system *sys) {
+    return sys->system == HHO_SYS_HEAR ? 6 : (sys->system == HHO_SYS_CH4CO2 ? 16 : 10);
+}
 
 double hho_pes(const hho_system *sys, const double *q) {
     if (sys->system == HHO_SYS_HEAR) return hho_hear_V(q[2]);
     if (sys->system == HHO_SYS_N2AR) return hho_n2ar_V_lab(q);
+    if (sys->system == HHO_SYS_CH4CO2) return ch4co2_V(q, NULL);
     double qmol[5];
     hho_co2ar_lab_to_mol(q, qmol);
     return hho_co2ar_V_mol(qmol[0], qmol[4]);
@@ -600,6 +805,10 @@ void hho_dpes(const hho_system *sys, const double *q, double *dVdq) {
     }
     if (sys->system == HHO_SYS_N2AR) {
         n2ar_dpes_lab(q, dVdq);
+        return;
+    }
+    if (sys->system == HHO_SYS_CH4CO2) {
+        ch4co2_V(q, dVdq);
         return;
     }
     co2ar_dpes_lab(q, dVdq);
@@ -617,6 +826,10 @@ void hho_dipole(const hho_system *sys, const double *q, double d[3]) {
         n2ar_dipole_lab(q, d);
         return;
     }
+    if (sys->system == HHO_SYS_CH4CO2) {
+        ch4co2_dipole_lab(q, d);
+        return;
+    }
     co2ar_dipole_lab(q, d);
 }
 
@@ -629,8 +842,38 @@ static void extract_q(const hho_system *sys, const double *qp, double *q) {
     for (int k = 0; k < n; k += 2) q[k / 2] = qp[k];
 }
 
+/* rhsMonomer for ROTOR (src/hawaii.c:501-532) at y[0..5] = (phi pphi theta ptheta psi ppsi) */
+static void rotor_rhs(const double *II, const double *y, const double *dV, double *yd) {
+    double pPhi = y[1], theta = y[2], pTheta = y[3], psi = y[4], pPsi = y[5];
+    double sin_theta = sin(theta), cos_theta = cos(theta);
+    double sin_psi = sin(psi), cos_psi = cos(psi);
+    double t1 = (pPhi - pPsi * cos_theta) * sin_psi + pTheta * sin_theta * cos_psi;
+    double t2 = (pPhi - pPsi * cos_theta) * cos_psi - pTheta * sin_theta * sin_psi;
+    yd[0] = t1 * sin_psi / (II[0] * sin_theta * sin_theta) + t2 * cos_psi / (II[1] * sin_theta * sin_theta);
+    yd[1] = -dV[0];
+    yd[2] = t1 * cos_psi / (II[0] * sin_theta) - t2 * sin_psi / (II[1] * sin_theta);
+    double t3 = pPhi * cos_theta - pPsi;
+    double t4 = pPsi * cos_theta - pPhi;
+    yd[3] = -t3 * (t4 * (II[0] - II[1]) * cos_psi * cos_psi +
+                   pTheta * (II[0] - II[1]) * sin_theta * sin_psi * cos_psi + t4 * II[1]) /
+                (II[0] * II[1] * sin_theta * sin_theta * sin_theta) - dV[1];
+    yd[4] = -t1 * cos_theta * sin_psi / (II[0] * sin_theta * sin_theta) -
+            t2 * cos_theta * cos_psi / (II[1] * sin_theta * sin_theta) + pPsi / II[2];
+    yd[5] = -t1 * t2 / (II[0] * sin_theta * sin_theta) + t1 * t2 / (II[1] * sin_theta * sin_theta) - dV[2];
+}
+
+/* rhsMonomer for LINEAR_MOLECULE (src/hawaii.c:481-494) at y[0..3] */
+static void linear_rhs(double I, const double *y, const double *dV, double *yd) {
+    double pphi = y[1], th = y[2], pth = y[3];
+    double s = sin(th), c = cos(th);
+    yd[0] = pphi / I / s / s;
+    yd[1] = -dV[0];
+    yd[2] = pth / I;
+    yd[3] = pphi * pphi * c / I / s / s / s - dV[1];
+}
+
 void hho_rhs(const hho_system *sys, const double *y, double *yd) {
-    double q[5], dV[5];
+    double q[8], dV[8];
     extract_q(sys, y, q);
     hho_dpes(sys, q, dV);
     double mu = sys->mu;
@@ -644,15 +887,28 @@ void hho_rhs(const hho_system *sys, const double *y, double *yd) {
     yd[1] = -dV[0];
     yd[2] = pTheta / (mu * R2);
     yd[3] = pPhi * pPhi * cT / (mu * R2 * sT3) - dV[1];
-    if (is_linear(sys)) {
-        double I = sys->II;
-        double pphi = y[7], th = y[8], pth = y[9];
-        double s = sin(th), c = cos(th);
-        yd[6] = pphi / I / s / s;
-        yd[7] = -dV[3];
-        yd[8] = pth / I;
-        yd[9] = pphi * pphi * c / I / s / s / s - dV[4];
+    if (is_linear(sys)) linear_rhs(sys->II, y + 6, dV + 3, yd + 6);
+    if (sys->system == HHO_SYS_CH4CO2) {
+        rotor_rhs(sys->II1, y + 6, dV + 3, yd + 6);
+        linear_rhs(sys->II, y + 12, dV + 6, yd + 12);
     }
+}
+
+/* kinetic energy of a ROTOR (src/hawaii.c:1090-1110) at qp[0..5] */
+static double rotor_kinetic(const double *II, const double *qp) {
+    double pphi = qp[1], theta = qp[2], ptheta = qp[3], psi = qp[4], ppsi = qp[5];
+    double sin_theta = sin(theta), cos_theta = cos(theta), sin_psi = sin(psi), cos_psi = cos(psi);
+    double a = (pphi - ppsi * cos_theta) * sin_psi + ptheta * sin_theta * cos_psi;
+    double b = (pphi - ppsi * cos_theta) * cos_psi - ptheta * sin_theta * sin_psi;
+    return a * a / (2.0 * II[0] * sin_theta * sin_theta) + b * b / (2.0 * II[1] * sin_theta * sin_theta) +
+           ppsi * ppsi / (2.0 * II[2]);
+}
+
+/* kinetic energy of a LINEAR_MOLECULE (src/hawaii.c:1076-1084) at qp[0..3] */
+static double linear_kinetic(double I, const double *qp) {
+    double pphi = qp[1], th = qp[2], pth = qp[3];
+    double s = sin(th);
+    return pth * pth / (2.0 * I) + pphi * pphi / (2.0 * I * s * s);
 }
 
 double hho_kinetic(const hho_system *sys, const double *qp) {
@@ -661,22 +917,74 @@ double hho_kinetic(const hho_system *sys, const double *qp) {
     double sT = sin(Theta);
     double K = pR * pR / (2.0 * mu) + pTheta * pTheta / (2.0 * mu * R * R) +
                pPhi * pPhi / (2.0 * mu * R * R * sT * sT);
-    if (is_linear(sys)) {
-        double I = sys->II, pphi = qp[7], th = qp[8], pth = qp[9];
-        double s = sin(th);
-        K += pth * pth / (2.0 * I) + pphi * pphi / (2.0 * I * s * s);
-    }
+    if (is_linear(sys)) K += linear_kinetic(sys->II, qp + 6);
+    if (sys->system == HHO_SYS_CH4CO2) K += rotor_kinetic(sys->II1, qp + 6) + linear_kinetic(sys->II, qp + 12);
     return K;
 }
 
 double hho_hamiltonian(const hho_system *sys, const double *qp) {
-    double q[5];
+    double q[8];
     extract_q(sys, qp, q);
     double V = hho_pes(sys, q);
     return hho_kinetic(sys, qp) + V;
 }
 
+static void quat_mul(const double a[4], const double b[4], double o[4]) {
+    double t[4] = {a[0] * b[0] - a[1] * b[1] - a[2] * b[2] - a[3] * b[3],
+                   a[0] * b[1] + a[1] * b[0] + a[2] * b[3] - a[3] * b[2],
+                   a[0] * b[2] - a[1] * b[3] + a[2] * b[0] + a[3] * b[1],
+                   a[0] * b[3] + a[1] * b[2] - a[2] * b[1] + a[3] * b[0]};
+    memcpy(o, t, sizeof t);
+}
+
+/* CH4-CO2 in the reference's lab frame: r = R (-sin T cos P, -sin T sin P, cos T),
+ * p the Cartesian momentum of (R, THETA, PHI); the CH4 orientation as the unit
+ * quaternion of S1^T = Sz(phi1)^T Sx(theta1)^T Sz(psi1)^T (body -> lab), its lab
+ * angular momentum S1^T L_body with L_body = (t1 / sin theta, t2 / sin theta, ppsi)
+ * of the rotor's kinetic energy (src/hawaii.c:1090-1110); the CO2 axis u and
+ * j = u x p_u */
+static void ch4co2_qp_to_cart(const hho_system *sys, const double *qp, double *cart) {
+    (void)sys;
+    double Phi = qp[0], pPhi = qp[1], Th = qp[2], pTh = qp[3], R = qp[4], pR = qp[5];
+    double sT = sin(Th), cT = cos(Th), sP = sin(Phi), cP = cos(Phi);
+    double rh[3] = {-sT * cP, -sT * sP, cT};
+    double eT[3] = {-cT * cP, -cT * sP, -sT};
+    double eP[3] = {sP, -cP, 0.0};
+    for (int i = 0; i < 3; ++i) {
+        cart[i] = R * rh[i];
+        cart[3 + i] = pR * rh[i] + pTh / R * eT[i] + pPhi / (R * sT) * eP[i];
+    }
+    double phi = qp[6], pphi = qp[7], th = qp[8], pth = qp[9], psi = qp[10], ppsi = qp[11];
+    double qa[4] = {cos(0.5 * phi), 0, 0, sin(0.5 * phi)};
+    double qb[4] = {cos(0.5 * th), sin(0.5 * th), 0, 0};
+    double qc[4] = {cos(0.5 * psi), 0, 0, sin(0.5 * psi)};
+    double qq[4];
+    quat_mul(qa, qb, qq);
+    quat_mul(qq, qc, cart + 6);
+    double st = sin(th), ct = cos(th), sp = sin(psi), cp = cos(psi);
+    double Lb[3] = {((pphi - ppsi * ct) * sp + pth * st * cp) / st,
+                    ((pphi - ppsi * ct) * cp - pth * st * sp) / st, ppsi};
+    double S1[3][3];
+    ch4co2_S1(phi, th, psi, S1);
+    mtv(S1, Lb, cart + 13);
+    double ph2 = qp[12], pph2 = qp[13], th2 = qp[14], pth2 = qp[15];
+    double s2 = sin(th2), c2 = cos(th2), sp2 = sin(ph2), cp2 = cos(ph2);
+    double u[3] = {-s2 * cp2, -s2 * sp2, c2};
+    double u_th[3] = {-c2 * cp2, -c2 * sp2, -s2};
+    double u_ph[3] = {s2 * sp2, -s2 * cp2, 0.0};
+    double pu[3];
+    for (int i = 0; i < 3; ++i) pu[i] = pth2 * u_th[i] + pph2 / (s2 * s2) * u_ph[i];
+    for (int i = 0; i < 3; ++i) cart[10 + i] = u[i];
+    cart[16] = u[1] * pu[2] - u[2] * pu[1];
+    cart[17] = u[2] * pu[0] - u[0] * pu[2];
+    cart[18] = u[0] * pu[1] - u[1] * pu[0];
+}
+
 void hho_qp_to_cart(const hho_system *sys, const double *qp, double *cart) {
+    if (sys->system == HHO_SYS_CH4CO2) {
+        ch4co2_qp_to_cart(sys, qp, cart);
+        return;
+    }
     double Phi = qp[0], pPhi = qp[1], Th = qp[2], pTh = qp[3], R = qp[4], pR = qp[5];
     double sT = sin(Th), cT = cos(Th), sP = sin(Phi), cP = cos(Phi);
     double Rh[3] = {sT * cP, sT * sP, cT};
@@ -728,6 +1036,14 @@ int hho_candidate(hho_mt *s, const hho_system *sys, const hho_params *p, double 
         qp[8] = acos(2.0 * hho_mt_drand(s) - 1.0);
         *draws += 2;
     }
+    if (sys->system == HHO_SYS_CH4CO2) {  /* ROTOR, then LINEAR_MOLECULE (hawaii.c:1260-1290) */
+        qp[6] = hho_mt_drand(s) * 2.0 * M_PI;
+        qp[8] = acos(2.0 * hho_mt_drand(s) - 1.0);
+        qp[10] = hho_mt_drand(s) * 2.0 * M_PI;
+        qp[12] = hho_mt_drand(s) * 2.0 * M_PI;
+        qp[14] = acos(2.0 * hho_mt_drand(s) - 1.0);
+        *draws += 5;
+    }
     /* p_generator */
     double sqrt_MUKT = sqrt(sys->mu / HkT * T);
     double sinTheta = sin(qp[2]);
@@ -744,6 +1060,24 @@ int hho_candidate(hho_mt *s, const hho_system *sys, const hho_params *p, double 
         qp[7] = sqrt_IIKT * sin_theta * x1;
         qp[9] = sqrt_IIKT * x0;
     }
+    if (sys->system == HHO_SYS_CH4CO2) {
+        /* p_generator_rotor (hawaii.c:1305-1327) */
+        double sIx = sqrt(sys->II1[0] / HkT * T), sIy = sqrt(sys->II1[1] / HkT * T), sIz = sqrt(sys->II1[2] / HkT * T);
+        double st = sin(qp[8]), ct = cos(qp[8]), sp = sin(qp[10]), cp = cos(qp[10]);
+        double x0 = generate_normal(s, draws);
+        double x1 = generate_normal(s, draws);
+        double x2 = generate_normal(s, draws);
+        qp[7] = sIx * st * sp * x0 + sIy * st * cp * x1 + sIz * ct * x2;
+        qp[9] = sIx * cp * x0 - sIy * sp * x1;
+        qp[11] = sIz * x2;
+        /* p_generator_linear_molecule (hawaii.c:1292-1303) */
+        double sqrt_IIKT = sqrt(sys->II / HkT * T);
+        double sin_theta = sin(qp[14]);
+        double y0 = generate_normal(s, draws);
+        double y1 = generate_normal(s, draws);
+        qp[13] = sqrt_IIKT * sin_theta * y1;
+        qp[15] = sqrt_IIKT * y0;
+    }
     /* Hamiltonian, then reject() */
     double E = hho_hamiltonian(sys, qp);
     double u = hho_mt_drand(s);
@@ -751,7 +1085,7 @@ int hho_candidate(hho_mt *s, const hho_system *sys, const hho_params *p, double 
     double Mval = exp(-p->pesmin * HkT / T);
     double M = 1.5 * Mval;
     double kin = hho_kinetic(sys, qp);
-    double q[5];
+    double q[8];
     extract_q(sys, qp, q);
     double pot = hho_pes(sys, q);
     double proposal = exp(-kin * HkT / T);
@@ -771,7 +1105,7 @@ long hho_sample(uint32_t seed, const hho_system *sys, const hho_params *p, doubl
     int QP = hho_qp_size(sys);
     long cand = 0;
     size_t got = 0;
-    double qp[10], E;
+    double qp[16], E;
     int draws;
     while (got < n) {
         ++cand;
@@ -787,7 +1121,7 @@ long hho_sample(uint32_t seed, const hho_system *sys, const hho_params *p, doubl
 /* DOP853 with dense output (Hairer-Norsett-Wanner); step control and        */
 /* initial step as in the standard published algorithm.                      */
 /* ======================================================================== */
-#define NMAX 10
+#define NMAX 16
 
 typedef struct {
     const hho_system *sys;
@@ -945,7 +1279,7 @@ static int half_traj(const hho_system *sys, const hho_params *p, const double *y
             if (!dense) { dop853_dense(&I, y, y_new, ht, K, F); dense = 1; }
             double x = ((double)k * dt - t) / ht;
             dense_eval(n, y, F, x, ys);
-            double q[5], d[3];
+            double q[8], d[3];
             extract_q(sys, ys, q);
             hho_dipole(sys, q, d);
             st->nsamples++;
@@ -979,7 +1313,7 @@ int hho_correlation_eval(const hho_system *sys, const hho_params *p, const doubl
     double *fw = calloc(N, sizeof(double)), *bw = calloc(N, sizeof(double));
     memset(crln, 0, N * sizeof(double));
     memset(st, 0, sizeof *st);
-    double q[5], mu0[3];
+    double q[8], mu0[3];
     extract_q(sys, qp0, q);
     hho_dipole(sys, q, mu0);
     fw[0] = bw[0] = mu0[0] * mu0[0] + mu0[1] * mu0[1] + mu0[2] * mu0[2];
@@ -1007,7 +1341,7 @@ int hho_correlation_parts(const hho_system *sys, const hho_params *p, const doub
     memset(fw, 0, N * sizeof(double));
     memset(bw, 0, N * sizeof(double));
     memset(st, 0, sizeof *st);
-    double q[5], mu0[3];
+    double q[8], mu0[3];
     extract_q(sys, qp0, q);
     hho_dipole(sys, q, mu0);
     fw[0] = bw[0] = mu0[0] * mu0[0] + mu0[1] * mu0[1] + mu0[2] * mu0[2];
@@ -1232,6 +1566,7 @@ static void *m0_worker(void *arg) {
 int hho_m0(const hho_system *sys, const hho_params *p, const double *T, int nT,
            uint64_t n_samples, uint64_t seed, uint64_t offset, int nthreads,
            double *wsum, double *wsq) {
+    if (sys->system == HHO_SYS_CH4CO2) return -1;  /* no CH4-CO2 moment integrand */
     if (nT > 64 || nT < 1) return -1;
     if (nthreads < 1) nthreads = 1;
     if (nthreads > 256) nthreads = 256;

@@ -27,7 +27,7 @@
 extern "C" {
 #endif
 
-enum { HHO_SYS_HEAR = 0, HHO_SYS_CO2AR = 1, HHO_SYS_N2AR = 2 };
+enum { HHO_SYS_HEAR = 0, HHO_SYS_CO2AR = 1, HHO_SYS_N2AR = 2, HHO_SYS_CH4CO2 = 3 };
 enum { HHO_PS_FREE_AND_METASTABLE = 1, HHO_PS_BOUND = 2, HHO_PS_ALL = 3 };
 
 /* per-half-trajectory status codes (same numbering as the CUDA library) */
@@ -43,7 +43,8 @@ enum {
 typedef struct {
     int system;      /* HHO_SYS_* */
     double mu;       /* reduced mass, a.u. */
-    double II;       /* moment of inertia of the linear monomer, a.u. (CO2-Ar, N2-Ar) */
+    double II;       /* moment of inertia of the linear monomer, a.u. (CO2-Ar, N2-Ar; CO2 of CH4-CO2) */
+    double II1[3];   /* principal moments of the rotor (CH4 of CH4-CO2), a.u. */
 } hho_system;
 
 typedef struct {
@@ -98,8 +99,14 @@ void hho_dipole(const hho_system *sys, const double *q, double d[3]);
 void hho_rhs(const hho_system *sys, const double *y, double *dydt);
 double hho_kinetic(const hho_system *sys, const double *qp);
 double hho_hamiltonian(const hho_system *sys, const double *qp);
-/* spherical phase point -> Cartesian (r, p[, u, j]) */
+/* spherical phase point -> Cartesian (r, p[, u, j]); CH4-CO2: (r, p, quaternion of
+ * the CH4 body -> lab rotation, u_CO2, L_CH4, j_CO2), 19 values */
 void hho_qp_to_cart(const hho_system *sys, const double *qp, double *cart);
+/* CH4-CO2: lab coordinates -> (R, PHI1K, THETA1K, PHI2K, THETA2K) (src/angles_handler.cpp:357-419),
+ * the body-frame dipole (PES-IDS/ai_ids_ch4_co2.cpp:672-1067) and the stand-in potential */
+void hho_ch4co2_lab_to_kal(const double *qlab, double *qkal);
+void hho_ch4co2_dipole_kal(const double *qkal, double d[3]);
+double hho_ch4co2_V_lab(const double *q);
 
 /* ---- sampler (hawaii.c:1206-1421, 2976-2994) ---- */
 /* draws one candidate; returns 1 when accepted (reject + pair-state filter);

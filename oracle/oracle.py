@@ -13,7 +13,7 @@ import numpy as np
 HERE = os.path.dirname(os.path.abspath(__file__))
 REF_DIR = os.path.join(HERE, "_ref")
 
-SYS_HEAR, SYS_CO2AR, SYS_N2AR = 0, 1, 2
+SYS_HEAR, SYS_CO2AR, SYS_N2AR, SYS_CH4CO2 = 0, 1, 2, 3
 PS_FREE_AND_METASTABLE, PS_BOUND, PS_ALL = 1, 2, 3
 
 _dp = np.ctypeslib.ndpointer(dtype=np.float64, flags="C_CONTIGUOUS")
@@ -21,7 +21,7 @@ _u32p = np.ctypeslib.ndpointer(dtype=np.uint32, flags="C_CONTIGUOUS")
 
 
 class System(C.Structure):
-    _fields_ = [("system", C.c_int), ("mu", C.c_double), ("II", C.c_double)]
+    _fields_ = [("system", C.c_int), ("mu", C.c_double), ("II", C.c_double), ("II1", C.c_double * 3)]
 
 
 class Params(C.Structure):
@@ -103,12 +103,20 @@ def lib():
         L.hho_array_weights.argtypes = [C.c_int, C.c_double, C.c_double, _dp, C.c_int, C.c_double, _dp]
         L.hho_correlation_sum_array.argtypes = [C.POINTER(System), C.POINTER(Params), _dp, C.c_size_t, C.c_int,
                                                 _dp, C.c_int, _dp]
+        L.hho_ch4co2_lab_to_kal.argtypes = [_dp, _dp]
+        L.hho_ch4co2_dipole_kal.argtypes = [_dp, _dp]
+        L.hho_ch4co2_V_lab.restype = C.c_double
+        L.hho_ch4co2_V_lab.argtypes = [_dp]
         _lib = L
     return _lib
 
 
 def qp_size(system: int) -> int:
-    return 6 if system == SYS_HEAR else 10
+    return {SYS_HEAR: 6, SYS_CH4CO2: 16}.get(system, 10)
+
+
+def q_size(system: int) -> int:
+    return qp_size(system) // 2
 
 
 def mt_stream(seed: int, n: int) -> np.ndarray:
@@ -192,7 +200,7 @@ def m0_scale(params):
 
 def qp_to_cart(sysd, qp):
     qp = np.ascontiguousarray(qp, dtype=np.float64)
-    out = np.empty(6 if sysd.system == SYS_HEAR else 12)
+    out = np.empty({SYS_HEAR: 6, SYS_CH4CO2: 19}.get(sysd.system, 12))
     lib().hho_qp_to_cart(C.byref(sysd), qp, out)
     return out
 
@@ -202,7 +210,7 @@ def pes(sysd, q):
 
 
 def dpes(sysd, q):
-    out = np.zeros(5)
+    out = np.zeros(max(5, q_size(sysd.system)))
     lib().hho_dpes(C.byref(sysd), np.ascontiguousarray(q, dtype=np.float64), out)
     return out
 
@@ -241,6 +249,18 @@ def correlation_sum_array(sysd, params, qp0, w, nthreads=None):
     lib().hho_correlation_sum_array(C.byref(sysd), C.byref(params), qp0.ravel(), qp0.shape[0],
                                     nthreads or os.cpu_count(), w.ravel(), n_sat, out)
     return out.reshape(n_sat, params.N)
+
+
+def ch4co2_lab_to_kal(q):
+    out = np.zeros(5)
+    lib().hho_ch4co2_lab_to_kal(np.ascontiguousarray(q, dtype=np.float64), out)
+    return out
+
+
+def ch4co2_dipole_kal(qkal):
+    out = np.zeros(3)
+    lib().hho_ch4co2_dipole_kal(np.ascontiguousarray(qkal, dtype=np.float64), out)
+    return out
 
 
 def n2ar_energy_cm(d):
@@ -295,6 +315,10 @@ def ref(name):
             L.dpes_co2ar.argtypes = [C.c_double, C.c_double, C.POINTER(C.c_double), C.POINTER(C.c_double)]
         elif name == "co2ar_ids":
             L.ref_co2ar_dip_mol.argtypes = [C.c_double, C.c_double, _dp]
+        elif name == "ch4co2_ids":
+            for f in ("ref_ch4co2_dipole_vector", "ref_ch4co2_lab_to_kal", "ref_ch4co2_dipole_lab"):
+                getattr(L, f).argtypes = [_dp, _dp]
+            L.ref_ch4co2_init()
         elif name == "n2ar_pip":
             L.ref_n2ar_pes_pip.argtypes = [_dp, _dp]
             L.ref_n2ar_pes_jac.argtypes = [_dp, _dp]

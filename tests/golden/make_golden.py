@@ -82,6 +82,36 @@ def make_ref_surfaces():
     print("wrote", out, os.path.getsize(out), "bytes")
 
 
+def make_ch4co2_dipole():
+    """tests/golden/ref_ch4co2_dipole.npz: the reference's CH4-CO2 dipole chain compiled in
+    oracle/_ref (PES-IDS/ai_ids_ch4_co2.cpp, PES-IDS/ai_ids_ch4_co2_lib.cpp,
+    src/angles_handler.cpp) at seeded lab-frame points (PHI THETA R PHI1 THETA1 PSI1 PHI2 THETA2):
+    the molecular-frame coordinates, the body-frame dipole and the lab-frame dipole."""
+    root = os.path.dirname(os.path.dirname(os.path.dirname(os.path.abspath(__file__))))
+    sys.path.insert(0, root)
+    from oracle import oracle as O
+    O.build()
+    L = O.ref("ch4co2_ids")
+    rng = np.random.default_rng(4096)
+    n = 600
+    R = np.concatenate([rng.uniform(4.0, 45.0, n - 8), [4.75, 5.0, 9.5, 10.0, 25.0, 29.999, 30.0, 40.0]])
+    q = np.column_stack([rng.uniform(0, 2 * np.pi, n), np.arccos(rng.uniform(-1, 1, n)), R,
+                         rng.uniform(0, 2 * np.pi, n), np.arccos(rng.uniform(-1, 1, n)),
+                         rng.uniform(0, 2 * np.pi, n), rng.uniform(0, 2 * np.pi, n),
+                         np.arccos(rng.uniform(-1, 1, n))])
+    kal = np.zeros((n, 5))
+    dk = np.zeros((n, 3))
+    dl = np.zeros((n, 3))
+    for i in range(n):
+        L.ref_ch4co2_lab_to_kal(np.ascontiguousarray(q[i]), kal[i])
+        L.ref_ch4co2_dipole_vector(np.ascontiguousarray(kal[i]), dk[i])
+        L.ref_ch4co2_dipole_lab(np.ascontiguousarray(q[i]), dl[i])
+    out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "ref_ch4co2_dipole.npz")
+    np.savez_compressed(out, q=q, kal=kal, dip_kal=dk, dip_lab=dl)
+    print("wrote", out, os.path.getsize(out), "bytes")
+
+
 if __name__ == "__main__":
     main()
     make_ref_surfaces()
+    make_ch4co2_dipole()

@@ -13,6 +13,11 @@ MU_N2AR = 30016.287464295514
 II_N2 = 55141.90310147907
 PESMIN_N2AR = -97.3 / 2.1947463136320e5
 RMIN_N2AR = 4.51
+# CH4-CO2 (example_configs/CF-F-CH4-CO2.conf:6,25,27-28,50,55)
+MU_CH4CO2 = 2.141790360592430e+04
+II_CH4 = 2.093840965876434e+04
+PESMIN_CH4CO2 = -1.562522273622102e-03
+RMIN_CH4CO2 = 4.751
 
 
 def oracle_system(name):
@@ -20,15 +25,19 @@ def oracle_system(name):
         return O.System(O.SYS_HEAR, MU_HEAR, 0.0)
     if name == "n2ar":
         return O.System(O.SYS_N2AR, MU_N2AR, II_N2)
+    if name == "ch4co2":
+        return O.System(O.SYS_CH4CO2, MU_CH4CO2, II_CO2, (II_CH4, II_CH4, II_CH4))
     return O.System(O.SYS_CO2AR, MU_CO2AR, II_CO2)
 
 
 def _pesmin(name):
-    return {"hear": PESMIN_HEAR, "co2ar": PESMIN_CO2AR, "n2ar": PESMIN_N2AR}[name]
+    return {"hear": PESMIN_HEAR, "co2ar": PESMIN_CO2AR, "n2ar": PESMIN_N2AR, "ch4co2": PESMIN_CH4CO2}[name]
 
 
 def _rmin(name, Rmin):
-    return RMIN_N2AR if (name == "n2ar" and Rmin is None) else (4.0 if Rmin is None else Rmin)
+    if Rmin is not None:
+        return Rmin
+    return {"n2ar": RMIN_N2AR, "ch4co2": RMIN_CH4CO2}.get(name, 4.0)
 
 
 def oracle_params(name, N, dt, tol=1e-12, ps=O.PS_FREE_AND_METASTABLE, Rmin=None, Rmax=40.0, Rcut=40.0,
