@@ -39,6 +39,11 @@ WORKLOAD = dict(system="co2ar", n_traj=102400, T=300.0, seed=7, N=32768, dt=100.
 # N2-Ar PIP-NN workload (rigid N2 + Ar, PES-IDS/ai_pes_n2_ar_pip_nn.cpp surfaces)
 N2AR = dict(n_traj=262144, T=200.0, seed=7, N=16384, dt=100.0, Rmin=4.51, Rmax=40.0, Rcut=40.0,
             pesmin=-97.3 / 2.1947463136320e5, mu=30016.287464295514, II=55141.90310147907, fp64_tol=1e-12)
+# CH4-CO2 rotor + linear molecule (example_configs/CF-F-CH4-CO2.conf: dt 200 a.u., 21 samples,
+# R in [4.751, 40]); four temperature sets in one launch; stand-in PES, reference dipole
+CH4CO2 = dict(n_per_T=262144, Ts=(100.0, 200.0, 300.0, 400.0), seed=2066497031, N=21, dt=200.0, Rmin=4.751,
+              Rmax=40.0, Rcut=40.0, pesmin=-1.562522273622102e-03, mu=2.141790360592430e+04,
+              II1=2.093840965876434e+04, II2=2.819827114123505e+05, fp64_tol=1e-12)
 METRIC = "traj/s/GPU, batched mixed-precision vs FP64 plain, at C(t) rel err ≤1e-4"
 PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "traffic.json")
@@ -59,6 +64,8 @@ def parse():
     ap.add_argument("--cpu-sample", type=int, default=4096)
     ap.add_argument("--no-n2ar", action="store_true", help="skip the N2-Ar PIP-NN workload")
     ap.add_argument("--n2ar-trajectories", type=int, default=N2AR["n_traj"])
+    ap.add_argument("--no-ch4co2", action="store_true", help="skip the CH4-CO2 four-temperature workload")
+    ap.add_argument("--ch4co2-per-T", type=int, default=CH4CO2["n_per_T"])
     return ap.parse_args()
 
 
@@ -98,6 +105,50 @@ def bench_n2ar(args, hh, H):
         out["accuracy"] = {"m0_rel_err": float(d[0]), "ct_err_t_le_1e5au": float(d[:kc].max()),
                            "fp64_horizon_k": kh, "ct_err_within_fp64_horizon": float(d[:max(kh, 1)].max()),
                            "ct_err_all": float(d.max()), "fp64_floor_all": float(floor.max())}
+    return out
+
+
+def bench_ch4co2(args, hh, H):
+    """CH4-CO2: 4 x n_per_T trajectories (one set per temperature) in one call, mixed
+    (FP32 PES, stages and batched dipole; FP64 state and C(t)) against the FP64 path on
+    the same initial conditions."""
+    w = CH4CO2
+    n = args.ch4co2_per_T
+    ms = hh.init_ms(w["mu"], hh.ROTOR, hh.LINEAR_MOLECULE, (w["II1"],) * 3, (w["II2"], w["II2"]), w["seed"])
+
+    def params(tol=w["fp64_tol"]):
+        return H.CalcParams(ps=hh.PAIR_STATE_FREE_AND_METASTABLE, sampler_Rmin=w["Rmin"], sampler_Rmax=w["Rmax"],
+                            pesmin=w["pesmin"], sampling_time=w["dt"], MaxTrajectoryLength=w["N"],
+                            cvode_tolerance=tol, Rcut=w["Rcut"], partial_partition_function_ratio=1.0,
+                            mixed_tolerance=args.mixed_tol)
+
+    def run(prec, tol=w["fp64_tol"]):
+        return hh.correlation_temperatures(ms, params(tol), w["Ts"], n, prec, seed=w["seed"])
+
+    run(hh.PRECISION_MIXED)   # grows the device buffers to the timed size
+    cm, _, sm = run(hh.PRECISION_MIXED)
+    run(hh.PRECISION_FP64)
+    cp, _, sp = run(hh.PRECISION_FP64)
+    tot = len(w["Ts"]) * n
+    sm, sp = sm.as_dict(), sp.as_dict()
+    mixed = tot / (sm["total_ms"] / 1e3)
+    plain = tot / (sp["total_ms"] / 1e3)
+    out = {"workload": f"CH4-CO2 rotor + linear molecule, {len(w['Ts'])} x {n} trajectories at T = "
+                       f"{'/'.join(str(int(t)) for t in w['Ts'])} K in one call, {w['N']} samples at dt {w['dt']} a.u., "
+                       f"R in [{w['Rmin']}, {w['Rmax']}]; stand-in site-site PES (the reference has no source for "
+                       "its CH4-CO2 PES), reference dipole",
+           "mixed_traj_per_s": mixed, "plain_fp64_traj_per_s": plain, "speedup_mixed_vs_plain": mixed / plain,
+           "mixed_ms": sm["total_ms"], "plain_ms": sp["total_ms"], "mixed_rtol": args.mixed_tol,
+           "fp64_rtol": w["fp64_tol"], "kernel_launches": sm["n_kernel_launches"],
+           "stats_mixed": {k: sm[k] for k in ("n_candidates", "n_steps", "n_rhs", "n_samples", "n_failed",
+                                              "sample_ms", "traj_ms")}}
+    if not args.no_accuracy:
+        per_T = []
+        for i in range(len(w["Ts"])):
+            c0 = abs(cp[i][0])
+            d = np.abs(cm[i] - cp[i]) / c0
+            per_T.append({"T": w["Ts"][i], "m0_rel_err": float(d[0]), "ct_err_all": float(d.max())})
+        out["accuracy"] = per_T
     return out
 
 
@@ -353,6 +404,9 @@ def main():
     n2ar = None
     if rank == 0 and ws == 1 and not args.no_n2ar:
         n2ar = bench_n2ar(args, hh, H)
+    ch4co2 = None
+    if rank == 0 and ws == 1 and not args.no_ch4co2:
+        ch4co2 = bench_ch4co2(args, hh, H)
 
     if rank == 0:
         h2d = C.sizeof(_lib.CalcParamsC) + 8 + 4 + 8 + 4
@@ -372,6 +426,7 @@ def main():
                         "d2h_bytes_per_step": d2h},
                 "gpu_launches": launches, "clocks": ck, "roofline": roof, "cpu_baseline": cpu,
                 "n2ar_pip_nn": n2ar,
+                "ch4co2_four_temperatures": ch4co2,
                 "stats_last_step": {k: last[k] for k in ("n_candidates", "n_steps", "n_rejected_steps", "n_rhs",
                                                          "n_samples", "n_dense", "n_failed", "sample_ms",
                                                          "traj_ms")}}

@@ -6,12 +6,12 @@ include/hh_cuda.h); `hawaii` mirrors the reference's host interface on top of it
 from . import _lib
 from ._lib import HHError
 from .hawaii import (ATOM, LINEAR_MOLECULE, PAIR_STATE_ALL, PAIR_STATE_BOUND,
-                     PAIR_STATE_FREE_AND_METASTABLE, PRECISION_FP64, PRECISION_MIXED,
-                     SYSTEM_CO2_AR, SYSTEM_HE_AR, SYSTEM_N2_AR, CalcParams, CFnc, CFncArray, MoleculeSystem,
+                     PAIR_STATE_FREE_AND_METASTABLE, PRECISION_FP64, PRECISION_MIXED, ROTOR,
+                     SYSTEM_CH4_CO2, SYSTEM_CO2_AR, SYSTEM_HE_AR, SYSTEM_N2_AR, CalcParams, CFnc, CFncArray, MoleculeSystem,
                      SFnc, analytic_full_partition_function_by_V, calculate_correlation_and_save,
                      calculate_correlation_array_and_save, correlation_array_iteration,
                      calculate_m0, correlation_from_initial_conditions, correlation_iteration,
-                     correlation_iterations,
+                     correlation_iterations, correlation_temperatures,
                      idct_cf_to_sf, init_ms, read_correlation_function, read_spectral_function,
                      sample_initial_conditions, write_correlation_function,
                      write_spectral_function)

@@ -27,12 +27,14 @@ HH_M0_NOALLOC_MAX_T = 256
 
 HH_MONOMER_ATOM = 0
 HH_MONOMER_LINEAR_MOLECULE = 4
+HH_MONOMER_ROTOR = 6
 HH_PAIR_STATE_FREE_AND_METASTABLE = 1
 HH_PAIR_STATE_BOUND = 2
 HH_PAIR_STATE_ALL = 3
 HH_SYSTEM_HE_AR = 1
 HH_SYSTEM_CO2_AR = 2
 HH_SYSTEM_N2_AR = 3
+HH_SYSTEM_CH4_CO2 = 4
 HH_PRECISION_FP64 = 0
 HH_PRECISION_MIXED = 1
 
@@ -41,7 +43,7 @@ EXPORTS = (
     "hh_cuda_init", "hh_cuda_seed", "hh_cuda_sample", "hh_cuda_correlation", "hh_cuda_correlation_multi",
     "hh_cuda_correlation_ic", "hh_cuda_m0", "hh_cuda_idct_cf_to_sf", "hh_cuda_strerror",
     "hh_cuda_mt_stream", "hh_cuda_debug_inject", "hh_cuda_debug_item_trace", "hh_cuda_fma_peak",
-    "hh_cuda_shutdown", "hh_cuda_m0_noalloc", "hh_cuda_correlation_array",
+    "hh_cuda_shutdown", "hh_cuda_m0_noalloc", "hh_cuda_correlation_array", "hh_cuda_correlation_temperatures",
 )
 
 
@@ -106,6 +108,8 @@ def load(path: str | None = None):
                                       C.c_int, _dp, C.POINTER(C.c_double), C.POINTER(Stats)]
     L.hh_cuda_correlation_multi.argtypes = [C.POINTER(CalcParamsC), C.c_double, C.c_uint32, C.c_uint64,
                                             C.c_uint32, C.c_int, _dp, _dp, C.POINTER(Stats)]
+    L.hh_cuda_correlation_temperatures.argtypes = [C.POINTER(CalcParamsC), _dp, C.c_int, C.c_uint32, C.c_uint64,
+                                                   C.c_int, _dp, _dp, C.POINTER(Stats)]
     L.hh_cuda_correlation_ic.argtypes = [C.POINTER(CalcParamsC), _dp, C.c_uint64, C.c_int, _dp,
                                          C.POINTER(Stats)]
     L.hh_cuda_m0.argtypes = [C.POINTER(CalcParamsC), _dp, C.c_int, C.c_uint64, C.c_uint64, C.c_int,

@@ -23,7 +23,7 @@ UNITS = [
     ("hh_sampler.cu", ["-fmad=false"]),
 ]
 # host-only units (the host compiler sees the generated tables as plain arrays)
-HOST_UNITS = ["hh_n2ar_host.cpp"]
+HOST_UNITS = ["hh_n2ar_host.cpp", "hh_ch4co2_host.cpp"]
 CXX = os.environ.get("CXX", "g++")
 
 

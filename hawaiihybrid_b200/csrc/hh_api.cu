@@ -10,6 +10,8 @@
 #include <vector>
 
 #include "../../include/hh_cuda.h"
+#include "hh_ch4co2_dip.cuh"
+#include "hh_ch4co2_fold.h"
 #include "hh_co2ar_tables.h"
 #include "hh_consts.h"
 #include "hh_fft.cuh"
@@ -87,6 +89,14 @@ struct Ctx {
   N2arDipFold *d_n2ar_fold = nullptr;  // N2-Ar dipole models, folded (hh_n2ar_fold.h)
   N2arPesNet<double> *d_n2ar_pes_d = nullptr;  // N2-Ar PES network, FP64 and FP32
   N2arPesNet<float> *d_n2ar_pes_f = nullptr;
+  // CH4-CO2: rotor moments, stand-in surface constants, folded dipole table
+  SamplerExtra sx{};
+  double2 *d_ch4_cd = nullptr;
+  float4 *d_ch4_cf = nullptr;
+  unsigned char *d_ch4_y2 = nullptr;
+  unsigned int *d_ch4_grp = nullptr;
+  unsigned short *d_ch4_gcount = nullptr;
+  int ch4_E = 0, ch4_G = 0;
   // MT19937 stream
   uint32_t *d_mt = nullptr;
   DevBuf<uint32_t> words[2];
@@ -107,6 +117,12 @@ struct Ctx {
   DevBuf<uint4> trace;
   // CORRELATION_ARRAY weights [n][n_sat]: with ratios (C(t)) and without (nstar)
   DevBuf<double> sat_w, sat_wraw;
+  // CH4-CO2 record path: sample records, their dipoles, the piece sort
+  DevBuf<unsigned char> rec, rec_mu;
+  DevBuf<int> rec_len, rec_status, rec_sorted;
+  DevBuf<unsigned int> seg_cnt;
+  DevBuf<long long> seg_w0;
+  DevBuf<unsigned long long> rec_nfail;
   // M0
   DevBuf<double> m0_partials, m0_out;
   // FFT, and the CUDA graph of its kernel sequence for the current (N, dt, buffers)
@@ -251,7 +267,7 @@ int sample_into(const hh_calc_params *p, double T, uint64_t n, double *d_out, ui
     CK(launch_candidates(g.sys, g.mu, g.II, T, p->sampler_Rmin, p->sampler_Rmax, p->pesmin,
                          p->pair_state, g.d_tab, g.words[g.cur].p, g.wvalid, g.wpos - g.wbase, g.D,
                          ncand, g.accept.p, g.consumed.p, g.qp_cand.p, g.energy.p, g.scal.p,
-                         g.st));
+                         g.sx, g.st));
     g_launches += 1;
     unsigned long long first_irr = 0;
     CK(cudaMemcpyAsync(&first_irr, g.scal.p, sizeof first_irr, cudaMemcpyDeviceToHost, g.st));
@@ -336,6 +352,117 @@ int run_traj_dispatch(int precision, const TrajParams &P, const TrajIO &io) {
   return launch_traj<SYS_CO2AR, double, double, false>(P, io, nullptr);
 }
 
+// device memory the CH4-CO2 record path may hold for one chunk of trajectories
+constexpr size_t CH4_RECORD_BUDGET = size_t(24) << 30;
+
+// CH4-CO2: the trajectory kernel writes every sample as a record, then the
+// records are sorted by radial piece, their dipoles evaluated in batches and
+// C(t) accumulated with the reference's per-sample tests (hh_ch4co2_dip.cuh).
+// Trajectories go through in chunks whose records fit CH4_RECORD_BUDGET.
+template <typename PHYS>
+int run_records_t(const TrajParams &P, const double *d_ic, uint64_t n, uint64_t per_iter,
+                  int precision, const double *d_satw, int n_sat, unsigned long long *cnt_dev) {
+  const int N = P.N;
+  const int stride = 2 * N - 1;
+  const size_t rec_b = HH_REC_WORDS * sizeof(PHYS), mu_b = 4 * sizeof(PHYS);
+  const size_t per_traj = (size_t)stride * (rec_b + mu_b + sizeof(int)) + 4 * sizeof(int);
+  uint64_t chunk = std::max<uint64_t>(1, CH4_RECORD_BUDGET / per_traj);
+  chunk = std::min<uint64_t>(chunk, (uint64_t)((INT32_MAX - 32 * CH4_NSEG) / stride));
+  chunk = std::min<uint64_t>(chunk, n);
+  const size_t slots = (size_t)chunk * stride;
+  CK(g.rec.ensure(slots * rec_b));
+  CK(g.rec_mu.ensure(slots * mu_b));
+  CK(g.rec_sorted.ensure(slots + 32 * CH4_NSEG));
+  CK(g.rec_len.ensure(2 * chunk));
+  CK(g.rec_status.ensure(2 * chunk));
+  CK(g.seg_cnt.ensure(2 * CH4_NSEG));
+  CK(g.seg_w0.ensure(CH4_NSEG + 1));
+  CK(g.rec_nfail.ensure(1));
+  CK(cudaMemsetAsync(g.rec_nfail.p, 0, sizeof(unsigned long long), g.st));
+  Ch4Co2Fold fold;
+  fold.n_entry = g.ch4_E;
+  fold.n_group = g.ch4_G;
+  fold.cf = g.d_ch4_cf;
+  fold.cd = g.d_ch4_cd;
+  fold.y2 = g.d_ch4_y2;
+  fold.grp = g.d_ch4_grp;
+  fold.gcount = g.d_ch4_gcount;
+  for (int i = 0; i < CH4_NSEG - 1; ++i) fold.seg_hi[i] = hh_ch4co2_seg_hi[i];
+  for (int i = 0; i < CH4_NSEG; ++i) fold.centre[i] = hh_ch4co2_centre[i];
+  auto dip = ch4_dipole_kernel<PHYS>;
+  const size_t dsmem = (size_t)CH4_DIP_WARPS * CH4_NY2 * 32 * sizeof(PHYS);
+  if (dsmem > 48 * 1024) CK(cudaFuncSetAttribute(dip, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsmem));
+  int dper = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&dper, dip, 32 * CH4_DIP_WARPS, dsmem));
+  const int dgrid = std::max(1, dper) * g.num_sms;
+  for (uint64_t base = 0; base < n; base += chunk) {
+    const uint64_t nc = std::min<uint64_t>(chunk, n - base);
+    CK(cudaMemsetAsync(g.queue.p, 0, sizeof(unsigned int), g.st));
+    CK(cudaMemsetAsync(g.seg_cnt.p, 0, 2 * CH4_NSEG * sizeof(unsigned int), g.st));
+    CK(cudaMemsetAsync(g.rec_sorted.p, 0xff, (nc * stride + 32 * CH4_NSEG) * sizeof(int), g.st));
+    TrajIO io;
+    memset(&io, 0, sizeof io);
+    io.ic = d_ic + base * g.QP;
+    io.n_items = (int)(2 * nc);
+    io.queue = g.queue.p;
+    io.crln = g.crln.p;
+    io.counters = cnt_dev;
+    io.status_hist = g.status_hist.p;
+    io.traj_per_iter = (long long)per_iter;
+    io.records = g.rec.p;
+    io.rec_stride = stride;
+    io.rec_len = g.rec_len.p;
+    io.rec_status = g.rec_status.p;
+    for (int k = 0; k < 3; ++k) io.inv_I1[k] = 1.0 / g.sx.II1[k];
+    io.lj = g.sx.lj;
+    int rc = (precision == HH_PRECISION_MIXED) ? launch_traj<SYS_CH4CO2, float, float, false>(P, io, nullptr)
+                                               : launch_traj<SYS_CH4CO2, double, double, false>(P, io, nullptr);
+    if (rc) return rc;
+    Ch4SortArgs sa;
+    sa.records = g.rec.p;
+    sa.rec_len = g.rec_len.p;
+    sa.n_traj = (long long)nc;
+    sa.stride = stride;
+    sa.N = N;
+    sa.count = g.seg_cnt.p;
+    sa.cursor = g.seg_cnt.p + CH4_NSEG;
+    sa.warp0 = g.seg_w0.p;
+    sa.sorted = g.rec_sorted.p;
+    for (int i = 0; i < CH4_NSEG - 1; ++i) sa.seg_hi[i] = hh_ch4co2_seg_hi[i];
+    const long long nslots = (long long)nc * stride;
+    const int sgrid = (int)std::min<long long>((nslots + 255) / 256, 8LL * g.num_sms);
+    ch4_seg_count_kernel<PHYS><<<sgrid, 256, 0, g.st>>>(sa);
+    ch4_seg_scan_kernel<<<1, 32, 0, g.st>>>(sa);
+    ch4_seg_scatter_kernel<PHYS><<<sgrid, 256, 0, g.st>>>(sa);
+    CK(cudaGetLastError());
+    Ch4DipArgs da;
+    da.f = fold;
+    da.records = g.rec.p;
+    da.sorted = g.rec_sorted.p;
+    da.warp0 = g.seg_w0.p;
+    da.mu = g.rec_mu.p;
+    dip<<<dgrid, 32 * CH4_DIP_WARPS, dsmem, g.st>>>(da);
+    CK(cudaGetLastError());
+    Ch4CorrArgs ca;
+    ca.mu = g.rec_mu.p;
+    ca.rec_len = g.rec_len.p;
+    ca.rec_status = g.rec_status.p;
+    ca.n_traj = (long long)nc;
+    ca.traj_base = (long long)base;
+    ca.traj_per_iter = (long long)per_iter;
+    ca.stride = stride;
+    ca.crln = g.crln.p;
+    ca.sat_w = d_satw;
+    ca.n_sat = n_sat;
+    ca.status_hist = g.status_hist.p;
+    ca.n_failed = g.rec_nfail.p;
+    ch4_corr_kernel<PHYS><<<(unsigned)((nc + 255) / 256), 256, 0, g.st>>>(P, ca);
+    CK(cudaGetLastError());
+    g_launches += 5;
+  }
+  return HH_OK;
+}
+
 // integrate both branches of n trajectories whose phase points are in d_ic;
 // trajectories [i*per_iter, (i+1)*per_iter) accumulate into C(t) slice i
 int run_trajectories(const hh_calc_params *p, const double *d_ic, uint64_t n, uint64_t per_iter,
@@ -399,9 +526,19 @@ int run_trajectories(const hh_calc_params *p, const double *d_ic, uint64_t n, ui
     io.item_trace = g.trace.p;
   }
   CK(cudaEventRecord(g.ev[2], g.st));
+  int nfail = 0;
+  if (g.sys == SYS_CH4CO2) {
+    int rc = (precision == HH_PRECISION_MIXED)
+                 ? run_records_t<float>(P, d_ic, n, per_iter, precision, d_satw, n_sat, g.counters.p)
+                 : run_records_t<double>(P, d_ic, n, per_iter, precision, d_satw, n_sat, g.counters.p);
+    if (rc) return rc;
+    unsigned long long nf = 0;
+    CK(cudaMemcpyAsync(&nf, g.rec_nfail.p, sizeof nf, cudaMemcpyDeviceToHost, g.st));
+    CK(cudaStreamSynchronize(g.st));
+    nfail = (int)nf;
+  } else {
   int rc = run_traj_dispatch(precision, P, io);
   if (rc) return rc;
-  int nfail = 0;
   CK(cudaMemcpyAsync(&nfail, g.fail_count.p, sizeof nfail, cudaMemcpyDeviceToHost, g.st));
   CK(cudaStreamSynchronize(g.st));
   if (nfail > 0) {
@@ -427,6 +564,7 @@ int run_trajectories(const hh_calc_params *p, const double *d_ic, uint64_t n, ui
     io2.item_trace = nullptr;
     rc = run_traj_dispatch(precision, P2, io2);
     if (rc) return rc;
+  }
   }
   CK(cudaEventRecord(g.ev[3], g.st));
   CK(cudaMemcpyAsync(crln_host, g.crln.p, N * n_iter * sizeof(double), cudaMemcpyDeviceToHost, g.st));
@@ -550,6 +688,12 @@ int hh_cuda_init(int device, const hh_system_desc *sys) {
     if (sys->monomer1_type != HH_MONOMER_LINEAR_MOLECULE || sys->monomer2_type != HH_MONOMER_ATOM)
       return HH_E_UNSUPPORTED_SYSTEM;
     if (!(sys->II1[0] > 0) || sys->II1[0] != sys->II1[1]) return HH_E_INVALID_ARGUMENT;
+  } else if (sid == HH_SYSTEM_CH4_CO2) {
+    if (sys->monomer1_type != HH_MONOMER_ROTOR || sys->monomer2_type != HH_MONOMER_LINEAR_MOLECULE)
+      return HH_E_UNSUPPORTED_SYSTEM;
+    if (!(sys->II1[0] > 0) || !(sys->II1[1] > 0) || !(sys->II1[2] > 0) || !(sys->II2[0] > 0) ||
+        sys->II2[0] != sys->II2[1])
+      return HH_E_INVALID_ARGUMENT;
   } else {
     return HH_E_UNSUPPORTED_SYSTEM;
   }
@@ -586,11 +730,42 @@ int hh_cuda_init(int device, const hh_system_desc *sys) {
     CK(cudaMemcpy(g.d_n2ar_pes_d, &pes_d, sizeof pes_d, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(g.d_n2ar_pes_f, &pes_f, sizeof pes_f, cudaMemcpyHostToDevice));
   }
-  g.sys = (sid == HH_SYSTEM_HE_AR) ? SYS_HEAR : (sid == HH_SYSTEM_N2_AR) ? SYS_N2AR : SYS_CO2AR;
+  if (sid == HH_SYSTEM_CH4_CO2 && !g.d_ch4_cd) {
+    Ch4Co2FoldHost f;
+    if (ch4co2_build_fold(&f) != 0) return HH_E_UNSUPPORTED_SYSTEM;
+    const size_t E = (size_t)f.n_entry;
+    std::vector<float4> cf(HH_CH4CO2_NSEG * E);
+    for (size_t i = 0; i < cf.size(); ++i)
+      cf[i] = make_float4((float)f.coef[4 * i], (float)f.coef[4 * i + 1], (float)f.coef[4 * i + 2],
+                          (float)f.coef[4 * i + 3]);
+    CK(cudaMalloc(&g.d_ch4_cd, f.coef.size() * sizeof(double)));
+    CK(cudaMalloc(&g.d_ch4_cf, cf.size() * sizeof(float4)));
+    CK(cudaMalloc(&g.d_ch4_y2, E));
+    CK(cudaMalloc(&g.d_ch4_grp, f.grp.size() * sizeof(unsigned int)));
+    CK(cudaMalloc(&g.d_ch4_gcount, f.gcount.size() * sizeof(unsigned short)));
+    CK(cudaMemcpy(g.d_ch4_cd, f.coef.data(), f.coef.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(g.d_ch4_cf, cf.data(), cf.size() * sizeof(float4), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(g.d_ch4_y2, f.y2.data(), E, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(g.d_ch4_grp, f.grp.data(), f.grp.size() * sizeof(unsigned int), cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(g.d_ch4_gcount, f.gcount.data(), f.gcount.size() * sizeof(unsigned short),
+                  cudaMemcpyHostToDevice));
+    g.ch4_E = f.n_entry;
+    g.ch4_G = f.n_group;
+  }
+  g.sys = (sid == HH_SYSTEM_HE_AR)    ? SYS_HEAR
+          : (sid == HH_SYSTEM_N2_AR)  ? SYS_N2AR
+          : (sid == HH_SYSTEM_CH4_CO2) ? SYS_CH4CO2
+                                      : SYS_CO2AR;
   g.mu = sys->mu;
-  g.II = (sid == HH_SYSTEM_HE_AR) ? 0.0 : sys->II1[0];
-  g.QP = (sid == HH_SYSTEM_HE_AR) ? 6 : 10;
-  g.D = (sid == HH_SYSTEM_HE_AR) ? 10 : 16;
+  // the linear monomer's moment: monomer 1, or CO2 as monomer 2 of CH4-CO2
+  g.II = (sid == HH_SYSTEM_HE_AR) ? 0.0 : (sid == HH_SYSTEM_CH4_CO2 ? sys->II2[0] : sys->II1[0]);
+  g.QP = (sid == HH_SYSTEM_HE_AR) ? 6 : (sid == HH_SYSTEM_CH4_CO2 ? 16 : 10);
+  g.D = (sid == HH_SYSTEM_HE_AR) ? 10 : (sid == HH_SYSTEM_CH4_CO2 ? 25 : 16);
+  memset(&g.sx, 0, sizeof g.sx);
+  if (sid == HH_SYSTEM_CH4_CO2) {
+    for (int k = 0; k < 3; ++k) g.sx.II1[k] = sys->II1[k];
+    hh_ch4co2_lj_pairs(g.sx.lj.A, g.sx.lj.B);
+  }
   g.p_accept = 0.25;
   return HH_OK;
 }
@@ -669,6 +844,56 @@ int hh_cuda_correlation_multi(const hh_calc_params *p, double T, uint32_t seed,
   return HH_OK;
 }
 
+int hh_cuda_correlation_temperatures(const hh_calc_params *p, const double *T, int nT, uint32_t seed,
+                                     uint64_t n_per_T, int precision_mode, double *crln_sums,
+                                     double *ntraj, hh_stats *stats) {
+  if (!g.init) return HH_E_NOT_INITIALIZED;
+  int rc = check_params(p);
+  if (rc) return rc;
+  if (!T || nT < 1 || !crln_sums || n_per_T == 0 || n_per_T * (uint64_t)nT > (uint64_t)(INT32_MAX / 2))
+    return HH_E_INVALID_ARGUMENT;
+  for (int i = 0; i < nT; ++i)
+    if (!(T[i] > 0)) return HH_E_INVALID_ARGUMENT;
+  if (precision_mode != HH_PRECISION_FP64 && precision_mode != HH_PRECISION_MIXED)
+    return HH_E_INVALID_ARGUMENT;
+  CK(cudaSetDevice(g.device));
+  if (seed > 0) {
+    rc = reseed(seed);
+    if (rc) return rc;
+  }
+  hh_stats local;
+  memset(&local, 0, sizeof local);
+  g_launches = 0;
+  const uint64_t n = n_per_T * (uint64_t)nT;
+  CK(g.qp0.ensure(n * g.QP));
+  CK(cudaEventRecord(g.ev[0], g.st));
+  const long long wpos0 = g.wpos;
+  uint64_t ncand = 0;
+  for (int i = 0; i < nT; ++i) {
+    uint64_t nc = 0;
+    rc = sample_into(p, T[i], n_per_T, g.qp0.p + (size_t)i * n_per_T * g.QP, &nc);
+    if (rc) return rc;
+    ncand += nc;
+  }
+  CK(cudaEventRecord(g.ev[1], g.st));
+  rc = pregen_words(g.wpos - wpos0);
+  if (rc) return rc;
+  rc = run_trajectories(p, g.qp0.p, n, n_per_T, precision_mode, crln_sums, &local);
+  if (rc) return rc;
+  float ms = 0.f;
+  CK(cudaEventElapsedTime(&ms, g.ev[0], g.ev[1]));
+  local.sample_ms = ms;
+  CK(cudaEventElapsedTime(&ms, g.ev[0], g.ev[3]));
+  local.total_ms = ms;
+  local.n_candidates = ncand;
+  local.n_accepted = n;
+  local.n_kernel_launches = g_launches;
+  if (ntraj)
+    for (int i = 0; i < nT; ++i) ntraj[i] = (double)n_per_T;
+  if (stats) *stats = local;
+  return HH_OK;
+}
+
 int hh_cuda_correlation_array(const hh_calc_params *p, double base_T, const double *sat_T,
                               const double *ppf_ratios, int n_sat, uint32_t seed, uint64_t n_accept,
                               int precision_mode, double *crln_sums, double *nstar, double *ntraj,
@@ -705,7 +930,7 @@ int hh_cuda_correlation_array(const hh_calc_params *p, double base_T, const doub
   rc = pregen_words(g.wpos - wpos0);
   if (rc) return rc;
   CK(launch_sat_weights(g.sys, g.mu, g.II, p->pesmin, p->pair_state, g.d_tab, g.qp0.p, (long long)n_accept,
-                        base_T, sat_T, ppf_ratios, n_sat, g.sat_w.p, g.sat_wraw.p, g.st));
+                        base_T, sat_T, ppf_ratios, n_sat, g.sat_w.p, g.sat_wraw.p, g.sx, g.st));
   g_launches += 1;
   CK(cudaEventRecord(g.ev[1], g.st));
   hh_calc_params p1 = *p;
@@ -765,6 +990,7 @@ int hh_cuda_correlation_ic(const hh_calc_params *p, const double *qp0, uint64_t 
 int hh_cuda_m0(const hh_calc_params *p, const double *T, int nT, uint64_t n_samples,
                uint64_t seed, int precision_mode, double *m, double *err) {
   if (!g.init) return HH_E_NOT_INITIALIZED;
+  if (g.sys == SYS_CH4CO2) return HH_E_UNSUPPORTED_SYSTEM;  // no CH4-CO2 moment integrand
   if (!p || !T || nT < 1 || !m || n_samples == 0) return HH_E_INVALID_ARGUMENT;
   if (!(p->sampler_Rmin > 0) || !(p->sampler_Rmax > p->sampler_Rmin)) return HH_E_INVALID_ARGUMENT;
   if (p->pair_state < 1 || p->pair_state > 3) return HH_E_INVALID_ARGUMENT;
@@ -934,6 +1160,7 @@ int hh_cuda_fma_peak(int precision, double *tflops) {
 int hh_cuda_m0_noalloc(const hh_calc_params *p, const double *T, int nT, uint64_t n_samples,
                        uint64_t seed, int precision_mode, double *m, double *err) {
   if (!g.init) return HH_E_NOT_INITIALIZED;
+  if (g.sys == SYS_CH4CO2) return HH_E_UNSUPPORTED_SYSTEM;
   if (!p || !T || nT < 1 || !m || n_samples == 0) return HH_E_INVALID_ARGUMENT;
   if (nT > HH_M0_NOALLOC_MAX_T) return HH_E_SCRATCH_LIMIT;
   if (!(p->sampler_Rmin > 0) || !(p->sampler_Rmax > p->sampler_Rmin)) return HH_E_INVALID_ARGUMENT;
@@ -1007,6 +1234,14 @@ void hh_cuda_shutdown(void) {
   g.trace.release();
   g.sat_w.release();
   g.sat_wraw.release();
+  g.rec.release();
+  g.rec_mu.release();
+  g.rec_len.release();
+  g.rec_status.release();
+  g.rec_sorted.release();
+  g.seg_cnt.release();
+  g.seg_w0.release();
+  g.rec_nfail.release();
   g.m0_partials.release();
   g.m0_out.release();
   g.f_cf.release();
@@ -1019,6 +1254,11 @@ void hh_cuda_shutdown(void) {
   if (g.d_n2ar_fold) cudaFree(g.d_n2ar_fold);
   if (g.d_n2ar_pes_d) cudaFree(g.d_n2ar_pes_d);
   if (g.d_n2ar_pes_f) cudaFree(g.d_n2ar_pes_f);
+  if (g.d_ch4_cd) cudaFree(g.d_ch4_cd);
+  if (g.d_ch4_cf) cudaFree(g.d_ch4_cf);
+  if (g.d_ch4_y2) cudaFree(g.d_ch4_y2);
+  if (g.d_ch4_grp) cudaFree(g.d_ch4_grp);
+  if (g.d_ch4_gcount) cudaFree(g.d_ch4_gcount);
   if (g.d_mt) cudaFree(g.d_mt);
   for (auto &e : g.ev)
     if (e) cudaEventDestroy(e);

@@ -1,0 +1,372 @@
+// Batched CH4-CO2 dipole and the correlation step of the record path.
+//
+// The induced dipole of PES-IDS/ai_ids_ch4_co2.cpp:672-1067 is, per Cartesian
+// component c of the CH4 body frame,
+//   mu_c = sum_e  Y1_e(n1) Y2_e(n2) K_e(R)
+// over 8,661 entries e = (c, Y1, Y2) (hh_ch4co2_host.cpp folds the 320 radial
+// functions of each entry into one piecewise cubic on their common grid of 30
+// pieces).  n1 and n2 are the directions of the intermolecular axis and of the
+// CO2 axis in the CH4 body frame; Y1 (l <= 13) and Y2 (even l <= 12) are real
+// spherical harmonics with the Legendre normalisation sqrt((l-m)!/(l+m)!) (the
+// table carries the inverse factor), computed from the unit vectors by the
+// three-term recurrence in l and (x + i y)^m, without angles.
+//
+// Inside a trajectory kernel the 32 lanes of a warp sit at different R, so each
+// coefficient load would be a 32-way gather over pieces.  Instead the trajectory
+// kernel writes each sample as a record and:
+//   1. seg_count / seg_scan / seg_scatter sort the valid records by radial piece,
+//      each piece padded to a multiple of 32, so every warp task has one piece;
+//   2. dipole_kernel: a warp evaluates 32 records of one piece; the coefficient
+//      stream of that piece is the same for all lanes (broadcast loads), Y2 sits
+//      per lane in shared memory, Y1 is generated in the order of the stream;
+//   3. corr_kernel applies the reference's per-sample tests in order (NaN dipole,
+//      |C| > 1e100, |C_k / C_k-1| > 1e10: src/hawaii.c:2183-2243) and adds
+//      w mu0.mu(t_k) of every trajectory that passes into C(t).
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "hh_ch4co2_tables.h"
+#include "hh_traj.cuh"
+
+namespace hh {
+
+constexpr int CH4_NSEG = HH_CH4CO2_NSEG;
+constexpr int CH4_L1 = HH_CH4CO2_L1MAX;
+constexpr int CH4_L2 = HH_CH4CO2_L2MAX;
+constexpr int CH4_NY2 = 91;  // even l2 <= 12, all m2 and cos/sin
+constexpr int CH4_DIP_WARPS = 4;
+
+// folded dipole table in device memory (built by ch4co2_build_fold)
+struct Ch4Co2Fold {
+  int n_entry, n_group;
+  const float4 *cf;             // [NSEG][n_entry] (c0, c1, c2, c3), FP32
+  const double2 *cd;            // [NSEG][n_entry][2] (c0, c1), (c2, c3), FP64
+  const unsigned char *y2;      // [n_entry] index of Y2 in the per-lane array
+  const unsigned int *grp;      // [n_group] cs | comp << 1 | entries << 3
+  const unsigned short *gcount; // [(l, m) in m-major order] groups at that Y1
+  double seg_hi[CH4_NSEG - 1];
+  double centre[CH4_NSEG];
+};
+
+struct Ch4SortArgs {
+  const void *records;
+  const int *rec_len;
+  long long n_traj;           // trajectories of this chunk
+  int stride, N;
+  unsigned int *count;        // [NSEG]
+  unsigned int *cursor;       // [NSEG]
+  long long *warp0;           // [NSEG + 1] first warp task of each piece; [NSEG] = total
+  int *sorted;                // record index per task slot, -1 for padding
+  double seg_hi[CH4_NSEG - 1];
+};
+
+template <typename PHYS> __device__ __forceinline__ int ch4_seg(const double *hi, PHYS R) {
+  int s = 0;
+#pragma unroll 1
+  while (s < CH4_NSEG - 1 && double(R) >= hi[s]) ++s;
+  return s;
+}
+
+// slot sl of trajectory t holds a stored sample
+__device__ __forceinline__ bool ch4_valid(const int *rec_len, long long t, int sl, int N) {
+  if (sl == 0) return true;
+  if (sl < N) return sl <= rec_len[2 * t];
+  return sl - (N - 1) <= rec_len[2 * t + 1];
+}
+
+template <typename PHYS> __device__ __forceinline__ PHYS ch4_rec_R(const void *records, long long i) {
+  const PHYS *r = static_cast<const PHYS *>(records) + i * HH_REC_WORDS;
+  return sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+}
+
+template <typename PHYS>
+__global__ void __launch_bounds__(256) ch4_seg_count_kernel(Ch4SortArgs a) {
+  __shared__ unsigned int h[CH4_NSEG];
+  for (int i = threadIdx.x; i < CH4_NSEG; i += blockDim.x) h[i] = 0;
+  __syncthreads();
+  const long long n = a.n_traj * a.stride;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long t = i / a.stride;
+    const int sl = (int)(i - t * a.stride);
+    if (ch4_valid(a.rec_len, t, sl, a.N)) atomicAdd(&h[ch4_seg(a.seg_hi, ch4_rec_R<PHYS>(a.records, i))], 1u);
+  }
+  __syncthreads();
+  for (int i = threadIdx.x; i < CH4_NSEG; i += blockDim.x)
+    if (h[i]) atomicAdd(&a.count[i], h[i]);
+}
+
+// one warp: piece offsets in warp tasks, cursors reset
+__global__ void ch4_seg_scan_kernel(Ch4SortArgs a) {
+  if (threadIdx.x == 0) {
+    long long w = 0;
+    for (int s = 0; s < CH4_NSEG; ++s) {
+      a.warp0[s] = w;
+      w += (a.count[s] + 31) / 32;
+      a.cursor[s] = 0;
+    }
+    a.warp0[CH4_NSEG] = w;
+  }
+}
+
+template <typename PHYS>
+__global__ void __launch_bounds__(256) ch4_seg_scatter_kernel(Ch4SortArgs a) {
+  const long long n = a.n_traj * a.stride;
+  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
+       i += (long long)gridDim.x * blockDim.x) {
+    const long long t = i / a.stride;
+    const int sl = (int)(i - t * a.stride);
+    if (!ch4_valid(a.rec_len, t, sl, a.N)) continue;
+    const int s = ch4_seg(a.seg_hi, ch4_rec_R<PHYS>(a.records, i));
+    const unsigned pos = atomicAdd(&a.cursor[s], 1u);
+    a.sorted[a.warp0[s] * 32 + pos] = (int)i;
+  }
+}
+
+struct Ch4DipArgs {
+  Ch4Co2Fold f;
+  const void *records;
+  const int *sorted;
+  const long long *warp0;
+  void *mu;                   // [record][4] lab-frame dipole in the surface precision
+};
+
+// Y2 of the CO2 axis n2 in the CH4 frame: even l <= 12, in the order
+// m = 0..12, l = m..12 (even), cos then sin
+template <typename T>
+__device__ __forceinline__ void ch4_y2(T x, T y, T z, T *Y, int lane) {
+  T C = T(1), S = T(0), pm = T(1);
+  int idx = 0;
+#pragma unroll 1
+  for (int m = 0; m <= CH4_L2; ++m) {
+    if (m > 0) {
+      const T c = C * x - S * y;
+      S = C * y + S * x;
+      C = c;
+      pm = -pm * sqrt(T(2 * m - 1) / T(2 * m));
+    }
+    T qa = T(1), qb = T(0);
+#pragma unroll 1
+    for (int l = m; l <= CH4_L2; ++l) {
+      T q;
+      if (l == m) q = T(1);
+      else if (l == m + 1) q = sqrt(T(2 * m + 1)) * z;
+      else q = (T(2 * l - 1) * z * qa - sqrt(T((l - 1) * (l - 1) - m * m)) * qb) / sqrt(T(l * l - m * m));
+      if ((l & 1) == 0) {
+        Y[(idx++) * 32 + lane] = pm * C * q;
+        if (m > 0) Y[(idx++) * 32 + lane] = pm * S * q;
+      }
+      qb = qa;
+      qa = q;
+    }
+  }
+}
+
+template <typename PHYS>
+__global__ void __launch_bounds__(32 * CH4_DIP_WARPS) ch4_dipole_kernel(Ch4DipArgs a) {
+  extern __shared__ __align__(16) unsigned char smem_raw[];
+  __shared__ long long w0[CH4_NSEG + 1];
+  for (int i = threadIdx.x; i <= CH4_NSEG; i += blockDim.x) w0[i] = a.warp0[i];
+  __syncthreads();
+  const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+  PHYS *Y2 = reinterpret_cast<PHYS *>(smem_raw) + (size_t)warp * CH4_NY2 * 32;
+  const long long total = w0[CH4_NSEG];
+  const long long nw = (long long)gridDim.x * CH4_DIP_WARPS;
+  for (long long w = (long long)blockIdx.x * CH4_DIP_WARPS + warp; w < total; w += nw) {
+    int seg = 0;
+    while (seg < CH4_NSEG - 1 && w0[seg + 1] <= w) ++seg;
+    const int mine = a.sorted[w * 32 + lane];
+    // padding lanes evaluate lane 0's record (always valid) and store nothing; the
+    // shuffle runs in every lane
+    const int first = __shfl_sync(0xffffffffu, mine, 0);
+    const int src = mine >= 0 ? mine : first;
+    const PHYS *rec = static_cast<const PHYS *>(a.records) + (size_t)src * HH_REC_WORDS;
+    const PHYS r[3] = {rec[0], rec[1], rec[2]};
+    const PHYS qt[4] = {rec[3], rec[4], rec[5], rec[6]};
+    const PHYS u[3] = {rec[7], rec[8], rec[9]};
+    PHYS M[3][3];
+    quat_matrix<PHYS>(qt, M);
+    const PHYS R = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+    const PHYS iR = PHYS(1) / R;
+    const PHYS iu = PHYS(1) / sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    // body-frame directions n = M^T v
+    PHYS n1[3], n2[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+      n1[k] = (M[0][k] * r[0] + M[1][k] * r[1] + M[2][k] * r[2]) * iR;
+      n2[k] = (M[0][k] * u[0] + M[1][k] * u[1] + M[2][k] * u[2]) * iu;
+    }
+    ch4_y2<PHYS>(n2[0], n2[1], n2[2], Y2, lane);
+    __syncwarp();
+    const PHYS x = R - PHYS(a.f.centre[seg]);
+    const float4 *cf = a.f.cf + (size_t)seg * a.f.n_entry;
+    const double2 *cd = a.f.cd + (size_t)seg * a.f.n_entry * 2;
+    PHYS acc0 = PHYS(0), acc1 = PHYS(0), acc2 = PHYS(0);
+    PHYS C = PHYS(1), S = PHYS(0), pm = PHYS(1);
+    int g = 0, e = 0, lm = 0;
+    const PHYS z1 = n1[2];
+#pragma unroll 1
+    for (int m = 0; m <= CH4_L1; ++m) {
+      if (m > 0) {
+        const PHYS c = C * n1[0] - S * n1[1];
+        S = C * n1[1] + S * n1[0];
+        C = c;
+        pm = -pm * sqrt(PHYS(2 * m - 1) / PHYS(2 * m));
+      }
+      PHYS qa = PHYS(1), qb = PHYS(0);
+#pragma unroll 1
+      for (int l = m; l <= CH4_L1; ++l, ++lm) {
+        PHYS q;
+        if (l == m) q = PHYS(1);
+        else if (l == m + 1) q = sqrt(PHYS(2 * m + 1)) * z1;
+        else q = (PHYS(2 * l - 1) * z1 * qa - sqrt(PHYS((l - 1) * (l - 1) - m * m)) * qb) / sqrt(PHYS(l * l - m * m));
+        qb = qa;
+        qa = q;
+        const PHYS Yc = pm * C * q, Ys = pm * S * q;
+        const int ng = __ldg(&a.f.gcount[lm]);
+#pragma unroll 1
+        for (int gg = 0; gg < ng; ++gg, ++g) {
+          const unsigned d = __ldg(&a.f.grp[g]);
+          const int cnt = int(d >> 3);
+          PHYS s = PHYS(0);
+          if constexpr (sizeof(PHYS) == 4) {
+#pragma unroll 4
+            for (int i = 0; i < cnt; ++i) {
+              const float4 c4 = __ldg(&cf[e + i]);
+              const float v = c4.x + x * (c4.y + x * (c4.z + x * c4.w));
+              s += Y2[int(__ldg(&a.f.y2[e + i])) * 32 + lane] * v;
+            }
+          } else {
+#pragma unroll 2
+            for (int i = 0; i < cnt; ++i) {
+              const double2 lo = __ldg(&cd[2 * (e + i)]), hi = __ldg(&cd[2 * (e + i) + 1]);
+              const double v = lo.x + x * (lo.y + x * (hi.x + x * hi.y));
+              s += Y2[int(__ldg(&a.f.y2[e + i])) * 32 + lane] * v;
+            }
+          }
+          e += cnt;
+          const PHYS t = ((d & 1u) ? Ys : Yc) * s;
+          const unsigned comp = (d >> 1) & 3u;
+          if (comp == 0) acc0 += t;
+          else if (comp == 1) acc1 += t;
+          else acc2 += t;
+        }
+      }
+    }
+    if (seg == CH4_NSEG - 1) {
+      const PHYS i2 = iR * iR, i6 = i2 * i2 * i2;
+      acc0 *= i6;
+      acc1 *= i6;
+      acc2 *= i6;
+    }
+    if (mine >= 0) {
+      PHYS *o = static_cast<PHYS *>(a.mu) + (size_t)mine * 4;
+#pragma unroll
+      for (int i = 0; i < 3; ++i) o[i] = M[i][0] * acc0 + M[i][1] * acc1 + M[i][2] * acc2;
+    }
+    __syncwarp();
+  }
+}
+
+struct Ch4CorrArgs {
+  const void *mu;
+  const int *rec_len;
+  const int *rec_status;
+  long long n_traj;           // trajectories of this chunk
+  long long traj_base;        // index of the chunk's first trajectory
+  long long traj_per_iter;
+  int stride;
+  double *crln;
+  const double *sat_w;        // [traj][n_sat] (global trajectory index) or nullptr
+  int n_sat;
+  unsigned int *status_hist;
+  unsigned long long *n_failed;
+};
+
+template <typename PHYS>
+__device__ __forceinline__ PHYS ch4_val(const PHYS *mu, long long slot, const PHYS *m0) {
+  const PHYS *d = mu + slot * 4;
+  return m0[0] * d[0] + m0[1] * d[1] + m0[2] * d[2];
+}
+
+// one thread per trajectory of the chunk
+template <typename PHYS>
+__global__ void __launch_bounds__(256) ch4_corr_kernel(TrajParams P, Ch4CorrArgs a) {
+  const long long t = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  const bool live = t < a.n_traj;
+  const PHYS *mu = static_cast<const PHYS *>(a.mu);
+  const long long base = (live ? t : 0) * a.stride;
+  PHYS m0[3] = {PHYS(0), PHYS(0), PHYS(0)};
+  int len[2] = {0, 0};
+  bool failed = false;
+  if (live) {
+#pragma unroll
+    for (int c = 0; c < 3; ++c) m0[c] = mu[base * 4 + c];
+    for (int dir = 0; dir < 2; ++dir) {
+      const long long item = 2 * (a.traj_base + t) + dir;
+      int st = a.rec_status[2 * t + dir];
+      len[dir] = a.rec_len[2 * t + dir];
+      PHYS prev = PHYS(0);
+      for (int k = 1; k <= len[dir]; ++k) {
+        const long long slot = base + (dir ? P.N - 1 + k : k);
+        const PHYS *d = mu + slot * 4;
+        int code = -1;
+        const PHYS val = m0[0] * d[0] + m0[1] * d[1] + m0[2] * d[2];
+        if (isnan(d[0]) || isnan(d[1]) || isnan(d[2])) code = HH_ST_NAN_DIPOLE;
+        else if (item == P.inject_item && k == P.inject_k) code = P.inject_status;
+        else if (fabs(double(val)) > 1e100) code = HH_ST_OVERFLOW;
+        else if (k > 1 && fabs(double(val) / double(prev)) > 1e10) code = HH_ST_JUMP;
+        if (code >= 0) {
+          st = code;
+          if (code >= HH_ST_NAN_DIPOLE) failed = true;
+          len[dir] = k - 1;
+          break;
+        }
+        prev = val;
+      }
+      atomicAdd(&a.status_hist[st], 1u);
+    }
+    if (failed) atomicAdd(a.n_failed, 1ull);
+  }
+  const long long gt = a.traj_base + (live ? t : 0);
+  const long long slice = (a.n_sat > 0) ? 0 : gt / a.traj_per_iter;
+  const unsigned full = 0xffffffffu;
+  const bool uniform = __all_sync(full, __shfl_sync(full, slice, 0) == slice);
+  const bool add = live && !failed;
+  const int nsl = a.n_sat > 0 ? a.n_sat : 1;
+  for (int s = 0; s < nsl; ++s) {
+    const double ws = P.weight * (a.n_sat > 0 ? (add ? a.sat_w[gt * a.n_sat + s] : 0.0) : 1.0);
+    double *C = a.crln + (a.n_sat > 0 ? (long long)s * P.N : slice * P.N);
+    const PHYS c0 = m0[0] * m0[0] + m0[1] * m0[1] + m0[2] * m0[2];
+    // both branches add their t = 0 term
+    double v0 = add ? 2.0 * ws * double(c0) : 0.0;
+    if (uniform) {
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) v0 += __shfl_down_sync(full, v0, o);
+      if ((threadIdx.x & 31) == 0 && v0 != 0.0) atomicAdd(&C[0], v0);
+    } else if (v0 != 0.0) {
+      atomicAdd(&C[0], v0);
+    }
+    for (int dir = 0; dir < 2; ++dir) {
+      const int my = add ? len[dir] : 0;
+      int mx = my;
+#pragma unroll
+      for (int o = 16; o > 0; o >>= 1) mx = max(mx, __shfl_xor_sync(full, mx, o));
+      for (int k = 1; k <= mx; ++k) {
+        double v = 0.0;
+        if (k <= my) v = ws * double(ch4_val(mu, base + (dir ? P.N - 1 + k : k), m0));
+        if (uniform) {
+#pragma unroll
+          for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(full, v, o);
+          if ((threadIdx.x & 31) == 0 && v != 0.0) atomicAdd(&C[k], v);
+        } else if (v != 0.0) {
+          atomicAdd(&C[k], v);
+        }
+      }
+    }
+  }
+}
+
+}  // namespace hh

@@ -1,0 +1,17 @@
+// CH4-CO2 dipole table folded for the batched dipole kernel (hh_ch4co2_dip.cuh),
+// built on the host by hh_ch4co2_host.cpp from the generated tables.
+#pragma once
+#include <vector>
+
+struct Ch4Co2FoldHost {
+  int n_entry = 0, n_group = 0;
+  std::vector<double> coef;             // [NSEG][n_entry][4]: cubic in R - centre of each piece
+  std::vector<unsigned char> y2;        // [n_entry]: Y2 index (m2-major, even l2, cos then sin)
+  std::vector<unsigned int> grp;        // [n_group]: cs | comp << 1 | entries << 3
+  std::vector<unsigned short> gcount;   // [(l1, m1), m1-major]: groups at that Y1
+};
+
+// entries e = (component, Y1, Y2) with K_e(R) = sum over the reference's terms of
+// coef * rad_b(R) * N(l1, m1) * N(l2, m2), N(l, m) = sqrt((l+m)!/(l-m)!) (the kernel's
+// harmonics carry sqrt((l-m)!/(l+m)!)); returns 0, or -1 on an unexpected table
+int ch4co2_build_fold(Ch4Co2FoldHost *out);

@@ -1,0 +1,85 @@
+// Host builder of the folded CH4-CO2 dipole table (hh_ch4co2_fold.h) from the
+// expanded reference tables of hh_ch4co2_tables.h, in FP64.
+#include <algorithm>
+#include <cmath>
+#include <map>
+#include <tuple>
+
+#include "hh_ch4co2_fold.h"
+#include "hh_ch4co2_tables.h"
+
+namespace {
+void lm_of(int code, int *l, int *m, int *cs) {
+  const int i = code >> 1;
+  int L = 0;
+  while ((L + 1) * (L + 2) / 2 <= i) ++L;
+  *l = L;
+  *m = i - L * (L + 1) / 2;
+  *cs = code & 1;
+}
+double norm_lm(int l, int m) {  // sqrt((l+m)! / (l-m)!)
+  double p = 1.0;
+  for (int k = l - m + 1; k <= l + m; ++k) p *= k;
+  return std::sqrt(p);
+}
+}  // namespace
+
+int ch4co2_build_fold(Ch4Co2FoldHost *out) {
+  // Y2 index in the kernel's generation order
+  std::map<std::tuple<int, int, int>, int> y2idx;
+  int n2 = 0;
+  for (int m = 0; m <= HH_CH4CO2_L2MAX; ++m)
+    for (int l = m; l <= HH_CH4CO2_L2MAX; ++l)
+      if ((l & 1) == 0) {
+        y2idx[{l, m, 0}] = n2++;
+        if (m > 0) y2idx[{l, m, 1}] = n2++;
+      }
+  // entries keyed in the kernel's loop order: m1, l1, cs1, component, Y2
+  using Key = std::tuple<int, int, int, int, int>;
+  std::map<Key, std::vector<double>> acc;
+  for (int t = 0; t < HH_CH4CO2_NTERM; ++t) {
+    const short *ix = hh_ch4co2_tidx[t];
+    int l1, m1, c1, l2, m2, c2;
+    lm_of(ix[2], &l1, &m1, &c1);
+    lm_of(ix[3], &l2, &m2, &c2);
+    if (l1 > HH_CH4CO2_L1MAX) return -1;
+    auto it = y2idx.find({l2, m2, c2});
+    if (it == y2idx.end()) return -1;
+    std::vector<double> &k = acc[Key(m1, l1, c1, ix[1], it->second)];
+    if (k.empty()) k.assign(HH_CH4CO2_NSEG * 4, 0.0);
+    const double w = hh_ch4co2_tcoef[t] * norm_lm(l1, m1) * norm_lm(l2, m2);
+    for (int s = 0; s < HH_CH4CO2_NSEG; ++s)
+      for (int j = 0; j < 4; ++j) k[s * 4 + j] += w * hh_ch4co2_rad[ix[0]][s][j];
+  }
+  const int E = (int)acc.size();
+  out->n_entry = E;
+  out->coef.assign((size_t)HH_CH4CO2_NSEG * E * 4, 0.0);
+  out->y2.assign(E, 0);
+  out->grp.clear();
+  out->gcount.assign((HH_CH4CO2_L1MAX + 1) * (HH_CH4CO2_L1MAX + 2) / 2, 0);
+  // (l1, m1) -> position in the m1-major order of the kernel
+  auto lm_pos = [](int l, int m) {
+    int p = 0;
+    for (int mm = 0; mm < m; ++mm) p += HH_CH4CO2_L1MAX + 1 - mm;
+    return p + (l - m);
+  };
+  int e = 0;
+  Key prev(-1, -1, -1, -1, -1);
+  for (auto &kv : acc) {
+    const Key &k = kv.first;
+    const bool same = std::get<0>(k) == std::get<0>(prev) && std::get<1>(k) == std::get<1>(prev) &&
+                      std::get<2>(k) == std::get<2>(prev) && std::get<3>(k) == std::get<3>(prev);
+    if (!same) {
+      out->grp.push_back((unsigned)std::get<2>(k) | ((unsigned)std::get<3>(k) << 1));
+      out->gcount[lm_pos(std::get<1>(k), std::get<0>(k))]++;
+    }
+    out->grp.back() += 1u << 3;
+    out->y2[e] = (unsigned char)std::get<4>(k);
+    for (int s = 0; s < HH_CH4CO2_NSEG; ++s)
+      for (int j = 0; j < 4; ++j) out->coef[((size_t)s * E + e) * 4 + j] = kv.second[s * 4 + j];
+    prev = k;
+    ++e;
+  }
+  out->n_group = (int)out->grp.size();
+  return 0;
+}

@@ -20,8 +20,8 @@ cudaError_t launch_candidates(int sys, double mu, double II, double T, double Rm
                               const uint32_t *words, long long n_words, long long word_base, int D,
                               long long n_cand, unsigned char *accept, unsigned char *consumed,
                               double *qp, double *energy, unsigned long long *first_irregular,
-                              cudaStream_t st) {
-  SamplerArgs a{sys, mu, II, T, Rmin, Rmax, pesmin, pair_state};
+                              const SamplerExtra &x, cudaStream_t st) {
+  SamplerArgs a{sys, mu, II, T, Rmin, Rmax, pesmin, pair_state, x};
   size_t smem = (sys == SYS_CO2AR) ? sizeof(Co2arTables<double>) : 0;
   long long blocks = (n_cand + 255) / 256;
   candidate_kernel<<<(unsigned)blocks, 256, smem, st>>>(a, gtab, words, n_words, word_base, D,
@@ -33,9 +33,9 @@ cudaError_t launch_candidates(int sys, double mu, double II, double T, double Rm
 cudaError_t launch_sat_weights(int sys, double mu, double II, double pesmin, int pair_state,
                                const Co2arTablesGlobal *gtab, const double *qp, long long n, double T0,
                                const double *Ts, const double *ratio, int n_sat, double *w, double *wraw,
-                               cudaStream_t st) {
+                               const SamplerExtra &x, cudaStream_t st) {
   if (n_sat < 1 || n_sat > SAT_MAX) return cudaErrorInvalidValue;
-  SamplerArgs a{sys, mu, II, T0, 0.0, 0.0, pesmin, pair_state};
+  SamplerArgs a{sys, mu, II, T0, 0.0, 0.0, pesmin, pair_state, x};
   SatArgs s;
   s.n_sat = n_sat;
   s.T0 = T0;

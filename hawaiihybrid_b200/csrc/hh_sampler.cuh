@@ -3,10 +3,11 @@
 // The reference draws every candidate phase point from one MT19937 stream
 // (thirdparty/mtwist.c, seeded by mt_seed32 in init_ms, src/hawaii.c:157-163)
 // and consumes a fixed number of words per candidate (src/hawaii.c:1206-1421):
-//   q_generator: R, Phi, Theta (+ phi1, theta1 for a linear monomer)
-//   p_generator: 3 (+2) Box-Muller normals, 2 words each
+//   q_generator: R, Phi, Theta (+ phi1, theta1 for a linear monomer; + phi1,
+//                theta1, psi1 of a rotor and phi2, theta2 of a second, linear monomer)
+//   p_generator: 3 (+2, or +3+2) Box-Muller normals, 2 words each
 //   reject:      1 word
-// i.e. D = 10 (atom-atom) or 16 (linear-atom) words.  A Box-Muller draw only
+// i.e. D = 10 (atom-atom), 16 (linear-atom) or 25 (rotor-linear) words.  A Box-Muller draw only
 // retries when its first word is exactly 0 (log(0) = -inf).
 //
 // GPU mapping:
@@ -103,6 +104,7 @@ struct SamplerArgs {
   double T;
   double Rmin, Rmax, pesmin;
   int pair_state;  // 1 free+metastable, 2 bound, 3 all
+  SamplerExtra x;
 };
 
 // reference operation order is kept; FP contraction is disabled for this code
@@ -130,7 +132,19 @@ __device__ __forceinline__ double kinetic(const SamplerArgs &a, const double *qp
   double sT = sin(Theta);
   double K = pR * pR / (2.0 * mu) + pTheta * pTheta / (2.0 * mu * R * R) +
              pPhi * pPhi / (2.0 * mu * R * R * sT * sT);
-  if (a.sys != SYS_HEAR) {
+  if (a.sys == SYS_CH4CO2) {
+    // ROTOR (src/hawaii.c:1090-1110), then the LINEAR_MOLECULE (1119-1127)
+    const double *II = a.x.II1;
+    double pphi1t = qp[7], theta = qp[8], ptheta1t = qp[9], psi = qp[10], ppsi1t = qp[11];
+    double sin_theta = sin(theta), cos_theta = cos(theta), sin_psi = sin(psi), cos_psi = cos(psi);
+    double t1 = (pphi1t - ppsi1t * cos_theta) * sin_psi + ptheta1t * sin_theta * cos_psi;
+    double t2 = (pphi1t - ppsi1t * cos_theta) * cos_psi - ptheta1t * sin_theta * sin_psi;
+    K += t1 * t1 / (2.0 * II[0] * sin_theta * sin_theta) + t2 * t2 / (2.0 * II[1] * sin_theta * sin_theta) +
+         ppsi1t * ppsi1t / (2.0 * II[2]);
+    double I = a.II, pphi = qp[13], th = qp[14], pth = qp[15];
+    double s = sin(th);
+    K += pth * pth / (2.0 * I) + pphi * pphi / (2.0 * I * s * s);
+  } else if (a.sys != SYS_HEAR) {
     double I = a.II, pphi = qp[7], th = qp[8], pth = qp[9];
     double s = sin(th);
     K += pth * pth / (2.0 * I) + pphi * pphi / (2.0 * I * s * s);
@@ -144,6 +158,12 @@ __device__ __forceinline__ double potential(const SamplerArgs &a, const Co2arTab
     double V, dV;
     hear_V_dV<double>(qp[4], 1.0 / qp[4], V, dV);
     return V;
+  }
+  if (a.sys == SYS_CH4CO2) {
+    double y[19], M[3][3];
+    ch4co2_qp_to_state(qp, a.x.II1, y);
+    quat_matrix<double>(y + 6, M);
+    return ch4co2_lj<double>(a.x.lj, M, y, y + 10).V;
   }
   double y[12];
   qp_to_state<SYS_CO2AR>(qp, y);
@@ -180,15 +200,21 @@ __global__ void __launch_bounds__(256) candidate_kernel(
   const long long limit = n_words;
   int retries = 0;
   bool overrun = false;
-  const int QP = (a.sys == SYS_HEAR) ? 6 : 10;
-  double qp[10];
+  const int QP = (a.sys == SYS_HEAR) ? 6 : (a.sys == SYS_CH4CO2 ? 16 : 10);
+  double qp[16];
   double RMIN = a.Rmin, RMAX = a.Rmax, T = a.T;
   // q_generator (src/hawaii.c:1232-1290)
   double R3 = mt_d(words, pos) * (RMAX * RMAX * RMAX - RMIN * RMIN * RMIN) + RMIN * RMIN * RMIN;
   qp[4] = pow(R3, 1.0 / 3.0);
   qp[0] = mt_d(words, pos) * 2.0 * HH_PI;
   qp[2] = acos(2.0 * mt_d(words, pos) - 1.0);
-  if (a.sys != SYS_HEAR) {
+  if (a.sys == SYS_CH4CO2) {
+    qp[6] = mt_d(words, pos) * 2.0 * HH_PI;
+    qp[8] = acos(2.0 * mt_d(words, pos) - 1.0);
+    qp[10] = mt_d(words, pos) * 2.0 * HH_PI;
+    qp[12] = mt_d(words, pos) * 2.0 * HH_PI;
+    qp[14] = acos(2.0 * mt_d(words, pos) - 1.0);
+  } else if (a.sys != SYS_HEAR) {
     qp[6] = mt_d(words, pos) * 2.0 * HH_PI;
     qp[8] = acos(2.0 * mt_d(words, pos) - 1.0);
   }
@@ -201,7 +227,27 @@ __global__ void __launch_bounds__(256) candidate_kernel(
   qp[1] = sqrt_MUKT * qp[4] * sinTheta * x0;
   qp[3] = sqrt_MUKT * qp[4] * x1;
   qp[5] = sqrt_MUKT * x2;
-  if (a.sys != SYS_HEAR) {
+  if (a.sys == SYS_CH4CO2) {
+    // p_generator_rotor (src/hawaii.c:1305-1327)
+    double sqrt_IIx = sqrt(a.x.II1[0] / HH_HKT * T);
+    double sqrt_IIy = sqrt(a.x.II1[1] / HH_HKT * T);
+    double sqrt_IIz = sqrt(a.x.II1[2] / HH_HKT * T);
+    double sin_theta = sin(qp[8]), cos_theta = cos(qp[8]);
+    double sin_psi = sin(qp[10]), cos_psi = cos(qp[10]);
+    double r0 = bm_normal(words, pos, limit, retries, overrun);
+    double r1 = bm_normal(words, pos, limit, retries, overrun);
+    double r2 = bm_normal(words, pos, limit, retries, overrun);
+    qp[7] = sqrt_IIx * sin_theta * sin_psi * r0 + sqrt_IIy * sin_theta * cos_psi * r1 + sqrt_IIz * cos_theta * r2;
+    qp[9] = sqrt_IIx * cos_psi * r0 - sqrt_IIy * sin_psi * r1;
+    qp[11] = sqrt_IIz * r2;
+    // p_generator_linear_molecule of the second monomer (src/hawaii.c:1292-1303)
+    double sqrt_IIKT = sqrt(a.II / HH_HKT * T);
+    double sin_t2 = sin(qp[14]);
+    double m0 = bm_normal(words, pos, limit, retries, overrun);
+    double m1 = bm_normal(words, pos, limit, retries, overrun);
+    qp[13] = sqrt_IIKT * sin_t2 * m1;
+    qp[15] = sqrt_IIKT * m0;
+  } else if (a.sys != SYS_HEAR) {
     double sqrt_IIKT = sqrt(a.II / HH_HKT * T);
     double sin_theta = sin(qp[8]);
     double m0 = bm_normal(words, pos, limit, retries, overrun);
@@ -258,8 +304,8 @@ __global__ void __launch_bounds__(256) sat_weight_kernel(SamplerArgs a, SatArgs 
   __syncthreads();
   const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
   if (i >= n) return;
-  const int QP = (a.sys == SYS_HEAR) ? 6 : 10;
-  double q[10];
+  const int QP = (a.sys == SYS_HEAR) ? 6 : (a.sys == SYS_CH4CO2 ? 16 : 10);
+  double q[16];
   for (int c = 0; c < QP; ++c) q[c] = qp[i * QP + c];
   const double E = kinetic(a, q) + potential(a, tb, q);
   const double T0 = s.T0;

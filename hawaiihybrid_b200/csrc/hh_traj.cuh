@@ -26,6 +26,7 @@
 
 #include <type_traits>
 
+#include "hh_ch4co2.cuh"
 #include "hh_consts.h"
 #include "hh_dop853_tableau.h"
 #include "hh_n2ar.cuh"
@@ -33,7 +34,7 @@
 
 namespace hh {
 
-enum { SYS_HEAR = 1, SYS_CO2AR = 2, SYS_N2AR = 3 };
+enum { SYS_HEAR = 1, SYS_CO2AR = 2, SYS_N2AR = 3, SYS_CH4CO2 = 4 };
 
 struct TrajParams {
   double mu, II;
@@ -69,7 +70,17 @@ struct TrajIO {
   const void *pesnet;         // N2-Ar: the PES network (N2arPesNet) in the surface precision
   const double *sat_w;        // CORRELATION_ARRAY: [n_traj][n_sat] weights (nullptr: one C(t))
   int n_sat;                  // satellite temperatures; their C(t) are consecutive N-slices
+  // CH4-CO2: samples are written as records (r, quaternion, u) in the surface
+  // precision, HH_REC_WORDS words each, at traj * rec_stride + slot (slot 0: t = 0;
+  // k: forward sample k; N - 1 + k: backward sample k), for the batched dipole
+  void *records;
+  int rec_stride;             // 2 * MaxTrajectoryLength - 1
+  int *rec_len;               // [item]: samples stored (k = 1 .. rec_len)
+  int *rec_status;            // [item]: end status of the integration
+  double inv_I1[3];           // 1 / principal moments of CH4
+  Ch4Co2Lj lj;
 };
+constexpr int HH_REC_WORDS = 12;  // r[3], q[4], u[3], padding
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
   unsigned long long t;
@@ -119,6 +130,8 @@ template <typename PHYS, typename STG, bool COMP> struct HeArSys {
   static constexpr int QP = 6;
   // components the dipole and the R > Rcut test read: r
   static constexpr int NQ = 3;
+  static constexpr bool RECORDS = false;
+  static constexpr int MOM2 = 6;  // no second momentum block
   static __device__ __forceinline__ constexpr int qidx(int i) { return i; }
   double inv_mu;
   // y in FP64 (the state) or in the stage precision (stage points)
@@ -181,6 +194,8 @@ template <typename PHYS, typename STG, bool COMP> struct Co2ArSys {
   static constexpr int QP = 10;
   // components the dipole and the R > Rcut test read: r and u
   static constexpr int NQ = 6;
+  static constexpr bool RECORDS = false;
+  static constexpr int MOM2 = 9;  // j
   static __device__ __forceinline__ constexpr int qidx(int i) { return i < 3 ? i : i + 3; }
   double inv_mu, inv_II;
   const Co2arTables<PHYS> *tb;
@@ -246,6 +261,8 @@ template <typename PHYS, typename STG, bool COMP> struct N2ArSys {
   static constexpr int N = 12;
   static constexpr int QP = 10;
   static constexpr int NQ = 6;
+  static constexpr bool RECORDS = false;
+  static constexpr int MOM2 = 9;  // j
   static __device__ __forceinline__ constexpr int qidx(int i) { return i < 3 ? i : i + 3; }
   double inv_mu, inv_II;
   const N2arDipFold *fold;      // shared-memory copies
@@ -489,18 +506,21 @@ template <class Sys, typename PHYS, typename STG>
 __device__ __noinline__ void item_setup(const Sys &sys, const TrajParams &P, const double *qp,
                                         int dir, double *y0, STG *f0, PHYS *mu0, double *h_out) {
   constexpr int N = Sys::N;
-  constexpr int SYS = (N == 6) ? SYS_HEAR : SYS_CO2AR;
-  qp_to_state<SYS>(qp, y0);
+  if constexpr (Sys::N == 19) {
+    ch4co2_qp_to_state(qp, nullptr, y0);
+  } else {
+    qp_to_state<(N == 6) ? SYS_HEAR : SYS_CO2AR>(qp, y0);
+  }
   double q0[Sys::NQ];
 #pragma unroll
   for (int c = 0; c < Sys::NQ; ++c) q0[c] = y0[Sys::qidx(c)];
   sys.dipole(q0, mu0);
   if (dir) {
-    // invert_momenta (src/hawaii.c:1171-1188): p -> -p, j -> -j
+    // invert_momenta (src/hawaii.c:1171-1188): p -> -p, j -> -j (and L)
 #pragma unroll
     for (int i = 3; i < 6; ++i) y0[i] = -y0[i];
 #pragma unroll
-    for (int i = 9; i < N; ++i) y0[i] = -y0[i];
+    for (int i = Sys::MOM2; i < N; ++i) y0[i] = -y0[i];
   }
   sys.rhs(y0, f0);
   // the sampled window bounds the first step (one sample interval when N = 1,
@@ -621,6 +641,13 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
           }
 #pragma unroll
           for (int c = 0; c < 3; ++c) mu0[c] = mu_t[c];
+          if constexpr (Sys::RECORDS) {
+            if ((item & 1) == 0) {
+              PHYS *rec = static_cast<PHYS *>(io.records) + (size_t)traj * io.rec_stride * HH_REC_WORDS;
+#pragma unroll
+              for (int c = 0; c < Sys::NQ; ++c) rec[c] = PHYS(y_t[Sys::qidx(c)]);
+            }
+          }
           nrhs += 2;
           t = 0.0;
           k = 1;
@@ -742,14 +769,24 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
               v = (v + ws->F[0][c][o]) * xs;
               q[c] = ws->qold[c][o] + double(v);
             }
-            PHYS d[3];
-            sys.dipole(q, d);
             ++nsamp;
             own[u] = o;
             kks[u] = kk;
-            nan_[u] = isnan(d[0]) || isnan(d[1]) || isnan(d[2]);
             out_[u] = q[0] * q[0] + q[1] * q[1] + q[2] * q[2] > P.Rcut * P.Rcut;
-            ws->res[jj] = ws->mu0[0][o] * d[0] + ws->mu0[1][o] * d[1] + ws->mu0[2][o] * d[2];
+            if constexpr (Sys::RECORDS) {
+              const int it = ws->item[o];
+              const size_t slot = (size_t)(it >> 1) * io.rec_stride + ((it & 1) ? P.N - 1 + kk : kk);
+              PHYS *rec = static_cast<PHYS *>(io.records) + slot * HH_REC_WORDS;
+#pragma unroll
+              for (int c = 0; c < Sys::NQ; ++c) rec[c] = PHYS(q[c]);
+              nan_[u] = false;
+              ws->res[jj] = PHYS(1);
+            } else {
+              PHYS d[3];
+              sys.dipole(q, d);
+              nan_[u] = isnan(d[0]) || isnan(d[1]) || isnan(d[2]);
+              ws->res[jj] = ws->mu0[0][o] * d[0] + ws->mu0[1][o] * d[1] + ws->mu0[2][o] * d[2];
+            }
           }
         }
         __syncwarp();
@@ -762,7 +799,10 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
             const int j = base + jj;
             const PHYS val = ws->res[jj];
             unsigned code = 0xffffffffu;
-            if (nan_[u]) code = (unsigned(j) << 3) | 1u;
+            if (Sys::RECORDS) {
+              // a record's dipole checks run after the batched evaluation
+              if (out_[u]) code = (unsigned(j + 1) << 3);
+            } else if (nan_[u]) code = (unsigned(j) << 3) | 1u;
             else if (ws->item[o] == P.inject_item && kks[u] == P.inject_k) code = (unsigned(j) << 3) | 4u;
             else if (fabs(double(val)) > 1e100) code = (unsigned(j) << 3) | 2u;
             else {
@@ -787,7 +827,9 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
             const int stop = (cut == 0xffffffffu) ? end_o : min(end_o, int(cut >> 3));
             const int chunk_end = min(end_o, base + m);
             if (j < stop) {
-              if (io.n_sat == 0) {
+              if (Sys::RECORDS) {
+                // written in (1)
+              } else if (io.n_sat == 0) {
                 atomicAdd(&ws->crln[o][kks[u]], P.weight * double(val));
               } else {
                 const double *w = ws->satw[o];
@@ -839,7 +881,13 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
       if (k >= P.N) status = HH_ST_OK;
       else if (++since > P.max_steps || ++total > P.max_total_steps) status = HH_ST_MAXSTEPS;
     }
-    if (active && status >= 0) {
+    if (Sys::RECORDS && active && status >= 0) {
+      io.rec_len[item] = k - 1;
+      io.rec_status[item] = status;
+      ++nitems;
+      item = -1;
+    }
+    if (!Sys::RECORDS && active && status >= 0) {
       const int traj = item >> 1;
       // the t = 0 term is added by branches that are not dropped, so a replay
       // with the opposite weight removes exactly what a dropped trajectory added
@@ -901,7 +949,7 @@ template <int SYS, typename PHYS, typename STG> constexpr size_t traj_smem_bytes
   return (SYS == SYS_CO2AR   ? smem_tables_bytes<PHYS>()
           : SYS == SYS_N2AR ? sizeof(N2arDipFold) + sizeof(N2arPesNet<PHYS>)
                             : 0) +
-         traj_warps<PHYS>() * sizeof(WarpSamples<STG, PHYS, (SYS == SYS_HEAR ? 3 : 6)>);
+         traj_warps<PHYS>() * sizeof(WarpSamples<STG, PHYS, (SYS == SYS_HEAR ? 3 : SYS == SYS_CH4CO2 ? 10 : 6)>);
 }
 
 template <int SYS, typename PHYS, typename STG, bool COMP>
@@ -912,6 +960,16 @@ __global__ void __launch_bounds__(traj_threads<PHYS>(), TRAJ_MIN_BLOCKS)
     using Sys = HeArSys<PHYS, STG, COMP>;
     Sys sys;
     sys.inv_mu = 1.0 / P.mu;
+    auto *ws = reinterpret_cast<WarpSamples<STG, PHYS, Sys::NQ> *>(smem_raw);
+    traj_body<Sys, PHYS, STG>(sys, P, io, ws);
+  } else if (SYS == SYS_CH4CO2) {
+    using Sys = Ch4Co2Sys<PHYS, STG, COMP>;
+    Sys sys;
+    sys.inv_mu = 1.0 / P.mu;
+    sys.inv_II = 1.0 / P.II;
+#pragma unroll
+    for (int k = 0; k < 3; ++k) sys.inv_I1[k] = io.inv_I1[k];
+    sys.lj = io.lj;
     auto *ws = reinterpret_cast<WarpSamples<STG, PHYS, Sys::NQ> *>(smem_raw);
     traj_body<Sys, PHYS, STG>(sys, P, io, ws);
   } else if (SYS == SYS_N2AR) {

@@ -39,6 +39,7 @@ II_CO2 = m_O / 2.0 * l_CO2 * l_CO2
 # ---- MonomerType (src/hawaii.h:183-190) ----
 ATOM = 0
 LINEAR_MOLECULE = 4
+ROTOR = 6
 
 # ---- PairState (src/hawaii.h:290-300) ----
 PAIR_STATE_NONE = 0
@@ -50,6 +51,7 @@ PAIR_STATE_ALL = 3
 SYSTEM_HE_AR = _lib.HH_SYSTEM_HE_AR
 SYSTEM_CO2_AR = _lib.HH_SYSTEM_CO2_AR
 SYSTEM_N2_AR = _lib.HH_SYSTEM_N2_AR
+SYSTEM_CH4_CO2 = _lib.HH_SYSTEM_CH4_CO2
 
 PRECISION_FP64 = _lib.HH_PRECISION_FP64
 PRECISION_MIXED = _lib.HH_PRECISION_MIXED
@@ -116,7 +118,8 @@ def init_ms(mu: float, t1: int, t2: int, II1: Optional[Sequence[float]], II2: Op
     """init_ms (src/hawaii.c:173-270): bind the pair to the device and seed the sampler stream.
 
     system_id names the device surface (the role of the plugin .so in the reference);
-    it defaults from the monomer types (ATOM+ATOM -> He-Ar, LINEAR+ATOM -> CO2-Ar)."""
+    it defaults from the monomer types (ATOM+ATOM -> He-Ar, LINEAR+ATOM -> CO2-Ar,
+    ROTOR+LINEAR -> CH4-CO2)."""
     if mu <= 0:
         raise ValueError(f"invalid reduced mass ({mu:.5e}) -- must be positive")
     if system_id is None:
@@ -124,6 +127,8 @@ def init_ms(mu: float, t1: int, t2: int, II1: Optional[Sequence[float]], II2: Op
             system_id = SYSTEM_HE_AR
         elif t1 == LINEAR_MOLECULE and t2 == ATOM:
             system_id = SYSTEM_CO2_AR
+        elif t1 == ROTOR and t2 == LINEAR_MOLECULE:
+            system_id = SYSTEM_CH4_CO2
         else:
             raise HHError(_lib.HH_E_UNSUPPORTED_SYSTEM, "no device surface for these monomers")
     ms = MoleculeSystem(system_id, mu, t1, t2, tuple(II1 or (0, 0, 0)) + (0.0,) * (3 - len(II1 or (0, 0, 0))),
@@ -203,6 +208,21 @@ def correlation_iterations(ms: MoleculeSystem, params: CalcParams, Temperature: 
     check(L.hh_cuda_correlation_multi(C.byref(pc), Temperature, seed, n_per_iteration, n_iterations,
                                       precision, crln, ntraj, C.byref(st)))
     return crln.reshape(n_iterations, -1), ntraj, st
+
+
+def correlation_temperatures(ms: MoleculeSystem, params: CalcParams, temperatures: Sequence[float],
+                             n_per_temperature: int, precision: int = PRECISION_FP64, seed: int = 0):
+    """The CORRELATION_SINGLE pass at several temperatures in one launch: returns
+    (crln_sums[nT, N], ntraj[nT], stats)."""
+    L = _bind(ms)
+    T = np.ascontiguousarray(temperatures, dtype=np.float64)
+    crln = np.zeros(T.size * params.MaxTrajectoryLength, dtype=np.float64)
+    ntraj = np.zeros(T.size, dtype=np.float64)
+    st = _lib.Stats()
+    pc = params.to_c()
+    check(L.hh_cuda_correlation_temperatures(C.byref(pc), T, T.size, seed, n_per_temperature, precision,
+                                             crln, ntraj, C.byref(st)))
+    return crln.reshape(T.size, -1), ntraj, st
 
 
 def correlation_from_initial_conditions(ms: MoleculeSystem, params: CalcParams, qp0: np.ndarray,
@@ -354,11 +374,14 @@ def calculate_m0(ms: MoleculeSystem, params: CalcParams, temperatures: Sequence[
 
 
 def analytic_full_partition_function_by_V(ms: MoleculeSystem, Temperature: float) -> float:
-    """src/hawaii.c:5071-5090 (ATOM-ATOM and LINEAR_MOLECULE-ATOM)."""
+    """src/hawaii.c:5071-5090 (ATOM-ATOM, LINEAR_MOLECULE-ATOM, ROTOR-LINEAR_MOLECULE)."""
     if ms.m1_type == ATOM and ms.m2_type == ATOM:
         return (2.0 * math.pi * ms.mu * Temperature / HkT) ** 1.5
     if ms.m1_type == LINEAR_MOLECULE and ms.m2_type == ATOM:
         return 4.0 * math.pi * (2.0 * math.pi * Temperature / HkT) ** 2.5 * ms.mu ** 1.5 * ms.II1[0]
+    if ms.m1_type == ROTOR and ms.m2_type == LINEAR_MOLECULE:
+        return (32.0 * math.pi ** 3 * (2.0 * math.pi * Temperature / HkT) ** 4.0 * ms.mu ** 1.5 *
+                math.sqrt(ms.II1[0] * ms.II1[1] * ms.II1[2]) * ms.II2[0])
     raise NotImplementedError("analytic_full_partition_function_by_V")
 
 

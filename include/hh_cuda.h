@@ -53,6 +53,7 @@ extern "C" {
 /* MonomerType values of the reference (src/hawaii.h:183-190) */
 #define HH_MONOMER_ATOM 0
 #define HH_MONOMER_LINEAR_MOLECULE 4
+#define HH_MONOMER_ROTOR 6
 
 /* PairState of the reference (src/hawaii.h:290-300) */
 #define HH_PAIR_STATE_FREE_AND_METASTABLE 1
@@ -64,6 +65,11 @@ extern "C" {
 #define HH_SYSTEM_HE_AR 1
 #define HH_SYSTEM_CO2_AR 2
 #define HH_SYSTEM_N2_AR 3   /* PIP-NN surfaces of PES-IDS/ai_pes_n2_ar_pip_nn.cpp, ai_ids_n2_ar_pip_nn.cpp */
+#define HH_SYSTEM_CH4_CO2 4 /* ROTOR (CH4, II1) + LINEAR_MOLECULE (CO2, II2): the dipole of
+                               PES-IDS/ai_ids_ch4_co2.cpp; the reference tree has no source for its
+                               CH4-CO2 PES (PES-IDS/ai_pes_ch4_co2.h), so trajectories run on a
+                               site-site Lennard-Jones stand-in whose minimum is the config's pesmin.
+                               No M0 (HH_E_UNSUPPORTED_SYSTEM). */
 
 /* precision modes */
 #define HH_PRECISION_FP64 0  /* FP64 surfaces and stages: the plain drop-in path */
@@ -135,6 +141,16 @@ int hh_cuda_correlation(const hh_calc_params *p, double T, uint32_t seed, uint64
 int hh_cuda_correlation_multi(const hh_calc_params *p, double T, uint32_t seed,
                               uint64_t n_per_iteration, uint32_t n_iterations, int precision_mode,
                               double *crln_sums, double *ntraj, hh_stats *stats);
+
+/* The reference's CORRELATION_SINGLE run repeated at nT temperatures (one driver
+ * run per TEMPERATURE, src/hawaii.c:2970-3012 each): n_per_T phase points are
+ * sampled at T[0], then T[1], ... from one stream (seed as in hh_cuda_sample), and
+ * all nT * n_per_T trajectories are integrated together, so the long trajectories
+ * of the cold sets run beside the short ones of the hot sets.  crln_sums[i][k]
+ * (nT x MaxTrajectoryLength) and ntraj[i] per temperature. */
+int hh_cuda_correlation_temperatures(const hh_calc_params *p, const double *T, int nT, uint32_t seed,
+                                     uint64_t n_per_T, int precision_mode, double *crln_sums,
+                                     double *ntraj, hh_stats *stats);
 
 /* CORRELATION_ARRAY: n_accept trajectories sampled at base_T, each added to the
  * C(t) of every satellite temperature sat_T[s] with the reference's reweighting

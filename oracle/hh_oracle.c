@@ -437,16 +437,25 @@ void hho_ch4co2_dipole_kal(const double *qkal, double d[3]) {
     for (int k = 0; k <= HH_CH4CO2_L2MAX; ++k) { t2[0][k] = cos(k * qkal[3]); t2[1][k] = sin(k * qkal[3]); }
     double rad[HH_CH4CO2_NB];
     for (int b = 0; b < HH_CH4CO2_NB; ++b) rad[b] = ch4co2_rad(b, R);
+    /* harmonic values by code 2 * (l(l+1)/2 + m) + cs */
+    double Y1[(HH_CH4CO2_L1MAX + 1) * (HH_CH4CO2_L1MAX + 2)], Y2[(HH_CH4CO2_L2MAX + 1) * (HH_CH4CO2_L2MAX + 2)];
+    for (int l = 0; l <= HH_CH4CO2_L1MAX; ++l)
+        for (int m = 0; m <= l; ++m)
+            for (int cs = 0; cs < 2; ++cs) {
+                int i = l * (l + 1) / 2 + m;
+                Y1[2 * i + cs] = P1[i] * (m ? t1[cs][m] : 1.0);
+            }
+    for (int l = 0; l <= HH_CH4CO2_L2MAX; ++l)
+        for (int m = 0; m <= l; ++m)
+            for (int cs = 0; cs < 2; ++cs) {
+                int i = l * (l + 1) / 2 + m;
+                Y2[2 * i + cs] = P2[i] * (m ? t2[cs][m] : 1.0);
+            }
     double acc[HH_CH4CO2_NB][3];
     memset(acc, 0, sizeof acc);
     for (int t = 0; t < HH_CH4CO2_NTERM; ++t) {
         const short *ix = hh_ch4co2_tidx[t];
-        int i1 = ix[2] >> 1, c1 = ix[2] & 1, i2 = ix[3] >> 1, c2 = ix[3] & 1;
-        int l1 = (int)((sqrt(8.0 * i1 + 1.0) - 1.0) / 2.0), l2 = (int)((sqrt(8.0 * i2 + 1.0) - 1.0) / 2.0);
-        int m1 = i1 - l1 * (l1 + 1) / 2, m2 = i2 - l2 * (l2 + 1) / 2;
-        double y1 = P1[i1] * (m1 ? t1[c1][m1] : 1.0);
-        double y2 = P2[i2] * (m2 ? t2[c2][m2] : 1.0);
-        acc[ix[0]][ix[1]] += hh_ch4co2_tcoef[t] * y1 * y2;
+        acc[ix[0]][ix[1]] += hh_ch4co2_tcoef[t] * Y1[ix[2]] * Y2[ix[3]];
     }
     d[0] = d[1] = d[2] = 0.0;
     for (int b = 0; b < HH_CH4CO2_NB; ++b)

@@ -60,6 +60,9 @@ def lib_system(name, seed=1):
     if name == "n2ar":
         return hh.init_ms(MU_N2AR, hh.LINEAR_MOLECULE, hh.ATOM, (II_N2, II_N2), None, seed,
                           system_id=hh.SYSTEM_N2_AR)
+    if name == "ch4co2":
+        return hh.init_ms(MU_CH4CO2, hh.ROTOR, hh.LINEAR_MOLECULE, (II_CH4, II_CH4, II_CH4), (II_CO2, II_CO2),
+                          seed)
     return hh.init_ms(MU_CO2AR, hh.LINEAR_MOLECULE, hh.ATOM, (II_CO2, II_CO2), None, seed)
 
 

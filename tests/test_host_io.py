@@ -53,3 +53,14 @@ def test_partition_function_and_params():
     assert abs(pf / (4 * np.pi * (2 * np.pi * kT) ** 2.5 * 3.8e4 ** 1.5 * 2.8e5) - 1) < 1e-14
     c = hh.CalcParams(MaxTrajectoryLength=128).to_c()
     assert c.MaxTrajectoryLength == 128 and c.pair_state == 1
+
+
+def test_rotor_linear_partition_function_matches_reference_log():
+    """src/hawaii.c:5083-5085 for CH4-CO2; the reference's own run prints
+    'Analytic partition function divided by V: 4.16497e+10' at 100 K
+    (example_configs/CF-F-CH4-CO2-100.0.conf.out)."""
+    from tests.helpers import II_CH4, II_CO2, MU_CH4CO2
+    ms = H.MoleculeSystem(H.SYSTEM_CH4_CO2, MU_CH4CO2, hh.ROTOR, hh.LINEAR_MOLECULE, (II_CH4,) * 3,
+                          (II_CO2, II_CO2, 0.0))
+    assert ms.QP_SIZE == 16
+    assert f"{hh.analytic_full_partition_function_by_V(ms, 100.0):.5e}" == "4.16497e+10"
