@@ -367,12 +367,13 @@ int run_records_t(const TrajParams &P, const double *d_ic, uint64_t n, uint64_t 
   const size_t rec_b = HH_REC_WORDS * sizeof(PHYS), mu_b = 4 * sizeof(PHYS);
   const size_t per_traj = (size_t)stride * (rec_b + mu_b + sizeof(int)) + 4 * sizeof(int);
   uint64_t chunk = std::max<uint64_t>(1, CH4_RECORD_BUDGET / per_traj);
-  chunk = std::min<uint64_t>(chunk, (uint64_t)((INT32_MAX - 32 * CH4_NSEG) / stride));
+  chunk = std::min<uint64_t>(chunk, (uint64_t)((INT32_MAX - 128 * CH4_NSEG) / stride));
   chunk = std::min<uint64_t>(chunk, n);
   const size_t slots = (size_t)chunk * stride;
   CK(g.rec.ensure(slots * rec_b));
   CK(g.rec_mu.ensure(slots * mu_b));
-  CK(g.rec_sorted.ensure(slots + 32 * CH4_NSEG));
+  const int task = 32 * ch4_dip_s<PHYS>();
+  CK(g.rec_sorted.ensure(slots + (size_t)task * CH4_NSEG));
   CK(g.rec_len.ensure(2 * chunk));
   CK(g.rec_status.ensure(2 * chunk));
   CK(g.seg_cnt.ensure(2 * CH4_NSEG));
@@ -390,7 +391,7 @@ int run_records_t(const TrajParams &P, const double *d_ic, uint64_t n, uint64_t 
   for (int i = 0; i < CH4_NSEG - 1; ++i) fold.seg_hi[i] = hh_ch4co2_seg_hi[i];
   for (int i = 0; i < CH4_NSEG; ++i) fold.centre[i] = hh_ch4co2_centre[i];
   auto dip = ch4_dipole_kernel<PHYS>;
-  const size_t dsmem = (size_t)CH4_DIP_WARPS * CH4_NY2 * 32 * sizeof(PHYS);
+  const size_t dsmem = ch4_dip_smem<PHYS>();
   if (dsmem > 48 * 1024) CK(cudaFuncSetAttribute(dip, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsmem));
   int dper = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&dper, dip, 32 * CH4_DIP_WARPS, dsmem));
@@ -399,7 +400,7 @@ int run_records_t(const TrajParams &P, const double *d_ic, uint64_t n, uint64_t 
     const uint64_t nc = std::min<uint64_t>(chunk, n - base);
     CK(cudaMemsetAsync(g.queue.p, 0, sizeof(unsigned int), g.st));
     CK(cudaMemsetAsync(g.seg_cnt.p, 0, 2 * CH4_NSEG * sizeof(unsigned int), g.st));
-    CK(cudaMemsetAsync(g.rec_sorted.p, 0xff, (nc * stride + 32 * CH4_NSEG) * sizeof(int), g.st));
+    CK(cudaMemsetAsync(g.rec_sorted.p, 0xff, (nc * stride + (size_t)task * CH4_NSEG) * sizeof(int), g.st));
     TrajIO io;
     memset(&io, 0, sizeof io);
     io.ic = d_ic + base * g.QP;
@@ -428,6 +429,7 @@ int run_records_t(const TrajParams &P, const double *d_ic, uint64_t n, uint64_t 
     sa.cursor = g.seg_cnt.p + CH4_NSEG;
     sa.warp0 = g.seg_w0.p;
     sa.sorted = g.rec_sorted.p;
+    sa.task = task;
     for (int i = 0; i < CH4_NSEG - 1; ++i) sa.seg_hi[i] = hh_ch4co2_seg_hi[i];
     const long long nslots = (long long)nc * stride;
     const int sgrid = (int)std::min<long long>((nslots + 255) / 256, 8LL * g.num_sms);

@@ -15,10 +15,13 @@
 // coefficient load would be a 32-way gather over pieces.  Instead the trajectory
 // kernel writes each sample as a record and:
 //   1. seg_count / seg_scan / seg_scatter sort the valid records by radial piece,
-//      each piece padded to a multiple of 32, so every warp task has one piece;
-//   2. dipole_kernel: a warp evaluates 32 records of one piece; the coefficient
-//      stream of that piece is the same for all lanes (broadcast loads), Y2 sits
-//      per lane in shared memory, Y1 is generated in the order of the stream;
+//      each piece padded to a multiple of the warp task (32 S records), so every
+//      warp task has one piece;
+//   2. dipole_kernel: a warp evaluates 32 S records of one piece, S per lane; the
+//      coefficient stream of that piece is the same for all lanes (broadcast loads,
+//      shared by a lane's S records), the S values of Y2 of each index sit side by
+//      side in shared memory (one vector load), Y1 is generated in the order of the
+//      stream;
 //   3. corr_kernel applies the reference's per-sample tests in order (NaN dipole,
 //      |C| > 1e100, |C_k / C_k-1| > 1e10: src/hawaii.c:2183-2243) and adds
 //      w mu0.mu(t_k) of every trajectory that passes into C(t).
@@ -59,6 +62,7 @@ struct Ch4SortArgs {
   unsigned int *cursor;       // [NSEG]
   long long *warp0;           // [NSEG + 1] first warp task of each piece; [NSEG] = total
   int *sorted;                // record index per task slot, -1 for padding
+  int task;                   // records per warp task (32 S)
   double seg_hi[CH4_NSEG - 1];
 };
 
@@ -104,7 +108,7 @@ __global__ void ch4_seg_scan_kernel(Ch4SortArgs a) {
     long long w = 0;
     for (int s = 0; s < CH4_NSEG; ++s) {
       a.warp0[s] = w;
-      w += (a.count[s] + 31) / 32;
+      w += (a.count[s] + a.task - 1) / a.task;
       a.cursor[s] = 0;
     }
     a.warp0[CH4_NSEG] = w;
@@ -121,7 +125,7 @@ __global__ void __launch_bounds__(256) ch4_seg_scatter_kernel(Ch4SortArgs a) {
     if (!ch4_valid(a.rec_len, t, sl, a.N)) continue;
     const int s = ch4_seg(a.seg_hi, ch4_rec_R<PHYS>(a.records, i));
     const unsigned pos = atomicAdd(&a.cursor[s], 1u);
-    a.sorted[a.warp0[s] * 32 + pos] = (int)i;
+    a.sorted[a.warp0[s] * a.task + pos] = (int)i;
   }
 }
 
@@ -133,17 +137,50 @@ struct Ch4DipArgs {
   void *mu;                   // [record][4] lab-frame dipole in the surface precision
 };
 
+// records per lane of the dipole kernel (S values of a Y2 index are one shared-
+// memory vector).  More records per lane share each coefficient load among more
+// samples; fewer leave room for more resident warps (the per-lane Y2 arrays take
+// 91 x 32 x S values per warp).
+#ifndef HH_CH4_DIP_S_FP32
+#define HH_CH4_DIP_S_FP32 4
+#endif
+#ifndef HH_CH4_DIP_S_FP64
+#define HH_CH4_DIP_S_FP64 1
+#endif
+template <typename PHYS> __host__ __device__ constexpr int ch4_dip_s() {
+  return sizeof(PHYS) == 4 ? HH_CH4_DIP_S_FP32 : HH_CH4_DIP_S_FP64;
+}
+template <typename PHYS> __host__ __device__ constexpr size_t ch4_dip_smem() {
+  return (size_t)CH4_DIP_WARPS * CH4_NY2 * 32 * ch4_dip_s<PHYS>() * sizeof(PHYS);
+}
+
+template <typename PHYS, int S> struct Vec;
+template <> struct Vec<float, 4> { using T = float4; };
+template <> struct Vec<float, 2> { using T = float2; };
+template <> struct Vec<float, 1> { using T = float; };
+template <> struct Vec<double, 2> { using T = double2; };
+template <> struct Vec<double, 1> { using T = double; };
+template <typename V> __device__ __forceinline__ auto vget(const V &v, int s);
+__device__ __forceinline__ float vget(const float4 &v, int s) {
+  return s == 0 ? v.x : s == 1 ? v.y : s == 2 ? v.z : v.w;
+}
+__device__ __forceinline__ double vget(const double2 &v, int s) { return s == 0 ? v.x : v.y; }
+__device__ __forceinline__ float vget(const float2 &v, int s) { return s == 0 ? v.x : v.y; }
+__device__ __forceinline__ float vget(const float &v, int) { return v; }
+__device__ __forceinline__ double vget(const double &v, int) { return v; }
+
 // Y2 of the CO2 axis n2 in the CH4 frame: even l <= 12, in the order
-// m = 0..12, l = m..12 (even), cos then sin
-template <typename T>
-__device__ __forceinline__ void ch4_y2(T x, T y, T z, T *Y, int lane) {
-  T C = T(1), S = T(0), pm = T(1);
+// m = 0..12, l = m..12 (even), cos then sin; Y[idx * 32 S + lane S + s]
+template <typename T, int S>
+__device__ __forceinline__ void ch4_y2(T x, T y, T z, T *Y, int lane, int s_) {
+  T C = T(1), Sn = T(0), pm = T(1);
   int idx = 0;
+  T *Yl = Y + lane * S + s_;
 #pragma unroll 1
   for (int m = 0; m <= CH4_L2; ++m) {
     if (m > 0) {
-      const T c = C * x - S * y;
-      S = C * y + S * x;
+      const T c = C * x - Sn * y;
+      Sn = C * y + Sn * x;
       C = c;
       pm = -pm * sqrt(T(2 * m - 1) / T(2 * m));
     }
@@ -155,8 +192,8 @@ __device__ __forceinline__ void ch4_y2(T x, T y, T z, T *Y, int lane) {
       else if (l == m + 1) q = sqrt(T(2 * m + 1)) * z;
       else q = (T(2 * l - 1) * z * qa - sqrt(T((l - 1) * (l - 1) - m * m)) * qb) / sqrt(T(l * l - m * m));
       if ((l & 1) == 0) {
-        Y[(idx++) * 32 + lane] = pm * C * q;
-        if (m > 0) Y[(idx++) * 32 + lane] = pm * S * q;
+        Yl[(idx++) * 32 * S] = pm * C * q;
+        if (m > 0) Yl[(idx++) * 32 * S] = pm * Sn * q;
       }
       qb = qa;
       qa = q;
@@ -166,105 +203,176 @@ __device__ __forceinline__ void ch4_y2(T x, T y, T z, T *Y, int lane) {
 
 template <typename PHYS>
 __global__ void __launch_bounds__(32 * CH4_DIP_WARPS) ch4_dipole_kernel(Ch4DipArgs a) {
+  constexpr int S = ch4_dip_s<PHYS>();
+  using V = typename Vec<PHYS, S>::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ long long w0[CH4_NSEG + 1];
   for (int i = threadIdx.x; i <= CH4_NSEG; i += blockDim.x) w0[i] = a.warp0[i];
   __syncthreads();
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-  PHYS *Y2 = reinterpret_cast<PHYS *>(smem_raw) + (size_t)warp * CH4_NY2 * 32;
+  PHYS *Y2 = reinterpret_cast<PHYS *>(smem_raw) + (size_t)warp * CH4_NY2 * 32 * S;
+  const V *Y2v = reinterpret_cast<const V *>(Y2) + lane;
   const long long total = w0[CH4_NSEG];
   const long long nw = (long long)gridDim.x * CH4_DIP_WARPS;
   for (long long w = (long long)blockIdx.x * CH4_DIP_WARPS + warp; w < total; w += nw) {
     int seg = 0;
     while (seg < CH4_NSEG - 1 && w0[seg + 1] <= w) ++seg;
-    const int mine = a.sorted[w * 32 + lane];
-    // padding lanes evaluate lane 0's record (always valid) and store nothing; the
-    // shuffle runs in every lane
-    const int first = __shfl_sync(0xffffffffu, mine, 0);
-    const int src = mine >= 0 ? mine : first;
-    const PHYS *rec = static_cast<const PHYS *>(a.records) + (size_t)src * HH_REC_WORDS;
-    const PHYS r[3] = {rec[0], rec[1], rec[2]};
-    const PHYS qt[4] = {rec[3], rec[4], rec[5], rec[6]};
-    const PHYS u[3] = {rec[7], rec[8], rec[9]};
-    PHYS M[3][3];
-    quat_matrix<PHYS>(qt, M);
-    const PHYS R = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
-    const PHYS iR = PHYS(1) / R;
-    const PHYS iu = PHYS(1) / sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
-    // body-frame directions n = M^T v
-    PHYS n1[3], n2[3];
+    // record s of this lane: task slot s * 32 + lane; padding slots evaluate the
+    // task's first record (always valid) and store nothing.  Shuffles run in every lane.
+    int mine[S];
+    PHYS x[S], M[S][3][3], n1[S][3], iR6[S];
+    const int first = __shfl_sync(0xffffffffu, a.sorted[w * 32 * S + lane], 0);
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-      n1[k] = (M[0][k] * r[0] + M[1][k] * r[1] + M[2][k] * r[2]) * iR;
-      n2[k] = (M[0][k] * u[0] + M[1][k] * u[1] + M[2][k] * u[2]) * iu;
+    for (int s = 0; s < S; ++s) {
+      mine[s] = a.sorted[w * 32 * S + s * 32 + lane];
+      const int src = mine[s] >= 0 ? mine[s] : first;
+      const PHYS *rec = static_cast<const PHYS *>(a.records) + (size_t)src * HH_REC_WORDS;
+      const PHYS r[3] = {rec[0], rec[1], rec[2]};
+      const PHYS qt[4] = {rec[3], rec[4], rec[5], rec[6]};
+      const PHYS u[3] = {rec[7], rec[8], rec[9]};
+      quat_matrix<PHYS>(qt, M[s]);
+      const PHYS R = sqrt(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+      const PHYS iR = PHYS(1) / R;
+      const PHYS iu = PHYS(1) / sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+      PHYS n2[3];
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        n1[s][k] = (M[s][0][k] * r[0] + M[s][1][k] * r[1] + M[s][2][k] * r[2]) * iR;
+        n2[k] = (M[s][0][k] * u[0] + M[s][1][k] * u[1] + M[s][2][k] * u[2]) * iu;
+      }
+      ch4_y2<PHYS, S>(n2[0], n2[1], n2[2], Y2, lane, s);
+      x[s] = R - PHYS(a.f.centre[seg]);
+      const PHYS i2 = iR * iR;
+      iR6[s] = i2 * i2 * i2;
     }
-    ch4_y2<PHYS>(n2[0], n2[1], n2[2], Y2, lane);
     __syncwarp();
-    const PHYS x = R - PHYS(a.f.centre[seg]);
     const float4 *cf = a.f.cf + (size_t)seg * a.f.n_entry;
     const double2 *cd = a.f.cd + (size_t)seg * a.f.n_entry * 2;
-    PHYS acc0 = PHYS(0), acc1 = PHYS(0), acc2 = PHYS(0);
-    PHYS C = PHYS(1), S = PHYS(0), pm = PHYS(1);
+    PHYS acc[S][3], C[S], Sn[S], qa[S], qb[S];
+#pragma unroll
+    for (int s = 0; s < S; ++s) {
+      acc[s][0] = acc[s][1] = acc[s][2] = PHYS(0);
+      C[s] = PHYS(1);
+      Sn[s] = PHYS(0);
+    }
+    PHYS pm = PHYS(1);
     int g = 0, e = 0, lm = 0;
-    const PHYS z1 = n1[2];
 #pragma unroll 1
     for (int m = 0; m <= CH4_L1; ++m) {
       if (m > 0) {
-        const PHYS c = C * n1[0] - S * n1[1];
-        S = C * n1[1] + S * n1[0];
-        C = c;
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+          const PHYS c = C[s] * n1[s][0] - Sn[s] * n1[s][1];
+          Sn[s] = C[s] * n1[s][1] + Sn[s] * n1[s][0];
+          C[s] = c;
+        }
         pm = -pm * sqrt(PHYS(2 * m - 1) / PHYS(2 * m));
       }
-      PHYS qa = PHYS(1), qb = PHYS(0);
+#pragma unroll
+      for (int s = 0; s < S; ++s) {
+        qa[s] = PHYS(1);
+        qb[s] = PHYS(0);
+      }
 #pragma unroll 1
       for (int l = m; l <= CH4_L1; ++l, ++lm) {
-        PHYS q;
-        if (l == m) q = PHYS(1);
-        else if (l == m + 1) q = sqrt(PHYS(2 * m + 1)) * z1;
-        else q = (PHYS(2 * l - 1) * z1 * qa - sqrt(PHYS((l - 1) * (l - 1) - m * m)) * qb) / sqrt(PHYS(l * l - m * m));
-        qb = qa;
-        qa = q;
-        const PHYS Yc = pm * C * q, Ys = pm * S * q;
+        const PHYS ca = PHYS(2 * l - 1), cb = sqrt(PHYS((l - 1) * (l - 1) - m * m));
+        const PHYS id = (l > m + 1) ? PHYS(1) / sqrt(PHYS(l * l - m * m)) : PHYS(0);
+        const PHYS c1 = sqrt(PHYS(2 * m + 1));
+        PHYS Yc[S], Ys[S];
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+          const PHYS z = n1[s][2];
+          const PHYS q = (l == m) ? PHYS(1) : (l == m + 1) ? c1 * z : (ca * z * qa[s] - cb * qb[s]) * id;
+          qb[s] = qa[s];
+          qa[s] = q;
+          Yc[s] = pm * C[s] * q;
+          Ys[s] = pm * Sn[s] * q;
+        }
         const int ng = __ldg(&a.f.gcount[lm]);
 #pragma unroll 1
         for (int gg = 0; gg < ng; ++gg, ++g) {
           const unsigned d = __ldg(&a.f.grp[g]);
           const int cnt = int(d >> 3);
-          PHYS s = PHYS(0);
-          if constexpr (sizeof(PHYS) == 4) {
-#pragma unroll 4
-            for (int i = 0; i < cnt; ++i) {
-              const float4 c4 = __ldg(&cf[e + i]);
-              const float v = c4.x + x * (c4.y + x * (c4.z + x * c4.w));
-              s += Y2[int(__ldg(&a.f.y2[e + i])) * 32 + lane] * v;
+          // per-power sums A_j = sum_e Y2_e c_je, collapsed by Horner at the end of the
+          // group; four entries' loads are issued before their arithmetic
+          PHYS A0[S], A1[S], A2[S], A3[S];
+#pragma unroll
+          for (int s = 0; s < S; ++s) A0[s] = A1[s] = A2[s] = A3[s] = PHYS(0);
+          int i = 0;
+#pragma unroll 1
+          for (; i + 4 <= cnt; i += 4) {
+            PHYS c[4][4];
+            int id[4];
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              if constexpr (sizeof(PHYS) == 4) {
+                const float4 c4 = __ldg(&cf[e + i + j]);
+                c[j][0] = c4.x; c[j][1] = c4.y; c[j][2] = c4.z; c[j][3] = c4.w;
+              } else {
+                const double2 lo = __ldg(&cd[2 * (e + i + j)]), hi = __ldg(&cd[2 * (e + i + j) + 1]);
+                c[j][0] = lo.x; c[j][1] = lo.y; c[j][2] = hi.x; c[j][3] = hi.y;
+              }
+              id[j] = int(__ldg(&a.f.y2[e + i + j]));
             }
-          } else {
-#pragma unroll 2
-            for (int i = 0; i < cnt; ++i) {
-              const double2 lo = __ldg(&cd[2 * (e + i)]), hi = __ldg(&cd[2 * (e + i) + 1]);
-              const double v = lo.x + x * (lo.y + x * (hi.x + x * hi.y));
-              s += Y2[int(__ldg(&a.f.y2[e + i])) * 32 + lane] * v;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              const V yv = Y2v[id[j] * 32];
+#pragma unroll
+              for (int s = 0; s < S; ++s) {
+                const PHYS y = vget(yv, s);
+                A0[s] += y * c[j][0];
+                A1[s] += y * c[j][1];
+                A2[s] += y * c[j][2];
+                A3[s] += y * c[j][3];
+              }
             }
           }
+#pragma unroll 1
+          for (; i < cnt; ++i) {
+            PHYS c0, c1_, c2, c3;
+            if constexpr (sizeof(PHYS) == 4) {
+              const float4 c4 = __ldg(&cf[e + i]);
+              c0 = c4.x; c1_ = c4.y; c2 = c4.z; c3 = c4.w;
+            } else {
+              const double2 lo = __ldg(&cd[2 * (e + i)]), hi = __ldg(&cd[2 * (e + i) + 1]);
+              c0 = lo.x; c1_ = lo.y; c2 = hi.x; c3 = hi.y;
+            }
+            const V yv = Y2v[int(__ldg(&a.f.y2[e + i])) * 32];
+#pragma unroll
+            for (int s = 0; s < S; ++s) {
+              const PHYS y = vget(yv, s);
+              A0[s] += y * c0;
+              A1[s] += y * c1_;
+              A2[s] += y * c2;
+              A3[s] += y * c3;
+            }
+          }
+          PHYS sum[S];
+#pragma unroll
+          for (int s = 0; s < S; ++s) sum[s] = A0[s] + x[s] * (A1[s] + x[s] * (A2[s] + x[s] * A3[s]));
           e += cnt;
-          const PHYS t = ((d & 1u) ? Ys : Yc) * s;
           const unsigned comp = (d >> 1) & 3u;
-          if (comp == 0) acc0 += t;
-          else if (comp == 1) acc1 += t;
-          else acc2 += t;
+#pragma unroll
+          for (int s = 0; s < S; ++s) {
+            const PHYS t = ((d & 1u) ? Ys[s] : Yc[s]) * sum[s];
+            if (comp == 0) acc[s][0] += t;
+            else if (comp == 1) acc[s][1] += t;
+            else acc[s][2] += t;
+          }
         }
       }
     }
-    if (seg == CH4_NSEG - 1) {
-      const PHYS i2 = iR * iR, i6 = i2 * i2 * i2;
-      acc0 *= i6;
-      acc1 *= i6;
-      acc2 *= i6;
-    }
-    if (mine >= 0) {
-      PHYS *o = static_cast<PHYS *>(a.mu) + (size_t)mine * 4;
 #pragma unroll
-      for (int i = 0; i < 3; ++i) o[i] = M[i][0] * acc0 + M[i][1] * acc1 + M[i][2] * acc2;
+    for (int s = 0; s < S; ++s) {
+      if (seg == CH4_NSEG - 1) {
+#pragma unroll
+        for (int c = 0; c < 3; ++c) acc[s][c] *= iR6[s];
+      }
+      if (mine[s] >= 0) {
+        PHYS *o = static_cast<PHYS *>(a.mu) + (size_t)mine[s] * 4;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) o[i] = M[s][i][0] * acc[s][0] + M[s][i][1] * acc[s][1] + M[s][i][2] * acc[s][2];
+      }
     }
     __syncwarp();
   }
