@@ -99,6 +99,8 @@ struct Ctx {
   int ch4_E = 0, ch4_G = 0;
   // MT19937 stream
   uint32_t *d_mt = nullptr;
+  unsigned short *d_mt_jump_seg = nullptr, *d_mt_jump_coarse = nullptr;  // jump-ahead tables
+  DevBuf<uint32_t> mt_seg_states;
   DevBuf<uint32_t> words[2];
   int cur = 0;
   long long wbase = 0, wvalid = 0, wpos = 0;
@@ -175,20 +177,39 @@ int check_params(const hh_calc_params *p) {
 }
 
 // make words [wpos, need_end) resident in words[cur]
+// blocks a request of nblk blocks generates: long requests go by whole segments
+long long mt_round_blocks(long long nblk) {
+  return nblk >= 2 * MT_SEG_BLOCKS ? (nblk + MT_SEG_BLOCKS - 1) / MT_SEG_BLOCKS * MT_SEG_BLOCKS : nblk;
+}
+
+// nblk (from mt_round_blocks) blocks of the stream into out, on stream s
+int gen_blocks(uint32_t *out, long long nblk, cudaStream_t s) {
+  if (nblk >= 2 * MT_SEG_BLOCKS) {
+    const int nseg = (int)(nblk / MT_SEG_BLOCKS);
+    CK(g.mt_seg_states.ensure((size_t)nseg * MT_N));
+    CK(launch_mt_generate_segments(g.d_mt, out, nseg, g.mt_seg_states.p, g.d_mt_jump_seg, g.d_mt_jump_coarse, s));
+    g_launches += 4;
+  } else {
+    CK(launch_mt_generate(g.d_mt, out, nblk, s));
+    g_launches += 1;
+  }
+  return HH_OK;
+}
+
 int ensure_words(long long need_end) {
   if (g.wbase <= g.wpos && g.wbase + g.wvalid >= need_end) return HH_OK;
   long long end_old = g.wbase + g.wvalid;
   long long left = std::max(0LL, end_old - g.wpos);
   long long gen = need_end - (g.wpos + left);
-  long long nblk = (gen + MT_N - 1) / MT_N + 1;
+  long long nblk = mt_round_blocks((gen + MT_N - 1) / MT_N + 1);
   int nxt = 1 - g.cur;
   CK(g.words[nxt].ensure((size_t)(left + nblk * MT_N)));
   if (left) {
     CK(cudaMemcpyAsync(g.words[nxt].p, g.words[g.cur].p + (g.wpos - g.wbase),
                        (size_t)left * sizeof(uint32_t), cudaMemcpyDeviceToDevice, g.st));
   }
-  CK(launch_mt_generate(g.d_mt, g.words[nxt].p + left, nblk, g.st));
-  g_launches += 1;
+  int rc = gen_blocks(g.words[nxt].p + left, nblk, g.st);
+  if (rc) return rc;
   g.cur = nxt;
   g.wbase = g.wpos;
   g.wvalid = left + nblk * MT_N;
@@ -217,7 +238,7 @@ int pregen_words(long long n) {
   const long long end_old = g.wbase + g.wvalid;
   const long long left = std::max(0LL, end_old - g.wpos);
   const long long gen = need_end - (g.wpos + left);
-  const long long nblk = (gen + MT_N - 1) / MT_N + 1;
+  const long long nblk = mt_round_blocks((gen + MT_N - 1) / MT_N + 1);
   const int nxt = 1 - g.cur;
   CK(g.words[nxt].ensure((size_t)(left + nblk * MT_N)));
   CK(cudaEventRecord(g.ev_sampled, g.st));
@@ -226,8 +247,8 @@ int pregen_words(long long n) {
     CK(cudaMemcpyAsync(g.words[nxt].p, g.words[g.cur].p + (g.wpos - g.wbase),
                        (size_t)left * sizeof(uint32_t), cudaMemcpyDeviceToDevice, g.st2));
   }
-  CK(launch_mt_generate(g.d_mt, g.words[nxt].p + left, nblk, g.st2));
-  g_launches += 1;
+  int rc = gen_blocks(g.words[nxt].p + left, nblk, g.st2);
+  if (rc) return rc;
   CK(cudaEventRecord(g.ev_pregen, g.st2));
   g.pregen_pending = true;
   g.cur = nxt;
@@ -711,6 +732,7 @@ int hh_cuda_init(int device, const hh_system_desc *sys) {
     CK(cudaDeviceGetAttribute(&g.num_sms, cudaDevAttrMultiProcessorCount, device));
     CK(cudaMalloc(&g.d_tab, sizeof(Co2arTablesGlobal)));
     CK(cudaMalloc(&g.d_mt, MT_N * sizeof(uint32_t)));
+    CK(upload_mt_jump_tables(&g.d_mt_jump_seg, &g.d_mt_jump_coarse));
     static Co2arTablesGlobal host_tab;
     build_tables(&host_tab);
     CK(cudaMemcpy(g.d_tab, &host_tab, sizeof host_tab, cudaMemcpyHostToDevice));
@@ -1262,6 +1284,9 @@ void hh_cuda_shutdown(void) {
   if (g.d_ch4_grp) cudaFree(g.d_ch4_grp);
   if (g.d_ch4_gcount) cudaFree(g.d_ch4_gcount);
   if (g.d_mt) cudaFree(g.d_mt);
+  if (g.d_mt_jump_seg) cudaFree(g.d_mt_jump_seg);
+  if (g.d_mt_jump_coarse) cudaFree(g.d_mt_jump_coarse);
+  g.mt_seg_states.release();
   for (auto &e : g.ev)
     if (e) cudaEventDestroy(e);
   if (g.st) cudaStreamDestroy(g.st);

@@ -23,6 +23,14 @@ struct SamplerExtra {
 // reference's operation order is kept)
 cudaError_t launch_mt_seed(uint32_t seed, uint32_t *state, cudaStream_t st);
 cudaError_t launch_mt_generate(uint32_t *state, uint32_t *out, long long n_blocks, cudaStream_t st);
+// n_seg segments of MT_SEG_BLOCKS blocks each from the current state (segment start
+// states found by jumping ahead; seg_states holds n_seg * 624 words); the state
+// advances past the last segment
+constexpr long long MT_SEG_BLOCKS = 2048;  // HH_MT_SEG_BLOCKS of hh_mt_jump.h
+cudaError_t launch_mt_generate_segments(uint32_t *state, uint32_t *out, int n_seg, uint32_t *seg_states,
+                                        const unsigned short *jump_seg, const unsigned short *jump_coarse,
+                                        cudaStream_t st);
+cudaError_t upload_mt_jump_tables(unsigned short **seg, unsigned short **coarse);
 cudaError_t launch_candidates(int sys, double mu, double II, double T, double Rmin, double Rmax,
                               double pesmin, int pair_state, const Co2arTablesGlobal *gtab,
                               const uint32_t *words, long long n_words, long long word_base, int D,

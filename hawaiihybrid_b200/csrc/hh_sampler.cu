@@ -15,6 +15,38 @@ cudaError_t launch_mt_generate(uint32_t *state, uint32_t *out, long long n_block
   return cudaGetLastError();
 }
 
+size_t mt_jump_smem() { return MT_JUMP_WIN * sizeof(uint32_t) + 10240 * sizeof(unsigned short); }
+
+cudaError_t launch_mt_generate_segments(uint32_t *state, uint32_t *out, int n_seg, uint32_t *seg_states,
+                                        const unsigned short *jump_seg, const unsigned short *jump_coarse,
+                                        cudaStream_t st) {
+  static_assert(HH_MT_JUMP_SEG_N <= 10240 && HH_MT_JUMP_COARSE_N <= 10240, "jump tables exceed the buffer");
+  const size_t smem = mt_jump_smem();
+  cudaError_t e = cudaFuncSetAttribute(mt_jump_chain_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  if (e != cudaSuccess) return e;
+  // segment 0 starts from the current state
+  e = cudaMemcpyAsync(seg_states, state, MT_N * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
+  if (e != cudaSuccess) return e;
+  const int n_coarse = (n_seg + HH_MT_COARSE - 1) / HH_MT_COARSE;
+  // coarse chain on one CTA: states 0, C, 2C, ...; then the fine chains of each interval
+  mt_jump_chain_kernel<<<1, MT_JUMP_THREADS, smem, st>>>(seg_states, 0, HH_MT_COARSE, n_coarse - 1, n_seg,
+                                                         jump_coarse, HH_MT_JUMP_COARSE_N);
+  mt_jump_chain_kernel<<<n_coarse, MT_JUMP_THREADS, smem, st>>>(seg_states, HH_MT_COARSE, 1, HH_MT_COARSE - 1,
+                                                                n_seg, jump_seg, HH_MT_JUMP_SEG_N);
+  mt_generate_segments_kernel<<<n_seg, 256, 0, st>>>(seg_states, out, n_seg, state);
+  return cudaGetLastError();
+}
+
+cudaError_t upload_mt_jump_tables(unsigned short **seg, unsigned short **coarse) {
+  cudaError_t e = cudaMalloc(seg, HH_MT_JUMP_SEG_N * sizeof(unsigned short));
+  if (e == cudaSuccess) e = cudaMalloc(coarse, HH_MT_JUMP_COARSE_N * sizeof(unsigned short));
+  if (e == cudaSuccess)
+    e = cudaMemcpy(*seg, hh_mt_jump_seg, sizeof hh_mt_jump_seg, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(*coarse, hh_mt_jump_coarse, sizeof hh_mt_jump_coarse, cudaMemcpyHostToDevice);
+  return e;
+}
+
 cudaError_t launch_candidates(int sys, double mu, double II, double T, double Rmin, double Rmax,
                               double pesmin, int pair_state, const Co2arTablesGlobal *gtab,
                               const uint32_t *words, long long n_words, long long word_base, int D,

@@ -21,6 +21,13 @@
 // A zero word at a Box-Muller position shifts every later candidate's window:
 // the candidate kernel reports the first such candidate and the host restarts
 // the following round right after it.
+//
+// Long requests of the stream (the 100 K rejection step of CH4-CO2 takes about
+// 1.5e9 words per call) are generated in segments of HH_MT_SEG_BLOCKS blocks, one
+// CTA each, from segment start states found by jumping ahead (hh_mt_jump.h):
+// a chain of coarse jumps (HH_MT_COARSE segments each) on one CTA, then the fine
+// jumps of every coarse interval in parallel.  The words are the same as those of
+// the sequential generator.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -28,6 +35,7 @@
 
 #include "hh_consts.h"
 #include "hh_internal.h"
+#include "hh_mt_jump.h"
 #include "hh_physics.cuh"
 #include "hh_traj.cuh"
 
@@ -62,6 +70,31 @@ __global__ void mt_seed_kernel(uint32_t seed, uint32_t *state) {
 
 // Advance the generator by n_blocks refreshes, writing 624 tempered words per
 // refresh to out.  One CTA of 256 threads; the state lives in shared memory.
+// one refresh of the 624 words in shared memory, in place (three dependency
+// phases); every thread of the CTA (>= 227 threads) calls it
+__device__ __forceinline__ void mt_refresh_smem(uint32_t *mt) {
+  const int tid = threadIdx.x;
+  uint32_t v;
+  if (tid < MT_N - MT_M) v = mt_twist(mt[tid], mt[tid + 1], mt[tid + MT_M]);
+  __syncthreads();
+  if (tid < MT_N - MT_M) mt[tid] = v;
+  __syncthreads();
+  {
+    int i = tid + (MT_N - MT_M);
+    if (tid < MT_N - MT_M) v = mt_twist(mt[i], mt[i + 1], mt[i - (MT_N - MT_M)]);
+    __syncthreads();
+    if (tid < MT_N - MT_M) mt[i] = v;
+    __syncthreads();
+  }
+  {
+    int i = tid + 2 * (MT_N - MT_M);
+    if (i < MT_N) v = mt_twist(mt[i], mt[(i + 1) % MT_N], mt[i - (MT_N - MT_M)]);
+    __syncthreads();
+    if (i < MT_N) mt[i] = v;
+    __syncthreads();
+  }
+}
+
 __global__ void __launch_bounds__(256) mt_generate_kernel(uint32_t *state, uint32_t *out,
                                                           long long n_blocks) {
   __shared__ uint32_t mt[MT_N];
@@ -96,6 +129,68 @@ __global__ void __launch_bounds__(256) mt_generate_kernel(uint32_t *state, uint3
   }
   __syncthreads();
   for (int i = threadIdx.x; i < MT_N; i += blockDim.x) state[i] = mt[i];
+}
+
+// Chains of jumps: CTA c starts from states[c * chain_stride] (a 624-word block
+// state) and writes the states `step`, 2 step, ... n_jumps * step segments later to
+// states[c * chain_stride + k * step], k = 1..n_jumps, stopping before index n_states.
+// One jump of J words (bits: set-bit positions of x^J mod phi) XORs windows of the
+// 19,937 + 623 stream words after the state, which are generated in shared memory.
+constexpr int MT_JUMP_WIN = 33 * MT_N;  // the state and the 32 blocks after it
+constexpr int MT_JUMP_THREADS = 640;
+__global__ void __launch_bounds__(MT_JUMP_THREADS) mt_jump_chain_kernel(uint32_t *states, int chain_stride,
+                                                                       int step, int n_jumps, int n_states,
+                                                                       const unsigned short *bits, int n_bits) {
+  extern __shared__ uint32_t jsm[];
+  uint32_t *win = jsm;                                         // MT_JUMP_WIN words
+  unsigned short *bs = reinterpret_cast<unsigned short *>(jsm + MT_JUMP_WIN);
+  for (int i = threadIdx.x; i < n_bits; i += blockDim.x) bs[i] = bits[i];
+  const long long base = (long long)blockIdx.x * chain_stride;
+  for (int i = threadIdx.x; i < MT_N; i += blockDim.x) win[i] = states[base * MT_N + i];
+  __syncthreads();
+  for (int k = 1; k <= n_jumps; ++k) {
+    const long long dst = base + (long long)k * step;
+    if (dst >= n_states) break;
+    // the 32 blocks after the state: block b + 1 from block b, refreshed in place in
+    // a copy at its own position
+    for (int b = 0; b < 32; ++b) {
+      uint32_t *cur = win + (b + 1) * MT_N;
+      for (int i = threadIdx.x; i < MT_N; i += blockDim.x) cur[i] = win[b * MT_N + i];
+      __syncthreads();
+      mt_refresh_smem(cur);
+    }
+    uint32_t acc = 0;
+    if (threadIdx.x < MT_N) {
+      const int j = threadIdx.x;
+#pragma unroll 4
+      for (int t = 0; t < n_bits; ++t) acc ^= win[bs[t] + j];
+    }
+    __syncthreads();
+    if (threadIdx.x < MT_N) {
+      win[threadIdx.x] = acc;
+      states[dst * MT_N + threadIdx.x] = acc;
+    }
+    __syncthreads();
+  }
+}
+
+// Segment s: HH_MT_SEG_BLOCKS blocks from states[s], tempered words to
+// out + s * HH_MT_SEG_BLOCKS * 624; the last segment's final block becomes the
+// generator state.
+__global__ void __launch_bounds__(256) mt_generate_segments_kernel(const uint32_t *states, uint32_t *out,
+                                                                   int n_seg, uint32_t *final_state) {
+  __shared__ uint32_t mt[MT_N];
+  const int s = blockIdx.x;
+  for (int i = threadIdx.x; i < MT_N; i += blockDim.x) mt[i] = states[(size_t)s * MT_N + i];
+  __syncthreads();
+  uint32_t *o = out + (size_t)s * HH_MT_SEG_BLOCKS * MT_N;
+  for (int b = 0; b < HH_MT_SEG_BLOCKS; ++b) {
+    mt_refresh_smem(mt);
+    for (int i = threadIdx.x; i < MT_N; i += blockDim.x) o[(size_t)b * MT_N + i] = mt_temper(mt[i]);
+  }
+  __syncthreads();
+  if (s == n_seg - 1)
+    for (int i = threadIdx.x; i < MT_N; i += blockDim.x) final_state[i] = mt[i];
 }
 
 struct SamplerArgs {

@@ -26,6 +26,18 @@ def test_mt_stream_bit_exact(lib):
     assert abs(out[:1].astype(np.float64)[0] * 2.0 ** -32 - O.mt_stream(1, 1)[0] * 2.0 ** -32) == 0
 
 
+@pytest.mark.parametrize("n", [3_000_000, 45_000_000])
+def test_mt_stream_segmented_bit_exact(lib, n):
+    """Long requests are generated in segments from jumped-ahead states (fine jumps only
+    for 3e6 words; coarse and fine jumps for 4.5e7): every word equals the sequential
+    stream of the oracle."""
+    lib_system("hear")
+    out = np.empty(n, dtype=np.uint32)
+    assert lib.hh_cuda_mt_stream(2066497031, n, out) == 0
+    ref = O.mt_stream(2066497031, n)
+    assert np.array_equal(out, ref)
+
+
 @pytest.mark.parametrize("name,seed,T,n", [("hear", 42, 300.0, 3000), ("co2ar", 7, 300.0, 3000),
                                            ("hear", 5, 100.0, 1000), ("co2ar", 11, 150.0, 1000)])
 def test_sampler_matches_oracle(name, seed, T, n):
