@@ -67,7 +67,7 @@ class CalcParamsC(C.Structure):
         ("sampler_Rmin", C.c_double), ("sampler_Rmax", C.c_double), ("pesmin", C.c_double),
         ("sampling_time", C.c_double), ("MaxTrajectoryLength", C.c_size_t), ("Rcut", C.c_double),
         ("cvode_tolerance", C.c_double), ("partial_partition_function_ratio", C.c_double),
-        ("mixed_tolerance", C.c_double), ("max_steps", C.c_long),
+        ("mixed_tolerance", C.c_double), ("max_steps", C.c_long), ("use_zimmermann_trick", C.c_int),
     ]
 
 

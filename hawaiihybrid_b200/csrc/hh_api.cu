@@ -125,6 +125,7 @@ struct Ctx {
   DevBuf<unsigned int> seg_cnt;
   DevBuf<long long> seg_w0;
   DevBuf<unsigned long long> rec_nfail;
+  DevBuf<int> zim_fail;  // Zimmermann estimate on the record path: dropped trajectories
   // M0
   DevBuf<double> m0_partials, m0_out;
   // FFT, and the CUDA graph of its kernel sequence for the current (N, dt, buffers)
@@ -173,10 +174,10 @@ int check_params(const hh_calc_params *p) {
   if (!(p->Rcut > 0) || !(p->cvode_tolerance > 0)) return HH_E_INVALID_ARGUMENT;
   if (p->pair_state < 1 || p->pair_state > 3) return HH_E_INVALID_ARGUMENT;
   if (p->MaxTrajectoryLength > (size_t)INT32_MAX) return HH_E_INVALID_ARGUMENT;
+  if (p->use_zimmermann_trick && p->pair_state != HH_PAIR_STATE_BOUND) return HH_E_INVALID_ARGUMENT;
   return HH_OK;
 }
 
-// make words [wpos, need_end) resident in words[cur]
 // blocks a request of nblk blocks generates: long requests go by whole segments
 long long mt_round_blocks(long long nblk) {
   return nblk >= 2 * MT_SEG_BLOCKS ? (nblk + MT_SEG_BLOCKS - 1) / MT_SEG_BLOCKS * MT_SEG_BLOCKS : nblk;
@@ -196,6 +197,7 @@ int gen_blocks(uint32_t *out, long long nblk, cudaStream_t s) {
   return HH_OK;
 }
 
+// make words [wpos, need_end) resident in words[cur]
 int ensure_words(long long need_end) {
   if (g.wbase <= g.wpos && g.wbase + g.wvalid >= need_end) return HH_OK;
   long long end_old = g.wbase + g.wvalid;
@@ -382,7 +384,7 @@ constexpr size_t CH4_RECORD_BUDGET = size_t(24) << 30;
 // Trajectories go through in chunks whose records fit CH4_RECORD_BUDGET.
 template <typename PHYS>
 int run_records_t(const TrajParams &P, const double *d_ic, uint64_t n, uint64_t per_iter,
-                  int precision, const double *d_satw, int n_sat, unsigned long long *cnt_dev) {
+                  int precision, const double *d_satw, int n_sat, unsigned long long *cnt_dev, bool zimm) {
   const int N = P.N;
   const int stride = 2 * N - 1;
   const size_t rec_b = HH_REC_WORDS * sizeof(PHYS), mu_b = 4 * sizeof(PHYS);
@@ -401,6 +403,7 @@ int run_records_t(const TrajParams &P, const double *d_ic, uint64_t n, uint64_t 
   CK(g.seg_w0.ensure(CH4_NSEG + 1));
   CK(g.rec_nfail.ensure(1));
   CK(cudaMemsetAsync(g.rec_nfail.p, 0, sizeof(unsigned long long), g.st));
+  if (zimm) CK(g.zim_fail.ensure(chunk));
   Ch4Co2Fold fold;
   fold.n_entry = g.ch4_E;
   fold.n_group = g.ch4_G;
@@ -479,9 +482,71 @@ int run_records_t(const TrajParams &P, const double *d_ic, uint64_t n, uint64_t 
     ca.n_sat = n_sat;
     ca.status_hist = g.status_hist.p;
     ca.n_failed = g.rec_nfail.p;
+    ca.fail_out = zimm ? g.zim_fail.p : nullptr;
+    ca.len_out = zimm ? g.rec_len.p : nullptr;
     ch4_corr_kernel<PHYS><<<(unsigned)((nc + 255) / 256), 256, 0, g.st>>>(P, ca);
     CK(cudaGetLastError());
     g_launches += 5;
+    if (zimm) {
+      ZimmArgs za;
+      za.series = g.rec_mu.p;
+      za.len = g.rec_len.p;
+      za.failed = g.zim_fail.p;
+      za.n_traj = (long long)nc;
+      za.traj_base = (long long)base;
+      za.traj_per_iter = (long long)per_iter;
+      za.stride = stride;
+      za.N = N;
+      za.w = 2.0 * P.weight / N;  // ppf ALU^3 / N
+      za.crln = g.crln.p;
+      zimm_kernel<PHYS><<<(unsigned)std::min<uint64_t>(nc, 16ull * g.num_sms), 256, 0, g.st>>>(za);
+      CK(cudaGetLastError());
+      g_launches += 1;
+    }
+  }
+  return HH_OK;
+}
+
+// Zimmermann estimate for the systems with an inline dipole: the trajectory kernel
+// writes the dipole vector of every stored sample, then zimm_kernel forms each
+// trajectory's lagged products.  Trajectories go through in chunks whose series fit
+// CH4_RECORD_BUDGET.  Dropped trajectories are skipped (no compensation pass).
+template <typename PHYS>
+int run_series_t(const TrajParams &P, const TrajIO &io0, const double *d_ic, uint64_t n, uint64_t per_iter,
+                 int precision) {
+  const int N = P.N;
+  const int stride = 2 * N - 1;
+  const size_t per_traj = (size_t)stride * 4 * sizeof(PHYS) + 2 * sizeof(int);
+  uint64_t chunk = std::max<uint64_t>(1, CH4_RECORD_BUDGET / per_traj);
+  chunk = std::min<uint64_t>(chunk, n);
+  CK(g.rec_mu.ensure((size_t)chunk * stride * 4 * sizeof(PHYS)));
+  CK(g.rec_len.ensure(2 * chunk));
+  for (uint64_t base = 0; base < n; base += chunk) {
+    const uint64_t nc = std::min<uint64_t>(chunk, n - base);
+    CK(cudaMemsetAsync(g.queue.p, 0, sizeof(unsigned int), g.st));
+    CK(cudaMemsetAsync(g.fail_flag.p, 0, nc * sizeof(int), g.st));
+    TrajIO io = io0;
+    io.ic = d_ic + base * g.QP;
+    io.n_items = (int)(2 * nc);
+    io.series = g.rec_mu.p;
+    io.rec_stride = stride;
+    io.rec_len = g.rec_len.p;
+    int rc = run_traj_dispatch(precision, P, io);
+    if (rc) return rc;
+    ZimmArgs za;
+    za.series = g.rec_mu.p;
+    za.len = g.rec_len.p;
+    za.failed = g.fail_flag.p;
+    za.n_traj = (long long)nc;
+    za.traj_base = (long long)base;
+    za.traj_per_iter = (long long)per_iter;
+    za.stride = stride;
+    za.N = N;
+    za.w = 2.0 * P.weight / N;  // ppf ALU^3 / N
+    za.crln = g.crln.p;
+    zimm_kernel<PHYS><<<(unsigned)std::min<uint64_t>(nc, 16ull * g.num_sms), 256, 0, g.st>>>(za);
+    CK(cudaGetLastError());
+    g_launches += 1;
   }
   return HH_OK;
 }
@@ -525,6 +590,7 @@ int run_trajectories(const hh_calc_params *p, const double *d_ic, uint64_t n, ui
   CK(cudaMemsetAsync(g.fail_flag.p, 0, n * sizeof(int), g.st));
   CK(cudaMemsetAsync(g.fail_count.p, 0, sizeof(int), g.st));
   TrajIO io;
+  memset(&io, 0, sizeof io);
   io.ic = d_ic;
   io.items = nullptr;
   io.n_items = (int)(2 * n);
@@ -550,15 +616,23 @@ int run_trajectories(const hh_calc_params *p, const double *d_ic, uint64_t n, ui
   }
   CK(cudaEventRecord(g.ev[2], g.st));
   int nfail = 0;
+  const bool zimm = p->use_zimmermann_trick != 0;
   if (g.sys == SYS_CH4CO2) {
     int rc = (precision == HH_PRECISION_MIXED)
-                 ? run_records_t<float>(P, d_ic, n, per_iter, precision, d_satw, n_sat, g.counters.p)
-                 : run_records_t<double>(P, d_ic, n, per_iter, precision, d_satw, n_sat, g.counters.p);
+                 ? run_records_t<float>(P, d_ic, n, per_iter, precision, d_satw, n_sat, g.counters.p, zimm)
+                 : run_records_t<double>(P, d_ic, n, per_iter, precision, d_satw, n_sat, g.counters.p, zimm);
     if (rc) return rc;
     unsigned long long nf = 0;
     CK(cudaMemcpyAsync(&nf, g.rec_nfail.p, sizeof nf, cudaMemcpyDeviceToHost, g.st));
     CK(cudaStreamSynchronize(g.st));
     nfail = (int)nf;
+  } else if (zimm) {
+    if (n_sat > 0) return HH_E_INVALID_ARGUMENT;
+    int rc = (precision == HH_PRECISION_MIXED) ? run_series_t<float>(P, io, d_ic, n, per_iter, precision)
+                                               : run_series_t<double>(P, io, d_ic, n, per_iter, precision);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(&nfail, g.fail_count.p, sizeof nfail, cudaMemcpyDeviceToHost, g.st));
+    CK(cudaStreamSynchronize(g.st));
   } else {
   int rc = run_traj_dispatch(precision, P, io);
   if (rc) return rc;
@@ -1266,6 +1340,7 @@ void hh_cuda_shutdown(void) {
   g.seg_cnt.release();
   g.seg_w0.release();
   g.rec_nfail.release();
+  g.zim_fail.release();
   g.m0_partials.release();
   g.m0_out.release();
   g.f_cf.release();

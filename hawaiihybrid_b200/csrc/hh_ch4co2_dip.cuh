@@ -391,6 +391,10 @@ struct Ch4CorrArgs {
   int n_sat;
   unsigned int *status_hist;
   unsigned long long *n_failed;
+  // check only (Zimmermann estimate): per trajectory 1 when dropped, and the stored
+  // samples per item cut at a soft injected failure, instead of adding into crln
+  int *fail_out;
+  int *len_out;
 };
 
 template <typename PHYS>
@@ -437,7 +441,13 @@ __global__ void __launch_bounds__(256) ch4_corr_kernel(TrajParams P, Ch4CorrArgs
       atomicAdd(&a.status_hist[st], 1u);
     }
     if (failed) atomicAdd(a.n_failed, 1ull);
+    if (a.fail_out) {
+      a.fail_out[t] = failed ? 1 : 0;
+      a.len_out[2 * t] = len[0];
+      a.len_out[2 * t + 1] = len[1];
+    }
   }
+  if (a.fail_out) return;
   const long long gt = a.traj_base + (live ? t : 0);
   const long long slice = (a.n_sat > 0) ? 0 : gt / a.traj_per_iter;
   const unsigned full = 0xffffffffu;
@@ -473,6 +483,54 @@ __global__ void __launch_bounds__(256) ch4_corr_kernel(TrajParams P, Ch4CorrArgs
           atomicAdd(&C[k], v);
         }
       }
+    }
+  }
+}
+
+// Zimmermann estimate (correlation_eval_zimmerman_trick, src/hawaii.c:1888-2114): per
+// trajectory the dipole vectors d[c], c = 0..2N-2, with d[N-1] = mu0, d[N-1+k] = mu(t_k)
+// and d[N-1-k] = mu(-t_k) (zero past a branch's stored samples), give
+//   C(s) += w sum_{c < N} d[c] . d[c+s],   w = ppf ALU^3 / N,
+// for trajectories that were not dropped.  One block per trajectory (grid-stride),
+// one lag per thread; the products are summed in FP64.
+struct ZimmArgs {
+  const void *series;         // [traj][slot][4] in the surface precision
+  const int *len;             // [2 traj] stored samples per branch
+  const int *failed;          // [traj] 1 when dropped
+  long long n_traj, traj_base, traj_per_iter;
+  int stride, N;
+  double w;
+  double *crln;
+};
+
+template <typename PHYS>
+__device__ __forceinline__ void zimm_d(const PHYS *sv, int N, int lf, int lb, int c, double d[3]) {
+  int slot = -1;
+  if (c == N - 1) slot = 0;
+  else if (c > N - 1) { if (c - (N - 1) <= lf) slot = c - (N - 1); }
+  else if ((N - 1) - c <= lb) slot = N - 1 + ((N - 1) - c);
+  if (slot < 0) { d[0] = d[1] = d[2] = 0.0; return; }
+  const PHYS *v = sv + (size_t)slot * 4;
+  d[0] = double(v[0]); d[1] = double(v[1]); d[2] = double(v[2]);
+}
+
+template <typename PHYS>
+__global__ void __launch_bounds__(256) zimm_kernel(ZimmArgs a) {
+  const int N = a.N;
+  for (long long t = blockIdx.x; t < a.n_traj; t += gridDim.x) {
+    if (a.failed[t]) continue;
+    const PHYS *sv = static_cast<const PHYS *>(a.series) + (size_t)t * a.stride * 4;
+    const int lf = a.len[2 * t], lb = a.len[2 * t + 1];
+    double *C = a.crln + ((a.traj_base + t) / a.traj_per_iter) * N;
+    for (int s = threadIdx.x; s < N; s += blockDim.x) {
+      double acc = 0.0;
+      for (int c = 0; c < N; ++c) {
+        double x[3], y[3];
+        zimm_d(sv, N, lf, lb, c, x);
+        zimm_d(sv, N, lf, lb, c + s, y);
+        acc += x[0] * y[0] + x[1] * y[1] + x[2] * y[2];
+      }
+      if (acc != 0.0) atomicAdd(&C[s], a.w * acc);
     }
   }
 }

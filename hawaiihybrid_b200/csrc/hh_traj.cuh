@@ -79,6 +79,10 @@ struct TrajIO {
   int *rec_status;            // [item]: end status of the integration
   double inv_I1[3];           // 1 / principal moments of CH4
   Ch4Co2Lj lj;
+  // Zimmermann estimate: the lab-frame dipole of every stored sample, 4 values of
+  // the surface precision per slot (slots as for records), instead of mu0 . mu(t_k)
+  // added into crln; rec_len receives the stored samples per item
+  void *series;
 };
 constexpr int HH_REC_WORDS = 12;  // r[3], q[4], u[3], padding
 
@@ -647,6 +651,12 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
 #pragma unroll
               for (int c = 0; c < Sys::NQ; ++c) rec[c] = PHYS(y_t[Sys::qidx(c)]);
             }
+          } else {
+            if (io.series && (item & 1) == 0) {
+              PHYS *sv = static_cast<PHYS *>(io.series) + (size_t)traj * io.rec_stride * 4;
+#pragma unroll
+              for (int c = 0; c < 3; ++c) sv[c] = mu_t[c];
+            }
           }
           nrhs += 2;
           t = 0.0;
@@ -786,6 +796,13 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
               sys.dipole(q, d);
               nan_[u] = isnan(d[0]) || isnan(d[1]) || isnan(d[2]);
               ws->res[jj] = ws->mu0[0][o] * d[0] + ws->mu0[1][o] * d[1] + ws->mu0[2][o] * d[2];
+              if (io.series) {
+                const int it = ws->item[o];
+                const size_t slot = (size_t)(it >> 1) * io.rec_stride + ((it & 1) ? P.N - 1 + kk : kk);
+                PHYS *sv = static_cast<PHYS *>(io.series) + slot * 4;
+#pragma unroll
+                for (int c = 0; c < 3; ++c) sv[c] = d[c];
+              }
             }
           }
         }
@@ -827,7 +844,7 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
             const int stop = (cut == 0xffffffffu) ? end_o : min(end_o, int(cut >> 3));
             const int chunk_end = min(end_o, base + m);
             if (j < stop) {
-              if (Sys::RECORDS) {
+              if (Sys::RECORDS || io.series) {
                 // written in (1)
               } else if (io.n_sat == 0) {
                 atomicAdd(&ws->crln[o][kks[u]], P.weight * double(val));
@@ -891,7 +908,8 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
       const int traj = item >> 1;
       // the t = 0 term is added by branches that are not dropped, so a replay
       // with the opposite weight removes exactly what a dropped trajectory added
-      if (!hard) {
+      if (io.series) io.rec_len[item] = k - 1;
+      if (!hard && !io.series) {
         const PHYS c0 = mu0[0] * mu0[0] + mu0[1] * mu0[1] + mu0[2] * mu0[2];
         if (io.n_sat == 0) {
           atomicAdd(&crln[0], P.weight * double(c0));

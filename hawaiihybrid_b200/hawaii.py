@@ -76,6 +76,8 @@ class CalcParams:
     satellite_temperatures: Sequence[float] = ()
     partial_partition_function_ratios: Sequence[float] = ()
     cf_filenames: Sequence[str] = ()
+    # correlation_eval_zimmerman_trick instead of correlation_eval (BOUND pairs only)
+    use_zimmermann_trick: bool = False
     # device-path knobs (no reference counterpart)
     mixed_tolerance: float = 1e-8
     max_steps: int = 50000
@@ -85,7 +87,7 @@ class CalcParams:
             int(self.ps), float(self.sampler_Rmin), float(self.sampler_Rmax), float(self.pesmin),
             float(self.sampling_time), int(self.MaxTrajectoryLength), float(self.Rcut),
             float(self.cvode_tolerance), float(self.partial_partition_function_ratio),
-            float(self.mixed_tolerance), int(self.max_steps))
+            float(self.mixed_tolerance), int(self.max_steps), int(bool(self.use_zimmermann_trick)))
 
 
 @dataclasses.dataclass

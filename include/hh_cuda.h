@@ -96,6 +96,10 @@ typedef struct {
     double partial_partition_function_ratio;
     double mixed_tolerance;         /* rtol = atol of the mixed path; 0 selects 1e-8 */
     long max_steps;                 /* internal steps between two samples; 0 selects 50000 */
+    int use_zimmermann_trick;       /* use_zimmermann_trick: C_i(s) = sum_{c<N} d[c].d[c+s] ALU^3 / N
+                                       over the dipole series of both branches
+                                       (correlation_eval_zimmerman_trick, src/hawaii.c:1888-2114);
+                                       only with HH_PAIR_STATE_BOUND (src/hawaii.c:2942-2945) */
 } hh_calc_params;
 
 typedef struct {

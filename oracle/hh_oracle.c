@@ -1261,8 +1261,19 @@ static void dense_eval(int n, const double *y_old, double F[7][NMAX], double x, 
 }
 
 /* one direction of correlation_eval: samples k = 1..N-1 of mu0 . mu(t_k) */
+static int half_traj_ex(const hho_system *sys, const hho_params *p, const double *y0,
+                        const double mu0[3], double *corr, double *vec, int vstep, hho_traj_stats *st,
+                        int *hard);
 static int half_traj(const hho_system *sys, const hho_params *p, const double *y0,
                      const double mu0[3], double *corr, hho_traj_stats *st, int *hard) {
+    return half_traj_ex(sys, p, y0, mu0, corr, NULL, 0, st, hard);
+}
+
+/* one direction of correlation_eval: samples k = 1..N-1 of mu0 . mu(t_k); with vec != NULL
+ * also the dipole vector of sample k at vec + 3 * k * vstep (vstep = +-1) */
+static int half_traj_ex(const hho_system *sys, const hho_params *p, const double *y0,
+                        const double mu0[3], double *corr, double *vec, int vstep, hho_traj_stats *st,
+                        int *hard) {
     integ I = {sys, hho_qp_size(sys), p->rtol, p->atol, 0};
     int n = I.n;
     double y[NMAX], f[NMAX], y_new[NMAX], K[16][NMAX], F[7][NMAX], ys[NMAX];
@@ -1301,6 +1312,7 @@ static int half_traj(const hho_system *sys, const hho_params *p, const double *y
                 if (ratio > 1e10) { status = HHO_ST_JUMP; *hard = 1; goto done; }
             }
             corr[k] = curr;
+            if (vec) for (int c = 0; c < 3; ++c) vec[3 * (long)k * vstep + c] = d[c];
             ++k;
             since = 0;
             if (ys[4] > p->Rcut) goto done;
@@ -1365,6 +1377,47 @@ int hho_correlation_parts(const hho_system *sys, const hho_params *p, const doub
     return st->failed;
 }
 
+/* correlation_eval_zimmerman_trick (src/hawaii.c:1888-2114): dipole vectors d[2N-1] with
+ * d[N-1] = mu0, d[N-1+k] = mu(t_k), d[N-1-k] = mu(-t_k) (zero past an exit), then
+ * crln[s] = sum_{c < N} d[c] . d[c+s] * ALU^3 / N.  A failure of either branch returns 1
+ * with crln zero, like the reference's return 1 */
+int hho_correlation_eval_zimmermann(const hho_system *sys, const hho_params *p, const double *qp0,
+                                    double *crln, hho_traj_stats *st) {
+    int n = hho_qp_size(sys);
+    size_t N = p->N;
+    double *d = calloc(3 * (2 * N - 1), sizeof(double));
+    double *tmp = calloc(N, sizeof(double));
+    memset(crln, 0, N * sizeof(double));
+    memset(st, 0, sizeof *st);
+    double q[8], mu0[3];
+    extract_q(sys, qp0, q);
+    hho_dipole(sys, q, mu0);
+    double *centre = d + 3 * (N - 1);
+    for (int c = 0; c < 3; ++c) centre[c] = mu0[c];
+    int hard = 0;
+    st->status_fwd = half_traj_ex(sys, p, qp0, mu0, tmp, centre, 1, st, &hard);
+    if (!hard) {
+        double y[NMAX];
+        memcpy(y, qp0, n * sizeof(double));
+        for (int i = 1; i < n; i += 2) y[i] = -y[i];
+        st->status_bwd = half_traj_ex(sys, p, y, mu0, tmp, centre, -1, st, &hard);
+    }
+    if (hard) {
+        st->failed = 1;
+    } else {
+        for (size_t s = 0; s < N; ++s) {
+            double acc = 0.0;
+            for (size_t c = 0; c < N; ++c)
+                acc += (d[3 * c] * d[3 * (c + s)] + d[3 * c + 1] * d[3 * (c + s) + 1] +
+                        d[3 * c + 2] * d[3 * (c + s) + 2]) * ALU * ALU * ALU;
+            crln[s] = acc / (double)N;
+        }
+    }
+    free(d);
+    free(tmp);
+    return st->failed;
+}
+
 int hho_propagate(const hho_system *sys, const hho_params *p, const double *qp0,
                   double t_end, double *qp_out, long *nsteps) {
     integ I = {sys, hho_qp_size(sys), p->rtol, p->atol, 0};
@@ -1403,6 +1456,7 @@ typedef struct {
     hho_traj_stats *stats;
     const double *w;   /* CORRELATION_ARRAY: [n][n_sat] weights, or NULL */
     int n_sat;
+    int zimmermann;
 } corr_job;
 
 static void *corr_worker(void *arg) {
@@ -1412,7 +1466,8 @@ static void *corr_worker(void *arg) {
     double *crln = malloc(N * sizeof(double));
     for (size_t i = J->begin; i < J->end; ++i) {
         hho_traj_stats st;
-        hho_correlation_eval(J->sys, J->p, J->qp0 + i * n, crln, &st);
+        if (J->zimmermann) hho_correlation_eval_zimmermann(J->sys, J->p, J->qp0 + i * n, crln, &st);
+        else hho_correlation_eval(J->sys, J->p, J->qp0 + i * n, crln, &st);
         if (J->w) {
             for (int s = 0; s < J->n_sat; ++s)
                 for (size_t k = 0; k < N; ++k) J->sum[s * N + k] += J->w[i * J->n_sat + s] * crln[k];
@@ -1434,7 +1489,7 @@ int hho_correlation_sum(const hho_system *sys, const hho_params *p, const double
     if (nthreads > 256) nthreads = 256;
     for (int w = 0; w < nthreads; ++w) {
         jobs[w] = (corr_job){sys, p, qp0, n * w / nthreads, n * (w + 1) / nthreads,
-                             calloc(N, sizeof(double)), stats, NULL, 0};
+                             calloc(N, sizeof(double)), stats, NULL, 0, p->zimmermann};
         pthread_create(&th[w], NULL, corr_worker, &jobs[w]);
     }
     memset(crln_sum, 0, N * sizeof(double));

@@ -57,6 +57,7 @@ typedef struct {
     double rtol, atol;       /* integrator tolerances (cvode_tolerance) */
     double ppf_ratio;        /* partial_partition_function_ratio */
     long max_steps;          /* internal steps allowed between two samples */
+    int zimmermann;          /* use_zimmermann_trick: hho_correlation_sum uses the Zimmermann estimate */
 } hho_params;
 
 typedef struct {
@@ -120,6 +121,9 @@ long hho_sample(uint32_t seed, const hho_system *sys, const hho_params *p, doubl
 /* ---- integrator + correlation_eval (hawaii.c:2116-2347) ---- */
 int hho_correlation_eval(const hho_system *sys, const hho_params *p, const double *qp0,
                          double *crln, hho_traj_stats *st);
+/* correlation_eval_zimmerman_trick (src/hawaii.c:1888-2114) */
+int hho_correlation_eval_zimmermann(const hho_system *sys, const hho_params *p, const double *qp0,
+                                    double *crln, hho_traj_stats *st);
 /* both branches separately (mu0.mu(t_k), no ALU^3 / 2 scaling, no dropping) */
 int hho_correlation_parts(const hho_system *sys, const hho_params *p, const double *qp0,
                           double *fw, double *bw, hho_traj_stats *st);

@@ -30,7 +30,7 @@ class Params(C.Structure):
         ("Rmin", C.c_double), ("Rmax", C.c_double), ("pesmin", C.c_double),
         ("sampling_time", C.c_double), ("N", C.c_size_t), ("Rcut", C.c_double),
         ("rtol", C.c_double), ("atol", C.c_double), ("ppf_ratio", C.c_double),
-        ("max_steps", C.c_long),
+        ("max_steps", C.c_long), ("zimmermann", C.c_int),
     ]
 
 
@@ -103,6 +103,8 @@ def lib():
         L.hho_array_weights.argtypes = [C.c_int, C.c_double, C.c_double, _dp, C.c_int, C.c_double, _dp]
         L.hho_correlation_sum_array.argtypes = [C.POINTER(System), C.POINTER(Params), _dp, C.c_size_t, C.c_int,
                                                 _dp, C.c_int, _dp]
+        L.hho_correlation_eval_zimmermann.argtypes = [C.POINTER(System), C.POINTER(Params), _dp, _dp,
+                                                      C.POINTER(TrajStats)]
         L.hho_ch4co2_lab_to_kal.argtypes = [_dp, _dp]
         L.hho_ch4co2_dipole_kal.argtypes = [_dp, _dp]
         L.hho_ch4co2_V_lab.restype = C.c_double
@@ -142,6 +144,14 @@ def correlation_eval(sysd, params, qp0):
     st = TrajStats()
     lib().hho_correlation_eval(C.byref(sysd), C.byref(params), np.ascontiguousarray(qp0, dtype=np.float64),
                                crln, C.byref(st))
+    return crln, st
+
+
+def correlation_eval_zimmermann(sysd, params, qp0):
+    crln = np.zeros(params.N, dtype=np.float64)
+    st = TrajStats()
+    lib().hho_correlation_eval_zimmermann(C.byref(sysd), C.byref(params),
+                                          np.ascontiguousarray(qp0, dtype=np.float64), crln, C.byref(st))
     return crln, st
 
 

@@ -33,7 +33,7 @@ def test_library_exports_every_declared_symbol():
 def test_struct_layouts_match_header():
     from hawaiihybrid_b200 import _lib
     assert C.sizeof(_lib.SystemDesc) == 4 + 4 + 8 + 4 + 4 + 48
-    assert C.sizeof(_lib.CalcParamsC) == 8 + 8 * 4 + 8 + 8 * 4 + 8
+    assert C.sizeof(_lib.CalcParamsC) == 8 + 8 * 4 + 8 + 8 * 4 + 8 + 8   # ... max_steps, use_zimmermann_trick
     assert C.sizeof(_lib.Stats) == 8 * 8 + 8 * 8 + 3 * 8 + 8
 
 
