@@ -17,6 +17,7 @@
 #include "hh_fft.cuh"
 #include "hh_internal.h"
 #include "hh_m0.cuh"
+#include "hh_prmu.cuh"
 #include "hh_traj.cuh"
 
 namespace hh {
@@ -126,6 +127,9 @@ struct Ctx {
   DevBuf<long long> seg_w0;
   DevBuf<unsigned long long> rec_nfail;
   DevBuf<int> zim_fail;  // Zimmermann estimate on the record path: dropped trajectories
+  // PR_MU: complex series (two buffers) and the spectrum
+  DevBuf<double2> pm_a, pm_b;
+  DevBuf<double> pm_sf;
   // M0
   DevBuf<double> m0_partials, m0_out;
   // FFT, and the CUDA graph of its kernel sequence for the current (N, dt, buffers)
@@ -560,6 +564,7 @@ int run_trajectories(const hh_calc_params *p, const double *d_ic, uint64_t n, ui
   // C(t) slices: one per iteration, or one per satellite temperature
   const uint64_t n_iter = (n_sat > 0) ? (uint64_t)n_sat : (n + per_iter - 1) / per_iter;
   TrajParams P;
+  memset(&P, 0, sizeof P);
   P.mu = g.mu;
   P.II = g.II;
   P.dt = p->sampling_time;
@@ -992,6 +997,165 @@ int hh_cuda_correlation_temperatures(const hh_calc_params *p, const double *T, i
   return HH_OK;
 }
 
+int hh_cuda_prmu(const hh_calc_params *p, double T, double R0, double approx_freq_max, int allow_truncating,
+                 uint32_t seed, uint64_t n_traj, int precision_mode, double *nu, double *sf, size_t sf_len,
+                 size_t *n_freq, double *ntraj, hh_stats *stats) {
+  if (!g.init) return HH_E_NOT_INITIALIZED;
+  if (g.sys == SYS_CH4CO2) return HH_E_UNSUPPORTED_SYSTEM;
+  int rc = check_params(p);
+  if (rc) return rc;
+  if (!(T > 0) || !(R0 > 0) || !(approx_freq_max > 0) || !nu || !sf || !n_freq || n_traj == 0 ||
+      n_traj > (uint64_t)(INT32_MAX / 2))
+    return HH_E_INVALID_ARGUMENT;
+  if (precision_mode != HH_PRECISION_FP64 && precision_mode != HH_PRECISION_MIXED)
+    return HH_E_INVALID_ARGUMENT;
+  const size_t N = p->MaxTrajectoryLength;
+  if (N < 2 || (N & (N - 1))) return HH_E_NOT_POWER_OF_TWO;  // gsl_fft_real_radix2_transform
+  const double dt = p->sampling_time;
+  // frequency grid (src/hawaii.c:3189-3200)
+  const double step = 1.0 / (dt * HH_ATU) / HH_LIGHTSPEED_CM / (double)N;
+  const double fmax_theory = 1.0 / (HH_LIGHTSPEED_CM * dt * HH_ATU) / 2.0;
+  if (approx_freq_max > fmax_theory) return HH_E_INVALID_ARGUMENT;
+  const size_t L = (size_t)(int)(approx_freq_max / step) + 1;
+  *n_freq = L;
+  if (sf_len < L) return HH_E_INVALID_ARGUMENT;
+  CK(cudaSetDevice(g.device));
+  if (seed > 0) {
+    rc = reseed(seed);
+    if (rc) return rc;
+  }
+  hh_stats local;
+  memset(&local, 0, sizeof local);
+  g_launches = 0;
+  // draws: q_generator, R := R0, p_generator, inward pR; one word fewer than a candidate
+  CK(g.qp0.ensure(n_traj * g.QP));
+  CK(cudaEventRecord(g.ev[0], g.st));
+  const int D0 = g.D;
+  const double pa0 = g.p_accept;
+  g.D = D0 - 1;
+  g.sx.prmu_R0 = R0;
+  g.p_accept = 1.0;
+  uint64_t ncand = 0;
+  rc = sample_into(p, T, n_traj, g.qp0.p, &ncand);
+  g.D = D0;
+  g.sx.prmu_R0 = 0.0;
+  g.p_accept = pa0;
+  if (rc) return rc;
+  CK(cudaEventRecord(g.ev[1], g.st));
+  // forward branches with samples k = 1..N at t = k dt, ending after R > R0
+  TrajParams P;
+  memset(&P, 0, sizeof P);
+  P.mu = g.mu;
+  P.II = g.II;
+  P.dt = dt;
+  P.N = (int)N + 1;
+  P.Rcut = R0;
+  const double tol = (precision_mode == HH_PRECISION_MIXED)
+                         ? (p->mixed_tolerance > 0 ? p->mixed_tolerance : 1e-8)
+                         : p->cvode_tolerance;
+  P.rtol = P.atol = tol;
+  P.max_steps = p->max_steps > 0 ? p->max_steps : 50000;
+  P.max_total_steps = 4000000;
+  P.noise_floor = 16.0 * 5.96e-8;
+  P.inject_item = P.inject_k = -1;
+  P.prmu = 1;
+  const int stride = (int)N + 1;
+  const size_t ps = (precision_mode == HH_PRECISION_MIXED) ? sizeof(float) : sizeof(double);
+  const size_t per_traj = (size_t)stride * 4 * ps + 2 * 2 * N * sizeof(double2) + 4 * sizeof(int);
+  const uint64_t chunk = std::min<uint64_t>(n_traj, std::max<uint64_t>(1, CH4_RECORD_BUDGET / per_traj));
+  CK(g.rec_mu.ensure((size_t)chunk * stride * 4 * ps));
+  CK(g.rec_len.ensure(2 * chunk));
+  CK(g.rec_status.ensure(2 * chunk));
+  CK(g.pm_a.ensure(2 * chunk * N));
+  CK(g.pm_b.ensure(2 * chunk * N));
+  CK(g.pm_sf.ensure(L));
+  CK(g.counters.ensure(16));
+  CK(g.status_hist.ensure(2 * HH_ST_COUNT));
+  CK(g.queue.ensure(1));
+  CK(g.rec_nfail.ensure(1));
+  CK(cudaMemsetAsync(g.pm_sf.p, 0, L * sizeof(double), g.st));
+  CK(cudaMemsetAsync(g.counters.p, 0, 16 * sizeof(unsigned long long), g.st));
+  CK(cudaMemsetAsync(g.rec_nfail.p, 0, sizeof(unsigned long long), g.st));
+  CK(cudaEventRecord(g.ev[2], g.st));
+  const double sf_coeff = HH_HARTREE * pow(HH_ALU, 6) * HH_ATU * R0 * R0 * dt * dt;
+  for (uint64_t base = 0; base < n_traj; base += chunk) {
+    const uint64_t nc = std::min<uint64_t>(chunk, n_traj - base);
+    CK(cudaMemsetAsync(g.queue.p, 0, sizeof(unsigned int), g.st));
+    TrajIO io;
+    memset(&io, 0, sizeof io);
+    io.ic = g.qp0.p + base * g.QP;
+    io.n_items = (int)nc;
+    io.fwd_only = 1;
+    io.queue = g.queue.p;
+    io.crln = g.pm_sf.p;
+    io.counters = g.counters.p;
+    io.status_hist = g.status_hist.p + HH_ST_COUNT;  // the records' statuses are counted below
+    io.traj_per_iter = (long long)n_traj;
+    io.series = g.rec_mu.p;
+    io.rec_stride = stride;
+    io.rec_len = g.rec_len.p;
+    io.rec_status = g.rec_status.p;
+    io.dipnet = g.d_n2ar_fold;
+    io.pesnet = (precision_mode == HH_PRECISION_MIXED) ? (const void *)g.d_n2ar_pes_f : (const void *)g.d_n2ar_pes_d;
+    rc = run_traj_dispatch(precision_mode, P, io);
+    if (rc) return rc;
+    PrmuPackArgs pa;
+    pa.series = g.rec_mu.p;
+    pa.len = g.rec_len.p;
+    pa.status = g.rec_status.p;
+    pa.qp = g.qp0.p + base * g.QP;
+    pa.QP = g.QP;
+    pa.n_traj = (long long)nc;
+    pa.N = (int)N;
+    pa.stride = stride;
+    pa.allow_trunc = allow_truncating ? 1 : 0;
+    pa.coeff = sf_coeff / g.mu;
+    pa.z = g.pm_a.p;
+    pa.counted = g.rec_nfail.p;
+    const long long tot = (long long)nc * (long long)N;
+    if (precision_mode == HH_PRECISION_MIXED)
+      prmu_pack_kernel<float><<<(unsigned)((tot + 255) / 256), 256, 0, g.st>>>(pa);
+    else
+      prmu_pack_kernel<double><<<(unsigned)((tot + 255) / 256), 256, 0, g.st>>>(pa);
+    CK(cudaGetLastError());
+    const long long B = 2 * (long long)nc;
+    double2 *x = g.pm_a.p, *y = g.pm_b.p;
+    for (long long s = 1; s < (long long)N; s *= 2) {
+      stockham_batch_kernel<<<(unsigned)((B * ((long long)N / 2) + 255) / 256), 256, 0, g.st>>>(x, y, (long long)N, s, B);
+      std::swap(x, y);
+    }
+    prmu_accum_kernel<<<(unsigned)((L + 255) / 256), 256, 0, g.st>>>(x, B, (int)N, (int)L, g.pm_sf.p);
+    CK(cudaGetLastError());
+    g_launches += 2 + (unsigned long long)__builtin_ctzll((unsigned long long)N);  // pack, accumulate, passes
+  }
+  CK(cudaEventRecord(g.ev[3], g.st));
+  unsigned long long counted = 0;
+  unsigned long long cnt[8];
+  CK(cudaMemcpyAsync(sf, g.pm_sf.p, L * sizeof(double), cudaMemcpyDeviceToHost, g.st));
+  CK(cudaMemcpyAsync(&counted, g.rec_nfail.p, sizeof counted, cudaMemcpyDeviceToHost, g.st));
+  CK(cudaMemcpyAsync(cnt, g.counters.p, sizeof cnt, cudaMemcpyDeviceToHost, g.st));
+  CK(cudaStreamSynchronize(g.st));
+  for (size_t i = 0; i < L; ++i) nu[i] = step * (double)i;
+  if (ntraj) *ntraj = (double)counted;
+  float ms = 0.f;
+  local.n_candidates = ncand;
+  local.n_accepted = n_traj;
+  local.n_steps = cnt[0];
+  local.n_rejected_steps = cnt[1];
+  local.n_rhs = cnt[2];
+  local.n_samples = cnt[3];
+  local.n_failed = n_traj - counted;
+  CK(cudaEventElapsedTime(&ms, g.ev[0], g.ev[1]));
+  local.sample_ms = ms;
+  CK(cudaEventElapsedTime(&ms, g.ev[2], g.ev[3]));
+  local.traj_ms = ms;
+  CK(cudaEventElapsedTime(&ms, g.ev[0], g.ev[3]));
+  local.total_ms = ms;
+  local.n_kernel_launches = g_launches;
+  if (stats) *stats = local;
+  return HH_OK;
+}
+
 int hh_cuda_correlation_array(const hh_calc_params *p, double base_T, const double *sat_T,
                               const double *ppf_ratios, int n_sat, uint32_t seed, uint64_t n_accept,
                               int precision_mode, double *crln_sums, double *nstar, double *ntraj,
@@ -1341,6 +1505,9 @@ void hh_cuda_shutdown(void) {
   g.seg_w0.release();
   g.rec_nfail.release();
   g.zim_fail.release();
+  g.pm_a.release();
+  g.pm_b.release();
+  g.pm_sf.release();
   g.m0_partials.release();
   g.m0_out.release();
   g.f_cf.release();

@@ -17,6 +17,9 @@ constexpr int SAT_MAX = 64;  // satellite temperatures of one CORRELATION_ARRAY 
 struct SamplerExtra {
   double II1[3];
   Ch4Co2Lj lj;
+  // PR_MU draws (R0 > 0): R := R0 before the momenta, pR made inward, no rejection
+  // step and no pair-state filter (src/hawaii.c:3566-3573)
+  double prmu_R0;
 };
 
 // sampler (hh_sampler.cu, compiled without floating-point contraction so the

@@ -313,6 +313,8 @@ __global__ void __launch_bounds__(256) candidate_kernel(
     qp[6] = mt_d(words, pos) * 2.0 * HH_PI;
     qp[8] = acos(2.0 * mt_d(words, pos) - 1.0);
   }
+  const bool prmu = a.x.prmu_R0 > 0.0;
+  if (prmu) qp[4] = a.x.prmu_R0;
   // p_generator (src/hawaii.c:1292-1380)
   double sqrt_MUKT = sqrt(a.mu / HH_HKT * T);
   double sinTheta = sin(qp[2]);
@@ -350,10 +352,13 @@ __global__ void __launch_bounds__(256) candidate_kernel(
     qp[7] = sqrt_IIKT * sin_theta * m1;
     qp[9] = sqrt_IIKT * m0;
   }
-  if (pos + 1 > limit) overrun = true;
+  if (!prmu && pos + 1 > limit) overrun = true;
   bool acc = false;
   double E = 0.0;
-  if (!overrun) {
+  if (prmu) {
+    if (qp[5] > 0.0) qp[5] = -qp[5];
+    acc = !overrun;
+  } else if (!overrun) {
     // Hamiltonian, then reject() (src/hawaii.c:1382-1421), then the filter (2981-2994)
     double kin = kinetic(a, qp);
     double pot = potential(a, tb, qp);

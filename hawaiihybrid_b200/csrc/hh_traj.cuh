@@ -51,6 +51,9 @@ struct TrajParams {
   // FP32 stages only: rounding-noise level of the stage derivatives, in units
   // of their magnitude, added to the error tolerance
   double noise_floor;
+  // PR_MU samples (src/hawaii.c:3661-3688): a NaN dipole leaves its sample at zero
+  // and no other per-sample test runs; the branch ends after R > Rcut
+  int prmu;
 };
 
 struct TrajIO {
@@ -83,6 +86,7 @@ struct TrajIO {
   // the surface precision per slot (slots as for records), instead of mu0 . mu(t_k)
   // added into crln; rec_len receives the stored samples per item
   void *series;
+  int fwd_only;               // items are the forward branches only (item = 2 * index)
 };
 constexpr int HH_REC_WORDS = 12;  // r[3], q[4], u[3], padding
 
@@ -610,6 +614,7 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
   int k = 1;
   int since = 0, total = 0;
   bool rejected = false;
+  bool exited = false;  // the item ended by R > Rcut
   unsigned long long t_begin = 0ull;
   unsigned s0 = 0, m0 = 0;
   for (;;) {
@@ -624,7 +629,7 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
       if (need) {
         const unsigned idx = base + __popc(needmask & ((1u << lane) - 1u));
         if (idx < (unsigned)io.n_items) {
-          item = io.items ? io.items[idx] : (int)idx;
+          item = io.items ? io.items[idx] : (io.fwd_only ? 2 * (int)idx : (int)idx);
           const int traj = item >> 1;
           crln = io.crln + (size_t)(traj / io.traj_per_iter) * (size_t)P.N;
           satw = io.sat_w ? io.sat_w + (size_t)traj * io.n_sat : nullptr;
@@ -663,6 +668,7 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
           k = 1;
           since = total = 0;
           rejected = false;
+          exited = false;
           prev = curr = PHYS(0);
         } else {
           item = -2;
@@ -800,9 +806,11 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
                 const int it = ws->item[o];
                 const size_t slot = (size_t)(it >> 1) * io.rec_stride + ((it & 1) ? P.N - 1 + kk : kk);
                 PHYS *sv = static_cast<PHYS *>(io.series) + slot * 4;
+                const bool zero = P.prmu && nan_[u];
 #pragma unroll
-                for (int c = 0; c < 3; ++c) sv[c] = d[c];
+                for (int c = 0; c < 3; ++c) sv[c] = zero ? PHYS(0) : d[c];
               }
+              if (P.prmu && nan_[u]) out_[u] = false;
             }
           }
         }
@@ -816,8 +824,8 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
             const int j = base + jj;
             const PHYS val = ws->res[jj];
             unsigned code = 0xffffffffu;
-            if (Sys::RECORDS) {
-              // a record's dipole checks run after the batched evaluation
+            if (Sys::RECORDS || P.prmu) {
+              // a record's dipole checks run after the batched evaluation; PR_MU has none
               if (out_[u]) code = (unsigned(j + 1) << 3);
             } else if (nan_[u]) code = (unsigned(j) << 3) | 1u;
             else if (ws->item[o] == P.inject_item && kks[u] == P.inject_k) code = (unsigned(j) << 3) | 4u;
@@ -873,7 +881,7 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
         }
         if (cut != 0xffffffffu) {
           switch (cut & 7u) {
-            case 0: status = HH_ST_OK; break;  // R > Rcut
+            case 0: status = HH_ST_OK; exited = true; break;  // R > Rcut
             case 1: status = HH_ST_NAN_DIPOLE; hard = 1; break;
             case 2: status = HH_ST_OVERFLOW; hard = 1; break;
             case 3: status = HH_ST_JUMP; hard = 1; break;
@@ -908,7 +916,10 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
       const int traj = item >> 1;
       // the t = 0 term is added by branches that are not dropped, so a replay
       // with the opposite weight removes exactly what a dropped trajectory added
-      if (io.series) io.rec_len[item] = k - 1;
+      if (io.series) {
+        io.rec_len[item] = k - 1;
+        if (io.rec_status) io.rec_status[item] = status | (exited ? 16 : 0);
+      }
       if (!hard && !io.series) {
         const PHYS c0 = mu0[0] * mu0[0] + mu0[1] * mu0[1] + mu0[2] * mu0[2];
         if (io.n_sat == 0) {

@@ -227,6 +227,45 @@ def correlation_temperatures(ms: MoleculeSystem, params: CalcParams, temperature
     return crln.reshape(T.size, -1), ntraj, st
 
 
+def prmu_iteration(ms: MoleculeSystem, params: CalcParams, Temperature: float, R0: float, n: int,
+                   approximate_frequency_max: float, allow_truncating: bool = False,
+                   precision: int = PRECISION_FP64, seed: int = 0):
+    """One pass of calculate_spectral_function_using_prmu_representation_and_save
+    (src/hawaii.c:3148-3978): returns (nu, sum over counted trajectories of
+    SF_COEFF pR/mu sum_c |F_c|^2, counted trajectories, stats)."""
+    L = _bind(ms)
+    N = int(params.MaxTrajectoryLength)
+    cap = N // 2 + 2
+    nu = np.zeros(cap)
+    sf = np.zeros(cap)
+    nf = C.c_size_t()
+    ntraj = C.c_double()
+    st = _lib.Stats()
+    pc = params.to_c()
+    check(L.hh_cuda_prmu(C.byref(pc), Temperature, R0, approximate_frequency_max, int(allow_truncating), seed, n,
+                         precision, nu, sf, cap, C.byref(nf), C.byref(ntraj), C.byref(st)))
+    k = nf.value
+    return nu[:k], sf[:k], ntraj.value, st
+
+
+def calculate_spectral_function_using_prmu_representation(ms: MoleculeSystem, params: CalcParams,
+                                                           Temperature: float, R0: float,
+                                                           approximate_frequency_max: float,
+                                                           allow_truncating: bool = False,
+                                                           precision: int = PRECISION_FP64) -> SFnc:
+    """The PR_MU spectral function over params.niterations passes of
+    params.total_trajectories / params.niterations trajectories, divided by the trajectories
+    counted (src/hawaii.c:3974-3977)."""
+    per = max(1, int(params.total_trajectories) // max(1, int(params.niterations)))
+    total, nt, nu = None, 0.0, None
+    for it in range(max(1, int(params.niterations))):
+        nu, sf, c, _ = prmu_iteration(ms, params, Temperature, R0, per, approximate_frequency_max,
+                                      allow_truncating, precision, seed=ms.seed if it == 0 else 0)
+        total = sf if total is None else total + sf
+        nt += c
+    return SFnc(nu=nu, data=total / nt, ntraj=nt, Temperature=Temperature, normalized=True)
+
+
 def correlation_from_initial_conditions(ms: MoleculeSystem, params: CalcParams, qp0: np.ndarray,
                                         precision: int = PRECISION_FP64):
     """correlation_eval + accumulation over caller-supplied phase points."""

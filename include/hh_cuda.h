@@ -156,6 +156,20 @@ int hh_cuda_correlation_temperatures(const hh_calc_params *p, const double *T, i
                                      uint64_t n_per_T, int precision_mode, double *crln_sums,
                                      double *ntraj, hh_stats *stats);
 
+/* PR_MU spectral function (calculate_spectral_function_using_prmu_representation_and_save,
+ * src/hawaii.c:3148-3978) for monomers without requantization: n_traj phase points drawn as
+ * q_generator, R := R0, p_generator with pR made inward (no rejection step); each trajectory
+ * is integrated forward with the dipole sampled at t = (k+1) dt, k = 0..N-1, until R > R0;
+ * its Connes-apodized dipole components are Fourier transformed and
+ * sf[i] = sum SF_COEFF pR/mu sum_c |F_c(i)|^2 on nu[i] = i / (dt ATU c N) (cm^-1) for the
+ * *n_freq = (int)(approx_freq_max / step) + 1 frequencies (sf_len must hold them).  A
+ * trajectory whose integration fails, or that is still inside R0 after N samples (unless
+ * allow_truncating), is skipped; *ntraj counts the others (divide sf by it, as the reference's
+ * final loop does).  N must be a power of two.  Not available for CH4-CO2. */
+int hh_cuda_prmu(const hh_calc_params *p, double T, double R0, double approx_freq_max, int allow_truncating,
+                 uint32_t seed, uint64_t n_traj, int precision_mode, double *nu, double *sf, size_t sf_len,
+                 size_t *n_freq, double *ntraj, hh_stats *stats);
+
 /* CORRELATION_ARRAY: n_accept trajectories sampled at base_T, each added to the
  * C(t) of every satellite temperature sat_T[s] with the reference's reweighting
  * w = exp(-E HkT / base_T / T (base_T - T)) / WTT (0 for free pairs above base_T)

@@ -1030,9 +1030,10 @@ static double generate_normal(hho_mt *s, int *draws) {
     }
 }
 
-int hho_candidate(hho_mt *s, const hho_system *sys, const hho_params *p, double T,
-                  double *qp, double *energy, int *draws) {
-    *draws = 0;
+/* q_generator + p_generator (hawaii.c:1232-1380); R0 > 0 replaces the drawn R before the
+ * momenta, as the PR_MU loop does (hawaii.c:3566-3567) */
+static void gen_qp(hho_mt *s, const hho_system *sys, const hho_params *p, double T, double *qp, int *draws,
+                   double R0) {
     double RMIN = p->Rmin, RMAX = p->Rmax;
     /* q_generator */
     double R3 = hho_mt_drand(s) * (RMAX * RMAX * RMAX - RMIN * RMIN * RMIN) + RMIN * RMIN * RMIN;
@@ -1053,6 +1054,7 @@ int hho_candidate(hho_mt *s, const hho_system *sys, const hho_params *p, double 
         qp[14] = acos(2.0 * hho_mt_drand(s) - 1.0);
         *draws += 5;
     }
+    if (R0 > 0) qp[4] = R0;
     /* p_generator */
     double sqrt_MUKT = sqrt(sys->mu / HkT * T);
     double sinTheta = sin(qp[2]);
@@ -1087,6 +1089,12 @@ int hho_candidate(hho_mt *s, const hho_system *sys, const hho_params *p, double 
         qp[13] = sqrt_IIKT * sin_theta * y1;
         qp[15] = sqrt_IIKT * y0;
     }
+}
+
+int hho_candidate(hho_mt *s, const hho_system *sys, const hho_params *p, double T,
+                  double *qp, double *energy, int *draws) {
+    *draws = 0;
+    gen_qp(s, sys, p, T, qp, draws, 0.0);
     /* Hamiltonian, then reject() */
     double E = hho_hamiltonian(sys, qp);
     double u = hho_mt_drand(s);
@@ -1263,17 +1271,20 @@ static void dense_eval(int n, const double *y_old, double F[7][NMAX], double x, 
 /* one direction of correlation_eval: samples k = 1..N-1 of mu0 . mu(t_k) */
 static int half_traj_ex(const hho_system *sys, const hho_params *p, const double *y0,
                         const double mu0[3], double *corr, double *vec, int vstep, hho_traj_stats *st,
-                        int *hard);
+                        int *hard, int nochecks, int *exited);
 static int half_traj(const hho_system *sys, const hho_params *p, const double *y0,
                      const double mu0[3], double *corr, hho_traj_stats *st, int *hard) {
-    return half_traj_ex(sys, p, y0, mu0, corr, NULL, 0, st, hard);
+    return half_traj_ex(sys, p, y0, mu0, corr, NULL, 0, st, hard, 0, NULL);
 }
 
 /* one direction of correlation_eval: samples k = 1..N-1 of mu0 . mu(t_k); with vec != NULL
- * also the dipole vector of sample k at vec + 3 * k * vstep (vstep = +-1) */
+ * also the dipole vector of sample k at vec + 3 * k * vstep (vstep = +-1).  nochecks (the
+ * PR_MU loop, hawaii.c:3661-3688): a NaN dipole leaves its sample at zero and no other test
+ * runs; *exited (optional) tells whether the branch ended by R > Rcut */
 static int half_traj_ex(const hho_system *sys, const hho_params *p, const double *y0,
                         const double mu0[3], double *corr, double *vec, int vstep, hho_traj_stats *st,
-                        int *hard) {
+                        int *hard, int nochecks, int *exited) {
+    if (exited) *exited = 0;
     integ I = {sys, hho_qp_size(sys), p->rtol, p->atol, 0};
     int n = I.n;
     double y[NMAX], f[NMAX], y_new[NMAX], K[16][NMAX], F[7][NMAX], ys[NMAX];
@@ -1303,6 +1314,15 @@ static int half_traj_ex(const hho_system *sys, const hho_params *p, const double
             extract_q(sys, ys, q);
             hho_dipole(sys, q, d);
             st->nsamples++;
+            if (nochecks) {
+                if (!(isnan(d[0]) || isnan(d[1]) || isnan(d[2]))) {
+                    if (vec) for (int c = 0; c < 3; ++c) vec[3 * (long)k * vstep + c] = d[c];
+                    if (ys[4] > p->Rcut) { ++k; if (exited) *exited = 1; goto done; }
+                }
+                ++k;
+                since = 0;
+                continue;
+            }
             if (isnan(d[0]) || isnan(d[1]) || isnan(d[2])) { status = HHO_ST_NAN_DIPOLE; *hard = 1; goto done; }
             prev = curr;
             curr = mu0[0] * d[0] + mu0[1] * d[1] + mu0[2] * d[2];
@@ -1395,12 +1415,12 @@ int hho_correlation_eval_zimmermann(const hho_system *sys, const hho_params *p, 
     double *centre = d + 3 * (N - 1);
     for (int c = 0; c < 3; ++c) centre[c] = mu0[c];
     int hard = 0;
-    st->status_fwd = half_traj_ex(sys, p, qp0, mu0, tmp, centre, 1, st, &hard);
+    st->status_fwd = half_traj_ex(sys, p, qp0, mu0, tmp, centre, 1, st, &hard, 0, NULL);
     if (!hard) {
         double y[NMAX];
         memcpy(y, qp0, n * sizeof(double));
         for (int i = 1; i < n; i += 2) y[i] = -y[i];
-        st->status_bwd = half_traj_ex(sys, p, y, mu0, tmp, centre, -1, st, &hard);
+        st->status_bwd = half_traj_ex(sys, p, y, mu0, tmp, centre, -1, st, &hard, 0, NULL);
     }
     if (hard) {
         st->failed = 1;
@@ -1416,6 +1436,61 @@ int hho_correlation_eval_zimmermann(const hho_system *sys, const hho_params *p, 
     free(d);
     free(tmp);
     return st->failed;
+}
+
+static void fft_backward(double *re, double *im, size_t L);
+
+/* PR_MU (calculate_spectral_function_using_prmu_representation_and_save, hawaii.c:3148-3978)
+ * without requantization, collision times, spin weights and histograms.  n trajectories are
+ * drawn from the stream of `seed` (q_generator, R := R0, p_generator, pR made inward; no
+ * rejection step); each is integrated forward with samples at t = (k+1) dt, k = 0..N-1, until
+ * R > R0; its dipole components are apodized (Connes), Fourier transformed and
+ * sf[i] += SF_COEFF pR/mu sum_c |F_c(i)|^2 for i < L.  A trajectory whose integration fails, or
+ * that is still inside R0 after N samples (unless allow_trunc), is skipped and not counted.
+ * qp_out (optional) receives the drawn phase points.  Returns the trajectories counted. */
+long hho_prmu(const hho_system *sys, const hho_params *p, double T, double R0, int allow_trunc, uint32_t seed,
+              size_t n, double *sf, size_t L, double *qp_out) {
+    hho_mt s;
+    hho_mt_seed(&s, seed);
+    const size_t N = p->N;
+    const int QP = hho_qp_size(sys);
+    const double SF_COEFF = Hartree * pow(ALU, 6) * ATU * R0 * R0 * p->sampling_time * p->sampling_time;
+    hho_params pp = *p;
+    pp.N = N + 1;       /* samples k = 1..N at t = k dt */
+    pp.Rcut = R0;
+    double *re = malloc(N * sizeof(double)), *im = malloc(N * sizeof(double));
+    double *vec = calloc(3 * (N + 1), sizeof(double));
+    double *tmp = calloc(N + 1, sizeof(double));
+    memset(sf, 0, L * sizeof(double));
+    long counted = 0;
+    for (size_t t = 0; t < n; ++t) {
+        double qp[16];
+        int draws = 0;
+        gen_qp(&s, sys, p, T, qp, &draws, R0);
+        if (qp[5] > 0.0) qp[5] = -qp[5];
+        if (qp_out) memcpy(qp_out + t * QP, qp, QP * sizeof(double));
+        const double pr_mu = -qp[5] / sys->mu;
+        hho_traj_stats st;
+        memset(&st, 0, sizeof st);
+        memset(vec, 0, 3 * (N + 1) * sizeof(double));
+        int hard = 0, exited = 0;
+        const double mu0[3] = {0, 0, 0};
+        int status = half_traj_ex(sys, &pp, qp, mu0, tmp, vec, 1, &st, &hard, 1, &exited);
+        if (status != HHO_OK) continue;
+        if (!exited && !allow_trunc) continue;
+        for (int c = 0; c < 3; ++c) {
+            for (size_t j = 0; j < N; ++j) {
+                double r = (double)j / (double)N;   /* connes_apodization, hawaii.c:5401-5410 */
+                re[j] = vec[3 * (j + 1) + c] * (1.0 - r * r) * (1.0 - r * r);
+                im[j] = 0.0;
+            }
+            fft_backward(re, im, N);
+            for (size_t i = 0; i < L; ++i) sf[i] += SF_COEFF * pr_mu * (re[i] * re[i] + im[i] * im[i]);
+        }
+        ++counted;
+    }
+    free(re); free(im); free(vec); free(tmp);
+    return counted;
 }
 
 int hho_propagate(const hho_system *sys, const hho_params *p, const double *qp0,

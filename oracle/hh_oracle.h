@@ -121,6 +121,10 @@ long hho_sample(uint32_t seed, const hho_system *sys, const hho_params *p, doubl
 /* ---- integrator + correlation_eval (hawaii.c:2116-2347) ---- */
 int hho_correlation_eval(const hho_system *sys, const hho_params *p, const double *qp0,
                          double *crln, hho_traj_stats *st);
+/* PR_MU spectral function (src/hawaii.c:3148-3978), core: returns the trajectories counted,
+ * sf[0..L) the unnormalised sum */
+long hho_prmu(const hho_system *sys, const hho_params *p, double T, double R0, int allow_trunc, uint32_t seed,
+              size_t n, double *sf, size_t L, double *qp_out);
 /* correlation_eval_zimmerman_trick (src/hawaii.c:1888-2114) */
 int hho_correlation_eval_zimmermann(const hho_system *sys, const hho_params *p, const double *qp0,
                                     double *crln, hho_traj_stats *st);

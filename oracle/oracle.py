@@ -105,6 +105,9 @@ def lib():
                                                 _dp, C.c_int, _dp]
         L.hho_correlation_eval_zimmermann.argtypes = [C.POINTER(System), C.POINTER(Params), _dp, _dp,
                                                       C.POINTER(TrajStats)]
+        L.hho_prmu.restype = C.c_long
+        L.hho_prmu.argtypes = [C.POINTER(System), C.POINTER(Params), C.c_double, C.c_double, C.c_int, C.c_uint32,
+                               C.c_size_t, _dp, C.c_size_t, C.c_void_p]
         L.hho_ch4co2_lab_to_kal.argtypes = [_dp, _dp]
         L.hho_ch4co2_dipole_kal.argtypes = [_dp, _dp]
         L.hho_ch4co2_V_lab.restype = C.c_double
@@ -153,6 +156,15 @@ def correlation_eval_zimmermann(sysd, params, qp0):
     lib().hho_correlation_eval_zimmermann(C.byref(sysd), C.byref(params),
                                           np.ascontiguousarray(qp0, dtype=np.float64), crln, C.byref(st))
     return crln, st
+
+
+def prmu(sysd, params, T, R0, n, L, seed, allow_trunc=False, with_qp=False):
+    """PR_MU core: (unnormalised sf[0..L), trajectories counted[, drawn phase points])"""
+    sf = np.zeros(L)
+    qp = np.zeros((n, qp_size(sysd.system))) if with_qp else None
+    cnt = lib().hho_prmu(C.byref(sysd), C.byref(params), T, R0, int(allow_trunc), seed, n, sf, L,
+                         qp.ctypes.data_as(C.c_void_p) if with_qp else None)
+    return (sf, cnt, qp) if with_qp else (sf, cnt)
 
 
 def correlation_parts(sysd, params, qp0):
