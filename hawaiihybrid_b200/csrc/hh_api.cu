@@ -94,10 +94,9 @@ struct Ctx {
   SamplerExtra sx{};
   double2 *d_ch4_cd = nullptr;
   float4 *d_ch4_cf = nullptr;
-  unsigned char *d_ch4_y2 = nullptr;
-  unsigned int *d_ch4_grp = nullptr;
-  unsigned short *d_ch4_gcount = nullptr;
-  int ch4_E = 0, ch4_G = 0;
+  unsigned int *d_ch4_y2 = nullptr;
+  unsigned int *d_ch4_meta = nullptr;
+  int ch4_B = 0;
   // MT19937 stream
   uint32_t *d_mt = nullptr;
   unsigned short *d_mt_jump_seg = nullptr, *d_mt_jump_coarse = nullptr;  // jump-ahead tables
@@ -409,13 +408,11 @@ int run_records_t(const TrajParams &P, const double *d_ic, uint64_t n, uint64_t 
   CK(cudaMemsetAsync(g.rec_nfail.p, 0, sizeof(unsigned long long), g.st));
   if (zimm) CK(g.zim_fail.ensure(chunk));
   Ch4Co2Fold fold;
-  fold.n_entry = g.ch4_E;
-  fold.n_group = g.ch4_G;
+  fold.n_batch = g.ch4_B;
   fold.cf = g.d_ch4_cf;
   fold.cd = g.d_ch4_cd;
   fold.y2 = g.d_ch4_y2;
-  fold.grp = g.d_ch4_grp;
-  fold.gcount = g.d_ch4_gcount;
+  fold.meta = g.d_ch4_meta;
   for (int i = 0; i < CH4_NSEG - 1; ++i) fold.seg_hi[i] = hh_ch4co2_seg_hi[i];
   for (int i = 0; i < CH4_NSEG; ++i) fold.centre[i] = hh_ch4co2_centre[i];
   auto dip = ch4_dipole_kernel<PHYS>;
@@ -836,24 +833,21 @@ int hh_cuda_init(int device, const hh_system_desc *sys) {
   if (sid == HH_SYSTEM_CH4_CO2 && !g.d_ch4_cd) {
     Ch4Co2FoldHost f;
     if (ch4co2_build_fold(&f) != 0) return HH_E_UNSUPPORTED_SYSTEM;
-    const size_t E = (size_t)f.n_entry;
-    std::vector<float4> cf(HH_CH4CO2_NSEG * E);
+    // the padded batch stream (whole batches of 4 entries per group)
+    const size_t B = (size_t)f.n_batch;
+    std::vector<float4> cf(HH_CH4CO2_NSEG * 4 * B);
     for (size_t i = 0; i < cf.size(); ++i)
-      cf[i] = make_float4((float)f.coef[4 * i], (float)f.coef[4 * i + 1], (float)f.coef[4 * i + 2],
-                          (float)f.coef[4 * i + 3]);
-    CK(cudaMalloc(&g.d_ch4_cd, f.coef.size() * sizeof(double)));
+      cf[i] = make_float4((float)f.bcoef[4 * i], (float)f.bcoef[4 * i + 1], (float)f.bcoef[4 * i + 2],
+                          (float)f.bcoef[4 * i + 3]);
+    CK(cudaMalloc(&g.d_ch4_cd, f.bcoef.size() * sizeof(double)));
     CK(cudaMalloc(&g.d_ch4_cf, cf.size() * sizeof(float4)));
-    CK(cudaMalloc(&g.d_ch4_y2, E));
-    CK(cudaMalloc(&g.d_ch4_grp, f.grp.size() * sizeof(unsigned int)));
-    CK(cudaMalloc(&g.d_ch4_gcount, f.gcount.size() * sizeof(unsigned short)));
-    CK(cudaMemcpy(g.d_ch4_cd, f.coef.data(), f.coef.size() * sizeof(double), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&g.d_ch4_y2, 4 * B));
+    CK(cudaMalloc(&g.d_ch4_meta, B * sizeof(unsigned int)));
+    CK(cudaMemcpy(g.d_ch4_cd, f.bcoef.data(), f.bcoef.size() * sizeof(double), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(g.d_ch4_cf, cf.data(), cf.size() * sizeof(float4), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(g.d_ch4_y2, f.y2.data(), E, cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(g.d_ch4_grp, f.grp.data(), f.grp.size() * sizeof(unsigned int), cudaMemcpyHostToDevice));
-    CK(cudaMemcpy(g.d_ch4_gcount, f.gcount.data(), f.gcount.size() * sizeof(unsigned short),
-                  cudaMemcpyHostToDevice));
-    g.ch4_E = f.n_entry;
-    g.ch4_G = f.n_group;
+    CK(cudaMemcpy(g.d_ch4_y2, f.by2.data(), 4 * B, cudaMemcpyHostToDevice));
+    CK(cudaMemcpy(g.d_ch4_meta, f.bmeta.data(), B * sizeof(unsigned int), cudaMemcpyHostToDevice));
+    g.ch4_B = f.n_batch;
   }
   g.sys = (sid == HH_SYSTEM_HE_AR)    ? SYS_HEAR
           : (sid == HH_SYSTEM_N2_AR)  ? SYS_N2AR
@@ -1523,8 +1517,7 @@ void hh_cuda_shutdown(void) {
   if (g.d_ch4_cd) cudaFree(g.d_ch4_cd);
   if (g.d_ch4_cf) cudaFree(g.d_ch4_cf);
   if (g.d_ch4_y2) cudaFree(g.d_ch4_y2);
-  if (g.d_ch4_grp) cudaFree(g.d_ch4_grp);
-  if (g.d_ch4_gcount) cudaFree(g.d_ch4_gcount);
+  if (g.d_ch4_meta) cudaFree(g.d_ch4_meta);
   if (g.d_mt) cudaFree(g.d_mt);
   if (g.d_mt_jump_seg) cudaFree(g.d_mt_jump_seg);
   if (g.d_mt_jump_coarse) cudaFree(g.d_mt_jump_coarse);

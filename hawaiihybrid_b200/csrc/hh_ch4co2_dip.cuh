@@ -3,7 +3,7 @@
 // The induced dipole of PES-IDS/ai_ids_ch4_co2.cpp:672-1067 is, per Cartesian
 // component c of the CH4 body frame,
 //   mu_c = sum_e  Y1_e(n1) Y2_e(n2) K_e(R)
-// over 8,661 entries e = (c, Y1, Y2) (hh_ch4co2_host.cpp folds the 320 radial
+// over 8,658 entries e = (c, Y1, Y2) (hh_ch4co2_host.cpp folds the 320 radial
 // functions of each entry into one piecewise cubic on their common grid of 30
 // pieces).  n1 and n2 are the directions of the intermolecular axis and of the
 // CO2 axis in the CH4 body frame; Y1 (l <= 13) and Y2 (even l <= 12) are real
@@ -19,8 +19,9 @@
 //      warp task has one piece;
 //   2. dipole_kernel: a warp evaluates 32 S records of one piece, S per lane; the
 //      coefficient stream of that piece is the same for all lanes (broadcast loads,
-//      shared by a lane's S records), the S values of Y2 of each index sit side by
-//      side in shared memory (one vector load), Y1 is generated in the order of the
+//      shared by a lane's S records) and is walked in batches of 4 entries, the next
+//      batch loaded while one is summed; the S values of Y2 of each index sit side by
+//      side in shared memory (one vector load); Y1 is generated in the order of the
 //      stream;
 //   3. corr_kernel applies the reference's per-sample tests in order (NaN dipole,
 //      |C| > 1e100, |C_k / C_k-1| > 1e10: src/hawaii.c:2183-2243) and adds
@@ -41,14 +42,15 @@ constexpr int CH4_L2 = HH_CH4CO2_L2MAX;
 constexpr int CH4_NY2 = 91;  // even l2 <= 12, all m2 and cos/sin
 constexpr int CH4_DIP_WARPS = 4;
 
-// folded dipole table in device memory (built by ch4co2_build_fold)
+// folded dipole table in device memory (built by ch4co2_build_fold): the entries in
+// batches of 4, each group (one Y1, cos or sin, one component) padded with zero
+// entries to whole batches
 struct Ch4Co2Fold {
-  int n_entry, n_group;
-  const float4 *cf;             // [NSEG][n_entry] (c0, c1, c2, c3), FP32
-  const double2 *cd;            // [NSEG][n_entry][2] (c0, c1), (c2, c3), FP64
-  const unsigned char *y2;      // [n_entry] index of Y2 in the per-lane array
-  const unsigned int *grp;      // [n_group] cs | comp << 1 | entries << 3
-  const unsigned short *gcount; // [(l, m) in m-major order] groups at that Y1
+  int n_batch;
+  const float4 *cf;             // [NSEG][4 n_batch] (c0, c1, c2, c3), FP32
+  const double2 *cd;            // [NSEG][4 n_batch][2] (c0, c1), (c2, c3), FP64
+  const unsigned int *y2;       // [n_batch] the batch's four Y2 indices, one byte each
+  const unsigned int *meta;     // [n_batch] cs | comp << 1 | (ends its group) << 3 | lm << 8
   double seg_hi[CH4_NSEG - 1];
   double centre[CH4_NSEG];
 };
@@ -246,119 +248,118 @@ __global__ void __launch_bounds__(32 * CH4_DIP_WARPS) ch4_dipole_kernel(Ch4DipAr
       iR6[s] = i2 * i2 * i2;
     }
     __syncwarp();
-    const float4 *cf = a.f.cf + (size_t)seg * a.f.n_entry;
-    const double2 *cd = a.f.cd + (size_t)seg * a.f.n_entry * 2;
-    PHYS acc[S][3], C[S], Sn[S], qa[S], qb[S];
+    const float4 *cf = a.f.cf + (size_t)seg * 4 * a.f.n_batch;
+    const double2 *cd = a.f.cd + (size_t)seg * 8 * a.f.n_batch;
+    PHYS acc[S][3], C[S], Sn[S], qa[S], qb[S], Yc[S], Ys[S];
+    // per-power sums A_j = sum_e Y2_e c_je of the current group, collapsed by Horner
+    // at its end
+    PHYS A0[S], A1[S], A2[S], A3[S];
 #pragma unroll
     for (int s = 0; s < S; ++s) {
       acc[s][0] = acc[s][1] = acc[s][2] = PHYS(0);
       C[s] = PHYS(1);
       Sn[s] = PHYS(0);
+      qa[s] = qb[s] = Yc[s] = Ys[s] = PHYS(0);
+      A0[s] = A1[s] = A2[s] = A3[s] = PHYS(0);
     }
     PHYS pm = PHYS(1);
-    int g = 0, e = 0, lm = 0;
-#pragma unroll 1
-    for (int m = 0; m <= CH4_L1; ++m) {
-      if (m > 0) {
+    // Y1 position in the m-major order (l, m); "before (0, 0)" at the start
+    int m = -1, l = CH4_L1, lm = -1;
+    // one flat loop over the batches; the next batch's coefficients, indices and
+    // descriptor are loaded while this one is summed
+    PHYS cn[4][4];
+    unsigned idn, dn;
+    auto load = [&](int b) {
 #pragma unroll
-        for (int s = 0; s < S; ++s) {
-          const PHYS c = C[s] * n1[s][0] - Sn[s] * n1[s][1];
-          Sn[s] = C[s] * n1[s][1] + Sn[s] * n1[s][0];
-          C[s] = c;
+      for (int j = 0; j < 4; ++j) {
+        if constexpr (sizeof(PHYS) == 4) {
+          const float4 c4 = __ldg(&cf[4 * b + j]);
+          cn[j][0] = c4.x; cn[j][1] = c4.y; cn[j][2] = c4.z; cn[j][3] = c4.w;
+        } else {
+          const double2 lo = __ldg(&cd[2 * (4 * b + j)]), hi = __ldg(&cd[2 * (4 * b + j) + 1]);
+          cn[j][0] = lo.x; cn[j][1] = lo.y; cn[j][2] = hi.x; cn[j][3] = hi.y;
         }
-        pm = -pm * sqrt(PHYS(2 * m - 1) / PHYS(2 * m));
       }
-#pragma unroll
-      for (int s = 0; s < S; ++s) {
-        qa[s] = PHYS(1);
-        qb[s] = PHYS(0);
-      }
+      idn = __ldg(&a.f.y2[b]);
+      dn = __ldg(&a.f.meta[b]);
+    };
+    load(0);
+    const int nb = a.f.n_batch;
 #pragma unroll 1
-      for (int l = m; l <= CH4_L1; ++l, ++lm) {
-        const PHYS ca = PHYS(2 * l - 1), cb = sqrt(PHYS((l - 1) * (l - 1) - m * m));
-        const PHYS id = (l > m + 1) ? PHYS(1) / sqrt(PHYS(l * l - m * m)) : PHYS(0);
-        const PHYS c1 = sqrt(PHYS(2 * m + 1));
-        PHYS Yc[S], Ys[S];
+    for (int b = 0; b < nb; ++b) {
+      PHYS c[4][4];
 #pragma unroll
-        for (int s = 0; s < S; ++s) {
-          const PHYS z = n1[s][2];
-          const PHYS q = (l == m) ? PHYS(1) : (l == m + 1) ? c1 * z : (ca * z * qa[s] - cb * qb[s]) * id;
-          qb[s] = qa[s];
-          qa[s] = q;
-          Yc[s] = pm * C[s] * q;
-          Ys[s] = pm * Sn[s] * q;
-        }
-        const int ng = __ldg(&a.f.gcount[lm]);
+      for (int j = 0; j < 4; ++j)
+#pragma unroll
+        for (int k = 0; k < 4; ++k) c[j][k] = cn[j][k];
+      const unsigned ids = idn, d = dn;
+      if (b + 1 < nb) load(b + 1);
+      V yv[4];
+#pragma unroll
+      for (int j = 0; j < 4; ++j) yv[j] = Y2v[int((ids >> (8 * j)) & 0xffu) * 32];
+      // advance Y1 to this batch's (l, m) by the three-term recurrence in l and
+      // (x + i y)^m (the same for every lane of the warp)
+      const int want = int(d >> 8);
 #pragma unroll 1
-        for (int gg = 0; gg < ng; ++gg, ++g) {
-          const unsigned d = __ldg(&a.f.grp[g]);
-          const int cnt = int(d >> 3);
-          // per-power sums A_j = sum_e Y2_e c_je, collapsed by Horner at the end of the
-          // group; four entries' loads are issued before their arithmetic
-          PHYS A0[S], A1[S], A2[S], A3[S];
-#pragma unroll
-          for (int s = 0; s < S; ++s) A0[s] = A1[s] = A2[s] = A3[s] = PHYS(0);
-          int i = 0;
-#pragma unroll 1
-          for (; i + 4 <= cnt; i += 4) {
-            PHYS c[4][4];
-            int id[4];
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-              if constexpr (sizeof(PHYS) == 4) {
-                const float4 c4 = __ldg(&cf[e + i + j]);
-                c[j][0] = c4.x; c[j][1] = c4.y; c[j][2] = c4.z; c[j][3] = c4.w;
-              } else {
-                const double2 lo = __ldg(&cd[2 * (e + i + j)]), hi = __ldg(&cd[2 * (e + i + j) + 1]);
-                c[j][0] = lo.x; c[j][1] = lo.y; c[j][2] = hi.x; c[j][3] = hi.y;
-              }
-              id[j] = int(__ldg(&a.f.y2[e + i + j]));
-            }
-#pragma unroll
-            for (int j = 0; j < 4; ++j) {
-              const V yv = Y2v[id[j] * 32];
-#pragma unroll
-              for (int s = 0; s < S; ++s) {
-                const PHYS y = vget(yv, s);
-                A0[s] += y * c[j][0];
-                A1[s] += y * c[j][1];
-                A2[s] += y * c[j][2];
-                A3[s] += y * c[j][3];
-              }
-            }
-          }
-#pragma unroll 1
-          for (; i < cnt; ++i) {
-            PHYS c0, c1_, c2, c3;
-            if constexpr (sizeof(PHYS) == 4) {
-              const float4 c4 = __ldg(&cf[e + i]);
-              c0 = c4.x; c1_ = c4.y; c2 = c4.z; c3 = c4.w;
-            } else {
-              const double2 lo = __ldg(&cd[2 * (e + i)]), hi = __ldg(&cd[2 * (e + i) + 1]);
-              c0 = lo.x; c1_ = lo.y; c2 = hi.x; c3 = hi.y;
-            }
-            const V yv = Y2v[int(__ldg(&a.f.y2[e + i])) * 32];
+      while (lm < want) {
+        ++lm;
+        if (l == CH4_L1) {
+          ++m;
+          l = m;
+          if (m > 0) {
 #pragma unroll
             for (int s = 0; s < S; ++s) {
-              const PHYS y = vget(yv, s);
-              A0[s] += y * c0;
-              A1[s] += y * c1_;
-              A2[s] += y * c2;
-              A3[s] += y * c3;
+              const PHYS cc = C[s] * n1[s][0] - Sn[s] * n1[s][1];
+              Sn[s] = C[s] * n1[s][1] + Sn[s] * n1[s][0];
+              C[s] = cc;
             }
+            pm = -pm * sqrt(PHYS(2 * m - 1) / PHYS(2 * m));
           }
-          PHYS sum[S];
-#pragma unroll
-          for (int s = 0; s < S; ++s) sum[s] = A0[s] + x[s] * (A1[s] + x[s] * (A2[s] + x[s] * A3[s]));
-          e += cnt;
-          const unsigned comp = (d >> 1) & 3u;
 #pragma unroll
           for (int s = 0; s < S; ++s) {
-            const PHYS t = ((d & 1u) ? Ys[s] : Yc[s]) * sum[s];
-            if (comp == 0) acc[s][0] += t;
-            else if (comp == 1) acc[s][1] += t;
-            else acc[s][2] += t;
+            qa[s] = PHYS(1);
+            qb[s] = PHYS(0);
           }
+        } else {
+          ++l;
+          const PHYS ca = PHYS(2 * l - 1), cb = sqrt(PHYS((l - 1) * (l - 1) - m * m));
+          const PHYS id = (l > m + 1) ? PHYS(1) / sqrt(PHYS(l * l - m * m)) : PHYS(0);
+          const PHYS c1 = sqrt(PHYS(2 * m + 1));
+#pragma unroll
+          for (int s = 0; s < S; ++s) {
+            const PHYS z = n1[s][2];
+            const PHYS q = (l == m + 1) ? c1 * z : (ca * z * qa[s] - cb * qb[s]) * id;
+            qb[s] = qa[s];
+            qa[s] = q;
+          }
+        }
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+          Yc[s] = pm * C[s] * qa[s];
+          Ys[s] = pm * Sn[s] * qa[s];
+        }
+      }
+#pragma unroll
+      for (int j = 0; j < 4; ++j) {
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+          const PHYS y = vget(yv[j], s);
+          A0[s] += y * c[j][0];
+          A1[s] += y * c[j][1];
+          A2[s] += y * c[j][2];
+          A3[s] += y * c[j][3];
+        }
+      }
+      if (d & 8u) {
+        const unsigned comp = (d >> 1) & 3u;
+#pragma unroll
+        for (int s = 0; s < S; ++s) {
+          const PHYS sum = A0[s] + x[s] * (A1[s] + x[s] * (A2[s] + x[s] * A3[s]));
+          const PHYS t = ((d & 1u) ? Ys[s] : Yc[s]) * sum;
+          if (comp == 0) acc[s][0] += t;
+          else if (comp == 1) acc[s][1] += t;
+          else acc[s][2] += t;
+          A0[s] = A1[s] = A2[s] = A3[s] = PHYS(0);
         }
       }
     }

@@ -9,6 +9,12 @@ struct Ch4Co2FoldHost {
   std::vector<unsigned char> y2;        // [n_entry]: Y2 index (m2-major, even l2, cos then sin)
   std::vector<unsigned int> grp;        // [n_group]: cs | comp << 1 | entries << 3
   std::vector<unsigned short> gcount;   // [(l1, m1), m1-major]: groups at that Y1
+  // the same stream with every group padded to whole batches of 4 entries (zero
+  // coefficients), for the batched kernel loop
+  int n_batch = 0;
+  std::vector<double> bcoef;            // [NSEG][4 n_batch][4]
+  std::vector<unsigned char> by2;       // [4 n_batch]
+  std::vector<unsigned int> bmeta;      // [n_batch]: cs | comp << 1 | (last batch of its group) << 3 | lm << 8
 };
 
 // entries e = (component, Y1, Y2) with K_e(R) = sum over the reference's terms of

@@ -81,5 +81,36 @@ int ch4co2_build_fold(Ch4Co2FoldHost *out) {
     ++e;
   }
   out->n_group = (int)out->grp.size();
+  // padded batches: each group's entries followed by zero entries up to a multiple of 4
+  out->bcoef.clear();
+  out->by2.clear();
+  out->bmeta.clear();
+  std::vector<int> order;  // entry index or -1 (padding), in batch order
+  {
+    int g = 0, lm = 0, e0 = 0;
+    for (int m = 0; m <= HH_CH4CO2_L1MAX; ++m)
+      for (int l = m; l <= HH_CH4CO2_L1MAX; ++l, ++lm)
+        for (int k = 0; k < out->gcount[lm]; ++k, ++g) {
+          const unsigned d = out->grp[g];
+          const int cnt = int(d >> 3);
+          const int nb = (cnt + 3) / 4;
+          for (int b = 0; b < nb; ++b) {
+            for (int j = 0; j < 4; ++j) order.push_back(4 * b + j < cnt ? e0 + 4 * b + j : -1);
+            out->bmeta.push_back((d & 7u) | (b == nb - 1 ? 8u : 0u) | ((unsigned)lm << 8));
+          }
+          e0 += cnt;
+        }
+  }
+  out->n_batch = (int)out->bmeta.size();
+  const size_t EP = order.size();
+  out->bcoef.assign((size_t)HH_CH4CO2_NSEG * EP * 4, 0.0);
+  out->by2.assign(EP, 0);
+  for (size_t i = 0; i < EP; ++i) {
+    if (order[i] < 0) continue;
+    out->by2[i] = out->y2[order[i]];
+    for (int s = 0; s < HH_CH4CO2_NSEG; ++s)
+      for (int j = 0; j < 4; ++j)
+        out->bcoef[((size_t)s * EP + i) * 4 + j] = out->coef[((size_t)s * E + order[i]) * 4 + j];
+  }
   return 0;
 }
