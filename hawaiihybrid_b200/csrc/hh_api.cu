@@ -90,6 +90,7 @@ struct Ctx {
   N2arDipFold *d_n2ar_fold = nullptr;  // N2-Ar dipole models, folded (hh_n2ar_fold.h)
   N2arPesNet<double> *d_n2ar_pes_d = nullptr;  // N2-Ar PES network, FP64 and FP32
   N2arPesNet<float> *d_n2ar_pes_f = nullptr;
+  float4 *d_n2ar_tab = nullptr;  // N2-Ar mixed-path dipole table (hh_n2ar.cuh), built on the device
   // CH4-CO2: rotor moments, stand-in surface constants, folded dipole table
   SamplerExtra sx{};
   double2 *d_ch4_cd = nullptr;
@@ -367,9 +368,11 @@ int run_traj_dispatch(int precision, const TrajParams &P, const TrajIO &io) {
     io2.dipnet = g.d_n2ar_fold;
     if (precision == HH_PRECISION_MIXED) {
       io2.pesnet = g.d_n2ar_pes_f;
+      io2.diptab = g.d_n2ar_tab;
       return launch_traj<SYS_N2AR, float, float, false>(P, io2, nullptr);
     }
     io2.pesnet = g.d_n2ar_pes_d;
+    io2.diptab = nullptr;
     return launch_traj<SYS_N2AR, double, double, false>(P, io2, nullptr);
   }
   // plain FP32 sums: compensation does not reduce the FP32 error of the surfaces,
@@ -607,6 +610,7 @@ int run_trajectories(const hh_calc_params *p, const double *d_ic, uint64_t n, ui
   io.item_trace = nullptr;
   io.dipnet = nullptr;
   io.pesnet = nullptr;
+  io.diptab = nullptr;
   io.sat_w = d_satw;
   io.n_sat = n_sat;
   uint32_t *trace_host = g_trace_host;
@@ -829,6 +833,10 @@ int hh_cuda_init(int device, const hh_system_desc *sys) {
     CK(cudaMalloc(&g.d_n2ar_pes_f, sizeof pes_f));
     CK(cudaMemcpy(g.d_n2ar_pes_d, &pes_d, sizeof pes_d, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(g.d_n2ar_pes_f, &pes_f, sizeof pes_f, cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&g.d_n2ar_tab, (size_t)N2T_CELLS * N2T_CELL_F4 * sizeof(float4)));
+    n2ar_tab_build_kernel<<<N2T_CELLS, 128>>>(g.d_n2ar_fold, g.d_n2ar_tab);
+    CK(cudaGetLastError());
+    CK(cudaDeviceSynchronize());
   }
   if (sid == HH_SYSTEM_CH4_CO2 && !g.d_ch4_cd) {
     Ch4Co2FoldHost f;
@@ -1358,6 +1366,50 @@ int hh_cuda_mt_stream(uint32_t seed, uint64_t n, uint32_t *out) {
   return reseed(seed);
 }
 
+namespace {
+// body-frame N2-Ar dipole at (R, T) as each precision path evaluates it
+__global__ void n2ar_dip_probe_kernel(const N2arDipFold *F, const float4 *tab, const double *R, const double *T,
+                                      long long n, int mixed, double *out) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= n) return;
+  const double c = cos(T[i]), s = sin(T[i]);
+  const N2arDipBody<double> d = mixed ? n2ar_dip_body_mixed(tab, F, R[i], c, fabs(s)) : n2ar_dip_body(F, R[i], c);
+  out[2 * i] = d.dx;
+  out[2 * i + 1] = d.dz;
+}
+}  // namespace
+
+int hh_cuda_debug_n2ar_dipole(int precision, const double *R, const double *T, uint64_t n, double *out) {
+  if (!g.init) return HH_E_NOT_INITIALIZED;
+  if (g.sys != SYS_N2AR || !g.d_n2ar_tab) return HH_E_UNSUPPORTED_SYSTEM;
+  if ((n && (!R || !T || !out)) || (precision != HH_PRECISION_FP64 && precision != HH_PRECISION_MIXED))
+    return HH_E_INVALID_ARGUMENT;
+  if (!n) return HH_OK;
+  CK(cudaSetDevice(g.device));
+  double *dR = nullptr, *dT = nullptr, *dO = nullptr;
+  int rc = HH_OK;
+  cudaError_t e = cudaMalloc(&dR, n * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&dT, n * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&dO, 2 * n * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemcpy(dR, R, n * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(dT, T, n * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    n2ar_dip_probe_kernel<<<(unsigned)((n + 127) / 128), 128, 0, g.st>>>(
+        g.d_n2ar_fold, g.d_n2ar_tab, dR, dT, (long long)n, precision == HH_PRECISION_MIXED, dO);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaStreamSynchronize(g.st);
+  if (e == cudaSuccess) e = cudaMemcpy(out, dO, 2 * n * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e != cudaSuccess) {
+    snprintf(g_errmsg, sizeof g_errmsg, "hh_cuda_debug_n2ar_dipole: %s", cudaGetErrorString(e));
+    rc = HH_E_CUDA;
+  }
+  if (dR) cudaFree(dR);
+  if (dT) cudaFree(dT);
+  if (dO) cudaFree(dO);
+  return rc;
+}
+
 int hh_cuda_debug_item_trace(uint32_t *out, uint64_t capacity_words) {
   g_trace_host = out;
   g_trace_cap = out ? capacity_words : 0;
@@ -1514,6 +1566,7 @@ void hh_cuda_shutdown(void) {
   if (g.d_n2ar_fold) cudaFree(g.d_n2ar_fold);
   if (g.d_n2ar_pes_d) cudaFree(g.d_n2ar_pes_d);
   if (g.d_n2ar_pes_f) cudaFree(g.d_n2ar_pes_f);
+  if (g.d_n2ar_tab) cudaFree(g.d_n2ar_tab);
   if (g.d_ch4_cd) cudaFree(g.d_ch4_cd);
   if (g.d_ch4_cf) cudaFree(g.d_ch4_cf);
   if (g.d_ch4_y2) cudaFree(g.d_ch4_y2);

@@ -275,4 +275,146 @@ static __device__ __noinline__ N2arDipBody<double> n2ar_dip_body(const N2arDipFo
   return out;
 }
 
+// Mixed-path dipole table.  The body-frame dipole (d_x, d_z) of n2ar_dip_body is a
+// smooth function of R and of the angle T in [0, pi] between r^ and u^ (the site
+// distances are analytic in T; in x = cos T they are not, at x = +-1).  The mixed
+// path replaces the network by a piecewise Chebyshev series of degree 9 in each
+// variable on cells of
+//   R: 0.5 bohr on [4.5, 12.5] (the switch edges 9.5 and 12.5 are cell edges),
+//      1.5 bohr on [12.5, 20], 4 bohr on [20, 60];   T: 12 cells of pi/12,
+// built on the device from the FP64 network at the Chebyshev nodes of every cell
+// (n2ar_tab_build_kernel) and evaluated in FP32.  The series error is below 1.3e-9
+// of the largest |d| at the same R (sampled against the network); FP32 evaluation
+// adds about 1e-7.  Outside [4.5, 60) bohr the mixed path evaluates the network.
+constexpr int N2T_DEG = 10;                 // Chebyshev coefficients per variable
+constexpr int N2T_NR = 16 + 5 + 10;         // R cells
+constexpr int N2T_NT = 12;                  // T cells
+constexpr int N2T_CELLS = N2T_NR * N2T_NT;
+constexpr int N2T_CELL_F4 = N2T_DEG * N2T_DEG / 2;  // float4 per cell: [i_R][j_T] (d_x, d_z) pairs
+constexpr double N2T_RLO = 4.5, N2T_RHI = 60.0;
+
+// lower edge and width of R cell i
+__host__ __device__ inline void n2t_rcell(int i, double &lo, double &w) {
+  if (i < 16) {
+    w = 0.5;
+    lo = 4.5 + 0.5 * i;
+  } else if (i < 21) {
+    w = 1.5;
+    lo = 12.5 + 1.5 * (i - 16);
+  } else {
+    w = 4.0;
+    lo = 20.0 + 4.0 * (i - 21);
+  }
+}
+
+// R cell of R in [4.5, 60) and the cell coordinate x in [-1, 1]
+__device__ __forceinline__ int n2t_rindex(float R, float &x) {
+  int i;
+  float lo, s;
+  if (R < 12.5f) {
+    i = min(max(int((R - 4.5f) * 2.0f), 0), 15);
+    lo = 4.5f + 0.5f * float(i);
+    s = 4.0f;
+  } else if (R < 20.0f) {
+    i = min(int((R - 12.5f) * (1.0f / 1.5f)), 4);
+    lo = 12.5f + 1.5f * float(i);
+    s = 2.0f / 1.5f;
+    i += 16;
+  } else {
+    i = min(int((R - 20.0f) * 0.25f), 9);
+    lo = 20.0f + 4.0f * float(i);
+    s = 0.5f;
+    i += 21;
+  }
+  x = (R - lo) * s - 1.0f;
+  return i;
+}
+
+// one block per cell: the network at the 10 x 10 Chebyshev nodes, then the
+// coefficients c_ij = (2 - d_i0)(2 - d_j0)/100 sum_ab f(x_a, y_b) T_i(x_a) T_j(y_b)
+static __global__ void __launch_bounds__(128) n2ar_tab_build_kernel(const N2arDipFold *F, float4 *tab) {
+  constexpr int D = N2T_DEG;
+  __shared__ double v[2][D][D];
+  const int cell = blockIdx.x, ir = cell / N2T_NT, it = cell - ir * N2T_NT;
+  double lo, w;
+  n2t_rcell(ir, lo, w);
+  const int t = threadIdx.x;
+  if (t < D * D) {
+    const int a = t / D, b = t - a * D;
+    const double xa = cospi((a + 0.5) / D), xb = cospi((b + 0.5) / D);
+    const double R = lo + 0.5 * w * (xa + 1.0);
+    const double T = (it + 0.5 * (xb + 1.0)) * (HH_PI / N2T_NT);
+    const N2arDipBody<double> d = n2ar_dip_body(F, R, cos(T));
+    v[0][a][b] = d.dx;
+    v[1][a][b] = d.dz;
+  }
+  __syncthreads();
+  if (t < D * D) {
+    const int i = t / D, j = t - i * D;
+    double sx = 0.0, sz = 0.0;
+    for (int a = 0; a < D; ++a) {
+      const double ca = cospi(i * (a + 0.5) / D);
+      for (int b = 0; b < D; ++b) {
+        const double wab = ca * cospi(j * (b + 0.5) / D);
+        sx += v[0][a][b] * wab;
+        sz += v[1][a][b] * wab;
+      }
+    }
+    const double f = (i ? 2.0 : 1.0) * (j ? 2.0 : 1.0) / double(D * D);
+    reinterpret_cast<float2 *>(tab)[(size_t)cell * D * D + i * D + j] =
+        make_float2(float(sx * f), float(sz * f));
+  }
+}
+
+// body-frame dipole from the table (FP32), R in [4.5, 60), T in [0, pi]
+__device__ __forceinline__ void n2ar_dip_tab(const float4 *tab, float R, float T, float &dx, float &dz) {
+  constexpr int D = N2T_DEG;
+  float xr;
+  const int ir = n2t_rindex(R, xr);
+  const float tc = T * float(N2T_NT / HH_PI);
+  const int it = min(max(int(tc), 0), N2T_NT - 1);
+  const float xt = 2.0f * (tc - float(it)) - 1.0f;
+  float Tt[D];
+  Tt[0] = 1.0f;
+  Tt[1] = xt;
+#pragma unroll
+  for (int j = 2; j < D; ++j) Tt[j] = 2.0f * xt * Tt[j - 1] - Tt[j - 2];
+  const float4 *c = tab + (size_t)(ir * N2T_NT + it) * N2T_CELL_F4;
+  float ax = 0.0f, az = 0.0f, r0 = 1.0f, r1 = xr;
+#pragma unroll
+  for (int i = 0; i < D; ++i) {
+    float ri;
+    if (i == 0) ri = 1.0f;
+    else if (i == 1) ri = xr;
+    else {
+      ri = 2.0f * xr * r1 - r0;
+      r0 = r1;
+      r1 = ri;
+    }
+    float sx = 0.0f, sz = 0.0f;
+#pragma unroll
+    for (int q = 0; q < D / 2; ++q) {
+      const float4 v = __ldg(&c[i * (D / 2) + q]);
+      sx += v.x * Tt[2 * q] + v.z * Tt[2 * q + 1];
+      sz += v.y * Tt[2 * q] + v.w * Tt[2 * q + 1];
+    }
+    ax += ri * sx;
+    az += ri * sz;
+  }
+  dx = ax;
+  dz = az;
+}
+
+// body-frame dipole of the mixed path at R, x = cos T, s = sin T >= 0: the table
+// inside its range, the FP64 network outside
+__device__ __forceinline__ N2arDipBody<double> n2ar_dip_body_mixed(const float4 *tab, const N2arDipFold *F,
+                                                                   double R, double x, double s) {
+  if (R >= N2T_RLO && R < N2T_RHI) {
+    float dx, dz;
+    n2ar_dip_tab(tab, float(R), atan2f(float(s), float(x)), dx, dz);
+    return {double(dx), double(dz)};
+  }
+  return n2ar_dip_body(F, R, x);
+}
+
 }  // namespace hh

@@ -71,6 +71,7 @@ struct TrajIO {
   uint4 *item_trace;          // optional per-item (steps, samples, t_start, t_end) in ns
   const void *dipnet;         // N2-Ar: the folded dipole models (N2arDipFold), global memory
   const void *pesnet;         // N2-Ar: the PES network (N2arPesNet) in the surface precision
+  const void *diptab;         // N2-Ar mixed path: the dipole table (float4, hh_n2ar.cuh) or nullptr
   const double *sat_w;        // CORRELATION_ARRAY: [n_traj][n_sat] weights (nullptr: one C(t))
   int n_sat;                  // satellite temperatures; their C(t) are consecutive N-slices
   // CH4-CO2: samples are written as records (r, quaternion, u) in the surface
@@ -275,6 +276,7 @@ template <typename PHYS, typename STG, bool COMP> struct N2ArSys {
   double inv_mu, inv_II;
   const N2arDipFold *fold;      // shared-memory copies
   const N2arPesNet<PHYS> *pes;
+  const float4 *dtab;           // mixed path: the dipole table (hh_n2ar.cuh), global memory
   template <typename YT> __device__ void rhs(const YT *y, STG *f) const {
     const PHYS r[3] = {PHYS(y[0]), PHYS(y[1]), PHYS(y[2])};
     const PHYS u[3] = {PHYS(y[6]), PHYS(y[7]), PHYS(y[8])};
@@ -314,7 +316,8 @@ template <typename PHYS, typename STG, bool COMP> struct N2ArSys {
     f[10] = STG(-(uh[2] * Gu[0] - uh[0] * Gu[2]));
     f[11] = STG(-(uh[0] * Gu[1] - uh[1] * Gu[0]));
   }
-  // q = (r[3], u[3]); the dipole is FP64 on both precision paths (hh_n2ar.cuh)
+  // q = (r[3], u[3]); the body-frame dipole is the FP64 network on the FP64 path and
+  // the FP32 table of hh_n2ar.cuh (the network outside its R range) on the mixed path
   __device__ void dipole(const double *q, PHYS d[3]) const {
     const double R2 = q[0] * q[0] + q[1] * q[1] + q[2] * q[2];
     const double iR = rsqrt(R2);
@@ -322,10 +325,14 @@ template <typename PHYS, typename STG, bool COMP> struct N2ArSys {
     const double rh[3] = {q[0] * iR, q[1] * iR, q[2] * iR};
     const double uh[3] = {q[3] * iu, q[4] * iu, q[5] * iu};
     const double x = rh[0] * uh[0] + rh[1] * uh[1] + rh[2] * uh[2];
-    const N2arDipBody<double> b = n2ar_dip_body(fold, R2 * iR, x);
     const double e[3] = {uh[0] - x * rh[0], uh[1] - x * rh[1], uh[2] - x * rh[2]};
     const double en2 = e[0] * e[0] + e[1] * e[1] + e[2] * e[2];
     const double ie = en2 > 0.0 ? rsqrt(en2) : 0.0;
+    N2arDipBody<double> b;
+    if constexpr (sizeof(PHYS) == 4)
+      b = dtab ? n2ar_dip_body_mixed(dtab, fold, R2 * iR, x, sqrt(en2)) : n2ar_dip_body(fold, R2 * iR, x);
+    else
+      b = n2ar_dip_body(fold, R2 * iR, x);
 #pragma unroll
     for (int c = 0; c < 3; ++c) d[c] = PHYS(b.dz * rh[c] + b.dx * e[c] * ie);
   }
@@ -1013,6 +1020,7 @@ __global__ void __launch_bounds__(traj_threads<PHYS>(), TRAJ_MIN_BLOCKS)
     __syncthreads();
     sys.fold = fold;
     sys.pes = pes;
+    sys.dtab = static_cast<const float4 *>(io.diptab);
     auto *ws = reinterpret_cast<WarpSamples<STG, PHYS, Sys::NQ> *>(smem_raw + sizeof(N2arDipFold) +
                                                                    sizeof(N2arPesNet<PHYS>));
     traj_body<Sys, PHYS, STG>(sys, P, io, ws);

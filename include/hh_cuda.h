@@ -233,6 +233,12 @@ int hh_cuda_debug_inject(int traj, int dir, int k, int status);
  * call fills with (steps, samples, start ns, end ns) per half-trajectory item
  * (item 2*traj + dir); NULL unregisters */
 int hh_cuda_debug_item_trace(uint32_t *out, uint64_t capacity_words);
+/* Diagnostic (no counterpart in the reference; the reference evaluates the N2-Ar
+ * dipole in PES-IDS/ai_ids_n2_ar_pip_nn.cpp:83-127): the body-frame dipole
+ * (d_x, d_z) of the N2-Ar system at n points (R[i] bohr, T[i] = angle between the
+ * intermolecular axis and the N2 axis) as the given precision path evaluates it,
+ * into out[2 n]: the FP64 network, or the mixed path's FP32 table. */
+int hh_cuda_debug_n2ar_dipole(int precision, const double *R, const double *T, uint64_t n, double *out);
 
 /* Diagnostic (no counterpart in the reference): measured FMA throughput of the
  * CUDA cores in TFLOP/s (precision HH_PRECISION_FP64 or, for FP32,

@@ -73,3 +73,41 @@ def test_m0_matches_oracle():
     np.testing.assert_allclose(m64, mref, rtol=1e-10)
     np.testing.assert_allclose(m32, m64, rtol=1e-4)
     assert np.all(e64 > 0) and np.all(e64 < 0.1 * m64)
+
+
+def test_mixed_dipole_table_matches_network():
+    """The mixed path's FP32 dipole table against the FP64 network (itself checked
+    against the oracle here): within 2e-6 of the largest |d| over T at the same R,
+    inside the table's range [4.5, 60) bohr and across its cell edges; outside it the
+    mixed path evaluates the network."""
+    import hawaiihybrid_b200 as hh
+    from hawaiihybrid_b200 import _lib
+    lib_system("n2ar")
+    L = _lib.load()
+    rng = np.random.default_rng(11)
+    n = 1500
+    R = np.concatenate([rng.uniform(4.5, 60.0, n), np.array([4.5, 9.5, 12.5, 20.0, 59.999]),
+                        rng.uniform(3.8, 4.5, 20), rng.uniform(60.0, 80.0, 20)])
+    T = np.concatenate([rng.uniform(0.0, np.pi, n), np.array([0.0, np.pi / 12, np.pi / 2, np.pi, 1e-4]),
+                        rng.uniform(0.0, np.pi, 40)])
+    m = len(R)
+    Tg = np.linspace(0.0, np.pi, 25)
+    Rs = np.repeat(R, len(Tg))
+    Ts = np.tile(Tg, m)
+
+    def dip(prec, r, t):
+        out = np.zeros(2 * len(r))
+        _lib.check(L.hh_cuda_debug_n2ar_dipole(prec, np.ascontiguousarray(r), np.ascontiguousarray(t), len(r), out))
+        return out.reshape(-1, 2)
+
+    d64 = dip(hh.PRECISION_FP64, R, T)
+    d32 = dip(hh.PRECISION_MIXED, R, T)
+    scale = np.abs(dip(hh.PRECISION_FP64, Rs, Ts)).reshape(m, -1).max(axis=1)
+    for i in range(0, m, 97):
+        ref = O.n2ar_dip_mol(R[i], T[i])
+        # the network's output is a difference of O(0.1) charges: about 1e-15 bohr e absolute
+        np.testing.assert_allclose(d64[i], [ref[0], ref[2]], rtol=0, atol=1e-14 + 1e-9 * scale[i])
+    err = np.abs(d32 - d64).max(axis=1) / scale
+    assert err.max() < 2e-6, (err.max(), R[np.argmax(err)], T[np.argmax(err)])
+    outside = (R < 4.5) | (R >= 60.0)
+    np.testing.assert_allclose(d32[outside], d64[outside], rtol=0, atol=1e-12)
