@@ -117,6 +117,8 @@ struct Ctx {
   DevBuf<unsigned long long> counters;
   DevBuf<unsigned int> status_hist, queue;
   DevBuf<int> fail_flag, fail_list, fail_count, items;
+  DevBuf<unsigned char> handoff;   // open items handed from the bulk to the solo kernel
+  DevBuf<unsigned int> hcount;     // n_handoff, solo cursor, closed items
   DevBuf<uint4> trace;
   // CORRELATION_ARRAY weights [n][n_sat]: with ratios (C(t)) and without (nstar)
   DevBuf<double> sat_w, sat_wraw;
@@ -351,6 +353,35 @@ int launch_traj(const TrajParams &P, const TrajIO &io, int *grid_out) {
   int grid = std::max(1, per_sm) * g.num_sms;
   long long need = (io.n_items + TRAJ_THREADS - 1) / TRAJ_THREADS;
   if (need < grid) grid = (int)std::max(1LL, need);
+  if constexpr (SYS == SYS_N2AR) {
+    // the last open items (and all items of a launch that small) run one per warp
+    // in the solo kernel, whose lanes share the right-hand side of one trajectory
+    auto solo = traj_kernel<SYS, PHYS, STG, COMP, true>;
+    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(solo, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    int per_sm_solo = 0;
+    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_solo, solo, TRAJ_THREADS, smem));
+    const int solo_grid = std::max(1, per_sm_solo) * g.num_sms;
+    const unsigned cap = (unsigned)solo_grid * (TRAJ_THREADS / 32);
+    CK(g.handoff.ensure((size_t)cap * sizeof(HandoffState<12, PHYS, STG>)));
+    CK(g.hcount.ensure(4));
+    CK(cudaMemsetAsync(g.hcount.p, 0, 4 * sizeof(unsigned int), g.st));
+    TrajIO io2 = io;
+    io2.handoff = g.handoff.p;
+    io2.n_handoff = g.hcount.p;
+    io2.solo_cursor = g.hcount.p + 1;
+    io2.done = g.hcount.p + 2;
+    io2.handoff_at = cap;
+    if ((unsigned)io.n_items > cap) {
+      kern<<<grid, TRAJ_THREADS, smem, g.st>>>(P, io2, g.d_tab);
+      CK(cudaGetLastError());
+      g_launches += 1;
+    }
+    solo<<<solo_grid, TRAJ_THREADS, smem, g.st>>>(P, io2, g.d_tab);
+    CK(cudaGetLastError());
+    g_launches += 1;
+    if (grid_out) *grid_out = grid;
+    return HH_OK;
+  }
   kern<<<grid, TRAJ_THREADS, smem, g.st>>>(P, io, g.d_tab);
   CK(cudaGetLastError());
   g_launches += 1;
@@ -1539,6 +1570,8 @@ void hh_cuda_shutdown(void) {
   g.fail_list.release();
   g.fail_count.release();
   g.items.release();
+  g.handoff.release();
+  g.hcount.release();
   g.trace.release();
   g.sat_w.release();
   g.sat_wraw.release();

@@ -134,18 +134,55 @@ template <typename T> struct N2arGrad {
   T g1, g2;  // dV/dd1, dV/dd2 in Hartree/bohr
 };
 
-// dV/dd1, dV/dd2 (Hartree/bohr) for d1 = |N1-Ar|, d2 = |N2-Ar|, out of line.  The
-// PIPs and their Jacobian are unrolled over the monomial table; the network is a
-// runtime loop over the 32 hidden units (forward and backward in one pass) with
-// the weights of `net` (shared memory in the kernels), so the code stays small.
+// Arithmetic of the PES gradient with the rounding of every operation fixed
+// (no contraction left to the compiler), so that the per-lane and the cooperative
+// gradient below give bit-identical results.
+__device__ __forceinline__ float n2_mul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double n2_mul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float n2_add(float a, float b) { return __fadd_rn(a, b); }
+__device__ __forceinline__ double n2_add(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float n2_sub(float a, float b) { return __fsub_rn(a, b); }
+__device__ __forceinline__ double n2_sub(double a, double b) { return __dsub_rn(a, b); }
+__device__ __forceinline__ float n2_fma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double n2_fma(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float n2_div(float a, float b) { return __fdiv_rn(a, b); }
+__device__ __forceinline__ double n2_div(double a, double b) { return __ddiv_rn(a, b); }
+
+// y(d) of an N-Ar pair and dy/dd as n2ar_pair_y, with fixed rounding
+template <typename T> __device__ __forceinline__ void n2ar_pair_y_rn(T d, T &y, T &dy) {
+  const T e = exp(-n2_mul(d, T(0.5)));
+  if (d < T(6)) {
+    y = e;
+    dy = -n2_mul(e, T(0.5));
+    return;
+  }
+  const T d2 = n2_mul(d, d), d6 = n2_mul(n2_mul(d2, d2), d2), d7 = n2_mul(d6, d);
+  const T a6 = n2_div(T(1e4), d6), a7 = n2_div(T(6e4), d7);
+  if (d < T(20)) {
+    const T w = T(14), r = n2_div(n2_sub(d, T(6)), w);
+    const T r2 = n2_mul(r, r), r3 = n2_mul(r2, r), r4 = n2_mul(r3, r), r5 = n2_mul(r4, r);
+    const T sw = n2_add(n2_sub(n2_mul(T(10), r3), n2_mul(T(15), r4)), n2_mul(T(6), r5));
+    const T ds = n2_div(n2_add(n2_sub(n2_mul(T(30), r2), n2_mul(T(60), r3)), n2_mul(T(30), r4)), w);
+    const T om = n2_sub(T(1), sw);
+    y = n2_add(n2_mul(om, e), n2_mul(sw, a6));
+    dy = n2_sub(n2_add(n2_sub(-n2_mul(ds, e), n2_mul(n2_mul(om, e), T(0.5))), n2_mul(ds, a6)), n2_mul(sw, a7));
+  } else {
+    y = a6;
+    dy = -a7;
+  }
+}
+
+// network inputs of the gradient: the scaled PIPs ptr_i = (p_i - mean_i) / scale_i
+// and the PIP Jacobian dp_i/dy_1, dp_i/dy_2 (the monomial table unrolled)
 template <typename T>
-__device__ __noinline__ N2arGrad<T> n2ar_pes_grad(const N2arPesNet<T> *net, T d1, T d2) {
+__device__ __forceinline__ void n2ar_grad_inputs(const N2arPesNet<T> *net, T d1, T d2, T (&ptr)[N2AR_PES_NP],
+                                                 T (&j1)[N2AR_PES_NP], T (&j2)[N2AR_PES_NP], T &dy1, T &dy2) {
   constexpr int NP = N2AR_PES_NP;
-  T y1, dy1, y2, dy2;
-  n2ar_pair_y(d1, y1, dy1);
-  n2ar_pair_y(d2, y2, dy2);
+  T y1, y2;
+  n2ar_pair_y_rn(d1, y1, dy1);
+  n2ar_pair_y_rn(d2, y2, dy2);
   const T y[3] = {exp(-T(N2AR_L) / T(2)), y1, y2};
-  T p[NP], j1[NP], j2[NP];
+  T p[NP];
 #pragma unroll
   for (int i = 0; i < NP; ++i) p[i] = j1[i] = j2[i] = T(0);
 #pragma unroll
@@ -154,8 +191,8 @@ __device__ __noinline__ N2arGrad<T> n2ar_pes_grad(const N2arPesNet<T> *net, T d1
     T prod = T(1);
 #pragma unroll
     for (int k = 0; k < 4; ++k)
-      if (hh_n2ar_pes_var[m][k] >= 0) prod *= y[hh_n2ar_pes_var[m][k]];
-    p[pi] += prod;
+      if (hh_n2ar_pes_var[m][k] >= 0) prod = n2_mul(prod, y[hh_n2ar_pes_var[m][k]]);
+    p[pi] = n2_add(p[pi], prod);
 #pragma unroll
     for (int k = 0; k < 4; ++k) {
       const int vk = hh_n2ar_pes_var[m][k];
@@ -163,38 +200,88 @@ __device__ __noinline__ N2arGrad<T> n2ar_pes_grad(const N2arPesNet<T> *net, T d1
         T d = T(1);
 #pragma unroll
         for (int i = 0; i < 4; ++i)
-          if (i != k && hh_n2ar_pes_var[m][i] >= 0) d *= y[hh_n2ar_pes_var[m][i]];
-        if (vk == 1) j1[pi] += d;
-        else j2[pi] += d;
+          if (i != k && hh_n2ar_pes_var[m][i] >= 0) d = n2_mul(d, y[hh_n2ar_pes_var[m][i]]);
+        if (vk == 1) j1[pi] = n2_add(j1[pi], d);
+        else j2[pi] = n2_add(j2[pi], d);
       }
     }
   }
-  T ptr[NP], a[NP];
 #pragma unroll
-  for (int i = 0; i < NP; ++i) {
-    ptr[i] = (p[i] - net->xmean[i]) * net->ixscale[i];
-    a[i] = T(0);
-  }
+  for (int i = 0; i < NP; ++i) ptr[i] = n2_mul(n2_sub(p[i], net->xmean[i]), net->ixscale[i]);
+}
+
+// SiLU'(h) W1 of one hidden unit
+template <typename T> __device__ __forceinline__ T n2ar_unit_grad(T h, T w1) {
+  const T e = exp(-h), r = n2_div(T(1), n2_add(T(1), e));
+  return n2_mul(n2_mul(r, n2_add(T(1), n2_mul(n2_mul(h, e), r))), w1);
+}
+
+// dV/dd1, dV/dd2 (Hartree/bohr) for d1 = |N1-Ar|, d2 = |N2-Ar|, out of line.  The
+// PIPs and their Jacobian are unrolled over the monomial table; the network is a
+// runtime loop over the 32 hidden units (forward and backward in one pass) with
+// the weights of `net` (shared memory in the kernels), so the code stays small.
+template <typename T>
+__device__ __noinline__ N2arGrad<T> n2ar_pes_grad(const N2arPesNet<T> *net, T d1, T d2) {
+  constexpr int NP = N2AR_PES_NP;
+  T ptr[NP], j1[NP], j2[NP], a[NP], dy1, dy2;
+  n2ar_grad_inputs(net, d1, d2, ptr, j1, j2, dy1, dy2);
+#pragma unroll
+  for (int i = 0; i < NP; ++i) a[i] = T(0);
 #pragma unroll 1
   for (int j = 0; j < N2AR_PES_NH; ++j) {
     const T *w = net->w0t[j];
     T h = net->b0[j];
 #pragma unroll
-    for (int i = 0; i < NP; ++i) h += ptr[i] * w[i];
-    const T e = exp(-h), r = T(1) / (T(1) + e);
-    const T g = r * (T(1) + h * e * r) * net->w1[j];  // SiLU'(h) W1
+    for (int i = 0; i < NP; ++i) h = n2_fma(ptr[i], w[i], h);
+    const T g = n2ar_unit_grad(h, net->w1[j]);
 #pragma unroll
-    for (int i = 0; i < NP; ++i) a[i] += w[i] * g;
+    for (int i = 0; i < NP; ++i) a[i] = n2_fma(w[i], g, a[i]);
   }
   T a1 = T(0), a2 = T(0);
 #pragma unroll
   for (int i = 0; i < NP; ++i) {
-    const T ai = a[i] * net->ixscale[i];
-    a1 += j1[i] * ai;
-    a2 += j2[i] * ai;
+    const T ai = n2_mul(a[i], net->ixscale[i]);
+    a1 = n2_fma(j1[i], ai, a1);
+    a2 = n2_fma(j2[i], ai, a2);
   }
-  const T s = net->yscale * T(1.0 / HH_HTOCM);
-  return {a1 * dy1 * s, a2 * dy2 * s};
+  const T s = n2_mul(net->yscale, T(1.0 / HH_HTOCM));
+  return {n2_mul(n2_mul(a1, dy1), s), n2_mul(n2_mul(a2, dy2), s)};
+}
+
+// n2ar_pes_grad with the 32 lanes of a warp on one (d1, d2), bit for bit: every
+// lane forms the network inputs, lane j evaluates hidden unit j (the same sum over
+// the 17 inputs, in the same order), lane i < 17 forms a_i = sum_j W0[i][j] g_j
+// over the units in the order of the per-lane loop from values shuffled out of the
+// other lanes, and every lane sums j1_i a_i / xscale_i and j2_i a_i / xscale_i over
+// i in order from the a_i shuffled out of lanes 0..16.  A trajectory therefore
+// takes the same steps in the solo kernel as in the bulk kernel.  All 32 lanes
+// call it with the same arguments.
+template <typename T>
+__device__ __noinline__ N2arGrad<T> n2ar_pes_grad_coop(const N2arPesNet<T> *net, T d1, T d2) {
+  static_assert(N2AR_PES_NH == 32 && N2AR_PES_NP <= 32, "one hidden unit per lane");
+  constexpr unsigned FULL = 0xffffffffu;
+  constexpr int NP = N2AR_PES_NP;
+  T ptr[NP], j1[NP], j2[NP], dy1, dy2;
+  n2ar_grad_inputs(net, d1, d2, ptr, j1, j2, dy1, dy2);
+  const int lane = threadIdx.x & 31;
+  const T *wt = net->w0t[lane];
+  T h = net->b0[lane];
+#pragma unroll
+  for (int i = 0; i < NP; ++i) h = n2_fma(ptr[i], wt[i], h);
+  const T g = n2ar_unit_grad(h, net->w1[lane]);
+  const int ir = lane < NP ? lane : NP - 1;
+  T a = T(0);
+#pragma unroll
+  for (int j = 0; j < N2AR_PES_NH; ++j) a = n2_fma(net->w0t[j][ir], __shfl_sync(FULL, g, j), a);
+  T a1 = T(0), a2 = T(0);
+#pragma unroll
+  for (int i = 0; i < NP; ++i) {
+    const T ai = n2_mul(__shfl_sync(FULL, a, i), net->ixscale[i]);
+    a1 = n2_fma(j1[i], ai, a1);
+    a2 = n2_fma(j2[i], ai, a2);
+  }
+  const T s = n2_mul(net->yscale, T(1.0 / HH_HTOCM));
+  return {n2_mul(n2_mul(a1, dy1), s), n2_mul(n2_mul(a2, dy2), s)};
 }
 
 // V (Hartree) for d1 = |N1-Ar|, d2 = |N2-Ar| (pes_xyz, ai_pes_n2_ar_pip_nn.cpp:127-132)

@@ -88,6 +88,16 @@ struct TrajIO {
   // added into crln; rec_len receives the stored samples per item
   void *series;
   int fwd_only;               // items are the forward branches only (item = 2 * index)
+  // hand-off of the last items of a launch to the solo kernel (one warp per item):
+  // the bulk kernel counts closed items in *done; once n_items - *done <= handoff_at
+  // its warps store the state of their open items in `handoff` (slots counted by
+  // *n_handoff) and stop; the solo kernel resumes them (cursor *solo_cursor), then
+  // takes what is left in the queue.  handoff == nullptr: no hand-off.
+  void *handoff;
+  unsigned int *n_handoff;
+  unsigned int *solo_cursor;
+  unsigned int *done;
+  unsigned int handoff_at;
 };
 constexpr int HH_REC_WORDS = 12;  // r[3], q[4], u[3], padding
 
@@ -135,6 +145,7 @@ __device__ void load_tables(Co2arTables<T> *s, const Co2arTablesGlobal *g) {
 
 // ---- systems ----
 template <typename PHYS, typename STG, bool COMP> struct HeArSys {
+  static constexpr bool SOLO = false;  // per-lane right-hand side only
   static constexpr int N = 6;
   static constexpr int QP = 6;
   // components the dipole and the R > Rcut test read: r
@@ -199,6 +210,7 @@ __device__ __noinline__ DipSums<T> co2ar_dip_sums(const Co2arTables<T> *tb, T R,
 }
 
 template <typename PHYS, typename STG, bool COMP> struct Co2ArSys {
+  static constexpr bool SOLO = false;
   static constexpr int N = 12;
   static constexpr int QP = 10;
   // components the dipole and the R > Rcut test read: r and u
@@ -266,7 +278,10 @@ template <typename PHYS, typename STG, bool COMP> struct Co2ArSys {
 // Dipole: mu = d_z r^ + d_x (u^ - x r^)/|u^ - x r^| with the body-frame (d_x, d_z) at
 // (R, x = r^.u^): the Euler-angle rotation of the reference (examples/correlation_n2_ar.cpp:52-76)
 // maps body z to r^ and body x to the in-plane normal to r^ on the N1 side.
-template <typename PHYS, typename STG, bool COMP> struct N2ArSys {
+// SOLO_: the right-hand side of one trajectory held by all 32 lanes of a warp,
+// evaluated cooperatively (n2ar_pes_grad_coop)
+template <typename PHYS, typename STG, bool COMP, bool SOLO_ = false> struct N2ArSys {
+  static constexpr bool SOLO = SOLO_;
   static constexpr int N = 12;
   static constexpr int QP = 10;
   static constexpr int NQ = 6;
@@ -291,7 +306,11 @@ template <typename PHYS, typename STG, bool COMP> struct N2ArSys {
     }
     const PHYS i1 = inv_sqrt(e1[0] * e1[0] + e1[1] * e1[1] + e1[2] * e1[2]);
     const PHYS i2 = inv_sqrt(e2[0] * e2[0] + e2[1] * e2[1] + e2[2] * e2[2]);
-    const N2arGrad<PHYS> g = n2ar_pes_grad<PHYS>(pes, PHYS(1) / i1, PHYS(1) / i2);
+    N2arGrad<PHYS> g;
+    if constexpr (SOLO)
+      g = n2ar_pes_grad_coop<PHYS>(pes, PHYS(1) / i1, PHYS(1) / i2);
+    else
+      g = n2ar_pes_grad<PHYS>(pes, PHYS(1) / i1, PHYS(1) / i2);
     const PHYS a1 = g.g1 * i1, a2 = g.g2 * i2;
     PHYS Gr[3], Gu[3];
 #pragma unroll
@@ -597,6 +616,16 @@ __device__ __forceinline__ void warp_add_counter(unsigned long long *dst, unsign
   if ((threadIdx.x & 31) == 0 && s) atomicAdd(dst, s);
 }
 
+// state of an open item between the bulk and the solo kernel
+template <int N, typename PHYS, typename STG> struct HandoffState {
+  double y[N];
+  STG f0[N];  // f(y) (first stage of the next step)
+  double t, h;
+  PHYS mu0[3], curr;
+  int item, k, since, total, flags;  // flags: rejected | exited << 1
+  unsigned steps, samples, t_begin;  // item trace so far
+};
+
 // ---------------------------------------------------------------------------
 // warp-synchronous persistent loop over half-trajectory items
 // ---------------------------------------------------------------------------
@@ -624,61 +653,144 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
   bool exited = false;  // the item ended by R > Rcut
   unsigned long long t_begin = 0ull;
   unsigned s0 = 0, m0 = 0;
+  // the owner of the warp's item in solo mode (every other lane mirrors it); all
+  // lanes own their items in bulk mode
+  const bool owner = !Sys::SOLO || lane == 0;
+  using Handoff = HandoffState<Sys::N, PHYS, STG>;
+  // start item `it` from its phase point (all lanes of the warp that call it)
+  auto start_item = [&](int it) {
+    item = it;
+    const int traj = item >> 1;
+    crln = io.crln + (size_t)(traj / io.traj_per_iter) * (size_t)P.N;
+    satw = io.sat_w ? io.sat_w + (size_t)traj * io.n_sat : nullptr;
+    if (io.item_trace) t_begin = globaltimer_ns();
+    s0 = nsteps;
+    m0 = nsamp;
+    // out-of-line set-up writes through pointers to temporaries only, so
+    // y, K and mu0 never become addressable and stay in registers
+    double y_t[N];
+    STG f_t[N];
+    PHYS mu_t[3];
+    item_setup<Sys, PHYS, STG>(sys, P, io.ic + (size_t)traj * Sys::QP, item & 1, y_t, f_t, mu_t, &h);
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+      y[i] = y_t[i];
+      K[0][i] = f_t[i];
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) mu0[c] = mu_t[c];
+    if (owner) {
+      if constexpr (Sys::RECORDS) {
+        if ((item & 1) == 0) {
+          PHYS *rec = static_cast<PHYS *>(io.records) + (size_t)traj * io.rec_stride * HH_REC_WORDS;
+#pragma unroll
+          for (int c = 0; c < Sys::NQ; ++c) rec[c] = PHYS(y_t[Sys::qidx(c)]);
+        }
+      } else {
+        if (io.series && (item & 1) == 0) {
+          PHYS *sv = static_cast<PHYS *>(io.series) + (size_t)traj * io.rec_stride * 4;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) sv[c] = mu_t[c];
+        }
+      }
+    }
+    nrhs += 2;
+    t = 0.0;
+    k = 1;
+    since = total = 0;
+    rejected = false;
+    exited = false;
+    prev = curr = PHYS(0);
+  };
+  auto item_of = [&](unsigned idx) {
+    return io.items ? io.items[idx] : (io.fwd_only ? 2 * (int)idx : (int)idx);
+  };
+  bool handing = false;  // bulk mode: this warp hands its open items to the solo kernel
+  unsigned round = 0;
   for (;;) {
-    // ---- refill: lanes without an item take the next ones (one atomic per warp) ----
-    const bool need = (item == -1);
-    const unsigned needmask = __ballot_sync(FULL, need);
-    if (needmask) {
-      unsigned base = 0;
-      const int leader = __ffs(needmask) - 1;
-      if (lane == leader) base = atomicAdd(io.queue, (unsigned)__popc(needmask));
-      base = __shfl_sync(FULL, base, leader);
-      if (need) {
-        const unsigned idx = base + __popc(needmask & ((1u << lane) - 1u));
-        if (idx < (unsigned)io.n_items) {
-          item = io.items ? io.items[idx] : (io.fwd_only ? 2 * (int)idx : (int)idx);
+    if constexpr (!Sys::SOLO) {
+      // ---- hand-off: once few items remain open, store them for the solo kernel ----
+      if (io.handoff && !handing && ((++round & 7u) == 0u)) {
+        unsigned done = 0;
+        if (lane == 0) done = *reinterpret_cast<volatile unsigned int *>(io.done);
+        done = __shfl_sync(FULL, done, 0);
+        handing = (unsigned)io.n_items - done <= io.handoff_at;
+      }
+      if (handing) {
+        if (item >= 0) {
+          Handoff *hs = static_cast<Handoff *>(io.handoff) + atomicAdd(io.n_handoff, 1u);
+#pragma unroll
+          for (int i = 0; i < N; ++i) {
+            hs->y[i] = y[i];
+            hs->f0[i] = K[0][i];
+          }
+          hs->t = t;
+          hs->h = h;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) hs->mu0[c] = mu0[c];
+          hs->curr = curr;
+          hs->item = item;
+          hs->k = k;
+          hs->since = since;
+          hs->total = total;
+          hs->flags = (rejected ? 1 : 0) | (exited ? 2 : 0);
+          hs->steps = nsteps - s0;
+          hs->samples = nsamp - m0;
+          hs->t_begin = (unsigned)(t_begin & 0xffffffffu);
+        }
+        item = -2;
+      }
+      // ---- refill: lanes without an item take the next ones (one atomic per warp) ----
+      const bool need = (item == -1);
+      const unsigned needmask = __ballot_sync(FULL, need);
+      if (needmask) {
+        unsigned base = 0;
+        const int leader = __ffs(needmask) - 1;
+        if (lane == leader) base = atomicAdd(io.queue, (unsigned)__popc(needmask));
+        base = __shfl_sync(FULL, base, leader);
+        if (need) {
+          const unsigned idx = base + __popc(needmask & ((1u << lane) - 1u));
+          if (idx < (unsigned)io.n_items) start_item(item_of(idx));
+          else item = -2;
+        }
+      }
+    } else {
+      // ---- solo refill: the warp resumes a handed-off item, else takes the next
+      // one from the queue; every lane holds the same item ----
+      if (item == -1) {
+        unsigned idx = 0;
+        if (lane == 0) idx = atomicAdd(io.solo_cursor, 1u);
+        idx = __shfl_sync(FULL, idx, 0);
+        if (idx < *io.n_handoff) {
+          const Handoff *hs = static_cast<const Handoff *>(io.handoff) + idx;
+#pragma unroll
+          for (int i = 0; i < N; ++i) {
+            y[i] = hs->y[i];
+            K[0][i] = hs->f0[i];
+          }
+          t = hs->t;
+          h = hs->h;
+#pragma unroll
+          for (int c = 0; c < 3; ++c) mu0[c] = hs->mu0[c];
+          prev = curr = hs->curr;
+          item = hs->item;
+          k = hs->k;
+          since = hs->since;
+          total = hs->total;
+          rejected = (hs->flags & 1) != 0;
+          exited = (hs->flags & 2) != 0;
+          s0 = nsteps - hs->steps;
+          m0 = nsamp - hs->samples;
+          t_begin = hs->t_begin;
           const int traj = item >> 1;
           crln = io.crln + (size_t)(traj / io.traj_per_iter) * (size_t)P.N;
           satw = io.sat_w ? io.sat_w + (size_t)traj * io.n_sat : nullptr;
-          if (io.item_trace) t_begin = globaltimer_ns();
-          s0 = nsteps;
-          m0 = nsamp;
-          // out-of-line set-up writes through pointers to temporaries only, so
-          // y, K and mu0 never become addressable and stay in registers
-          double y_t[N];
-          STG f_t[N];
-          PHYS mu_t[3];
-          item_setup<Sys, PHYS, STG>(sys, P, io.ic + (size_t)traj * Sys::QP, item & 1, y_t, f_t,
-                                     mu_t, &h);
-#pragma unroll
-          for (int i = 0; i < N; ++i) {
-            y[i] = y_t[i];
-            K[0][i] = f_t[i];
-          }
-#pragma unroll
-          for (int c = 0; c < 3; ++c) mu0[c] = mu_t[c];
-          if constexpr (Sys::RECORDS) {
-            if ((item & 1) == 0) {
-              PHYS *rec = static_cast<PHYS *>(io.records) + (size_t)traj * io.rec_stride * HH_REC_WORDS;
-#pragma unroll
-              for (int c = 0; c < Sys::NQ; ++c) rec[c] = PHYS(y_t[Sys::qidx(c)]);
-            }
-          } else {
-            if (io.series && (item & 1) == 0) {
-              PHYS *sv = static_cast<PHYS *>(io.series) + (size_t)traj * io.rec_stride * 4;
-#pragma unroll
-              for (int c = 0; c < 3; ++c) sv[c] = mu_t[c];
-            }
-          }
-          nrhs += 2;
-          t = 0.0;
-          k = 1;
-          since = total = 0;
-          rejected = false;
-          exited = false;
-          prev = curr = PHYS(0);
         } else {
-          item = -2;
+          unsigned q = 0;
+          if (lane == 0) q = atomicAdd(io.queue, 1u);
+          q = __shfl_sync(FULL, q, 0);
+          if (q < (unsigned)io.n_items) start_item(item_of(q));
+          else item = -2;
         }
       }
     }
@@ -733,23 +845,25 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
         int kl = (int)fmin(floor(t_new / dt), double(P.N - 1));
         while (kl + 1 <= P.N - 1 && double(kl + 1) * dt <= t_new) ++kl;
         while (kl > k && double(kl) * dt > t_new) --kl;
-        cnt = kl - k + 1;
+        cnt = owner ? kl - k + 1 : 0;  // solo mode: the owner's samples, evaluated by all lanes
+        if (owner) {
 #pragma unroll
-        for (int r = 0; r < 7; ++r)
+          for (int r = 0; r < 7; ++r)
 #pragma unroll
-          for (int c = 0; c < Sys::NQ; ++c) ws->F[r][c][lane] = F[r][c];
+            for (int c = 0; c < Sys::NQ; ++c) ws->F[r][c][lane] = F[r][c];
 #pragma unroll
-        for (int c = 0; c < Sys::NQ; ++c) ws->qold[c][lane] = y[Sys::qidx(c)];
+          for (int c = 0; c < Sys::NQ; ++c) ws->qold[c][lane] = y[Sys::qidx(c)];
 #pragma unroll
-        for (int c = 0; c < 3; ++c) ws->mu0[c][lane] = mu0[c];
-        ws->t0[lane] = t;
-        ws->inv_h[lane] = 1.0 / h_taken;
-        ws->prev[lane] = curr;
-        ws->crln[lane] = crln;
-        ws->satw[lane] = satw;
-        ws->kst[lane] = k;
-        ws->item[lane] = item;
-        ws->cut[lane] = 0xffffffffu;
+          for (int c = 0; c < 3; ++c) ws->mu0[c][lane] = mu0[c];
+          ws->t0[lane] = t;
+          ws->inv_h[lane] = 1.0 / h_taken;
+          ws->prev[lane] = curr;
+          ws->crln[lane] = crln;
+          ws->satw[lane] = satw;
+          ws->kst[lane] = k;
+          ws->item[lane] = item;
+          ws->cut[lane] = 0xffffffffu;
+        }
       }
       int incl = cnt;
 #pragma unroll
@@ -877,7 +991,7 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
         }
         __syncwarp();
       }
-      if (pending) {
+      if (pending && owner) {
         const unsigned cut = ws->cut[lane];
         const int stop = (cut == 0xffffffffu) ? my_off + cnt : min(my_off + cnt, int(cut >> 3));
         const int committed = stop - my_off;
@@ -899,6 +1013,15 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
           }
         }
       }
+      if constexpr (Sys::SOLO) {
+        // the other lanes follow the owner's progress
+        k = __shfl_sync(FULL, k, 0);
+        curr = __shfl_sync(FULL, curr, 0);
+        since = __shfl_sync(FULL, since, 0);
+        status = __shfl_sync(FULL, status, 0);
+        hard = __shfl_sync(FULL, hard, 0);
+        exited = __shfl_sync(FULL, exited ? 1 : 0, 0) != 0;
+      }
       __syncwarp();
     }
 
@@ -913,13 +1036,22 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
       if (k >= P.N) status = HH_ST_OK;
       else if (++since > P.max_steps || ++total > P.max_total_steps) status = HH_ST_MAXSTEPS;
     }
+    if constexpr (!Sys::SOLO) {
+      if (io.done) {
+        const unsigned closing = __ballot_sync(FULL, active && status >= 0);
+        if (lane == 0 && closing) atomicAdd(io.done, (unsigned)__popc(closing));
+      }
+    }
     if (Sys::RECORDS && active && status >= 0) {
-      io.rec_len[item] = k - 1;
-      io.rec_status[item] = status;
+      if (owner) {
+        io.rec_len[item] = k - 1;
+        io.rec_status[item] = status;
+      }
       ++nitems;
       item = -1;
     }
-    if (!Sys::RECORDS && active && status >= 0) {
+    if (!Sys::RECORDS && active && status >= 0 && !owner) item = -1;
+    if (!Sys::RECORDS && active && status >= 0 && owner) {
       const int traj = item >> 1;
       // the t = 0 term is added by branches that are not dropped, so a replay
       // with the opposite weight removes exactly what a dropped trajectory added
@@ -952,6 +1084,7 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
       item = -1;
     }
   }
+  if (!owner) nsteps = nrej = nrhs = ndense = nitems = 0;  // solo mode: counted once per item
   warp_add_counter(&io.counters[0], nsteps);
   warp_add_counter(&io.counters[1], nrej);
   warp_add_counter(&io.counters[2], nrhs);
@@ -988,9 +1121,11 @@ template <int SYS, typename PHYS, typename STG> constexpr size_t traj_smem_bytes
          traj_warps<PHYS>() * sizeof(WarpSamples<STG, PHYS, (SYS == SYS_HEAR ? 3 : SYS == SYS_CH4CO2 ? 10 : 6)>);
 }
 
-template <int SYS, typename PHYS, typename STG, bool COMP>
+// SOLO: one item per warp (the solo kernel of the hand-off; N2-Ar only)
+template <int SYS, typename PHYS, typename STG, bool COMP, bool SOLO = false>
 __global__ void __launch_bounds__(traj_threads<PHYS>(), TRAJ_MIN_BLOCKS)
     traj_kernel(TrajParams P, TrajIO io, const Co2arTablesGlobal *gtab) {
+  static_assert(!SOLO || SYS == SYS_N2AR, "cooperative right-hand side: N2-Ar only");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   if (SYS == SYS_HEAR) {
     using Sys = HeArSys<PHYS, STG, COMP>;
@@ -1009,7 +1144,7 @@ __global__ void __launch_bounds__(traj_threads<PHYS>(), TRAJ_MIN_BLOCKS)
     auto *ws = reinterpret_cast<WarpSamples<STG, PHYS, Sys::NQ> *>(smem_raw);
     traj_body<Sys, PHYS, STG>(sys, P, io, ws);
   } else if (SYS == SYS_N2AR) {
-    using Sys = N2ArSys<PHYS, STG, COMP>;
+    using Sys = N2ArSys<PHYS, STG, COMP, SOLO>;
     Sys sys;
     sys.inv_mu = 1.0 / P.mu;
     sys.inv_II = 1.0 / P.II;

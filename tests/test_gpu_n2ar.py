@@ -111,3 +111,34 @@ def test_mixed_dipole_table_matches_network():
     assert err.max() < 2e-6, (err.max(), R[np.argmax(err)], T[np.argmax(err)])
     outside = (R < 4.5) | (R >= 60.0)
     np.testing.assert_allclose(d32[outside], d64[outside], rtol=0, atol=1e-12)
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_solo_kernel_follows_the_bulk_path(precision):
+    """The last open items of a launch move to the solo kernel (one warp per item,
+    the PES network shared by the lanes); a launch with no more items than warp
+    slots runs there from the start.  The cooperative right-hand side is
+    bit-identical to the per-lane one, so every half-trajectory takes the same steps
+    either way: a 1500-trajectory launch (bulk, then hand-off) against the same
+    trajectories in three launches of 500 (solo only), per item, and the sum of
+    their C(t) against its C(t)."""
+    import hawaiihybrid_b200 as hh
+    from hawaiihybrid_b200 import _lib
+    ms = lib_system("n2ar")
+    L = _lib.load()
+    p = lib_params("n2ar", 2048, 100.0, mixed_tol=3e-8)
+    qp, _ = O.sample(31, oracle_system("n2ar"), oracle_params("n2ar", 2048, 100.0), 200.0, 1500)
+
+    def traced(q):
+        tr = np.zeros(4 * 2 * len(q), dtype=np.uint32)
+        _lib.check(L.hh_cuda_debug_item_trace(tr.ctypes.data, tr.size))
+        crln, st = hh.correlation_from_initial_conditions(ms, p, q, precision)
+        return tr.reshape(-1, 4), crln
+
+    tr_all, c_all = traced(qp)
+    parts = [traced(qp[c:c + 500]) for c in range(0, 1500, 500)]
+    steps = np.concatenate([t[:, 0] for t, _ in parts])
+    assert steps.min() > 0
+    np.testing.assert_array_equal(tr_all[:, 0], steps)   # accepted steps per item
+    c_sum = sum(c for _, c in parts)
+    np.testing.assert_allclose(c_sum, c_all, rtol=0, atol=1e-11 * abs(c_all[0]))
