@@ -66,6 +66,8 @@ def parse():
     ap.add_argument("--n2ar-trajectories", type=int, default=N2AR["n_traj"])
     ap.add_argument("--no-ch4co2", action="store_true", help="skip the CH4-CO2 four-temperature workload")
     ap.add_argument("--ch4co2-per-T", type=int, default=CH4CO2["n_per_T"])
+    ap.add_argument("--only-n2ar", action="store_true",
+                    help="run only the N2-Ar workload and print its block as the JSON line")
     ap.add_argument("--only-ch4co2", action="store_true",
                     help="run only the CH4-CO2 workload and print its block as the JSON line")
     return ap.parse_args()
@@ -261,6 +263,9 @@ def main():
     torch.cuda.set_device(local)
     if args.only_ch4co2:
         print(json.dumps({"ch4co2_four_temperatures": bench_ch4co2(args, hh, H)}), flush=True)
+        return 0
+    if args.only_n2ar:
+        print(json.dumps({"n2ar_pip_nn": bench_n2ar(args, hh, H)}), flush=True)
         return 0
     dist = None
     if ws > 1:
