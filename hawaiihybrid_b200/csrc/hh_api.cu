@@ -131,6 +131,7 @@ struct Ctx {
   DevBuf<int> zim_fail;  // Zimmermann estimate on the record path: dropped trajectories
   // PR_MU: complex series (two buffers) and the spectrum
   DevBuf<double2> pm_a, pm_b;
+  DevBuf<double2> zf_a, zf_b;   // Zimmermann FFT workspace
   DevBuf<double> pm_sf;
   // M0
   DevBuf<double> m0_partials, m0_out;
@@ -414,6 +415,45 @@ int run_traj_dispatch(int precision, const TrajParams &P, const TrajIO &io) {
 
 // device memory the CH4-CO2 record path may hold for one chunk of trajectories
 constexpr size_t CH4_RECORD_BUDGET = size_t(24) << 30;
+// FFT workspace of the Zimmermann estimate (two buffers)
+constexpr size_t ZIMM_FFT_BUDGET = size_t(2) << 30;
+
+// Zimmermann lagged sums of the za.n_traj trajectories whose dipole series are in
+// za.series, by batched FFT cross-correlation (hh_ch4co2_dip.cuh), in sub-chunks
+// whose transforms fit ZIMM_FFT_BUDGET
+template <typename PHYS>
+int zimm_fft(const ZimmArgs &za) {
+  const int N = za.N;
+  int L = 1;
+  while (L < 2 * N - 1) L <<= 1;
+  const size_t per = 3 * (size_t)L * sizeof(double2);
+  const long long m = std::max<long long>(1, std::min<long long>(za.n_traj, (long long)(ZIMM_FFT_BUDGET / (2 * per))));
+  CK(g.zf_a.ensure(3 * (size_t)m * L));
+  CK(g.zf_b.ensure(3 * (size_t)m * L));
+  const int passes = __builtin_ctz((unsigned)L);
+  for (long long t0 = 0; t0 < za.n_traj; t0 += m) {
+    const long long mm = std::min<long long>(m, za.n_traj - t0);
+    zimm_pack_kernel<PHYS><<<(unsigned)((3 * mm * L + 255) / 256), 256, 0, g.st>>>(za, L, t0, mm, g.zf_a.p);
+    CK(cudaGetLastError());
+    double2 *x = g.zf_a.p, *y = g.zf_b.p;
+    for (long long s = 1; s < L; s *= 2) {
+      stockham_batch_kernel<<<(unsigned)((3 * mm * (L / 2) + 255) / 256), 256, 0, g.st>>>(x, y, L, s, 3 * mm);
+      std::swap(x, y);
+    }
+    zimm_cross_kernel<<<(unsigned)((mm * L + 255) / 256), 256, 0, g.st>>>(x, L, mm, y);
+    CK(cudaGetLastError());
+    std::swap(x, y);
+    for (long long s = 1; s < L; s *= 2) {
+      stockham_batch_kernel<<<(unsigned)((mm * (L / 2) + 255) / 256), 256, 0, g.st>>>(x, y, L, s, mm);
+      std::swap(x, y);
+    }
+    const dim3 agrid((unsigned)((N + 255) / 256), (unsigned)((mm + 255) / 256));
+    zimm_accum_kernel<<<agrid, 256, 0, g.st>>>(x, L, N, mm, za.traj_base + t0, za.traj_per_iter, za.w / L, za.crln);
+    CK(cudaGetLastError());
+    g_launches += 3 + 2 * (unsigned long long)passes;
+  }
+  return HH_OK;
+}
 
 // CH4-CO2: the trajectory kernel writes every sample as a record, then the
 // records are sorted by radial piece, their dipoles evaluated in batches and
@@ -534,16 +574,15 @@ int run_records_t(const TrajParams &P, const double *d_ic, uint64_t n, uint64_t 
       za.N = N;
       za.w = 2.0 * P.weight / N;  // ppf ALU^3 / N
       za.crln = g.crln.p;
-      zimm_kernel<PHYS><<<(unsigned)std::min<uint64_t>(nc, 16ull * g.num_sms), 256, 0, g.st>>>(za);
-      CK(cudaGetLastError());
-      g_launches += 1;
+      const int rc = zimm_fft<PHYS>(za);
+      if (rc) return rc;
     }
   }
   return HH_OK;
 }
 
 // Zimmermann estimate for the systems with an inline dipole: the trajectory kernel
-// writes the dipole vector of every stored sample, then zimm_kernel forms each
+// writes the dipole vector of every stored sample, then zimm_fft forms each
 // trajectory's lagged products.  Trajectories go through in chunks whose series fit
 // CH4_RECORD_BUDGET.  Dropped trajectories are skipped (no compensation pass).
 template <typename PHYS>
@@ -579,9 +618,8 @@ int run_series_t(const TrajParams &P, const TrajIO &io0, const double *d_ic, uin
     za.N = N;
     za.w = 2.0 * P.weight / N;  // ppf ALU^3 / N
     za.crln = g.crln.p;
-    zimm_kernel<PHYS><<<(unsigned)std::min<uint64_t>(nc, 16ull * g.num_sms), 256, 0, g.st>>>(za);
-    CK(cudaGetLastError());
-    g_launches += 1;
+    rc = zimm_fft<PHYS>(za);
+    if (rc) return rc;
   }
   return HH_OK;
 }
@@ -1571,6 +1609,8 @@ void hh_cuda_shutdown(void) {
   g.fail_count.release();
   g.items.release();
   g.handoff.release();
+  g.zf_a.release();
+  g.zf_b.release();
   g.hcount.release();
   g.trace.release();
   g.sat_w.release();

@@ -492,8 +492,7 @@ __global__ void __launch_bounds__(256) ch4_corr_kernel(TrajParams P, Ch4CorrArgs
 // trajectory the dipole vectors d[c], c = 0..2N-2, with d[N-1] = mu0, d[N-1+k] = mu(t_k)
 // and d[N-1-k] = mu(-t_k) (zero past a branch's stored samples), give
 //   C(s) += w sum_{c < N} d[c] . d[c+s],   w = ppf ALU^3 / N,
-// for trajectories that were not dropped.  One block per trajectory (grid-stride),
-// one lag per thread; the products are summed in FP64.
+// for trajectories that were not dropped.
 struct ZimmArgs {
   const void *series;         // [traj][slot][4] in the surface precision
   const int *len;             // [2 traj] stored samples per branch
@@ -515,25 +514,75 @@ __device__ __forceinline__ void zimm_d(const PHYS *sv, int N, int lf, int lb, in
   d[0] = double(v[0]); d[1] = double(v[1]); d[2] = double(v[2]);
 }
 
+// FFT form of the lagged sum (the O(N^2) loop of src/hawaii.c:2089-2094).  With
+// a = d[0..N-1] and b = d[0..2N-2], zero-padded to L >= 2N - 1 (a power of two),
+// C(s) = sum_c a[c] . b[c+s] is the circular cross-correlation of a and b for
+// s < N (no term wraps), so with the transform F[k] = sum_j x_j e^{+2 pi i jk/L} of
+// stockham_batch_kernel:
+//   C(s) = (1/L) Re sum_k conj(P_k) e^{+2 pi i sk/L},  P_k = sum_comp conj(A_k) B_k.
+//   1. zimm_pack: per trajectory and component the complex series a_j + i b_j
+//      (zero for a dropped trajectory);
+//   2. log2 L Stockham passes over 3 series per trajectory;
+//   3. zimm_cross: A_k = (Z_k + conj Z_{L-k}) / 2, B_k = (Z_k - conj Z_{L-k}) / 2i, and
+//      conj(P_k) per trajectory;
+//   4. log2 L passes over one series per trajectory;
+//   5. zimm_accum: C(s) += w Re(.)/L into each trajectory's C(t) slice.
+// All transforms are FP64 on both precision paths.
 template <typename PHYS>
-__global__ void __launch_bounds__(256) zimm_kernel(ZimmArgs a) {
-  const int N = a.N;
-  for (long long t = blockIdx.x; t < a.n_traj; t += gridDim.x) {
-    if (a.failed[t]) continue;
+__global__ void __launch_bounds__(256) zimm_pack_kernel(ZimmArgs a, int L, long long t0, long long m, double2 *z) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= 3 * m * L) return;
+  const long long sr = i / L;
+  const int j = (int)(i - sr * L);
+  const long long t = t0 + sr / 3;
+  const int comp = (int)(sr % 3);
+  double av = 0.0, bv = 0.0;
+  if (!a.failed[t] && j <= 2 * a.N - 2) {
     const PHYS *sv = static_cast<const PHYS *>(a.series) + (size_t)t * a.stride * 4;
-    const int lf = a.len[2 * t], lb = a.len[2 * t + 1];
-    double *C = a.crln + ((a.traj_base + t) / a.traj_per_iter) * N;
-    for (int s = threadIdx.x; s < N; s += blockDim.x) {
-      double acc = 0.0;
-      for (int c = 0; c < N; ++c) {
-        double x[3], y[3];
-        zimm_d(sv, N, lf, lb, c, x);
-        zimm_d(sv, N, lf, lb, c + s, y);
-        acc += x[0] * y[0] + x[1] * y[1] + x[2] * y[2];
-      }
-      if (acc != 0.0) atomicAdd(&C[s], a.w * acc);
-    }
+    double d[3];
+    zimm_d(sv, a.N, a.len[2 * t], a.len[2 * t + 1], j, d);
+    bv = d[comp];
+    if (j < a.N) av = d[comp];
   }
+  z[i] = make_double2(av, bv);
+}
+
+__global__ void __launch_bounds__(256) zimm_cross_kernel(const double2 *Z, int L, long long m, double2 *pc) {
+  const long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x;
+  if (i >= m * L) return;
+  const long long t = i / L;
+  const int k = (int)(i - t * L);
+  const int kr = (L - k) & (L - 1);
+  double pr = 0.0, pi = 0.0;
+  for (int c = 0; c < 3; ++c) {
+    const double2 zk = Z[(3 * t + c) * L + k], zm = Z[(3 * t + c) * L + kr];
+    const double ar = 0.5 * (zk.x + zm.x), ai = 0.5 * (zk.y - zm.y);
+    const double br = 0.5 * (zk.y + zm.y), bi = -0.5 * (zk.x - zm.x);
+    pr += ar * br + ai * bi;  // conj(A) B
+    pi += ar * bi - ai * br;
+  }
+  pc[i] = make_double2(pr, -pi);
+}
+
+// grid: x over s < N, y over groups of 256 trajectories
+__global__ void __launch_bounds__(256) zimm_accum_kernel(const double2 *R, int L, int N, long long m,
+                                                         long long t_first, long long traj_per_iter, double w,
+                                                         double *crln) {
+  const int s = blockIdx.x * blockDim.x + threadIdx.x;
+  if (s >= N) return;
+  const long long lo = (long long)blockIdx.y * 256, hi = min(m, lo + 256);
+  long long slice = (t_first + lo) / traj_per_iter;
+  double acc = 0.0;
+  for (long long t = lo; t < hi; ++t) {
+    const long long sl = (t_first + t) / traj_per_iter;
+    if (sl != slice) {
+      if (acc != 0.0) atomicAdd(&crln[slice * N + s], w * acc);
+      acc = 0.0;
+      slice = sl;
+    }
+    acc += R[t * L + s].x;
+  }
+  if (acc != 0.0) atomicAdd(&crln[slice * N + s], w * acc);
 }
 
 }  // namespace hh
