@@ -44,7 +44,7 @@ EXPORTS = (
     "hh_cuda_correlation_ic", "hh_cuda_m0", "hh_cuda_idct_cf_to_sf", "hh_cuda_strerror",
     "hh_cuda_mt_stream", "hh_cuda_debug_inject", "hh_cuda_debug_item_trace", "hh_cuda_fma_peak",
     "hh_cuda_shutdown", "hh_cuda_m0_noalloc", "hh_cuda_correlation_array", "hh_cuda_correlation_temperatures",
-    "hh_cuda_prmu", "hh_cuda_debug_n2ar_dipole",
+    "hh_cuda_prmu", "hh_cuda_debug_n2ar_dipole", "hh_cuda_m2",
 )
 
 
@@ -118,6 +118,7 @@ def load(path: str | None = None):
                                          C.POINTER(Stats)]
     L.hh_cuda_m0.argtypes = [C.POINTER(CalcParamsC), _dp, C.c_int, C.c_uint64, C.c_uint64, C.c_int,
                              _dp, _dp]
+    L.hh_cuda_m2.argtypes = [C.POINTER(CalcParamsC), _dp, C.c_int, C.c_uint64, C.c_uint64, _dp, _dp]
     L.hh_cuda_m0_noalloc.argtypes = L.hh_cuda_m0.argtypes
     L.hh_cuda_correlation_array.argtypes = [C.POINTER(CalcParamsC), C.c_double, _dp, _dp, C.c_int, C.c_uint32,
                                             C.c_uint64, C.c_int, _dp, _dp, C.POINTER(C.c_double),

@@ -791,6 +791,24 @@ int launch_m0(const M0Args &a, int grid, bool mixed, double *partials) {
   return HH_OK;
 }
 
+// the second-moment kernels (FP64)
+int launch_m2(const M0Args &a, int grid, double *partials) {
+  const int block = 256;
+  if (g.sys == SYS_HEAR) {
+    m0_kernel<SYS_HEAR, double, false, 2><<<grid, block, 0, g.st>>>(a, g.d_tab, nullptr, partials);
+  } else if (g.sys == SYS_N2AR) {
+    const size_t smem = sizeof(N2arDipFold);
+    auto k = m0_kernel<SYS_N2AR, double, false, 2>;
+    CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+    k<<<grid, block, smem, g.st>>>(a, g.d_tab, g.d_n2ar_fold, partials);
+  } else {
+    m0_kernel<SYS_CO2AR, double, false, 2><<<grid, block, sizeof(Co2arTables<double>), g.st>>>(
+        a, g.d_tab, nullptr, partials);
+  }
+  CK(cudaGetLastError());
+  return HH_OK;
+}
+
 // ---------------------------------------------------------------------------
 // Scratch of hh_cuda_m0_noalloc: a fixed array compiled into the library, so
 // that M0 can run in a process that must not allocate device memory once its
@@ -1349,6 +1367,52 @@ int hh_cuda_m0(const hh_calc_params *p, const double *T, int nT, uint64_t n_samp
     a.offset = 0;
     a.seed = seed;
     int rc = launch_m0(a, grid, precision_mode == HH_PRECISION_MIXED, g.m0_partials.p);
+    if (rc) return rc;
+    m0_finalize_kernel<<<1, 32, 0, g.st>>>(g.m0_partials.p, grid, g.m0_out.p);
+    CK(cudaGetLastError());
+    double out[M0_MAXT * 2];
+    CK(cudaMemcpyAsync(out, g.m0_out.p, sizeof out, cudaMemcpyDeviceToHost, g.st));
+    CK(cudaStreamSynchronize(g.st));
+    for (int t = 0; t < a.nT; ++t) {
+      double mean = out[2 * t] / double(n_samples);
+      double var = out[2 * t + 1] / double(n_samples) - mean * mean;
+      m[t0 + t] = scale * mean;
+      if (err) err[t0 + t] = scale * sqrt(std::max(var, 0.0) / double(n_samples));
+    }
+  }
+  return HH_OK;
+}
+
+int hh_cuda_m2(const hh_calc_params *p, const double *T, int nT, uint64_t n_samples, uint64_t seed,
+               double *m, double *err) {
+  if (!g.init) return HH_E_NOT_INITIALIZED;
+  if (g.sys == SYS_CH4CO2) return HH_E_UNSUPPORTED_SYSTEM;  // no CH4-CO2 moment integrand
+  if (!p || !T || nT < 1 || !m || n_samples == 0) return HH_E_INVALID_ARGUMENT;
+  if (!(p->sampler_Rmin > 0) || !(p->sampler_Rmax > p->sampler_Rmin)) return HH_E_INVALID_ARGUMENT;
+  if (p->pair_state < 1 || p->pair_state > 3) return HH_E_INVALID_ARGUMENT;
+  for (int t = 0; t < nT; ++t)
+    if (!(T[t] > 0)) return HH_E_INVALID_ARGUMENT;
+  CK(cudaSetDevice(g.device));
+  const int grid = g.num_sms * 4;
+  CK(g.m0_partials.ensure((size_t)grid * M0_MAXT * 2));
+  CK(g.m0_out.ensure(M0_MAXT * 2));
+  const double scale = HH_SECONDCOEFF * 4.0 * HH_PI * (p->sampler_Rmax - p->sampler_Rmin);
+  for (int t0 = 0; t0 < nT; t0 += M0_MAXT) {
+    M0Args a;
+    memset(&a, 0, sizeof a);
+    a.sys = g.sys;
+    a.moment = 2;
+    a.inv_mu = 1.0 / g.mu;
+    a.inv_II = g.sys == SYS_HEAR ? 0.0 : 1.0 / g.II;
+    a.Rmin = p->sampler_Rmin;
+    a.Rmax = p->sampler_Rmax;
+    a.pair_state = p->pair_state;
+    a.nT = std::min(M0_MAXT, nT - t0);
+    for (int t = 0; t < a.nT; ++t) a.invkT[t] = HH_HKT / T[t0 + t];
+    a.n_samples = n_samples;
+    a.offset = 0;
+    a.seed = seed;
+    int rc = launch_m2(a, grid, g.m0_partials.p);
     if (rc) return rc;
     m0_finalize_kernel<<<1, 32, 0, g.st>>>(g.m0_partials.p, grid, g.m0_out.p);
     CK(cudaGetLastError());

@@ -13,6 +13,7 @@
 #define HH_HKT (HH_HARTREE / HH_BOLTZMANN)
 #define HH_PI 3.14159265358979323846
 #define HH_ZEROCOEFF (0.00361479637 / (4.0 * HH_PI))
+#define HH_SECONDCOEFF 13856114.29344114  // src/constants.h:30
 
 // per-half-trajectory status codes (the reference's failure modes,
 // src/hawaii.c:2172-2243)

@@ -19,6 +19,19 @@
 // Sums: per thread FP64 compensated sums of w and plain sums of w^2 per
 // temperature, a fixed-order block reduction, then one fixed-order pass over
 // the block partials.
+//
+// Second moment (calculate_M2, src/hawaii.c:1524-1617; VEGAS integrand_M2,
+// src/hep_hawaii.cpp:228-330): the integrand is |dmu/dt|^2 = qdot^T D D^T qdot with
+// D = dmu/dq and qdot = dH/dp.  At fixed q and kinetic energy K the momentum
+// direction is uniform in the mass-weighted metric, so E[qdot qdot^T | K] =
+// (2K/nu) M^-1 and
+//   M2(T) = SecondCoeff * 4 pi (Rmax - Rmin) * < R^2 (2K/nu) G(q) exp(-V/kT) 1[filter] >,
+//   G(q) = tr(D^T M^-1 D) = |grad_r mu|^2 / mu_red + sum_{b=1,2} |dmu/dphi_b|^2 / I,
+// with nu = 3 (atom-atom) or 5 (linear-atom) and phi_b rotations of u^ about two
+// axes normal to it.  G is formed by central differences with h = 1e-3 (bohr,
+// radian), as the reference forms D, from the FP64 lab-frame dipole of the
+// trajectory kernels at 10 displaced configurations.  The same samples, K included,
+// as M0.
 #pragma once
 
 #include <cuda_runtime.h>
@@ -34,6 +47,8 @@ constexpr int M0_MAXT = 16;  // temperatures per launch chunk
 
 struct M0Args {
   int sys;
+  int moment;                // 0: M0, 2: M2
+  double inv_mu, inv_II;     // M2: 1 / reduced mass, 1 / moment of inertia (a.u.)
   double Rmin, Rmax;
   int pair_state;
   int nT;
@@ -65,9 +80,52 @@ template <typename T> __device__ __forceinline__ T u24(uint32_t w) {
   return (T(w >> 8) + T(0.5)) * T(1.0 / 16777216.0);
 }
 
-template <int SYS, typename PHYS, bool COMP>
+// G(q) of the second moment at distance R and x = cos(angle between r^ and u^), in
+// the frame r^ = z, u^ = (s, 0, x): central differences of the lab dipole over the
+// three Cartesian displacements of r and (linear molecules) the rotations of u^
+// about y and about u^ x y
+template <class Sys>
+__device__ double m2_geometry(const Sys &sys, double R, double x, double inv_mu, double inv_II, bool rotor) {
+  const double h = 1.0e-3;
+  const double s = sqrt(fmax(0.0, (1.0 - x) * (1.0 + x)));
+  double q[6] = {0.0, 0.0, R, s, 0.0, x};
+  double dp[3], dm[3], gt = 0.0, gr = 0.0;
+  for (int a = 0; a < 3; ++a) {
+    const double q0 = q[a];
+    q[a] = q0 + h;
+    sys.dipole(q, dp);
+    q[a] = q0 - h;
+    sys.dipole(q, dm);
+    q[a] = q0;
+    for (int c = 0; c < 3; ++c) gt += (dp[c] - dm[c]) * (dp[c] - dm[c]);
+  }
+  if (rotor) {
+    double sh, ch;
+    sincos(h, &sh, &ch);
+    // about y: u^ -> u^ cos h +- (x, 0, -s) sin h
+    q[3] = s * ch + x * sh;
+    q[5] = x * ch - s * sh;
+    sys.dipole(q, dp);
+    q[3] = s * ch - x * sh;
+    q[5] = x * ch + s * sh;
+    sys.dipole(q, dm);
+    for (int c = 0; c < 3; ++c) gr += (dp[c] - dm[c]) * (dp[c] - dm[c]);
+    // about u^ x y: u^ -> u^ cos h +- y sin h
+    q[3] = s * ch;
+    q[5] = x * ch;
+    q[4] = sh;
+    sys.dipole(q, dp);
+    q[4] = -sh;
+    sys.dipole(q, dm);
+    for (int c = 0; c < 3; ++c) gr += (dp[c] - dm[c]) * (dp[c] - dm[c]);
+  }
+  return (gt * inv_mu + gr * inv_II) / (4.0 * h * h);
+}
+
+template <int SYS, typename PHYS, bool COMP, int MOMENT = 0>
 __global__ void __launch_bounds__(256) m0_kernel(M0Args a, const Co2arTablesGlobal *gtab,
                                                  const void *dipnet, double *partials) {
+  static_assert(MOMENT == 0 || sizeof(PHYS) == 8, "the second moment is evaluated in FP64");
   extern __shared__ unsigned char smem_raw[];
   Co2arTables<PHYS> *tb = reinterpret_cast<Co2arTables<PHYS> *>(smem_raw);
   N2arDipFold *fold = reinterpret_cast<N2arDipFold *>(smem_raw);
@@ -100,6 +158,10 @@ __global__ void __launch_bounds__(256) m0_kernel(M0Args a, const Co2arTablesGlob
       hear_V_dV<PHYS>(R, iR, V, dV);
       PHYS d = hear_dip<PHYS>(R, iR);
       mu2 = d * d;
+      if constexpr (MOMENT == 2) {
+        HeArSys<PHYS, PHYS, false> sys;
+        mu2 = m2_geometry(sys, R, 1.0, a.inv_mu, a.inv_II, false) * (2.0 / 3.0);
+      }
       kappa = -log(u24<PHYS>(w[5])) - log(u24<PHYS>(w[7])) * zc * zc;
     } else if (SYS == SYS_N2AR) {
       PHYS Phi = twopi * u24<PHYS>(w[1]);
@@ -112,8 +174,15 @@ __global__ void __launch_bounds__(256) m0_kernel(M0Args a, const Co2arTablesGlob
       // N1-Ar and N2-Ar distances with the N2 axis at angle acos(x) to r^
       const PHYS h = PHYS(N2AR_L / 2.0), base = R * R + h * h, t = PHYS(2) * h * R * x;
       V = n2ar_pes_energy<PHYS>(sqrt(base - t), sqrt(base + t));
-      const N2arDipBody<double> b = n2ar_dip_body(fold, double(R), double(x));
-      mu2 = PHYS(b.dx * b.dx + b.dz * b.dz);
+      if constexpr (MOMENT == 2) {
+        N2ArSys<PHYS, PHYS, false> sys;
+        sys.fold = fold;
+        sys.dtab = nullptr;
+        mu2 = m2_geometry(sys, R, x, a.inv_mu, a.inv_II, true) * (2.0 / 5.0);
+      } else {
+        const N2arDipBody<double> b = n2ar_dip_body(fold, double(R), double(x));
+        mu2 = PHYS(b.dx * b.dx + b.dz * b.dz);
+      }
       kappa = -log(u24<PHYS>(w[5])) - log(u24<PHYS>(w[6])) - log(u24<PHYS>(w[7])) * zc * zc;
     } else {
       // x = cos(angle between r^ and u^) from the sampled lab angles
@@ -130,6 +199,11 @@ __global__ void __launch_bounds__(256) m0_kernel(M0Args a, const Co2arTablesGlob
       PHYS dz, ax;
       co2ar_dip<PHYS, COMP>(tb->dipx, tb->dipz, tb->fdip, tb->rbound, tb->rlo, R, iR, x, dz, ax);
       mu2 = dz * dz + ax * ax * (PHYS(1) - x) * (PHYS(1) + x);
+      if constexpr (MOMENT == 2) {
+        Co2ArSys<PHYS, PHYS, COMP> sys;
+        sys.tb = tb;
+        mu2 = m2_geometry(sys, R, x, a.inv_mu, a.inv_II, true) * (2.0 / 5.0);
+      }
       kappa = -log(u24<PHYS>(w[5])) - log(u24<PHYS>(w[6])) - log(u24<PHYS>(w[7])) * zc * zc;
     }
     PHYS base = R * R * mu2;
@@ -141,6 +215,7 @@ __global__ void __launch_bounds__(256) m0_kernel(M0Args a, const Co2arTablesGlob
         if (a.pair_state == 1) keep = (H >= PHYS(0));
         else if (a.pair_state == 2) keep = (H <= PHYS(0));
         double wv = keep ? double(base * exp(-V * ikT[t])) : 0.0;
+        if constexpr (MOMENT == 2) wv *= double(kappa / ikT[t]);  // (2K/nu) G with K = kappa kT
         // compensated accumulation of w, plain accumulation of w^2
         double y = wv - c[t];
         double tt = s[t] + y;

@@ -414,6 +414,20 @@ def calculate_m0(ms: MoleculeSystem, params: CalcParams, temperatures: Sequence[
     return m, e
 
 
+def calculate_m2(ms: MoleculeSystem, params: CalcParams, temperatures: Sequence[float], n_samples: int,
+                 seed: int = 1) -> tuple[np.ndarray, np.ndarray]:
+    """Second moment M2(T) for every temperature from one batch of phase-space samples,
+    in FP64 (the quantity the reference prints as "T = ... => M2": calculate_M2,
+    src/hawaii.c:1524-1617, and the VEGAS integrand_M2, src/hep_hawaii.cpp:228-330)."""
+    L = _bind(ms)
+    T = np.ascontiguousarray(temperatures, dtype=np.float64)
+    m = np.empty(T.size)
+    e = np.empty(T.size)
+    pc = params.to_c()
+    check(L.hh_cuda_m2(C.byref(pc), T, T.size, n_samples, seed, m, e))
+    return m, e
+
+
 def analytic_full_partition_function_by_V(ms: MoleculeSystem, Temperature: float) -> float:
     """src/hawaii.c:5071-5090 (ATOM-ATOM, LINEAR_MOLECULE-ATOM, ROTOR-LINEAR_MOLECULE)."""
     if ms.m1_type == ATOM and ms.m2_type == ATOM:

@@ -191,6 +191,16 @@ int hh_cuda_correlation_ic(const hh_calc_params *p, const double *qp0, uint64_t 
 int hh_cuda_m0(const hh_calc_params *p, const double *T, int nT, uint64_t n_samples,
                uint64_t seed, int precision_mode, double *m, double *err);
 
+/* M2 at nT temperatures from n_samples phase-space points (Philox stream `seed`),
+ * all temperatures in one launch, in FP64: m[t] in the units of the reference's
+ * "T = ... => M2" and its one-sigma statistical error err[t].  Replaces
+ * calculate_M2 / mpi_calculate_M2 (src/hawaii.c:1524-1617, 1740-1856) and the VEGAS
+ * integrand_M2 (src/hep_hawaii.cpp:228-330): the same phase-space samples as
+ * hh_cuda_m0, with the momentum average of |dmu/dt|^2 taken at the sampled kinetic
+ * energy.  HH_E_UNSUPPORTED_SYSTEM for CH4-CO2. */
+int hh_cuda_m2(const hh_calc_params *p, const double *T, int nT, uint64_t n_samples,
+               uint64_t seed, double *m, double *err);
+
 /* Allocation-free M0 (no counterpart in the reference).
  *
  * Same arguments, samples and results as hh_cuda_m0, but the call allocates no

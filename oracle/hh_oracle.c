@@ -29,6 +29,7 @@
 #define EPSILON0 8.8541878128e-12
 #define HkT (Hartree / Boltzmann)
 #define ZeroCoeff (0.00361479637 / (4.0 * M_PI))
+#define SecondCoeff 13856114.29344114  /* src/constants.h:30 */
 
 /* ======================================================================== */
 /* MT19937 as configured by mtwist (thirdparty/mtwist.c:372-400, 640-796,   */
@@ -1657,7 +1658,38 @@ typedef struct {
     int nT;
     uint64_t begin, end, seed;
     double *wsum, *wsq;
+    int moment;  /* 0: M0, 2: M2 */
 } m0_job;
+
+/* Second moment (calculate_M2, src/hawaii.c:1524-1617; integrand_M2,               */
+/* src/hep_hawaii.cpp:228-330) in the reference's own coordinates: D = dmu/dq by     */
+/* central differences with h = 1e-3 in q = (Phi, Theta, R[, phi, theta]) as there,  */
+/* and the momentum average at kinetic energy K, E[|D^T qdot|^2 | K] =              */
+/* (2K/nu) sum_i |dmu/dq_i|^2 (M^-1)_ii with the diagonal inverse metric of H:       */
+/* 1/(mu R^2 sin^2 Theta), 1/(mu R^2), 1/mu, 1/(I sin^2 theta), 1/I.                */
+static double m2_geometry_q(const hho_system *sys, const double *q0, int nq) {
+    const double h = 1.0e-3;
+    double q[5], dp[3], dm[3], g = 0.0;
+    for (int i = 0; i < nq; ++i) q[i] = q0[i];
+    const double R = q0[2], sT = sin(q0[1]);
+    double minv[5] = {1.0 / (sys->mu * R * R * sT * sT), 1.0 / (sys->mu * R * R), 1.0 / sys->mu, 0.0, 0.0};
+    if (nq == 5) {
+        const double st = sin(q0[4]);
+        minv[3] = 1.0 / (sys->II * st * st);
+        minv[4] = 1.0 / sys->II;
+    }
+    for (int i = 0; i < nq; ++i) {
+        q[i] = q0[i] + h;
+        hho_dipole(sys, q, dp);
+        q[i] = q0[i] - h;
+        hho_dipole(sys, q, dm);
+        q[i] = q0[i];
+        double s2 = 0.0;
+        for (int c = 0; c < 3; ++c) s2 += (dp[c] - dm[c]) * (dp[c] - dm[c]);
+        g += s2 / (4.0 * h * h) * minv[i];
+    }
+    return g;
+}
 
 static void *m0_worker(void *arg) {
     m0_job *J = arg;
@@ -1689,12 +1721,17 @@ static void *m0_worker(void *arg) {
         double d[3];
         hho_dipole(J->sys, q, d);
         double base = R * R * (d[0] * d[0] + d[1] * d[1] + d[2] * d[2]);
+        if (J->moment == 2) {
+            const int nq = is_linear(J->sys) ? 5 : 3;
+            base = R * R * m2_geometry_q(J->sys, q, nq) * 2.0 / (is_linear(J->sys) ? 5.0 : 3.0);
+        }
         for (int t = 0; t < nT; ++t) {
             double H = kappa / invkT[t] + V;
             int keep = 1;
             if (J->p->pair_state == HHO_PS_FREE_AND_METASTABLE) keep = (H >= 0.0);
             else if (J->p->pair_state == HHO_PS_BOUND) keep = (H <= 0.0);
             double wv = keep ? base * exp(-V * invkT[t]) : 0.0;
+            if (J->moment == 2) wv *= kappa / invkT[t];  /* (2K/nu) G, K = kappa kT */
             J->wsum[t] += wv;
             J->wsq[t] += wv * wv;
         }
@@ -1702,9 +1739,9 @@ static void *m0_worker(void *arg) {
     return NULL;
 }
 
-int hho_m0(const hho_system *sys, const hho_params *p, const double *T, int nT,
-           uint64_t n_samples, uint64_t seed, uint64_t offset, int nthreads,
-           double *wsum, double *wsq) {
+static int moment_mc(const hho_system *sys, const hho_params *p, const double *T, int nT,
+                     uint64_t n_samples, uint64_t seed, uint64_t offset, int nthreads,
+                     double *wsum, double *wsq, int moment) {
     if (sys->system == HHO_SYS_CH4CO2) return -1;  /* no CH4-CO2 moment integrand */
     if (nT > 64 || nT < 1) return -1;
     if (nthreads < 1) nthreads = 1;
@@ -1714,7 +1751,7 @@ int hho_m0(const hho_system *sys, const hho_params *p, const double *T, int nT,
     for (int w = 0; w < nthreads; ++w) {
         jobs[w] = (m0_job){sys, p, T, nT, offset + n_samples * w / nthreads,
                            offset + n_samples * (w + 1) / nthreads, seed,
-                           calloc(nT, sizeof(double)), calloc(nT, sizeof(double))};
+                           calloc(nT, sizeof(double)), calloc(nT, sizeof(double)), moment};
         pthread_create(&th[w], NULL, m0_worker, &jobs[w]);
     }
     for (int t = 0; t < nT; ++t) wsum[t] = wsq[t] = 0.0;
@@ -1726,7 +1763,20 @@ int hho_m0(const hho_system *sys, const hho_params *p, const double *T, int nT,
     return 0;
 }
 
+int hho_m0(const hho_system *sys, const hho_params *p, const double *T, int nT,
+           uint64_t n_samples, uint64_t seed, uint64_t offset, int nthreads,
+           double *wsum, double *wsq) {
+    return moment_mc(sys, p, T, nT, n_samples, seed, offset, nthreads, wsum, wsq, 0);
+}
+
+int hho_m2(const hho_system *sys, const hho_params *p, const double *T, int nT,
+           uint64_t n_samples, uint64_t seed, uint64_t offset, int nthreads,
+           double *wsum, double *wsq) {
+    return moment_mc(sys, p, T, nT, n_samples, seed, offset, nthreads, wsum, wsq, 2);
+}
+
 double hho_m0_scale(const hho_params *p) { return ZeroCoeff * 4.0 * M_PI * (p->Rmax - p->Rmin); }
+double hho_m2_scale(const hho_params *p) { return SecondCoeff * 4.0 * M_PI * (p->Rmax - p->Rmin); }
 
 /* analytic_full_partition_function_by_V (src/hawaii.c:5071-5090) */
 double hho_analytic_pf(const hho_system *sys, double T) {

@@ -155,6 +155,11 @@ int hho_m0(const hho_system *sys, const hho_params *p, const double *T, int nT,
            uint64_t n_samples, uint64_t seed, uint64_t offset, int nthreads,
            double *wsum, double *wsq);
 double hho_m0_scale(const hho_params *p);  /* ZeroCoeff * 4 pi (Rmax - Rmin) */
+/* ---- second moment on the same samples (momentum average at the sampled K) ---- */
+int hho_m2(const hho_system *sys, const hho_params *p, const double *T, int nT,
+           uint64_t n_samples, uint64_t seed, uint64_t offset, int nthreads,
+           double *wsum, double *wsq);
+double hho_m2_scale(const hho_params *p);  /* SecondCoeff * 4 pi (Rmax - Rmin) */
 double hho_analytic_pf(const hho_system *sys, double T);
 
 #ifdef __cplusplus

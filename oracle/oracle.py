@@ -91,6 +91,9 @@ def lib():
                              C.c_uint64, C.c_uint64, C.c_int, _dp, _dp]
         L.hho_m0_scale.restype = C.c_double
         L.hho_m0_scale.argtypes = [C.POINTER(Params)]
+        L.hho_m2.argtypes = L.hho_m0.argtypes
+        L.hho_m2_scale.restype = C.c_double
+        L.hho_m2_scale.argtypes = [C.POINTER(Params)]
         L.hho_analytic_pf.restype = C.c_double
         L.hho_analytic_pf.argtypes = [C.POINTER(System), C.c_double]
         L.hho_n2ar_energy_cm.argtypes = [_dp, _dp]
@@ -218,6 +221,19 @@ def m0(sysd, params, T, n_samples, seed, offset=0, nthreads=None):
 
 def m0_scale(params):
     return lib().hho_m0_scale(C.byref(params))
+
+
+def m2(sysd, params, T, n_samples, seed, offset=0, nthreads=None):
+    T = np.ascontiguousarray(T, dtype=np.float64)
+    ws = np.zeros(T.size)
+    wq = np.zeros(T.size)
+    lib().hho_m2(C.byref(sysd), C.byref(params), T, T.size, n_samples, seed, offset,
+                 nthreads or os.cpu_count(), ws, wq)
+    return ws, wq
+
+
+def m2_scale(params):
+    return lib().hho_m2_scale(C.byref(params))
 
 
 def qp_to_cart(sysd, qp):

@@ -190,3 +190,33 @@ def test_multi_iteration_matches_consecutive_calls(lib):
     for i in range(3):
         assert rel_to_c0(c_multi[i], singles[i]) < 1e-12
     assert list(nt) == [300.0, 300.0, 300.0]
+
+
+@pytest.mark.parametrize("name", ["hear", "co2ar", "n2ar"])
+def test_m2_matches_oracle(name):
+    """M2 on the device (Cartesian central differences of the FP64 lab dipole) against
+    the oracle's restatement in the reference's coordinates, on the same Philox samples:
+    the two difference schemes agree to their truncation error."""
+    import hawaiihybrid_b200 as hh
+    ms = lib_system(name)
+    p = lib_params(name, 64, 100.0)
+    T = np.array([100.0, 200.0, 300.0])
+    n = 1 << 16
+    m, e = hh.calculate_m2(ms, p, T, n, seed=99)
+    ws, wq = O.m2(oracle_system(name), oracle_params(name, 64, 100.0), T, n, 99)
+    mref = O.m2_scale(oracle_params(name, 64, 100.0)) * ws / n
+    np.testing.assert_allclose(m, mref, rtol=1e-5)
+    assert np.all(e > 0) and np.all(e < 0.2 * m)
+
+
+@pytest.mark.parametrize("name,T,Rmin,published", [
+    ("co2ar", 100.0, 4.0, 4.41296e-01),   # example_configs/CF-F-CO2-Ar.conf.out:238 (VEGAS), +- 0.08 %
+    ("hear", 100.0, 3.0, 1.34536e-02),    # example_configs/CF-F-He-Ar.conf.out:239 (VEGAS), +- 0.02 %
+])
+def test_m2_physics_anchor(name, T, Rmin, published):
+    """M2 from 2^26 device samples against the reference's published VEGAS values:
+    within 0.3 % plus three standard errors."""
+    import hawaiihybrid_b200 as hh
+    ms = lib_system(name)
+    m, e = hh.calculate_m2(ms, lib_params(name, 64, 100.0, Rmin=Rmin), [T], 1 << 26, seed=7)
+    assert abs(m[0] - published) <= 3e-3 * published + 3 * e[0]

@@ -1,4 +1,4 @@
-"""CF->SF against the reference's golden pair and M0 against the reference's
+"""CF->SF against the reference's golden pair and M0, M2 against the reference's
 published physics values."""
 import os
 
@@ -43,4 +43,22 @@ def test_m0_physics_anchor(name, T, Rmin, published, tol):
     ws, wq = O.m0(oracle_system(name), p, [T], n, 12345)
     m = O.m0_scale(p) * ws[0] / n
     err = O.m0_scale(p) * np.sqrt(wq[0] / n - (ws[0] / n) ** 2) / np.sqrt(n)
+    assert abs(m - published) <= tol * published + 3 * err
+
+
+@pytest.mark.parametrize("name,T,Rmin,published,tol", [
+    # example_configs/CF-F-CO2-Ar.conf.out:238 (VEGAS, 72 ranks): 4.41296e-01 +- 0.08 %
+    ("co2ar", 100.0, 4.0, 4.41296e-01, 0.01),
+    # example_configs/CF-F-He-Ar.conf.out:239 (VEGAS): 1.34536e-02 +- 0.02 %
+    ("hear", 100.0, 3.0, 1.34536e-02, 0.01),
+])
+def test_m2_physics_anchor(name, T, Rmin, published, tol):
+    """The second moment on the M0 samples, with the momentum average of |dmu/dt|^2 taken
+    at the sampled kinetic energy and dmu/dq by central differences in the reference's
+    coordinates, against the reference's VEGAS values."""
+    p = oracle_params(name, 64, 100.0, Rmin=Rmin)
+    n = 2_000_000
+    ws, wq = O.m2(oracle_system(name), p, [T], n, 12345)
+    m = O.m2_scale(p) * ws[0] / n
+    err = O.m2_scale(p) * np.sqrt(wq[0] / n - (ws[0] / n) ** 2) / np.sqrt(n)
     assert abs(m - published) <= tol * published + 3 * err
