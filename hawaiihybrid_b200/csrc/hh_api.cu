@@ -354,16 +354,17 @@ int launch_traj(const TrajParams &P, const TrajIO &io, int *grid_out) {
   int grid = std::max(1, per_sm) * g.num_sms;
   long long need = (io.n_items + TRAJ_THREADS - 1) / TRAJ_THREADS;
   if (need < grid) grid = (int)std::max(1LL, need);
-  if constexpr (SYS == SYS_N2AR) {
+  {
     // the last open items (and all items of a launch that small) run one per warp
-    // in the solo kernel, whose lanes share the right-hand side of one trajectory
+    // in the solo kernel, one state component per lane
     auto solo = traj_kernel<SYS, PHYS, STG, COMP, true>;
     if (smem > 48 * 1024) CK(cudaFuncSetAttribute(solo, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
     int per_sm_solo = 0;
     CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_solo, solo, TRAJ_THREADS, smem));
     const int solo_grid = std::max(1, per_sm_solo) * g.num_sms;
     const unsigned cap = (unsigned)solo_grid * (TRAJ_THREADS / 32);
-    CK(g.handoff.ensure((size_t)cap * sizeof(HandoffState<12, PHYS, STG>)));
+    constexpr int NS = SYS == SYS_HEAR ? 6 : SYS == SYS_CH4CO2 ? 19 : 12;
+    CK(g.handoff.ensure((size_t)cap * sizeof(HandoffState<NS, PHYS, STG>)));
     CK(g.hcount.ensure(4));
     CK(cudaMemsetAsync(g.hcount.p, 0, 4 * sizeof(unsigned int), g.st));
     TrajIO io2 = io;
@@ -380,12 +381,7 @@ int launch_traj(const TrajParams &P, const TrajIO &io, int *grid_out) {
     solo<<<solo_grid, TRAJ_THREADS, smem, g.st>>>(P, io2, g.d_tab);
     CK(cudaGetLastError());
     g_launches += 1;
-    if (grid_out) *grid_out = grid;
-    return HH_OK;
   }
-  kern<<<grid, TRAJ_THREADS, smem, g.st>>>(P, io, g.d_tab);
-  CK(cudaGetLastError());
-  g_launches += 1;
   if (grid_out) *grid_out = grid;
   return HH_OK;
 }
@@ -461,7 +457,7 @@ int zimm_fft(const ZimmArgs &za) {
 // Trajectories go through in chunks whose records fit CH4_RECORD_BUDGET.
 template <typename PHYS>
 int run_records_t(const TrajParams &P, const double *d_ic, uint64_t n, uint64_t per_iter,
-                  int precision, const double *d_satw, int n_sat, unsigned long long *cnt_dev, bool zimm) {
+                  int precision, const double *d_satw, int n_sat, unsigned long long *cnt_dev, bool zimm, uint4 *trace = nullptr) {
   const int N = P.N;
   const int stride = 2 * N - 1;
   const size_t rec_b = HH_REC_WORDS * sizeof(PHYS), mu_b = 4 * sizeof(PHYS);
@@ -515,6 +511,7 @@ int run_records_t(const TrajParams &P, const double *d_ic, uint64_t n, uint64_t 
     io.rec_status = g.rec_status.p;
     for (int k = 0; k < 3; ++k) io.inv_I1[k] = 1.0 / g.sx.II1[k];
     io.lj = g.sx.lj;
+    io.item_trace = trace ? trace + 2 * base : nullptr;
     int rc = (precision == HH_PRECISION_MIXED) ? launch_traj<SYS_CH4CO2, float, float, false>(P, io, nullptr)
                                                : launch_traj<SYS_CH4CO2, double, double, false>(P, io, nullptr);
     if (rc) return rc;
@@ -694,8 +691,10 @@ int run_trajectories(const hh_calc_params *p, const double *d_ic, uint64_t n, ui
   const bool zimm = p->use_zimmermann_trick != 0;
   if (g.sys == SYS_CH4CO2) {
     int rc = (precision == HH_PRECISION_MIXED)
-                 ? run_records_t<float>(P, d_ic, n, per_iter, precision, d_satw, n_sat, g.counters.p, zimm)
-                 : run_records_t<double>(P, d_ic, n, per_iter, precision, d_satw, n_sat, g.counters.p, zimm);
+                 ? run_records_t<float>(P, d_ic, n, per_iter, precision, d_satw, n_sat, g.counters.p, zimm,
+                                        io.item_trace)
+                 : run_records_t<double>(P, d_ic, n, per_iter, precision, d_satw, n_sat, g.counters.p, zimm,
+                                         io.item_trace);
     if (rc) return rc;
     unsigned long long nf = 0;
     CK(cudaMemcpyAsync(&nf, g.rec_nfail.p, sizeof nf, cudaMemcpyDeviceToHost, g.st));

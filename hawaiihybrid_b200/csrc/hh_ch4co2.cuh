@@ -100,8 +100,8 @@ __device__ __noinline__ Ch4Co2Grad<T> ch4co2_lj(const Ch4Co2Lj &lj, const T (&M)
   return g;
 }
 
-template <typename PHYS, typename STG, bool COMP> struct Ch4Co2Sys {
-  static constexpr bool SOLO = false;
+template <typename PHYS, typename STG, bool COMP, bool SOLO_ = false> struct Ch4Co2Sys {
+  static constexpr bool SOLO = SOLO_;  // the solo kernel's instance
   static constexpr int N = 19;
   static constexpr int QP = 16;
   // components a sample reads: r, the quaternion and u

@@ -144,8 +144,9 @@ __device__ void load_tables(Co2arTables<T> *s, const Co2arTablesGlobal *g) {
 }
 
 // ---- systems ----
-template <typename PHYS, typename STG, bool COMP> struct HeArSys {
-  static constexpr bool SOLO = false;  // per-lane right-hand side only
+// SOLO_ (every system): the solo kernel's instance, one trajectory per warp
+template <typename PHYS, typename STG, bool COMP, bool SOLO_ = false> struct HeArSys {
+  static constexpr bool SOLO = SOLO_;
   static constexpr int N = 6;
   static constexpr int QP = 6;
   // components the dipole and the R > Rcut test read: r
@@ -209,8 +210,8 @@ __device__ __noinline__ DipSums<T> co2ar_dip_sums(const Co2arTables<T> *tb, T R,
   return {dz, ax};
 }
 
-template <typename PHYS, typename STG, bool COMP> struct Co2ArSys {
-  static constexpr bool SOLO = false;
+template <typename PHYS, typename STG, bool COMP, bool SOLO_ = false> struct Co2ArSys {
+  static constexpr bool SOLO = SOLO_;
   static constexpr int N = 12;
   static constexpr int QP = 10;
   // components the dipole and the R > Rcut test read: r and u
@@ -278,8 +279,8 @@ template <typename PHYS, typename STG, bool COMP> struct Co2ArSys {
 // Dipole: mu = d_z r^ + d_x (u^ - x r^)/|u^ - x r^| with the body-frame (d_x, d_z) at
 // (R, x = r^.u^): the Euler-angle rotation of the reference (examples/correlation_n2_ar.cpp:52-76)
 // maps body z to r^ and body x to the in-plane normal to r^ on the N1 side.
-// SOLO_: the right-hand side of one trajectory held by all 32 lanes of a warp,
-// evaluated cooperatively (n2ar_pes_grad_coop)
+// SOLO_: the solo kernel's instance (one trajectory per warp), whose right-hand side
+// the 32 lanes evaluate cooperatively (n2ar_pes_grad_coop)
 template <typename PHYS, typename STG, bool COMP, bool SOLO_ = false> struct N2ArSys {
   static constexpr bool SOLO = SOLO_;
   static constexpr int N = 12;
@@ -514,6 +515,119 @@ __device__ __forceinline__ void dense_stages(const Sys &sys, STG (&K)[16][Sys::N
   }
 }
 
+// ---- solo kernel: one trajectory per warp, component `lane` of the state per lane ----
+// The stage sums, the 8th-order solution, the error terms and the dense-output
+// coefficients of component i are formed by lane i with the same operations in
+// the same order as the per-lane functions above; the stage points are gathered
+// by shuffles and every lane evaluates the right-hand side on the full point.  The
+// error norm is summed over the components in order.  A trajectory therefore takes
+// the same steps in either kernel.
+template <int N, typename T> __device__ __forceinline__ T pick_component(const T (&v)[N], int c) {
+  T r = v[0];
+#pragma unroll
+  for (int i = 1; i < N; ++i)
+    if (c == i) r = v[i];
+  return r;
+}
+
+// K[S] of this lane's component from the stage point built from K[0..S-1]
+template <class Sys, typename STG, int S>
+__device__ __forceinline__ void cp_stage(const Sys &sys, STG (&K)[16][1], STG ys0, STG hs, int c) {
+  constexpr int N = Sys::N;
+  STG acc = STG(0);
+#pragma unroll
+  for (int j = 0; j < S; ++j)
+    if (hh_dop853_a[S][j] != 0.0) acc += STG(hh_dop853_a[S][j]) * K[j][0];
+  const STG ysc = ys0 + hs * acc;
+  STG ys[N], f[N];
+#pragma unroll
+  for (int i = 0; i < N; ++i) ys[i] = __shfl_sync(0xffffffffu, ysc, i);
+  sys.rhs(ys, f);
+  K[S][0] = pick_component<N>(f, c);
+}
+
+template <class Sys, typename STG>
+__device__ __forceinline__ double step_attempt_cp(const Sys &sys, const TrajParams &P, STG (&K)[16][1],
+                                                  double y, double h, double &y_new) {
+  constexpr int N = Sys::N;
+  const int lane = threadIdx.x & 31;
+  const int c = lane < N ? lane : N - 1;
+  const STG ys0 = STG(y);
+  const STG hs = STG(h);
+  cp_stage<Sys, STG, 1>(sys, K, ys0, hs, c);
+  cp_stage<Sys, STG, 2>(sys, K, ys0, hs, c);
+  cp_stage<Sys, STG, 3>(sys, K, ys0, hs, c);
+  cp_stage<Sys, STG, 4>(sys, K, ys0, hs, c);
+  cp_stage<Sys, STG, 5>(sys, K, ys0, hs, c);
+  cp_stage<Sys, STG, 6>(sys, K, ys0, hs, c);
+  cp_stage<Sys, STG, 7>(sys, K, ys0, hs, c);
+  cp_stage<Sys, STG, 8>(sys, K, ys0, hs, c);
+  cp_stage<Sys, STG, 9>(sys, K, ys0, hs, c);
+  cp_stage<Sys, STG, 10>(sys, K, ys0, hs, c);
+  cp_stage<Sys, STG, 11>(sys, K, ys0, hs, c);
+  {
+    STG acc = STG(0);
+#pragma unroll
+    for (int j = 0; j < 12; ++j)
+      if (hh_dop853_a[12][j] != 0.0) acc += STG(hh_dop853_a[12][j]) * K[j][0];
+    y_new = y + h * double(acc);
+    double yn[N];
+    STG f[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) yn[i] = __shfl_sync(0xffffffffu, y_new, i);
+    sys.rhs(yn, f);
+    K[12][0] = pick_component<N>(f, c);
+  }
+  STG sc = STG(P.atol) + STG(fmax(fabs(y), fabs(y_new))) * STG(P.rtol);
+  STG a5 = STG(0), a3 = STG(0), m5 = STG(0);
+#pragma unroll
+  for (int j = 0; j < 13; ++j) {
+    if (hh_dop853_e5[j] != 0.0) {
+      a5 += STG(hh_dop853_e5[j]) * K[j][0];
+      if (sizeof(STG) == 4) m5 += fabs(STG(hh_dop853_e5[j]) * K[j][0]);
+    }
+    if (hh_dop853_e3[j] != 0.0) a3 += STG(hh_dop853_e3[j]) * K[j][0];
+  }
+  if (sizeof(STG) == 4) sc += STG(fabs(h)) * STG(P.noise_floor) * m5;
+  const STG isc = STG(1) / sc;
+  const STG q5 = a5 * isc, q3 = a3 * isc;
+  STG e5 = STG(0), e3 = STG(0);
+#pragma unroll
+  for (int i = 0; i < N; ++i) {
+    const STG v5 = __shfl_sync(0xffffffffu, q5, i), v3 = __shfl_sync(0xffffffffu, q3, i);
+    e5 += v5 * v5;
+    e3 += v3 * v3;
+  }
+  if (e5 == STG(0) && e3 == STG(0)) return 0.0;
+  return fabs(h) * double(e5) / sqrt(double(e5 + STG(0.01) * e3) * N);
+}
+
+// stages 13..15 and this lane's dense-output coefficients F[0..6]
+template <class Sys, typename STG>
+__device__ __forceinline__ void dense_stages_cp(const Sys &sys, STG (&K)[16][1], double y_old, double y_new,
+                                                double h, STG (&F)[7]) {
+  constexpr int N = Sys::N;
+  const int lane = threadIdx.x & 31;
+  const int c = lane < N ? lane : N - 1;
+  const STG ys0 = STG(y_old);
+  const STG hs = STG(h);
+  cp_stage<Sys, STG, 13>(sys, K, ys0, hs, c);
+  cp_stage<Sys, STG, 14>(sys, K, ys0, hs, c);
+  cp_stage<Sys, STG, 15>(sys, K, ys0, hs, c);
+  double dy = y_new - y_old;
+  F[0] = STG(dy);
+  F[1] = STG(h * double(K[0][0]) - dy);
+  F[2] = STG(2.0 * dy - h * (double(K[12][0]) + double(K[0][0])));
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    STG acc = STG(0);
+#pragma unroll
+    for (int j = 0; j < 16; ++j)
+      if (hh_dop853_d[r][j] != 0.0) acc += STG(hh_dop853_d[r][j]) * K[j][0];
+    F[3 + r] = STG(h * double(acc));
+  }
+}
+
 // dense output y(t_old + x h) = y_old + x(F0 + (1-x)(F1 + x(F2 + ... ))); the
 // increment is formed in STG precision and added to the FP64 state
 template <class Sys, typename STG>
@@ -639,8 +753,11 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
   const double dt = P.dt;
   unsigned nsteps = 0, nrej = 0, nrhs = 0, nsamp = 0, ndense = 0, nitems = 0;
   // per-lane item state
-  STG K[16][N];
-  double y[N], y_new[N];
+  // bulk: the whole state per lane; solo: component `lane` (clamped to N - 1) per lane
+  constexpr int NL = Sys::SOLO ? 1 : N;
+  const int comp = lane < N ? lane : N - 1;
+  STG K[16][NL];
+  double y[NL], y_new[NL];
   double t = 0.0, h = 0.0;
   PHYS mu0[3] = {PHYS(0), PHYS(0), PHYS(0)};
   PHYS prev = PHYS(0), curr = PHYS(0);
@@ -672,10 +789,15 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
     STG f_t[N];
     PHYS mu_t[3];
     item_setup<Sys, PHYS, STG>(sys, P, io.ic + (size_t)traj * Sys::QP, item & 1, y_t, f_t, mu_t, &h);
+    if constexpr (Sys::SOLO) {
+      y[0] = pick_component<N>(y_t, comp);
+      K[0][0] = pick_component<N>(f_t, comp);
+    } else {
 #pragma unroll
-    for (int i = 0; i < N; ++i) {
-      y[i] = y_t[i];
-      K[0][i] = f_t[i];
+      for (int i = 0; i < N; ++i) {
+        y[i] = y_t[i];
+        K[0][i] = f_t[i];
+      }
     }
 #pragma unroll
     for (int c = 0; c < 3; ++c) mu0[c] = mu_t[c];
@@ -763,11 +885,8 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
         idx = __shfl_sync(FULL, idx, 0);
         if (idx < *io.n_handoff) {
           const Handoff *hs = static_cast<const Handoff *>(io.handoff) + idx;
-#pragma unroll
-          for (int i = 0; i < N; ++i) {
-            y[i] = hs->y[i];
-            K[0][i] = hs->f0[i];
-          }
+          y[0] = hs->y[comp];
+          K[0][0] = hs->f0[comp];
           t = hs->t;
           h = hs->h;
 #pragma unroll
@@ -808,7 +927,11 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
       if (!(h >= min_step)) {
         status = HH_ST_H_UNDERFLOW;
       } else {
-        const double err = step_attempt<Sys, STG>(sys, P, K, y, h, y_new);
+        double err;
+        if constexpr (Sys::SOLO)
+          err = step_attempt_cp<Sys, STG>(sys, P, K, y[0], h, y_new[0]);
+        else
+          err = step_attempt<Sys, STG>(sys, P, K, y, h, y_new);
         nrhs += 12;
         if (err < 1.0) {
           double fac = (err == 0.0) ? 10.0 : fmin(10.0, 0.9 * inv_eighth_root(err));
@@ -838,7 +961,20 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
       int cnt = 0;
       if (pending) {
         STG F[7][Sys::NQ];
-        dense_stages<Sys, STG>(sys, K, y, y_new, h_taken, F);
+        if constexpr (Sys::SOLO) {
+          // this lane's component; published below by the lane that holds it
+          STG Fc[7];
+          dense_stages_cp<Sys, STG>(sys, K, y[0], y_new[0], h_taken, Fc);
+#pragma unroll
+          for (int cq = 0; cq < Sys::NQ; ++cq)
+            if (Sys::qidx(cq) == lane) {
+#pragma unroll
+              for (int r = 0; r < 7; ++r) ws->F[r][cq][0] = Fc[r];
+              ws->qold[cq][0] = y[0];
+            }
+        } else {
+          dense_stages<Sys, STG>(sys, K, y, y_new, h_taken, F);
+        }
         nrhs += 3;
         ++ndense;
         const double t_new = t + h_taken;
@@ -847,12 +983,14 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
         while (kl > k && double(kl) * dt > t_new) --kl;
         cnt = owner ? kl - k + 1 : 0;  // solo mode: the owner's samples, evaluated by all lanes
         if (owner) {
+          if constexpr (!Sys::SOLO) {
 #pragma unroll
-          for (int r = 0; r < 7; ++r)
+            for (int r = 0; r < 7; ++r)
 #pragma unroll
-            for (int c = 0; c < Sys::NQ; ++c) ws->F[r][c][lane] = F[r][c];
+              for (int c = 0; c < Sys::NQ; ++c) ws->F[r][c][lane] = F[r][c];
 #pragma unroll
-          for (int c = 0; c < Sys::NQ; ++c) ws->qold[c][lane] = y[Sys::qidx(c)];
+            for (int c = 0; c < Sys::NQ; ++c) ws->qold[c][lane] = y[Sys::qidx(c)];
+          }
 #pragma unroll
           for (int c = 0; c < 3; ++c) ws->mu0[c][lane] = mu0[c];
           ws->t0[lane] = t;
@@ -1029,7 +1167,7 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
     if (active && status < 0 && accepted) {
       t += h_taken;
 #pragma unroll
-      for (int i = 0; i < N; ++i) {
+      for (int i = 0; i < NL; ++i) {
         y[i] = y_new[i];
         K[0][i] = K[12][i];  // FSAL
       }
@@ -1046,6 +1184,11 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
       if (owner) {
         io.rec_len[item] = k - 1;
         io.rec_status[item] = status;
+        if (io.item_trace) {
+          const unsigned long long t_end = globaltimer_ns();
+          io.item_trace[item] = make_uint4(nsteps - s0, nsamp - m0, (unsigned)(t_begin & 0xffffffffu),
+                                           (unsigned)(t_end & 0xffffffffu));
+        }
       }
       ++nitems;
       item = -1;
@@ -1121,20 +1264,19 @@ template <int SYS, typename PHYS, typename STG> constexpr size_t traj_smem_bytes
          traj_warps<PHYS>() * sizeof(WarpSamples<STG, PHYS, (SYS == SYS_HEAR ? 3 : SYS == SYS_CH4CO2 ? 10 : 6)>);
 }
 
-// SOLO: one item per warp (the solo kernel of the hand-off; N2-Ar only)
+// SOLO: one item per warp (the solo kernel of the hand-off)
 template <int SYS, typename PHYS, typename STG, bool COMP, bool SOLO = false>
 __global__ void __launch_bounds__(traj_threads<PHYS>(), TRAJ_MIN_BLOCKS)
     traj_kernel(TrajParams P, TrajIO io, const Co2arTablesGlobal *gtab) {
-  static_assert(!SOLO || SYS == SYS_N2AR, "cooperative right-hand side: N2-Ar only");
   extern __shared__ __align__(16) unsigned char smem_raw[];
   if (SYS == SYS_HEAR) {
-    using Sys = HeArSys<PHYS, STG, COMP>;
+    using Sys = HeArSys<PHYS, STG, COMP, SOLO>;
     Sys sys;
     sys.inv_mu = 1.0 / P.mu;
     auto *ws = reinterpret_cast<WarpSamples<STG, PHYS, Sys::NQ> *>(smem_raw);
     traj_body<Sys, PHYS, STG>(sys, P, io, ws);
   } else if (SYS == SYS_CH4CO2) {
-    using Sys = Ch4Co2Sys<PHYS, STG, COMP>;
+    using Sys = Ch4Co2Sys<PHYS, STG, COMP, SOLO>;
     Sys sys;
     sys.inv_mu = 1.0 / P.mu;
     sys.inv_II = 1.0 / P.II;
@@ -1160,7 +1302,7 @@ __global__ void __launch_bounds__(traj_threads<PHYS>(), TRAJ_MIN_BLOCKS)
                                                                    sizeof(N2arPesNet<PHYS>));
     traj_body<Sys, PHYS, STG>(sys, P, io, ws);
   } else {
-    using Sys = Co2ArSys<PHYS, STG, COMP>;
+    using Sys = Co2ArSys<PHYS, STG, COMP, SOLO>;
     Co2arTables<PHYS> *tb = reinterpret_cast<Co2arTables<PHYS> *>(smem_raw);
     load_tables<PHYS>(tb, gtab);
     __syncthreads();

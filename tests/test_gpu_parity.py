@@ -220,3 +220,38 @@ def test_m2_physics_anchor(name, T, Rmin, published):
     ms = lib_system(name)
     m, e = hh.calculate_m2(ms, lib_params(name, 64, 100.0, Rmin=Rmin), [T], 1 << 26, seed=7)
     assert abs(m[0] - published) <= 3e-3 * published + 3 * e[0]
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+@pytest.mark.parametrize("name,T,N,dt", [("hear", 300.0, 1024, 200.0), ("co2ar", 300.0, 1024, 100.0),
+                                         ("ch4co2", 300.0, 64, 200.0)])
+def test_solo_kernel_follows_the_bulk_path(name, T, N, dt, precision):
+    """The solo kernel (one trajectory per warp, one state component per lane) takes over
+    the last open items of a launch and runs launches with no more items than its warp
+    slots.  Its stage sums, error norm and dense output keep the per-lane operations and
+    their order, so every half-trajectory takes the same steps in either kernel: a
+    2500-trajectory launch (bulk, then hand-off) against the same trajectories in five
+    launches of 500 (solo only), per item, and the sum of their C(t) against its C(t)."""
+    import hawaiihybrid_b200 as hh
+    ms = lib_system(name)
+    L = _lib_handle()
+    p = lib_params(name, N, dt, mixed_tol=3e-8)
+    qp, _ = O.sample(31, oracle_system(name), oracle_params(name, N, dt), T, 2500)
+
+    def traced(q):
+        tr = np.zeros(4 * 2 * len(q), dtype=np.uint32)
+        assert L.hh_cuda_debug_item_trace(tr.ctypes.data, tr.size) == 0
+        crln, _ = hh.correlation_from_initial_conditions(ms, p, q, precision)
+        return tr.reshape(-1, 4), crln
+
+    tr_all, c_all = traced(qp)
+    parts = [traced(qp[c:c + 500]) for c in range(0, 2500, 500)]
+    steps = np.concatenate([t[:, 0] for t, _ in parts])
+    assert steps.min() > 0
+    np.testing.assert_array_equal(tr_all[:, 0], steps)
+    np.testing.assert_allclose(sum(c for _, c in parts), c_all, rtol=0, atol=1e-11 * abs(c_all[0]))
+
+
+def _lib_handle():
+    from hawaiihybrid_b200 import _lib
+    return _lib.load()
