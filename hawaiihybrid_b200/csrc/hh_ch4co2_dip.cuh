@@ -144,7 +144,7 @@ struct Ch4DipArgs {
 // samples; fewer leave room for more resident warps (the per-lane Y2 arrays take
 // 91 x 32 x S values per warp).
 #ifndef HH_CH4_DIP_S_FP32
-#define HH_CH4_DIP_S_FP32 4
+#define HH_CH4_DIP_S_FP32 2
 #endif
 #ifndef HH_CH4_DIP_S_FP64
 #define HH_CH4_DIP_S_FP64 1
