@@ -760,7 +760,7 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
   double y[NL], y_new[NL];
   double t = 0.0, h = 0.0;
   PHYS mu0[3] = {PHYS(0), PHYS(0), PHYS(0)};
-  PHYS prev = PHYS(0), curr = PHYS(0);
+  PHYS curr = PHYS(0);  // the item's last stored sample
   double *crln = io.crln;
   const double *satw = nullptr;  // this trajectory's satellite weights
   int item = -1;           // -1: needs an item, -2: queue exhausted
@@ -822,7 +822,7 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
     since = total = 0;
     rejected = false;
     exited = false;
-    prev = curr = PHYS(0);
+    curr = PHYS(0);
   };
   auto item_of = [&](unsigned idx) {
     return io.items ? io.items[idx] : (io.fwd_only ? 2 * (int)idx : (int)idx);
@@ -891,7 +891,7 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
           h = hs->h;
 #pragma unroll
           for (int c = 0; c < 3; ++c) mu0[c] = hs->mu0[c];
-          prev = curr = hs->curr;
+          curr = hs->curr;
           item = hs->item;
           k = hs->k;
           since = hs->since;
