@@ -146,6 +146,11 @@ def bench_ch4co2(args, hh, H):
            "fp64_rtol": w["fp64_tol"], "kernel_launches": sm["n_kernel_launches"],
            "stats_mixed": {k: sm[k] for k in ("n_candidates", "n_steps", "n_rhs", "n_samples", "n_failed",
                                               "sample_ms", "traj_ms")}}
+    from hawaiihybrid_b200 import _lib
+    s64, s32 = C.c_int(0), C.c_int(0)
+    _lib.check(_lib.load().hh_cuda_debug_tuning(C.byref(s64), C.byref(s32)))
+    out["dipole_records_per_lane"] = {"fp64": s64.value, "mixed": s32.value,
+                                      "how": "timed per precision on the first call's records (the warm-up)"}
     if not args.no_accuracy:
         per_T = []
         for i in range(len(w["Ts"])):

@@ -44,7 +44,7 @@ EXPORTS = (
     "hh_cuda_correlation_ic", "hh_cuda_m0", "hh_cuda_idct_cf_to_sf", "hh_cuda_strerror",
     "hh_cuda_mt_stream", "hh_cuda_debug_inject", "hh_cuda_debug_item_trace", "hh_cuda_fma_peak",
     "hh_cuda_shutdown", "hh_cuda_m0_noalloc", "hh_cuda_correlation_array", "hh_cuda_correlation_temperatures",
-    "hh_cuda_prmu", "hh_cuda_debug_n2ar_dipole", "hh_cuda_m2",
+    "hh_cuda_prmu", "hh_cuda_debug_n2ar_dipole", "hh_cuda_m2", "hh_cuda_debug_tuning",
 )
 
 
@@ -131,6 +131,7 @@ def load(path: str | None = None):
     L.hh_cuda_debug_item_trace.argtypes = [C.c_void_p, C.c_uint64]
     L.hh_cuda_fma_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
     L.hh_cuda_debug_n2ar_dipole.argtypes = [C.c_int, _dp, _dp, C.c_uint64, _dp]
+    L.hh_cuda_debug_tuning.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.hh_cuda_shutdown.restype = None
     for name in EXPORTS:
         if name not in ("hh_cuda_strerror", "hh_cuda_shutdown"):

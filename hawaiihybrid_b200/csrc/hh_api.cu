@@ -4,9 +4,11 @@
 #include <cuda_runtime.h>
 #include <stdint.h>
 #include <stdio.h>
+#include <stdlib.h>
 #include <string.h>
 
 #include <algorithm>
+#include <climits>
 #include <vector>
 
 #include "../../include/hh_cuda.h"
@@ -98,6 +100,7 @@ struct Ctx {
   unsigned int *d_ch4_y2 = nullptr;
   unsigned int *d_ch4_meta = nullptr;
   int ch4_B = 0;
+  int ch4_dip_s[2] = {0, 0};  // records per lane of the dipole kernel [FP64, mixed]; 0: not tuned yet
   // MT19937 stream
   uint32_t *d_mt = nullptr;
   unsigned short *d_mt_jump_seg = nullptr, *d_mt_jump_coarse = nullptr;  // jump-ahead tables
@@ -451,6 +454,38 @@ int zimm_fft(const ZimmArgs &za) {
   return HH_OK;
 }
 
+// one launchable variant of the CH4-CO2 dipole kernel (S records per lane)
+struct Ch4DipVariant {
+  void (*kern)(Ch4DipArgs);
+  int S;
+  size_t smem;
+  int grid;
+};
+
+template <typename PHYS, int S> int ch4_dip_variant(Ch4DipVariant *v) {
+  v->kern = ch4_dipole_kernel<PHYS, S>;
+  v->S = S;
+  v->smem = ch4_dip_smem<PHYS, S>();
+  if (v->smem > 48 * 1024)
+    CK(cudaFuncSetAttribute(v->kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v->smem));
+  int per = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per, v->kern, 32 * CH4_DIP_WARPS, v->smem));
+  v->grid = std::max(1, per) * g.num_sms;
+  return HH_OK;
+}
+
+// the dipole kernel's candidates per precision: S = 1, 2, 4 (FP32), 1, 2 (FP64)
+template <typename PHYS> int ch4_dip_candidates(Ch4DipVariant *v, int *n) {
+  int rc = ch4_dip_variant<PHYS, 1>(&v[0]);
+  if (!rc) rc = ch4_dip_variant<PHYS, 2>(&v[1]);
+  *n = 2;
+  if constexpr (sizeof(PHYS) == 4) {
+    if (!rc) rc = ch4_dip_variant<PHYS, 4>(&v[2]);
+    *n = 3;
+  }
+  return rc;
+}
+
 // CH4-CO2: the trajectory kernel writes every sample as a record, then the
 // records are sorted by radial piece, their dipoles evaluated in batches and
 // C(t) accumulated with the reference's per-sample tests (hh_ch4co2_dip.cuh).
@@ -468,8 +503,7 @@ int run_records_t(const TrajParams &P, const double *d_ic, uint64_t n, uint64_t 
   const size_t slots = (size_t)chunk * stride;
   CK(g.rec.ensure(slots * rec_b));
   CK(g.rec_mu.ensure(slots * mu_b));
-  const int task = 32 * ch4_dip_s<PHYS>();
-  CK(g.rec_sorted.ensure(slots + (size_t)task * CH4_NSEG));
+  CK(g.rec_sorted.ensure(slots + (size_t)32 * CH4_DIP_SMAX * CH4_NSEG));
   CK(g.rec_len.ensure(2 * chunk));
   CK(g.rec_status.ensure(2 * chunk));
   CK(g.seg_cnt.ensure(2 * CH4_NSEG));
@@ -485,17 +519,24 @@ int run_records_t(const TrajParams &P, const double *d_ic, uint64_t n, uint64_t 
   fold.meta = g.d_ch4_meta;
   for (int i = 0; i < CH4_NSEG - 1; ++i) fold.seg_hi[i] = hh_ch4co2_seg_hi[i];
   for (int i = 0; i < CH4_NSEG; ++i) fold.centre[i] = hh_ch4co2_centre[i];
-  auto dip = ch4_dipole_kernel<PHYS>;
-  const size_t dsmem = ch4_dip_smem<PHYS>();
-  if (dsmem > 48 * 1024) CK(cudaFuncSetAttribute(dip, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)dsmem));
-  int dper = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&dper, dip, 32 * CH4_DIP_WARPS, dsmem));
-  const int dgrid = std::max(1, dper) * g.num_sms;
+  // dipole kernel variants; the records per lane are picked per precision by timing
+  // every candidate on the first chunk of records (a dipole depends only on its
+  // record, so every variant writes the same values)
+  Ch4DipVariant cand[3];
+  int ncand = 0;
+  int rc0 = ch4_dip_candidates<PHYS>(cand, &ncand);
+  if (rc0) return rc0;
+  int &tuned_s = g.ch4_dip_s[sizeof(PHYS) == 4 ? 1 : 0];
+  if (tuned_s == 0) {
+    // HH_CH4_DIP_S fixes the records per lane (when it names a candidate) instead of timing
+    const char *env = getenv("HH_CH4_DIP_S");
+    const int want = env ? atoi(env) : 0;
+    for (int c = 0; c < ncand; ++c)
+      if (cand[c].S == want) tuned_s = want;
+  }
   for (uint64_t base = 0; base < n; base += chunk) {
     const uint64_t nc = std::min<uint64_t>(chunk, n - base);
     CK(cudaMemsetAsync(g.queue.p, 0, sizeof(unsigned int), g.st));
-    CK(cudaMemsetAsync(g.seg_cnt.p, 0, 2 * CH4_NSEG * sizeof(unsigned int), g.st));
-    CK(cudaMemsetAsync(g.rec_sorted.p, 0xff, (nc * stride + (size_t)task * CH4_NSEG) * sizeof(int), g.st));
     TrajIO io;
     memset(&io, 0, sizeof io);
     io.ic = d_ic + base * g.QP;
@@ -525,22 +566,67 @@ int run_records_t(const TrajParams &P, const double *d_ic, uint64_t n, uint64_t 
     sa.cursor = g.seg_cnt.p + CH4_NSEG;
     sa.warp0 = g.seg_w0.p;
     sa.sorted = g.rec_sorted.p;
-    sa.task = task;
     for (int i = 0; i < CH4_NSEG - 1; ++i) sa.seg_hi[i] = hh_ch4co2_seg_hi[i];
     const long long nslots = (long long)nc * stride;
     const int sgrid = (int)std::min<long long>((nslots + 255) / 256, 8LL * g.num_sms);
-    ch4_seg_count_kernel<PHYS><<<sgrid, 256, 0, g.st>>>(sa);
-    ch4_seg_scan_kernel<<<1, 32, 0, g.st>>>(sa);
-    ch4_seg_scatter_kernel<PHYS><<<sgrid, 256, 0, g.st>>>(sa);
-    CK(cudaGetLastError());
     Ch4DipArgs da;
     da.f = fold;
     da.records = g.rec.p;
     da.sorted = g.rec_sorted.p;
     da.warp0 = g.seg_w0.p;
     da.mu = g.rec_mu.p;
-    dip<<<dgrid, 32 * CH4_DIP_WARPS, dsmem, g.st>>>(da);
-    CK(cudaGetLastError());
+    // sort the records into warp tasks of 32 S for variant v
+    auto sort_for = [&](const Ch4DipVariant &v) -> int {
+      sa.task = 32 * v.S;
+      CK(cudaMemsetAsync(g.seg_cnt.p, 0, 2 * CH4_NSEG * sizeof(unsigned int), g.st));
+      CK(cudaMemsetAsync(g.rec_sorted.p, 0xff, (nc * stride + (size_t)sa.task * CH4_NSEG) * sizeof(int), g.st));
+      ch4_seg_count_kernel<PHYS><<<sgrid, 256, 0, g.st>>>(sa);
+      ch4_seg_scan_kernel<<<1, 32, 0, g.st>>>(sa);
+      ch4_seg_scatter_kernel<PHYS><<<sgrid, 256, 0, g.st>>>(sa);
+      CK(cudaGetLastError());
+      return HH_OK;
+    };
+    // the dipoles of the first max_tasks warp tasks with variant v
+    auto dipole_with = [&](const Ch4DipVariant &v, long long max_tasks, long long step) -> int {
+      da.max_tasks = max_tasks;
+      da.task_step = step;
+      v.kern<<<v.grid, 32 * CH4_DIP_WARPS, v.smem, g.st>>>(da);
+      CK(cudaGetLastError());
+      return HH_OK;
+    };
+    if (tuned_s == 0) {
+      cudaEvent_t e0, e1;
+      CK(cudaEventCreate(&e0));
+      CK(cudaEventCreate(&e1));
+      float best = 0.0f;
+      for (int c = 0; c < ncand; ++c) {
+        int rcs = sort_for(cand[c]);
+        if (rcs) return rcs;
+        // timing run: about 2^20 records for every variant, in tasks spread over all
+        // radial pieces
+        const long long step = std::max<long long>(1, nslots >> 20);
+        CK(cudaEventRecord(e0, g.st));
+        rcs = dipole_with(cand[c], (1LL << 20) / (32 * cand[c].S), step);
+        if (rcs) return rcs;
+        CK(cudaEventRecord(e1, g.st));
+        CK(cudaEventSynchronize(e1));
+        float ms = 0.0f;
+        CK(cudaEventElapsedTime(&ms, e0, e1));
+        if (tuned_s == 0 || ms < best) {
+          best = ms;
+          tuned_s = cand[c].S;
+        }
+      }
+      cudaEventDestroy(e0);
+      cudaEventDestroy(e1);
+      g_launches += 4 * (unsigned long long)ncand;
+    }
+    const Ch4DipVariant *use = &cand[0];
+    for (int c = 0; c < ncand; ++c)
+      if (cand[c].S == tuned_s) use = &cand[c];
+    int rcd = sort_for(*use);
+    if (!rcd) rcd = dipole_with(*use, LLONG_MAX, 1);
+    if (rcd) return rcd;
     Ch4CorrArgs ca;
     ca.mu = g.rec_mu.p;
     ca.rec_len = g.rec_len.p;
@@ -1540,6 +1626,13 @@ int hh_cuda_debug_n2ar_dipole(int precision, const double *R, const double *T, u
   if (dT) cudaFree(dT);
   if (dO) cudaFree(dO);
   return rc;
+}
+
+int hh_cuda_debug_tuning(int *ch4_dip_s_fp64, int *ch4_dip_s_mixed) {
+  if (!g.init) return HH_E_NOT_INITIALIZED;
+  if (ch4_dip_s_fp64) *ch4_dip_s_fp64 = g.ch4_dip_s[0];
+  if (ch4_dip_s_mixed) *ch4_dip_s_mixed = g.ch4_dip_s[1];
+  return HH_OK;
 }
 
 int hh_cuda_debug_item_trace(uint32_t *out, uint64_t capacity_words) {

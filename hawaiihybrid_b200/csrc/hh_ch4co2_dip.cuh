@@ -137,23 +137,20 @@ struct Ch4DipArgs {
   const int *sorted;
   const long long *warp0;
   void *mu;                   // [record][4] lab-frame dipole in the surface precision
+  // tasks evaluated: 0, task_step, 2 task_step, ... below the total, at most max_tasks
+  // of them (1 and all for a real run; a timing run takes a spread-out subset)
+  long long max_tasks;
+  long long task_step;
 };
 
-// records per lane of the dipole kernel (S values of a Y2 index are one shared-
-// memory vector).  More records per lane share each coefficient load among more
-// samples; fewer leave room for more resident warps (the per-lane Y2 arrays take
-// 91 x 32 x S values per warp).
-#ifndef HH_CH4_DIP_S_FP32
-#define HH_CH4_DIP_S_FP32 2
-#endif
-#ifndef HH_CH4_DIP_S_FP64
-#define HH_CH4_DIP_S_FP64 1
-#endif
-template <typename PHYS> __host__ __device__ constexpr int ch4_dip_s() {
-  return sizeof(PHYS) == 4 ? HH_CH4_DIP_S_FP32 : HH_CH4_DIP_S_FP64;
-}
-template <typename PHYS> __host__ __device__ constexpr size_t ch4_dip_smem() {
-  return (size_t)CH4_DIP_WARPS * CH4_NY2 * 32 * ch4_dip_s<PHYS>() * sizeof(PHYS);
+// S: records per lane of the dipole kernel (the S values of a Y2 index are one
+// shared-memory vector).  More records per lane share each coefficient load among
+// more samples; fewer leave room for more resident warps (the per-lane Y2 arrays
+// take 91 x 32 x S values per warp).  The host picks S per precision by timing the
+// candidates on the first chunk of records (hh_api.cu, ch4_tune_dipole).
+constexpr int CH4_DIP_SMAX = 4;
+template <typename PHYS, int S> __host__ __device__ constexpr size_t ch4_dip_smem() {
+  return (size_t)CH4_DIP_WARPS * CH4_NY2 * 32 * S * sizeof(PHYS);
 }
 
 template <typename PHYS, int S> struct Vec;
@@ -203,9 +200,8 @@ __device__ __forceinline__ void ch4_y2(T x, T y, T z, T *Y, int lane, int s_) {
   }
 }
 
-template <typename PHYS>
+template <typename PHYS, int S>
 __global__ void __launch_bounds__(32 * CH4_DIP_WARPS) ch4_dipole_kernel(Ch4DipArgs a) {
-  constexpr int S = ch4_dip_s<PHYS>();
   using V = typename Vec<PHYS, S>::T;
   extern __shared__ __align__(16) unsigned char smem_raw[];
   __shared__ long long w0[CH4_NSEG + 1];
@@ -214,9 +210,10 @@ __global__ void __launch_bounds__(32 * CH4_DIP_WARPS) ch4_dipole_kernel(Ch4DipAr
   const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
   PHYS *Y2 = reinterpret_cast<PHYS *>(smem_raw) + (size_t)warp * CH4_NY2 * 32 * S;
   const V *Y2v = reinterpret_cast<const V *>(Y2) + lane;
-  const long long total = w0[CH4_NSEG];
+  const long long total = min((w0[CH4_NSEG] + a.task_step - 1) / a.task_step, a.max_tasks);
   const long long nw = (long long)gridDim.x * CH4_DIP_WARPS;
-  for (long long w = (long long)blockIdx.x * CH4_DIP_WARPS + warp; w < total; w += nw) {
+  for (long long wi = (long long)blockIdx.x * CH4_DIP_WARPS + warp; wi < total; wi += nw) {
+    const long long w = wi * a.task_step;
     int seg = 0;
     while (seg < CH4_NSEG - 1 && w0[seg + 1] <= w) ++seg;
     // record s of this lane: task slot s * 32 + lane; padding slots evaluate the

@@ -249,6 +249,10 @@ int hh_cuda_debug_item_trace(uint32_t *out, uint64_t capacity_words);
  * intermolecular axis and the N2 axis) as the given precision path evaluates it,
  * into out[2 n]: the FP64 network, or the mixed path's FP32 table. */
 int hh_cuda_debug_n2ar_dipole(int precision, const double *R, const double *T, uint64_t n, double *out);
+/* Diagnostic (no counterpart in the reference): the records per lane that the
+ * CH4-CO2 dipole kernel's tuner picked for the FP64 and the mixed path on the first
+ * record-path call of this context (0 before that call). */
+int hh_cuda_debug_tuning(int *ch4_dip_s_fp64, int *ch4_dip_s_mixed);
 
 /* Diagnostic (no counterpart in the reference): measured FMA throughput of the
  * CUDA cores in TFLOP/s (precision HH_PRECISION_FP64 or, for FP32,

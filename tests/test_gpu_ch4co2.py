@@ -154,3 +154,22 @@ def test_m0_is_rejected():
     ms = lib_system("ch4co2")
     with pytest.raises(hh.HHError):
         hh.calculate_m0(ms, lib_params("ch4co2", N, DT), [300.0], 1 << 12)
+
+
+def test_dipole_tuner_picks_a_candidate():
+    """The first record-path call of a context times the dipole kernel's variants (1, 2, 4
+    records per lane for FP32; 1, 2 for FP64) and keeps the fastest; the C(t) of the
+    tuning call and of a later call on the same trajectories agree."""
+    import ctypes as C
+    import hawaiihybrid_b200 as hh
+    from hawaiihybrid_b200 import _lib
+    ms = lib_system("ch4co2")
+    L = _lib.load()
+    p = lib_params("ch4co2", 21, 200.0)
+    qp, _ = O.sample(3, oracle_system("ch4co2"), oracle_params("ch4co2", 21, 200.0), 300.0, 256)
+    c1, _ = hh.correlation_from_initial_conditions(ms, p, qp, hh.PRECISION_MIXED)
+    c2, _ = hh.correlation_from_initial_conditions(ms, p, qp, hh.PRECISION_MIXED)
+    s64, s32 = C.c_int(-1), C.c_int(-1)
+    assert L.hh_cuda_debug_tuning(C.byref(s64), C.byref(s32)) == 0
+    assert s32.value in (1, 2, 4)
+    np.testing.assert_allclose(c2, c1, rtol=0, atol=1e-12 * abs(c1[0]))
