@@ -1253,7 +1253,9 @@ __device__ __forceinline__ void load_words(void *dst, const void *src, size_t by
 // workload: both use every register (255), so 8 warps run per SM either way.
 // The FP64 kernels run 10 % faster as one block of 8 warps (one copy of the
 // surface tables per SM); the FP32-stage kernels are 1 % faster as two blocks of
-// 4.  TRAJ_MIN_BLOCKS is the blocks per SM the register allocation must allow.
+// 4.  With the solo hand-off and one pooled-sample job per lane, 4 and 8 warps per
+// block for both paths were within 1 % of each other on the CO2-Ar and N2-Ar
+// workloads.  TRAJ_MIN_BLOCKS is the blocks per SM the register allocation must allow.
 template <typename PHYS> constexpr int traj_warps() { return sizeof(PHYS) == 8 ? 8 : 4; }
 template <typename PHYS> constexpr int traj_threads() { return 32 * traj_warps<PHYS>(); }
 constexpr int TRAJ_MIN_BLOCKS = 1;
