@@ -430,7 +430,9 @@ def main():
                 "warmup": args.warmup, "ms_per_step": mixed_ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "fp32 surfaces + fp64 state", "data": "synthetic (Boltzmann-sampled "
                 "initial conditions, MT19937 seed 7 + 1000*rank)", "config": config(args, ws),
-                "plain_fp64": {"value": plain_value, "unit": "traj/s", "ms_per_step": plain_ms},
+                "plain_fp64": {"value": plain_value, "unit": "traj/s", "ms_per_step": plain_ms,
+                               "steps_per_call": max(1, args.plain_steps),
+                               "mixed_steps_per_call": args.steps},
                 "single_batch": {"mixed_traj_per_s": n * ws / (single_mixed_ms / 1e3),
                                  "mixed_ms": single_mixed_ms,
                                  "note": "one step submitted alone: its long-lived trajectories "
