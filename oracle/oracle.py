@@ -41,9 +41,14 @@ class TrajStats(C.Structure):
     ]
 
 
-def build(ref: str = "/root/reference") -> None:
-    """Build liboracle.so and, when the reference is present, oracle/_ref."""
-    subprocess.run(["make", "-s", "-C", HERE, f"REF={ref}", "all"], check=True)
+def build(ref: str | None = None) -> None:
+    """Build liboracle.so and, when the reference checkout is present, oracle/_ref.
+
+    `ref` (else the environment variable HH_REFERENCE_DIR) overrides the checkout
+    location that oracle/Makefile reads the reference sources from."""
+    ref = ref or os.environ.get("HH_REFERENCE_DIR")
+    cmd = ["make", "-s", "-C", HERE] + ([f"REF={ref}"] if ref else []) + ["all"]
+    subprocess.run(cmd, check=True)
 
 
 _lib = None

@@ -1,7 +1,8 @@
 """Build the golden fixtures used by the test suite from the reference checkout.
 
-Run once where the reference is present:
-    python tests/golden/make_golden.py /root/reference
+Run once where the reference checkout is present:
+    python tests/golden/make_golden.py <reference checkout>
+(or with the checkout in the environment variable HH_REFERENCE_DIR).
 Writes tests/golden/cf_sf_he_ar_1000.npz from the reference's own golden pair
 (tests/CF-F-He-Ar-1000.0.txt -> tests/SF-F-He-Ar-1000.0.txt, produced by the
 reference's CF_TO_SF, tests/convert-cf-to-sf.conf:6-9): the CF time grid and
@@ -32,7 +33,9 @@ def read_table(path):
 
 
 def main():
-    ref = sys.argv[1] if len(sys.argv) > 1 else "/root/reference"
+    ref = sys.argv[1] if len(sys.argv) > 1 else os.environ.get("HH_REFERENCE_DIR")
+    if not ref:
+        sys.exit("usage: make_golden.py <reference checkout> (or set HH_REFERENCE_DIR)")
     hcf, cf = read_table(os.path.join(ref, "tests", "CF-F-He-Ar-1000.0.txt"))
     hsf, sf = read_table(os.path.join(ref, "tests", "SF-F-He-Ar-1000.0.txt"))
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), "cf_sf_he_ar_1000.npz")

@@ -17,7 +17,7 @@ import ctypes as C
 import numpy as np
 import pytest
 
-from tests.helpers import II_CO2, MU_CO2AR, MU_HEAR, lib_params
+from tests.helpers import II_CO2, II_N2, MU_CO2AR, MU_HEAR, MU_N2AR, lib_params
 
 pytestmark = pytest.mark.gpu
 
@@ -29,6 +29,11 @@ def _init(name):
     L = _lib.load()
     if name == "hear":
         d = _lib.SystemDesc(_lib.HH_SYSTEM_HE_AR, MU_HEAR, _lib.HH_MONOMER_ATOM, _lib.HH_MONOMER_ATOM)
+    elif name == "n2ar":
+        # the N2-Ar kernels stage the folded dipole models in dynamic shared memory
+        d = _lib.SystemDesc(_lib.HH_SYSTEM_N2_AR, MU_N2AR, _lib.HH_MONOMER_LINEAR_MOLECULE,
+                            _lib.HH_MONOMER_ATOM)
+        d.II1[0] = d.II1[1] = II_N2
     else:
         d = _lib.SystemDesc(_lib.HH_SYSTEM_CO2_AR, MU_CO2AR, _lib.HH_MONOMER_LINEAR_MOLECULE,
                             _lib.HH_MONOMER_ATOM)
@@ -44,7 +49,8 @@ def _m0(L, entry, cp, T, n, seed, prec):
     return rc, m, e
 
 
-@pytest.mark.parametrize("name,prec", [("hear", 0), ("hear", 1), ("co2ar", 0), ("co2ar", 1)])
+@pytest.mark.parametrize("name,prec", [("hear", 0), ("hear", 1), ("co2ar", 0), ("co2ar", 1),
+                                       ("n2ar", 0), ("n2ar", 1)])
 def test_noalloc_matches_m0(name, prec):
     L, _lib = _init(name)
     cp = lib_params(name, 64, 100.0).to_c()
