@@ -1,18 +1,33 @@
 #!/usr/bin/env python3
 """Benchmark of the HAWAIIHYBRID trajectory hot path on B200.
 
-Workload (one step): a CORRELATION_SINGLE pass over 102,400 CO2-Ar
+Headline workload (one step): a CORRELATION_SINGLE pass over 102,400 CO2-Ar
 trajectories at T = 300 K (Boltzmann-sampled initial conditions from the
 MT19937 stream of seed 7, free+metastable pair state, R in [4, 40] bohr,
 Rcut = 40 bohr), 32,768 dipole samples at dt = 100 a.u. forward and backward,
 reduced into C(t).  The sampled initial conditions are generated on the
-device, so the inputs are resident in HBM when a step starts.
+device, so the inputs are resident in HBM when a step starts.  The K timed
+steps are one call of K iterations (the reference's iteration loop), and every
+arm it is compared with runs the same K iterations per call.
 
-  value   trajectories/s of the batched mixed-precision path (FP32 surfaces
-          and stages, FP64 state and C(t)), whole job
-  plain   the same for the FP64 drop-in path, same initial conditions
-  e2e     the mixed path timed around the public call (hh_cuda_correlation via
-          the Python mirror) with its host buffers
+  value     trajectories/s of the batched mixed-precision path (FP32 surfaces
+            and stages, FP64 state, error control and C(t)), whole job
+  plain     the FP64 drop-in path, same initial conditions, same K per call
+  fp64_at_mixed_rtol
+            the FP64 path at the mixed path's tolerance, same K per call: it
+            separates the gain of FP32 arithmetic from that of the tolerance
+  e2e       the mixed path timed around the public call (hh_cuda_correlation_multi
+            through the Python mirror) with its host buffers
+  parity    the FP64 path against the CPU oracle on the same initial
+            conditions at the workload sizes (first 4096 trajectories of the
+            headline workload at N = 32,768; N2-Ar, CH4-CO2 and He-Ar slices;
+            the sampler over the whole draw of one step; M0 on the same samples)
+
+The other workloads of the reference's benchmark set are reported beside the
+headline, each with its own mixed/FP64 ratio at equal iterations per call and a
+roofline fraction: He-Ar (10,240 x 65,536, FP64 and mixed, plus the spectral
+function), CO2-Ar Monte Carlo M0 (16 temperatures x 1e8 samples), N2-Ar PIP-NN
+(262,144 x 16,384) and CH4-CO2 (4 x 262,144 x 21).
 
 `python bench.py --impl reference` times the CPU restatement of the reference
 path (oracle/, FP64, all host cores) on a bounded sample of the same workload.
@@ -36,16 +51,22 @@ sys.path.insert(0, ROOT)
 WORKLOAD = dict(system="co2ar", n_traj=102400, T=300.0, seed=7, N=32768, dt=100.0, Rmin=4.0, Rmax=40.0,
                 Rcut=40.0, pesmin=-8.913727688689150e-04, mu=3.817083069753919e+04,
                 II=2.819827114123505e+05, fp64_tol=1e-12)
+# He-Ar atom-atom pair (PES-IDS/HeAr.h), the reference's plain FP64 CORRELATION_SINGLE case
+HEAR = dict(n_traj=10240, T=300.0, seed=42, N=65536, dt=200.0, Rmin=4.0, Rmax=40.0, Rcut=40.0,
+            pesmin=-9.424412560638486e-05, mu=6.632039160324215e+03, fp64_tol=1e-12, iters=4)
+# CO2-Ar Monte Carlo zeroth moment: 16 temperatures in one launch
+M0CFG = dict(n_samples=100_000_000, Ts=tuple(np.linspace(150.0, 400.0, 16)), seed=20240607, Rmin=4.0,
+             Rmax=40.0)
 # N2-Ar PIP-NN workload (rigid N2 + Ar, PES-IDS/ai_pes_n2_ar_pip_nn.cpp surfaces)
 N2AR = dict(n_traj=262144, T=200.0, seed=7, N=16384, dt=100.0, Rmin=4.51, Rmax=40.0, Rcut=40.0,
-            pesmin=-97.3 / 2.1947463136320e5, mu=30016.287464295514, II=55141.90310147907, fp64_tol=1e-12)
+            pesmin=-97.3 / 2.1947463136320e5, mu=30016.287464295514, II=55141.90310147907, fp64_tol=1e-12,
+            iters=2)
 # CH4-CO2 rotor + linear molecule (example_configs/CF-F-CH4-CO2.conf: dt 200 a.u., 21 samples,
 # R in [4.751, 40]); four temperature sets in one launch; stand-in PES, reference dipole
 CH4CO2 = dict(n_per_T=262144, Ts=(100.0, 200.0, 300.0, 400.0), seed=2066497031, N=21, dt=200.0, Rmin=4.751,
               Rmax=40.0, Rcut=40.0, pesmin=-1.562522273622102e-03, mu=2.141790360592430e+04,
               II1=2.093840965876434e+04, II2=2.819827114123505e+05, fp64_tol=1e-12)
 METRIC = "traj/s/GPU, batched mixed-precision vs FP64 plain, at C(t) rel err ≤1e-4"
-PEAKS = os.path.join(ROOT, "MEASURED_PEAKS.json")
 PROFILE_TRAFFIC = os.path.join(ROOT, "profiles", "traffic.json")
 
 
@@ -58,81 +79,201 @@ def parse():
     ap.add_argument("--trajectories", type=int, default=WORKLOAD["n_traj"])
     ap.add_argument("--samples", type=int, default=WORKLOAD["N"])
     ap.add_argument("--mixed-tol", type=float, default=3e-8)
-    ap.add_argument("--plain-steps", type=int, default=2)
     ap.add_argument("--no-accuracy", action="store_true")
+    ap.add_argument("--no-parity", action="store_true", help="skip the FP64-vs-oracle checks")
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--cpu-sample", type=int, default=4096)
+    ap.add_argument("--no-fp64", action="store_true", help="skip the FP64 arms of the headline workload")
+    ap.add_argument("--no-hear", action="store_true", help="skip the He-Ar workload")
+    ap.add_argument("--no-m0", action="store_true", help="skip the Monte Carlo M0 workload")
     ap.add_argument("--no-n2ar", action="store_true", help="skip the N2-Ar PIP-NN workload")
     ap.add_argument("--n2ar-trajectories", type=int, default=N2AR["n_traj"])
     ap.add_argument("--no-ch4co2", action="store_true", help="skip the CH4-CO2 four-temperature workload")
     ap.add_argument("--ch4co2-per-T", type=int, default=CH4CO2["n_per_T"])
-    ap.add_argument("--only-n2ar", action="store_true",
-                    help="run only the N2-Ar workload and print its block as the JSON line")
-    ap.add_argument("--only-ch4co2", action="store_true",
-                    help="run only the CH4-CO2 workload and print its block as the JSON line")
+    ap.add_argument("--only", choices=["n2ar", "ch4co2", "hear", "m0"],
+                    help="run only this workload and print its block as the JSON line")
     return ap.parse_args()
 
 
-def bench_n2ar(args, hh, H):
-    """N2-Ar PIP-NN: mixed (FP32 PES and stages, FP64 dipole and state) against the FP64
-    path on the same initial conditions; two mixed iterations per launch."""
+def _params(H, w, tol, mixed_tol, N=None):
+    return H.CalcParams(ps=1, sampler_Rmin=w["Rmin"], sampler_Rmax=w["Rmax"], pesmin=w["pesmin"],
+                        sampling_time=w["dt"], MaxTrajectoryLength=N or w["N"], cvode_tolerance=tol,
+                        Rcut=w["Rcut"], partial_partition_function_ratio=1.0, mixed_tolerance=mixed_tol)
+
+
+def _ct_errors(c_test, c_ref, floor_ref=None):
+    """max_k |C_test - C_ref| / C_ref(0) over the collision window t <= 1e5 a.u. (k < kc is
+    passed by the caller through floor_ref's horizon), the whole window and M0."""
+    c0 = abs(c_ref[0])
+    d = np.abs(np.asarray(c_test) - np.asarray(c_ref)) / c0
+    out = {"m0_rel_err": float(d[0]), "ct_err_all": float(d.max())}
+    if floor_ref is not None:
+        floor = np.abs(np.asarray(floor_ref) - np.asarray(c_ref)) / c0
+        run = np.maximum.accumulate(floor)
+        kh = int(np.argmax(run > 1e-8)) if np.any(run > 1e-8) else len(c_ref)
+        out.update({"fp64_horizon_k": kh, "ct_err_within_fp64_horizon": float(d[:max(kh, 1)].max()),
+                    "fp64_floor_all": float(floor.max())})
+    return out
+
+
+def _roof(work, t_s, p32, p64, kernel, note=None):
+    achieved = (work["fp32"] + work["fp64"]) / t_s / 1e12
+    frac = (work["fp32"] / (p32 * 1e12) + work["fp64"] / (p64 * 1e12)) / t_s
+    out = {"kernel": kernel, "achieved_tflops": achieved, "peak_tflops": achieved / frac if frac > 0 else None,
+           "frac": frac, "work_flops": work, "kernel_ms": 1e3 * t_s}
+    if note:
+        out["note"] = note
+    return out
+
+
+# ----------------------------------------------------------------------------
+# secondary workloads
+# ----------------------------------------------------------------------------
+def bench_hear(args, hh, H, peaks):
+    """He-Ar (config: 10,240 trajectories x 65,536 samples at dt 200 a.u., seed 42, FP64
+    rtol 1e-12): FP64 and mixed at the same iterations per call, the spectral function
+    of the C(t) by hh_cuda_idct_cf_to_sf, and the trajectory kernel's roofline."""
+    from hawaiihybrid_b200 import _lib, flops
+    w = HEAR
+    n, K = w["n_traj"], w["iters"]
+    ms = hh.init_ms(w["mu"], hh.ATOM, hh.ATOM, None, None, w["seed"])
+
+    def run(prec, tol=w["fp64_tol"]):
+        return hh.correlation_iterations(ms, _params(H, w, tol, args.mixed_tol), w["T"], n, K, prec,
+                                         seed=w["seed"])
+    run(hh.PRECISION_MIXED)
+    cm, _, sm = run(hh.PRECISION_MIXED)
+    run(hh.PRECISION_FP64)
+    cp, _, sp = run(hh.PRECISION_FP64)
+    c13, _, _ = hh.correlation_iteration(ms, _params(H, w, 1e-13, args.mixed_tol), w["T"], n,
+                                         hh.PRECISION_FP64, seed=w["seed"])
+    sm, sp = sm.as_dict(), sp.as_dict()
+    mixed = K * n / (sm["total_ms"] / 1e3)
+    plain = K * n / (sp["total_ms"] / 1e3)
+    # spectral function of the iteration-averaged FP64 C(t) (the CF file the reference writes)
+    cf = hh.CFnc(t=w["dt"] * np.arange(w["N"]), data=cp.mean(axis=0) / n, ntraj=float(n), Temperature=w["T"],
+                 normalized=True)
+    t0 = time.perf_counter()
+    sf = hh.idct_cf_to_sf(cf)
+    sf_ms = 1e3 * (time.perf_counter() - t0)
+    out = {"workload": f"He-Ar, {n} trajectories x {w['N']} samples at dt {w['dt']} a.u., T {w['T']} K, seed "
+                       f"{w['seed']}, R in [{w['Rmin']}, {w['Rmax']}]; C(t) -> SF by the FFT",
+           "iterations_per_call": K,
+           "mixed_traj_per_s": mixed, "plain_fp64_traj_per_s": plain, "speedup_same_K": mixed / plain,
+           "mixed_rtol": args.mixed_tol, "fp64_rtol": w["fp64_tol"],
+           "sf_call_ms": sf_ms, "sf_points": int(sf.data.size),
+           "accuracy": _ct_errors(cm[0], cp[0], c13),
+           "roofline": {
+               "mixed": _roof(flops.work("hear", sm, True), sm["traj_ms"] / 1e3, *peaks,
+                              "traj_kernel<He-Ar, float, float> (bulk + solo)"),
+               "fp64": _roof(flops.work("hear", sp, False), sp["traj_ms"] / 1e3, *peaks,
+                             "traj_kernel<He-Ar, double, double> (bulk + solo)")}}
+    return out
+
+
+def bench_m0(args, hh, H, peaks):
+    """CO2-Ar Monte Carlo zeroth moment: 16 temperatures from 150 to 400 K, 1e8 samples each,
+    all temperatures in one launch; FP32 integrand (FP64 compensated sums) against FP64."""
+    from hawaiihybrid_b200 import _lib, flops
+    w, c = WORKLOAD, M0CFG
+    ms = hh.init_ms(w["mu"], hh.LINEAR_MOLECULE, hh.ATOM, (w["II"], w["II"]), None, 1)
+    p = _params(H, dict(w, Rmin=c["Rmin"], Rmax=c["Rmax"]), w["fp64_tol"], args.mixed_tol, N=64)
+    T, n = np.array(c["Ts"]), c["n_samples"]
+    res, wall = {}, {}
+    for name, prec in (("mixed", hh.PRECISION_MIXED), ("fp64", hh.PRECISION_FP64)):
+        hh.calculate_m0(ms, p, T, n // 16, seed=c["seed"], precision=prec)   # warm-up
+        t0 = time.perf_counter()
+        res[name] = hh.calculate_m0(ms, p, T, n, seed=c["seed"], precision=prec)
+        wall[name] = time.perf_counter() - t0
+    # kernel time of each precision in a second, timed-per-kernel call
+    kms = {}
+    for name, prec in (("mixed", hh.PRECISION_MIXED), ("fp64", hh.PRECISION_FP64)):
+        _lib.kernel_ms(True)
+        hh.calculate_m0(ms, p, T, n, seed=c["seed"], precision=prec)
+        kms[name] = _lib.kernel_ms(False)["moment"]["ms"]
+    m32, e32 = res["mixed"]
+    m64, e64 = res["fp64"]
+    rel = np.abs(m32 - m64) / np.abs(m64)
+    return {"workload": f"CO2-Ar MC M0, {T.size} temperatures {T[0]:.0f}-{T[-1]:.0f} K x {n:.0e} samples in one "
+                        f"launch, R ~ U[{c['Rmin']}, {c['Rmax']}], isotropic angles, Boltzmann momenta, Philox "
+                        f"seed {c['seed']}",
+            "mixed_samples_per_s": n / wall["mixed"], "fp64_samples_per_s": n / wall["fp64"],
+            "speedup_mixed_vs_fp64": wall["fp64"] / wall["mixed"],
+            "timing": "host wall time of the synchronous call (one moment kernel, its fixed-order final "
+                      "sum and the copy of 16 results); the kernel time is in roofline",
+            "m0_rel_err_max": float(rel.max()),
+            "m0_rel_stat_err_max": float(np.max(e64 / np.abs(m64))),
+            "roofline": {
+                "mixed": _roof(flops.m0_work("co2ar", n, T.size, True), kms["mixed"] / 1e3, *peaks,
+                               "m0_kernel<CO2-Ar, float>"),
+                "fp64": _roof(flops.m0_work("co2ar", n, T.size, False), kms["fp64"] / 1e3, *peaks,
+                              "m0_kernel<CO2-Ar, double>")}}
+
+
+def bench_n2ar(args, hh, H, peaks):
+    """N2-Ar PIP-NN: mixed (FP32 PES network and stages, FP32 dipole table, FP64 state and
+    error control) against the FP64 path on the same initial conditions, both with two
+    iterations per launch."""
+    from hawaiihybrid_b200 import flops
     w = N2AR
-    n = args.n2ar_trajectories
+    n, K = args.n2ar_trajectories, w["iters"]
     ms = hh.init_ms(w["mu"], hh.LINEAR_MOLECULE, hh.ATOM, (w["II"], w["II"]), None, w["seed"],
                     system_id=hh.SYSTEM_N2_AR)
 
     def params(tol=w["fp64_tol"]):
-        return H.CalcParams(ps=hh.PAIR_STATE_FREE_AND_METASTABLE, sampler_Rmin=w["Rmin"], sampler_Rmax=w["Rmax"],
-                            pesmin=w["pesmin"], sampling_time=w["dt"], MaxTrajectoryLength=w["N"],
-                            cvode_tolerance=tol, Rcut=w["Rcut"], partial_partition_function_ratio=1.0,
-                            mixed_tolerance=args.mixed_tol)
+        return _params(H, w, tol, args.mixed_tol)
 
     c1, _, s1 = hh.correlation_iteration(ms, params(), w["T"], n, hh.PRECISION_MIXED, seed=w["seed"])
-    hh.correlation_iterations(ms, params(), w["T"], n, 2, hh.PRECISION_MIXED, seed=w["seed"])  # buffers
-    cs, _, sk = hh.correlation_iterations(ms, params(), w["T"], n, 2, hh.PRECISION_MIXED, seed=w["seed"])
-    c64, _, s64 = hh.correlation_iteration(ms, params(), w["T"], n, hh.PRECISION_FP64, seed=w["seed"])
-    mixed = 2 * n / (sk.as_dict()["total_ms"] / 1e3)
-    plain = n / (s64.as_dict()["total_ms"] / 1e3)
+    hh.correlation_iterations(ms, params(), w["T"], n, K, hh.PRECISION_MIXED, seed=w["seed"])  # buffers
+    cs, _, sk = hh.correlation_iterations(ms, params(), w["T"], n, K, hh.PRECISION_MIXED, seed=w["seed"])
+    hh.correlation_iteration(ms, params(), w["T"], 2048, hh.PRECISION_FP64, seed=w["seed"])  # FP64 buffers
+    cp, _, sp = hh.correlation_iterations(ms, params(), w["T"], n, K, hh.PRECISION_FP64, seed=w["seed"])
+    sk, sp = sk.as_dict(), sp.as_dict()
+    mixed = K * n / (sk["total_ms"] / 1e3)
+    plain = K * n / (sp["total_ms"] / 1e3)
     out = {"workload": f"N2-Ar PIP-NN, {n} trajectories x {w['N']} samples, dt {w['dt']} a.u., T {w['T']} K, "
-                       f"R in [{w['Rmin']}, {w['Rmax']}]", "mixed_traj_per_s": mixed, "plain_fp64_traj_per_s": plain,
-           "speedup_mixed_vs_plain": mixed / plain, "mixed_single_batch_traj_per_s": n / (s1.as_dict()["total_ms"] / 1e3),
+                       f"R in [{w['Rmin']}, {w['Rmax']}]",
+           "iterations_per_call": K,
+           "mixed_traj_per_s": mixed, "plain_fp64_traj_per_s": plain, "speedup_same_K": mixed / plain,
+           "mixed_single_batch_traj_per_s": n / (s1.as_dict()["total_ms"] / 1e3),
            "mixed_rtol": args.mixed_tol, "fp64_rtol": w["fp64_tol"],
-           "submission": "mixed: two iterations per launch; FP64: one iteration"}
+           "roofline": {
+               "mixed": _roof(flops.work("n2ar", sk, True), sk["traj_ms"] / 1e3, *peaks,
+                              "traj_kernel<N2-Ar, float, float> (bulk + solo)"),
+               "fp64": _roof(flops.work("n2ar", sp, False), sp["traj_ms"] / 1e3, *peaks,
+                             "traj_kernel<N2-Ar, double, double> (bulk + solo)")}}
     if not args.no_accuracy:
         c13, _, _ = hh.correlation_iteration(ms, params(1e-13), w["T"], n, hh.PRECISION_FP64, seed=w["seed"])
-        c0 = abs(c64[0])
-        d = np.abs(c1 - c64) / c0
-        floor = np.abs(c13 - c64) / c0
-        run = np.maximum.accumulate(floor)
-        kh = int(np.argmax(run > 1e-8)) if np.any(run > 1e-8) else w["N"]
+        acc = _ct_errors(cs[0], cp[0], c13)
         kc = min(w["N"], int(1e5 / w["dt"]) + 1)
-        out["accuracy"] = {"m0_rel_err": float(d[0]), "ct_err_t_le_1e5au": float(d[:kc].max()),
-                           "fp64_horizon_k": kh, "ct_err_within_fp64_horizon": float(d[:max(kh, 1)].max()),
-                           "ct_err_all": float(d.max()), "fp64_floor_all": float(floor.max())}
+        acc["ct_err_t_le_1e5au"] = float((np.abs(cs[0] - cp[0]) / abs(cp[0][0]))[:kc].max())
+        out["accuracy"] = acc
     return out
 
 
-def bench_ch4co2(args, hh, H):
+def bench_ch4co2(args, hh, H, peaks):
     """CH4-CO2: 4 x n_per_T trajectories (one set per temperature) in one call, mixed
-    (FP32 PES, stages and batched dipole; FP64 state and C(t)) against the FP64 path on
-    the same initial conditions."""
+    (FP32 PES, stages and batched dipole; FP64 state, error control and C(t)) against the
+    FP64 path on the same initial conditions."""
+    from hawaiihybrid_b200 import _lib, flops
     w = CH4CO2
     n = args.ch4co2_per_T
     ms = hh.init_ms(w["mu"], hh.ROTOR, hh.LINEAR_MOLECULE, (w["II1"],) * 3, (w["II2"], w["II2"]), w["seed"])
 
-    def params(tol=w["fp64_tol"]):
-        return H.CalcParams(ps=hh.PAIR_STATE_FREE_AND_METASTABLE, sampler_Rmin=w["Rmin"], sampler_Rmax=w["Rmax"],
-                            pesmin=w["pesmin"], sampling_time=w["dt"], MaxTrajectoryLength=w["N"],
-                            cvode_tolerance=tol, Rcut=w["Rcut"], partial_partition_function_ratio=1.0,
-                            mixed_tolerance=args.mixed_tol)
-
     def run(prec, tol=w["fp64_tol"]):
-        return hh.correlation_temperatures(ms, params(tol), w["Ts"], n, prec, seed=w["seed"])
+        return hh.correlation_temperatures(ms, _params(H, w, tol, args.mixed_tol), w["Ts"], n, prec,
+                                           seed=w["seed"])
 
-    run(hh.PRECISION_MIXED)   # grows the device buffers to the timed size
+    run(hh.PRECISION_MIXED)   # grows the device buffers to the timed size, tunes the dipole kernel
     cm, _, sm = run(hh.PRECISION_MIXED)
     run(hh.PRECISION_FP64)
     cp, _, sp = run(hh.PRECISION_FP64)
+    # per-kernel device times of one more call of each precision (kernels serialised)
+    kt = {}
+    for name, prec in (("mixed", hh.PRECISION_MIXED), ("fp64", hh.PRECISION_FP64)):
+        _lib.kernel_ms(True)
+        run(prec)
+        kt[name] = _lib.kernel_ms(False)
     tot = len(w["Ts"]) * n
     sm, sp = sm.as_dict(), sp.as_dict()
     mixed = tot / (sm["total_ms"] / 1e3)
@@ -141,23 +282,118 @@ def bench_ch4co2(args, hh, H):
                        f"{'/'.join(str(int(t)) for t in w['Ts'])} K in one call, {w['N']} samples at dt {w['dt']} a.u., "
                        f"R in [{w['Rmin']}, {w['Rmax']}]; stand-in site-site PES (the reference has no source for "
                        "its CH4-CO2 PES), reference dipole",
-           "mixed_traj_per_s": mixed, "plain_fp64_traj_per_s": plain, "speedup_mixed_vs_plain": mixed / plain,
+           "mixed_traj_per_s": mixed, "plain_fp64_traj_per_s": plain, "speedup_same_K": mixed / plain,
            "mixed_ms": sm["total_ms"], "plain_ms": sp["total_ms"], "mixed_rtol": args.mixed_tol,
            "fp64_rtol": w["fp64_tol"], "kernel_launches": sm["n_kernel_launches"],
            "stats_mixed": {k: sm[k] for k in ("n_candidates", "n_steps", "n_rhs", "n_samples", "n_failed",
-                                              "sample_ms", "traj_ms")}}
-    from hawaiihybrid_b200 import _lib
+                                              "sample_ms", "traj_ms")},
+           "kernel_ms": {p: {k: v["ms"] for k, v in d.items() if v["launches"]} for p, d in kt.items()}}
     s64, s32 = C.c_int(0), C.c_int(0)
     _lib.check(_lib.load().hh_cuda_debug_tuning(C.byref(s64), C.byref(s32)))
     out["dipole_records_per_lane"] = {"fp64": s64.value, "mixed": s32.value,
                                       "how": "timed per precision on the first call's records (the warm-up)"}
+    nb, ng = _lib.ch4co2_fold_shape()
+    fl = flops.ch4_dipole_flops(4 * nb, ng)
+    for name, st in (("mixed", sm), ("fp64", sp)):
+        dms = kt[name]["ch4_dipole"]["ms"]
+        if dms > 0:
+            work = {"fp32": float(fl * st["n_samples"]) if name == "mixed" else 0.0,
+                    "fp64": 0.0 if name == "mixed" else float(fl * st["n_samples"])}
+            out.setdefault("roofline", {})[name] = _roof(
+                work, dms / 1e3, *peaks, f"ch4_dipole_kernel<{'float' if name == 'mixed' else 'double'}>",
+                note=f"{fl} flops per record ({4 * nb} padded coefficient entries, {ng} groups) x the call's "
+                     f"records; time from a per-kernel timed call")
     if not args.no_accuracy:
-        per_T = []
-        for i in range(len(w["Ts"])):
-            c0 = abs(cp[i][0])
-            d = np.abs(cm[i] - cp[i]) / c0
-            per_T.append({"T": w["Ts"][i], "m0_rel_err": float(d[0]), "ct_err_all": float(d.max())})
-        out["accuracy"] = per_T
+        out["accuracy"] = [dict(T=w["Ts"][i], **_ct_errors(cm[i], cp[i])) for i in range(len(w["Ts"]))]
+    return out
+
+
+# ----------------------------------------------------------------------------
+# parity of the FP64 path against the CPU oracle at the workload sizes
+# ----------------------------------------------------------------------------
+def parity_block(args, hh, H, ms_co2, horizon_k, cpu):
+    from oracle import oracle as O
+    from tests.helpers import oracle_params, oracle_system
+    cores = os.cpu_count() or 1
+    out = {"definition": "FP64 GPU path against the FP64 CPU oracle on the same initial conditions: "
+                         "max_k |dC| / C(0) over the whole window and within the FP64 horizon (the window "
+                         "where FP64 at rtol 1e-12 and 1e-13 agree to 1e-8 C(0)); the oracle integrates the "
+                         "reference's spherical equations, the GPU the Cartesian ones"}
+    w = WORKLOAD
+    # 1. the sampler over the whole draw of one step (102,400 accepted trajectories)
+    sysd = oracle_system("co2ar")
+    op = oracle_params("co2ar", args.samples, w["dt"], tol=w["fp64_tol"])
+    p = _params(H, w, w["fp64_tol"], args.mixed_tol, N=args.samples)
+    qp_ref, nc_ref = O.sample(w["seed"], sysd, op, w["T"], args.trajectories)
+    qp_gpu, nc_gpu = hh.sample_initial_conditions(ms_co2, p, w["T"], args.trajectories, seed=w["seed"])
+    out["sampler_co2ar"] = {"accepted": args.trajectories, "n_candidates_gpu": nc_gpu,
+                            "n_candidates_oracle": int(nc_ref), "equal": nc_gpu == int(nc_ref),
+                            "qp_max_rel_diff": float(np.max(np.abs(qp_gpu - qp_ref) /
+                                                            np.maximum(np.abs(qp_ref), 1e-300)))}
+    # 2. CO2-Ar FP64 C(t): first S trajectories at N = 32,768 (the CPU-baseline leg's work)
+    S = args.cpu_sample
+    c_gpu, _ = hh.correlation_from_initial_conditions(ms_co2, p, qp_ref[:S])
+    c_gpu13, _ = hh.correlation_from_initial_conditions(ms_co2, _params(H, w, 1e-13, args.mixed_tol,
+                                                                           N=args.samples), qp_ref[:S])
+    c_ref = cpu["_ct"] if cpu and "_ct" in cpu else O.correlation_sum(sysd, op, qp_ref[:S], nthreads=cores)
+    e = _ct_errors(c_gpu, c_ref, c_gpu13)
+    out["co2ar"] = dict(trajectories=S, samples=args.samples, **e)
+    # 3. N2-Ar: 512 trajectories at N = 16,384, T = 200 K
+    s2 = oracle_system("n2ar")
+    w2 = N2AR
+    op2 = oracle_params("n2ar", w2["N"], w2["dt"], tol=w2["fp64_tol"])
+    q2, _ = O.sample(w2["seed"], s2, op2, w2["T"], 512)
+    ms2 = hh.init_ms(w2["mu"], hh.LINEAR_MOLECULE, hh.ATOM, (w2["II"], w2["II"]), None, w2["seed"],
+                     system_id=hh.SYSTEM_N2_AR)
+    g2, _ = hh.correlation_from_initial_conditions(ms2, _params(H, w2, w2["fp64_tol"], args.mixed_tol), q2)
+    g213, _ = hh.correlation_from_initial_conditions(ms2, _params(H, w2, 1e-13, args.mixed_tol), q2)
+    r2 = O.correlation_sum(s2, op2, q2, nthreads=cores)
+    out["n2ar"] = dict(trajectories=512, samples=w2["N"], **_ct_errors(g2, r2, g213))
+    # 4. CH4-CO2: 1,024 trajectories at each of the four temperatures, N = 21
+    s4 = oracle_system("ch4co2")
+    w4 = CH4CO2
+    op4 = oracle_params("ch4co2", w4["N"], w4["dt"], tol=w4["fp64_tol"])
+    ms4 = hh.init_ms(w4["mu"], hh.ROTOR, hh.LINEAR_MOLECULE, (w4["II1"],) * 3, (w4["II2"], w4["II2"]), w4["seed"])
+    worst = None
+    for T in w4["Ts"]:
+        q4, _ = O.sample(w4["seed"], s4, op4, T, 1024)
+        g4, _ = hh.correlation_from_initial_conditions(ms4, _params(H, w4, w4["fp64_tol"], args.mixed_tol), q4)
+        r4 = O.correlation_sum(s4, op4, q4, nthreads=cores)
+        e4 = _ct_errors(g4, r4)
+        if worst is None or e4["ct_err_all"] > worst["ct_err_all"]:
+            worst = dict(T=T, **e4)
+    out["ch4co2"] = dict(trajectories_per_T=1024, samples=w4["N"], worst_T=worst)
+    # 5. He-Ar: the whole workload (10,240 trajectories x 65,536 samples) and its sampler
+    s1 = oracle_system("hear")
+    w1 = HEAR
+    op1 = oracle_params("hear", w1["N"], w1["dt"], tol=w1["fp64_tol"])
+    ms1 = hh.init_ms(w1["mu"], hh.ATOM, hh.ATOM, None, None, w1["seed"])
+    p1 = _params(H, w1, w1["fp64_tol"], args.mixed_tol)
+    q1, n1 = O.sample(w1["seed"], s1, op1, w1["T"], w1["n_traj"])
+    q1g, n1g = hh.sample_initial_conditions(ms1, p1, w1["T"], w1["n_traj"], seed=w1["seed"])
+    g1, _ = hh.correlation_from_initial_conditions(ms1, p1, q1)
+    g113, _ = hh.correlation_from_initial_conditions(ms1, _params(H, w1, 1e-13, args.mixed_tol), q1)
+    r1 = O.correlation_sum(s1, op1, q1, nthreads=cores)
+    out["hear"] = dict(trajectories=w1["n_traj"], samples=w1["N"], n_candidates_equal=int(n1) == n1g,
+                       qp_max_rel_diff=float(np.max(np.abs(q1g - q1) / np.maximum(np.abs(q1), 1e-300))),
+                       **_ct_errors(g1, r1, g113))
+    # spectral function of the oracle's C(t) by the device FFT and by the oracle
+    cfd = r1 / w1["n_traj"]
+    _, sf_ref, _ = O.idct_cf_to_sf(cfd, w1["dt"])
+    sf_dev = hh.idct_cf_to_sf(hh.CFnc(t=w1["dt"] * np.arange(w1["N"]), data=cfd.copy(), ntraj=float(w1["n_traj"]),
+                                      Temperature=w1["T"], normalized=True)).data
+    out["hear"]["sf_max_rel_to_peak"] = float(np.max(np.abs(sf_dev - sf_ref)) / np.max(np.abs(sf_ref)))
+    # 6. M0: the FP64 integrand against the oracle on the same Philox samples
+    c = M0CFG
+    T = np.array(c["Ts"])
+    nm = 1 << 21
+    pm = _params(H, dict(w, Rmin=c["Rmin"], Rmax=c["Rmax"]), w["fp64_tol"], args.mixed_tol, N=64)
+    m64, _ = hh.calculate_m0(ms_co2, pm, T, nm, seed=c["seed"], precision=hh.PRECISION_FP64)
+    opm = oracle_params("co2ar", 64, w["dt"], Rmin=c["Rmin"], Rmax=c["Rmax"])
+    ws_, _ = O.m0(sysd, opm, T, nm, c["seed"], nthreads=cores)
+    mref = O.m0_scale(opm) * ws_ / nm
+    out["m0_co2ar"] = {"samples": nm, "temperatures": int(T.size),
+                       "max_rel_err": float(np.max(np.abs(m64 - mref) / np.abs(mref)))}
     return out
 
 
@@ -168,8 +404,10 @@ def config(args, ws):
             "pair_state": "FREE_AND_METASTABLE", "R_range_bohr": [WORKLOAD["Rmin"], WORKLOAD["Rmax"]],
             "Rcut_bohr": WORKLOAD["Rcut"], "fp64_rtol": WORKLOAD["fp64_tol"], "mixed_rtol": args.mixed_tol,
             "parallelism": f"dp{ws}" if ws > 1 else "single-gpu",
+            "iterations_per_call": args.steps,
             "l2": "256 MB flush before the timed call; working set (tables + C(t)) < 2 MB",
-            "submission": "the K timed steps are one call of K iterations (hh_cuda_correlation_multi)"}
+            "submission": "the K timed steps are one call of K iterations (hh_cuda_correlation_multi); "
+                          "the FP64 arms run the same K iterations per call"}
 
 
 # ----------------------------------------------------------------------------
@@ -266,12 +504,6 @@ def main():
     from hawaiihybrid_b200 import hawaii as H
 
     torch.cuda.set_device(local)
-    if args.only_ch4co2:
-        print(json.dumps({"ch4co2_four_temperatures": bench_ch4co2(args, hh, H)}), flush=True)
-        return 0
-    if args.only_n2ar:
-        print(json.dumps({"n2ar_pip_nn": bench_n2ar(args, hh, H)}), flush=True)
-        return 0
     dist = None
     if ws > 1:
         import datetime
@@ -281,14 +513,20 @@ def main():
     seed = WORKLOAD["seed"] + 1000 * rank   # one seed per rank, like the reference's per-rank seed table
     ms = hh.init_ms(WORKLOAD["mu"], hh.LINEAR_MOLECULE, hh.ATOM, (WORKLOAD["II"], WORKLOAD["II"]), None, seed,
                     device=local)
+    lib = _lib.load()
+    p32, p64 = C.c_double(), C.c_double()
+    _lib.check(lib.hh_cuda_fma_peak(_lib.HH_PRECISION_MIXED, C.byref(p32)))
+    _lib.check(lib.hh_cuda_fma_peak(_lib.HH_PRECISION_FP64, C.byref(p64)))
+    peaks = (p32.value, p64.value)
+    if args.only:
+        fn = {"n2ar": bench_n2ar, "ch4co2": bench_ch4co2, "hear": bench_hear, "m0": bench_m0}[args.only]
+        print(json.dumps({args.only: fn(args, hh, H, peaks)}), flush=True)
+        return 0
     n = args.trajectories
+    K = args.steps
 
     def params(tol=WORKLOAD["fp64_tol"]):
-        return H.CalcParams(ps=hh.PAIR_STATE_FREE_AND_METASTABLE, sampler_Rmin=WORKLOAD["Rmin"],
-                            sampler_Rmax=WORKLOAD["Rmax"], pesmin=WORKLOAD["pesmin"],
-                            sampling_time=WORKLOAD["dt"], MaxTrajectoryLength=args.samples,
-                            cvode_tolerance=tol, Rcut=WORKLOAD["Rcut"], partial_partition_function_ratio=1.0,
-                            mixed_tolerance=args.mixed_tol)
+        return _params(H, WORKLOAD, tol, args.mixed_tol, N=args.samples)
 
     p = params()
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=f"cuda:{local}")
@@ -298,12 +536,12 @@ def main():
             dist.barrier()
         torch.cuda.synchronize()
 
-    def run(prec, iters, pp=p):
-        """`iters` consecutive iterations (steps) of n trajectories in one pipelined call."""
+    def run(prec, iters, pp=p, nn=n):
+        """`iters` consecutive iterations (steps) of nn trajectories in one pipelined call."""
         flush.zero_()
         barrier()
         t0 = time.perf_counter()
-        crlns, ntrajs, st = hh.correlation_iterations(ms, pp, WORKLOAD["T"], n, iters, prec, seed=seed)
+        crlns, ntrajs, st = hh.correlation_iterations(ms, pp, WORKLOAD["T"], nn, iters, prec, seed=seed)
         if dist:   # the one exchange step of the path: C(t) and ntraj summed over ranks
             t = torch.from_numpy(np.concatenate([crlns.ravel(), ntrajs])).to(f"cuda:{local}")
             dist.all_reduce(t)
@@ -333,71 +571,74 @@ def main():
     # no allocation falls inside the timed call ----
     clocks = Clocks(local)
     clocks.start()
-    run(hh.PRECISION_MIXED, args.steps)
-    crlns_m, _, last, wall_m = run(hh.PRECISION_MIXED, args.steps)
+    run(hh.PRECISION_MIXED, K)
+    crlns_m, _, last, wall_m = run(hh.PRECISION_MIXED, K)
     ck = clocks.stop()
     launches = int(last["n_kernel_launches"])
-    mixed_ms = max_over_ranks(last["total_ms"]) / args.steps
-    mixed_wall = max_over_ranks(wall_m) / args.steps
+    mixed_ms = max_over_ranks(last["total_ms"]) / K
+    mixed_wall = max_over_ranks(wall_m) / K
     value = n * ws / (mixed_ms / 1e3)
     crln_m = crlns_m[0]
 
-    # ---- plain FP64 path on the same initial conditions ----
-    run(hh.PRECISION_FP64, max(1, args.plain_steps), params())  # warm-up at the timed size
-    crlns_p, _, st_p, _ = run(hh.PRECISION_FP64, max(1, args.plain_steps))
-    plain_ms = max_over_ranks(st_p["total_ms"]) / max(1, args.plain_steps)
-    plain_value = n * ws / (plain_ms / 1e3)
-    crln_p = crlns_p[0]
+    # ---- FP64 arms on the same initial conditions and the same K per call.  The FP64
+    # kernels' own buffers (the hand-off slots) are grown by a small untimed call; every
+    # other buffer already has the timed size ----
+    plain = fp64_rt = None
+    crln_p = None
+    if not args.no_fp64:
+        run(hh.PRECISION_FP64, 1, p, 1024)
+        crlns_p, _, st_p, _ = run(hh.PRECISION_FP64, K)
+        plain_ms = max_over_ranks(st_p["total_ms"]) / K
+        crln_p = crlns_p[0]
+        crlns_r, _, st_r, _ = run(hh.PRECISION_FP64, K, params(args.mixed_tol))
+        rt_ms = max_over_ranks(st_r["total_ms"]) / K
+        plain = {"value": n * ws / (plain_ms / 1e3), "unit": "traj/s", "ms_per_step": plain_ms,
+                 "iterations_per_call": K, "rtol": WORKLOAD["fp64_tol"]}
+        fp64_rt = {"value": n * ws / (rt_ms / 1e3), "unit": "traj/s", "ms_per_step": rt_ms,
+                   "iterations_per_call": K, "rtol": args.mixed_tol}
 
     # ---- accuracy of the mixed path against the FP64 path (same initial conditions) ----
     acc = None
-    if not args.no_accuracy:
-        c0 = abs(crln_p[0])
-        d = np.abs(crln_m - crln_p) / c0
-        kc = min(args.samples, int(1e5 / WORKLOAD["dt"]) + 1)   # collision window t <= 1e5 a.u.
-        acc = {"m0_rel_err": float(abs(crln_m[0] - crln_p[0]) / c0),
-               "ct_err_t_le_1e5au": float(d[:kc].max()),
-               "ct_err_all": float(d.max())}
-        # reproducibility of the FP64 answer itself: rtol 1e-13 against 1e-12
+    horizon_k = None
+    if not args.no_accuracy and crln_p is not None:
         crlns_t, _, _, _ = run(hh.PRECISION_FP64, 1, params(1e-13))
-        floor = np.abs(crlns_t[0] - crln_p) / c0
-        runmax = np.maximum.accumulate(floor)
-        kh = int(np.argmax(runmax > 1e-8)) if np.any(runmax > 1e-8) else args.samples
-        acc.update({"fp64_floor_all": float(floor.max()),
-                    "fp64_horizon_k": kh, "fp64_horizon_t_au": kh * WORKLOAD["dt"],
-                    "ct_err_within_fp64_horizon": float(d[:kh].max()) if kh > 0 else None,
-                    "definition": "max_k |C_mixed - C_fp64| / C_fp64(0) on the first step's trajectories; "
-                                  "fp64 horizon = first k where FP64 at rtol 1e-13 and 1e-12 differ by "
-                                  "more than 1e-8 C(0)"})
+        acc = _ct_errors(crln_m, crln_p, crlns_t[0])
+        kc = min(args.samples, int(1e5 / WORKLOAD["dt"]) + 1)   # collision window t <= 1e5 a.u.
+        acc["ct_err_t_le_1e5au"] = float((np.abs(crln_m - crln_p) / abs(crln_p[0]))[:kc].max())
+        acc["fp64_horizon_t_au"] = acc["fp64_horizon_k"] * WORKLOAD["dt"]
+        horizon_k = acc["fp64_horizon_k"]
+        acc["fp64_at_mixed_rtol"] = _ct_errors(crlns_r[0], crln_p, crlns_t[0])
+        acc["definition"] = ("max_k |C_mixed - C_fp64| / C_fp64(0) on the first step's trajectories; "
+                             "fp64 horizon = first k where FP64 at rtol 1e-13 and 1e-12 differ by more than "
+                             "1e-8 C(0)")
 
     # ---- roofline of the trajectory kernel (mixed path) ----
-    lib = _lib.load()
-    p32, p64 = C.c_double(), C.c_double()
-    _lib.check(lib.hh_cuda_fma_peak(_lib.HH_PRECISION_MIXED, C.byref(p32)))
-    _lib.check(lib.hh_cuda_fma_peak(_lib.HH_PRECISION_FP64, C.byref(p64)))
     w = flops.work("co2ar", last, mixed=True)
     t_s = last["traj_ms"] / 1e3
-    achieved = (w["fp32"] + w["fp64"]) / t_s / 1e12
-    frac = (w["fp32"] / (p32.value * 1e12) + w["fp64"] / (p64.value * 1e12)) / t_s
-    peak = achieved / frac if frac > 0 else None
-    wp = flops.work("co2ar", st_p, mixed=False)
-    frac_p = wp["fp64"] / (p64.value * 1e12) / (st_p["traj_ms"] / 1e3)
+    roof = _roof(w, t_s, *peaks, "traj_kernel<CO2-Ar, float, float> (mixed, bulk + solo)")
     # DRAM bytes per trajectory from one ncu capture of a single-iteration launch,
-    # scaled to the timed launch's n * steps trajectories (initial conditions and
-    # C(t) slices both grow with the trajectories a launch processes)
+    # scaled to the timed launch's n * K trajectories
     traffic = None
     if os.path.exists(PROFILE_TRAFFIC):
         try:
             tr = json.load(open(PROFILE_TRAFFIC))
-            traffic = tr["traj_kernel_mixed_bytes_per_trajectory"] * n * args.steps
+            traffic = tr["traj_kernel_mixed_bytes_per_trajectory"] * n * K
         except (ValueError, OSError, KeyError, TypeError):
             traffic = None
     roof = {"bound": "fp32+fp64 CUDA-core FMA (no tensor or HBM bound: ~1e-3 B/flop)",
-            "achieved": achieved, "peak": peak, "unit": "TFLOP/s", "frac": frac, "traffic": traffic,
-            "kernel": "traj_kernel<CO2-Ar, float, float> (mixed)",
+            "achieved": roof["achieved_tflops"], "peak": roof["peak_tflops"], "unit": "TFLOP/s",
+            "frac": roof["frac"], "traffic": traffic, "kernel": roof["kernel"],
             "peak_source": f"measured in-process FMA loops: fp32 {p32.value:.1f}, fp64 {p64.value:.1f} TFLOP/s; "
                            "peak = the blend for this kernel's fp32/fp64 mix",
-            "work_flops": w, "plain_fp64_frac": frac_p}
+            "work_flops": w}
+    if plain is not None:
+        roof["plain_fp64_frac"] = _roof(flops.work("co2ar", st_p, mixed=False), st_p["traj_ms"] / 1e3,
+                                        *peaks, "")["frac"]
+    # bulk / solo split of the trajectory kernel in one per-kernel timed call (kernels serialised)
+    _lib.kernel_ms(True)
+    run(hh.PRECISION_MIXED, K)
+    kt = _lib.kernel_ms(False)
+    roof["kernel_ms_split"] = {k: v["ms"] for k, v in kt.items() if v["launches"]}
 
     # ---- CPU baseline: the oracle on a bounded sample (rank 0, one GPU) ----
     cpu = None
@@ -410,40 +651,49 @@ def main():
         S = args.cpu_sample
         qp, _ = O.sample(WORKLOAD["seed"], sysd, op, WORKLOAD["T"], S)
         t0 = time.perf_counter()
-        O.correlation_sum(sysd, op, qp, nthreads=cores)
+        c_ct = O.correlation_sum(sysd, op, qp, nthreads=cores)
         cs = time.perf_counter() - t0
         cpu = {"value": S / cs, "unit": "traj/s", "cores": cores, "kind": "port",
                "sample": f"first {S} accepted trajectories of the workload, FP64 DOP853 rtol 1e-12, "
-                         f"{cores} threads, {cs:.1f} s"}
+                         f"{cores} threads, {cs:.1f} s", "_ct": c_ct}
 
-    n2ar = None
-    if rank == 0 and ws == 1 and not args.no_n2ar:
-        n2ar = bench_n2ar(args, hh, H)
-    ch4co2 = None
-    if rank == 0 and ws == 1 and not args.no_ch4co2:
-        ch4co2 = bench_ch4co2(args, hh, H)
+    parity = None
+    if rank == 0 and ws == 1 and not args.no_parity:
+        parity = parity_block(args, hh, H, ms, horizon_k, cpu)
+    if cpu:
+        cpu.pop("_ct", None)
+
+    extra = {}
+    if rank == 0 and ws == 1:
+        for flag, key, fn in ((args.no_hear, "hear_fp64_65536", bench_hear),
+                              (args.no_m0, "co2ar_m0_16T", bench_m0),
+                              (args.no_n2ar, "n2ar_pip_nn", bench_n2ar),
+                              (args.no_ch4co2, "ch4co2_four_temperatures", bench_ch4co2)):
+            if not flag:
+                extra[key] = fn(args, hh, H, peaks)
 
     if rank == 0:
         h2d = C.sizeof(_lib.CalcParamsC) + 8 + 4 + 8 + 4
         d2h = args.samples * 8 + 8 + C.sizeof(_lib.Stats)
-        line = {"metric": METRIC, "value": value, "unit": "traj/s", "n_gpus": ws, "steps": args.steps,
+        line = {"metric": METRIC, "value": value, "unit": "traj/s", "n_gpus": ws, "steps": K,
                 "warmup": args.warmup, "ms_per_step": mixed_ms, "higher_is_better": True, "scaling": "weak",
                 "vs_baseline": None, "dtype": "fp32 surfaces + fp64 state", "data": "synthetic (Boltzmann-sampled "
                 "initial conditions, MT19937 seed 7 + 1000*rank)", "config": config(args, ws),
-                "plain_fp64": {"value": plain_value, "unit": "traj/s", "ms_per_step": plain_ms,
-                               "steps_per_call": max(1, args.plain_steps),
-                               "mixed_steps_per_call": args.steps},
+                "plain_fp64": plain, "fp64_at_mixed_rtol": fp64_rt,
+                "speedup_same_K": value / plain["value"] if plain else None,
+                "speedup_same_rtol": value / fp64_rt["value"] if fp64_rt else None,
                 "single_batch": {"mixed_traj_per_s": n * ws / (single_mixed_ms / 1e3),
                                  "mixed_ms": single_mixed_ms,
                                  "note": "one step submitted alone: its long-lived trajectories "
-                                         "finish with the GPU mostly idle"},
-                "speedup_mixed_vs_plain": value / plain_value,
+                                         "finish with the GPU mostly idle.  A call's first MT19937 "
+                                         "words were generated on a side stream during the previous "
+                                         "call of the same size, so a run's very first call is slower"},
                 "accuracy": acc,
                 "e2e": {"value": n * ws / mixed_wall, "unit": "traj/s", "h2d_bytes_per_step": h2d,
                         "d2h_bytes_per_step": d2h},
                 "gpu_launches": launches, "clocks": ck, "roofline": roof, "cpu_baseline": cpu,
-                "n2ar_pip_nn": n2ar,
-                "ch4co2_four_temperatures": ch4co2,
+                "parity": parity,
+                **extra,
                 "stats_last_step": {k: last[k] for k in ("n_candidates", "n_steps", "n_rejected_steps", "n_rhs",
                                                          "n_samples", "n_dense", "n_failed", "sample_ms",
                                                          "traj_ms")}}

@@ -45,7 +45,11 @@ EXPORTS = (
     "hh_cuda_mt_stream", "hh_cuda_debug_inject", "hh_cuda_debug_item_trace", "hh_cuda_fma_peak",
     "hh_cuda_shutdown", "hh_cuda_m0_noalloc", "hh_cuda_correlation_array", "hh_cuda_correlation_temperatures",
     "hh_cuda_prmu", "hh_cuda_debug_n2ar_dipole", "hh_cuda_m2", "hh_cuda_debug_tuning",
+    "hh_cuda_debug_kernel_ms", "hh_cuda_debug_ch4co2_fold", "hh_cuda_moment_sums",
 )
+# kernel classes of hh_cuda_debug_kernel_ms
+HH_KT_NAMES = ("traj_bulk", "traj_solo", "ch4_dipole", "ch4_sort", "ch4_corr", "moment")
+HH_KT_COUNT = len(HH_KT_NAMES)
 
 
 class HHError(RuntimeError):
@@ -120,6 +124,8 @@ def load(path: str | None = None):
                              _dp, _dp]
     L.hh_cuda_m2.argtypes = [C.POINTER(CalcParamsC), _dp, C.c_int, C.c_uint64, C.c_uint64, _dp, _dp]
     L.hh_cuda_m0_noalloc.argtypes = L.hh_cuda_m0.argtypes
+    L.hh_cuda_moment_sums.argtypes = [C.POINTER(CalcParamsC), _dp, C.c_int, C.c_uint64, C.c_uint64, C.c_uint64,
+                                      C.c_int, C.c_int, _dp, _dp]
     L.hh_cuda_correlation_array.argtypes = [C.POINTER(CalcParamsC), C.c_double, _dp, _dp, C.c_int, C.c_uint32,
                                             C.c_uint64, C.c_int, _dp, _dp, C.POINTER(C.c_double),
                                             C.POINTER(Stats)]
@@ -132,6 +138,9 @@ def load(path: str | None = None):
     L.hh_cuda_fma_peak.argtypes = [C.c_int, C.POINTER(C.c_double)]
     L.hh_cuda_debug_n2ar_dipole.argtypes = [C.c_int, _dp, _dp, C.c_uint64, _dp]
     L.hh_cuda_debug_tuning.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.hh_cuda_debug_kernel_ms.argtypes = [C.c_int, _dp, np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS"),
+                                          C.c_int]
+    L.hh_cuda_debug_ch4co2_fold.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.hh_cuda_shutdown.restype = None
     for name in EXPORTS:
         if name not in ("hh_cuda_strerror", "hh_cuda_shutdown"):
@@ -144,3 +153,19 @@ def check(code: int) -> None:
     if code != HH_OK:
         msg = load().hh_cuda_strerror(code).decode()
         raise HHError(code, msg)
+
+
+def kernel_ms(enable: bool) -> dict:
+    """Per-kernel-class device time accumulated since the last call (hh_cuda_debug_kernel_ms),
+    then switch the timer on or off."""
+    ms = np.zeros(HH_KT_COUNT)
+    n = np.zeros(HH_KT_COUNT, dtype=np.uint64)
+    check(load().hh_cuda_debug_kernel_ms(int(bool(enable)), ms, n, HH_KT_COUNT))
+    return {name: {"ms": float(ms[i]), "launches": int(n[i])} for i, name in enumerate(HH_KT_NAMES)}
+
+
+def ch4co2_fold_shape() -> tuple[int, int]:
+    """(batches of 4 coefficient entries, groups) of the CH4-CO2 dipole stream per radial piece."""
+    nb, ng = C.c_int(0), C.c_int(0)
+    check(load().hh_cuda_debug_ch4co2_fold(C.byref(nb), C.byref(ng)))
+    return nb.value, ng.value

@@ -81,7 +81,9 @@ struct Ctx {
   double mu = 0.0, II = 0.0;
   int QP = 0, D = 0;
   cudaStream_t st = nullptr;
-  cudaEvent_t ev[4] = {nullptr, nullptr, nullptr, nullptr};
+  // [0, 1]: call; [2, 3]: trajectory launches; [4, 5]: autotuner timing runs;
+  // [6, 7]: per-kernel timer (hh_cuda_debug_kernel_ms)
+  cudaEvent_t ev[8] = {nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr, nullptr};
   // side stream that generates the MT19937 words of the next call while this
   // call's trajectories run
   cudaStream_t st2 = nullptr;
@@ -100,6 +102,7 @@ struct Ctx {
   unsigned int *d_ch4_y2 = nullptr;
   unsigned int *d_ch4_meta = nullptr;
   int ch4_B = 0;
+  int ch4_groups = 0;  // (Y1, component, cos/sin) groups of the batch stream
   int ch4_dip_s[2] = {0, 0};  // records per lane of the dipole kernel [FP64, mixed]; 0: not tuned yet
   // MT19937 stream
   uint32_t *d_mt = nullptr;
@@ -149,6 +152,28 @@ struct Ctx {
 
 Ctx g;
 unsigned long long g_launches = 0;  // kernel launches of the current call
+
+// per-kernel-class device time (hh_cuda_debug_kernel_ms): when on, kt_begin /
+// kt_end bracket a launch with events and wait for it
+struct KernelTimer {
+  bool on = false;
+  double ms[HH_KT_COUNT] = {};
+  unsigned long long n[HH_KT_COUNT] = {};
+};
+KernelTimer g_kt;
+inline void kt_begin() {
+  if (g_kt.on) cudaEventRecord(g.ev[6], g.st);
+}
+inline void kt_end(int cls) {
+  if (!g_kt.on) return;
+  cudaEventRecord(g.ev[7], g.st);
+  cudaEventSynchronize(g.ev[7]);
+  float ms = 0.f;
+  if (cudaEventElapsedTime(&ms, g.ev[6], g.ev[7]) == cudaSuccess) {
+    g_kt.ms[cls] += ms;
+    g_kt.n[cls] += 1;
+  }
+}
 int g_inject_item = -1, g_inject_k = -1, g_inject_status = 0;
 uint32_t *g_trace_host = nullptr;  // registered by hh_cuda_debug_item_trace for the next call
 uint64_t g_trace_cap = 0;
@@ -377,12 +402,16 @@ int launch_traj(const TrajParams &P, const TrajIO &io, int *grid_out) {
     io2.done = g.hcount.p + 2;
     io2.handoff_at = cap;
     if ((unsigned)io.n_items > cap) {
+      kt_begin();
       kern<<<grid, TRAJ_THREADS, smem, g.st>>>(P, io2, g.d_tab);
       CK(cudaGetLastError());
+      kt_end(HH_KT_TRAJ_BULK);
       g_launches += 1;
     }
+    kt_begin();
     solo<<<solo_grid, TRAJ_THREADS, smem, g.st>>>(P, io2, g.d_tab);
     CK(cudaGetLastError());
+    kt_end(HH_KT_TRAJ_SOLO);
     g_launches += 1;
   }
   if (grid_out) *grid_out = grid;
@@ -595,37 +624,39 @@ int run_records_t(const TrajParams &P, const double *d_ic, uint64_t n, uint64_t 
       return HH_OK;
     };
     if (tuned_s == 0) {
-      cudaEvent_t e0, e1;
-      CK(cudaEventCreate(&e0));
-      CK(cudaEventCreate(&e1));
       float best = 0.0f;
       for (int c = 0; c < ncand; ++c) {
         int rcs = sort_for(cand[c]);
         if (rcs) return rcs;
-        // timing run: about 2^20 records for every variant, in tasks spread over all
-        // radial pieces
+        // about 2^20 records for every variant, in tasks spread over all radial
+        // pieces: one untimed run (the variant's first launch), then the timed one
         const long long step = std::max<long long>(1, nslots >> 20);
-        CK(cudaEventRecord(e0, g.st));
         rcs = dipole_with(cand[c], (1LL << 20) / (32 * cand[c].S), step);
         if (rcs) return rcs;
-        CK(cudaEventRecord(e1, g.st));
-        CK(cudaEventSynchronize(e1));
+        CK(cudaEventRecord(g.ev[4], g.st));
+        rcs = dipole_with(cand[c], (1LL << 20) / (32 * cand[c].S), step);
+        if (rcs) return rcs;
+        CK(cudaEventRecord(g.ev[5], g.st));
+        CK(cudaEventSynchronize(g.ev[5]));
         float ms = 0.0f;
-        CK(cudaEventElapsedTime(&ms, e0, e1));
+        CK(cudaEventElapsedTime(&ms, g.ev[4], g.ev[5]));
         if (tuned_s == 0 || ms < best) {
           best = ms;
           tuned_s = cand[c].S;
         }
       }
-      cudaEventDestroy(e0);
-      cudaEventDestroy(e1);
-      g_launches += 4 * (unsigned long long)ncand;
+      g_launches += 5 * (unsigned long long)ncand;
     }
     const Ch4DipVariant *use = &cand[0];
     for (int c = 0; c < ncand; ++c)
       if (cand[c].S == tuned_s) use = &cand[c];
+    kt_begin();
     int rcd = sort_for(*use);
-    if (!rcd) rcd = dipole_with(*use, LLONG_MAX, 1);
+    kt_end(HH_KT_CH4_SORT);
+    if (rcd) return rcd;
+    kt_begin();
+    rcd = dipole_with(*use, LLONG_MAX, 1);
+    kt_end(HH_KT_CH4_DIPOLE);
     if (rcd) return rcd;
     Ch4CorrArgs ca;
     ca.mu = g.rec_mu.p;
@@ -642,8 +673,10 @@ int run_records_t(const TrajParams &P, const double *d_ic, uint64_t n, uint64_t 
     ca.n_failed = g.rec_nfail.p;
     ca.fail_out = zimm ? g.zim_fail.p : nullptr;
     ca.len_out = zimm ? g.rec_len.p : nullptr;
+    kt_begin();
     ch4_corr_kernel<PHYS><<<(unsigned)((nc + 255) / 256), 256, 0, g.st>>>(P, ca);
     CK(cudaGetLastError());
+    kt_end(HH_KT_CH4_CORR);
     g_launches += 5;
     if (zimm) {
       ZimmArgs za;
@@ -850,6 +883,7 @@ int run_trajectories(const hh_calc_params *p, const double *d_ic, uint64_t n, ui
 // launches the M0 kernel of the bound system over `grid` blocks; allocates nothing
 int launch_m0(const M0Args &a, int grid, bool mixed, double *partials) {
   const int block = 256;
+  kt_begin();
   if (g.sys == SYS_HEAR) {
     if (mixed) m0_kernel<SYS_HEAR, float, true><<<grid, block, 0, g.st>>>(a, g.d_tab, nullptr, partials);
     else m0_kernel<SYS_HEAR, double, false><<<grid, block, 0, g.st>>>(a, g.d_tab, nullptr, partials);
@@ -873,12 +907,14 @@ int launch_m0(const M0Args &a, int grid, bool mixed, double *partials) {
           a, g.d_tab, nullptr, partials);
   }
   CK(cudaGetLastError());
+  kt_end(HH_KT_MOMENT);
   return HH_OK;
 }
 
 // the second-moment kernels (FP64)
 int launch_m2(const M0Args &a, int grid, double *partials) {
   const int block = 256;
+  kt_begin();
   if (g.sys == SYS_HEAR) {
     m0_kernel<SYS_HEAR, double, false, 2><<<grid, block, 0, g.st>>>(a, g.d_tab, nullptr, partials);
   } else if (g.sys == SYS_N2AR) {
@@ -891,6 +927,7 @@ int launch_m2(const M0Args &a, int grid, double *partials) {
         a, g.d_tab, nullptr, partials);
   }
   CK(cudaGetLastError());
+  kt_end(HH_KT_MOMENT);
   return HH_OK;
 }
 
@@ -912,8 +949,10 @@ constexpr int NOALLOC_MAX_DEVICES = 64;
 double *g_m0_noalloc_ptr[NOALLOC_MAX_DEVICES] = {};  // device address per device, set on first use
 
 // Device address of the scratch on the current device `dev`.  The first call
-// per device asks the runtime for it; with lazy module loading that is also
-// when the driver places the array in device memory.
+// per device after the library is brought up asks the runtime for it; bringing
+// the library up (hh_cuda_init on a fresh context) and hh_cuda_shutdown forget the
+// cached addresses, because a context torn down and created again may place the
+// array elsewhere.
 int m0_noalloc_scratch(int dev, double **out) {
   if (dev < 0 || dev >= NOALLOC_MAX_DEVICES) return HH_E_INVALID_ARGUMENT;
   if (!g_m0_noalloc_ptr[dev]) {
@@ -923,6 +962,10 @@ int m0_noalloc_scratch(int dev, double **out) {
   }
   *out = g_m0_noalloc_ptr[dev];
   return HH_OK;
+}
+
+void m0_noalloc_forget() {
+  for (auto &ptr : g_m0_noalloc_ptr) ptr = nullptr;
 }
 
 }  // namespace
@@ -976,6 +1019,7 @@ int hh_cuda_init(int device, const hh_system_desc *sys) {
   if (g.init && g.device != device) hh_cuda_shutdown();
   CK(cudaSetDevice(device));
   if (!g.init) {
+    m0_noalloc_forget();
     CK(cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking));
     CK(cudaStreamCreateWithFlags(&g.st2, cudaStreamNonBlocking));
     CK(cudaEventCreateWithFlags(&g.ev_sampled, cudaEventDisableTiming));
@@ -1028,6 +1072,8 @@ int hh_cuda_init(int device, const hh_system_desc *sys) {
     CK(cudaMemcpy(g.d_ch4_y2, f.by2.data(), 4 * B, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(g.d_ch4_meta, f.bmeta.data(), B * sizeof(unsigned int), cudaMemcpyHostToDevice));
     g.ch4_B = f.n_batch;
+    g.ch4_groups = 0;
+    for (size_t b = 0; b < B; ++b) g.ch4_groups += (f.bmeta[b] & 8u) ? 1 : 0;
   }
   g.sys = (sid == HH_SYSTEM_HE_AR)    ? SYS_HEAR
           : (sid == HH_SYSTEM_N2_AR)  ? SYS_N2AR
@@ -1423,70 +1469,30 @@ int hh_cuda_correlation_ic(const hh_calc_params *p, const double *qp0, uint64_t 
   return HH_OK;
 }
 
-int hh_cuda_m0(const hh_calc_params *p, const double *T, int nT, uint64_t n_samples,
-               uint64_t seed, int precision_mode, double *m, double *err) {
+int hh_cuda_moment_sums(const hh_calc_params *p, const double *T, int nT, uint64_t n_samples,
+                        uint64_t sample_offset, uint64_t seed, int moment, int precision_mode,
+                        double *sum_w, double *sum_w2) {
   if (!g.init) return HH_E_NOT_INITIALIZED;
   if (g.sys == SYS_CH4CO2) return HH_E_UNSUPPORTED_SYSTEM;  // no CH4-CO2 moment integrand
-  if (!p || !T || nT < 1 || !m || n_samples == 0) return HH_E_INVALID_ARGUMENT;
+  if (!p || !T || nT < 1 || !sum_w || n_samples == 0) return HH_E_INVALID_ARGUMENT;
+  if (moment != 0 && moment != 2) return HH_E_INVALID_ARGUMENT;
   if (!(p->sampler_Rmin > 0) || !(p->sampler_Rmax > p->sampler_Rmin)) return HH_E_INVALID_ARGUMENT;
   if (p->pair_state < 1 || p->pair_state > 3) return HH_E_INVALID_ARGUMENT;
   if (precision_mode != HH_PRECISION_FP64 && precision_mode != HH_PRECISION_MIXED)
     return HH_E_INVALID_ARGUMENT;
+  if (moment == 2 && precision_mode != HH_PRECISION_FP64) return HH_E_INVALID_ARGUMENT;
+  if (sample_offset > UINT64_MAX - n_samples) return HH_E_INVALID_ARGUMENT;
   for (int t = 0; t < nT; ++t)
     if (!(T[t] > 0)) return HH_E_INVALID_ARGUMENT;
   CK(cudaSetDevice(g.device));
   const int grid = g.num_sms * 4;
   CK(g.m0_partials.ensure((size_t)grid * M0_MAXT * 2));
   CK(g.m0_out.ensure(M0_MAXT * 2));
-  const double scale = HH_ZEROCOEFF * 4.0 * HH_PI * (p->sampler_Rmax - p->sampler_Rmin);
   for (int t0 = 0; t0 < nT; t0 += M0_MAXT) {
     M0Args a;
     memset(&a, 0, sizeof a);
     a.sys = g.sys;
-    a.Rmin = p->sampler_Rmin;
-    a.Rmax = p->sampler_Rmax;
-    a.pair_state = p->pair_state;
-    a.nT = std::min(M0_MAXT, nT - t0);
-    for (int t = 0; t < a.nT; ++t) a.invkT[t] = HH_HKT / T[t0 + t];
-    a.n_samples = n_samples;
-    a.offset = 0;
-    a.seed = seed;
-    int rc = launch_m0(a, grid, precision_mode == HH_PRECISION_MIXED, g.m0_partials.p);
-    if (rc) return rc;
-    m0_finalize_kernel<<<1, 32, 0, g.st>>>(g.m0_partials.p, grid, g.m0_out.p);
-    CK(cudaGetLastError());
-    double out[M0_MAXT * 2];
-    CK(cudaMemcpyAsync(out, g.m0_out.p, sizeof out, cudaMemcpyDeviceToHost, g.st));
-    CK(cudaStreamSynchronize(g.st));
-    for (int t = 0; t < a.nT; ++t) {
-      double mean = out[2 * t] / double(n_samples);
-      double var = out[2 * t + 1] / double(n_samples) - mean * mean;
-      m[t0 + t] = scale * mean;
-      if (err) err[t0 + t] = scale * sqrt(std::max(var, 0.0) / double(n_samples));
-    }
-  }
-  return HH_OK;
-}
-
-int hh_cuda_m2(const hh_calc_params *p, const double *T, int nT, uint64_t n_samples, uint64_t seed,
-               double *m, double *err) {
-  if (!g.init) return HH_E_NOT_INITIALIZED;
-  if (g.sys == SYS_CH4CO2) return HH_E_UNSUPPORTED_SYSTEM;  // no CH4-CO2 moment integrand
-  if (!p || !T || nT < 1 || !m || n_samples == 0) return HH_E_INVALID_ARGUMENT;
-  if (!(p->sampler_Rmin > 0) || !(p->sampler_Rmax > p->sampler_Rmin)) return HH_E_INVALID_ARGUMENT;
-  if (p->pair_state < 1 || p->pair_state > 3) return HH_E_INVALID_ARGUMENT;
-  for (int t = 0; t < nT; ++t)
-    if (!(T[t] > 0)) return HH_E_INVALID_ARGUMENT;
-  CK(cudaSetDevice(g.device));
-  const int grid = g.num_sms * 4;
-  CK(g.m0_partials.ensure((size_t)grid * M0_MAXT * 2));
-  CK(g.m0_out.ensure(M0_MAXT * 2));
-  const double scale = HH_SECONDCOEFF * 4.0 * HH_PI * (p->sampler_Rmax - p->sampler_Rmin);
-  for (int t0 = 0; t0 < nT; t0 += M0_MAXT) {
-    M0Args a;
-    memset(&a, 0, sizeof a);
-    a.sys = g.sys;
-    a.moment = 2;
+    a.moment = moment;
     a.inv_mu = 1.0 / g.mu;
     a.inv_II = g.sys == SYS_HEAR ? 0.0 : 1.0 / g.II;
     a.Rmin = p->sampler_Rmin;
@@ -1495,9 +1501,10 @@ int hh_cuda_m2(const hh_calc_params *p, const double *T, int nT, uint64_t n_samp
     a.nT = std::min(M0_MAXT, nT - t0);
     for (int t = 0; t < a.nT; ++t) a.invkT[t] = HH_HKT / T[t0 + t];
     a.n_samples = n_samples;
-    a.offset = 0;
+    a.offset = sample_offset;
     a.seed = seed;
-    int rc = launch_m2(a, grid, g.m0_partials.p);
+    int rc = (moment == 2) ? launch_m2(a, grid, g.m0_partials.p)
+                           : launch_m0(a, grid, precision_mode == HH_PRECISION_MIXED, g.m0_partials.p);
     if (rc) return rc;
     m0_finalize_kernel<<<1, 32, 0, g.st>>>(g.m0_partials.p, grid, g.m0_out.p);
     CK(cudaGetLastError());
@@ -1505,12 +1512,45 @@ int hh_cuda_m2(const hh_calc_params *p, const double *T, int nT, uint64_t n_samp
     CK(cudaMemcpyAsync(out, g.m0_out.p, sizeof out, cudaMemcpyDeviceToHost, g.st));
     CK(cudaStreamSynchronize(g.st));
     for (int t = 0; t < a.nT; ++t) {
-      double mean = out[2 * t] / double(n_samples);
-      double var = out[2 * t + 1] / double(n_samples) - mean * mean;
-      m[t0 + t] = scale * mean;
-      if (err) err[t0 + t] = scale * sqrt(std::max(var, 0.0) / double(n_samples));
+      sum_w[t0 + t] = out[2 * t];
+      if (sum_w2) sum_w2[t0 + t] = out[2 * t + 1];
     }
   }
+  return HH_OK;
+}
+
+// moment m[t] = scale <w> and its one-sigma error from the sums over n samples
+static void moment_from_sums(const double *sw, const double *sw2, int nT, uint64_t n, double scale, double *m,
+                             double *err) {
+  for (int t = 0; t < nT; ++t) {
+    const double mean = sw[t] / double(n);
+    const double var = sw2[t] / double(n) - mean * mean;
+    m[t] = scale * mean;
+    if (err) err[t] = scale * sqrt(std::max(var, 0.0) / double(n));
+  }
+}
+
+int hh_cuda_m0(const hh_calc_params *p, const double *T, int nT, uint64_t n_samples,
+               uint64_t seed, int precision_mode, double *m, double *err) {
+  if (!g.init) return HH_E_NOT_INITIALIZED;
+  if (!m || nT < 1) return HH_E_INVALID_ARGUMENT;
+  std::vector<double> sw(nT), sw2(nT);
+  int rc = hh_cuda_moment_sums(p, T, nT, n_samples, 0, seed, 0, precision_mode, sw.data(), sw2.data());
+  if (rc) return rc;
+  const double scale = HH_ZEROCOEFF * 4.0 * HH_PI * (p->sampler_Rmax - p->sampler_Rmin);
+  moment_from_sums(sw.data(), sw2.data(), nT, n_samples, scale, m, err);
+  return HH_OK;
+}
+
+int hh_cuda_m2(const hh_calc_params *p, const double *T, int nT, uint64_t n_samples, uint64_t seed,
+               double *m, double *err) {
+  if (!g.init) return HH_E_NOT_INITIALIZED;
+  if (!m || nT < 1) return HH_E_INVALID_ARGUMENT;
+  std::vector<double> sw(nT), sw2(nT);
+  int rc = hh_cuda_moment_sums(p, T, nT, n_samples, 0, seed, 2, HH_PRECISION_FP64, sw.data(), sw2.data());
+  if (rc) return rc;
+  const double scale = HH_SECONDCOEFF * 4.0 * HH_PI * (p->sampler_Rmax - p->sampler_Rmin);
+  moment_from_sums(sw.data(), sw2.data(), nT, n_samples, scale, m, err);
   return HH_OK;
 }
 
@@ -1651,6 +1691,24 @@ int hh_cuda_debug_inject(int traj, int dir, int k, int status) {
   g_inject_item = 2 * traj + dir;
   g_inject_k = k;
   g_inject_status = status;
+  return HH_OK;
+}
+
+int hh_cuda_debug_ch4co2_fold(int *n_batch, int *n_groups) {
+  if (!g.init || !g.d_ch4_cd) return HH_E_NOT_INITIALIZED;
+  if (n_batch) *n_batch = g.ch4_B;
+  if (n_groups) *n_groups = g.ch4_groups;
+  return HH_OK;
+}
+
+int hh_cuda_debug_kernel_ms(int enable, double *ms, uint64_t *launches, int n) {
+  if (n < 0) return HH_E_INVALID_ARGUMENT;
+  for (int i = 0; i < std::min(n, (int)HH_KT_COUNT); ++i) {
+    if (ms) ms[i] = g_kt.ms[i];
+    if (launches) launches[i] = g_kt.n[i];
+  }
+  g_kt = KernelTimer();
+  g_kt.on = enable != 0;
   return HH_OK;
 }
 
@@ -1811,6 +1869,7 @@ void hh_cuda_shutdown(void) {
   if (g.ev_sampled) cudaEventDestroy(g.ev_sampled);
   if (g.ev_pregen) cudaEventDestroy(g.ev_pregen);
   g = Ctx();
+  m0_noalloc_forget();
 }
 
 }  // extern "C"

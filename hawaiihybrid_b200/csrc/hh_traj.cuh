@@ -426,6 +426,30 @@ __device__ __forceinline__ void solution_point(const STG (&K)[16][N], const doub
   }
 }
 
+// scaled error estimates of component i (column i of K) in FP64: the 5th- and
+// 3rd-order estimates sum_j e_j K_j over the tolerance scale atol + max(|y|,
+// |y_new|) rtol.  FP32 stages: the estimate cannot resolve errors below the
+// rounding noise of the stage derivatives, so that noise widens the scale.
+template <typename STG, int NK>
+__device__ __forceinline__ void err_terms(const STG (&K)[16][NK], int i, double y, double y_new, double h,
+                                          const TrajParams &P, double &q5, double &q3) {
+  double sc = P.atol + fmax(fabs(y), fabs(y_new)) * P.rtol;
+  double a5 = 0.0, a3 = 0.0, m5 = 0.0;
+#pragma unroll
+  for (int j = 0; j < 13; ++j) {
+    if (hh_dop853_e5[j] != 0.0) {
+      const double t = hh_dop853_e5[j] * double(K[j][i]);
+      a5 += t;
+      if (sizeof(STG) == 4) m5 += fabs(t);
+    }
+    if (hh_dop853_e3[j] != 0.0) a3 += hh_dop853_e3[j] * double(K[j][i]);
+  }
+  if (sizeof(STG) == 4) sc += fabs(h) * P.noise_floor * m5;
+  const double isc = 1.0 / sc;
+  q5 = a5 * isc;
+  q3 = a3 * isc;
+}
+
 // stages 1..12 of one step attempt from (y, K[0] = f(y)); y_new is the 8th-order
 // solution and K[12] = f(y_new); returns the error norm
 template <class Sys, typename STG>
@@ -448,30 +472,18 @@ __device__ __forceinline__ double step_attempt(const Sys &sys, const TrajParams 
 #undef HH_STAGE
   solution_point<N, STG>(K, y, h, y_new);
   sys.rhs(y_new, K[12]);
-  // error norm in the stage precision (FP32 stages have no FP64 error to resolve)
-  STG e5 = STG(0), e3 = STG(0);
+  // error control in FP64 on both paths: the 5th- and 3rd-order estimates are
+  // FP64 sums of the stage derivatives, scaled and normed in FP64
+  double e5 = 0.0, e3 = 0.0;
 #pragma unroll
   for (int i = 0; i < N; ++i) {
-    STG sc = STG(P.atol) + STG(fmax(fabs(y[i]), fabs(y_new[i]))) * STG(P.rtol);
-    STG a5 = STG(0), a3 = STG(0), m5 = STG(0);
-#pragma unroll
-    for (int j = 0; j < 13; ++j) {
-      if (hh_dop853_e5[j] != 0.0) {
-        a5 += STG(hh_dop853_e5[j]) * K[j][i];
-        if (sizeof(STG) == 4) m5 += fabs(STG(hh_dop853_e5[j]) * K[j][i]);
-      }
-      if (hh_dop853_e3[j] != 0.0) a3 += STG(hh_dop853_e3[j]) * K[j][i];
-    }
-    // FP32 stages: the estimate cannot resolve errors below the rounding noise of
-    // the stage derivatives, so that noise widens the tolerance
-    if (sizeof(STG) == 4) sc += STG(fabs(h)) * STG(P.noise_floor) * m5;
-    const STG isc = STG(1) / sc;
-    const STG q5 = a5 * isc, q3 = a3 * isc;
+    double q5, q3;
+    err_terms<STG>(K, i, y[i], y_new[i], h, P, q5, q3);
     e5 += q5 * q5;
     e3 += q3 * q3;
   }
-  if (e5 == STG(0) && e3 == STG(0)) return 0.0;
-  return fabs(h) * double(e5) / sqrt(double(e5 + STG(0.01) * e3) * N);
+  if (e5 == 0.0 && e3 == 0.0) return 0.0;
+  return fabs(h) * e5 / sqrt((e5 + 0.01 * e3) * N);
 }
 
 // err^(-1/8) for the step controller
@@ -578,28 +590,17 @@ __device__ __forceinline__ double step_attempt_cp(const Sys &sys, const TrajPara
     sys.rhs(yn, f);
     K[12][0] = pick_component<N>(f, c);
   }
-  STG sc = STG(P.atol) + STG(fmax(fabs(y), fabs(y_new))) * STG(P.rtol);
-  STG a5 = STG(0), a3 = STG(0), m5 = STG(0);
-#pragma unroll
-  for (int j = 0; j < 13; ++j) {
-    if (hh_dop853_e5[j] != 0.0) {
-      a5 += STG(hh_dop853_e5[j]) * K[j][0];
-      if (sizeof(STG) == 4) m5 += fabs(STG(hh_dop853_e5[j]) * K[j][0]);
-    }
-    if (hh_dop853_e3[j] != 0.0) a3 += STG(hh_dop853_e3[j]) * K[j][0];
-  }
-  if (sizeof(STG) == 4) sc += STG(fabs(h)) * STG(P.noise_floor) * m5;
-  const STG isc = STG(1) / sc;
-  const STG q5 = a5 * isc, q3 = a3 * isc;
-  STG e5 = STG(0), e3 = STG(0);
+  double q5, q3;
+  err_terms<STG>(K, 0, y, y_new, h, P, q5, q3);
+  double e5 = 0.0, e3 = 0.0;
 #pragma unroll
   for (int i = 0; i < N; ++i) {
-    const STG v5 = __shfl_sync(0xffffffffu, q5, i), v3 = __shfl_sync(0xffffffffu, q3, i);
+    const double v5 = __shfl_sync(0xffffffffu, q5, i), v3 = __shfl_sync(0xffffffffu, q3, i);
     e5 += v5 * v5;
     e3 += v3 * v3;
   }
-  if (e5 == STG(0) && e3 == STG(0)) return 0.0;
-  return fabs(h) * double(e5) / sqrt(double(e5 + STG(0.01) * e3) * N);
+  if (e5 == 0.0 && e3 == 0.0) return 0.0;
+  return fabs(h) * e5 / sqrt((e5 + 0.01 * e3) * N);
 }
 
 // stages 13..15 and this lane's dense-output coefficients F[0..6]

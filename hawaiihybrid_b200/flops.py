@@ -6,7 +6,7 @@ formulas in csrc/hh_physics.cuh and csrc/hh_traj.cuh; the event counts (RHS
 evaluations, steps, dense-output steps, samples) are measured by the kernels.
 For the mixed path the work is split into the part done in FP32 (surfaces,
 stage sums, dense-output increments) and the part done in FP64 (state
-updates, tolerances, kinematic terms).
+updates, error estimates and step control, kinematic terms).
 """
 from __future__ import annotations
 
@@ -25,15 +25,38 @@ SYSTEMS = {
     # CO2-Ar: |r|, |u|, x, Legendre P_l and P_l' to l = 10 (63), 6 radial cubics
     # with derivatives (72), 2 sums (24), force and torque (36), kinematics (15)
     "co2ar": dict(n=12, nq=6, rhs=234, rhs_fp64_kin=15, dip=196),
+    # N2-Ar: two pair functions y(d) (exp, quintic switch, 25 each), the 17 PIPs and
+    # their Jacobian over the monomial table (320), scaler (34), 32 hidden units x
+    # (17 FMA forward + SiLU' with exp and divide (7) + 17 FMA backward) = 2400,
+    # chain to d1, d2 (73), Cartesian forces and torques (70), kinematics (15).
+    # Dipole: mixed path = FP32 Chebyshev cell (atan2, cell index, 2 x 10 x 10 FMA,
+    # basis recurrences, rotation: 490); FP64 path = the folded network (2 ranges x
+    # 34 x 40 FMA, 40 SiLU differences with expm1 and divide, outputs: 6500)
+    "n2ar": dict(n=12, nq=6, rhs=2960, rhs_fp64_kin=15, dip=490, dip_fp64=6500),
 }
 
+# Monte Carlo moment integrand per sample (hh_m0.cuh), surface-precision part and
+# FP64 part (the 16 compensated sums of w and sums of w^2: 6 FP64 operations per
+# temperature).  CO2-Ar: angle transforms (30), surface value and gradient rows
+# (180), dipole sums (170), |mu|^2 (5), per temperature H, exp, weight (5 each).
+M0_PER_SAMPLE = {"co2ar": dict(phys=30 + 180 + 170 + 5, per_T=5, per_T_fp64=6)}
 
-def per_event(system: str) -> dict:
-    s = SYSTEMS[system]
+# CH4-CO2 batched dipole (ch4_dipole_kernel) per record: 4 FMA per (padded) entry
+# of the coefficient stream (the per-power sums), Horner and Y1 product per group
+# (5 per group end, about one per 4 entries), record geometry (quaternion matrix,
+# two frame vectors, Y2 table of 91 values: about 600)
+def ch4_dipole_flops(n_entries_padded: int, n_groups: int) -> int:
+    return 8 * n_entries_padded + 10 * n_groups + 600
+
+
+def per_event(system: str, mixed: bool = True) -> dict:
+    s = dict(SYSTEMS[system])
+    if not mixed and "dip_fp64" in s:
+        s["dip"] = s["dip_fp64"]
     n, nq = s["n"], s["nq"]
     comb_sum = sum(2 * k for k in _STAGE_NNZ) * n + 2 * _B_NNZ * n          # stage sums
     comb_upd = 2 * (len(_STAGE_NNZ) + 1) * n                                 # y + h*acc
-    err_sum = 2 * (_E5_NNZ + _E3_NNZ) * n
+    err_sum = 2 * (_E5_NNZ + _E3_NNZ) * n                                  # error estimates (FP64)
     err_fp64 = 8 * n + 20                                                    # scales, norm, controller
     dense_stage_sum = sum(2 * k for k in _EXTRA_NNZ) * n
     dense_stage_upd = 2 * len(_EXTRA_NNZ) * n
@@ -42,15 +65,25 @@ def per_event(system: str) -> dict:
     sample_fp64 = nq + 8                                                     # state add, |r|, Rcut test
     return dict(
         rhs=s["rhs"], rhs_fp64_kin=s["rhs_fp64_kin"], dip=s["dip"],
-        step_sum=comb_sum + err_sum, step_fp64=comb_upd + err_fp64,
+        step_sum=comb_sum, step_fp64=comb_upd + err_sum + err_fp64,
         dense_sum=dense_stage_sum + dense_rows, dense_fp64=dense_stage_upd,
         sample=sample_interp + s["dip"] + 6, sample_fp64=sample_fp64,
     )
 
 
+def m0_work(system: str, n_samples: int, nT: int, mixed: bool) -> dict:
+    """FP32 and FP64 flops of one M0 call over n_samples samples and nT temperatures."""
+    c = M0_PER_SAMPLE[system]
+    phys = n_samples * (c["phys"] + nT * c["per_T"])
+    f64 = n_samples * nT * c["per_T_fp64"]
+    if mixed:
+        return {"fp32": float(phys), "fp64": float(f64)}
+    return {"fp32": 0.0, "fp64": float(phys + f64)}
+
+
 def work(system: str, stats: dict, mixed: bool) -> dict:
     """FP32 and FP64 flops of one call from its measured event counts."""
-    e = per_event(system)
+    e = per_event(system, mixed)
     attempts = stats["n_steps"] + stats["n_rejected_steps"]
     n_rhs, n_dense, n_samp = stats["n_rhs"], stats["n_dense"], stats["n_samples"]
     phys = n_rhs * (e["rhs"] - e["rhs_fp64_kin"]) + n_samp * e["sample"] + attempts * e["step_sum"] \

@@ -28,6 +28,7 @@ Hartree = 4.3597447222071e-18
 HTOCM = 2.1947463136320e5
 HkT = Hartree / Boltzmann
 ZeroCoeff = 0.00361479637 / (4.0 * math.pi)
+SecondCoeff = 13856114.29344114
 RAMTOAMU = 1822.888485332
 m_He = 4.00260325413 * RAMTOAMU
 m_Ar = 39.9623831237 * RAMTOAMU
@@ -426,6 +427,34 @@ def calculate_m2(ms: MoleculeSystem, params: CalcParams, temperatures: Sequence[
     pc = params.to_c()
     check(L.hh_cuda_m2(C.byref(pc), T, T.size, n_samples, seed, m, e))
     return m, e
+
+
+def moment_sums(ms: MoleculeSystem, params: CalcParams, temperatures: Sequence[float], n_samples: int,
+                sample_offset: int = 0, seed: int = 1, moment: int = 0,
+                precision: int = PRECISION_FP64) -> tuple[np.ndarray, np.ndarray]:
+    """Per-temperature sums (sum w, sum w^2) of the M0 (moment 0) or M2 (moment 2) integrand
+    over the Philox samples [sample_offset, sample_offset + n_samples): one rank's share of
+    mpi_calculate_M0 / mpi_calculate_M2 (src/hawaii.c:1620-1738, 1740-1856)."""
+    L = _bind(ms)
+    T = np.ascontiguousarray(temperatures, dtype=np.float64)
+    sw = np.empty(T.size)
+    sw2 = np.empty(T.size)
+    pc = params.to_c()
+    check(L.hh_cuda_moment_sums(C.byref(pc), T, T.size, n_samples, sample_offset, seed, moment, precision, sw, sw2))
+    return sw, sw2
+
+
+def moment_scale(params: CalcParams, moment: int = 0) -> float:
+    """M = moment_scale * <w>: ZeroCoeff (SecondCoeff) * 4 pi (Rmax - Rmin)."""
+    coeff = ZeroCoeff if moment == 0 else SecondCoeff
+    return coeff * 4.0 * math.pi * (params.sampler_Rmax - params.sampler_Rmin)
+
+
+def moment_from_sums(sw: np.ndarray, sw2: np.ndarray, n_samples: int, scale: float) -> tuple[np.ndarray, np.ndarray]:
+    """(M, one-sigma error) from the integrand sums over n_samples samples."""
+    mean = np.asarray(sw) / n_samples
+    var = np.maximum(np.asarray(sw2) / n_samples - mean * mean, 0.0)
+    return scale * mean, scale * np.sqrt(var / n_samples)
 
 
 def analytic_full_partition_function_by_V(ms: MoleculeSystem, Temperature: float) -> float:

@@ -201,6 +201,19 @@ int hh_cuda_m0(const hh_calc_params *p, const double *T, int nT, uint64_t n_samp
 int hh_cuda_m2(const hh_calc_params *p, const double *T, int nT, uint64_t n_samples,
                uint64_t seed, double *m, double *err);
 
+/* Per-temperature sums of the moment integrand over the Philox samples
+ * [sample_offset, sample_offset + n_samples) of stream `seed`: sum_w[t] = sum of w,
+ * sum_w2[t] = sum of w^2 (may be NULL), moment 0 (M0, either precision) or 2 (M2,
+ * FP64).  This is the per-rank part of the reference's MPI moment integrals
+ * (mpi_calculate_M0 / mpi_calculate_M2, src/hawaii.c:1620-1738, 1740-1856: each rank
+ * integrates its own points, rank 0 sums the (m, q) pairs): ranks take disjoint
+ * counter ranges and the sums add, so M = scale * (sum over ranks of sum_w) / n_total
+ * with scale = ZeroCoeff (SecondCoeff) * 4 pi (Rmax - Rmin).  hh_cuda_m0 and
+ * hh_cuda_m2 are this call at offset 0 followed by that division. */
+int hh_cuda_moment_sums(const hh_calc_params *p, const double *T, int nT, uint64_t n_samples,
+                        uint64_t sample_offset, uint64_t seed, int moment, int precision_mode,
+                        double *sum_w, double *sum_w2);
+
 /* Allocation-free M0 (no counterpart in the reference).
  *
  * Same arguments, samples and results as hh_cuda_m0, but the call allocates no
@@ -215,10 +228,15 @@ int hh_cuda_m2(const hh_calc_params *p, const double *T, int nT, uint64_t n_samp
  *
  * Limits: nT <= HH_M0_NOALLOC_MAX_T, else HH_E_SCRATCH_LIMIT and nothing runs.
  * hh_cuda_init must have been called (it allocates the surface tables once).
- * The first call on a device looks up the array's device address; with lazy
- * module loading that is when the driver places the array, so make that first
- * call during set-up, before any stream capture.  There is one array per device:
- * calls whose GPU work overlaps (e.g. from two host threads) race on it. */
+ * The array is placed in device memory when the library's module loads, at the
+ * latest with the first kernel launch after hh_cuda_init.  The first call after
+ * the library is brought up (the first hh_cuda_init, or the first one after
+ * hh_cuda_shutdown) looks up the array's device address (cudaGetSymbolAddress),
+ * and that lookup must not fall inside a stream capture, so make that first call
+ * during set-up.  hh_cuda_shutdown forgets the address, so a context torn down
+ * (cudaDeviceReset) after hh_cuda_shutdown and brought up again by hh_cuda_init
+ * never reuses a stale one.  There is one array per device: calls whose GPU work
+ * overlaps (e.g. from two host threads) race on it. */
 #define HH_E_SCRATCH_LIMIT (-9)
 #define HH_M0_NOALLOC_MAX_T 256
 #define HH_M0_NOALLOC_SCRATCH_BYTES (8 * (1024 * 16 * 2 + 2 * HH_M0_NOALLOC_MAX_T))
@@ -253,6 +271,26 @@ int hh_cuda_debug_n2ar_dipole(int precision, const double *R, const double *T, u
  * CH4-CO2 dipole kernel's tuner picked for the FP64 and the mixed path on the first
  * record-path call of this context (0 before that call). */
 int hh_cuda_debug_tuning(int *ch4_dip_s_fp64, int *ch4_dip_s_mixed);
+
+/* Diagnostic (no counterpart in the reference): device time per kernel class.
+ * While switched on, every kernel of the classes below is bracketed by CUDA events
+ * and waited for (launches of a call then run one after another, so switch it on
+ * for a measurement call, not for a timed one).  Each call copies out the
+ * milliseconds and launches accumulated since the previous call (n entries at
+ * most, HH_KT_COUNT in all), resets them and sets the timer to `enable`. */
+#define HH_KT_TRAJ_BULK 0   /* traj_kernel, bulk launch */
+#define HH_KT_TRAJ_SOLO 1   /* traj_kernel, solo launch (last open items, one per warp) */
+#define HH_KT_CH4_DIPOLE 2  /* CH4-CO2 batched dipole kernel */
+#define HH_KT_CH4_SORT 3    /* CH4-CO2 record sort (count, scan, scatter) */
+#define HH_KT_CH4_CORR 4    /* CH4-CO2 per-sample tests and C(t) sums */
+#define HH_KT_MOMENT 5      /* M0 / M2 kernel */
+#define HH_KT_COUNT 6
+int hh_cuda_debug_kernel_ms(int enable, double *ms, uint64_t *launches, int n);
+/* Diagnostic (no counterpart in the reference): shape of the CH4-CO2 dipole's
+ * coefficient stream (batches of 4 entries per radial piece, and the (Y1,
+ * component, cos/sin) groups they form); HH_E_NOT_INITIALIZED before a CH4-CO2
+ * hh_cuda_init. */
+int hh_cuda_debug_ch4co2_fold(int *n_batch, int *n_groups);
 
 /* Diagnostic (no counterpart in the reference): measured FMA throughput of the
  * CUDA cores in TFLOP/s (precision HH_PRECISION_FP64 or, for FP32,
