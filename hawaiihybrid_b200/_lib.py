@@ -45,7 +45,7 @@ EXPORTS = (
     "hh_cuda_mt_stream", "hh_cuda_debug_inject", "hh_cuda_debug_item_trace", "hh_cuda_fma_peak",
     "hh_cuda_shutdown", "hh_cuda_m0_noalloc", "hh_cuda_correlation_array", "hh_cuda_correlation_temperatures",
     "hh_cuda_prmu", "hh_cuda_debug_n2ar_dipole", "hh_cuda_m2", "hh_cuda_debug_tuning",
-    "hh_cuda_debug_kernel_ms", "hh_cuda_debug_ch4co2_fold", "hh_cuda_moment_sums",
+    "hh_cuda_debug_kernel_ms", "hh_cuda_debug_ch4co2_fold", "hh_cuda_moment_sums", "hh_cuda_debug_traj_tuning",
 )
 # kernel classes of hh_cuda_debug_kernel_ms
 HH_KT_NAMES = ("traj_bulk", "traj_solo", "ch4_dipole", "ch4_sort", "ch4_corr", "moment")
@@ -141,6 +141,7 @@ def load(path: str | None = None):
     L.hh_cuda_debug_kernel_ms.argtypes = [C.c_int, _dp, np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS"),
                                           C.c_int]
     L.hh_cuda_debug_ch4co2_fold.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.hh_cuda_debug_traj_tuning.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.hh_cuda_shutdown.restype = None
     for name in EXPORTS:
         if name not in ("hh_cuda_strerror", "hh_cuda_shutdown"):
@@ -169,3 +170,12 @@ def ch4co2_fold_shape() -> tuple[int, int]:
     nb, ng = C.c_int(0), C.c_int(0)
     check(load().hh_cuda_debug_ch4co2_fold(C.byref(nb), C.byref(ng)))
     return nb.value, ng.value
+
+
+def traj_tuning(precision: int, set_warps: int = 0, set_handoff_div: int = 0) -> tuple[int, int]:
+    """(warps per block, hand-off divisor) of the trajectory launch for the bound system and
+    precision (0, 0 before the autotuner ran); set_* > 0 fixes, < 0 forgets the pick."""
+    w, d = C.c_int(0), C.c_int(0)
+    check(load().hh_cuda_debug_traj_tuning(int(precision), int(set_warps), int(set_handoff_div),
+                                           C.byref(w), C.byref(d)))
+    return w.value, d.value

@@ -74,6 +74,11 @@ template <typename T> struct DevBuf {
   }
 };
 
+struct TrajTune {
+  int warps;        // bulk kernel warps per block
+  int handoff_div;  // hand-off when at most (solo warp slots) / handoff_div items are open
+};
+
 struct Ctx {
   bool init = false;
   int device = -1;
@@ -104,6 +109,9 @@ struct Ctx {
   int ch4_B = 0;
   int ch4_groups = 0;  // (Y1, component, cos/sin) groups of the batch stream
   int ch4_dip_s[2] = {0, 0};  // records per lane of the dipole kernel [FP64, mixed]; 0: not tuned yet
+  // trajectory launch picks per [system][FP64, mixed] (warps == 0: not tuned yet)
+  TrajTune traj_tune[5][2] = {};
+  DevBuf<double> tune_crln, tune_cnt;  // the autotuner's scratch C(t) and counters
   // MT19937 stream
   uint32_t *d_mt = nullptr;
   unsigned short *d_mt_jump_seg = nullptr, *d_mt_jump_coarse = nullptr;  // jump-ahead tables
@@ -371,51 +379,156 @@ int sample_into(const hh_calc_params *p, double T, uint64_t n, double *d_out, ui
   return HH_OK;
 }
 
-template <int SYS, typename PHYS, typename STG, bool COMP>
-int launch_traj(const TrajParams &P, const TrajIO &io, int *grid_out) {
-  auto kern = traj_kernel<SYS, PHYS, STG, COMP>;
-  size_t smem = traj_smem_bytes<SYS, PHYS, STG>();
+// One trajectory launch: the bulk kernel (WARPS warps per block) until at most
+// cap / handoff_div items are open, then the solo kernel for the rest, where cap is
+// the solo kernel's warp slots.  With ev_split, events ev[4] (start), ev[5] (after the
+// bulk kernel) and ev[7] (end) are recorded for the autotuner.
+template <int SYS, typename PHYS, typename STG, bool COMP, int WARPS>
+int launch_traj_w(const TrajParams &P, const TrajIO &io, int handoff_div, bool ev_split) {
+  auto kern = traj_kernel<SYS, PHYS, STG, COMP, false, WARPS>;
+  const size_t smem = traj_smem_bytes<SYS, PHYS, STG, WARPS>();
   if (smem > 48 * 1024) CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
-  constexpr int TRAJ_THREADS = traj_threads<PHYS>();
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, TRAJ_THREADS, smem));
+  constexpr int THREADS = 32 * WARPS;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, THREADS, smem));
   int grid = std::max(1, per_sm) * g.num_sms;
-  long long need = (io.n_items + TRAJ_THREADS - 1) / TRAJ_THREADS;
+  long long need = (io.n_items + THREADS - 1) / THREADS;
   if (need < grid) grid = (int)std::max(1LL, need);
-  {
-    // the last open items (and all items of a launch that small) run one per warp
-    // in the solo kernel, one state component per lane
-    auto solo = traj_kernel<SYS, PHYS, STG, COMP, true>;
-    if (smem > 48 * 1024) CK(cudaFuncSetAttribute(solo, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
-    int per_sm_solo = 0;
-    CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_solo, solo, TRAJ_THREADS, smem));
-    const int solo_grid = std::max(1, per_sm_solo) * g.num_sms;
-    const unsigned cap = (unsigned)solo_grid * (TRAJ_THREADS / 32);
-    constexpr int NS = SYS == SYS_HEAR ? 6 : SYS == SYS_CH4CO2 ? 19 : 12;
-    CK(g.handoff.ensure((size_t)cap * sizeof(HandoffState<NS, PHYS, STG>)));
-    CK(g.hcount.ensure(4));
-    CK(cudaMemsetAsync(g.hcount.p, 0, 4 * sizeof(unsigned int), g.st));
-    TrajIO io2 = io;
-    io2.handoff = g.handoff.p;
-    io2.n_handoff = g.hcount.p;
-    io2.solo_cursor = g.hcount.p + 1;
-    io2.done = g.hcount.p + 2;
-    io2.handoff_at = cap;
-    if ((unsigned)io.n_items > cap) {
-      kt_begin();
-      kern<<<grid, TRAJ_THREADS, smem, g.st>>>(P, io2, g.d_tab);
-      CK(cudaGetLastError());
-      kt_end(HH_KT_TRAJ_BULK);
-      g_launches += 1;
-    }
+  // the last open items (and all items of a launch that small) run one per warp
+  // in the solo kernel, one state component per lane
+  auto solo = traj_kernel<SYS, PHYS, STG, COMP, true>;
+  constexpr int SOLO_THREADS = traj_threads<PHYS>();
+  const size_t smem_solo = traj_smem_bytes<SYS, PHYS, STG>();
+  if (smem_solo > 48 * 1024)
+    CK(cudaFuncSetAttribute(solo, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem_solo));
+  int per_sm_solo = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm_solo, solo, SOLO_THREADS, smem_solo));
+  const int solo_grid = std::max(1, per_sm_solo) * g.num_sms;
+  const unsigned cap = (unsigned)solo_grid * (SOLO_THREADS / 32);
+  constexpr int NS = SYS == SYS_HEAR ? 6 : SYS == SYS_CH4CO2 ? 19 : 12;
+  CK(g.handoff.ensure((size_t)cap * sizeof(HandoffState<NS, PHYS, STG>)));
+  CK(g.hcount.ensure(4));
+  CK(cudaMemsetAsync(g.hcount.p, 0, 4 * sizeof(unsigned int), g.st));
+  TrajIO io2 = io;
+  io2.handoff = g.handoff.p;
+  io2.n_handoff = g.hcount.p;
+  io2.solo_cursor = g.hcount.p + 1;
+  io2.done = g.hcount.p + 2;
+  io2.handoff_at = std::max(1u, cap / (unsigned)std::max(1, handoff_div));
+  if (ev_split) CK(cudaEventRecord(g.ev[4], g.st));
+  if ((unsigned)io.n_items > cap) {
     kt_begin();
-    solo<<<solo_grid, TRAJ_THREADS, smem, g.st>>>(P, io2, g.d_tab);
+    kern<<<grid, THREADS, smem, g.st>>>(P, io2, g.d_tab);
     CK(cudaGetLastError());
-    kt_end(HH_KT_TRAJ_SOLO);
+    kt_end(HH_KT_TRAJ_BULK);
     g_launches += 1;
   }
-  if (grid_out) *grid_out = grid;
+  if (ev_split) CK(cudaEventRecord(g.ev[5], g.st));
+  kt_begin();
+  solo<<<solo_grid, SOLO_THREADS, smem_solo, g.st>>>(P, io2, g.d_tab);
+  CK(cudaGetLastError());
+  kt_end(HH_KT_TRAJ_SOLO);
+  g_launches += 1;
+  if (ev_split) CK(cudaEventRecord(g.ev[7], g.st));
   return HH_OK;
+}
+
+template <int SYS, typename PHYS, typename STG, bool COMP>
+int launch_traj_pick(const TrajParams &P, const TrajIO &io, int warps, int handoff_div, bool ev_split) {
+  if (warps == TRAJ_WARPS_CANDIDATES[0])
+    return launch_traj_w<SYS, PHYS, STG, COMP, TRAJ_WARPS_CANDIDATES[0]>(P, io, handoff_div, ev_split);
+  return launch_traj_w<SYS, PHYS, STG, COMP, TRAJ_WARPS_CANDIDATES[1]>(P, io, handoff_div, ev_split);
+}
+
+// Autotuner of the trajectory launch (first large plain-C(t) call per system and
+// precision): the bulk kernel's warps per block and the hand-off threshold (how many
+// open items are left to the solo kernel, i.e. when the launch switches from 32
+// trajectories per warp to one).  Timed on the launch's first items, into scratch
+// C(t) and counters, so the call's own results are untouched:
+//   1. each warps-per-block candidate with the full hand-off threshold: bulk kernel time;
+//   2. with the faster shape, thresholds cap / 2 and cap / 4 against cap: launch time.
+// HH_TRAJ_WARPS (4 or 8) and HH_TRAJ_HANDOFF_DIV (1, 2 or 4) fix a choice instead.
+constexpr int TRAJ_TUNE_MIN_ITEMS = 16384;  // smaller launches use the defaults, untuned
+constexpr int TRAJ_TUNE_ITEMS = 32768;      // items the timing runs integrate
+
+template <int SYS, typename PHYS, typename STG, bool COMP>
+int tune_traj(const TrajParams &P, const TrajIO &io, TrajTune *out) {
+  const char *ew = getenv("HH_TRAJ_WARPS");
+  const char *ed = getenv("HH_TRAJ_HANDOFF_DIV");
+  int fixed_w = ew ? atoi(ew) : 0, fixed_d = ed ? atoi(ed) : 0;
+  if (fixed_w != TRAJ_WARPS_CANDIDATES[0] && fixed_w != TRAJ_WARPS_CANDIDATES[1]) fixed_w = 0;
+  if (fixed_d != 1 && fixed_d != 2 && fixed_d != 4) fixed_d = 0;
+  const int n_s = std::min(io.n_items, TRAJ_TUNE_ITEMS);
+  const int nsl = std::max(1, io.n_sat);
+  CK(g.tune_crln.ensure((size_t)P.N * nsl));
+  CK(g.tune_cnt.ensure(16 + 2 * HH_ST_COUNT + 1));
+  TrajIO t = io;
+  t.n_items = n_s;
+  t.items = nullptr;
+  t.crln = g.tune_crln.p;
+  t.counters = reinterpret_cast<unsigned long long *>(g.tune_cnt.p);
+  t.status_hist = reinterpret_cast<unsigned int *>(g.tune_cnt.p + 8);
+  t.queue = reinterpret_cast<unsigned int *>(g.tune_cnt.p + 8 + HH_ST_COUNT);
+  t.fail_flag = nullptr;
+  t.fail_list = nullptr;
+  t.fail_count = nullptr;
+  t.traj_per_iter = LLONG_MAX / 4;  // every sampled item into the one scratch slice
+  t.item_trace = nullptr;
+  TrajParams Pt = P;
+  Pt.inject_item = -1;
+  auto run = [&](int w, int d, float *bulk_ms, float *all_ms) -> int {
+    CK(cudaMemsetAsync(g.tune_cnt.p, 0, (16 + 2 * HH_ST_COUNT + 1) * sizeof(double), g.st));
+    CK(cudaMemsetAsync(g.tune_crln.p, 0, (size_t)P.N * nsl * sizeof(double), g.st));
+    int rc = launch_traj_pick<SYS, PHYS, STG, COMP>(Pt, t, w, d, true);
+    if (rc) return rc;
+    CK(cudaEventSynchronize(g.ev[7]));
+    CK(cudaEventElapsedTime(bulk_ms, g.ev[4], g.ev[5]));
+    CK(cudaEventElapsedTime(all_ms, g.ev[4], g.ev[7]));
+    return HH_OK;
+  };
+  float bulk, all;
+  int w_best = fixed_w ? fixed_w : traj_warps<PHYS>();
+  if (!fixed_w) {
+    float best = 0.f;
+    for (int c = 0; c < 2; ++c) {
+      const int w = TRAJ_WARPS_CANDIDATES[c];
+      int rc = run(w, 1, &bulk, &all);
+      if (rc) return rc;
+      if (c == 0 || bulk < best) {
+        best = bulk;
+        w_best = w;
+      }
+    }
+  }
+  int d_best = fixed_d ? fixed_d : 1;
+  if (!fixed_d) {
+    float best = 0.f;
+    for (int d : {1, 2, 4}) {
+      int rc = run(w_best, d, &bulk, &all);
+      if (rc) return rc;
+      if (d == 1 || all < best) {
+        best = all;
+        d_best = d;
+      }
+    }
+  }
+  out->warps = w_best;
+  out->handoff_div = d_best;
+  return HH_OK;
+}
+
+template <int SYS, typename PHYS, typename STG, bool COMP>
+int launch_traj(const TrajParams &P, const TrajIO &io, int *grid_out) {
+  (void)grid_out;
+  TrajTune &tt = g.traj_tune[SYS][sizeof(PHYS) == 4 ? 1 : 0];
+  const bool plain = !io.records && !io.series;
+  if (tt.warps == 0 && plain && io.n_items >= TRAJ_TUNE_MIN_ITEMS) {
+    int rc = tune_traj<SYS, PHYS, STG, COMP>(P, io, &tt);
+    if (rc) return rc;
+  }
+  const int w = tt.warps ? tt.warps : traj_warps<PHYS>();
+  const int d = tt.handoff_div ? tt.handoff_div : 1;
+  return launch_traj_pick<SYS, PHYS, STG, COMP>(P, io, w, d, false);
 }
 
 int run_traj_dispatch(int precision, const TrajParams &P, const TrajIO &io) {
@@ -1694,6 +1807,26 @@ int hh_cuda_debug_inject(int traj, int dir, int k, int status) {
   return HH_OK;
 }
 
+int hh_cuda_debug_traj_tuning(int precision, int set_warps, int set_handoff_div, int *warps, int *handoff_div) {
+  if (!g.init) return HH_E_NOT_INITIALIZED;
+  if (precision != HH_PRECISION_FP64 && precision != HH_PRECISION_MIXED) return HH_E_INVALID_ARGUMENT;
+  TrajTune &tt = g.traj_tune[g.sys][precision == HH_PRECISION_MIXED ? 1 : 0];
+  if (set_warps < 0 || set_handoff_div < 0) {
+    tt.warps = tt.handoff_div = 0;
+  } else if (set_warps > 0 || set_handoff_div > 0) {
+    if (set_warps > 0 && set_warps != TRAJ_WARPS_CANDIDATES[0] && set_warps != TRAJ_WARPS_CANDIDATES[1])
+      return HH_E_INVALID_ARGUMENT;
+    if (set_handoff_div > 0 && set_handoff_div != 1 && set_handoff_div != 2 && set_handoff_div != 4)
+      return HH_E_INVALID_ARGUMENT;
+    const int dw = precision == HH_PRECISION_MIXED ? traj_warps<float>() : traj_warps<double>();
+    tt.warps = set_warps > 0 ? set_warps : (tt.warps ? tt.warps : dw);
+    tt.handoff_div = set_handoff_div > 0 ? set_handoff_div : (tt.handoff_div ? tt.handoff_div : 1);
+  }
+  if (warps) *warps = tt.warps;
+  if (handoff_div) *handoff_div = tt.handoff_div;
+  return HH_OK;
+}
+
 int hh_cuda_debug_ch4co2_fold(int *n_batch, int *n_groups) {
   if (!g.init || !g.d_ch4_cd) return HH_E_NOT_INITIALIZED;
   if (n_batch) *n_batch = g.ch4_B;
@@ -1843,6 +1976,8 @@ void hh_cuda_shutdown(void) {
   g.pm_sf.release();
   g.m0_partials.release();
   g.m0_out.release();
+  g.tune_crln.release();
+  g.tune_cnt.release();
   g.f_cf.release();
   g.f_nu.release();
   g.f_sf.release();

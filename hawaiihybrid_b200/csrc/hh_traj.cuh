@@ -1250,28 +1250,31 @@ __device__ __forceinline__ void load_words(void *dst, const void *src, size_t by
   for (size_t i = threadIdx.x; i < bytes / 8; i += blockDim.x) d[i] = s[i];
 }
 
-// block shape of traj_kernel, measured per precision path on the CO2-Ar
-// workload: both use every register (255), so 8 warps run per SM either way.
-// The FP64 kernels run 10 % faster as one block of 8 warps (one copy of the
-// surface tables per SM); the FP32-stage kernels are 1 % faster as two blocks of
-// 4.  With the solo hand-off and one pooled-sample job per lane, 4 and 8 warps per
-// block for both paths were within 1 % of each other on the CO2-Ar and N2-Ar
-// workloads.  TRAJ_MIN_BLOCKS is the blocks per SM the register allocation must allow.
+// block shape of traj_kernel.  Both precision paths use every register (255), so
+// 8 warps run per SM whatever the block shape; 4 and 8 warps per block differ in
+// the copies of the surface tables per SM and in how blocks drain at the end of a
+// launch.  The bulk kernel is compiled for both (TRAJ_WARPS_CANDIDATES) and the
+// library times them on the first large call per system and precision (the
+// autotuner in hh_api.cu); traj_warps is the default before that and the block
+// shape of the solo kernel.  TRAJ_MIN_BLOCKS is the blocks per SM the register
+// allocation must allow.
 template <typename PHYS> constexpr int traj_warps() { return sizeof(PHYS) == 8 ? 8 : 4; }
 template <typename PHYS> constexpr int traj_threads() { return 32 * traj_warps<PHYS>(); }
+constexpr int TRAJ_WARPS_CANDIDATES[2] = {4, 8};
 constexpr int TRAJ_MIN_BLOCKS = 1;
 
 // dynamic shared memory of traj_kernel: coefficient tables (CO2-Ar) + one pool per warp
-template <int SYS, typename PHYS, typename STG> constexpr size_t traj_smem_bytes() {
+template <int SYS, typename PHYS, typename STG, int WARPS = traj_warps<PHYS>()>
+constexpr size_t traj_smem_bytes() {
   return (SYS == SYS_CO2AR   ? smem_tables_bytes<PHYS>()
           : SYS == SYS_N2AR ? sizeof(N2arDipFold) + sizeof(N2arPesNet<PHYS>)
                             : 0) +
-         traj_warps<PHYS>() * sizeof(WarpSamples<STG, PHYS, (SYS == SYS_HEAR ? 3 : SYS == SYS_CH4CO2 ? 10 : 6)>);
+         WARPS * sizeof(WarpSamples<STG, PHYS, (SYS == SYS_HEAR ? 3 : SYS == SYS_CH4CO2 ? 10 : 6)>);
 }
 
-// SOLO: one item per warp (the solo kernel of the hand-off)
-template <int SYS, typename PHYS, typename STG, bool COMP, bool SOLO = false>
-__global__ void __launch_bounds__(traj_threads<PHYS>(), TRAJ_MIN_BLOCKS)
+// SOLO: one item per warp (the solo kernel of the hand-off); WARPS: warps per block
+template <int SYS, typename PHYS, typename STG, bool COMP, bool SOLO = false, int WARPS = traj_warps<PHYS>()>
+__global__ void __launch_bounds__(32 * WARPS, TRAJ_MIN_BLOCKS)
     traj_kernel(TrajParams P, TrajIO io, const Co2arTablesGlobal *gtab) {
   extern __shared__ __align__(16) unsigned char smem_raw[];
   if (SYS == SYS_HEAR) {

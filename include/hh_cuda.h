@@ -286,6 +286,16 @@ int hh_cuda_debug_tuning(int *ch4_dip_s_fp64, int *ch4_dip_s_mixed);
 #define HH_KT_MOMENT 5      /* M0 / M2 kernel */
 #define HH_KT_COUNT 6
 int hh_cuda_debug_kernel_ms(int enable, double *ms, uint64_t *launches, int n);
+/* Tuning knob (no counterpart in the reference): the trajectory launch's block
+ * shape (bulk kernel warps per block, 4 or 8) and hand-off threshold (the launch
+ * switches from 32 trajectories per warp to one when at most (solo warp slots) /
+ * handoff_div items are open; 1, 2 or 4) for the bound system and `precision`.  The
+ * library times the candidates on the first plain-C(t) launch of at least 16,384
+ * half-trajectories per system and precision (environment HH_TRAJ_WARPS,
+ * HH_TRAJ_HANDOFF_DIV fix them instead).  set_* > 0 fixes a value, set_* < 0
+ * forgets the pick (tuned again on the next large call), 0 leaves it; *warps and
+ * *handoff_div receive the current pick (0: not tuned yet). */
+int hh_cuda_debug_traj_tuning(int precision, int set_warps, int set_handoff_div, int *warps, int *handoff_div);
 /* Diagnostic (no counterpart in the reference): shape of the CH4-CO2 dipole's
  * coefficient stream (batches of 4 entries per radial piece, and the (Y1,
  * component, cos/sin) groups they form); HH_E_NOT_INITIALIZED before a CH4-CO2

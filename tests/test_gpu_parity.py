@@ -255,3 +255,38 @@ def test_solo_kernel_follows_the_bulk_path(name, T, N, dt, precision):
 def _lib_handle():
     from hawaiihybrid_b200 import _lib
     return _lib.load()
+
+
+@pytest.mark.parametrize("precision", [0, 1])
+def test_traj_tuning_picks_follow_the_same_steps(precision):
+    """The autotuner's choices (bulk kernel warps per block, hand-off threshold) change
+    only how items are scheduled: every half-trajectory takes the same steps and the
+    C(t) agree to rounding, for forced picks and for the autotuner's own (9,000
+    CO2-Ar trajectories, above the tuning threshold of 16,384 items)."""
+    import hawaiihybrid_b200 as hh
+    from hawaiihybrid_b200 import _lib
+    ms = lib_system("co2ar")
+    L = _lib_handle()
+    p = lib_params("co2ar", 256, 100.0, mixed_tol=3e-8)
+    qp, _ = O.sample(17, oracle_system("co2ar"), oracle_params("co2ar", 256, 100.0), 300.0, 9000)
+
+    def traced():
+        tr = np.zeros(4 * 2 * len(qp), dtype=np.uint32)
+        assert L.hh_cuda_debug_item_trace(tr.ctypes.data, tr.size) == 0
+        crln, _ = hh.correlation_from_initial_conditions(ms, p, qp, precision)
+        return tr.reshape(-1, 4)[:, 0].copy(), crln
+
+    runs = {}
+    for w, d in ((4, 1), (8, 1), (8, 4), (4, 2)):
+        assert _lib.traj_tuning(precision, w, d) == (w, d)
+        runs[(w, d)] = traced()
+    _lib.traj_tuning(precision, -1, -1)
+    assert _lib.traj_tuning(precision) == (0, 0)
+    runs["auto"] = traced()
+    w, d = _lib.traj_tuning(precision)
+    assert w in (4, 8) and d in (1, 2, 4)
+    s0, c0 = runs[(4, 1)]
+    assert s0.min() > 0
+    for key, (s, c) in runs.items():
+        np.testing.assert_array_equal(s, s0, err_msg=str(key))
+        np.testing.assert_allclose(c, c0, rtol=0, atol=1e-11 * abs(c0[0]), err_msg=str(key))
