@@ -46,7 +46,10 @@ EXPORTS = (
     "hh_cuda_shutdown", "hh_cuda_m0_noalloc", "hh_cuda_correlation_array", "hh_cuda_correlation_temperatures",
     "hh_cuda_prmu", "hh_cuda_debug_n2ar_dipole", "hh_cuda_m2", "hh_cuda_debug_tuning",
     "hh_cuda_debug_kernel_ms", "hh_cuda_debug_ch4co2_fold", "hh_cuda_moment_sums", "hh_cuda_debug_traj_tuning",
+    "hh_cuda_debug_set_ch4_dipole", "hh_cuda_vegas",
 )
+HH_INTEGRAND_M0 = 0
+HH_INTEGRAND_PF = 1
 # kernel classes of hh_cuda_debug_kernel_ms
 HH_KT_NAMES = ("traj_bulk", "traj_solo", "ch4_dipole", "ch4_sort", "ch4_corr", "moment")
 HH_KT_COUNT = len(HH_KT_NAMES)
@@ -141,6 +144,9 @@ def load(path: str | None = None):
     L.hh_cuda_debug_kernel_ms.argtypes = [C.c_int, _dp, np.ctypeslib.ndpointer(dtype=np.uint64, flags="C_CONTIGUOUS"),
                                           C.c_int]
     L.hh_cuda_debug_ch4co2_fold.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int)]
+    L.hh_cuda_debug_set_ch4_dipole.argtypes = [C.c_int, C.c_int]
+    L.hh_cuda_vegas.argtypes = [C.POINTER(CalcParamsC), C.c_int, C.c_double, C.c_uint64, C.c_uint64, C.c_uint64,
+                                C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.hh_cuda_debug_traj_tuning.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.hh_cuda_shutdown.restype = None
     for name in EXPORTS:

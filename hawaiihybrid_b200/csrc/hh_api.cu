@@ -13,6 +13,7 @@
 
 #include "../../include/hh_cuda.h"
 #include "hh_ch4co2_dip.cuh"
+#include "hh_ch4co2_tc.cuh"
 #include "hh_ch4co2_fold.h"
 #include "hh_co2ar_tables.h"
 #include "hh_consts.h"
@@ -21,6 +22,7 @@
 #include "hh_m0.cuh"
 #include "hh_prmu.cuh"
 #include "hh_traj.cuh"
+#include "hh_vegas.cuh"
 
 namespace hh {
 // 8 independent FMA chains per thread; the loop body is 8 FMAs = 16 flops
@@ -108,6 +110,8 @@ struct Ctx {
   unsigned int *d_ch4_meta = nullptr;
   int ch4_B = 0;
   int ch4_groups = 0;  // (Y1, component, cos/sin) groups of the batch stream
+  unsigned char *d_ch4_tc = nullptr;  // coefficient images of the tensor-core dipole kernel
+  int *d_ch4_tc_err = nullptr;        // set by that kernel when an mbarrier wait gave up
   int ch4_dip_s[2] = {0, 0};  // records per lane of the dipole kernel [FP64, mixed]; 0: not tuned yet
   // trajectory launch picks per [system][FP64, mixed] (warps == 0: not tuned yet)
   TrajTune traj_tune[5][2] = {};
@@ -149,6 +153,8 @@ struct Ctx {
   DevBuf<double> pm_sf;
   // M0
   DevBuf<double> m0_partials, m0_out;
+  // VEGAS: grid edges, block sums, per-bin sums of F^2
+  DevBuf<double> vg_edges, vg_sums, vg_hist;
   // FFT, and the CUDA graph of its kernel sequence for the current (N, dt, buffers)
   DevBuf<double> f_cf, f_nu, f_sf;
   DevBuf<double2> f_a, f_b;
@@ -597,12 +603,25 @@ int zimm_fft(const ZimmArgs &za) {
 }
 
 // one launchable variant of the CH4-CO2 dipole kernel (S records per lane)
+// S: records per lane of ch4_dipole_kernel, or CH4_DIP_TC for the tensor-core kernel
+// (hh_ch4co2_tc.cuh: tasks of 128 records, one CTA per SM)
+constexpr int CH4_DIP_TC = -1;
 struct Ch4DipVariant {
   void (*kern)(Ch4DipArgs);
   int S;
   size_t smem;
   int grid;
+  int task() const { return S == CH4_DIP_TC ? CH4TC_M : 32 * S; }
 };
+
+int ch4_dip_tc_variant(Ch4DipVariant *v) {
+  v->kern = nullptr;
+  v->S = CH4_DIP_TC;
+  v->smem = CH4TC_SMEM;
+  CK(cudaFuncSetAttribute(ch4_dipole_tc_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)v->smem));
+  v->grid = g.num_sms;  // the kernel holds all 512 TMEM columns of its SM
+  return HH_OK;
+}
 
 template <typename PHYS, int S> int ch4_dip_variant(Ch4DipVariant *v) {
   v->kern = ch4_dipole_kernel<PHYS, S>;
@@ -616,14 +635,16 @@ template <typename PHYS, int S> int ch4_dip_variant(Ch4DipVariant *v) {
   return HH_OK;
 }
 
-// the dipole kernel's candidates per precision: S = 1, 2, 4 (FP32), 1, 2 (FP64)
+// the dipole kernel's candidates per precision: S = 1, 2, 4 and the tensor-core
+// kernel (FP32), S = 1, 2 (FP64)
 template <typename PHYS> int ch4_dip_candidates(Ch4DipVariant *v, int *n) {
   int rc = ch4_dip_variant<PHYS, 1>(&v[0]);
   if (!rc) rc = ch4_dip_variant<PHYS, 2>(&v[1]);
   *n = 2;
   if constexpr (sizeof(PHYS) == 4) {
     if (!rc) rc = ch4_dip_variant<PHYS, 4>(&v[2]);
-    *n = 3;
+    if (!rc) rc = ch4_dip_tc_variant(&v[3]);
+    *n = 4;
   }
   return rc;
 }
@@ -664,15 +685,16 @@ int run_records_t(const TrajParams &P, const double *d_ic, uint64_t n, uint64_t 
   // dipole kernel variants; the records per lane are picked per precision by timing
   // every candidate on the first chunk of records (a dipole depends only on its
   // record, so every variant writes the same values)
-  Ch4DipVariant cand[3];
+  Ch4DipVariant cand[4];
   int ncand = 0;
   int rc0 = ch4_dip_candidates<PHYS>(cand, &ncand);
   if (rc0) return rc0;
   int &tuned_s = g.ch4_dip_s[sizeof(PHYS) == 4 ? 1 : 0];
   if (tuned_s == 0) {
-    // HH_CH4_DIP_S fixes the records per lane (when it names a candidate) instead of timing
+    // HH_CH4_DIP_S fixes the records per lane (when it names a candidate; "tc" the
+    // tensor-core kernel) instead of timing
     const char *env = getenv("HH_CH4_DIP_S");
-    const int want = env ? atoi(env) : 0;
+    const int want = env ? (strcmp(env, "tc") == 0 ? CH4_DIP_TC : atoi(env)) : 0;
     for (int c = 0; c < ncand; ++c)
       if (cand[c].S == want) tuned_s = want;
   }
@@ -717,9 +739,9 @@ int run_records_t(const TrajParams &P, const double *d_ic, uint64_t n, uint64_t 
     da.sorted = g.rec_sorted.p;
     da.warp0 = g.seg_w0.p;
     da.mu = g.rec_mu.p;
-    // sort the records into warp tasks of 32 S for variant v
+    // sort the records into the tasks of variant v (32 S records, 128 for tensor cores)
     auto sort_for = [&](const Ch4DipVariant &v) -> int {
-      sa.task = 32 * v.S;
+      sa.task = v.task();
       CK(cudaMemsetAsync(g.seg_cnt.p, 0, 2 * CH4_NSEG * sizeof(unsigned int), g.st));
       CK(cudaMemsetAsync(g.rec_sorted.p, 0xff, (nc * stride + (size_t)sa.task * CH4_NSEG) * sizeof(int), g.st));
       ch4_seg_count_kernel<PHYS><<<sgrid, 256, 0, g.st>>>(sa);
@@ -730,9 +752,25 @@ int run_records_t(const TrajParams &P, const double *d_ic, uint64_t n, uint64_t 
     };
     // the dipoles of the first max_tasks warp tasks with variant v
     auto dipole_with = [&](const Ch4DipVariant &v, long long max_tasks, long long step) -> int {
-      da.max_tasks = max_tasks;
-      da.task_step = step;
-      v.kern<<<v.grid, 32 * CH4_DIP_WARPS, v.smem, g.st>>>(da);
+      if (v.S == CH4_DIP_TC) {
+        if constexpr (sizeof(PHYS) == 4) {
+          Ch4TcArgs ta;
+          ta.records = static_cast<const float *>(g.rec.p ? (const void *)g.rec.p : nullptr);
+          ta.sorted = g.rec_sorted.p;
+          ta.warp0 = g.seg_w0.p;
+          ta.blob = g.d_ch4_tc;
+          ta.mu = reinterpret_cast<float *>(g.rec_mu.p);
+          for (int i = 0; i < CH4_NSEG; ++i) ta.centre[i] = hh_ch4co2_centre[i];
+          ta.max_tasks = max_tasks;
+          ta.task_step = step;
+          ta.err = g.d_ch4_tc_err;
+          ch4_dipole_tc_kernel<<<v.grid, CH4TC_M, v.smem, g.st>>>(ta);
+        }
+      } else {
+        da.max_tasks = max_tasks;
+        da.task_step = step;
+        v.kern<<<v.grid, 32 * CH4_DIP_WARPS, v.smem, g.st>>>(da);
+      }
       CK(cudaGetLastError());
       return HH_OK;
     };
@@ -744,10 +782,10 @@ int run_records_t(const TrajParams &P, const double *d_ic, uint64_t n, uint64_t 
         // about 2^20 records for every variant, in tasks spread over all radial
         // pieces: one untimed run (the variant's first launch), then the timed one
         const long long step = std::max<long long>(1, nslots >> 20);
-        rcs = dipole_with(cand[c], (1LL << 20) / (32 * cand[c].S), step);
+        rcs = dipole_with(cand[c], (1LL << 20) / cand[c].task(), step);
         if (rcs) return rcs;
         CK(cudaEventRecord(g.ev[4], g.st));
-        rcs = dipole_with(cand[c], (1LL << 20) / (32 * cand[c].S), step);
+        rcs = dipole_with(cand[c], (1LL << 20) / cand[c].task(), step);
         if (rcs) return rcs;
         CK(cudaEventRecord(g.ev[5], g.st));
         CK(cudaEventSynchronize(g.ev[5]));
@@ -929,8 +967,15 @@ int run_trajectories(const hh_calc_params *p, const double *d_ic, uint64_t n, ui
                                          io.item_trace);
     if (rc) return rc;
     unsigned long long nf = 0;
+    int tc_err = 0;
     CK(cudaMemcpyAsync(&nf, g.rec_nfail.p, sizeof nf, cudaMemcpyDeviceToHost, g.st));
+    CK(cudaMemcpyAsync(&tc_err, g.d_ch4_tc_err, sizeof tc_err, cudaMemcpyDeviceToHost, g.st));
     CK(cudaStreamSynchronize(g.st));
+    if (tc_err) {
+      CK(cudaMemsetAsync(g.d_ch4_tc_err, 0, sizeof(int), g.st));
+      snprintf(g_errmsg, sizeof g_errmsg, "tensor-core dipole kernel: an mbarrier wait timed out");
+      return HH_E_CUDA;
+    }
     nfail = (int)nf;
   } else if (zimm) {
     if (n_sat > 0) return HH_E_INVALID_ARGUMENT;
@@ -1081,6 +1126,55 @@ void m0_noalloc_forget() {
   for (auto &ptr : g_m0_noalloc_ptr) ptr = nullptr;
 }
 
+// Lepage's grid refinement (J. Comput. Phys. 27 (1978) 192) of one VEGAS iteration:
+// per dimension, the per-bin sums d_i of F^2 are smoothed with their neighbours,
+// normalised, compressed to m_i = ((1 - r_i) / -ln r_i)^alpha (r_i = d_i / sum d), and
+// the new edges split the cumulative m into NB equal parts, interpolating linearly
+// inside the old bins.  A dimension without any non-zero d keeps its grid.
+void vegas_refine(std::vector<double> &edges, const std::vector<double> &hist, int D, double alpha) {
+  const int NB = VEGAS_NB;
+  std::vector<double> sm(NB), m(NB), cum(NB + 1), ne(NB + 1);
+  for (int d = 0; d < D; ++d) {
+    const double *h = hist.data() + (size_t)d * NB;
+    double *e = edges.data() + (size_t)d * (NB + 1);
+    sm[0] = 0.5 * (h[0] + h[1]);
+    for (int i = 1; i < NB - 1; ++i) sm[i] = (h[i - 1] + h[i] + h[i + 1]) / 3.0;
+    sm[NB - 1] = 0.5 * (h[NB - 2] + h[NB - 1]);
+    double tot = 0.0;
+    for (int i = 0; i < NB; ++i) tot += sm[i];
+    if (!(tot > 0.0)) continue;
+    double M = 0.0;
+    for (int i = 0; i < NB; ++i) {
+      const double r = sm[i] / tot;
+      m[i] = (r > 0.0 && r < 1.0) ? pow((1.0 - r) / -log(r), alpha) : (r >= 1.0 ? 1.0 : 0.0);
+      M += m[i];
+    }
+    if (!(M > 0.0)) continue;
+    cum[0] = 0.0;
+    for (int i = 0; i < NB; ++i) cum[i + 1] = cum[i] + m[i];
+    ne[0] = e[0];
+    ne[NB] = e[NB];
+    int j = 0;
+    for (int k = 1; k < NB; ++k) {
+      const double target = M * double(k) / double(NB);
+      while (j < NB - 1 && cum[j + 1] < target) ++j;
+      const double frac = m[j] > 0.0 ? (target - cum[j]) / m[j] : 0.0;
+      ne[k] = e[j] + std::min(1.0, std::max(0.0, frac)) * (e[j + 1] - e[j]);
+    }
+    for (int k = 0; k <= NB; ++k) e[k] = ne[k];
+  }
+}
+
+template <int SYS> int launch_vegas(const VegasArgs &a, int grid) {
+  const size_t smem = vegas_smem<SYS>();
+  CK(cudaFuncSetAttribute(vegas_kernel<SYS>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  kt_begin();
+  vegas_kernel<SYS><<<grid, VEGAS_THREADS, smem, g.st>>>(a, g.d_tab, g.d_n2ar_fold);
+  CK(cudaGetLastError());
+  kt_end(HH_KT_MOMENT);
+  return HH_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -1184,6 +1278,12 @@ int hh_cuda_init(int device, const hh_system_desc *sys) {
     CK(cudaMemcpy(g.d_ch4_cf, cf.data(), cf.size() * sizeof(float4), cudaMemcpyHostToDevice));
     CK(cudaMemcpy(g.d_ch4_y2, f.by2.data(), 4 * B, cudaMemcpyHostToDevice));
     CK(cudaMemcpy(g.d_ch4_meta, f.bmeta.data(), B * sizeof(unsigned int), cudaMemcpyHostToDevice));
+    std::vector<float> tc_blob;
+    if (ch4co2_build_tc_blob(f, &tc_blob) != 0) return HH_E_UNSUPPORTED_SYSTEM;
+    CK(cudaMalloc(&g.d_ch4_tc, tc_blob.size() * sizeof(float)));
+    CK(cudaMemcpy(g.d_ch4_tc, tc_blob.data(), tc_blob.size() * sizeof(float), cudaMemcpyHostToDevice));
+    CK(cudaMalloc(&g.d_ch4_tc_err, sizeof(int)));
+    CK(cudaMemset(g.d_ch4_tc_err, 0, sizeof(int)));
     g.ch4_B = f.n_batch;
     g.ch4_groups = 0;
     for (size_t b = 0; b < B; ++b) g.ch4_groups += (f.bmeta[b] & 8u) ? 1 : 0;
@@ -1667,6 +1767,82 @@ int hh_cuda_m2(const hh_calc_params *p, const double *T, int nT, uint64_t n_samp
   return HH_OK;
 }
 
+int hh_cuda_vegas(const hh_calc_params *p, int integrand, double T, uint64_t niterations, uint64_t npoints,
+                  uint64_t seed, double *m, double *q) {
+  if (!g.init) return HH_E_NOT_INITIALIZED;
+  if (g.sys == SYS_CH4CO2) return HH_E_UNSUPPORTED_SYSTEM;  // no CH4-CO2 moment integrand
+  if (!p || !m || !(T > 0) || niterations == 0 || npoints < 2) return HH_E_INVALID_ARGUMENT;
+  if (integrand != VEGAS_INTEGRAND_M0 && integrand != VEGAS_INTEGRAND_PF) return HH_E_INVALID_ARGUMENT;
+  if (!(p->sampler_Rmin > 0) || !(p->sampler_Rmax > p->sampler_Rmin)) return HH_E_INVALID_ARGUMENT;
+  if (p->pair_state < 1 || p->pair_state > 3) return HH_E_INVALID_ARGUMENT;
+  if (niterations > (uint64_t)1 << 20 || npoints > ((uint64_t)1 << 62) / niterations) return HH_E_INVALID_ARGUMENT;
+  CK(cudaSetDevice(g.device));
+  const int D = g.QP;
+  const int grid = (int)std::max<uint64_t>(1, std::min<uint64_t>((uint64_t)g.num_sms * 4,
+                                                                  (npoints + VEGAS_THREADS - 1) / VEGAS_THREADS));
+  CK(g.vg_edges.ensure((size_t)D * (VEGAS_NB + 1)));
+  CK(g.vg_sums.ensure(2 * (size_t)grid));
+  CK(g.vg_hist.ensure((size_t)D * VEGAS_NB));
+  std::vector<double> edges((size_t)D * (VEGAS_NB + 1)), hist((size_t)D * VEGAS_NB), sums(2 * (size_t)grid);
+  for (int d = 0; d < D; ++d)
+    for (int k = 0; k <= VEGAS_NB; ++k) edges[(size_t)d * (VEGAS_NB + 1) + k] = double(k) / VEGAS_NB;
+  VegasArgs a;
+  memset(&a, 0, sizeof a);
+  a.s.sys = g.sys;
+  a.s.mu = g.mu;
+  a.s.II = g.II;
+  a.s.Rmin = p->sampler_Rmin;
+  a.s.Rmax = p->sampler_Rmax;
+  a.s.pair_state = p->pair_state;
+  a.D = D;
+  a.integrand = integrand;
+  a.inv_kT = HH_HKT / T;
+  a.n = npoints;
+  a.seed = seed;
+  a.edges = g.vg_edges.p;
+  a.sums = g.vg_sums.p;
+  a.hist = g.vg_hist.p;
+  // weighted average of the iterations after the first (hep::accumulate of results
+  // begin() + 1 .. end(), src/hep_hawaii.cpp:352), weights 1 / variance
+  double wsum = 0.0, wv = 0.0, first_v = 0.0, first_e = 0.0;
+  for (uint64_t it = 0; it < niterations; ++it) {
+    CK(cudaMemcpyAsync(g.vg_edges.p, edges.data(), edges.size() * sizeof(double), cudaMemcpyHostToDevice, g.st));
+    CK(cudaMemsetAsync(g.vg_hist.p, 0, hist.size() * sizeof(double), g.st));
+    a.id0 = it * npoints;
+    int rc = g.sys == SYS_HEAR ? launch_vegas<SYS_HEAR>(a, grid)
+             : g.sys == SYS_N2AR ? launch_vegas<SYS_N2AR>(a, grid)
+                                 : launch_vegas<SYS_CO2AR>(a, grid);
+    if (rc) return rc;
+    CK(cudaMemcpyAsync(sums.data(), g.vg_sums.p, sums.size() * sizeof(double), cudaMemcpyDeviceToHost, g.st));
+    CK(cudaMemcpyAsync(hist.data(), g.vg_hist.p, hist.size() * sizeof(double), cudaMemcpyDeviceToHost, g.st));
+    CK(cudaStreamSynchronize(g.st));
+    double S = 0.0, S2 = 0.0;
+    for (int b = 0; b < grid; ++b) {
+      S += sums[2 * b];
+      S2 += sums[2 * b + 1];
+    }
+    const double n = double(npoints);
+    const double mean = S / n;
+    const double var = std::max(S2 / n - mean * mean, 0.0) / (n - 1.0);  // variance of the mean
+    if (it == 0) {
+      first_v = mean;
+      first_e = sqrt(var);
+    } else if (var > 0.0) {
+      wsum += 1.0 / var;
+      wv += mean / var;
+    }
+    if (it + 1 < niterations) vegas_refine(edges, hist, D, 1.5);
+  }
+  if (niterations == 1 || !(wsum > 0.0)) {
+    *m = first_v;
+    if (q) *q = first_e;
+  } else {
+    *m = wv / wsum;
+    if (q) *q = sqrt(1.0 / wsum);
+  }
+  return HH_OK;
+}
+
 // the transform's kernels on g.st: pack, log2(2N) Stockham passes, finish
 void idct_enqueue(size_t N, double dt) {
   const long long L = 2 * (long long)N;
@@ -1827,6 +2003,16 @@ int hh_cuda_debug_traj_tuning(int precision, int set_warps, int set_handoff_div,
   return HH_OK;
 }
 
+int hh_cuda_debug_set_ch4_dipole(int precision, int variant) {
+  if (!g.init) return HH_E_NOT_INITIALIZED;
+  if (precision != HH_PRECISION_FP64 && precision != HH_PRECISION_MIXED) return HH_E_INVALID_ARGUMENT;
+  const bool mixed = precision == HH_PRECISION_MIXED;
+  const bool ok = variant == 0 || variant == 1 || variant == 2 || (mixed && (variant == 4 || variant == CH4_DIP_TC));
+  if (!ok) return HH_E_INVALID_ARGUMENT;
+  g.ch4_dip_s[mixed ? 1 : 0] = variant;
+  return HH_OK;
+}
+
 int hh_cuda_debug_ch4co2_fold(int *n_batch, int *n_groups) {
   if (!g.init || !g.d_ch4_cd) return HH_E_NOT_INITIALIZED;
   if (n_batch) *n_batch = g.ch4_B;
@@ -1978,6 +2164,9 @@ void hh_cuda_shutdown(void) {
   g.m0_out.release();
   g.tune_crln.release();
   g.tune_cnt.release();
+  g.vg_edges.release();
+  g.vg_sums.release();
+  g.vg_hist.release();
   g.f_cf.release();
   g.f_nu.release();
   g.f_sf.release();
@@ -1993,6 +2182,8 @@ void hh_cuda_shutdown(void) {
   if (g.d_ch4_cf) cudaFree(g.d_ch4_cf);
   if (g.d_ch4_y2) cudaFree(g.d_ch4_y2);
   if (g.d_ch4_meta) cudaFree(g.d_ch4_meta);
+  if (g.d_ch4_tc) cudaFree(g.d_ch4_tc);
+  if (g.d_ch4_tc_err) cudaFree(g.d_ch4_tc_err);
   if (g.d_mt) cudaFree(g.d_mt);
   if (g.d_mt_jump_seg) cudaFree(g.d_mt_jump_seg);
   if (g.d_mt_jump_coarse) cudaFree(g.d_mt_jump_coarse);

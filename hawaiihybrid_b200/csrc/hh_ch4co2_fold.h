@@ -21,3 +21,9 @@ struct Ch4Co2FoldHost {
 // coef * rad_b(R) * N(l1, m1) * N(l2, m2), N(l, m) = sqrt((l+m)!/(l-m)!) (the kernel's
 // harmonics carry sqrt((l-m)!/(l+m)!)); returns 0, or -1 on an unexpected table
 int ch4co2_build_fold(Ch4Co2FoldHost *out);
+
+// coefficient images of the tensor-core dipole kernel (hh_ch4co2_tc.cuh): per radial
+// piece, pass and K-chunk the TF32 (hi, lo) split of B_c[Y1 column, 4 Y2 + power] in
+// the layout of hh_ch4co2_tc_layout.h; blob holds NSEG * CH4TC_PIECE_BYTES / 4 floats.
+// Returns 0, or -1 on an unexpected table.
+int ch4co2_build_tc_blob(const Ch4Co2FoldHost &f, std::vector<float> *blob);

@@ -2,11 +2,14 @@
 // expanded reference tables of hh_ch4co2_tables.h, in FP64.
 #include <algorithm>
 #include <cmath>
+#include <cstdint>
+#include <cstring>
 #include <map>
 #include <tuple>
 
 #include "hh_ch4co2_fold.h"
 #include "hh_ch4co2_tables.h"
+#include "hh_ch4co2_tc_layout.h"
 
 namespace {
 void lm_of(int code, int *l, int *m, int *cs) {
@@ -16,6 +19,15 @@ void lm_of(int code, int *l, int *m, int *cs) {
   *l = L;
   *m = i - L * (L + 1) / 2;
   *cs = code & 1;
+}
+// nearest TF32 value (10 explicit mantissa bits, ties away from zero) of a float
+float tf32_rna(float v) {
+  uint32_t b;
+  memcpy(&b, &v, 4);
+  b = (b + 0x1000u) & ~0x1FFFu;
+  float r;
+  memcpy(&r, &b, 4);
+  return r;
 }
 double norm_lm(int l, int m) {  // sqrt((l+m)! / (l-m)!)
   double p = 1.0;
@@ -112,5 +124,52 @@ int ch4co2_build_fold(Ch4Co2FoldHost *out) {
       for (int j = 0; j < 4; ++j)
         out->bcoef[((size_t)s * EP + i) * 4 + j] = out->coef[((size_t)s * E + order[i]) * 4 + j];
   }
+  return 0;
+}
+
+int ch4co2_build_tc_blob(const Ch4Co2FoldHost &f, std::vector<float> *blob) {
+  using namespace hh;
+  const int E = f.n_entry;
+  // B[piece][component][column][K] in FP64 from the entry stream (groups in (m1, l1, cs,
+  // component) order, gcount groups per (l1, m1) in m-major order)
+  const size_t per_comp = (size_t)CH4TC_N * CH4TC_K;
+  std::vector<double> B((size_t)HH_CH4CO2_NSEG * 3 * per_comp, 0.0);
+  int g = 0, e = 0, lm = 0;
+  for (int m = 0; m <= HH_CH4CO2_L1MAX; ++m)
+    for (int l = m; l <= HH_CH4CO2_L1MAX; ++l, ++lm)
+      for (int k = 0; k < f.gcount[lm]; ++k, ++g) {
+        const unsigned d = f.grp[g];
+        const int cs = int(d & 1u), comp = int((d >> 1) & 3u), cnt = int(d >> 3);
+        if (comp > 2 || (m == 0 && cs == 1)) return -1;
+        const int col = ch4tc_y1_col(l, m, cs, HH_CH4CO2_L1MAX);
+        if (col >= CH4TC_NY1) return -1;
+        for (int i = 0; i < cnt; ++i, ++e) {
+          const int y2 = f.y2[e];
+          for (int s = 0; s < HH_CH4CO2_NSEG; ++s)
+            for (int j = 0; j < 4; ++j)
+              B[((size_t)s * 3 + comp) * per_comp + (size_t)col * CH4TC_K + 4 * y2 + j] =
+                  f.coef[((size_t)s * E + e) * 4 + j];
+        }
+      }
+  if (e != E) return -1;
+  blob->assign((size_t)HH_CH4CO2_NSEG * CH4TC_PIECE_BYTES / 4, 0.0f);
+  for (int s = 0; s < HH_CH4CO2_NSEG; ++s)
+    for (int q = 0; q < 2; ++q) {
+      const int ncomp = q == 0 ? 2 : 1, img = (q == 0 ? CH4TC_IMG0 : CH4TC_IMG1) / 4;
+      for (int c = 0; c < CH4TC_NCHUNK; ++c) {
+        float *hi = blob->data() + ch4tc_blob_off(s, q, c) / 4, *lo = hi + img;
+        for (int cc = 0; cc < ncomp; ++cc) {
+          const int comp = q == 0 ? cc : 2;
+          for (int n = 0; n < CH4TC_N; ++n)
+            for (int kk = 0; kk < CH4TC_KC; ++kk) {
+              const double v = B[((size_t)s * 3 + comp) * per_comp + (size_t)n * CH4TC_K + CH4TC_KC * c + kk];
+              const float h = tf32_rna((float)v);
+              const int off = ch4tc_img_off(cc * CH4TC_N + n, kk);
+              hi[off] = h;
+              lo[off] = tf32_rna((float)(v - (double)h));
+            }
+        }
+      }
+    }
   return 0;
 }

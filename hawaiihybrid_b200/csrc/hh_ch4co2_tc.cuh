@@ -1,0 +1,447 @@
+// CH4-CO2 dipole on the 5th-generation tensor cores (tcgen05, TMEM accumulators).
+//
+// Per radial piece p the dipole of PES-IDS/ai_ids_ch4_co2.cpp:672-1067 is a bilinear
+// form in the two sets of real harmonics (hh_ch4co2_dip.cuh has the entry stream):
+//   mu_c(r) = sum_n Y1_n(r) T_c[r, n],   T_c[r, n] = sum_{k, j} Y2_k(r) x(r)^j B_c,p[n, 4k + j]
+// with n over the 196 Y1 functions (l1 <= 13, m-major, cos then sin), k over the 91 Y2
+// functions, j over the 4 powers of x = R - centre_p of the piece's cubic, and B the
+// folded coefficients (zero where the reference has no term).  For a tile of 128
+// records of one piece the inner sum is a GEMM
+//   T_c (128 x 196) = A (128 x 364) . B_c,p^T,   A[r, 4k + j] = Y2_k(r) x(r)^j,
+// run on the tensor cores in TF32 with a three-product split for FP32 accuracy
+// (A = A_hi + A_lo, B = B_hi + B_lo, T = A_hi B_hi + A_hi B_lo + A_lo B_hi: the
+// dropped A_lo B_lo is 2^-22 of a product).  The outer sum over n (196 FMAs per
+// component) and the rotation to the lab frame run on the CUDA cores from TMEM.
+//
+// Mapping (one CTA of 128 threads per SM, persistent over the 128-record tasks):
+//   - thread t owns record t of the task: geometry, Y2 (shared memory), x powers, and
+//     its row of A written into shared memory in the canonical no-swizzle K-major
+//     layout (8-row x 16-byte core matrices; K-adjacent cores 128 B apart, 8-row
+//     groups 512 B apart);
+//   - K is walked in chunks of 16 (23 chunks for K = 368, the last 4 columns zero);
+//     the chunk's B_hi | B_lo image (built on the host in the same layout) arrives by
+//     one bulk copy (cp.async.bulk, this GPU's memory only, no multicast) into a
+//     double-buffered stage tracked by an mbarrier;
+//   - thread 0 issues the tcgen05.mma instructions of a chunk (M = 128, N = 208, K = 8
+//     each) and commits them to the stage's mbarrier, which frees the stage;
+//   - TMEM holds two 208-column accumulators: pass 0 computes components 0 and 1,
+//     pass 1 component 2 (the three would need 624 of the 512 columns);
+//   - after a pass thread t reads its TMEM lane (tcgen05.ld 32x32b) and forms
+//     sum_n Y1_n T[t, n] with Y1 generated by its recurrence in column order.
+// Every mbarrier wait is bounded: on a timeout the CTA records the error in *err,
+// stops issuing work, waits (bounded) for what it issued and frees its TMEM.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+#include "hh_ch4co2_dip.cuh"
+#include "hh_ch4co2_tc_layout.h"
+
+namespace hh {
+
+constexpr int CH4TC_A_BYTES = CH4TC_M * CH4TC_KC * 4;    // one A image (hi or lo): 8 KB
+constexpr int CH4TC_STAGE_B = 2 * CH4TC_IMG0;            // B_hi | B_lo of the widest pass
+// dynamic shared memory: 2 stages x (A_hi, A_lo, B_hi | B_lo), Y2 of the task
+constexpr size_t CH4TC_SMEM = 2 * (2 * CH4TC_A_BYTES + CH4TC_STAGE_B) + (size_t)CH4_NY2 * CH4TC_M * 4 + 1024;
+constexpr unsigned CH4TC_TMEM_COLS = 512;
+constexpr unsigned CH4TC_COL1 = 256;            // TMEM column of the second accumulator
+constexpr long long CH4TC_WAIT_LIMIT = 1LL << 24;  // polls of an mbarrier before giving up
+
+struct Ch4TcArgs {
+  const float *records;       // FP32 records (r, quaternion, u, pad)
+  const int *sorted;          // record index per task slot, -1 for padding (tasks of 128)
+  const long long *warp0;     // first task of each piece; [NSEG] = total tasks
+  const unsigned char *blob;  // B images (ch4tc_blob_off), 16-byte aligned
+  float *mu;                  // [record][4] lab-frame dipole
+  double centre[CH4_NSEG];
+  long long max_tasks, task_step;  // as Ch4DipArgs: a timing run takes a spread-out subset
+  int *err;                   // set when an mbarrier wait gave up
+};
+
+__device__ __forceinline__ uint32_t smem_u32(const void *p) {
+  return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+
+// shared-memory matrix descriptor: no swizzle, K-major, LBO 128 B (K-adjacent core
+// matrices), SBO 512 B (8-row groups), descriptor version 1
+__device__ __forceinline__ uint64_t ch4tc_desc(uint32_t saddr) {
+  return (uint64_t)((saddr >> 4) & 0x3FFFu) | ((uint64_t)(128u >> 4) << 16) | ((uint64_t)(512u >> 4) << 32) |
+         (1ull << 46);
+}
+
+// instruction descriptor: D F32, A and B TF32, both K-major, N = 208, M = 128
+constexpr uint32_t CH4TC_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(CH4TC_N >> 3) << 17) |
+                                 ((uint32_t)(CH4TC_M >> 4) << 24);
+
+__device__ __forceinline__ float tf32_round(float v) {
+  uint32_t r;
+  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
+  return __uint_as_float(r);
+}
+
+__device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+}
+
+// bounded wait for the phase of parity `par`; false on a timeout
+__device__ __forceinline__ bool mbar_wait(uint64_t *bar, unsigned par) {
+  const uint32_t a = smem_u32(bar);
+  for (long long i = 0; i < CH4TC_WAIT_LIMIT; ++i) {
+    uint32_t done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(done)
+        : "r"(a), "r"(par)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+
+// one bulk copy of `bytes` from global memory into shared memory, completing on `bar`
+__device__ __forceinline__ void ch4tc_load(void *dst, const void *src, unsigned bytes, uint64_t *bar) {
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+               : "memory");
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                   smem_u32(dst)),
+               "l"(src), "r"(bytes), "r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void ch4tc_mma(uint32_t d_tmem, uint64_t a_desc, uint64_t b_desc, uint32_t acc) {
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.b32 p, %4, 0;\n\t"
+      "tcgen05.mma.cta_group::1.kind::tf32 [%0], %1, %2, %3, p;\n\t}" ::"r"(d_tmem),
+      "l"(a_desc), "l"(b_desc), "r"(CH4TC_IDESC), "r"(acc)
+      : "memory");
+}
+
+__device__ __forceinline__ void ch4tc_commit(uint64_t *bar) {
+  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];" ::"r"(smem_u32(bar))
+               : "memory");
+}
+
+__device__ __forceinline__ void tc_fence_before() { asm volatile("tcgen05.fence::before_thread_sync;" ::: "memory"); }
+__device__ __forceinline__ void tc_fence_after() { asm volatile("tcgen05.fence::after_thread_sync;" ::: "memory"); }
+
+// 16 consecutive TMEM columns of this thread's lane
+__device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
+  uint32_t r[16];
+  asm volatile(
+      "tcgen05.ld.sync.aligned.32x32b.x16.b32 {%0, %1, %2, %3, %4, %5, %6, %7, %8, %9, %10, %11, %12, %13, %14, "
+      "%15}, [%16];"
+      : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),
+        "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]), "=r"(r[15])
+      : "r"(taddr));
+  asm volatile("tcgen05.wait::ld.sync.aligned;" ::: "memory");
+#pragma unroll
+  for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
+}
+
+// Y2 of the CO2 axis (x, y, z) in the CH4 frame into Y[idx * 128 + t], in the order of
+// ch4_y2: m = 0..12, l = m..12 even, cos then sin
+__device__ __forceinline__ void ch4tc_y2(float x, float y, float z, float *Y, int t) {
+  float C = 1.f, Sn = 0.f, pm = 1.f;
+  int idx = 0;
+#pragma unroll 1
+  for (int m = 0; m <= CH4_L2; ++m) {
+    if (m > 0) {
+      const float c = C * x - Sn * y;
+      Sn = C * y + Sn * x;
+      C = c;
+      pm = -pm * sqrtf(float(2 * m - 1) / float(2 * m));
+    }
+    float qa = 1.f, qb = 0.f;
+#pragma unroll 1
+    for (int l = m; l <= CH4_L2; ++l) {
+      float q;
+      if (l == m) q = 1.f;
+      else if (l == m + 1) q = sqrtf(float(2 * m + 1)) * z;
+      else q = (float(2 * l - 1) * z * qa - sqrtf(float((l - 1) * (l - 1) - m * m)) * qb) / sqrtf(float(l * l - m * m));
+      if ((l & 1) == 0) {
+        Y[(idx++) * CH4TC_M + t] = pm * C * q;
+        if (m > 0) Y[(idx++) * CH4TC_M + t] = pm * Sn * q;
+      }
+      qb = qa;
+      qa = q;
+    }
+  }
+}
+
+// sum_n Y1_n(n1) T[n] over the 196 columns at TMEM address `taddr` (this thread's
+// lane), Y1 generated in column order by the recurrence of ch4_dipole_kernel
+__device__ __forceinline__ float ch4tc_y1_dot(uint32_t taddr, const float n1[3]) {
+  float acc = 0.f;
+  float C = 1.f, Sn = 0.f, pm = 1.f, qa = 0.f, qb = 0.f;
+  int m = 0, l = 0;
+  // position in the (m, l, cs) walk: the next Y1 value to produce
+  bool sin_next = false;
+  float ys_pending = 0.f;
+#pragma unroll 1
+  for (int c0 = 0; c0 < CH4TC_NY1; c0 += 16) {
+    float v[16];
+    tmem_ld16(taddr + (uint32_t)c0, v);
+#pragma unroll
+    for (int i = 0; i < 16; ++i) {
+      if (c0 + i < CH4TC_NY1) {
+        float y;
+        if (sin_next) {
+          y = ys_pending;
+          sin_next = false;
+        } else {
+          // advance to (l, m): the first call starts at (0, 0)
+          if (c0 + i == 0) {
+            qa = 1.f;
+            qb = 0.f;
+          } else if (l == CH4_L1) {
+            ++m;
+            l = m;
+            const float cc = C * n1[0] - Sn * n1[1];
+            Sn = C * n1[1] + Sn * n1[0];
+            C = cc;
+            pm = -pm * sqrtf(float(2 * m - 1) / float(2 * m));
+            qa = 1.f;
+            qb = 0.f;
+          } else {
+            ++l;
+            const float ca = float(2 * l - 1), cb = sqrtf(float((l - 1) * (l - 1) - m * m));
+            const float id = (l > m + 1) ? 1.f / sqrtf(float(l * l - m * m)) : 0.f;
+            const float c1 = sqrtf(float(2 * m + 1));
+            const float z = n1[2];
+            const float q = (l == m + 1) ? c1 * z : (ca * z * qa - cb * qb) * id;
+            qb = qa;
+            qa = q;
+          }
+          y = pm * C * qa;
+          if (m > 0) {
+            ys_pending = pm * Sn * qa;
+            sin_next = true;
+          }
+        }
+        acc = fmaf(y, v[i], acc);
+      }
+    }
+  }
+  return acc;
+}
+
+__global__ void __launch_bounds__(CH4TC_M, 1) ch4_dipole_tc_kernel(Ch4TcArgs a) {
+  extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
+  unsigned char *smem = reinterpret_cast<unsigned char *>(
+      (reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~uintptr_t(1023));
+  // stage s: A_hi, A_lo, B (hi | lo)
+  unsigned char *stA[2][2], *stB[2];
+#pragma unroll
+  for (int s = 0; s < 2; ++s) {
+    unsigned char *base = smem + (size_t)s * (2 * CH4TC_A_BYTES + CH4TC_STAGE_B);
+    stA[s][0] = base;
+    stA[s][1] = base + CH4TC_A_BYTES;
+    stB[s] = base + 2 * CH4TC_A_BYTES;
+  }
+  float *Y2s = reinterpret_cast<float *>(smem + 2 * (2 * CH4TC_A_BYTES + CH4TC_STAGE_B));
+  __shared__ __align__(8) uint64_t bar_load[2], bar_mma[2];
+  __shared__ uint32_t tmem_base_s;
+  __shared__ int bad_s;
+  __shared__ long long w0[CH4_NSEG + 1];
+  const int t = threadIdx.x, warp = t >> 5;
+  for (int i = t; i <= CH4_NSEG; i += blockDim.x) w0[i] = a.warp0[i];
+  if (t == 0) {
+    mbar_init(&bar_load[0], 1);
+    mbar_init(&bar_load[1], 1);
+    mbar_init(&bar_mma[0], 1);
+    mbar_init(&bar_mma[1], 1);
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+    bad_s = 0;
+  }
+  if (warp == 0) {
+    asm volatile("tcgen05.alloc.cta_group::1.sync.aligned.shared::cta.b32 [%0], %1;" ::"r"(smem_u32(&tmem_base_s)),
+                 "r"(CH4TC_TMEM_COLS)
+                 : "memory");
+    asm volatile("tcgen05.relinquish_alloc_permit.cta_group::1.sync.aligned;" ::: "memory");
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  const uint32_t tmem = tmem_base_s;
+  const long long total = min((w0[CH4_NSEG] + a.task_step - 1) / a.task_step, a.max_tasks);
+  auto seg_of = [&](long long task) {
+    int s = 0;
+    while (s < CH4_NSEG - 1 && w0[s + 1] <= task) ++s;
+    return s;
+  };
+  // chunk sequence: g counts the chunks this CTA has issued; stage g & 1; the n-th
+  // completion of a stage's barriers belongs to its chunk g = 2 n + stage
+  unsigned g = 0;
+  // the chunk after (task, q, c) in this CTA's walk, for the B prefetch
+  auto next_chunk = [&](long long task, int q, int c, long long &nt, int &nq, int &nc) -> bool {
+    nt = task;
+    nq = q;
+    nc = c + 1;
+    if (nc == CH4TC_NCHUNK) {
+      nc = 0;
+      nq = q + 1;
+      if (nq == 2) {
+        nq = 0;
+        nt = task + gridDim.x;
+        if (nt >= total) return false;
+      }
+    }
+    return true;
+  };
+  auto issue_load = [&](long long task, int q, int c, int s) {
+    const int seg = seg_of(task * a.task_step);
+    const unsigned bytes = q == 0 ? 2 * CH4TC_IMG0 : 2 * CH4TC_IMG1;
+    ch4tc_load(stB[s], a.blob + ch4tc_blob_off(seg, q, c), bytes, &bar_load[s]);
+  };
+  long long task0 = blockIdx.x;
+  if (t == 0 && task0 < total) issue_load(task0, 0, 0, 0);
+  for (long long task = task0; task < total; task += gridDim.x) {
+    const long long w = task * a.task_step;
+    const int seg = seg_of(w);
+    // ---- this thread's record: geometry, Y2, powers of x ----
+    const int first = a.sorted[w * CH4TC_M];
+    const int mine = a.sorted[w * CH4TC_M + t];
+    const int src = mine >= 0 ? mine : first;
+    const float *rec = a.records + (size_t)src * HH_REC_WORDS;
+    float M[3][3], n1[3], n2[3];
+    {
+      const float r[3] = {rec[0], rec[1], rec[2]};
+      const float qt[4] = {rec[3], rec[4], rec[5], rec[6]};
+      const float u[3] = {rec[7], rec[8], rec[9]};
+      quat_matrix<float>(qt, M);
+      const float R = sqrtf(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+      const float iR = 1.f / R;
+      const float iu = 1.f / sqrtf(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+#pragma unroll
+      for (int k = 0; k < 3; ++k) {
+        n1[k] = (M[0][k] * r[0] + M[1][k] * r[1] + M[2][k] * r[2]) * iR;
+        n2[k] = (M[0][k] * u[0] + M[1][k] * u[1] + M[2][k] * u[2]) * iu;
+      }
+    }
+    const float R = sqrtf(rec[0] * rec[0] + rec[1] * rec[1] + rec[2] * rec[2]);
+    const float x = R - float(a.centre[seg]);
+    const float xp[4] = {1.f, x, x * x, x * x * x};
+    __syncthreads();  // the previous task's last chunk no longer reads Y2s
+    ch4tc_y2(n2[0], n2[1], n2[2], Y2s, t);
+    float acc[3] = {0.f, 0.f, 0.f};
+    for (int q = 0; q < 2; ++q) {
+      const int ntile = q == 0 ? 2 : 1;
+      for (int c = 0; c < CH4TC_NCHUNK; ++c, ++g) {
+        const int s = g & 1;
+        // ---- A chunk: row t, columns 16 c .. 16 c + 15 (k = 4 c .. 4 c + 3, j = 0..3) ----
+        float *Ah = reinterpret_cast<float *>(stA[s][0]);
+        float *Al = reinterpret_cast<float *>(stA[s][1]);
+#pragma unroll
+        for (int kq = 0; kq < 4; ++kq) {
+          const int k = 4 * c + kq;
+          const float y2 = (k < CH4_NY2) ? Y2s[k * CH4TC_M + t] : 0.f;
+          float4 hi, lo;
+          float *ph = &hi.x, *pl = &lo.x;
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            const float v = y2 * xp[j];
+            const float h = tf32_round(v);
+            ph[j] = h;
+            pl[j] = tf32_round(v - h);
+          }
+          *reinterpret_cast<float4 *>(Ah + ch4tc_img_off(t, 4 * kq)) = hi;
+          *reinterpret_cast<float4 *>(Al + ch4tc_img_off(t, 4 * kq)) = lo;
+        }
+        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+        __syncthreads();
+        if (t == 0 && !bad_s) {
+          if (!mbar_wait(&bar_load[s], (g >> 1) & 1)) {
+            bad_s = 1;
+            atomicExch(a.err, 1);
+          } else {
+            tc_fence_after();
+            const uint32_t a_hi = smem_u32(stA[s][0]), a_lo = smem_u32(stA[s][1]);
+            const uint32_t b_hi = smem_u32(stB[s]);
+            const uint32_t b_lo = b_hi + (q == 0 ? CH4TC_IMG0 : CH4TC_IMG1);
+#pragma unroll 1
+            for (int nt = 0; nt < ntile; ++nt) {
+              const uint32_t d = tmem + (nt == 0 ? 0u : CH4TC_COL1);
+              const uint32_t boff = (uint32_t)nt * (CH4TC_N / 8) * 512u;
+#pragma unroll
+              for (int ks = 0; ks < 2; ++ks) {
+                const uint32_t ko = (uint32_t)ks * 256u;
+                const uint32_t first_acc = (c == 0 && ks == 0) ? 0u : 1u;
+                ch4tc_mma(d, ch4tc_desc(a_hi + ko), ch4tc_desc(b_hi + boff + ko), first_acc);
+                ch4tc_mma(d, ch4tc_desc(a_hi + ko), ch4tc_desc(b_lo + boff + ko), 1u);
+                ch4tc_mma(d, ch4tc_desc(a_lo + ko), ch4tc_desc(b_hi + boff + ko), 1u);
+              }
+            }
+            ch4tc_commit(&bar_mma[s]);
+            // prefetch the next chunk's B into the other stage once its MMAs (chunk g - 1)
+            // are done
+            long long nt_;
+            int nq, nc;
+            if (next_chunk(task, q, c, nt_, nq, nc)) {
+              const int s1 = s ^ 1;
+              if (g >= 1 && !mbar_wait(&bar_mma[s1], ((g - 1) >> 1) & 1)) {
+                bad_s = 1;
+                atomicExch(a.err, 1);
+              } else {
+                issue_load(nt_, nq, nc, s1);
+              }
+            }
+          }
+        }
+        // the other stage is free for the next chunk's A once thread 0 has seen
+        // chunk g - 1's MMAs complete (above)
+        __syncthreads();
+      }
+      // ---- all MMAs of this pass done: read the accumulators ----
+      if (t == 0 && !bad_s) {
+        if (!mbar_wait(&bar_mma[(g - 1) & 1], ((g - 1) >> 1) & 1)) {
+          bad_s = 1;
+          atomicExch(a.err, 1);
+        }
+      }
+      __syncthreads();
+      tc_fence_after();
+      if (!bad_s) {
+        const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+        if (q == 0) {
+          acc[0] = ch4tc_y1_dot(lane_addr, n1);
+          acc[1] = ch4tc_y1_dot(lane_addr + CH4TC_COL1, n1);
+        } else {
+          acc[2] = ch4tc_y1_dot(lane_addr, n1);
+        }
+      }
+      // the accumulators are rewritten by the next pass's first MMAs
+      tc_fence_before();
+      __syncthreads();
+      tc_fence_after();
+    }
+    if (bad_s) break;
+    if (seg == CH4_NSEG - 1) {
+      const float i2 = 1.f / (R * R);
+      const float i6 = i2 * i2 * i2;
+#pragma unroll
+      for (int cc = 0; cc < 3; ++cc) acc[cc] *= i6;
+    }
+    if (mine >= 0) {
+      float *o = a.mu + (size_t)mine * 4;
+#pragma unroll
+      for (int i = 0; i < 3; ++i) o[i] = M[i][0] * acc[0] + M[i][1] * acc[1] + M[i][2] * acc[2];
+    }
+  }
+  // a CTA that gave up waits (bounded) for the work it issued before freeing TMEM
+  if (bad_s && t == 0 && g > 0) {
+    mbar_wait(&bar_mma[(g - 1) & 1], ((g - 1) >> 1) & 1);
+    mbar_wait(&bar_load[g & 1], (g >> 1) & 1);
+  }
+  tc_fence_before();
+  __syncthreads();
+  tc_fence_after();
+  if (warp == 0)
+    asm volatile("tcgen05.dealloc.cta_group::1.sync.aligned.b32 %0, %1;" ::"r"(tmem), "r"(CH4TC_TMEM_COLS)
+                 : "memory");
+}
+
+}  // namespace hh

@@ -444,6 +444,32 @@ def moment_sums(ms: MoleculeSystem, params: CalcParams, temperatures: Sequence[f
     return sw, sw2
 
 
+INTEGRAND_M0 = _lib.HH_INTEGRAND_M0
+INTEGRAND_PF = _lib.HH_INTEGRAND_PF
+
+
+def c_mpi_perform_integration(ms: MoleculeSystem, integrand: int, params: CalcParams, Temperature: float,
+                              niterations: int, npoints: int, seed: int = 1) -> tuple[float, float]:
+    """VEGAS integral of integrand_M0 / integrand_pf (src/hep_hawaii.cpp:122-201, 332-389):
+    returns (m, q), the value and error before the driver's scaling."""
+    L = _bind(ms)
+    m, q = C.c_double(), C.c_double()
+    pc = params.to_c()
+    check(L.hh_cuda_vegas(C.byref(pc), int(integrand), float(Temperature), int(niterations), int(npoints),
+                          int(seed), C.byref(m), C.byref(q)))
+    return m.value, q.value
+
+
+def calculate_m0_vegas(ms: MoleculeSystem, params: CalcParams, Temperature: float, niterations: int = 12,
+                       npoints: int = 1000000, seed: int = 1) -> tuple[float, float]:
+    """The CALCULATION_PHASE_SPACE_M0 case of the reference driver (src/driver.c:3390-3447):
+    VEGAS M0 scaled by ZeroCoeff / analytic_full_partition_function_by_V; defaults
+    hep_m0_niterations = 12, hep_m0_npoints = 1e6."""
+    m, q = c_mpi_perform_integration(ms, INTEGRAND_M0, params, Temperature, niterations, npoints, seed)
+    s = ZeroCoeff / analytic_full_partition_function_by_V(ms, Temperature)
+    return m * s, q * s
+
+
 def moment_scale(params: CalcParams, moment: int = 0) -> float:
     """M = moment_scale * <w>: ZeroCoeff (SecondCoeff) * 4 pi (Rmax - Rmin)."""
     coeff = ZeroCoeff if moment == 0 else SecondCoeff

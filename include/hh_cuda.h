@@ -214,6 +214,22 @@ int hh_cuda_moment_sums(const hh_calc_params *p, const double *T, int nT, uint64
                         uint64_t sample_offset, uint64_t seed, int moment, int precision_mode,
                         double *sum_w, double *sum_w2);
 
+/* VEGAS integration of the reference's phase-space integrands:
+ * c_mpi_perform_integration(ms, integrand, params, T, niterations, npoints, &m, &q)
+ * (src/hep_hawaii.h:16, src/hep_hawaii.cpp:332-389, driven by src/driver.c:3390-3447 for
+ * M0).  integrand HH_INTEGRAND_M0 (integrand_M0, src/hep_hawaii.cpp:148-201) or
+ * HH_INTEGRAND_PF (integrand_pf, 122-146) over the unit hypercube through the
+ * reference's transform_variables map; niterations iterations of npoints samples
+ * each (Philox stream `seed`), the grid (128 bins per dimension) refined after every
+ * iteration by Lepage's algorithm (alpha 1.5); m and q are the 1/variance-weighted
+ * average of the iterations after the first and its error, in the reference's units
+ * before the driver's scaling (M0 = m * ZeroCoeff / pf_analytic).  FP64.  ATOM + ATOM
+ * and LINEAR_MOLECULE + ATOM systems; HH_E_UNSUPPORTED_SYSTEM for CH4-CO2. */
+#define HH_INTEGRAND_M0 0
+#define HH_INTEGRAND_PF 1
+int hh_cuda_vegas(const hh_calc_params *p, int integrand, double T, uint64_t niterations, uint64_t npoints,
+                  uint64_t seed, double *m, double *q);
+
 /* Allocation-free M0 (no counterpart in the reference).
  *
  * Same arguments, samples and results as hh_cuda_m0, but the call allocates no
@@ -267,10 +283,16 @@ int hh_cuda_debug_item_trace(uint32_t *out, uint64_t capacity_words);
  * intermolecular axis and the N2 axis) as the given precision path evaluates it,
  * into out[2 n]: the FP64 network, or the mixed path's FP32 table. */
 int hh_cuda_debug_n2ar_dipole(int precision, const double *R, const double *T, uint64_t n, double *out);
-/* Diagnostic (no counterpart in the reference): the records per lane that the
- * CH4-CO2 dipole kernel's tuner picked for the FP64 and the mixed path on the first
- * record-path call of this context (0 before that call). */
+/* Diagnostic (no counterpart in the reference): the CH4-CO2 dipole kernel variant
+ * that the tuner picked for the FP64 and the mixed path on the first record-path call
+ * of this context: records per lane (1, 2 or 4) of the CUDA-core kernel, -1 for the
+ * tensor-core kernel (mixed path only), 0 before that call. */
 int hh_cuda_debug_tuning(int *ch4_dip_s_fp64, int *ch4_dip_s_mixed);
+/* Tuning knob (no counterpart in the reference): fixes the CH4-CO2 dipole kernel
+ * variant of `precision` (values as above; 0 lets the tuner time them again on the
+ * next record-path call).  The environment variable HH_CH4_DIP_S (1, 2, 4 or "tc")
+ * fixes the first pick instead. */
+int hh_cuda_debug_set_ch4_dipole(int precision, int variant);
 
 /* Diagnostic (no counterpart in the reference): device time per kernel class.
  * While switched on, every kernel of the classes below is bracketed by CUDA events

@@ -1778,6 +1778,167 @@ int hho_m2(const hho_system *sys, const hho_params *p, const double *T, int nT,
 double hho_m0_scale(const hho_params *p) { return ZeroCoeff * 4.0 * M_PI * (p->Rmax - p->Rmin); }
 double hho_m2_scale(const hho_params *p) { return SecondCoeff * 4.0 * M_PI * (p->Rmax - p->Rmin); }
 
+/* ======================================================================== */
+/* VEGAS (c_mpi_perform_integration, src/hep_hawaii.cpp:332-389, through    */
+/* hep-mc 0.7, absent here): Lepage's algorithm (J. Comput. Phys. 27 (1978) */
+/* 192) restated.  The integrand and its unit-hypercube map follow          */
+/* integrand_M0 / integrand_pf and transform_variables                     */
+/* (src/hep_hawaii.cpp:8-201), including x[0] for both R and Phi.  Sample i */
+/* of iteration it draws Philox4x32-10 words at counter (id_lo, id_hi, b, 0),*/
+/* id = it * npoints + i, b = 0..2; u = (w + 1/2) 2^-32.                    */
+/* ======================================================================== */
+#define VG_NB 128
+#define VG_MAXD 10
+
+static double vg_integrand(const hho_system *sys, const hho_params *p, int integrand, double invkT,
+                           const double *x, int D) {
+    double qp[16], jac = 1.0;
+    qp[4] = 1.0 / x[0]; jac *= qp[4] * qp[4];
+    qp[5] = tan(M_PI * (x[5] - 0.5)); jac *= M_PI * (1.0 + qp[5] * qp[5]);
+    qp[0] = x[0] * 2.0 * M_PI; jac *= 2.0 * M_PI;
+    qp[1] = tan(M_PI * (x[1] - 0.5)); jac *= M_PI * (1.0 + qp[1] * qp[1]);
+    qp[2] = x[2] * M_PI; jac *= M_PI;
+    qp[3] = tan(M_PI * (x[3] - 0.5)); jac *= M_PI * (1.0 + qp[3] * qp[3]);
+    if (D == 10) {
+        qp[6] = x[6] * 2.0 * M_PI; jac *= 2.0 * M_PI;
+        qp[7] = tan(M_PI * (x[7] - 0.5)); jac *= M_PI * (1.0 + qp[7] * qp[7]);
+        qp[8] = x[8] * M_PI; jac *= M_PI;
+        qp[9] = tan(M_PI * (x[9] - 0.5)); jac *= M_PI * (1.0 + qp[9] * qp[9]);
+    }
+    double R = qp[4];
+    if (R < p->Rmin || R > p->Rmax) return 0.0;
+    double H = hho_hamiltonian(sys, qp);
+    if (p->pair_state == HHO_PS_FREE_AND_METASTABLE && H < 0.0) return 0.0;
+    if (p->pair_state == HHO_PS_BOUND && H > 0.0) return 0.0;
+    double dipsq = 1.0;
+    if (integrand == 0) {
+        double q[8], d[3];
+        extract_q(sys, qp, q);
+        hho_dipole(sys, q, d);
+        dipsq = d[0] * d[0] + d[1] * d[1] + d[2] * d[2];
+    }
+    return jac * dipsq * exp(-H * invkT);
+}
+
+typedef struct {
+    const hho_system *sys;
+    const hho_params *p;
+    int integrand, D;
+    double invkT;
+    uint64_t id0, begin, end, seed;
+    const double *edges;
+    double s, s2;
+    double *hist;
+} vg_job;
+
+static void *vg_worker(void *arg) {
+    vg_job *J = arg;
+    uint32_t key[2] = {(uint32_t)J->seed, (uint32_t)(J->seed >> 32)};
+    for (uint64_t i = J->begin; i < J->end; ++i) {
+        uint64_t id = J->id0 + i;
+        uint32_t w[12];
+        for (uint32_t c = 0; c < 3; ++c) {
+            uint32_t ctr[4] = {(uint32_t)id, (uint32_t)(id >> 32), c, 0u};
+            hho_philox4x32_10(ctr, key, w + 4 * c);
+        }
+        double x[VG_MAXD], wgt = 1.0;
+        int bin[VG_MAXD];
+        for (int d = 0; d < J->D; ++d) {
+            double u = ((double)w[d] + 0.5) / 4294967296.0;
+            double v = u * VG_NB;
+            int b = (int)v;
+            if (b > VG_NB - 1) b = VG_NB - 1;
+            const double *e = J->edges + d * (VG_NB + 1);
+            x[d] = e[b] + (v - b) * (e[b + 1] - e[b]);
+            wgt *= VG_NB * (e[b + 1] - e[b]);
+            bin[d] = b;
+        }
+        double F = vg_integrand(J->sys, J->p, J->integrand, J->invkT, x, J->D) * wgt;
+        J->s += F;
+        J->s2 += F * F;
+        if (F != 0.0)
+            for (int d = 0; d < J->D; ++d) J->hist[d * VG_NB + bin[d]] += F * F;
+    }
+    return NULL;
+}
+
+/* one refinement step per dimension: 3-point smoothing (2-point at the ends), the
+ * compression m_i = ((1 - r_i) / ln(1 / r_i))^alpha of the normalised r_i, and new
+ * edges at equal steps of the cumulative m */
+static void vg_refine(double *edges, const double *hist, int D, double alpha) {
+    for (int d = 0; d < D; ++d) {
+        const double *h = hist + d * VG_NB;
+        double *e = edges + d * (VG_NB + 1);
+        double sm[VG_NB], m[VG_NB], cum[VG_NB + 1], ne[VG_NB + 1], tot = 0.0, M = 0.0;
+        sm[0] = 0.5 * (h[0] + h[1]);
+        for (int i = 1; i < VG_NB - 1; ++i) sm[i] = (h[i - 1] + h[i] + h[i + 1]) / 3.0;
+        sm[VG_NB - 1] = 0.5 * (h[VG_NB - 2] + h[VG_NB - 1]);
+        for (int i = 0; i < VG_NB; ++i) tot += sm[i];
+        if (!(tot > 0.0)) continue;
+        for (int i = 0; i < VG_NB; ++i) {
+            double r = sm[i] / tot;
+            m[i] = (r > 0.0 && r < 1.0) ? pow((1.0 - r) / log(1.0 / r), alpha) : (r >= 1.0 ? 1.0 : 0.0);
+            M += m[i];
+        }
+        if (!(M > 0.0)) continue;
+        cum[0] = 0.0;
+        for (int i = 0; i < VG_NB; ++i) cum[i + 1] = cum[i] + m[i];
+        ne[0] = e[0];
+        ne[VG_NB] = e[VG_NB];
+        int j = 0;
+        for (int k = 1; k < VG_NB; ++k) {
+            double target = M * k / VG_NB;
+            while (j < VG_NB - 1 && cum[j + 1] < target) ++j;
+            double fr = m[j] > 0.0 ? (target - cum[j]) / m[j] : 0.0;
+            if (fr < 0.0) fr = 0.0;
+            if (fr > 1.0) fr = 1.0;
+            ne[k] = e[j] + fr * (e[j + 1] - e[j]);
+        }
+        memcpy(e, ne, sizeof ne);
+    }
+}
+
+int hho_vegas(const hho_system *sys, const hho_params *p, int integrand, double T, uint64_t niter,
+              uint64_t npoints, uint64_t seed, int nthreads, double *m, double *q) {
+    if (sys->system == HHO_SYS_CH4CO2 || niter == 0 || npoints < 2) return -1;
+    if (nthreads < 1) nthreads = 1;
+    if (nthreads > 256) nthreads = 256;
+    const int D = hho_qp_size(sys);
+    double edges[VG_MAXD * (VG_NB + 1)];
+    for (int d = 0; d < D; ++d)
+        for (int k = 0; k <= VG_NB; ++k) edges[d * (VG_NB + 1) + k] = (double)k / VG_NB;
+    double wsum = 0.0, wv = 0.0, v0 = 0.0, e0 = 0.0;
+    for (uint64_t it = 0; it < niter; ++it) {
+        pthread_t th[256];
+        vg_job jobs[256];
+        for (int t = 0; t < nthreads; ++t) {
+            jobs[t] = (vg_job){sys, p, integrand, D, HkT / T, it * npoints, npoints * t / nthreads,
+                               npoints * (t + 1) / nthreads, seed, edges, 0.0, 0.0,
+                               calloc(D * VG_NB, sizeof(double))};
+            pthread_create(&th[t], NULL, vg_worker, &jobs[t]);
+        }
+        double S = 0.0, S2 = 0.0, hist[VG_MAXD * VG_NB];
+        memset(hist, 0, sizeof hist);
+        for (int t = 0; t < nthreads; ++t) {
+            pthread_join(th[t], NULL);
+            S += jobs[t].s;
+            S2 += jobs[t].s2;
+            for (int i = 0; i < D * VG_NB; ++i) hist[i] += jobs[t].hist[i];
+            free(jobs[t].hist);
+        }
+        double n = (double)npoints, mean = S / n;
+        double var = (S2 / n - mean * mean);
+        if (var < 0.0) var = 0.0;
+        var /= (n - 1.0);
+        if (it == 0) { v0 = mean; e0 = sqrt(var); }
+        else if (var > 0.0) { wsum += 1.0 / var; wv += mean / var; }
+        if (it + 1 < niter) vg_refine(edges, hist, D, 1.5);
+    }
+    if (niter == 1 || !(wsum > 0.0)) { *m = v0; *q = e0; }
+    else { *m = wv / wsum; *q = sqrt(1.0 / wsum); }
+    return 0;
+}
+
 /* analytic_full_partition_function_by_V (src/hawaii.c:5071-5090) */
 double hho_analytic_pf(const hho_system *sys, double T) {
     if (sys->system == HHO_SYS_HEAR) return pow(2.0 * M_PI * sys->mu * T / HkT, 1.5);

@@ -155,6 +155,9 @@ int hho_m0(const hho_system *sys, const hho_params *p, const double *T, int nT,
            uint64_t n_samples, uint64_t seed, uint64_t offset, int nthreads,
            double *wsum, double *wsq);
 double hho_m0_scale(const hho_params *p);  /* ZeroCoeff * 4 pi (Rmax - Rmin) */
+/* ---- VEGAS of the reference's integrand_M0 (integrand 0) / integrand_pf (1) ---- */
+int hho_vegas(const hho_system *sys, const hho_params *p, int integrand, double T, uint64_t niter,
+              uint64_t npoints, uint64_t seed, int nthreads, double *m, double *q);
 /* ---- second moment on the same samples (momentum average at the sampled K) ---- */
 int hho_m2(const hho_system *sys, const hho_params *p, const double *T, int nT,
            uint64_t n_samples, uint64_t seed, uint64_t offset, int nthreads,

@@ -224,6 +224,26 @@ def m0(sysd, params, T, n_samples, seed, offset=0, nthreads=None):
     return ws, wq
 
 
+def vegas(sysd, params, integrand, T, niter, npoints, seed, nthreads=None):
+    """(m, q) of the VEGAS restatement (hho_vegas); integrand 0 = M0, 1 = partition function."""
+    L = lib()
+    L.hho_vegas.argtypes = [C.POINTER(System), C.POINTER(Params), C.c_int, C.c_double, C.c_uint64, C.c_uint64,
+                            C.c_uint64, C.c_int, C.POINTER(C.c_double), C.POINTER(C.c_double)]
+    m, q = C.c_double(), C.c_double()
+    rc = L.hho_vegas(C.byref(sysd), C.byref(params), int(integrand), float(T), int(niter), int(npoints), int(seed),
+                     nthreads or os.cpu_count(), C.byref(m), C.byref(q))
+    if rc:
+        raise ValueError("unsupported system or arguments")
+    return m.value, q.value
+
+
+def analytic_pf(sysd, T):
+    L = lib()
+    L.hho_analytic_pf.restype = C.c_double
+    L.hho_analytic_pf.argtypes = [C.POINTER(System), C.c_double]
+    return L.hho_analytic_pf(C.byref(sysd), float(T))
+
+
 def m0_scale(params):
     return lib().hho_m0_scale(C.byref(params))
 

@@ -173,3 +173,31 @@ def test_dipole_tuner_picks_a_candidate():
     assert L.hh_cuda_debug_tuning(C.byref(s64), C.byref(s32)) == 0
     assert s32.value in (1, 2, 4)
     np.testing.assert_allclose(c2, c1, rtol=0, atol=1e-12 * abs(c1[0]))
+
+
+@pytest.mark.parametrize("variant", [1, 2, 4, -1])
+def test_mixed_dipole_variants(variant):  # noqa: selected by -k variants
+    """Every variant of the FP32 record-path dipole (1, 2 or 4 records per lane on the
+    CUDA cores; -1: the tcgen05 tensor-core kernel, TF32 with a three-product split)
+    against the oracle: C(0) over 400 sampled configurations (every radial piece the
+    sampler reaches) within 2e-5, and a 600-trajectory C(t) within 1e-4 of C(0) of the
+    FP64 path on the same initial conditions."""
+    import hawaiihybrid_b200 as hh
+    from hawaiihybrid_b200 import _lib
+    ms = lib_system("ch4co2")
+    L = _lib.load()
+    assert L.hh_cuda_debug_set_ch4_dipole(1, variant) == 0
+    try:
+        qp, _ = O.sample(3, oracle_system("ch4co2"), oracle_params("ch4co2", 1, DT), 400.0, 400)
+        ref = O.correlation_sum(oracle_system("ch4co2"), oracle_params("ch4co2", 1, DT), qp)
+        c, _ = hh.correlation_from_initial_conditions(ms, lib_params("ch4co2", 1, DT), qp, 1)
+        assert abs(c[0] - ref[0]) <= 2e-5 * ref[0]
+        qp, _ = O.sample(11, oracle_system("ch4co2"), oracle_params("ch4co2", N, DT), 200.0, 600)
+        c64, _ = hh.correlation_from_initial_conditions(ms, lib_params("ch4co2", N, DT), qp, 0)
+        c32, _ = hh.correlation_from_initial_conditions(ms, lib_params("ch4co2", N, DT, mixed_tol=3e-8), qp, 1)
+        assert rel_to_c0(c32, c64) < 1e-4
+        s64, s32 = C.c_int(0), C.c_int(0)
+        assert L.hh_cuda_debug_tuning(C.byref(s64), C.byref(s32)) == 0
+        assert s32.value == variant
+    finally:
+        L.hh_cuda_debug_set_ch4_dipole(1, 0)

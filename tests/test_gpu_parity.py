@@ -290,3 +290,29 @@ def test_traj_tuning_picks_follow_the_same_steps(precision):
     for key, (s, c) in runs.items():
         np.testing.assert_array_equal(s, s0, err_msg=str(key))
         np.testing.assert_allclose(c, c0, rtol=0, atol=1e-11 * abs(c0[0]), err_msg=str(key))
+
+
+@pytest.mark.parametrize("name,integrand,T", [("hear", 0, 100.0), ("co2ar", 0, 100.0), ("co2ar", 1, 300.0),
+                                              ("n2ar", 0, 300.0)])
+def test_vegas_matches_oracle(name, integrand, T):
+    """VEGAS (c_mpi_perform_integration) on the device against the oracle's restatement on
+    the same Philox samples: six iterations of 40,000 points, the grid refined between
+    them; the grids differ only by the rounding of the per-bin sums."""
+    import hawaiihybrid_b200 as hh
+    ms = lib_system(name)
+    p = lib_params(name, 64, 100.0)
+    m, q = hh.c_mpi_perform_integration(ms, integrand, p, T, 6, 40_000, seed=11)
+    mr, qr = O.vegas(oracle_system(name), oracle_params(name, 64, 100.0), integrand, T, 6, 40_000, 11)
+    assert m > 0 and q > 0
+    np.testing.assert_allclose(m, mr, rtol=1e-8)
+    np.testing.assert_allclose(q, qr, rtol=1e-6)
+
+
+@pytest.mark.parametrize("name,published,rel", [("co2ar", 6.25651e-4, 0.01), ("hear", 2.08597e-6, 0.005)])
+def test_vegas_m0_published_values(name, published, rel):
+    """The reference driver's VEGAS M0 (12 iterations, 1e6 points, scaled by ZeroCoeff /
+    pf_analytic) at 100 K reproduces the published values within their accuracy."""
+    import hawaiihybrid_b200 as hh
+    ms = lib_system(name)
+    m0, err = hh.calculate_m0_vegas(ms, lib_params(name, 64, 100.0), 100.0, 12, 1_000_000, seed=3)
+    assert abs(m0 - published) <= rel * published + 3 * err

@@ -62,3 +62,22 @@ def test_m2_physics_anchor(name, T, Rmin, published, tol):
     m = O.m2_scale(p) * ws[0] / n
     err = O.m2_scale(p) * np.sqrt(wq[0] / n - (ws[0] / n) ** 2) / np.sqrt(n)
     assert abs(m - published) <= tol * published + 3 * err
+
+
+def test_oracle_vegas_reproduces_published_m0():
+    """The oracle's VEGAS restatement of c_mpi_perform_integration(INTEGRAND_M0) (Lepage's
+    grid refinement over the reference's transform_variables map), scaled like the driver
+    by ZeroCoeff / pf_analytic, reproduces the published VEGAS M0 at 100 K, and its
+    partition-function integral over the R shell matches the analytic value times the
+    shell volume (1 % at 300 K, where the well adds a little)."""
+    import math
+    from hawaiihybrid_b200 import hawaii as H
+    for name, published in (("co2ar", 6.25651e-4), ("hear", 2.08597e-6)):
+        sysd, p = oracle_system(name), oracle_params(name, 64, 100.0)
+        m, q = O.vegas(sysd, p, 0, 100.0, 12, 200_000, 1)
+        pf = O.analytic_pf(sysd, 100.0)
+        m0, e0 = m * H.ZeroCoeff / pf, q * H.ZeroCoeff / pf
+        assert abs(m0 - published) <= 0.01 * published + 3 * e0
+        mp, qp = O.vegas(sysd, p, 1, 300.0, 8, 100_000, 2)
+        shell = 4.0 * math.pi / 3.0 * (p.Rmax ** 3 - p.Rmin ** 3)
+        assert abs(mp / shell / O.analytic_pf(sysd, 300.0) - 1.0) < 0.01 + 3 * qp / mp
