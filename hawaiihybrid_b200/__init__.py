@@ -5,7 +5,7 @@ include/hh_cuda.h); `hawaii` mirrors the reference's host interface on top of it
 """
 from . import _lib
 from ._lib import HHError
-from .hawaii import (ATOM, LINEAR_MOLECULE, PAIR_STATE_ALL, PAIR_STATE_BOUND,
+from .hawaii import (ATOM, LINEAR_MOLECULE, LINEAR_MOLECULE_REQ_HALFINTEGER, LINEAR_MOLECULE_REQ_INTEGER, PAIR_STATE_ALL, PAIR_STATE_BOUND,
                      PAIR_STATE_FREE_AND_METASTABLE, PRECISION_FP64, PRECISION_MIXED, ROTOR,
                      SYSTEM_CH4_CO2, SYSTEM_CO2_AR, SYSTEM_HE_AR, SYSTEM_N2_AR, CalcParams, CFnc, CFncArray, MoleculeSystem,
                      SFnc, analytic_full_partition_function_by_V, calculate_correlation_and_save,

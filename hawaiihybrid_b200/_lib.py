@@ -46,8 +46,9 @@ EXPORTS = (
     "hh_cuda_shutdown", "hh_cuda_m0_noalloc", "hh_cuda_correlation_array", "hh_cuda_correlation_temperatures",
     "hh_cuda_prmu", "hh_cuda_debug_n2ar_dipole", "hh_cuda_m2", "hh_cuda_debug_tuning",
     "hh_cuda_debug_kernel_ms", "hh_cuda_debug_ch4co2_fold", "hh_cuda_moment_sums", "hh_cuda_debug_traj_tuning",
-    "hh_cuda_debug_set_ch4_dipole", "hh_cuda_vegas",
+    "hh_cuda_debug_set_ch4_dipole", "hh_cuda_vegas", "hh_cuda_set_requantization",
 )
+HH_REQ_NONE, HH_REQ_INTEGER, HH_REQ_HALFINTEGER = 0, 1, 2
 HH_INTEGRAND_M0 = 0
 HH_INTEGRAND_PF = 1
 # kernel classes of hh_cuda_debug_kernel_ms
@@ -67,6 +68,11 @@ class SystemDesc(C.Structure):
         ("monomer1_type", C.c_int), ("monomer2_type", C.c_int),
         ("II1", C.c_double * 3), ("II2", C.c_double * 3),
     ]
+
+
+class Requantization(C.Structure):
+    _fields_ = [("mode", C.c_int), ("torque_cache_len", C.c_size_t), ("torque_limit", C.c_double),
+                ("even_j_spin_weight", C.c_double), ("odd_j_spin_weight", C.c_double)]
 
 
 class CalcParamsC(C.Structure):
@@ -145,6 +151,7 @@ def load(path: str | None = None):
                                           C.c_int]
     L.hh_cuda_debug_ch4co2_fold.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.hh_cuda_debug_set_ch4_dipole.argtypes = [C.c_int, C.c_int]
+    L.hh_cuda_set_requantization.argtypes = [C.POINTER(Requantization)]
     L.hh_cuda_vegas.argtypes = [C.POINTER(CalcParamsC), C.c_int, C.c_double, C.c_uint64, C.c_uint64, C.c_uint64,
                                 C.POINTER(C.c_double), C.POINTER(C.c_double)]
     L.hh_cuda_debug_traj_tuning.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]

@@ -113,6 +113,7 @@ struct Ctx {
   unsigned char *d_ch4_tc = nullptr;  // coefficient images of the tensor-core dipole kernel
   int *d_ch4_tc_err = nullptr;        // set by that kernel when an mbarrier wait gave up
   int ch4_dip_s[2] = {0, 0};  // records per lane of the dipole kernel [FP64, mixed]; 0: not tuned yet
+  hh_requantization req{};  // PR_MU requantization of monomer 1 (hh_cuda_set_requantization)
   // trajectory launch picks per [system][FP64, mixed] (warps == 0: not tuned yet)
   TrajTune traj_tune[5][2] = {};
   DevBuf<double> tune_crln, tune_cnt;  // the autotuner's scratch C(t) and counters
@@ -389,9 +390,9 @@ int sample_into(const hh_calc_params *p, double T, uint64_t n, double *d_out, ui
 // cap / handoff_div items are open, then the solo kernel for the rest, where cap is
 // the solo kernel's warp slots.  With ev_split, events ev[4] (start), ev[5] (after the
 // bulk kernel) and ev[7] (end) are recorded for the autotuner.
-template <int SYS, typename PHYS, typename STG, bool COMP, int WARPS>
+template <int SYS, typename PHYS, typename STG, bool COMP, int WARPS, bool REQ = false>
 int launch_traj_w(const TrajParams &P, const TrajIO &io, int handoff_div, bool ev_split) {
-  auto kern = traj_kernel<SYS, PHYS, STG, COMP, false, WARPS>;
+  auto kern = traj_kernel<SYS, PHYS, STG, COMP, false, WARPS, REQ>;
   const size_t smem = traj_smem_bytes<SYS, PHYS, STG, WARPS>();
   if (smem > 48 * 1024) CK(cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
@@ -402,7 +403,7 @@ int launch_traj_w(const TrajParams &P, const TrajIO &io, int handoff_div, bool e
   if (need < grid) grid = (int)std::max(1LL, need);
   // the last open items (and all items of a launch that small) run one per warp
   // in the solo kernel, one state component per lane
-  auto solo = traj_kernel<SYS, PHYS, STG, COMP, true>;
+  auto solo = traj_kernel<SYS, PHYS, STG, COMP, true, traj_warps<PHYS>(), REQ>;
   constexpr int SOLO_THREADS = traj_threads<PHYS>();
   const size_t smem_solo = traj_smem_bytes<SYS, PHYS, STG>();
   if (smem_solo > 48 * 1024)
@@ -535,6 +536,23 @@ int launch_traj(const TrajParams &P, const TrajIO &io, int *grid_out) {
   const int w = tt.warps ? tt.warps : traj_warps<PHYS>();
   const int d = tt.handoff_div ? tt.handoff_div : 1;
   return launch_traj_pick<SYS, PHYS, STG, COMP>(P, io, w, d, false);
+}
+
+// PR_MU with requantization: the REQ kernels of the linear-monomer systems
+int run_traj_dispatch_req(int precision, const TrajParams &P, const TrajIO &io) {
+  const bool mixed = precision == HH_PRECISION_MIXED;
+  if (g.sys == SYS_N2AR) {
+    TrajIO io2 = io;
+    io2.dipnet = g.d_n2ar_fold;
+    io2.pesnet = mixed ? (const void *)g.d_n2ar_pes_f : (const void *)g.d_n2ar_pes_d;
+    io2.diptab = mixed ? g.d_n2ar_tab : nullptr;
+    return mixed ? launch_traj_w<SYS_N2AR, float, float, false, traj_warps<float>(), true>(P, io2, 1, false)
+                 : launch_traj_w<SYS_N2AR, double, double, false, traj_warps<double>(), true>(P, io2, 1, false);
+  }
+  if (g.sys == SYS_CO2AR)
+    return mixed ? launch_traj_w<SYS_CO2AR, float, float, false, traj_warps<float>(), true>(P, io, 1, false)
+                 : launch_traj_w<SYS_CO2AR, double, double, false, traj_warps<double>(), true>(P, io, 1, false);
+  return HH_E_UNSUPPORTED_SYSTEM;
 }
 
 int run_traj_dispatch(int precision, const TrajParams &P, const TrajIO &io) {
@@ -1435,6 +1453,7 @@ int hh_cuda_prmu(const hh_calc_params *p, double T, double R0, double approx_fre
                  size_t *n_freq, double *ntraj, hh_stats *stats) {
   if (!g.init) return HH_E_NOT_INITIALIZED;
   if (g.sys == SYS_CH4CO2) return HH_E_UNSUPPORTED_SYSTEM;
+  if (g.req.mode != HH_REQ_NONE && g.sys == SYS_HEAR) return HH_E_UNSUPPORTED_SYSTEM;
   int rc = check_params(p);
   if (rc) return rc;
   if (!(T > 0) || !(R0 > 0) || !(approx_freq_max > 0) || !nu || !sf || !n_freq || n_traj == 0 ||
@@ -1492,6 +1511,12 @@ int hh_cuda_prmu(const hh_calc_params *p, double T, double R0, double approx_fre
   P.noise_floor = 16.0 * 5.96e-8;
   P.inject_item = P.inject_k = -1;
   P.prmu = 1;
+  const bool req = g.req.mode != HH_REQ_NONE;
+  if (req) {
+    P.req_mode = g.req.mode;
+    P.req_len = (int)g.req.torque_cache_len;
+    P.req_limit = g.req.torque_limit;
+  }
   const int stride = (int)N + 1;
   const size_t ps = (precision_mode == HH_PRECISION_MIXED) ? sizeof(float) : sizeof(double);
   const size_t per_traj = (size_t)stride * 4 * ps + 2 * 2 * N * sizeof(double2) + 4 * sizeof(int);
@@ -1530,9 +1555,12 @@ int hh_cuda_prmu(const hh_calc_params *p, double T, double R0, double approx_fre
     io.rec_status = g.rec_status.p;
     io.dipnet = g.d_n2ar_fold;
     io.pesnet = (precision_mode == HH_PRECISION_MIXED) ? (const void *)g.d_n2ar_pes_f : (const void *)g.d_n2ar_pes_d;
-    rc = run_traj_dispatch(precision_mode, P, io);
+    rc = req ? run_traj_dispatch_req(precision_mode, P, io) : run_traj_dispatch(precision_mode, P, io);
     if (rc) return rc;
     PrmuPackArgs pa;
+    pa.req_mode = g.req.mode;
+    pa.even_w = g.req.even_j_spin_weight;
+    pa.odd_w = g.req.odd_j_spin_weight;
     pa.series = g.rec_mu.p;
     pa.len = g.rec_len.p;
     pa.status = g.rec_status.p;
@@ -2000,6 +2028,21 @@ int hh_cuda_debug_traj_tuning(int precision, int set_warps, int set_handoff_div,
   }
   if (warps) *warps = tt.warps;
   if (handoff_div) *handoff_div = tt.handoff_div;
+  return HH_OK;
+}
+
+int hh_cuda_set_requantization(const hh_requantization *r) {
+  if (!g.init) return HH_E_NOT_INITIALIZED;
+  if (!r || r->mode == HH_REQ_NONE) {
+    memset(&g.req, 0, sizeof g.req);
+    return HH_OK;
+  }
+  if (r->mode != HH_REQ_INTEGER && r->mode != HH_REQ_HALFINTEGER) return HH_E_INVALID_ARGUMENT;
+  if (r->torque_cache_len < 1 || r->torque_cache_len > 16383 || !(r->torque_limit > 0)) return HH_E_INVALID_ARGUMENT;
+  // spin weights only for half-integer requantization (src/hawaii.c:3579-3593)
+  if (r->mode == HH_REQ_INTEGER && (r->even_j_spin_weight > 0 || r->odd_j_spin_weight > 0))
+    return HH_E_INVALID_ARGUMENT;
+  g.req = *r;
   return HH_OK;
 }
 

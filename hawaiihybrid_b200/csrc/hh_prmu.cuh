@@ -21,6 +21,7 @@
 #include <stdint.h>
 
 #include "hh_consts.h"
+#include "hh_traj.cuh"
 
 namespace hh {
 
@@ -36,7 +37,26 @@ struct PrmuPackArgs {
   double coeff;               // SF_COEFF / mu
   double2 *z;                 // [2 traj][N]
   unsigned long long *counted;
+  // spin weights of a LINEAR_MOLECULE_REQ_HALFINTEGER monomer (src/hawaii.c:3575-3594):
+  // req_mode 2 and a positive weight select even_w / odd_w by the parity of
+  // round(j_ini - 1.5), j_ini the requantized initial |j|; otherwise weight 1
+  int req_mode;
+  double even_w, odd_w;
 };
+
+// the trajectory weight of PR_MU from the drawn linear-monomer phase point
+// (phi, p_phi, theta, p_theta at qp[6..9]): j_monomer (src/hawaii.c:398-431), then
+// the requantized length
+__device__ __forceinline__ double prmu_spin_weight(const PrmuPackArgs &a, const double *qp) {
+  if (a.req_mode != 2 || !(a.even_w > 0.0 || a.odd_w > 0.0)) return 1.0;
+  const double phi = qp[6], pphi = qp[7], th = qp[8], pth = qp[9];
+  const double ct = cos(th) / sin(th);
+  const double j0 = -pth * sin(phi) - pphi * cos(phi) * ct, j1 = pth * cos(phi) - pphi * sin(phi) * ct;
+  const double jl = sqrt(j0 * j0 + j1 * j1 + pphi * pphi);
+  const double jini = req_closest(2, jl);
+  const long long j_int = llround(jini - 1.5);
+  return (j_int % 2 == 0) ? a.even_w : a.odd_w;
+}
 
 template <typename PHYS>
 __global__ void __launch_bounds__(256) prmu_pack_kernel(PrmuPackArgs a) {
@@ -47,7 +67,7 @@ __global__ void __launch_bounds__(256) prmu_pack_kernel(PrmuPackArgs a) {
   const int st = a.status[2 * t];
   const bool include = (st & 15) == HH_ST_OK && ((st & 16) || a.allow_trunc);
   const double pr_mu = -a.qp[t * a.QP + 5];
-  const double sw = include ? sqrt(a.coeff * pr_mu) : 0.0;
+  const double sw = include ? sqrt(a.coeff * pr_mu * prmu_spin_weight(a, a.qp + t * a.QP)) : 0.0;
   if (j == 0 && include) atomicAdd(a.counted, 1ull);
   double d[3] = {0.0, 0.0, 0.0};
   if (include && j + 1 <= a.len[2 * t]) {

@@ -54,6 +54,11 @@ struct TrajParams {
   // PR_MU samples (src/hawaii.c:3661-3688): a NaN dipole leaves its sample at zero
   // and no other per-sample test runs; the branch ends after R > Rcut
   int prmu;
+  // PR_MU requantization of the linear monomer (REQ kernels only): 1 integer, 2
+  // half-integer angular momentum (LINEAR_MOLECULE_REQ_INTEGER / _HALFINTEGER), 0 none;
+  // the torque cache length and limit that switch it (src/hawaii.c:3604-3662)
+  int req_mode, req_len;
+  double req_limit;
 };
 
 struct TrajIO {
@@ -358,6 +363,28 @@ template <typename PHYS, typename STG, bool COMP, bool SOLO_ = false> struct N2A
   }
 };
 
+// find_closest_integer / find_closest_half_integer (src/hawaii.c:360-393): the
+// requantized |j| of the linear monomer.  The half-integer rule returns 0 below 0.25,
+// 0.5 below 1 (the nearer of 0.5 and 1.5) and floor(j) + 0.5 above (the nearer of
+// floor(j) + 0.5 and floor(j) + 1.5).
+__device__ __forceinline__ double req_closest(int mode, double j) {
+  if (mode == 1) return round(j);
+  if (j < 0.25) return 0.0;
+  if (j < 1.0) return 0.5;
+  return floor(j) + 0.5;
+}
+
+// trajectory_apply_requantization (src/trajectory.c:93-136) on the Cartesian angular
+// momentum j of the linear monomer: j scaled to the requantized length (the reference
+// scales p_phi and p_theta, to which j is linear; zero when |j| <= 1e-15)
+__device__ __forceinline__ void req_rescale(int mode, double &j0, double &j1, double &j2) {
+  const double jl = sqrt(j0 * j0 + j1 * j1 + j2 * j2);
+  const double s = jl > 1e-15 ? req_closest(mode, jl) / jl : 0.0;
+  j0 *= s;
+  j1 *= s;
+  j2 *= s;
+}
+
 // spherical phase point (reference layout, src/hawaii.h:210-284) -> Cartesian
 template <int SYS>
 __device__ __forceinline__ void qp_to_state(const double *qp, double *y) {
@@ -659,6 +686,10 @@ __device__ __noinline__ void item_setup(const Sys &sys, const TrajParams &P, con
     ch4co2_qp_to_state(qp, nullptr, y0);
   } else {
     qp_to_state<(N == 6) ? SYS_HEAR : SYS_CO2AR>(qp, y0);
+    // PR_MU requantization at the start of the trajectory (src/hawaii.c:3558): the
+    // switch is on when a trajectory starts
+    if constexpr (N == 12)
+      if (P.req_mode) req_rescale(P.req_mode, y0[9], y0[10], y0[11]);
   }
   double q0[Sys::NQ];
 #pragma unroll
@@ -740,13 +771,21 @@ template <int N, typename PHYS, typename STG> struct HandoffState {
   double t, h;
   PHYS mu0[3], curr;
   int item, k, since, total, flags;  // flags: rejected | exited << 1
+  int req;                           // requantization switch and torque runs (REQ kernels)
   unsigned steps, samples, t_begin;  // item trace so far
 };
 
 // ---------------------------------------------------------------------------
 // warp-synchronous persistent loop over half-trajectory items
 // ---------------------------------------------------------------------------
-template <class Sys, typename PHYS, typename STG>
+// REQ: PR_MU requantization of the linear monomer (src/hawaii.c:3604-3662,
+// src/trajectory.c:146-183).  Steps land on every sample time, where the reference's
+// make_step returns; at sample k the switch of sample k - 1 decides whether j is
+// requantized (and the stages restarted from the new state), then the torque |dj/dt|
+// at sample k enters the switch: on once the last req_len torques are all <= the
+// limit, off once they are all >= it.  The torque cache starts as zeros, i.e. with
+// req_len values below the limit.
+template <class Sys, typename PHYS, typename STG, bool REQ = false>
 __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, const TrajIO &io,
                                           WarpSamples<STG, PHYS, Sys::NQ> *ws_block) {
   constexpr int N = Sys::N;
@@ -771,6 +810,10 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
   int since = 0, total = 0;
   bool rejected = false;
   bool exited = false;  // the item ended by R > Rcut
+  // REQ: bit 0 the requantization switch, bits 1..15 the run of trailing torques <= the
+  // limit, bits 16..30 the run of trailing torques >= the limit (each capped at req_len)
+  int req = 0;
+  const int req_cap = REQ ? min(P.req_len, 16383) : 0;
   unsigned long long t_begin = 0ull;
   unsigned s0 = 0, m0 = 0;
   // the owner of the warp's item in solo mode (every other lane mirrors it); all
@@ -826,6 +869,7 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
     rejected = false;
     exited = false;
     curr = PHYS(0);
+    if constexpr (REQ) req = 1 | (req_cap << 1);
   };
   auto item_of = [&](unsigned idx) {
     return io.items ? io.items[idx] : (io.fwd_only ? 2 * (int)idx : (int)idx);
@@ -859,6 +903,7 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
           hs->since = since;
           hs->total = total;
           hs->flags = (rejected ? 1 : 0) | (exited ? 2 : 0);
+          hs->req = req;
           hs->steps = nsteps - s0;
           hs->samples = nsamp - m0;
           hs->t_begin = (unsigned)(t_begin & 0xffffffffu);
@@ -900,6 +945,7 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
           since = hs->since;
           total = hs->total;
           rejected = (hs->flags & 1) != 0;
+          req = hs->req;
           exited = (hs->flags & 2) != 0;
           s0 = nsteps - hs->steps;
           m0 = nsamp - hs->samples;
@@ -923,29 +969,41 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
     int status = -1;  // >= 0: this lane's item ended with that status this round
     int hard = 0;
     bool accepted = false;
+    bool landed = false;  // REQ: the step ends exactly at sample time k dt
     double h_taken = 0.0;
     if (active) {
       // 10 * spacing of doubles above t (t >= 0 and finite)
       const double min_step = 10.0 * (__longlong_as_double(__double_as_longlong(t) + 1) - t);
-      if (!(h >= min_step)) {
+      double h_att = h;
+      bool clamp = false;
+      if constexpr (REQ) {
+        const double to_k = double(k) * dt - t;
+        if (h_att >= to_k) {
+          h_att = to_k;
+          clamp = true;
+        }
+      }
+      if (!(h_att >= min_step)) {
         status = HH_ST_H_UNDERFLOW;
       } else {
         double err;
         if constexpr (Sys::SOLO)
-          err = step_attempt_cp<Sys, STG>(sys, P, K, y[0], h, y_new[0]);
+          err = step_attempt_cp<Sys, STG>(sys, P, K, y[0], h_att, y_new[0]);
         else
-          err = step_attempt<Sys, STG>(sys, P, K, y, h, y_new);
+          err = step_attempt<Sys, STG>(sys, P, K, y, h_att, y_new);
         nrhs += 12;
         if (err < 1.0) {
           double fac = (err == 0.0) ? 10.0 : fmin(10.0, 0.9 * inv_eighth_root(err));
           if (rejected) fac = fmin(1.0, fac);
           rejected = false;
-          h_taken = h;
-          h *= fac;
+          h_taken = h_att;
+          // a step shortened to land on a sample time keeps the longer proposal
+          h = clamp ? fmax(h, h_att * fac) : h_att * fac;
+          landed = clamp;
           accepted = true;
           ++nsteps;
         } else {
-          h *= fmax(0.2, 0.9 * inv_eighth_root(err));
+          h = h_att * fmax(0.2, 0.9 * inv_eighth_root(err));
           rejected = true;
           ++nrej;
         }
@@ -959,7 +1017,8 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
     // and all lanes evaluate the pooled (owner, k) jobs in chunks.  A sample
     // the reference would not have stored (after an R > Rcut exit or a
     // failure) is cut off per owner with an atomicMin on (end, reason).
-    bool pending = accepted && (double(k) * dt <= t + h_taken);
+    bool pending = accepted && (landed || double(k) * dt <= t + h_taken);
+    const double t_land = double(k) * dt;  // REQ: the sample time a landed step ends at
     if (__any_sync(FULL, pending)) {
       int cnt = 0;
       if (pending) {
@@ -967,7 +1026,14 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
         if constexpr (Sys::SOLO) {
           // this lane's component; published below by the lane that holds it
           STG Fc[7];
-          dense_stages_cp<Sys, STG>(sys, K, y[0], y_new[0], h_taken, Fc);
+          if constexpr (REQ) {
+            // the sample is the step's end point: y_old + dy at x = 1
+            Fc[0] = STG(y_new[0] - y[0]);
+#pragma unroll
+            for (int r = 1; r < 7; ++r) Fc[r] = STG(0);
+          } else {
+            dense_stages_cp<Sys, STG>(sys, K, y[0], y_new[0], h_taken, Fc);
+          }
 #pragma unroll
           for (int cq = 0; cq < Sys::NQ; ++cq)
             if (Sys::qidx(cq) == lane) {
@@ -976,14 +1042,24 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
               ws->qold[cq][0] = y[0];
             }
         } else {
-          dense_stages<Sys, STG>(sys, K, y, y_new, h_taken, F);
+          if constexpr (REQ) {
+#pragma unroll
+            for (int c = 0; c < Sys::NQ; ++c) {
+              F[0][c] = STG(y_new[Sys::qidx(c)] - y[Sys::qidx(c)]);
+#pragma unroll
+              for (int r = 1; r < 7; ++r) F[r][c] = STG(0);
+            }
+          } else {
+            dense_stages<Sys, STG>(sys, K, y, y_new, h_taken, F);
+          }
         }
-        nrhs += 3;
+        if (!REQ) nrhs += 3;
         ++ndense;
         const double t_new = t + h_taken;
         int kl = (int)fmin(floor(t_new / dt), double(P.N - 1));
         while (kl + 1 <= P.N - 1 && double(kl + 1) * dt <= t_new) ++kl;
         while (kl > k && double(kl) * dt > t_new) --kl;
+        if (REQ && landed) kl = k;
         cnt = owner ? kl - k + 1 : 0;  // solo mode: the owner's samples, evaluated by all lanes
         if (owner) {
           if constexpr (!Sys::SOLO) {
@@ -1168,7 +1244,54 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
 
     // ---- advance accepted lanes; close finished items ----
     if (active && status < 0 && accepted) {
-      t += h_taken;
+      if constexpr (REQ) {
+        if (landed) {
+          // torque |dj/dt| at the sample from f(y_new) (the potential depends on q only,
+          // so the rescale below leaves it unchanged)
+          double a[3];
+          if constexpr (Sys::SOLO) {
+#pragma unroll
+            for (int i = 0; i < 3; ++i) a[i] = double(__shfl_sync(FULL, K[12][0], Sys::MOM2 + i));
+          } else {
+#pragma unroll
+            for (int i = 0; i < 3; ++i) a[i] = double(K[12][Sys::MOM2 + i]);
+          }
+          const double tq = sqrt(a[0] * a[0] + a[1] * a[1] + a[2] * a[2]);
+          if (req & 1) {
+            // requantization with the switch of the previous sample, then the stages
+            // restart from the new state (CVodeReInit in make_step)
+            if constexpr (Sys::SOLO) {
+              double j[3];
+#pragma unroll
+              for (int i = 0; i < 3; ++i) j[i] = __shfl_sync(FULL, y_new[0], Sys::MOM2 + i);
+              req_rescale(P.req_mode, j[0], j[1], j[2]);
+#pragma unroll
+              for (int i = 0; i < 3; ++i)
+                if (comp == Sys::MOM2 + i) y_new[0] = j[i];
+              double yn[N];
+              STG f[N];
+#pragma unroll
+              for (int i = 0; i < N; ++i) yn[i] = __shfl_sync(FULL, y_new[0], i);
+              sys.rhs(yn, f);
+              K[12][0] = pick_component<N>(f, comp);
+            } else {
+              req_rescale(P.req_mode, y_new[Sys::MOM2], y_new[Sys::MOM2 + 1], y_new[Sys::MOM2 + 2]);
+              sys.rhs(y_new, K[12]);
+            }
+            nrhs += 1;
+          }
+          int le = (req >> 1) & 0x7fff, ge = (req >> 16) & 0x7fff;
+          le = tq <= P.req_limit ? min(le + 1, req_cap) : 0;
+          ge = tq >= P.req_limit ? min(ge + 1, req_cap) : 0;
+          int on = req & 1;
+          if (le >= P.req_len) on = 1;
+          else if (ge >= P.req_len) on = 0;
+          req = on | (le << 1) | (ge << 16);
+        }
+        t = landed ? t_land : t + h_taken;
+      } else {
+        t += h_taken;
+      }
 #pragma unroll
       for (int i = 0; i < NL; ++i) {
         y[i] = y_new[i];
@@ -1273,17 +1396,20 @@ constexpr size_t traj_smem_bytes() {
 }
 
 // SOLO: one item per warp (the solo kernel of the hand-off); WARPS: warps per block
-template <int SYS, typename PHYS, typename STG, bool COMP, bool SOLO = false, int WARPS = traj_warps<PHYS>()>
+// REQ: PR_MU requantization compiled in (linear-molecule systems only)
+template <int SYS, typename PHYS, typename STG, bool COMP, bool SOLO = false, int WARPS = traj_warps<PHYS>(),
+          bool REQ = false>
 __global__ void __launch_bounds__(32 * WARPS, TRAJ_MIN_BLOCKS)
     traj_kernel(TrajParams P, TrajIO io, const Co2arTablesGlobal *gtab) {
+  static_assert(!REQ || SYS == SYS_CO2AR || SYS == SYS_N2AR, "requantization of a linear monomer");
   extern __shared__ __align__(16) unsigned char smem_raw[];
-  if (SYS == SYS_HEAR) {
+  if constexpr (SYS == SYS_HEAR) {
     using Sys = HeArSys<PHYS, STG, COMP, SOLO>;
     Sys sys;
     sys.inv_mu = 1.0 / P.mu;
     auto *ws = reinterpret_cast<WarpSamples<STG, PHYS, Sys::NQ> *>(smem_raw);
     traj_body<Sys, PHYS, STG>(sys, P, io, ws);
-  } else if (SYS == SYS_CH4CO2) {
+  } else if constexpr (SYS == SYS_CH4CO2) {
     using Sys = Ch4Co2Sys<PHYS, STG, COMP, SOLO>;
     Sys sys;
     sys.inv_mu = 1.0 / P.mu;
@@ -1293,7 +1419,7 @@ __global__ void __launch_bounds__(32 * WARPS, TRAJ_MIN_BLOCKS)
     sys.lj = io.lj;
     auto *ws = reinterpret_cast<WarpSamples<STG, PHYS, Sys::NQ> *>(smem_raw);
     traj_body<Sys, PHYS, STG>(sys, P, io, ws);
-  } else if (SYS == SYS_N2AR) {
+  } else if constexpr (SYS == SYS_N2AR) {
     using Sys = N2ArSys<PHYS, STG, COMP, SOLO>;
     Sys sys;
     sys.inv_mu = 1.0 / P.mu;
@@ -1308,7 +1434,7 @@ __global__ void __launch_bounds__(32 * WARPS, TRAJ_MIN_BLOCKS)
     sys.dtab = static_cast<const float4 *>(io.diptab);
     auto *ws = reinterpret_cast<WarpSamples<STG, PHYS, Sys::NQ> *>(smem_raw + sizeof(N2arDipFold) +
                                                                    sizeof(N2arPesNet<PHYS>));
-    traj_body<Sys, PHYS, STG>(sys, P, io, ws);
+    traj_body<Sys, PHYS, STG, REQ>(sys, P, io, ws);
   } else {
     using Sys = Co2ArSys<PHYS, STG, COMP, SOLO>;
     Co2arTables<PHYS> *tb = reinterpret_cast<Co2arTables<PHYS> *>(smem_raw);
@@ -1319,7 +1445,7 @@ __global__ void __launch_bounds__(32 * WARPS, TRAJ_MIN_BLOCKS)
     sys.inv_II = 1.0 / P.II;
     sys.tb = tb;
     auto *ws = reinterpret_cast<WarpSamples<STG, PHYS, Sys::NQ> *>(smem_raw + smem_tables_bytes<PHYS>());
-    traj_body<Sys, PHYS, STG>(sys, P, io, ws);
+    traj_body<Sys, PHYS, STG, REQ>(sys, P, io, ws);
   }
 }
 

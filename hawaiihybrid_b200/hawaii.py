@@ -40,6 +40,8 @@ II_CO2 = m_O / 2.0 * l_CO2 * l_CO2
 # ---- MonomerType (src/hawaii.h:183-190) ----
 ATOM = 0
 LINEAR_MOLECULE = 4
+LINEAR_MOLECULE_REQ_INTEGER = 104
+LINEAR_MOLECULE_REQ_HALFINTEGER = 204
 ROTOR = 6
 
 # ---- PairState (src/hawaii.h:290-300) ----
@@ -79,6 +81,9 @@ class CalcParams:
     cf_filenames: Sequence[str] = ()
     # correlation_eval_zimmerman_trick instead of correlation_eval (BOUND pairs only)
     use_zimmermann_trick: bool = False
+    # PR_MU spin weights of a LINEAR_MOLECULE_REQ_HALFINTEGER monomer (src/hawaii.h:336-337)
+    even_j_spin_weight: float = 0.0
+    odd_j_spin_weight: float = 0.0
     # device-path knobs (no reference counterpart)
     mixed_tolerance: float = 1e-8
     max_steps: int = 50000
@@ -102,6 +107,9 @@ class MoleculeSystem:
     II2: tuple = (0.0, 0.0, 0.0)
     seed: int = 0
     device: int = 0
+    # Monomer fields of a requantized monomer 1 (src/hawaii.h:210-235)
+    torque_cache_len: int = 0
+    torque_limit: float = 0.0
 
     @property
     def QP_SIZE(self) -> int:
@@ -112,7 +120,8 @@ class MoleculeSystem:
         return self.QP_SIZE // 2
 
     def desc(self) -> _lib.SystemDesc:
-        return _lib.SystemDesc(self.system_id, self.mu, self.m1_type, self.m2_type,
+        # the device surfaces take the plain monomer types; requantization is set per call
+        return _lib.SystemDesc(self.system_id, self.mu, self.m1_type % 100, self.m2_type % 100,
                                (C.c_double * 3)(*self.II1), (C.c_double * 3)(*self.II2))
 
 
@@ -128,7 +137,7 @@ def init_ms(mu: float, t1: int, t2: int, II1: Optional[Sequence[float]], II2: Op
     if system_id is None:
         if t1 == ATOM and t2 == ATOM:
             system_id = SYSTEM_HE_AR
-        elif t1 == LINEAR_MOLECULE and t2 == ATOM:
+        elif t1 % 100 == LINEAR_MOLECULE and t2 == ATOM:
             system_id = SYSTEM_CO2_AR
         elif t1 == ROTOR and t2 == LINEAR_MOLECULE:
             system_id = SYSTEM_CH4_CO2
@@ -235,6 +244,11 @@ def prmu_iteration(ms: MoleculeSystem, params: CalcParams, Temperature: float, R
     (src/hawaii.c:3148-3978): returns (nu, sum over counted trajectories of
     SF_COEFF pR/mu sum_c |F_c|^2, counted trajectories, stats)."""
     L = _bind(ms)
+    mode = {LINEAR_MOLECULE_REQ_INTEGER: _lib.HH_REQ_INTEGER,
+            LINEAR_MOLECULE_REQ_HALFINTEGER: _lib.HH_REQ_HALFINTEGER}.get(ms.m1_type, _lib.HH_REQ_NONE)
+    req = _lib.Requantization(mode, int(ms.torque_cache_len), float(ms.torque_limit),
+                              float(params.even_j_spin_weight), float(params.odd_j_spin_weight))
+    check(L.hh_cuda_set_requantization(C.byref(req)))
     N = int(params.MaxTrajectoryLength)
     cap = N // 2 + 2
     nu = np.zeros(cap)
@@ -243,8 +257,11 @@ def prmu_iteration(ms: MoleculeSystem, params: CalcParams, Temperature: float, R
     ntraj = C.c_double()
     st = _lib.Stats()
     pc = params.to_c()
-    check(L.hh_cuda_prmu(C.byref(pc), Temperature, R0, approximate_frequency_max, int(allow_truncating), seed, n,
-                         precision, nu, sf, cap, C.byref(nf), C.byref(ntraj), C.byref(st)))
+    try:
+        check(L.hh_cuda_prmu(C.byref(pc), Temperature, R0, approximate_frequency_max, int(allow_truncating), seed,
+                             n, precision, nu, sf, cap, C.byref(nf), C.byref(ntraj), C.byref(st)))
+    finally:
+        L.hh_cuda_set_requantization(None)
     k = nf.value
     return nu[:k], sf[:k], ntraj.value, st
 

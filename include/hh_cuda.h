@@ -156,8 +156,33 @@ int hh_cuda_correlation_temperatures(const hh_calc_params *p, const double *T, i
                                      uint64_t n_per_T, int precision_mode, double *crln_sums,
                                      double *ntraj, hh_stats *stats);
 
+/* Requantization of monomer 1 in PR_MU (no effect on the other paths): the monomer
+ * types LINEAR_MOLECULE_REQ_INTEGER / LINEAR_MOLECULE_REQ_HALFINTEGER (src/hawaii.h:183-190)
+ * with the Monomer's torque_cache_len and torque_limit (src/hawaii.h:210-235) and
+ * CalcParams' even_j_spin_weight / odd_j_spin_weight (src/hawaii.h:336-337).  The
+ * linear monomer's |j| is requantized to the nearest integer (find_closest_integer) or
+ * half-integer (find_closest_half_integer, src/hawaii.c:360-393) when its trajectory
+ * starts and, while the switch is on, at every sample (trajectory_apply_requantization
+ * in make_step, src/trajectory.c:93-183); the torque at each sample switches it on
+ * after torque_cache_len torques <= torque_limit and off after as many >= it
+ * (src/hawaii.c:3604-3662).  Half-integer runs weight each trajectory by the even or
+ * odd spin weight of round(j_ini - 1.5) when either is positive.  A NULL argument or
+ * mode HH_REQ_NONE switches it off.  Linear-monomer systems (CO2-Ar, N2-Ar). */
+#define HH_REQ_NONE 0
+#define HH_REQ_INTEGER 1
+#define HH_REQ_HALFINTEGER 2
+typedef struct {
+    int mode;                   /* HH_REQ_* */
+    size_t torque_cache_len;    /* 1 .. 16383 */
+    double torque_limit;        /* a.u., > 0 */
+    double even_j_spin_weight;  /* HH_REQ_HALFINTEGER only; both <= 0: weight 1 */
+    double odd_j_spin_weight;
+} hh_requantization;
+int hh_cuda_set_requantization(const hh_requantization *r);
+
 /* PR_MU spectral function (calculate_spectral_function_using_prmu_representation_and_save,
- * src/hawaii.c:3148-3978) for monomers without requantization: n_traj phase points drawn as
+ * src/hawaii.c:3148-3978), with the requantization of hh_cuda_set_requantization when it is
+ * on: n_traj phase points drawn as
  * q_generator, R := R0, p_generator with pR made inward (no rejection step); each trajectory
  * is integrated forward with the dipole sampled at t = (k+1) dt, k = 0..N-1, until R > R0;
  * its Connes-apodized dipole components are Fourier transformed and

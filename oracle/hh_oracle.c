@@ -1449,6 +1449,186 @@ static void fft_backward(double *re, double *im, size_t L);
  * sf[i] += SF_COEFF pR/mu sum_c |F_c(i)|^2 for i < L.  A trajectory whose integration fails, or
  * that is still inside R0 after N samples (unless allow_trunc), is skipped and not counted.
  * qp_out (optional) receives the drawn phase points.  Returns the trajectories counted. */
+/* ---- requantization of the linear monomer in PR_MU ------------------------------- */
+/* find_closest_integer / find_closest_half_integer (src/hawaii.c:360-393) */
+static double req_closest_ref(int mode, double j) {
+    if (mode == 1) return round(j);
+    if (j < 0.25) return 0.0;
+    if (j < 1.0) return (fabs(j - 0.5) < fabs(j - 1.5)) ? 0.5 : 1.5;
+    double r = 0.0;
+    while (j - r >= 1.0) r += 1.0;
+    double lower = r + 0.5, higher = r + 1.5;
+    return (fabs(j - lower) < fabs(j - higher)) ? lower : higher;
+}
+
+/* j_monomer of the linear monomer at qp[6..9] = (phi, p_phi, theta, p_theta)
+ * (src/hawaii.c:398-431) */
+static double j_len(const double *qp) {
+    double phi = qp[6], pphi = qp[7], th = qp[8], pth = qp[9];
+    double j0 = -pth * sin(phi) - pphi * cos(phi) / tan(th);
+    double j1 = pth * cos(phi) - pphi * sin(phi) / tan(th);
+    return sqrt(j0 * j0 + j1 * j1 + pphi * pphi);
+}
+
+/* trajectory_apply_requantization (src/trajectory.c:93-136) */
+static void req_apply(int mode, double *qp) {
+    double jl = j_len(qp);
+    double s = (jl > 1e-15) ? req_closest_ref(mode, jl) / jl : 0.0;
+    qp[7] *= s;
+    qp[9] *= s;
+}
+
+/* torque_monomer (src/hawaii.c:433-472): |tau| from dV/dphi, dV/dtheta of monomer 1 */
+static double torque_len(const hho_system *sys, const double *qp) {
+    double q[8], dV[8];
+    extract_q(sys, qp, q);
+    hho_dpes(sys, q, dV);
+    double phi = qp[6], th = qp[8], dphi = dV[3], dth = dV[4];
+    double tx = sin(phi) * dth + cos(phi) / tan(th) * dphi;
+    double ty = -cos(phi) * dth + sin(phi) / tan(th) * dphi;
+    double tz = -dphi;
+    return sqrt(tx * tx + ty * ty + tz * tz);
+}
+
+/* one DOP853 step from (t, y, f) whose attempts are cut to end at t_land when they
+ * would pass it; *landed tells whether the accepted step ends there.  A cut step that
+ * is accepted keeps the longer of the current and the proposed next step. */
+static int dop853_step_land(integ *I, double t, const double *y, const double *f, double *h_io,
+                            double *h_taken, double K[16][NMAX], double *y_new, long *nrej, double t_land,
+                            int *landed) {
+    double h = *h_io;
+    for (;;) {
+        double h_att = h;
+        int clamp = 0;
+        if (h_att >= t_land - t) { h_att = t_land - t; clamp = 1; }
+        double hh = h_att, ht = 0.0;
+        long nr0 = *nrej;
+        int rc = dop853_step(I, t, y, f, &hh, &ht, K, y_new, nrej);
+        if (rc) return rc;
+        if (*nrej == nr0) {   /* accepted at the first attempt of size h_att */
+            *h_taken = h_att;
+            *h_io = clamp ? fmax(h, hh) : hh;
+            *landed = clamp;
+            return 0;
+        }
+        /* dop853_step shrank and retried internally; its accepted step is shorter
+         * than t_land - t, so the step did not land */
+        *h_taken = ht;
+        *h_io = hh;
+        *landed = 0;
+        return 0;
+    }
+}
+
+/* PR_MU branch with requantization (src/hawaii.c:3604-3700): steps land on every sample
+ * time; at sample k the switch of sample k - 1 requantizes j (and restarts the stages),
+ * the torque at the sample then updates the switch (on after `len` torques <= limit,
+ * off after `len` >= limit; the cache starts with zeros); the dipole is stored unless
+ * NaN, and the branch ends after R > Rcut */
+static int half_traj_req(const hho_system *sys, const hho_params *p, const double *y0, const hho_req *rq,
+                         double *vec, hho_traj_stats *st, int *exited) {
+    *exited = 0;
+    integ I = {sys, hho_qp_size(sys), p->rtol, p->atol, 0};
+    int n = I.n;
+    double y[NMAX], f[NMAX], y_new[NMAX], K[16][NMAX];
+    memcpy(y, y0, n * sizeof(double));
+    f_eval(&I, y, f);
+    double dt = p->sampling_time;
+    double h = initial_step(&I, y, f, dt * (double)(p->N - 1));
+    double t = 0.0;
+    size_t k = 1;
+    long since = 0;
+    int on = 1, le = rq->len, ge = 0;
+    int status = HHO_OK;
+    while (k < p->N) {
+        double ht;
+        int landed = 0;
+        int rc = dop853_step_land(&I, t, y, f, &h, &ht, K, y_new, &st->nrej, (double)k * dt, &landed);
+        if (rc) { status = rc; break; }
+        st->nsteps++;
+        if (landed) {
+            memcpy(f, K[12], n * sizeof(double));
+            double tq = torque_len(sys, y_new);
+            if (on) {
+                req_apply(rq->mode, y_new);
+                f_eval(&I, y_new, f);
+            }
+            le = (tq <= rq->limit) ? (le + 1 > rq->len ? rq->len : le + 1) : 0;
+            ge = (tq >= rq->limit) ? (ge + 1 > rq->len ? rq->len : ge + 1) : 0;
+            if (le >= rq->len) on = 1;
+            else if (ge >= rq->len) on = 0;
+            double q[8], d[3];
+            extract_q(sys, y_new, q);
+            hho_dipole(sys, q, d);
+            st->nsamples++;
+            t = (double)k * dt;
+            memcpy(y, y_new, n * sizeof(double));
+            since = 0;
+            if (!(isnan(d[0]) || isnan(d[1]) || isnan(d[2]))) {
+                for (int c = 0; c < 3; ++c) vec[3 * (long)k + c] = d[c];
+                if (y[4] > p->Rcut) { ++k; *exited = 1; break; }
+            }
+            ++k;
+        } else {
+            t += ht;
+            memcpy(y, y_new, n * sizeof(double));
+            memcpy(f, K[12], n * sizeof(double));
+            if (++since > p->max_steps) { status = HHO_ST_MAXSTEPS; break; }
+        }
+    }
+    st->nrhs += I.nrhs;
+    return status;
+}
+
+long hho_prmu_req(const hho_system *sys, const hho_params *p, double T, double R0, int allow_trunc,
+                  uint32_t seed, size_t n, const hho_req *rq, double *sf, size_t L, double *qp_out) {
+    hho_mt s;
+    hho_mt_seed(&s, seed);
+    const size_t N = p->N;
+    const int QP = hho_qp_size(sys);
+    const double SF_COEFF = Hartree * pow(ALU, 6) * ATU * R0 * R0 * p->sampling_time * p->sampling_time;
+    hho_params pp = *p;
+    pp.N = N + 1;
+    pp.Rcut = R0;
+    double *re = malloc(N * sizeof(double)), *im = malloc(N * sizeof(double));
+    double *vec = calloc(3 * (N + 1), sizeof(double));
+    memset(sf, 0, L * sizeof(double));
+    long counted = 0;
+    for (size_t t = 0; t < n; ++t) {
+        double qp[16];
+        int draws = 0;
+        gen_qp(&s, sys, p, T, qp, &draws, R0);
+        if (qp[5] > 0.0) qp[5] = -qp[5];
+        if (qp_out) memcpy(qp_out + t * QP, qp, QP * sizeof(double));
+        const double pr_mu = -qp[5] / sys->mu;
+        req_apply(rq->mode, qp);   /* the switch is on when the trajectory starts */
+        double w = 1.0;
+        if (rq->mode == 2 && (rq->even_w > 0.0 || rq->odd_w > 0.0)) {
+            int j_int = (int)round(j_len(qp) - 1.5);
+            w = (j_int % 2 == 0) ? rq->even_w : rq->odd_w;
+        }
+        hho_traj_stats st;
+        memset(&st, 0, sizeof st);
+        memset(vec, 0, 3 * (N + 1) * sizeof(double));
+        int exited = 0;
+        int status = half_traj_req(sys, &pp, qp, rq, vec, &st, &exited);
+        if (status != HHO_OK) continue;
+        if (!exited && !allow_trunc) continue;
+        for (int c = 0; c < 3; ++c) {
+            for (size_t j = 0; j < N; ++j) {
+                double r = (double)j / (double)N;
+                re[j] = vec[3 * (j + 1) + c] * (1.0 - r * r) * (1.0 - r * r);
+                im[j] = 0.0;
+            }
+            fft_backward(re, im, N);
+            for (size_t i = 0; i < L; ++i) sf[i] += SF_COEFF * pr_mu * (re[i] * re[i] + im[i] * im[i]) * w;
+        }
+        ++counted;
+    }
+    free(re); free(im); free(vec);
+    return counted;
+}
+
 long hho_prmu(const hho_system *sys, const hho_params *p, double T, double R0, int allow_trunc, uint32_t seed,
               size_t n, double *sf, size_t L, double *qp_out) {
     hho_mt s;

@@ -123,6 +123,11 @@ int hho_correlation_eval(const hho_system *sys, const hho_params *p, const doubl
                          double *crln, hho_traj_stats *st);
 /* PR_MU spectral function (src/hawaii.c:3148-3978), core: returns the trajectories counted,
  * sf[0..L) the unnormalised sum */
+/* requantization of the linear monomer in PR_MU: mode 1 integer, 2 half-integer; torque
+ * cache length and limit; even / odd spin weights (half-integer, both <= 0: weight 1) */
+typedef struct { int mode, len; double limit, even_w, odd_w; } hho_req;
+long hho_prmu_req(const hho_system *sys, const hho_params *p, double T, double R0, int allow_trunc,
+                  uint32_t seed, size_t n, const hho_req *rq, double *sf, size_t L, double *qp_out);
 long hho_prmu(const hho_system *sys, const hho_params *p, double T, double R0, int allow_trunc, uint32_t seed,
               size_t n, double *sf, size_t L, double *qp_out);
 /* correlation_eval_zimmerman_trick (src/hawaii.c:1888-2114) */

@@ -175,6 +175,23 @@ def prmu(sysd, params, T, R0, n, L, seed, allow_trunc=False, with_qp=False):
     return (sf, cnt, qp) if with_qp else (sf, cnt)
 
 
+class Req(C.Structure):
+    _fields_ = [("mode", C.c_int), ("len", C.c_int), ("limit", C.c_double), ("even_w", C.c_double),
+                ("odd_w", C.c_double)]
+
+
+def prmu_req(sysd, params, T, R0, n, L, seed, req, allow_trunc=False):
+    """PR_MU with requantization of the linear monomer: (unnormalised sf[0..L), counted)"""
+    Lb = lib()
+    Lb.hho_prmu_req.restype = C.c_long
+    Lb.hho_prmu_req.argtypes = [C.POINTER(System), C.POINTER(Params), C.c_double, C.c_double, C.c_int, C.c_uint32,
+                                C.c_size_t, C.POINTER(Req), _dp, C.c_size_t, C.c_void_p]
+    sf = np.zeros(L)
+    cnt = Lb.hho_prmu_req(C.byref(sysd), C.byref(params), T, R0, int(allow_trunc), seed, n, C.byref(req), sf, L,
+                          None)
+    return sf, cnt
+
+
 def correlation_parts(sysd, params, qp0):
     fw = np.zeros(params.N)
     bw = np.zeros(params.N)

@@ -61,3 +61,33 @@ def test_rejects_unsupported():
     ms = lib_system("ch4co2")
     with pytest.raises(hh.HHError):
         hh.prmu_iteration(ms, lib_params("ch4co2", 64, 200.0), 300.0, R0, 4, 100.0)
+
+
+@pytest.mark.parametrize("name,mode,even,odd", [("co2ar", 1, 0.0, 0.0), ("co2ar", 2, 1.0, 0.5),
+                                                ("n2ar", 2, 0.0, 0.0)])
+def test_requantized_spectrum_matches_oracle(name, mode, even, odd):
+    """PR_MU with a LINEAR_MOLECULE_REQ_INTEGER / _HALFINTEGER monomer (src/trajectory.c:93-136,
+    src/hawaii.c:3548-3662): the initial requantization, the torque-cache switch (5 samples,
+    limit 1e-7 a.u.) that requantizes |j| at every sample while the pair is apart, and the
+    half-integer spin weights, against the oracle's restatement in the reference's
+    spherical coordinates.  Both land their steps on the sample times."""
+    import hawaiihybrid_b200 as hh
+    from tests.helpers import II_CO2, II_N2, MU_CO2AR, MU_N2AR
+    N, dt, T, n, fmax, seed = 1024, 200.0, 300.0, 24, 500.0, 5
+    t1 = hh.LINEAR_MOLECULE_REQ_INTEGER if mode == 1 else hh.LINEAR_MOLECULE_REQ_HALFINTEGER
+    if name == "co2ar":
+        ms = hh.init_ms(MU_CO2AR, t1, hh.ATOM, (II_CO2, II_CO2), None, seed)
+    else:
+        ms = hh.init_ms(MU_N2AR, t1, hh.ATOM, (II_N2, II_N2), None, seed, system_id=hh.SYSTEM_N2_AR)
+    ms.torque_cache_len, ms.torque_limit = 5, 1e-7
+    p = lib_params(name, N, dt)
+    p.even_j_spin_weight, p.odd_j_spin_weight = even, odd
+    nu, sf, cnt, _ = hh.prmu_iteration(ms, p, T, R0, n, fmax, False, 0, seed=seed)
+    req = O.Req(mode, 5, 1e-7, even, odd)
+    ref, cnt_ref = O.prmu_req(oracle_system(name), oracle_params(name, N, dt), T, R0, n, sf.size, seed, req)
+    assert cnt == cnt_ref and cnt > 0
+    assert np.max(np.abs(sf - ref)) <= 1e-6 * np.max(np.abs(ref))
+    # requantization changes the spectrum against the plain monomer on the same draws
+    ms_plain = lib_system(name, seed)
+    _, sf0, _, _ = hh.prmu_iteration(ms_plain, lib_params(name, N, dt), T, R0, n, fmax, False, 0, seed=seed)
+    assert np.max(np.abs(sf0 - sf)) > 1e-4 * np.max(np.abs(sf0))
