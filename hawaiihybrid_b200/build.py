@@ -14,7 +14,9 @@ LIBDIR = os.path.join(PKG, "lib")
 LIB = os.path.join(LIBDIR, "libhh_cuda.so")
 NVCC = os.environ.get("NVCC", "/usr/local/cuda/bin/nvcc")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-O3"]
+# --split-compile=0: nvcc optimises the unit's kernels on every host core in parallel
+# (the register allocation of the trajectory kernels is the same as a serial build's)
+COMMON = ["-O3", "-lineinfo", "-std=c++17", "-Xcompiler", "-fPIC", "-Xptxas", "-O3", "--split-compile=0"]
 
 # translation units and their extra flags; the sampler keeps the reference's
 # arithmetic order (no FMA contraction) so initial conditions match it closely
