@@ -47,6 +47,7 @@ EXPORTS = (
     "hh_cuda_prmu", "hh_cuda_debug_n2ar_dipole", "hh_cuda_m2", "hh_cuda_debug_tuning",
     "hh_cuda_debug_kernel_ms", "hh_cuda_debug_ch4co2_fold", "hh_cuda_moment_sums", "hh_cuda_debug_traj_tuning",
     "hh_cuda_debug_set_ch4_dipole", "hh_cuda_vegas", "hh_cuda_set_requantization",
+    "hh_write_correlation_function_ext", "hh_write_spectral_function_ext",
 )
 HH_REQ_NONE, HH_REQ_INTEGER, HH_REQ_HALFINTEGER = 0, 1, 2
 HH_INTEGRAND_M0 = 0
@@ -157,7 +158,7 @@ def load(path: str | None = None):
     L.hh_cuda_debug_traj_tuning.argtypes = [C.c_int, C.c_int, C.c_int, C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.hh_cuda_shutdown.restype = None
     for name in EXPORTS:
-        if name not in ("hh_cuda_strerror", "hh_cuda_shutdown"):
+        if name not in ("hh_cuda_strerror", "hh_cuda_shutdown") and not name.startswith("hh_write_"):
             getattr(L, name).restype = C.c_int
     _lib = L
     return L

@@ -25,7 +25,7 @@ UNITS = [
     ("hh_sampler.cu", ["-fmad=false"]),
 ]
 # host-only units (the host compiler sees the generated tables as plain arrays)
-HOST_UNITS = ["hh_n2ar_host.cpp", "hh_ch4co2_host.cpp"]
+HOST_UNITS = ["hh_n2ar_host.cpp", "hh_ch4co2_host.cpp", "hh_writers.cpp"]
 CXX = os.environ.get("CXX", "g++")
 
 
@@ -68,7 +68,7 @@ def build(force: bool = False, verbose: bool = False, extra: list[str] | None = 
         subprocess.run(cmd, check=True)
         objs.append(obj)
     tmp = LIB + ".tmp"
-    cmd = [NVCC, *ARCH, "-shared", "-o", tmp, *objs, "-lcudart"]
+    cmd = [NVCC, *ARCH, "-shared", "-o", tmp, *objs, "-lcudart", "-lpthread"]
     subprocess.run(cmd, check=True)
     os.replace(tmp, LIB)
     for o in objs:

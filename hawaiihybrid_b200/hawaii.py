@@ -521,18 +521,38 @@ def _header(fp, kind: str, T: float, ntraj: float, n: int) -> None:
     fp.write(f"# {kind}: {n}\n")
 
 
-def write_correlation_function_ext(fp, cf: CFnc) -> int:
-    """Rewrite an open CF file (truncate, write, flush, fsync)."""
-    fp.seek(0)
-    fp.truncate(0)
-    if not cf.normalized and cf.ntraj <= 0:
-        raise ValueError(f"cannot normalize correlation function: trajectories count is {cf.ntraj:.2f}")
-    _header(fp, "MAXIMUM TRAJECTORY LENGTH", cf.Temperature, cf.ntraj, cf.len)
-    data = cf.data if cf.normalized else cf.data / cf.ntraj
-    fp.writelines(f"{t:.2f} {v:.10e}\n" for t, v in zip(cf.t, data))
+def _write_native(fp, entry: str, x: np.ndarray, data: np.ndarray, T: float, ntraj: float,
+                  normalized: bool) -> int:
+    """Run one of the library's writers (hh_write_*_ext) on the open Python file fp."""
+    if not normalized and ntraj <= 0:
+        raise ValueError(f"cannot normalize: trajectories count is {ntraj:.2f}")
     fp.flush()
-    os.fsync(fp.fileno())
-    return fp.tell()
+    libc = C.CDLL(None)
+    libc.fdopen.restype = C.c_void_p
+    libc.fdopen.argtypes = [C.c_int, C.c_char_p]
+    libc.fclose.argtypes = [C.c_void_p]
+    cfp = libc.fdopen(os.dup(fp.fileno()), b"w")
+    if not cfp:
+        raise OSError("fdopen failed")
+    try:
+        fn = getattr(_lib.load(), entry)
+        fn.restype = C.c_long
+        fn.argtypes = [C.c_void_p, _lib._dp, _lib._dp, C.c_size_t, C.c_double, C.c_double, C.c_int]
+        n = fn(cfp, np.ascontiguousarray(x, dtype=np.float64), np.ascontiguousarray(data, dtype=np.float64),
+               len(data), float(T), float(ntraj), int(bool(normalized)))
+    finally:
+        libc.fclose(cfp)
+    fp.seek(0, os.SEEK_END)
+    if n < 0:
+        raise HHError(int(n), "CF/SF writer failed")
+    return int(n)
+
+
+def write_correlation_function_ext(fp, cf: CFnc) -> int:
+    """Rewrite an open CF file (truncate, write, flush, fsync): the library's
+    hh_write_correlation_function_ext, the same bytes as the reference's writer."""
+    return _write_native(fp, "hh_write_correlation_function_ext", cf.t, cf.data, cf.Temperature, cf.ntraj,
+                         cf.normalized)
 
 
 def write_correlation_function(filename: str, cf: CFnc) -> int:
@@ -542,12 +562,8 @@ def write_correlation_function(filename: str, cf: CFnc) -> int:
 
 def write_spectral_function(filename: str, sf: SFnc) -> int:
     with open(filename, "w") as fp:
-        _header(fp, "SPECTRAL FUNCTION LENGTH", sf.Temperature, sf.ntraj, sf.len)
-        data = sf.data if sf.normalized else sf.data / sf.ntraj
-        fp.writelines(f"{n:.10f}   {v:.10e}\n" for n, v in zip(sf.nu, data))
-        fp.flush()
-        os.fsync(fp.fileno())
-        return fp.tell()
+        return _write_native(fp, "hh_write_spectral_function_ext", sf.nu, sf.data, sf.Temperature, sf.ntraj,
+                             sf.normalized)
 
 
 def _read_table(filename: str):

@@ -34,6 +34,7 @@
 
 #include <stddef.h>
 #include <stdint.h>
+#include <stdio.h>
 
 #ifdef __cplusplus
 extern "C" {
@@ -283,6 +284,17 @@ int hh_cuda_vegas(const hh_calc_params *p, int integrand, double T, uint64_t nit
 #define HH_M0_NOALLOC_SCRATCH_BYTES (8 * (1024 * 16 * 2 + 2 * HH_M0_NOALLOC_MAX_T))
 int hh_cuda_m0_noalloc(const hh_calc_params *p, const double *T, int nT, uint64_t n_samples,
                        uint64_t seed, int precision_mode, double *m, double *err);
+
+/* CF and SF text files: write_correlation_function_ext / write_spectral_function_ext
+ * (src/hawaii.c:4150-4284) with the same bytes (header, then "%.2f %.10e" or
+ * "%.10f   %.10e" lines; data divided by ntraj unless normalized), formatted in
+ * parallel on the host threads and written with one fwrite, then flushed and fsync'd.
+ * fp is an open stream; it is truncated first.  Returns the characters written or a
+ * negative HH_E_* code.  No device is needed. */
+long hh_write_correlation_function_ext(FILE *fp, const double *t, const double *data, size_t len,
+                                       double Temperature, double ntraj, int normalized);
+long hh_write_spectral_function_ext(FILE *fp, const double *nu, const double *data, size_t len,
+                                    double Temperature, double ntraj, int normalized);
 
 /* CF -> SF: apodizes cf in place (as the reference does), N a power of two. */
 int hh_cuda_idct_cf_to_sf(double *cf, size_t N, double dt, double *nu, double *sf);

@@ -64,3 +64,31 @@ def test_rotor_linear_partition_function_matches_reference_log():
                           (II_CO2, II_CO2, 0.0))
     assert ms.QP_SIZE == 16
     assert f"{hh.analytic_full_partition_function_by_V(ms, 100.0):.5e}" == "4.16497e+10"
+
+
+def test_native_writers_match_the_reference_format(tmp_path):
+    """hh_write_correlation_function_ext / hh_write_spectral_function_ext (the parallel
+    formatter of the library, no device needed) write the reference's bytes: its header
+    lines and one printf-formatted line per point, divided by ntraj unless normalized."""
+    import numpy as np
+    from hawaiihybrid_b200 import hawaii as H
+    rng = np.random.default_rng(3)
+    N = 10000
+    cf = H.CFnc(t=200.0 * np.arange(N), data=rng.standard_normal(N) * 1e-60, ntraj=1234.0, Temperature=300.0,
+                normalized=False)
+    p = tmp_path / "cf.txt"
+    n = H.write_correlation_function(str(p), cf)
+    lines = p.read_text().splitlines()
+    assert n == p.stat().st_size
+    assert lines[0] == "# HAWAII HYBRID v0.1" and lines[1].startswith("# Saved on ")
+    assert lines[2:5] == ["# TEMPERATURE: 300.00", "# AVERAGE OVER 1234.00 TRAJECTORIES",
+                          f"# MAXIMUM TRAJECTORY LENGTH: {N}"]
+    assert lines[5:] == ["%.2f %.10e" % (t, v / 1234.0) for t, v in zip(cf.t, cf.data)]
+    back = H.read_correlation_function(str(p))
+    np.testing.assert_allclose(back.data, cf.data / 1234.0, rtol=1e-10)
+    sf = H.SFnc(nu=np.linspace(0, 500, N), data=rng.random(N), ntraj=10.0, Temperature=150.0, normalized=True)
+    q = tmp_path / "sf.txt"
+    H.write_spectral_function(str(q), sf)
+    ls = q.read_text().splitlines()
+    assert ls[4] == f"# SPECTRAL FUNCTION LENGTH: {N}"
+    assert ls[5:] == ["%.10f   %.10e" % (a, b) for a, b in zip(sf.nu, sf.data)]
