@@ -782,7 +782,7 @@ int run_records_t(const TrajParams &P, const double *d_ic, uint64_t n, uint64_t 
           ta.max_tasks = max_tasks;
           ta.task_step = step;
           ta.err = g.d_ch4_tc_err;
-          ch4_dipole_tc_kernel<<<v.grid, CH4TC_M, v.smem, g.st>>>(ta);
+          ch4_dipole_tc_kernel<<<v.grid, CH4TC_THREADS, v.smem, g.st>>>(ta);
         }
       } else {
         da.max_tasks = max_tasks;
@@ -1302,6 +1302,27 @@ int hh_cuda_init(int device, const hh_system_desc *sys) {
     CK(cudaMemcpy(g.d_ch4_tc, tc_blob.data(), tc_blob.size() * sizeof(float), cudaMemcpyHostToDevice));
     CK(cudaMalloc(&g.d_ch4_tc_err, sizeof(int)));
     CK(cudaMemset(g.d_ch4_tc_err, 0, sizeof(int)));
+    // the harmonics' recurrence coefficients by (m, l) (hh_ch4co2_tc.cuh)
+    {
+      float alpha[CH4_L1 + 1][CH4_L1 + 1] = {}, beta[CH4_L1 + 1][CH4_L1 + 1] = {}, pmv[CH4_L1 + 1];
+      double pm = 1.0;
+      for (int m = 0; m <= CH4_L1; ++m) {
+        if (m > 0) pm = -pm * sqrt(double(2 * m - 1) / double(2 * m));
+        pmv[m] = (float)pm;
+        for (int l = m + 1; l <= CH4_L1; ++l) {
+          if (l == m + 1) {
+            alpha[m][l] = (float)sqrt(double(2 * m + 1));
+          } else {
+            const double id = 1.0 / sqrt(double(l * l - m * m));
+            alpha[m][l] = (float)(double(2 * l - 1) * id);
+            beta[m][l] = (float)(sqrt(double((l - 1) * (l - 1) - m * m)) * id);
+          }
+        }
+      }
+      CK(cudaMemcpyToSymbol(c_ch4tc_alpha, alpha, sizeof alpha));
+      CK(cudaMemcpyToSymbol(c_ch4tc_beta, beta, sizeof beta));
+      CK(cudaMemcpyToSymbol(c_ch4tc_pm, pmv, sizeof pmv));
+    }
     g.ch4_B = f.n_batch;
     g.ch4_groups = 0;
     for (size_t b = 0; b < B; ++b) g.ch4_groups += (f.bmeta[b] & 8u) ? 1 : 0;

@@ -9,13 +9,18 @@
 // records of one piece the inner sum is a GEMM
 //   T_c (128 x 196) = A (128 x 364) . B_c,p^T,   A[r, 4k + j] = Y2_k(r) x(r)^j,
 // run on the tensor cores in TF32 with a three-product split for FP32 accuracy
-// (A = A_hi + A_lo, B = B_hi + B_lo, T = A_hi B_hi + A_hi B_lo + A_lo B_hi: the
-// dropped A_lo B_lo is 2^-22 of a product).  The outer sum over n (196 FMAs per
-// component) and the rotation to the lab frame run on the CUDA cores from TMEM.
+// (A = A_hi + A_lo with A_hi the TF32 part the tensor core reads and A_lo = A - A_hi;
+// B = B_hi + B_lo rounded on the host; T = A_hi B_hi + A_hi B_lo + A_lo B_hi: the
+// dropped A_lo B_lo is about 2^-20 of a product).  The outer sum over n (196 FMAs per
+// component) and the rotation to the lab frame run on the CUDA cores from TMEM.  The
+// harmonics' recurrences take their integer-only square roots from constant tables,
+// so neither the split nor the recurrences use the transcendental pipe.
 //
-// Mapping (one CTA of 128 threads per SM, persistent over the 128-record tasks):
-//   - thread t owns record t of the task: geometry, Y2 (shared memory), x powers, and
-//     its row of A written into shared memory in the canonical no-swizzle K-major
+// Mapping (one CTA of 256 threads per SM, persistent over the 128-record tasks; two
+// warps per TMEM lane quadrant):
+//   - threads t and t + 128 own record t of the task: geometry, Y2 (shared memory), x
+//     powers, and its row of A (half the K columns each) written into shared memory in
+//     the canonical no-swizzle K-major
 //     layout (8-row x 16-byte core matrices; K-adjacent cores 128 B apart, 8-row
 //     groups 512 B apart);
 //   - K is walked in chunks of 16 (23 chunks for K = 368, the last 4 columns zero);
@@ -27,7 +32,8 @@
 //   - TMEM holds two 208-column accumulators: pass 0 computes components 0 and 1,
 //     pass 1 component 2 (the three would need 624 of the 512 columns);
 //   - after a pass thread t reads its TMEM lane (tcgen05.ld 32x32b) and forms
-//     sum_n Y1_n T[t, n] with Y1 generated by its recurrence in column order.
+//     sum_n Y1_n T[t, n] with Y1 generated by its recurrence in column order (pass 0:
+//     the two halves take one component each).
 // Every mbarrier wait is bounded: on a timeout the CTA records the error in *err,
 // stops issuing work, waits (bounded) for what it issued and frees its TMEM.
 #pragma once
@@ -74,11 +80,9 @@ __device__ __forceinline__ uint64_t ch4tc_desc(uint32_t saddr) {
 constexpr uint32_t CH4TC_IDESC = (1u << 4) | (2u << 7) | (2u << 10) | ((uint32_t)(CH4TC_N >> 3) << 17) |
                                  ((uint32_t)(CH4TC_M >> 4) << 24);
 
-__device__ __forceinline__ float tf32_round(float v) {
-  uint32_t r;
-  asm("cvt.rna.tf32.f32 %0, %1;" : "=r"(r) : "f"(v));
-  return __uint_as_float(r);
-}
+// the TF32 part the tensor core reads of an FP32 operand: its low 13 mantissa bits
+// cleared (one integer AND, no conversion instruction); v - tf32_hi(v) is exact in FP32
+__device__ __forceinline__ float tf32_hi(float v) { return __uint_as_float(__float_as_uint(v) & 0xFFFFE000u); }
 
 __device__ __forceinline__ void mbar_init(uint64_t *bar, unsigned count) {
   asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
@@ -142,10 +146,21 @@ __device__ __forceinline__ void tmem_ld16(uint32_t taddr, float (&v)[16]) {
   for (int i = 0; i < 16; ++i) v[i] = __uint_as_float(r[i]);
 }
 
+// Coefficients of the harmonics' recurrences, set once per context by the host: for
+// (l, m) with l > m the normalised three-term recurrence Q_l = alpha z Q_(l-1) -
+// beta Q_(l-2), i.e. alpha =
+// (2l - 1) / sqrt(l^2 - m^2), beta = sqrt((l - 1)^2 - m^2) / sqrt(l^2 - m^2) (alpha =
+// sqrt(2m + 1), beta = 0 at l = m + 1), and per m the factor pm_m of (x + i y)^m
+// (pm_0 = 1, pm_m = -pm_(m-1) sqrt((2m - 1) / 2m)): the recurrence of ch4_dipole_kernel
+// with its integer-only square roots taken out of the loop.
+__constant__ float c_ch4tc_alpha[CH4_L1 + 1][CH4_L1 + 1];  // [m][l]
+__constant__ float c_ch4tc_beta[CH4_L1 + 1][CH4_L1 + 1];
+__constant__ float c_ch4tc_pm[CH4_L1 + 1];
+
 // Y2 of the CO2 axis (x, y, z) in the CH4 frame into Y[idx * 128 + t], in the order of
 // ch4_y2: m = 0..12, l = m..12 even, cos then sin
 __device__ __forceinline__ void ch4tc_y2(float x, float y, float z, float *Y, int t) {
-  float C = 1.f, Sn = 0.f, pm = 1.f;
+  float C = 1.f, Sn = 0.f;
   int idx = 0;
 #pragma unroll 1
   for (int m = 0; m <= CH4_L2; ++m) {
@@ -153,32 +168,30 @@ __device__ __forceinline__ void ch4tc_y2(float x, float y, float z, float *Y, in
       const float c = C * x - Sn * y;
       Sn = C * y + Sn * x;
       C = c;
-      pm = -pm * sqrtf(float(2 * m - 1) / float(2 * m));
     }
+    const float pm = c_ch4tc_pm[m];
     float qa = 1.f, qb = 0.f;
 #pragma unroll 1
     for (int l = m; l <= CH4_L2; ++l) {
-      float q;
-      if (l == m) q = 1.f;
-      else if (l == m + 1) q = sqrtf(float(2 * m + 1)) * z;
-      else q = (float(2 * l - 1) * z * qa - sqrtf(float((l - 1) * (l - 1) - m * m)) * qb) / sqrtf(float(l * l - m * m));
-      if ((l & 1) == 0) {
-        Y[(idx++) * CH4TC_M + t] = pm * C * q;
-        if (m > 0) Y[(idx++) * CH4TC_M + t] = pm * Sn * q;
+      if (l > m) {
+        const float q = c_ch4tc_alpha[m][l] * z * qa - c_ch4tc_beta[m][l] * qb;
+        qb = qa;
+        qa = q;
       }
-      qb = qa;
-      qa = q;
+      if ((l & 1) == 0) {
+        Y[(idx++) * CH4TC_M + t] = pm * C * qa;
+        if (m > 0) Y[(idx++) * CH4TC_M + t] = pm * Sn * qa;
+      }
     }
   }
 }
 
 // sum_n Y1_n(n1) T[n] over the 196 columns at TMEM address `taddr` (this thread's
-// lane), Y1 generated in column order by the recurrence of ch4_dipole_kernel
+// lane), Y1 generated in column order (m-major, l = m..13, cos then sin)
 __device__ __forceinline__ float ch4tc_y1_dot(uint32_t taddr, const float n1[3]) {
   float acc = 0.f;
   float C = 1.f, Sn = 0.f, pm = 1.f, qa = 0.f, qb = 0.f;
   int m = 0, l = 0;
-  // position in the (m, l, cs) walk: the next Y1 value to produce
   bool sin_next = false;
   float ys_pending = 0.f;
 #pragma unroll 1
@@ -187,14 +200,14 @@ __device__ __forceinline__ float ch4tc_y1_dot(uint32_t taddr, const float n1[3])
     tmem_ld16(taddr + (uint32_t)c0, v);
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
-      if (c0 + i < CH4TC_NY1) {
+      const int c = c0 + i;
+      if (c < CH4TC_NY1) {
         float y;
         if (sin_next) {
           y = ys_pending;
           sin_next = false;
         } else {
-          // advance to (l, m): the first call starts at (0, 0)
-          if (c0 + i == 0) {
+          if (c == 0) {
             qa = 1.f;
             qb = 0.f;
           } else if (l == CH4_L1) {
@@ -203,16 +216,12 @@ __device__ __forceinline__ float ch4tc_y1_dot(uint32_t taddr, const float n1[3])
             const float cc = C * n1[0] - Sn * n1[1];
             Sn = C * n1[1] + Sn * n1[0];
             C = cc;
-            pm = -pm * sqrtf(float(2 * m - 1) / float(2 * m));
+            pm = c_ch4tc_pm[m];
             qa = 1.f;
             qb = 0.f;
           } else {
             ++l;
-            const float ca = float(2 * l - 1), cb = sqrtf(float((l - 1) * (l - 1) - m * m));
-            const float id = (l > m + 1) ? 1.f / sqrtf(float(l * l - m * m)) : 0.f;
-            const float c1 = sqrtf(float(2 * m + 1));
-            const float z = n1[2];
-            const float q = (l == m + 1) ? c1 * z : (ca * z * qa - cb * qb) * id;
+            const float q = c_ch4tc_alpha[m][l] * n1[2] * qa - c_ch4tc_beta[m][l] * qb;
             qb = qa;
             qa = q;
           }
@@ -229,7 +238,12 @@ __device__ __forceinline__ float ch4tc_y1_dot(uint32_t taddr, const float n1[3])
   return acc;
 }
 
-__global__ void __launch_bounds__(CH4TC_M, 1) ch4_dipole_tc_kernel(Ch4TcArgs a) {
+// 256 threads: two warps per TMEM lane quadrant.  Thread t works on record row = t % 128;
+// half = t / 128 splits the A rows' K columns (half 0: k = 4c, 4c + 1; half 1: 4c + 2,
+// 4c + 3) and the epilogue (pass 0: half h reads component h; pass 1: half 0).
+constexpr int CH4TC_THREADS = 2 * CH4TC_M;
+
+__global__ void __launch_bounds__(CH4TC_THREADS, 1) ch4_dipole_tc_kernel(Ch4TcArgs a) {
   extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
   unsigned char *smem = reinterpret_cast<unsigned char *>(
       (reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~uintptr_t(1023));
@@ -247,7 +261,9 @@ __global__ void __launch_bounds__(CH4TC_M, 1) ch4_dipole_tc_kernel(Ch4TcArgs a) 
   __shared__ uint32_t tmem_base_s;
   __shared__ int bad_s;
   __shared__ long long w0[CH4_NSEG + 1];
+  __shared__ float acc1_s[CH4TC_M];  // component 1 from half 1 to half 0
   const int t = threadIdx.x, warp = t >> 5;
+  const int row = t & (CH4TC_M - 1), half = t / CH4TC_M;
   for (int i = t; i <= CH4_NSEG; i += blockDim.x) w0[i] = a.warp0[i];
   if (t == 0) {
     mbar_init(&bar_load[0], 1);
@@ -304,7 +320,7 @@ __global__ void __launch_bounds__(CH4TC_M, 1) ch4_dipole_tc_kernel(Ch4TcArgs a) 
     const int seg = seg_of(w);
     // ---- this thread's record: geometry, Y2, powers of x ----
     const int first = a.sorted[w * CH4TC_M];
-    const int mine = a.sorted[w * CH4TC_M + t];
+    const int mine = a.sorted[w * CH4TC_M + row];
     const int src = mine >= 0 ? mine : first;
     const float *rec = a.records + (size_t)src * HH_REC_WORDS;
     float M[3][3], n1[3], n2[3];
@@ -326,7 +342,8 @@ __global__ void __launch_bounds__(CH4TC_M, 1) ch4_dipole_tc_kernel(Ch4TcArgs a) 
     const float x = R - float(a.centre[seg]);
     const float xp[4] = {1.f, x, x * x, x * x * x};
     __syncthreads();  // the previous task's last chunk no longer reads Y2s
-    ch4tc_y2(n2[0], n2[1], n2[2], Y2s, t);
+    if (half == 0) ch4tc_y2(n2[0], n2[1], n2[2], Y2s, row);
+    __syncthreads();
     float acc[3] = {0.f, 0.f, 0.f};
     for (int q = 0; q < 2; ++q) {
       const int ntile = q == 0 ? 2 : 1;
@@ -336,20 +353,21 @@ __global__ void __launch_bounds__(CH4TC_M, 1) ch4_dipole_tc_kernel(Ch4TcArgs a) 
         float *Ah = reinterpret_cast<float *>(stA[s][0]);
         float *Al = reinterpret_cast<float *>(stA[s][1]);
 #pragma unroll
-        for (int kq = 0; kq < 4; ++kq) {
+        for (int kh = 0; kh < 2; ++kh) {
+          const int kq = 2 * half + kh;
           const int k = 4 * c + kq;
-          const float y2 = (k < CH4_NY2) ? Y2s[k * CH4TC_M + t] : 0.f;
+          const float y2 = (k < CH4_NY2) ? Y2s[k * CH4TC_M + row] : 0.f;
           float4 hi, lo;
           float *ph = &hi.x, *pl = &lo.x;
 #pragma unroll
           for (int j = 0; j < 4; ++j) {
             const float v = y2 * xp[j];
-            const float h = tf32_round(v);
+            const float h = tf32_hi(v);
             ph[j] = h;
-            pl[j] = tf32_round(v - h);
+            pl[j] = v - h;
           }
-          *reinterpret_cast<float4 *>(Ah + ch4tc_img_off(t, 4 * kq)) = hi;
-          *reinterpret_cast<float4 *>(Al + ch4tc_img_off(t, 4 * kq)) = lo;
+          *reinterpret_cast<float4 *>(Ah + ch4tc_img_off(row, 4 * kq)) = hi;
+          *reinterpret_cast<float4 *>(Al + ch4tc_img_off(row, 4 * kq)) = lo;
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
@@ -405,11 +423,11 @@ __global__ void __launch_bounds__(CH4TC_M, 1) ch4_dipole_tc_kernel(Ch4TcArgs a) 
       __syncthreads();
       tc_fence_after();
       if (!bad_s) {
-        const uint32_t lane_addr = tmem + ((uint32_t)(warp * 32) << 16);
+        const uint32_t lane_addr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
         if (q == 0) {
-          acc[0] = ch4tc_y1_dot(lane_addr, n1);
-          acc[1] = ch4tc_y1_dot(lane_addr + CH4TC_COL1, n1);
-        } else {
+          acc[half] = ch4tc_y1_dot(lane_addr + (half ? CH4TC_COL1 : 0u), n1);
+          if (half) acc1_s[row] = acc[1];
+        } else if (half == 0) {
           acc[2] = ch4tc_y1_dot(lane_addr, n1);
         }
       }
@@ -419,13 +437,14 @@ __global__ void __launch_bounds__(CH4TC_M, 1) ch4_dipole_tc_kernel(Ch4TcArgs a) 
       tc_fence_after();
     }
     if (bad_s) break;
+    acc[1] = acc1_s[row];  // written before the pass-end barrier above
     if (seg == CH4_NSEG - 1) {
       const float i2 = 1.f / (R * R);
       const float i6 = i2 * i2 * i2;
 #pragma unroll
       for (int cc = 0; cc < 3; ++cc) acc[cc] *= i6;
     }
-    if (mine >= 0) {
+    if (half == 0 && mine >= 0) {
       float *o = a.mu + (size_t)mine * 4;
 #pragma unroll
       for (int i = 0; i < 3; ++i) o[i] = M[i][0] * acc[0] + M[i][1] * acc[1] + M[i][2] * acc[2];

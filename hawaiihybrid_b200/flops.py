@@ -6,7 +6,7 @@ formulas in csrc/hh_physics.cuh and csrc/hh_traj.cuh; the event counts (RHS
 evaluations, steps, dense-output steps, samples) are measured by the kernels.
 For the mixed path the work is split into the part done in FP32 (surfaces,
 stage sums, dense-output increments) and the part done in FP64 (state
-updates, error estimates and step control, kinematic terms).
+updates, error norm and step control, kinematic terms).
 """
 from __future__ import annotations
 
@@ -56,7 +56,7 @@ def per_event(system: str, mixed: bool = True) -> dict:
     n, nq = s["n"], s["nq"]
     comb_sum = sum(2 * k for k in _STAGE_NNZ) * n + 2 * _B_NNZ * n          # stage sums
     comb_upd = 2 * (len(_STAGE_NNZ) + 1) * n                                 # y + h*acc
-    err_sum = 2 * (_E5_NNZ + _E3_NNZ) * n                                  # error estimates (FP64)
+    err_sum = 2 * (_E5_NNZ + _E3_NNZ) * n                                  # error estimates (stage sums)
     err_fp64 = 8 * n + 20                                                    # scales, norm, controller
     dense_stage_sum = sum(2 * k for k in _EXTRA_NNZ) * n
     dense_stage_upd = 2 * len(_EXTRA_NNZ) * n
@@ -65,7 +65,7 @@ def per_event(system: str, mixed: bool = True) -> dict:
     sample_fp64 = nq + 8                                                     # state add, |r|, Rcut test
     return dict(
         rhs=s["rhs"], rhs_fp64_kin=s["rhs_fp64_kin"], dip=s["dip"],
-        step_sum=comb_sum, step_fp64=comb_upd + err_sum + err_fp64,
+        step_sum=comb_sum + err_sum, step_fp64=comb_upd + err_fp64,
         dense_sum=dense_stage_sum + dense_rows, dense_fp64=dense_stage_upd,
         sample=sample_interp + s["dip"] + 6, sample_fp64=sample_fp64,
     )
