@@ -286,8 +286,10 @@ def bench_ch4co2(args, hh, H, peaks):
            "mixed_traj_per_s": mixed, "plain_fp64_traj_per_s": plain, "speedup_same_K": mixed / plain,
            "mixed_ms": sm["total_ms"], "plain_ms": sp["total_ms"], "mixed_rtol": args.mixed_tol,
            "fp64_rtol": w["fp64_tol"], "kernel_launches": sm["n_kernel_launches"],
-           "stats_mixed": {k: sm[k] for k in ("n_candidates", "n_steps", "n_rhs", "n_samples", "n_failed",
-                                              "sample_ms", "traj_ms")},
+           "stats_mixed": {k: sm[k] for k in ("n_candidates", "n_steps", "n_rejected_steps", "n_rhs", "n_samples",
+                                              "n_failed", "sample_ms", "traj_ms")},
+           "stats_fp64": {k: sp[k] for k in ("n_steps", "n_rejected_steps", "n_rhs", "n_samples", "n_failed",
+                                             "sample_ms", "traj_ms")},
            "kernel_ms": {p: {k: v["ms"] for k, v in d.items() if v["launches"]} for p, d in kt.items()}}
     s64, s32 = C.c_int(0), C.c_int(0)
     _lib.check(_lib.load().hh_cuda_debug_tuning(C.byref(s64), C.byref(s32)))

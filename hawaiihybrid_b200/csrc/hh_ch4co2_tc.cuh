@@ -18,15 +18,16 @@
 //
 // Mapping (one CTA of 256 threads per SM, persistent over the 128-record tasks; two
 // warps per TMEM lane quadrant):
-//   - threads t and t + 128 own record t of the task: geometry, Y2 (shared memory), x
-//     powers, and its row of A (half the K columns each) written into shared memory in
-//     the canonical no-swizzle K-major
+//   - threads t and t + 128 own record t of the task: geometry, x powers, Y2 generated
+//     chunk by chunk from its recurrence (in registers), and its row of A (half the K
+//     columns each) written into shared memory in the canonical no-swizzle K-major
 //     layout (8-row x 16-byte core matrices; K-adjacent cores 128 B apart, 8-row
 //     groups 512 B apart);
 //   - K is walked in chunks of 16 (23 chunks for K = 368, the last 4 columns zero);
 //     the chunk's B_hi | B_lo image (built on the host in the same layout) arrives by
-//     one bulk copy (cp.async.bulk, this GPU's memory only, no multicast) into a
-//     double-buffered stage tracked by an mbarrier;
+//     one bulk copy (cp.async.bulk, this GPU's memory only, no multicast) into a ring
+//     of three stages tracked by mbarriers: the copy of chunk g + 1 is issued once
+//     chunk g - 2's MMAs are done, so two chunks of MMAs stay queued behind it;
 //   - thread 0 issues the tcgen05.mma instructions of a chunk (M = 128, N = 208, K = 8
 //     each) and commits them to the stage's mbarrier, which frees the stage;
 //   - TMEM holds two 208-column accumulators: pass 0 computes components 0 and 1,
@@ -48,8 +49,9 @@ namespace hh {
 
 constexpr int CH4TC_A_BYTES = CH4TC_M * CH4TC_KC * 4;    // one A image (hi or lo): 8 KB
 constexpr int CH4TC_STAGE_B = 2 * CH4TC_IMG0;            // B_hi | B_lo of the widest pass
-// dynamic shared memory: 2 stages x (A_hi, A_lo, B_hi | B_lo), Y2 of the task
-constexpr size_t CH4TC_SMEM = 2 * (2 * CH4TC_A_BYTES + CH4TC_STAGE_B) + (size_t)CH4_NY2 * CH4TC_M * 4 + 1024;
+constexpr int CH4TC_STAGES = 3;
+// dynamic shared memory: 3 stages x (A_hi, A_lo, B_hi | B_lo) = 204 KB, 1 KB alignment
+constexpr size_t CH4TC_SMEM = CH4TC_STAGES * (2 * CH4TC_A_BYTES + CH4TC_STAGE_B) + 1024;
 constexpr unsigned CH4TC_TMEM_COLS = 512;
 constexpr unsigned CH4TC_COL1 = 256;            // TMEM column of the second accumulator
 constexpr long long CH4TC_WAIT_LIMIT = 1LL << 24;  // polls of an mbarrier before giving up
@@ -157,34 +159,59 @@ __constant__ float c_ch4tc_alpha[CH4_L1 + 1][CH4_L1 + 1];  // [m][l]
 __constant__ float c_ch4tc_beta[CH4_L1 + 1][CH4_L1 + 1];
 __constant__ float c_ch4tc_pm[CH4_L1 + 1];
 
-// Y2 of the CO2 axis (x, y, z) in the CH4 frame into Y[idx * 128 + t], in the order of
-// ch4_y2: m = 0..12, l = m..12 even, cos then sin
-__device__ __forceinline__ void ch4tc_y2(float x, float y, float z, float *Y, int t) {
-  float C = 1.f, Sn = 0.f;
-  int idx = 0;
-#pragma unroll 1
-  for (int m = 0; m <= CH4_L2; ++m) {
-    if (m > 0) {
+// Y2 of the CO2 axis (x, y, z) in the CH4 frame, one value per next() in the order of
+// ch4_y2 (m = 0..12, l = m..12 even, cos then sin).  The state is the recurrence's at
+// the position (m, l) to visit next; the caller asks for at most CH4_NY2 values.
+struct Ch4TcY2Gen {
+  float x, y, z, C, Sn, pm, qa, qb, pend;
+  int m, l;
+  bool sin_next;
+  __device__ __forceinline__ void reset(float x_, float y_, float z_) {
+    x = x_;
+    y = y_;
+    z = z_;
+    C = 1.f;
+    Sn = 0.f;
+    pm = c_ch4tc_pm[0];
+    qa = 1.f;
+    qb = 0.f;
+    pend = 0.f;
+    m = 0;
+    l = 0;
+    sin_next = false;
+  }
+  __device__ __forceinline__ void advance() {
+    if (l == CH4_L2) {
+      ++m;
+      l = m;
       const float c = C * x - Sn * y;
       Sn = C * y + Sn * x;
       C = c;
-    }
-    const float pm = c_ch4tc_pm[m];
-    float qa = 1.f, qb = 0.f;
-#pragma unroll 1
-    for (int l = m; l <= CH4_L2; ++l) {
-      if (l > m) {
-        const float q = c_ch4tc_alpha[m][l] * z * qa - c_ch4tc_beta[m][l] * qb;
-        qb = qa;
-        qa = q;
-      }
-      if ((l & 1) == 0) {
-        Y[(idx++) * CH4TC_M + t] = pm * C * qa;
-        if (m > 0) Y[(idx++) * CH4TC_M + t] = pm * Sn * qa;
-      }
+      pm = c_ch4tc_pm[m];
+      qa = 1.f;
+      qb = 0.f;
+    } else {
+      ++l;
+      const float q = c_ch4tc_alpha[m][l] * z * qa - c_ch4tc_beta[m][l] * qb;
+      qb = qa;
+      qa = q;
     }
   }
-}
+  __device__ __forceinline__ float next() {
+    if (sin_next) {
+      sin_next = false;
+      return pend;
+    }
+    if (l & 1) advance();  // odd l carry no term; the next l is even
+    const float v = pm * C * qa;
+    if (m > 0) {
+      pend = pm * Sn * qa;
+      sin_next = true;
+    }
+    advance();
+    return v;
+  }
+};
 
 // sum_n Y1_n(n1) T[n] over the 196 columns at TMEM address `taddr` (this thread's
 // lane), Y1 generated in column order (m-major, l = m..13, cos then sin)
@@ -248,16 +275,10 @@ __global__ void __launch_bounds__(CH4TC_THREADS, 1) ch4_dipole_tc_kernel(Ch4TcAr
   unsigned char *smem = reinterpret_cast<unsigned char *>(
       (reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~uintptr_t(1023));
   // stage s: A_hi, A_lo, B (hi | lo)
-  unsigned char *stA[2][2], *stB[2];
-#pragma unroll
-  for (int s = 0; s < 2; ++s) {
-    unsigned char *base = smem + (size_t)s * (2 * CH4TC_A_BYTES + CH4TC_STAGE_B);
-    stA[s][0] = base;
-    stA[s][1] = base + CH4TC_A_BYTES;
-    stB[s] = base + 2 * CH4TC_A_BYTES;
-  }
-  float *Y2s = reinterpret_cast<float *>(smem + 2 * (2 * CH4TC_A_BYTES + CH4TC_STAGE_B));
-  __shared__ __align__(8) uint64_t bar_load[2], bar_mma[2];
+  constexpr size_t STAGE_BYTES = 2 * CH4TC_A_BYTES + CH4TC_STAGE_B;
+  auto stA = [&](int s, int lo) { return smem + (size_t)s * STAGE_BYTES + (size_t)lo * CH4TC_A_BYTES; };
+  auto stB = [&](int s) { return smem + (size_t)s * STAGE_BYTES + 2 * CH4TC_A_BYTES; };
+  __shared__ __align__(8) uint64_t bar_load[CH4TC_STAGES], bar_mma[CH4TC_STAGES];
   __shared__ uint32_t tmem_base_s;
   __shared__ int bad_s;
   __shared__ long long w0[CH4_NSEG + 1];
@@ -266,10 +287,10 @@ __global__ void __launch_bounds__(CH4TC_THREADS, 1) ch4_dipole_tc_kernel(Ch4TcAr
   const int row = t & (CH4TC_M - 1), half = t / CH4TC_M;
   for (int i = t; i <= CH4_NSEG; i += blockDim.x) w0[i] = a.warp0[i];
   if (t == 0) {
-    mbar_init(&bar_load[0], 1);
-    mbar_init(&bar_load[1], 1);
-    mbar_init(&bar_mma[0], 1);
-    mbar_init(&bar_mma[1], 1);
+    for (int s = 0; s < CH4TC_STAGES; ++s) {
+      mbar_init(&bar_load[s], 1);
+      mbar_init(&bar_mma[s], 1);
+    }
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     bad_s = 0;
   }
@@ -289,9 +310,11 @@ __global__ void __launch_bounds__(CH4TC_THREADS, 1) ch4_dipole_tc_kernel(Ch4TcAr
     while (s < CH4_NSEG - 1 && w0[s + 1] <= task) ++s;
     return s;
   };
-  // chunk sequence: g counts the chunks this CTA has issued; stage g & 1; the n-th
-  // completion of a stage's barriers belongs to its chunk g = 2 n + stage
-  unsigned g = 0;
+  // chunk sequence: g counts the chunks this CTA has walked; chunk g uses stage g % 3,
+  // and the n-th completion of a stage's barriers belongs to its chunk 3 n + stage.
+  // Thread 0 keeps gl (loads issued), gw (loads seen complete) and gm (chunks whose
+  // MMAs were committed) for the bounded drain after a timeout.
+  unsigned g = 0, gl = 0, gw = 0, gm = 0;
   // the chunk after (task, q, c) in this CTA's walk, for the B prefetch
   auto next_chunk = [&](long long task, int q, int c, long long &nt, int &nq, int &nc) -> bool {
     nt = task;
@@ -311,10 +334,13 @@ __global__ void __launch_bounds__(CH4TC_THREADS, 1) ch4_dipole_tc_kernel(Ch4TcAr
   auto issue_load = [&](long long task, int q, int c, int s) {
     const int seg = seg_of(task * a.task_step);
     const unsigned bytes = q == 0 ? 2 * CH4TC_IMG0 : 2 * CH4TC_IMG1;
-    ch4tc_load(stB[s], a.blob + ch4tc_blob_off(seg, q, c), bytes, &bar_load[s]);
+    ch4tc_load(stB(s), a.blob + ch4tc_blob_off(seg, q, c), bytes, &bar_load[s]);
   };
   long long task0 = blockIdx.x;
-  if (t == 0 && task0 < total) issue_load(task0, 0, 0, 0);
+  if (t == 0 && task0 < total) {
+    issue_load(task0, 0, 0, 0);
+    gl = 1;
+  }
   for (long long task = task0; task < total; task += gridDim.x) {
     const long long w = task * a.task_step;
     const int seg = seg_of(w);
@@ -341,22 +367,24 @@ __global__ void __launch_bounds__(CH4TC_THREADS, 1) ch4_dipole_tc_kernel(Ch4TcAr
     const float R = sqrtf(rec[0] * rec[0] + rec[1] * rec[1] + rec[2] * rec[2]);
     const float x = R - float(a.centre[seg]);
     const float xp[4] = {1.f, x, x * x, x * x * x};
-    __syncthreads();  // the previous task's last chunk no longer reads Y2s
-    if (half == 0) ch4tc_y2(n2[0], n2[1], n2[2], Y2s, row);
-    __syncthreads();
     float acc[3] = {0.f, 0.f, 0.f};
+    Ch4TcY2Gen y2g;
     for (int q = 0; q < 2; ++q) {
       const int ntile = q == 0 ? 2 : 1;
+      y2g.reset(n2[0], n2[1], n2[2]);
       for (int c = 0; c < CH4TC_NCHUNK; ++c, ++g) {
-        const int s = g & 1;
+        const int s = g % CH4TC_STAGES;
+        // Y2_k of the chunk's four k (both halves walk the recurrence; each uses two)
+        float y2c[4];
+#pragma unroll
+        for (int kq = 0; kq < 4; ++kq) y2c[kq] = (4 * c + kq < CH4_NY2) ? y2g.next() : 0.f;
         // ---- A chunk: row t, columns 16 c .. 16 c + 15 (k = 4 c .. 4 c + 3, j = 0..3) ----
-        float *Ah = reinterpret_cast<float *>(stA[s][0]);
-        float *Al = reinterpret_cast<float *>(stA[s][1]);
+        float *Ah = reinterpret_cast<float *>(stA(s, 0));
+        float *Al = reinterpret_cast<float *>(stA(s, 1));
 #pragma unroll
         for (int kh = 0; kh < 2; ++kh) {
           const int kq = 2 * half + kh;
-          const int k = 4 * c + kq;
-          const float y2 = (k < CH4_NY2) ? Y2s[k * CH4TC_M + row] : 0.f;
+          const float y2 = half ? y2c[2 + kh] : y2c[kh];
           float4 hi, lo;
           float *ph = &hi.x, *pl = &lo.x;
 #pragma unroll
@@ -372,13 +400,14 @@ __global__ void __launch_bounds__(CH4TC_THREADS, 1) ch4_dipole_tc_kernel(Ch4TcAr
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
         if (t == 0 && !bad_s) {
-          if (!mbar_wait(&bar_load[s], (g >> 1) & 1)) {
+          if (!mbar_wait(&bar_load[s], (g / CH4TC_STAGES) & 1)) {
             bad_s = 1;
             atomicExch(a.err, 1);
           } else {
+            gw = g + 1;
             tc_fence_after();
-            const uint32_t a_hi = smem_u32(stA[s][0]), a_lo = smem_u32(stA[s][1]);
-            const uint32_t b_hi = smem_u32(stB[s]);
+            const uint32_t a_hi = smem_u32(stA(s, 0)), a_lo = smem_u32(stA(s, 1));
+            const uint32_t b_hi = smem_u32(stB(s));
             const uint32_t b_lo = b_hi + (q == 0 ? CH4TC_IMG0 : CH4TC_IMG1);
 #pragma unroll 1
             for (int nt = 0; nt < ntile; ++nt) {
@@ -394,28 +423,30 @@ __global__ void __launch_bounds__(CH4TC_THREADS, 1) ch4_dipole_tc_kernel(Ch4TcAr
               }
             }
             ch4tc_commit(&bar_mma[s]);
-            // prefetch the next chunk's B into the other stage once its MMAs (chunk g - 1)
-            // are done
+            gm = g + 1;
+            // prefetch the next chunk's B into stage (g + 1) % 3 once that stage's last
+            // MMAs (chunk g - 2) are done; chunks g - 1 and g stay queued meanwhile
             long long nt_;
             int nq, nc;
             if (next_chunk(task, q, c, nt_, nq, nc)) {
-              const int s1 = s ^ 1;
-              if (g >= 1 && !mbar_wait(&bar_mma[s1], ((g - 1) >> 1) & 1)) {
+              const int s1 = (g + 1) % CH4TC_STAGES;
+              if (g >= 2 && !mbar_wait(&bar_mma[s1], ((g - 2) / CH4TC_STAGES) & 1)) {
                 bad_s = 1;
                 atomicExch(a.err, 1);
               } else {
                 issue_load(nt_, nq, nc, s1);
+                gl = g + 2;
               }
             }
           }
         }
-        // the other stage is free for the next chunk's A once thread 0 has seen
-        // chunk g - 1's MMAs complete (above)
+        // stage (g + 1) % 3 is free for the next chunk's A once thread 0 has seen chunk
+        // g - 2's MMAs complete (above)
         __syncthreads();
       }
       // ---- all MMAs of this pass done: read the accumulators ----
       if (t == 0 && !bad_s) {
-        if (!mbar_wait(&bar_mma[(g - 1) & 1], ((g - 1) >> 1) & 1)) {
+        if (!mbar_wait(&bar_mma[(g - 1) % CH4TC_STAGES], ((g - 1) / CH4TC_STAGES) & 1)) {
           bad_s = 1;
           atomicExch(a.err, 1);
         }
@@ -425,8 +456,9 @@ __global__ void __launch_bounds__(CH4TC_THREADS, 1) ch4_dipole_tc_kernel(Ch4TcAr
       if (!bad_s) {
         const uint32_t lane_addr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
         if (q == 0) {
-          acc[half] = ch4tc_y1_dot(lane_addr + (half ? CH4TC_COL1 : 0u), n1);
-          if (half) acc1_s[row] = acc[1];
+          const float v = ch4tc_y1_dot(lane_addr + (half ? CH4TC_COL1 : 0u), n1);
+          if (half) acc1_s[row] = v;
+          else acc[0] = v;
         } else if (half == 0) {
           acc[2] = ch4tc_y1_dot(lane_addr, n1);
         }
@@ -451,9 +483,9 @@ __global__ void __launch_bounds__(CH4TC_THREADS, 1) ch4_dipole_tc_kernel(Ch4TcAr
     }
   }
   // a CTA that gave up waits (bounded) for the work it issued before freeing TMEM
-  if (bad_s && t == 0 && g > 0) {
-    mbar_wait(&bar_mma[(g - 1) & 1], ((g - 1) >> 1) & 1);
-    mbar_wait(&bar_load[g & 1], (g >> 1) & 1);
+  if (bad_s && t == 0) {
+    if (gm > 0) mbar_wait(&bar_mma[(gm - 1) % CH4TC_STAGES], ((gm - 1) / CH4TC_STAGES) & 1);
+    for (unsigned h = gw; h < gl; ++h) mbar_wait(&bar_load[h % CH4TC_STAGES], (h / CH4TC_STAGES) & 1);
   }
   tc_fence_before();
   __syncthreads();
