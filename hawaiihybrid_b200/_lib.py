@@ -46,14 +46,14 @@ EXPORTS = (
     "hh_cuda_shutdown", "hh_cuda_m0_noalloc", "hh_cuda_correlation_array", "hh_cuda_correlation_temperatures",
     "hh_cuda_prmu", "hh_cuda_debug_n2ar_dipole", "hh_cuda_m2", "hh_cuda_debug_tuning",
     "hh_cuda_debug_kernel_ms", "hh_cuda_debug_ch4co2_fold", "hh_cuda_moment_sums", "hh_cuda_debug_traj_tuning",
-    "hh_cuda_debug_set_ch4_dipole", "hh_cuda_vegas", "hh_cuda_set_requantization",
+    "hh_cuda_debug_set_ch4_dipole", "hh_cuda_debug_set_defer", "hh_cuda_vegas", "hh_cuda_set_requantization",
     "hh_write_correlation_function_ext", "hh_write_spectral_function_ext",
 )
 HH_REQ_NONE, HH_REQ_INTEGER, HH_REQ_HALFINTEGER = 0, 1, 2
 HH_INTEGRAND_M0 = 0
 HH_INTEGRAND_PF = 1
 # kernel classes of hh_cuda_debug_kernel_ms
-HH_KT_NAMES = ("traj_bulk", "traj_solo", "ch4_dipole", "ch4_sort", "ch4_corr", "moment")
+HH_KT_NAMES = ("traj_bulk", "traj_solo", "ch4_dipole", "ch4_sort", "ch4_corr", "moment", "samples")
 HH_KT_COUNT = len(HH_KT_NAMES)
 
 
@@ -152,6 +152,7 @@ def load(path: str | None = None):
                                           C.c_int]
     L.hh_cuda_debug_ch4co2_fold.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.hh_cuda_debug_set_ch4_dipole.argtypes = [C.c_int, C.c_int]
+    L.hh_cuda_debug_set_defer.argtypes = [C.c_int, C.POINTER(C.c_int)]
     L.hh_cuda_set_requantization.argtypes = [C.POINTER(Requantization)]
     L.hh_cuda_vegas.argtypes = [C.POINTER(CalcParamsC), C.c_int, C.c_double, C.c_uint64, C.c_uint64, C.c_uint64,
                                 C.POINTER(C.c_double), C.POINTER(C.c_double)]
@@ -184,6 +185,15 @@ def ch4co2_fold_shape() -> tuple[int, int]:
     nb, ng = C.c_int(0), C.c_int(0)
     check(load().hh_cuda_debug_ch4co2_fold(C.byref(nb), C.byref(ng)))
     return nb.value, ng.value
+
+
+def defer_samples(mode: int = -1) -> int:
+    """Placement of the mixed path's sample dipoles (hh_cuda_debug_set_defer): 0 in the
+    trajectory kernel, 1 CO2-Ar deferred to the sample kernels, 2 CO2-Ar and N2-Ar;
+    -1 only reads it.  Returns the mode before the call."""
+    prev = C.c_int(0)
+    check(load().hh_cuda_debug_set_defer(int(mode), C.byref(prev)))
+    return prev.value
 
 
 def traj_tuning(precision: int, set_warps: int = 0, set_handoff_div: int = 0) -> tuple[int, int]:

@@ -17,6 +17,7 @@
 #include "hh_ch4co2_fold.h"
 #include "hh_co2ar_tables.h"
 #include "hh_consts.h"
+#include "hh_defer.cuh"
 #include "hh_fft.cuh"
 #include "hh_internal.h"
 #include "hh_m0.cuh"
@@ -139,6 +140,13 @@ struct Ctx {
   DevBuf<unsigned char> handoff;   // open items handed from the bulk to the solo kernel
   DevBuf<unsigned int> hcount;     // n_handoff, solo cursor, closed items
   DevBuf<uint4> trace;
+  // deferred samples (hh_defer.cuh): contexts and their count (+ the largest count of a
+  // call's launches), first/last sample value per context, per-item state
+  DevBuf<unsigned char> dctx, dvals, item_mu0;
+  DevBuf<unsigned long long> dcount;
+  DevBuf<int> item_status;
+  DevBuf<unsigned> item_fail;
+  double defer_est = 32.0;  // contexts per item, from the previous calls
   // CORRELATION_ARRAY weights [n][n_sat]: with ratios (C(t)) and without (nstar)
   DevBuf<double> sat_w, sat_wraw;
   // CH4-CO2 record path: sample records, their dipoles, the piece sort
@@ -485,6 +493,7 @@ int tune_traj(const TrajParams &P, const TrajIO &io, TrajTune *out) {
   Pt.inject_item = -1;
   auto run = [&](int w, int d, float *bulk_ms, float *all_ms) -> int {
     CK(cudaMemsetAsync(g.tune_cnt.p, 0, (16 + 2 * HH_ST_COUNT + 1) * sizeof(double), g.st));
+    if (t.ctx_count) CK(cudaMemsetAsync(t.ctx_count, 0, sizeof(unsigned long long), g.st));
     CK(cudaMemsetAsync(g.tune_crln.p, 0, (size_t)P.N * nsl * sizeof(double), g.st));
     int rc = launch_traj_pick<SYS, PHYS, STG, COMP>(Pt, t, w, d, true);
     if (rc) return rc;
@@ -519,6 +528,8 @@ int tune_traj(const TrajParams &P, const TrajIO &io, TrajTune *out) {
       }
     }
   }
+  // the timing runs' sample contexts are scratch
+  if (t.ctx_count) CK(cudaMemsetAsync(t.ctx_count, 0, sizeof(unsigned long long), g.st));
   out->warps = w_best;
   out->handoff_div = d_best;
   return HH_OK;
@@ -576,6 +587,78 @@ int run_traj_dispatch(int precision, const TrajParams &P, const TrajIO &io) {
   // which comes from the radial rows, and cost 12 % of the kernel's time
   if (precision == HH_PRECISION_MIXED) return launch_traj<SYS_CO2AR, float, float, false>(P, io, nullptr);
   return launch_traj<SYS_CO2AR, double, double, false>(P, io, nullptr);
+}
+
+// ---------------------------------------------------------------------------
+// deferred samples (hh_defer.cuh)
+// ---------------------------------------------------------------------------
+// the mixed path's plain C(t) of the systems with a surface dipole; records, series,
+// satellite temperatures, PR_MU and a failure injection with a soft status keep
+// in-kernel samples.  g_defer (hh_cuda_debug_set_defer; environment HH_DEFER_SAMPLES,
+// default 1): 0 in-kernel samples for every call, 1 deferred for CO2-Ar, 2 also N2-Ar.
+using DeferCtx = SampleCtx<float, 6>;
+constexpr size_t DEFER_CTX_BYTES = sizeof(DeferCtx) + 2 * sizeof(float);  // + first/last value
+int g_defer = [] {
+  const char *e = getenv("HH_DEFER_SAMPLES");
+  return e ? atoi(e) : 1;
+}();
+bool defer_eligible(int precision, const TrajParams &P, const TrajIO &io) {
+  const bool sys_ok = g.sys == SYS_CO2AR ? g_defer >= 1 : (g.sys == SYS_N2AR && g_defer >= 2);
+  return sys_ok && precision == HH_PRECISION_MIXED && io.n_sat == 0 && !io.series && !io.records && !P.prmu &&
+         (P.inject_item < 0 || P.inject_status >= HH_ST_NAN_DIPOLE);
+}
+
+// the sample kernels for the contexts of the launch just made with io; n_items and
+// items as io's; traj_base: io.ic's first trajectory in the call (for the fail list)
+template <int SYS>
+int run_deferred_sys(const TrajParams &P, const TrajIO &io, long long traj_base) {
+  DeferArgs a;
+  memset(&a, 0, sizeof a);
+  a.ctx = io.ctx;
+  a.ctx_count = io.ctx_count;
+  a.ctx_cap = io.ctx_cap;
+  a.items = io.items;
+  a.n_items = io.n_items;
+  a.item_status = io.item_status;
+  a.item_mu0 = io.item_mu0;
+  a.item_fail = g.item_fail.p + 2 * traj_base;
+  a.first_v = g.dvals.p;
+  a.last_v = g.dvals.p + io.ctx_cap * sizeof(float);
+  a.crln = io.crln;
+  a.traj_per_iter = io.traj_per_iter;
+  a.status_hist = io.status_hist;
+  a.fail_flag = io.fail_flag;
+  a.fail_list = io.fail_list;
+  a.fail_count = io.fail_count;
+  a.traj_base = traj_base;
+  a.peak = g.dcount.p + 1;
+  auto eval = defer_eval_kernel<SYS, float, float>;
+  const size_t smem = DeferSys<SYS, float, float>::smem();
+  if (smem > 48 * 1024) CK(cudaFuncSetAttribute(eval, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eval, DEFER_THREADS, smem));
+  const int grid = std::max(1, per_sm) * g.num_sms;
+  kt_begin();
+  eval<<<grid, DEFER_THREADS, smem, g.st>>>(a, P, io, g.d_tab);
+  CK(cudaGetLastError());
+  defer_jump_kernel<float, float, 6><<<8 * g.num_sms, DEFER_THREADS, 0, g.st>>>(a, P);
+  CK(cudaGetLastError());
+  defer_items_kernel<float><<<(unsigned)std::max(1, (io.n_items + DEFER_THREADS - 1) / DEFER_THREADS),
+                              DEFER_THREADS, 0, g.st>>>(a, P);
+  CK(cudaGetLastError());
+  kt_end(HH_KT_SAMPLES);
+  g_launches += 3;
+  return HH_OK;
+}
+
+int run_deferred(const TrajParams &P, const TrajIO &io, long long traj_base) {
+  if (g.sys == SYS_N2AR) {
+    TrajIO io2 = io;
+    io2.dipnet = g.d_n2ar_fold;
+    io2.diptab = g.d_n2ar_tab;
+    return run_deferred_sys<SYS_N2AR>(P, io2, traj_base);
+  }
+  return run_deferred_sys<SYS_CO2AR>(P, io, traj_base);
 }
 
 // device memory the CH4-CO2 record path may hold for one chunk of trajectories
@@ -909,6 +992,136 @@ int run_series_t(const TrajParams &P, const TrajIO &io0, const double *d_ic, uin
   return HH_OK;
 }
 
+// The plain C(t) launches of run_trajectories, then the replay of failed trajectories
+// (the reference drops a trajectory whose correlation_eval returns 1 while still
+// counting it: both branches are replayed with the opposite weight).  With deferred
+// samples the iterations go in launches whose sample contexts fit the buffer (at most
+// 32 GiB and 40 % of the free memory, or HH_DEFER_BUDGET_MB); a launch that wrote
+// more contexts than the buffer holds repeats the call with a larger estimate of
+// contexts per item (HH_DEFER_EST sets the first one), and a second overflow with
+// in-kernel samples.
+int run_plain(int precision, const TrajParams &P, const TrajIO &io0, uint64_t n, uint64_t per_iter,
+              uint64_t n_iter, int *nfail_out) {
+  const size_t N = (size_t)P.N;
+  const bool eligible = defer_eligible(precision, P, io0);
+  for (int attempt = 0;; ++attempt) {
+    const bool defer = eligible && attempt < 2;
+    if (attempt > 0) {
+      CK(cudaMemsetAsync(g.crln.p, 0, N * n_iter * sizeof(double), g.st));
+      CK(cudaMemsetAsync(g.counters.p, 0, 16 * sizeof(unsigned long long), g.st));
+      CK(cudaMemsetAsync(g.status_hist.p, 0, 2 * HH_ST_COUNT * sizeof(unsigned int), g.st));
+      CK(cudaMemsetAsync(g.fail_flag.p, 0, n * sizeof(int), g.st));
+      CK(cudaMemsetAsync(g.fail_count.p, 0, sizeof(int), g.st));
+    }
+    CK(cudaMemsetAsync(g.queue.p, 0, sizeof(unsigned int), g.st));
+    TrajIO io = io0;
+    unsigned long long cap = 0;
+    uint64_t it_launch = n_iter, items_launch = 2 * n;
+    if (defer) {
+      size_t free_b = 0, total_b = 0;
+      CK(cudaMemGetInfo(&free_b, &total_b));
+      double budget = std::min(32.0 * double(1ull << 30), 0.4 * double(free_b + g.dctx.cap + g.dvals.cap));
+      if (const char *eb = getenv("HH_DEFER_BUDGET_MB")) budget = std::max(1.0, atof(eb)) * double(1 << 20);
+      if (attempt == 0)
+        if (const char *ee = getenv("HH_DEFER_EST")) g.defer_est = std::max(0.01, atof(ee));
+      const double per_item = g.defer_est * double(DEFER_CTX_BYTES);
+      const uint64_t max_items = (uint64_t)std::max(1.0, budget / per_item);
+      it_launch = std::min<uint64_t>(n_iter, std::max<uint64_t>(1, max_items / (2 * per_iter)));
+      items_launch = 2 * std::min<uint64_t>(n, it_launch * per_iter);
+      cap = (unsigned long long)(g.defer_est * double(items_launch)) + 4096ull;
+      CK(g.dctx.ensure(cap * sizeof(DeferCtx)));
+      CK(g.dvals.ensure(cap * 2 * sizeof(float)));
+      CK(g.dcount.ensure(2));
+      CK(g.item_status.ensure(2 * n));
+      CK(g.item_mu0.ensure(2 * n * 4 * sizeof(float)));
+      CK(g.item_fail.ensure(2 * n));
+      CK(cudaMemsetAsync(g.item_fail.p, 0xff, 2 * n * sizeof(unsigned), g.st));
+      CK(cudaMemsetAsync(g.dcount.p, 0, 2 * sizeof(unsigned long long), g.st));
+      io.ctx = g.dctx.p;
+      io.ctx_count = g.dcount.p;
+      io.ctx_cap = cap;
+      io.item_status = g.item_status.p;
+      io.item_mu0 = g.item_mu0.p;
+    }
+    if (!defer) {
+      int rc = run_traj_dispatch(precision, P, io);
+      if (rc) return rc;
+    } else {
+      for (uint64_t i0 = 0; i0 < n_iter; i0 += it_launch) {
+        const uint64_t t0 = i0 * per_iter, t1 = std::min(n, (i0 + it_launch) * per_iter);
+        TrajIO il = io;
+        il.ic = io.ic + t0 * (uint64_t)g.QP;
+        il.n_items = (int)(2 * (t1 - t0));
+        il.crln = io.crln + i0 * N;
+        il.fail_flag = io.fail_flag + t0;
+        il.item_status = g.item_status.p + 2 * t0;
+        il.item_mu0 = g.item_mu0.p + 2 * t0 * 4 * sizeof(float);
+        il.item_trace = io.item_trace ? io.item_trace + 2 * t0 : nullptr;
+        if (i0 > 0) {
+          CK(cudaMemsetAsync(g.queue.p, 0, sizeof(unsigned int), g.st));
+          CK(cudaMemsetAsync(g.dcount.p, 0, sizeof(unsigned long long), g.st));
+        }
+        int rc = run_traj_dispatch(precision, P, il);
+        if (rc) return rc;
+        rc = run_deferred(P, il, (long long)t0);
+        if (rc) return rc;
+      }
+    }
+    int nfail = 0;
+    unsigned long long peak = 0;
+    CK(cudaMemcpyAsync(&nfail, g.fail_count.p, sizeof nfail, cudaMemcpyDeviceToHost, g.st));
+    if (defer) CK(cudaMemcpyAsync(&peak, g.dcount.p + 1, sizeof peak, cudaMemcpyDeviceToHost, g.st));
+    CK(cudaStreamSynchronize(g.st));
+    if (defer) {
+      const double per = double(peak) / double(std::max<uint64_t>(1, items_launch));
+      if (peak > cap) {
+        g.defer_est = std::max(2.0 * g.defer_est, 1.25 * per);
+        continue;
+      }
+      g.defer_est = std::max(8.0, 1.25 * per);
+    }
+    if (nfail > 0) {
+      std::vector<int> fl(nfail), it(2 * (size_t)nfail);
+      CK(cudaMemcpy(fl.data(), g.fail_list.p, nfail * sizeof(int), cudaMemcpyDeviceToHost));
+      for (int i = 0; i < nfail; ++i) {
+        it[2 * i] = 2 * fl[i];
+        it[2 * i + 1] = 2 * fl[i] + 1;
+      }
+      CK(g.items.ensure(it.size()));
+      CK(cudaMemcpyAsync(g.items.p, it.data(), it.size() * sizeof(int), cudaMemcpyHostToDevice, g.st));
+      CK(cudaMemsetAsync(g.queue.p, 0, sizeof(unsigned int), g.st));
+      TrajParams P2 = P;
+      P2.weight = -P.weight;
+      TrajIO io2 = io;
+      io2.items = g.items.p;
+      io2.n_items = (int)it.size();
+      io2.fail_flag = nullptr;
+      io2.counters = g.counters.p + 8;  // replay work is not counted twice
+      io2.status_hist = g.status_hist.p + HH_ST_COUNT;
+      io2.item_trace = nullptr;
+      if (defer) {
+        io2.ctx_cap = g.dctx.cap / sizeof(DeferCtx);
+        if (io2.ctx_cap > g.dvals.cap / (2 * sizeof(float))) io2.ctx_cap = g.dvals.cap / (2 * sizeof(float));
+        CK(cudaMemsetAsync(g.dcount.p, 0, 2 * sizeof(unsigned long long), g.st));
+      }
+      int rc = run_traj_dispatch(precision, P2, io2);
+      if (rc) return rc;
+      if (defer) {
+        rc = run_deferred(P2, io2, 0);
+        if (rc) return rc;
+        CK(cudaMemcpyAsync(&peak, g.dcount.p + 1, sizeof peak, cudaMemcpyDeviceToHost, g.st));
+        CK(cudaStreamSynchronize(g.st));
+        if (peak > io2.ctx_cap) {
+          g.defer_est *= 2.0;
+          continue;
+        }
+      }
+    }
+    *nfail_out = nfail;
+    return HH_OK;
+  }
+}
+
 // integrate both branches of n trajectories whose phase points are in d_ic;
 // trajectories [i*per_iter, (i+1)*per_iter) accumulate into C(t) slice i
 int run_trajectories(const hh_calc_params *p, const double *d_ic, uint64_t n, uint64_t per_iter,
@@ -1003,34 +1216,8 @@ int run_trajectories(const hh_calc_params *p, const double *d_ic, uint64_t n, ui
     CK(cudaMemcpyAsync(&nfail, g.fail_count.p, sizeof nfail, cudaMemcpyDeviceToHost, g.st));
     CK(cudaStreamSynchronize(g.st));
   } else {
-  int rc = run_traj_dispatch(precision, P, io);
-  if (rc) return rc;
-  CK(cudaMemcpyAsync(&nfail, g.fail_count.p, sizeof nfail, cudaMemcpyDeviceToHost, g.st));
-  CK(cudaStreamSynchronize(g.st));
-  if (nfail > 0) {
-    // the reference drops a trajectory whose correlation_eval returns 1 while
-    // still counting it; both branches are replayed with the opposite weight
-    std::vector<int> fl(nfail), it(2 * (size_t)nfail);
-    CK(cudaMemcpy(fl.data(), g.fail_list.p, nfail * sizeof(int), cudaMemcpyDeviceToHost));
-    for (int i = 0; i < nfail; ++i) {
-      it[2 * i] = 2 * fl[i];
-      it[2 * i + 1] = 2 * fl[i] + 1;
-    }
-    CK(g.items.ensure(it.size()));
-    CK(cudaMemcpyAsync(g.items.p, it.data(), it.size() * sizeof(int), cudaMemcpyHostToDevice, g.st));
-    CK(cudaMemsetAsync(g.queue.p, 0, sizeof(unsigned int), g.st));
-    TrajParams P2 = P;
-    P2.weight = -P.weight;
-    TrajIO io2 = io;
-    io2.items = g.items.p;
-    io2.n_items = (int)it.size();
-    io2.fail_flag = nullptr;
-    io2.counters = g.counters.p + 8;           // replay work is not counted twice
-    io2.status_hist = g.status_hist.p + HH_ST_COUNT;
-    io2.item_trace = nullptr;
-    rc = run_traj_dispatch(precision, P2, io2);
+    int rc = run_plain(precision, P, io, n, per_iter, n_iter, &nfail);
     if (rc) return rc;
-  }
   }
   CK(cudaEventRecord(g.ev[3], g.st));
   CK(cudaMemcpyAsync(crln_host, g.crln.p, N * n_iter * sizeof(double), cudaMemcpyDeviceToHost, g.st));
@@ -2074,6 +2261,13 @@ int hh_cuda_debug_set_ch4_dipole(int precision, int variant) {
   const bool ok = variant == 0 || variant == 1 || variant == 2 || (mixed && (variant == 4 || variant == CH4_DIP_TC));
   if (!ok) return HH_E_INVALID_ARGUMENT;
   g.ch4_dip_s[mixed ? 1 : 0] = variant;
+  return HH_OK;
+}
+
+int hh_cuda_debug_set_defer(int mode, int *previous) {
+  if (mode < -1 || mode > 2) return HH_E_INVALID_ARGUMENT;
+  if (previous) *previous = g_defer;
+  if (mode >= 0) g_defer = mode;
   return HH_OK;
 }
 

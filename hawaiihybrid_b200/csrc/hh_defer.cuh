@@ -1,0 +1,225 @@
+// Deferred sample evaluation of the plain C(t) path.
+//
+// The trajectory kernel runs at 8 warps per SM (its stage arrays fill the register
+// file), which leaves the dipole evaluation at the sample times latency-bound: a
+// dense-output step of a free-flight segment stores dozens of samples, each an
+// interpolation plus a surface evaluation of a few hundred dependent instructions.
+// With io.ctx set the kernel interpolates only r (for the reference's R > Rcut exit,
+// src/hawaii.c:2244) and writes one SampleCtx per dense-output step; the kernels here
+// then run the per-sample work at full occupancy:
+//   defer_eval_kernel   pooled (context, sample) pairs, 32 per warp round: y(t_k) from
+//                       the context, the dipole, mu0 . mu(t_k) into C(t_k), and the
+//                       reference's per-sample tests (src/hawaii.c:2183-2243: NaN
+//                       dipole, |value| > 1e100, |value / previous| > 1e10 for k > 1)
+//                       within the context, and the failure-injection hook of the
+//                       in-kernel path (hard statuses only); the first failure per item
+//                       is kept as (k << 3) | reason with atomicMin;
+//   defer_jump_kernel   the jump test across contexts (first sample of a context
+//                       against the last of the item's previous context);
+//   defer_items_kernel  per item: the status (a sample failure, else the integration's),
+//                       the t = 0 term |mu0|^2 of items that did not fail, and the
+//                       list of failed trajectories.
+// A failed trajectory is replayed with the opposite weight by the host, which
+// removes everything it added; the replay takes the same path, so its samples are
+// exactly those the first pass accumulated.  Samples after a failure are therefore
+// accumulated too (only NaN and |value| > 1e100 are skipped, in both passes), which
+// leaves C(t) as the in-kernel path makes it: failed trajectories contribute nothing.
+#pragma once
+
+#include <cuda_runtime.h>
+#include <math.h>
+#include <stdint.h>
+
+#include "hh_traj.cuh"
+
+namespace hh {
+
+constexpr int DEFER_THREADS = 256;
+
+struct DeferArgs {
+  const void *ctx;                      // SampleCtx<STG, NQ>[ctx_cap]
+  const unsigned long long *ctx_count;  // contexts written (may exceed ctx_cap)
+  unsigned long long ctx_cap;
+  const int *items;                     // defer_items_kernel: explicit item list or nullptr
+  int n_items;
+  const int *item_status;               // [item]
+  const void *item_mu0;                 // [item][4] PHYS: mu0, |mu0|^2
+  unsigned *item_fail;                  // [item] (k << 3) | reason of the first failure, ~0u none
+  void *first_v, *last_v;               // [ctx] PHYS: the context's first and last sample value
+  double *crln;                         // C(t) slices, traj_per_iter trajectories each
+  long long traj_per_iter;
+  unsigned int *status_hist;
+  int *fail_flag, *fail_list, *fail_count;  // fail_flag == nullptr: replay pass
+  long long traj_base;                  // the launch's first trajectory in the call (fail list)
+  unsigned long long *peak;             // largest context count of the call's launches
+};
+
+__device__ __forceinline__ unsigned long long defer_count(const DeferArgs &a) {
+  const unsigned long long c = *a.ctx_count;
+  return c < a.ctx_cap ? c : a.ctx_cap;
+}
+
+// the dipole of the bound system with its surfaces staged in shared memory
+template <int SYS, typename PHYS, typename STG> struct DeferSys;
+template <typename PHYS, typename STG> struct DeferSys<SYS_CO2AR, PHYS, STG> {
+  static constexpr int NQ = 6;
+  static constexpr size_t smem() { return smem_tables_bytes<PHYS>(); }
+  Co2ArSys<PHYS, STG, false, false> sys;
+  __device__ void init(unsigned char *sm, const Co2arTablesGlobal *gtab, const TrajIO &) {
+    auto *tb = reinterpret_cast<Co2arTables<PHYS> *>(sm);
+    load_tables<PHYS>(tb, gtab);
+    sys.tb = tb;
+  }
+};
+template <typename PHYS, typename STG> struct DeferSys<SYS_N2AR, PHYS, STG> {
+  static constexpr int NQ = 6;
+  static constexpr size_t smem() { return sizeof(N2arDipFold); }
+  N2ArSys<PHYS, STG, false, false> sys;
+  __device__ void init(unsigned char *sm, const Co2arTablesGlobal *, const TrajIO &io) {
+    auto *fold = reinterpret_cast<N2arDipFold *>(sm);
+    load_words(fold, io.dipnet, sizeof(N2arDipFold));
+    sys.fold = fold;
+    sys.pes = nullptr;
+    sys.dtab = static_cast<const float4 *>(io.diptab);
+  }
+};
+
+template <int SYS, typename PHYS, typename STG>
+__global__ void __launch_bounds__(DEFER_THREADS) defer_eval_kernel(DeferArgs a, TrajParams P, TrajIO io,
+                                                                   const Co2arTablesGlobal *gtab) {
+  using DS = DeferSys<SYS, PHYS, STG>;
+  constexpr int NQ = DS::NQ;
+  using Ctx = SampleCtx<STG, NQ>;
+  constexpr unsigned FULL = 0xffffffffu;
+  extern __shared__ __align__(16) unsigned char df_smem[];
+  DS ds;
+  ds.init(df_smem, gtab, io);
+  __syncthreads();
+  const unsigned long long count = defer_count(a);
+  const Ctx *ctx = static_cast<const Ctx *>(a.ctx);
+  const PHYS *mu0s = static_cast<const PHYS *>(a.item_mu0);
+  PHYS *first_v = static_cast<PHYS *>(a.first_v);
+  PHYS *last_v = static_cast<PHYS *>(a.last_v);
+  const int lane = threadIdx.x & 31;
+  const unsigned long long gw = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const unsigned long long nw = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
+  for (unsigned long long base = gw * 32; base < count; base += nw * 32) {
+    // the warp's 32 contexts and the prefix sum of their sample counts
+    const unsigned long long ci = base + lane;
+    const int n = ci < count ? ctx[ci].n : 0;
+    int incl = n;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+      const int v = __shfl_up_sync(FULL, incl, o);
+      if (lane >= o) incl += v;
+    }
+    const int off = incl - n;
+    const int total = __shfl_sync(FULL, incl, 31);
+    PHYS tail = PHYS(0);  // the last sample of the previous round
+    for (int j0 = 0; j0 < total; j0 += 32) {
+      const int j = j0 + lane;
+      int o = 0;  // owner: the largest lane whose offset is <= j
+#pragma unroll
+      for (int step = 16; step > 0; step >>= 1) {
+        const int oc = __shfl_sync(FULL, off, o + step);
+        if (oc <= j) o += step;
+      }
+      const int jj = j - __shfl_sync(FULL, off, o);
+      const bool valid = j < total;
+      PHYS v = PHYS(0);
+      bool nan = false;
+      int kk = 0, item = 0, nn = 0;
+      if (valid) {
+        const Ctx &c = ctx[base + o];
+        item = c.item;
+        nn = c.n;
+        kk = c.k0 + jj;
+        const double x = (double(kk) * P.dt - c.t0) * c.inv_h;
+        const STG xs = STG(x), x1 = STG(1) - STG(x);
+        double q[NQ];
+#pragma unroll
+        for (int cq = 0; cq < NQ; ++cq) {
+          STG w = c.F[6][cq] * xs;
+          w = (w + c.F[5][cq]) * x1;
+          w = (w + c.F[4][cq]) * xs;
+          w = (w + c.F[3][cq]) * x1;
+          w = (w + c.F[2][cq]) * xs;
+          w = (w + c.F[1][cq]) * x1;
+          w = (w + c.F[0][cq]) * xs;
+          q[cq] = c.qold[cq] + double(w);
+        }
+        PHYS d[3];
+        ds.sys.dipole(q, d);
+        nan = isnan(d[0]) || isnan(d[1]) || isnan(d[2]);
+        const PHYS *m = mu0s + (size_t)item * 4;
+        v = m[0] * d[0] + m[1] * d[1] + m[2] * d[2];
+      }
+      // the previous sample of the same context: lane - 1, or the last of the
+      // previous round (jj == 0 is the cross-context case of defer_jump_kernel)
+      PHYS pv = __shfl_up_sync(FULL, v, 1);
+      if (lane == 0) pv = tail;
+      tail = __shfl_sync(FULL, v, 31);
+      if (valid) {
+        unsigned code = 0xffffffffu;
+        if (nan) code = (unsigned(kk) << 3) | 1u;
+        else if (item + 2 * a.traj_base == P.inject_item && kk == P.inject_k) code = (unsigned(kk) << 3) | 4u;
+        else if (fabs(double(v)) > 1e100) code = (unsigned(kk) << 3) | 2u;
+        else if (jj > 0 && kk > 1 && fabs(double(v) / double(pv)) > 1e10) code = (unsigned(kk) << 3) | 3u;
+        if (code != 0xffffffffu) atomicMin(&a.item_fail[item], code);
+        if (!isnan(v) && !(fabs(double(v)) > 1e100)) {
+          double *crln = a.crln + (size_t)((item >> 1) / a.traj_per_iter) * (size_t)P.N;
+          atomicAdd(&crln[kk], P.weight * double(v));
+        }
+        if (jj == 0) first_v[base + o] = v;
+        if (jj == nn - 1) last_v[base + o] = v;
+      }
+    }
+  }
+}
+
+template <typename PHYS, typename STG, int NQ>
+__global__ void __launch_bounds__(DEFER_THREADS) defer_jump_kernel(DeferArgs a, TrajParams P) {
+  using Ctx = SampleCtx<STG, NQ>;
+  const unsigned long long count = defer_count(a);
+  const Ctx *ctx = static_cast<const Ctx *>(a.ctx);
+  const PHYS *first_v = static_cast<const PHYS *>(a.first_v);
+  const PHYS *last_v = static_cast<const PHYS *>(a.last_v);
+  for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < count;
+       i += (unsigned long long)gridDim.x * blockDim.x) {
+    const int prev = ctx[i].prev, k0 = ctx[i].k0, item = ctx[i].item;
+    if (prev < 0 || k0 <= 1) continue;
+    if (item + 2 * a.traj_base == P.inject_item && k0 == P.inject_k) continue;  // the injected failure comes first
+    const PHYS v = first_v[i], pv = last_v[prev];
+    if (fabs(double(v) / double(pv)) > 1e10) atomicMin(&a.item_fail[item], (unsigned(k0) << 3) | 3u);
+  }
+}
+
+template <typename PHYS>
+__global__ void __launch_bounds__(DEFER_THREADS) defer_items_kernel(DeferArgs a, TrajParams P) {
+  const PHYS *mu0s = static_cast<const PHYS *>(a.item_mu0);
+  if (blockIdx.x == 0 && threadIdx.x == 0) atomicMax(a.peak, *a.ctx_count);
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < a.n_items; idx += gridDim.x * blockDim.x) {
+    const int item = a.items ? a.items[idx] : idx;
+    const unsigned fc = a.item_fail[item];
+    a.item_fail[item] = 0xffffffffu;  // clean for the next pass
+    const bool hard = fc != 0xffffffffu;
+    int status = a.item_status[item];
+    if (hard) {
+      const unsigned r = fc & 7u;
+      status = r == 1u ? HH_ST_NAN_DIPOLE : r == 2u ? HH_ST_OVERFLOW : r == 3u ? HH_ST_JUMP : P.inject_status;
+    }
+    atomicAdd(&a.status_hist[status], 1u);
+    const int traj = item >> 1;
+    if (!hard) {
+      double *crln = a.crln + (size_t)(traj / a.traj_per_iter) * (size_t)P.N;
+      atomicAdd(&crln[0], P.weight * double(mu0s[(size_t)item * 4 + 3]));
+    } else if (a.fail_flag) {
+      if (atomicExch(&a.fail_flag[traj], 1) == 0) {
+        const int slot = atomicAdd(a.fail_count, 1);
+        a.fail_list[slot] = (int)(traj + a.traj_base);
+      }
+    }
+  }
+}
+
+}  // namespace hh

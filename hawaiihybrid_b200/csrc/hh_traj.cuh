@@ -103,8 +103,29 @@ struct TrajIO {
   unsigned int *solo_cursor;
   unsigned int *done;
   unsigned int handoff_at;
+  // deferred samples (plain C(t)): the kernel interpolates only r at the sample
+  // times (the R > Rcut exit) and writes one SampleCtx per dense-output step into
+  // `ctx` (index from *ctx_count; none past ctx_cap); the sample kernels of
+  // hh_defer.cuh then evaluate the dipoles, accumulate C(t) and apply the per-sample
+  // tests.  At an item's end the kernel writes its status to item_status instead of
+  // adding the t = 0 term and counting the status.  ctx == nullptr: in-kernel samples.
+  void *ctx;
+  unsigned long long *ctx_count;
+  unsigned long long ctx_cap;
+  int *item_status;           // [item]
+  void *item_mu0;             // [item][4] surface precision: mu0 and |mu0|^2
 };
 constexpr int HH_REC_WORDS = 12;  // r[3], q[4], u[3], padding
+
+// dense-output context of one step's stored samples k0 .. k0 + n - 1 of an item:
+// y(t0 + x h) = qold + sum_r F[r] (x, 1 - x alternating powers), x = (k dt - t0) inv_h;
+// prev: the item's previous context (-1 for its first)
+template <typename STG, int NQ> struct alignas(16) SampleCtx {
+  STG F[7][NQ];
+  double qold[NQ];
+  double t0, inv_h;
+  int item, k0, n, prev;
+};
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
   unsigned long long t;
@@ -777,6 +798,7 @@ template <int N, typename PHYS, typename STG> struct HandoffState {
   int item, k, since, total, flags;  // flags: rejected | exited << 1
   int req;                           // requantization switch and torque runs (REQ kernels)
   unsigned steps, samples, t_begin;  // item trace so far
+  int last_ctx;                      // deferred samples: the item's last context
 };
 
 // ---------------------------------------------------------------------------
@@ -810,6 +832,9 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
   double *crln = io.crln;
   const double *satw = nullptr;  // this trajectory's satellite weights
   int item = -1;           // -1: needs an item, -2: queue exhausted
+  // deferred samples: contexts instead of in-kernel dipoles (plain C(t) only)
+  const bool defer = !Sys::RECORDS && io.ctx != nullptr;
+  int last_ctx = -1;       // deferred samples: the item's last context
   int k = 1;
   int since = 0, total = 0;
   bool rejected = false;
@@ -874,6 +899,13 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
     exited = false;
     curr = PHYS(0);
     if constexpr (REQ) req = 1 | (req_cap << 1);
+    last_ctx = -1;
+    if (defer && owner) {
+      PHYS *m = static_cast<PHYS *>(io.item_mu0) + (size_t)item * 4;
+#pragma unroll
+      for (int c = 0; c < 3; ++c) m[c] = mu_t[c];
+      m[3] = mu_t[0] * mu_t[0] + mu_t[1] * mu_t[1] + mu_t[2] * mu_t[2];
+    }
   };
   auto item_of = [&](unsigned idx) {
     return io.items ? io.items[idx] : (io.fwd_only ? 2 * (int)idx : (int)idx);
@@ -911,6 +943,7 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
           hs->steps = nsteps - s0;
           hs->samples = nsamp - m0;
           hs->t_begin = (unsigned)(t_begin & 0xffffffffu);
+          hs->last_ctx = last_ctx;
         }
         item = -2;
       }
@@ -954,6 +987,7 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
           s0 = nsteps - hs->steps;
           m0 = nsamp - hs->samples;
           t_begin = hs->t_begin;
+          last_ctx = hs->last_ctx;
           const int traj = item >> 1;
           crln = io.crln + (size_t)(traj / io.traj_per_iter) * (size_t)P.N;
           satw = io.sat_w ? io.sat_w + (size_t)traj * io.n_sat : nullptr;
@@ -1118,6 +1152,10 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
             double q[Sys::NQ];
 #pragma unroll
             for (int c = 0; c < Sys::NQ; ++c) {
+              if (c >= 3 && defer) {  // deferred: only r, for the R > Rcut test
+                q[c] = 0.0;
+                continue;
+              }
               STG v = ws->F[6][c][o] * xs;
               v = (v + ws->F[5][c][o]) * x1;
               v = (v + ws->F[4][c][o]) * xs;
@@ -1137,6 +1175,9 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
               PHYS *rec = static_cast<PHYS *>(io.records) + slot * HH_REC_WORDS;
 #pragma unroll
               for (int c = 0; c < Sys::NQ; ++c) rec[c] = PHYS(q[c]);
+              nan_[u] = false;
+              ws->res[jj] = PHYS(1);
+            } else if (defer) {
               nan_[u] = false;
               ws->res[jj] = PHYS(1);
             } else {
@@ -1166,8 +1207,9 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
             const int j = base + jj;
             const PHYS val = ws->res[jj];
             unsigned code = 0xffffffffu;
-            if (Sys::RECORDS || P.prmu) {
-              // a record's dipole checks run after the batched evaluation; PR_MU has none
+            if (Sys::RECORDS || P.prmu || defer) {
+              // a record's or a deferred sample's dipole checks run after the batched
+              // evaluation; PR_MU has none
               if (out_[u]) code = (unsigned(j + 1) << 3);
             } else if (nan_[u]) code = (unsigned(j) << 3) | 1u;
             else if (ws->item[o] == P.inject_item && kks[u] == P.inject_k) code = (unsigned(j) << 3) | 4u;
@@ -1194,8 +1236,8 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
             const int stop = (cut == 0xffffffffu) ? end_o : min(end_o, int(cut >> 3));
             const int chunk_end = min(end_o, base + m);
             if (j < stop) {
-              if (Sys::RECORDS || io.series) {
-                // written in (1)
+              if (Sys::RECORDS || io.series || defer) {
+                // written in (1), or by the sample kernels
               } else if (io.n_sat == 0) {
                 atomicAdd(&ws->crln[o][kks[u]], P.weight * double(val));
               } else {
@@ -1211,6 +1253,44 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
           }
         }
         __syncwarp();
+      }
+      if constexpr (!Sys::RECORDS) {
+        if (defer) {
+          // one context per owner with stored samples (one atomic per warp)
+          int nc = 0;
+          if (pending && owner) {
+            const unsigned cut = ws->cut[lane];
+            nc = ((cut == 0xffffffffu) ? my_off + cnt : min(my_off + cnt, int(cut >> 3))) - my_off;
+          }
+          const unsigned wm = __ballot_sync(FULL, nc > 0);
+          if (wm) {
+            unsigned long long cbase = 0;
+            const int leader = __ffs(wm) - 1;
+            if (lane == leader) cbase = atomicAdd(io.ctx_count, (unsigned long long)__popc(wm));
+            cbase = __shfl_sync(FULL, cbase, leader);
+            if (nc > 0) {
+              const unsigned long long idx = cbase + __popc(wm & ((1u << lane) - 1u));
+              if (idx < io.ctx_cap) {
+                const int col = Sys::SOLO ? 0 : lane;
+                auto *cx = static_cast<SampleCtx<STG, Sys::NQ> *>(io.ctx) + idx;
+#pragma unroll
+                for (int r = 0; r < 7; ++r)
+#pragma unroll
+                  for (int c = 0; c < Sys::NQ; ++c) cx->F[r][c] = ws->F[r][c][col];
+#pragma unroll
+                for (int c = 0; c < Sys::NQ; ++c) cx->qold[c] = ws->qold[c][col];
+                cx->t0 = ws->t0[lane];
+                cx->inv_h = ws->inv_h[lane];
+                cx->item = item;
+                cx->k0 = k;
+                cx->n = nc;
+                cx->prev = last_ctx;
+              }
+              // past the capacity the host repeats the call with a larger buffer
+              last_ctx = (int)idx;
+            }
+          }
+        }
       }
       if (pending && owner) {
         const unsigned cut = ws->cut[lane];
@@ -1332,7 +1412,10 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
         io.rec_len[item] = k - 1;
         if (io.rec_status) io.rec_status[item] = status | (exited ? 16 : 0);
       }
-      if (!hard && !io.series) {
+      if (defer) {
+        // the sample kernels add the t = 0 term and count the status
+        io.item_status[item] = status;
+      } else if (!hard && !io.series) {
         const PHYS c0 = mu0[0] * mu0[0] + mu0[1] * mu0[1] + mu0[2] * mu0[2];
         if (io.n_sat == 0) {
           atomicAdd(&crln[0], P.weight * double(c0));
@@ -1346,7 +1429,7 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
         io.item_trace[item] = make_uint4(nsteps - s0, nsamp - m0, (unsigned)(t_begin & 0xffffffffu),
                                          (unsigned)(t_end & 0xffffffffu));
       }
-      atomicAdd(&io.status_hist[status], 1u);
+      if (!defer) atomicAdd(&io.status_hist[status], 1u);
       ++nitems;
       if (hard && io.fail_flag) {
         if (atomicExch(&io.fail_flag[traj], 1) == 0) {

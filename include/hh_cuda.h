@@ -331,6 +331,15 @@ int hh_cuda_debug_tuning(int *ch4_dip_s_fp64, int *ch4_dip_s_mixed);
  * fixes the first pick instead. */
 int hh_cuda_debug_set_ch4_dipole(int precision, int variant);
 
+/* Diagnostic (no counterpart in the reference): where the mixed path's plain C(t)
+ * evaluates the dipoles at the sample times.  mode 0: inside the trajectory kernel;
+ * 1 (the default, or the environment variable HH_DEFER_SAMPLES): CO2-Ar deferred to
+ * the sample kernels (the trajectory kernel writes one dense-output context per step
+ * and tests only R > Rcut); 2: CO2-Ar and N2-Ar deferred; -1 leaves the mode as it is.
+ * *previous (if not NULL) receives the mode before the call.  Both placements give the
+ * same samples and C(t) up to the order of the FP64 sums. */
+int hh_cuda_debug_set_defer(int mode, int *previous);
+
 /* Diagnostic (no counterpart in the reference): device time per kernel class.
  * While switched on, every kernel of the classes below is bracketed by CUDA events
  * and waited for (launches of a call then run one after another, so switch it on
@@ -343,7 +352,8 @@ int hh_cuda_debug_set_ch4_dipole(int precision, int variant);
 #define HH_KT_CH4_SORT 3    /* CH4-CO2 record sort (count, scan, scatter) */
 #define HH_KT_CH4_CORR 4    /* CH4-CO2 per-sample tests and C(t) sums */
 #define HH_KT_MOMENT 5      /* M0 / M2 kernel */
-#define HH_KT_COUNT 6
+#define HH_KT_SAMPLES 6     /* deferred samples: dipoles, per-sample tests and C(t) sums */
+#define HH_KT_COUNT 7
 int hh_cuda_debug_kernel_ms(int enable, double *ms, uint64_t *launches, int n);
 /* Tuning knob (no counterpart in the reference): the trajectory launch's block
  * shape (bulk kernel warps per block, 4 or 8) and hand-off threshold (the launch
