@@ -616,8 +616,16 @@ def main():
                              "1e-8 C(0)")
 
     # ---- roofline of the trajectory kernel (mixed path) ----
-    w = flops.work("co2ar", last, mixed=True)
-    t_s = last["traj_ms"] / 1e3
+    # per-kernel device times of one more call of the same K iterations (kernels serialised):
+    # the trajectory kernel (bulk + solo launches) and the deferred sample kernels
+    _lib.kernel_ms(True)
+    run(hh.PRECISION_MIXED, K)
+    kt = _lib.kernel_ms(False)
+    w_all = flops.work("co2ar", last, mixed=True)
+    w_smp = flops.sample_work("co2ar", last, mixed=True)
+    deferred = kt["samples"]["launches"] > 0
+    w = {k: w_all[k] - (w_smp[k] if deferred else 0.0) for k in w_all}
+    t_s = (kt["traj_bulk"]["ms"] + kt["traj_solo"]["ms"]) / 1e3
     roof = _roof(w, t_s, *peaks, "traj_kernel<CO2-Ar, float, float> (mixed, bulk + solo)")
     # DRAM bytes per trajectory from one ncu capture of a single-iteration launch,
     # scaled to the timed launch's n * K trajectories
@@ -637,11 +645,15 @@ def main():
     if plain is not None:
         roof["plain_fp64_frac"] = _roof(flops.work("co2ar", st_p, mixed=False), st_p["traj_ms"] / 1e3,
                                         *peaks, "")["frac"]
-    # bulk / solo split of the trajectory kernel in one per-kernel timed call (kernels serialised)
-    _lib.kernel_ms(True)
-    run(hh.PRECISION_MIXED, K)
-    kt = _lib.kernel_ms(False)
     roof["kernel_ms_split"] = {k: v["ms"] for k, v in kt.items() if v["launches"]}
+    if deferred:
+        sk = _roof(w_smp, kt["samples"]["ms"] / 1e3, *peaks,
+                   "defer_eval_kernel<CO2-Ar, float> + per-sample tests + per-item pass")
+        roof["sample_kernels"] = {k: sk[k] for k in ("kernel", "achieved_tflops", "peak_tflops", "frac",
+                                                     "work_flops", "kernel_ms")}
+    roof["work_split"] = ("trajectory kernel: steps, dense output and the R > Rcut tests; sample kernels: "
+                          "interpolation, dipole and mu0 product of every stored sample"
+                          if deferred else "trajectory kernel: all work (samples in the kernel)")
 
     # ---- CPU baseline: the oracle on a bounded sample (rank 0, one GPU) ----
     cpu = None

@@ -90,6 +90,7 @@ __global__ void __launch_bounds__(DEFER_THREADS) defer_eval_kernel(DeferArgs a, 
   using DS = DeferSys<SYS, PHYS, STG>;
   constexpr int NQ = DS::NQ;
   using Ctx = SampleCtx<STG, NQ>;
+  static_assert(sizeof(STG) == 4 && sizeof(PHYS) == 4 && NQ % 2 == 0 && sizeof(Ctx) % 16 == 0, "vector loads of the context");
   constexpr unsigned FULL = 0xffffffffu;
   extern __shared__ __align__(16) unsigned char df_smem[];
   DS ds;
@@ -130,29 +131,50 @@ __global__ void __launch_bounds__(DEFER_THREADS) defer_eval_kernel(DeferArgs a, 
       bool nan = false;
       int kk = 0, item = 0, nn = 0;
       if (valid) {
-        const Ctx &c = ctx[base + o];
-        item = c.item;
-        nn = c.n;
-        kk = c.k0 + jj;
-        const double x = (double(kk) * P.dt - c.t0) * c.inv_h;
+        // the context in 16-byte loads: qold, (t0, inv_h), (item, k0, n, prev), F
+        const Ctx *cp = ctx + base + o;
+        double qo[NQ];
+#pragma unroll
+        for (int i = 0; i < NQ / 2; ++i) {
+          const double2 v2 = reinterpret_cast<const double2 *>(cp->qold)[i];
+          qo[2 * i] = v2.x;
+          qo[2 * i + 1] = v2.y;
+        }
+        const double2 th = *reinterpret_cast<const double2 *>(&cp->t0);
+        const int4 hd = *reinterpret_cast<const int4 *>(&cp->item);
+        STG F[7 * NQ];
+#pragma unroll
+        for (int i = 0; i < 7 * NQ / 4; ++i) {
+          const float4 v4 = reinterpret_cast<const float4 *>(&cp->F[0][0])[i];
+          F[4 * i] = v4.x;
+          F[4 * i + 1] = v4.y;
+          F[4 * i + 2] = v4.z;
+          F[4 * i + 3] = v4.w;
+        }
+#pragma unroll
+        for (int i = 4 * (7 * NQ / 4); i < 7 * NQ; ++i) F[i] = (&cp->F[0][0])[i];
+        item = hd.x;
+        nn = hd.z;
+        kk = hd.y + jj;
+        const double x = (double(kk) * P.dt - th.x) * th.y;
         const STG xs = STG(x), x1 = STG(1) - STG(x);
         double q[NQ];
 #pragma unroll
         for (int cq = 0; cq < NQ; ++cq) {
-          STG w = c.F[6][cq] * xs;
-          w = (w + c.F[5][cq]) * x1;
-          w = (w + c.F[4][cq]) * xs;
-          w = (w + c.F[3][cq]) * x1;
-          w = (w + c.F[2][cq]) * xs;
-          w = (w + c.F[1][cq]) * x1;
-          w = (w + c.F[0][cq]) * xs;
-          q[cq] = c.qold[cq] + double(w);
+          STG w = F[6 * NQ + cq] * xs;
+          w = (w + F[5 * NQ + cq]) * x1;
+          w = (w + F[4 * NQ + cq]) * xs;
+          w = (w + F[3 * NQ + cq]) * x1;
+          w = (w + F[2 * NQ + cq]) * xs;
+          w = (w + F[1 * NQ + cq]) * x1;
+          w = (w + F[0 * NQ + cq]) * xs;
+          q[cq] = qo[cq] + double(w);
         }
         PHYS d[3];
         ds.sys.dipole(q, d);
         nan = isnan(d[0]) || isnan(d[1]) || isnan(d[2]);
-        const PHYS *m = mu0s + (size_t)item * 4;
-        v = m[0] * d[0] + m[1] * d[1] + m[2] * d[2];
+        const float4 m = *reinterpret_cast<const float4 *>(mu0s + (size_t)item * 4);
+        v = m.x * d[0] + m.y * d[1] + m.z * d[2];
       }
       // the previous sample of the same context: lane - 1, or the last of the
       // previous round (jj == 0 is the cross-context case of defer_jump_kernel)
@@ -186,7 +208,8 @@ __global__ void __launch_bounds__(DEFER_THREADS) defer_jump_kernel(DeferArgs a, 
   const PHYS *last_v = static_cast<const PHYS *>(a.last_v);
   for (unsigned long long i = (unsigned long long)blockIdx.x * blockDim.x + threadIdx.x; i < count;
        i += (unsigned long long)gridDim.x * blockDim.x) {
-    const int prev = ctx[i].prev, k0 = ctx[i].k0, item = ctx[i].item;
+    const int4 hd = *reinterpret_cast<const int4 *>(&ctx[i].item);  // item, k0, n, prev
+    const int prev = hd.w, k0 = hd.y, item = hd.x;
     if (prev < 0 || k0 <= 1) continue;
     if (item + 2 * a.traj_base == P.inject_item && k0 == P.inject_k) continue;  // the injected failure comes first
     const PHYS v = first_v[i], pv = last_v[prev];

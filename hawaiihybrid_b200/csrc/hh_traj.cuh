@@ -120,11 +120,12 @@ constexpr int HH_REC_WORDS = 12;  // r[3], q[4], u[3], padding
 // dense-output context of one step's stored samples k0 .. k0 + n - 1 of an item:
 // y(t0 + x h) = qold + sum_r F[r] (x, 1 - x alternating powers), x = (k dt - t0) inv_h;
 // prev: the item's previous context (-1 for its first)
+// (field order: 16-byte aligned groups for vector loads)
 template <typename STG, int NQ> struct alignas(16) SampleCtx {
-  STG F[7][NQ];
   double qold[NQ];
   double t0, inv_h;
   int item, k0, n, prev;
+  STG F[7][NQ];
 };
 
 __device__ __forceinline__ unsigned long long globaltimer_ns() {
@@ -1059,6 +1060,7 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
     const double t_land = double(k) * dt;  // REQ: the sample time a landed step ends at
     if (__any_sync(FULL, pending)) {
       int cnt = 0;
+      int nsafe = 0;  // deferred samples: stored without per-sample R > Rcut tests
       if (pending) {
         STG F[7][Sys::NQ];
         if constexpr (Sys::SOLO) {
@@ -1099,6 +1101,37 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
         while (kl > k && double(kl) * dt > t_new) --kl;
         if (REQ && landed) kl = k;
         cnt = owner ? kl - k + 1 : 0;  // solo mode: the owner's samples, evaluated by all lanes
+        if constexpr (!Sys::SOLO && !Sys::RECORDS) {
+          // deferred samples: no sample of the step can pass R > Rcut when the bound
+          // |r(x)| <= max(|r_old|, |r_old + F0|) + sum_i c_i |F_i| of the dense-output
+          // polynomial y = y_old + F0 x + F1 x(1-x) + F2 x^2(1-x) + ... + F6 x^4(1-x)^3
+          // (c_i the maxima of its basis on [0, 1]; |r_old + F0 x| is convex in x) stays
+          // below Rcut with a margin for the FP32 evaluation; such steps store all
+          // their samples without pooled tests
+          if (defer && cnt > 0) {
+            constexpr double cb[7] = {0.0, 0.25, 4.0 / 27.0, 1.0 / 16.0, 108.0 / 3125.0, 1.0 / 64.0,
+                                      6912.0 / 823543.0};
+            double ro2 = 0.0, rn2 = 0.0, f02 = 0.0, tail = 0.0;
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+              const double qo = y[Sys::qidx(c)], f0 = double(F[0][c]);
+              ro2 += qo * qo;
+              rn2 += (qo + f0) * (qo + f0);
+              f02 += f0 * f0;
+            }
+#pragma unroll
+            for (int r = 1; r < 7; ++r) {
+              const double a0 = F[r][0], a1 = F[r][1], a2 = F[r][2];
+              tail += cb[r] * sqrt(a0 * a0 + a1 * a1 + a2 * a2);
+            }
+            const double bound = fmax(sqrt(ro2), sqrt(rn2)) + tail;
+            if (bound + 1e-5 * (sqrt(f02) + tail) + 1e-12 * bound < P.Rcut) {
+              nsafe = cnt;
+              nsamp += cnt;  // evaluated by the sample kernels
+              cnt = 0;
+            }
+          }
+        }
         if (owner) {
           if constexpr (!Sys::SOLO) {
 #pragma unroll
@@ -1260,7 +1293,7 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
           int nc = 0;
           if (pending && owner) {
             const unsigned cut = ws->cut[lane];
-            nc = ((cut == 0xffffffffu) ? my_off + cnt : min(my_off + cnt, int(cut >> 3))) - my_off;
+            nc = nsafe + ((cut == 0xffffffffu) ? my_off + cnt : min(my_off + cnt, int(cut >> 3))) - my_off;
           }
           const unsigned wm = __ballot_sync(FULL, nc > 0);
           if (wm) {
@@ -1295,7 +1328,7 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
       if (pending && owner) {
         const unsigned cut = ws->cut[lane];
         const int stop = (cut == 0xffffffffu) ? my_off + cnt : min(my_off + cnt, int(cut >> 3));
-        const int committed = stop - my_off;
+        const int committed = nsafe + stop - my_off;
         if (committed > 0) {
           k += committed;
           curr = ws->last[lane];

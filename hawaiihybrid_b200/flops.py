@@ -81,6 +81,16 @@ def m0_work(system: str, n_samples: int, nT: int, mixed: bool) -> dict:
     return {"fp32": 0.0, "fp64": float(phys + f64)}
 
 
+def sample_work(system: str, stats: dict, mixed: bool) -> dict:
+    """FP32 and FP64 flops of the per-sample work of one call (dense-output interpolation,
+    dipole, product with mu0): the deferred sample kernels' share of `work`."""
+    e = per_event(system, mixed)
+    n_samp = stats["n_samples"]
+    if mixed:
+        return {"fp32": float(n_samp * e["sample"]), "fp64": float(n_samp * e["sample_fp64"])}
+    return {"fp32": 0.0, "fp64": float(n_samp * (e["sample"] + e["sample_fp64"]))}
+
+
 def work(system: str, stats: dict, mixed: bool) -> dict:
     """FP32 and FP64 flops of one call from its measured event counts."""
     e = per_event(system, mixed)
