@@ -92,7 +92,32 @@ def parse():
     ap.add_argument("--ch4co2-per-T", type=int, default=CH4CO2["n_per_T"])
     ap.add_argument("--only", choices=["n2ar", "ch4co2", "hear", "m0"],
                     help="run only this workload and print its block as the JSON line")
+    ap.add_argument("--profile-case", choices=["co2ar", "co2ar_multi", "ch4co2"],
+                    help="run a small case of a workload twice for an ncu capture (the second "
+                         "call is the one to capture) and exit: co2ar one iteration and co2ar_multi "
+                         "8 iterations of 16,384 mixed trajectories; ch4co2 4 x 16,384 mixed")
     return ap.parse_args()
+
+
+def profile_case(args, hh, H):
+    """Small inputs larger than L2 for ncu (a few GB on the device at most): two identical
+    calls, so a capture with -s skips the first call's launches."""
+    w = WORKLOAD
+    if args.profile_case in ("co2ar", "co2ar_multi"):
+        ms = hh.init_ms(w["mu"], hh.LINEAR_MOLECULE, hh.ATOM, (w["II"], w["II"]), None, w["seed"])
+        p = _params(H, w, w["fp64_tol"], args.mixed_tol)
+        K = 1 if args.profile_case == "co2ar" else 8
+        for _ in range(2):
+            _, _, st = hh.correlation_iterations(ms, p, w["T"], 16384, K, hh.PRECISION_MIXED, seed=w["seed"])
+    else:
+        c = CH4CO2
+        ms = hh.init_ms(c["mu"], hh.ROTOR, hh.LINEAR_MOLECULE, (c["II1"],) * 3, (c["II2"], c["II2"]), c["seed"])
+        p = _params(H, c, c["fp64_tol"], args.mixed_tol)
+        for _ in range(2):
+            _, _, st = hh.correlation_temperatures(ms, p, c["Ts"], 16384, hh.PRECISION_MIXED, seed=c["seed"])
+    st = st.as_dict()
+    print(json.dumps({"profile_case": args.profile_case, "traj_ms": st["traj_ms"], "n_steps": st["n_steps"],
+                      "n_kernel_launches": st["n_kernel_launches"]}), flush=True)
 
 
 def _params(H, w, tol, mixed_tol, N=None):
@@ -521,6 +546,8 @@ def main():
     _lib.check(lib.hh_cuda_fma_peak(_lib.HH_PRECISION_MIXED, C.byref(p32)))
     _lib.check(lib.hh_cuda_fma_peak(_lib.HH_PRECISION_FP64, C.byref(p64)))
     peaks = (p32.value, p64.value)
+    if args.profile_case:
+        return profile_case(args, hh, H)
     if args.only:
         fn = {"n2ar": bench_n2ar, "ch4co2": bench_ch4co2, "hear": bench_hear, "m0": bench_m0}[args.only]
         print(json.dumps({args.only: fn(args, hh, H, peaks)}), flush=True)

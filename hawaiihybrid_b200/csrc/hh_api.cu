@@ -992,6 +992,15 @@ int run_series_t(const TrajParams &P, const TrajIO &io0, const double *d_ic, uin
   return HH_OK;
 }
 
+// The bulk trajectory kernel's warps start each round together (TrajParams::block_sync):
+// they then fetch the same step code at the same time, where unsynchronised warps at
+// different phases of the loop thrash the instruction cache (CO2-Ar mixed, deferred
+// samples: 22.0 -> 8.9 ms per iteration).  HH_TRAJ_BLOCK_SYNC=0 switches it off.
+int traj_block_sync() {
+  const char *e = getenv("HH_TRAJ_BLOCK_SYNC");
+  return e ? (atoi(e) != 0) : 1;
+}
+
 // The plain C(t) launches of run_trajectories, then the replay of failed trajectories
 // (the reference drops a trajectory whose correlation_eval returns 1 while still
 // counting it: both branches are replayed with the opposite weight).  With deferred
@@ -1148,6 +1157,7 @@ int run_trajectories(const hh_calc_params *p, const double *d_ic, uint64_t n, ui
   P.inject_item = g_inject_item;
   P.inject_k = g_inject_k;
   P.inject_status = g_inject_status;
+  P.block_sync = traj_block_sync();
   CK(g.crln.ensure(N * n_iter));
   CK(g.counters.ensure(16));
   CK(g.status_hist.ensure(2 * HH_ST_COUNT));
@@ -1719,6 +1729,7 @@ int hh_cuda_prmu(const hh_calc_params *p, double T, double R0, double approx_fre
   P.noise_floor = 16.0 * 5.96e-8;
   P.inject_item = P.inject_k = -1;
   P.prmu = 1;
+  P.block_sync = traj_block_sync();
   const bool req = g.req.mode != HH_REQ_NONE;
   if (req) {
     P.req_mode = g.req.mode;

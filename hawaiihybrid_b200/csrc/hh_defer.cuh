@@ -64,11 +64,27 @@ template <int SYS, typename PHYS, typename STG> struct DeferSys;
 template <typename PHYS, typename STG> struct DeferSys<SYS_CO2AR, PHYS, STG> {
   static constexpr int NQ = 6;
   static constexpr size_t smem() { return smem_tables_bytes<PHYS>(); }
-  Co2ArSys<PHYS, STG, false, false> sys;
+  const Co2arTables<PHYS> *tb;
   __device__ void init(unsigned char *sm, const Co2arTablesGlobal *gtab, const TrajIO &) {
-    auto *tb = reinterpret_cast<Co2arTables<PHYS> *>(sm);
-    load_tables<PHYS>(tb, gtab);
-    sys.tb = tb;
+    auto *t = reinterpret_cast<Co2arTables<PHYS> *>(sm);
+    load_tables<PHYS>(t, gtab);
+    tb = t;
+  }
+  // Co2ArSys::dipole (the mixed path's, plain sums) with the surface sums inlined: this
+  // kernel is their only call site
+  __device__ __forceinline__ void dipole(const double *q, PHYS d[3]) const {
+    PHYS r[3] = {PHYS(q[0]), PHYS(q[1]), PHYS(q[2])};
+    PHYS u[3] = {PHYS(q[3]), PHYS(q[4]), PHYS(q[5])};
+    PHYS R2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+    PHYS iR = inv_sqrt(R2);
+    PHYS iu = inv_sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    PHYS rh[3] = {r[0] * iR, r[1] * iR, r[2] * iR};
+    PHYS uh[3] = {u[0] * iu, u[1] * iu, u[2] * iu};
+    PHYS x = rh[0] * uh[0] + rh[1] * uh[1] + rh[2] * uh[2];
+    PHYS dz, ax;
+    co2ar_dip<PHYS, false>(tb->dipx, tb->dipz, tb->fdip, tb->rbound, tb->rlo, R2 * iR, iR, x, dz, ax);
+#pragma unroll
+    for (int c = 0; c < 3; ++c) d[c] = dz * rh[c] - ax * (uh[c] - x * rh[c]);
   }
 };
 template <typename PHYS, typename STG> struct DeferSys<SYS_N2AR, PHYS, STG> {
@@ -82,10 +98,11 @@ template <typename PHYS, typename STG> struct DeferSys<SYS_N2AR, PHYS, STG> {
     sys.pes = nullptr;
     sys.dtab = static_cast<const float4 *>(io.diptab);
   }
+  __device__ __forceinline__ void dipole(const double *q, PHYS d[3]) const { sys.dipole(q, d); }
 };
 
 template <int SYS, typename PHYS, typename STG>
-__global__ void __launch_bounds__(DEFER_THREADS) defer_eval_kernel(DeferArgs a, TrajParams P, TrajIO io,
+__global__ void __launch_bounds__(DEFER_THREADS, SYS == SYS_CO2AR ? 4 : 1) defer_eval_kernel(DeferArgs a, TrajParams P, TrajIO io,
                                                                    const Co2arTablesGlobal *gtab) {
   using DS = DeferSys<SYS, PHYS, STG>;
   constexpr int NQ = DS::NQ;
@@ -171,7 +188,7 @@ __global__ void __launch_bounds__(DEFER_THREADS) defer_eval_kernel(DeferArgs a, 
           q[cq] = qo[cq] + double(w);
         }
         PHYS d[3];
-        ds.sys.dipole(q, d);
+        ds.dipole(q, d);
         nan = isnan(d[0]) || isnan(d[1]) || isnan(d[2]);
         const float4 m = *reinterpret_cast<const float4 *>(mu0s + (size_t)item * 4);
         v = m.x * d[0] + m.y * d[1] + m.z * d[2];

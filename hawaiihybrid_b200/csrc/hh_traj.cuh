@@ -59,6 +59,9 @@ struct TrajParams {
   // the torque cache length and limit that switch it (src/hawaii.c:3604-3662)
   int req_mode, req_len;
   double req_limit;
+  // bulk kernel: the block's warps start every round together (one barrier per round),
+  // so they walk the step code in step and share its instruction fetches
+  int block_sync;
 };
 
 struct TrajIO {
@@ -1001,7 +1004,12 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
         }
       }
     }
-    if (__all_sync(FULL, item == -2)) break;
+    bool all_done = __all_sync(FULL, item == -2);
+    if constexpr (!Sys::SOLO) {
+      // block-uniform exit with the round barrier (every warp takes every round)
+      if (P.block_sync) all_done = __syncthreads_and(all_done ? 1 : 0) != 0;
+    }
+    if (all_done) break;
     const bool active = (item >= 0);
 
     // ---- one step attempt for every lane that holds an item ----

@@ -2,9 +2,12 @@
 one dense-output context per step and tests only R > Rcut; the sample kernels evaluate the
 dipoles, accumulate C(t) and apply the per-sample tests (src/hawaii.c:2183-2243).  Checked
 against the in-kernel placement on the same trajectories: the same steps, samples and
-statuses, C(t) equal up to the order of the FP64 sums, the same failure handling, and the
-same result when the iterations of a call are split over several launches or the context
-buffer overflows."""
+statuses, C(t) equal up to the order of the FP64 sums (N2-Ar) or to the FP32 rounding of the
+dipole surface (CO2-Ar: the sample kernel inlines it, the trajectory kernel calls one shared
+copy, and the compiler may fuse their multiply-adds differently), the same failure handling,
+and the same result when the iterations of a call are split over several launches or the
+context buffer overflows.  Also: the bulk kernel's per-round block barrier changes no
+result."""
 import numpy as np
 import pytest
 
@@ -42,6 +45,10 @@ def _same_stats(sa, sb):
     assert list(sa.status) == list(sb.status)
 
 
+# C(t) agreement of the two placements, in units of C(0)
+PLACEMENT_TOL = {"co2ar": 1e-7, "n2ar": 1e-12}
+
+
 @pytest.mark.parametrize("name", ["co2ar", "n2ar"])
 def test_deferred_samples_match_in_kernel(name):
     import hawaiihybrid_b200 as hh
@@ -51,7 +58,7 @@ def test_deferred_samples_match_in_kernel(name):
     p = lib_params(name, N, dt, mixed_tol=3e-8)
     (ca, sa), (cb, sb) = _in_kernel_then_deferred(
         lambda: hh.correlation_from_initial_conditions(ms, p, qp, hh.PRECISION_MIXED))
-    assert rel_to_c0(cb, ca) < 1e-12
+    assert rel_to_c0(cb, ca) < PLACEMENT_TOL[name]
     _same_stats(sa, sb)
 
 
@@ -70,7 +77,7 @@ def test_deferred_failure_matches_in_kernel(lib, status):
     finally:
         lib.hh_cuda_debug_inject(-1, 0, 0, 0)
     assert sa.n_failed == 1 and sb.n_failed == 1
-    assert rel_to_c0(cb, ca) < 1e-12
+    assert rel_to_c0(cb, ca) < PLACEMENT_TOL[name]
     assert list(sa.status) == list(sb.status)
 
 
@@ -99,3 +106,22 @@ def test_deferred_launch_split_and_overflow(monkeypatch):
     for s in (s2, s3):
         _same_stats(s1, s)
     assert list(nt1) == list(nt2) == list(nt3)
+
+
+@pytest.mark.parametrize("name,precision", [("hear", 0), ("hear", 1), ("co2ar", 0), ("co2ar", 1),
+                                            ("n2ar", 0), ("n2ar", 1), ("ch4co2", 1)])
+def test_block_barrier_changes_nothing(monkeypatch, name, precision):
+    """The bulk kernel with and without its per-round block barrier integrates the same
+    steps and gives the same C(t) (up to the order of the FP64 sums)."""
+    import hawaiihybrid_b200 as hh
+    ms = lib_system(name, 9)
+    N, dt = (21, 200.0) if name == "ch4co2" else (2048, 100.0)
+    qp, _ = O.sample(9, oracle_system(name), oracle_params(name, N, dt), 300.0, 1024)
+    p = lib_params(name, N, dt, mixed_tol=3e-8)
+    out = []
+    for bs in ("0", "1"):
+        monkeypatch.setenv("HH_TRAJ_BLOCK_SYNC", bs)
+        out.append(hh.correlation_from_initial_conditions(ms, p, qp, precision))
+    (ca, sa), (cb, sb) = out
+    assert rel_to_c0(cb, ca) < 1e-12
+    _same_stats(sa, sb)
