@@ -995,10 +995,11 @@ int run_series_t(const TrajParams &P, const TrajIO &io0, const double *d_ic, uin
 // The bulk trajectory kernel's warps start each round together (TrajParams::block_sync):
 // they then fetch the same step code at the same time, where unsynchronised warps at
 // different phases of the loop thrash the instruction cache (CO2-Ar mixed, deferred
-// samples: 22.0 -> 8.9 ms per iteration).  HH_TRAJ_BLOCK_SYNC=0 switches it off.
+// samples: 22.0 -> 8.9 ms per iteration).  HH_TRAJ_BLOCK_SYNC=n puts the barrier on every
+// n-th round instead, 0 switches it off.
 int traj_block_sync() {
   const char *e = getenv("HH_TRAJ_BLOCK_SYNC");
-  return e ? (atoi(e) != 0) : 1;
+  return e ? std::max(0, atoi(e)) : 1;
 }
 
 // The plain C(t) launches of run_trajectories, then the replay of failed trajectories

@@ -22,7 +22,7 @@
 // A failed trajectory is replayed with the opposite weight by the host, which
 // removes everything it added; the replay takes the same path, so its samples are
 // exactly those the first pass accumulated.  Samples after a failure are therefore
-// accumulated too (only NaN and |value| > 1e100 are skipped, in both passes), which
+// accumulated too (only NaN and infinite values are skipped, in both passes), which
 // leaves C(t) as the in-kernel path makes it: failed trajectories contribute nothing.
 #pragma once
 
@@ -61,30 +61,83 @@ __device__ __forceinline__ unsigned long long defer_count(const DeferArgs &a) {
 
 // the dipole of the bound system with its surfaces staged in shared memory
 template <int SYS, typename PHYS, typename STG> struct DeferSys;
+// CO2-Ar dipole surface for the sample kernel: the rows of the x and z tables padded to
+// 12 FP32 words (a0..a3 | b4..b7 | A k 0 0), three 16-byte loads each, and the
+// interval found by one lookup of floor(4 R) (every interval bound is a multiple of
+// 1/4 bohr, so the lookup gives the reference's `R < bound` interval exactly).  The
+// sums are those of co2ar_dip (plain, l = 0, 2, .., 10 in order).
+struct DeferCo2arDip {
+  float4 row[CO2AR_NINT][2][CO2AR_NL][3];  // [interval][x, z][l / 2][12 words]
+  float rlo[CO2AR_NINT];
+  int fdip[CO2AR_NINT];
+  unsigned char ivl[164];                  // interval of R in [j / 4, (j + 1) / 4), j <= 160
+};
 template <typename PHYS, typename STG> struct DeferSys<SYS_CO2AR, PHYS, STG> {
   static constexpr int NQ = 6;
-  static constexpr size_t smem() { return smem_tables_bytes<PHYS>(); }
-  const Co2arTables<PHYS> *tb;
-  __device__ void init(unsigned char *sm, const Co2arTablesGlobal *gtab, const TrajIO &) {
-    auto *t = reinterpret_cast<Co2arTables<PHYS> *>(sm);
-    load_tables<PHYS>(t, gtab);
-    tb = t;
+  static constexpr size_t smem() { return (sizeof(DeferCo2arDip) + 15) / 16 * 16; }
+  const DeferCo2arDip *t;
+  __device__ void init(unsigned char *sm, const Co2arTablesGlobal *g, const TrajIO &) {
+    auto *d = reinterpret_cast<DeferCo2arDip *>(sm);
+    float *w = reinterpret_cast<float *>(d->row);
+    constexpr int NW = CO2AR_NINT * 2 * CO2AR_NL * 12;
+    for (int e = threadIdx.x; e < NW; e += blockDim.x) {
+      const int k = e % 12, li = (e / 12) % CO2AR_NL, c = (e / (12 * CO2AR_NL)) % 2, i = e / (24 * CO2AR_NL);
+      const double *src = (c == 0 ? g->dipx : g->dipz) + (i * CO2AR_NL + li) * CO2AR_ROW;
+      w[e] = k < CO2AR_ROW ? float(src[k]) : 0.f;
+    }
+    for (int i = threadIdx.x; i < CO2AR_NINT; i += blockDim.x) {
+      d->rlo[i] = float(g->rlo[i]);
+      d->fdip[i] = g->fdip[i];
+    }
+    for (int j = threadIdx.x; j < 164; j += blockDim.x) {
+      const double r = 0.25 * j;
+      int i = 0;
+      while (i < CO2AR_NINT - 1 && !(r < g->rbound[i])) ++i;
+      d->ivl[j] = (unsigned char)i;
+    }
+    t = d;
   }
-  // Co2ArSys::dipole (the mixed path's, plain sums) with the surface sums inlined: this
-  // kernel is their only call site
-  __device__ __forceinline__ void dipole(const double *q, PHYS d[3]) const {
-    PHYS r[3] = {PHYS(q[0]), PHYS(q[1]), PHYS(q[2])};
-    PHYS u[3] = {PHYS(q[3]), PHYS(q[4]), PHYS(q[5])};
-    PHYS R2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
-    PHYS iR = inv_sqrt(R2);
-    PHYS iu = inv_sqrt(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
-    PHYS rh[3] = {r[0] * iR, r[1] * iR, r[2] * iR};
-    PHYS uh[3] = {u[0] * iu, u[1] * iu, u[2] * iu};
-    PHYS x = rh[0] * uh[0] + rh[1] * uh[1] + rh[2] * uh[2];
-    PHYS dz, ax;
-    co2ar_dip<PHYS, false>(tb->dipx, tb->dipz, tb->fdip, tb->rbound, tb->rlo, R2 * iR, iR, x, dz, ax);
+  __device__ __forceinline__ float radial(const float4 *rw, float R, float tt, float iR4, float iR5, float iR6,
+                                          float iR7, int fl) const {
+    const float4 a = rw[0];
+    float c = ((a.w * tt + a.z) * tt + a.y) * tt + a.x;
+    if (fl & 1) {
+      const float4 b = rw[1];
+      c += b.x * iR4 + b.y * iR5 + b.z * iR6 + b.w * iR7;
+    }
+    if (fl & 2) {
+      const float4 e = rw[2];
+      c += e.x * expf(e.y * R);
+    }
+    return c;
+  }
+  static constexpr bool FLOAT_Q = true;  // takes the sample position in FP32
+  __device__ __forceinline__ void dipole(const float *q, PHYS d[3]) const {
+    const float r[3] = {q[0], q[1], q[2]};
+    const float u[3] = {q[3], q[4], q[5]};
+    const float R2 = r[0] * r[0] + r[1] * r[1] + r[2] * r[2];
+    const float iR = rsqrtf(R2);
+    const float iu = rsqrtf(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
+    const float rh[3] = {r[0] * iR, r[1] * iR, r[2] * iR};
+    const float uh[3] = {u[0] * iu, u[1] * iu, u[2] * iu};
+    const float x = rh[0] * uh[0] + rh[1] * uh[1] + rh[2] * uh[2];
+    const float R = R2 * iR;
+    const int i = t->ivl[min(int(R * 4.f), 163)];
+    const float tt = R - t->rlo[i];
+    const int fl = t->fdip[i];
+    float P[11], dP[11];
+    legendre10(x, P, dP);
+    const float iR2 = iR * iR, iR4 = iR2 * iR2, iR5 = iR4 * iR, iR6 = iR5 * iR, iR7 = iR6 * iR;
+    float dz = 0.f, ax = 0.f;
 #pragma unroll
-    for (int c = 0; c < 3; ++c) d[c] = dz * rh[c] - ax * (uh[c] - x * rh[c]);
+    for (int li = 0; li < CO2AR_NL; ++li) {
+      const float av = radial(t->row[i][0][li], R, tt, iR4, iR5, iR6, iR7, fl);
+      const float bv = radial(t->row[i][1][li], R, tt, iR4, iR5, iR6, iR7, fl);
+      dz += P[2 * li] * bv;
+      ax += dP[2 * li] * av;
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) d[c] = PHYS(dz * rh[c] - ax * (uh[c] - x * rh[c]));
   }
 };
 template <typename PHYS, typename STG> struct DeferSys<SYS_N2AR, PHYS, STG> {
@@ -98,6 +151,7 @@ template <typename PHYS, typename STG> struct DeferSys<SYS_N2AR, PHYS, STG> {
     sys.pes = nullptr;
     sys.dtab = static_cast<const float4 *>(io.diptab);
   }
+  static constexpr bool FLOAT_Q = false;
   __device__ __forceinline__ void dipole(const double *q, PHYS d[3]) const { sys.dipole(q, d); }
 };
 
@@ -175,20 +229,43 @@ __global__ void __launch_bounds__(DEFER_THREADS, SYS == SYS_CO2AR ? 4 : 1) defer
         kk = hd.y + jj;
         const double x = (double(kk) * P.dt - th.x) * th.y;
         const STG xs = STG(x), x1 = STG(1) - STG(x);
-        double q[NQ];
-#pragma unroll
-        for (int cq = 0; cq < NQ; ++cq) {
-          STG w = F[6 * NQ + cq] * xs;
-          w = (w + F[5 * NQ + cq]) * x1;
-          w = (w + F[4 * NQ + cq]) * xs;
-          w = (w + F[3 * NQ + cq]) * x1;
-          w = (w + F[2 * NQ + cq]) * xs;
-          w = (w + F[1 * NQ + cq]) * x1;
-          w = (w + F[0 * NQ + cq]) * xs;
-          q[cq] = qo[cq] + double(w);
-        }
         PHYS d[3];
-        ds.dipole(q, d);
+        if constexpr (DS::FLOAT_Q) {
+          // y = y_old + F0 x + F1 x(1-x) + F2 x^2(1-x) + ... + F6 x^4(1-x)^3 with the
+          // basis formed once and one FMA per term; the position in FP32
+          STG bs[7];
+          bs[0] = xs;
+          bs[1] = xs * x1;
+          bs[2] = bs[1] * xs;
+          bs[3] = bs[2] * x1;
+          bs[4] = bs[3] * xs;
+          bs[5] = bs[4] * x1;
+          bs[6] = bs[5] * xs;
+          float qf[NQ];
+#pragma unroll
+          for (int cq = 0; cq < NQ; ++cq) {
+            STG w = F[cq] * bs[0];
+#pragma unroll
+            for (int r = 1; r < 7; ++r) w = fmaf(F[r * NQ + cq], bs[r], w);
+            qf[cq] = float(qo[cq]) + w;
+          }
+          ds.dipole(qf, d);
+        } else {
+          // the trajectory kernel's interpolation (hh_traj.cuh) in its order
+          double q[NQ];
+#pragma unroll
+          for (int cq = 0; cq < NQ; ++cq) {
+            STG w = F[6 * NQ + cq] * xs;
+            w = (w + F[5 * NQ + cq]) * x1;
+            w = (w + F[4 * NQ + cq]) * xs;
+            w = (w + F[3 * NQ + cq]) * x1;
+            w = (w + F[2 * NQ + cq]) * xs;
+            w = (w + F[1 * NQ + cq]) * x1;
+            w = (w + F[0 * NQ + cq]) * xs;
+            q[cq] = qo[cq] + double(w);
+          }
+          ds.dipole(q, d);
+        }
         nan = isnan(d[0]) || isnan(d[1]) || isnan(d[2]);
         const float4 m = *reinterpret_cast<const float4 *>(mu0s + (size_t)item * 4);
         v = m.x * d[0] + m.y * d[1] + m.z * d[2];
@@ -199,13 +276,16 @@ __global__ void __launch_bounds__(DEFER_THREADS, SYS == SYS_CO2AR ? 4 : 1) defer
       if (lane == 0) pv = tail;
       tail = __shfl_sync(FULL, v, 31);
       if (valid) {
+        // the reference's tests on an FP32 value: |v| > 1e100 is v = +-inf, and
+        // |v / pv| > 1e10 is |v| > 1e10 |pv| (1e10 is exact in FP32; a zero pv fails
+        // any v != 0, NaN fails neither)
         unsigned code = 0xffffffffu;
         if (nan) code = (unsigned(kk) << 3) | 1u;
         else if (item + 2 * a.traj_base == P.inject_item && kk == P.inject_k) code = (unsigned(kk) << 3) | 4u;
-        else if (fabs(double(v)) > 1e100) code = (unsigned(kk) << 3) | 2u;
-        else if (jj > 0 && kk > 1 && fabs(double(v) / double(pv)) > 1e10) code = (unsigned(kk) << 3) | 3u;
+        else if (isinf(v)) code = (unsigned(kk) << 3) | 2u;
+        else if (jj > 0 && kk > 1 && fabsf(v) > 1e10f * fabsf(pv)) code = (unsigned(kk) << 3) | 3u;
         if (code != 0xffffffffu) atomicMin(&a.item_fail[item], code);
-        if (!isnan(v) && !(fabs(double(v)) > 1e100)) {
+        if (!isnan(v) && !isinf(v)) {
           double *crln = a.crln + (size_t)((item >> 1) / a.traj_per_iter) * (size_t)P.N;
           atomicAdd(&crln[kk], P.weight * double(v));
         }
@@ -230,7 +310,7 @@ __global__ void __launch_bounds__(DEFER_THREADS) defer_jump_kernel(DeferArgs a, 
     if (prev < 0 || k0 <= 1) continue;
     if (item + 2 * a.traj_base == P.inject_item && k0 == P.inject_k) continue;  // the injected failure comes first
     const PHYS v = first_v[i], pv = last_v[prev];
-    if (fabs(double(v) / double(pv)) > 1e10) atomicMin(&a.item_fail[item], (unsigned(k0) << 3) | 3u);
+    if (fabs(double(v)) > 1e10 * fabs(double(pv))) atomicMin(&a.item_fail[item], (unsigned(k0) << 3) | 3u);
   }
 }
 

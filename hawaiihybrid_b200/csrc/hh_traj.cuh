@@ -59,8 +59,9 @@ struct TrajParams {
   // the torque cache length and limit that switch it (src/hawaii.c:3604-3662)
   int req_mode, req_len;
   double req_limit;
-  // bulk kernel: the block's warps start every round together (one barrier per round),
-  // so they walk the step code in step and share its instruction fetches
+  // bulk kernel: the block's warps start every block_sync-th round together (a block
+  // barrier), so they walk the step code in step and share its instruction fetches;
+  // 0: no barrier
   int block_sync;
 };
 
@@ -916,6 +917,7 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
   };
   bool handing = false;  // bulk mode: this warp hands its open items to the solo kernel
   unsigned round = 0;
+  int sync_round = 0;    // bulk mode: rounds since the last block barrier
   for (;;) {
     if constexpr (!Sys::SOLO) {
       // ---- hand-off: once few items remain open, store them for the solo kernel ----
@@ -1006,8 +1008,12 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
     }
     bool all_done = __all_sync(FULL, item == -2);
     if constexpr (!Sys::SOLO) {
-      // block-uniform exit with the round barrier (every warp takes every round)
-      if (P.block_sync) all_done = __syncthreads_and(all_done ? 1 : 0) != 0;
+      // block-uniform exit with the round barrier, every block_sync-th round (every
+      // warp takes every round; between barriers no warp leaves)
+      if (P.block_sync) {
+        all_done = (sync_round == 0) ? (__syncthreads_and(all_done ? 1 : 0) != 0) : false;
+        if (++sync_round == P.block_sync) sync_round = 0;
+      }
     }
     if (all_done) break;
     const bool active = (item >= 0);

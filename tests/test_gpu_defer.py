@@ -2,9 +2,9 @@
 one dense-output context per step and tests only R > Rcut; the sample kernels evaluate the
 dipoles, accumulate C(t) and apply the per-sample tests (src/hawaii.c:2183-2243).  Checked
 against the in-kernel placement on the same trajectories: the same steps, samples and
-statuses, C(t) equal up to the order of the FP64 sums (N2-Ar) or to the FP32 rounding of the
-dipole surface (CO2-Ar: the sample kernel inlines it, the trajectory kernel calls one shared
-copy, and the compiler may fuse their multiply-adds differently), the same failure handling,
+statuses, C(t) equal up to the order of the FP64 sums (N2-Ar) or to FP32 rounding (CO2-Ar:
+the sample kernel has its own FP32 interpolation and dipole-surface code, with the sample
+position in FP32, so a sample's dipole may differ by a few ulps), the same failure handling,
 and the same result when the iterations of a call are split over several launches or the
 context buffer overflows.  Also: the bulk kernel's per-round block barrier changes no
 result."""
@@ -46,7 +46,7 @@ def _same_stats(sa, sb):
 
 
 # C(t) agreement of the two placements, in units of C(0)
-PLACEMENT_TOL = {"co2ar": 1e-7, "n2ar": 1e-12}
+PLACEMENT_TOL = {"co2ar": 1e-6, "n2ar": 1e-12}
 
 
 @pytest.mark.parametrize("name", ["co2ar", "n2ar"])
