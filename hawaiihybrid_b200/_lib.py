@@ -53,7 +53,7 @@ HH_REQ_NONE, HH_REQ_INTEGER, HH_REQ_HALFINTEGER = 0, 1, 2
 HH_INTEGRAND_M0 = 0
 HH_INTEGRAND_PF = 1
 # kernel classes of hh_cuda_debug_kernel_ms
-HH_KT_NAMES = ("traj_bulk", "traj_solo", "ch4_dipole", "ch4_sort", "ch4_corr", "moment", "samples")
+HH_KT_NAMES = ("traj_bulk", "traj_solo", "ch4_dipole", "ch4_sort", "ch4_corr", "moment", "samples", "item_start")
 HH_KT_COUNT = len(HH_KT_NAMES)
 
 

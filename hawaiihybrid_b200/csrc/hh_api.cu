@@ -146,6 +146,7 @@ struct Ctx {
   DevBuf<unsigned long long> dcount;
   DevBuf<int> item_status;
   DevBuf<unsigned> item_fail;
+  DevBuf<unsigned char> istart;  // precomputed item starts (ItemStart per item)
   double defer_est = 32.0;  // contexts per item, from the previous calls
   // CORRELATION_ARRAY weights [n][n_sat]: with ratios (C(t)) and without (nstar)
   DevBuf<double> sat_w, sat_wraw;
@@ -651,6 +652,25 @@ int run_deferred_sys(const TrajParams &P, const TrajIO &io, long long traj_base)
   return HH_OK;
 }
 
+// the launch's item starts (CO2-Ar) into buf, which then backs io.setup
+using DeferStart = ItemStart<12, float, float>;
+int run_item_starts(const TrajParams &P, TrajIO &io, unsigned char *buf) {
+  if (g.sys != SYS_CO2AR) return HH_OK;
+  auto k = item_start_kernel<float, float>;
+  const size_t smem = smem_tables_bytes<float>();
+  if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  int per_sm = 0;
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 256, smem));
+  const int grid = std::max(1, std::min(per_sm * g.num_sms, (io.n_items + 255) / 256));
+  kt_begin();
+  k<<<grid, 256, smem, g.st>>>(P, io, g.d_tab, buf);
+  CK(cudaGetLastError());
+  kt_end(HH_KT_ITEM_START);
+  g_launches += 1;
+  io.setup = buf;
+  return HH_OK;
+}
+
 int run_deferred(const TrajParams &P, const TrajIO &io, long long traj_base) {
   if (g.sys == SYS_N2AR) {
     TrajIO io2 = io;
@@ -1045,6 +1065,7 @@ int run_plain(int precision, const TrajParams &P, const TrajIO &io0, uint64_t n,
       CK(g.item_status.ensure(2 * n));
       CK(g.item_mu0.ensure(2 * n * 4 * sizeof(float)));
       CK(g.item_fail.ensure(2 * n));
+      if (g.sys == SYS_CO2AR) CK(g.istart.ensure(2 * n * sizeof(DeferStart)));
       CK(cudaMemsetAsync(g.item_fail.p, 0xff, 2 * n * sizeof(unsigned), g.st));
       CK(cudaMemsetAsync(g.dcount.p, 0, 2 * sizeof(unsigned long long), g.st));
       io.ctx = g.dctx.p;
@@ -1071,7 +1092,9 @@ int run_plain(int precision, const TrajParams &P, const TrajIO &io0, uint64_t n,
           CK(cudaMemsetAsync(g.queue.p, 0, sizeof(unsigned int), g.st));
           CK(cudaMemsetAsync(g.dcount.p, 0, sizeof(unsigned long long), g.st));
         }
-        int rc = run_traj_dispatch(precision, P, il);
+        int rc = run_item_starts(P, il, g.istart.p + 2 * t0 * sizeof(DeferStart));
+        if (rc) return rc;
+        rc = run_traj_dispatch(precision, P, il);
         if (rc) return rc;
         rc = run_deferred(P, il, (long long)t0);
         if (rc) return rc;
@@ -1113,6 +1136,10 @@ int run_plain(int precision, const TrajParams &P, const TrajIO &io0, uint64_t n,
         io2.ctx_cap = g.dctx.cap / sizeof(DeferCtx);
         if (io2.ctx_cap > g.dvals.cap / (2 * sizeof(float))) io2.ctx_cap = g.dvals.cap / (2 * sizeof(float));
         CK(cudaMemsetAsync(g.dcount.p, 0, 2 * sizeof(unsigned long long), g.st));
+      }
+      if (defer) {
+        int rc = run_item_starts(P2, io2, g.istart.p);
+        if (rc) return rc;
       }
       int rc = run_traj_dispatch(precision, P2, io2);
       if (rc) return rc;

@@ -118,8 +118,21 @@ struct TrajIO {
   unsigned long long ctx_cap;
   int *item_status;           // [item]
   void *item_mu0;             // [item][4] surface precision: mu0 and |mu0|^2
+  // precomputed item starts (ItemStart per item, item_start_kernel) or nullptr: the
+  // kernel then loads an item's initial state instead of running item_setup, whose
+  // lane-divergent cost otherwise stalls the whole warp (and, with the block barrier,
+  // the block) at every refill
+  const void *setup;
 };
 constexpr int HH_REC_WORDS = 12;  // r[3], q[4], u[3], padding
+
+// initial state of an item as item_setup makes it
+template <int N, typename PHYS, typename STG> struct alignas(16) ItemStart {
+  double y0[N];
+  double h;
+  STG f0[N];
+  PHYS mu0[3];
+};
 
 // dense-output context of one step's stored samples k0 .. k0 + n - 1 of an item:
 // y(t0 + x h) = qold + sum_r F[r] (x, 1 - x alternating powers), x = (k dt - t0) inv_h;
@@ -868,7 +881,19 @@ __device__ __forceinline__ void traj_body(const Sys &sys, const TrajParams &P, c
     double y_t[N];
     STG f_t[N];
     PHYS mu_t[3];
-    item_setup<Sys, PHYS, STG>(sys, P, io.ic + (size_t)traj * Sys::QP, item & 1, y_t, f_t, mu_t, &h);
+    if (io.setup) {
+      const auto *st = static_cast<const ItemStart<N, PHYS, STG> *>(io.setup) + item;
+#pragma unroll
+      for (int i = 0; i < N; ++i) {
+        y_t[i] = st->y0[i];
+        f_t[i] = st->f0[i];
+      }
+#pragma unroll
+      for (int c = 0; c < 3; ++c) mu_t[c] = st->mu0[c];
+      h = st->h;
+    } else {
+      item_setup<Sys, PHYS, STG>(sys, P, io.ic + (size_t)traj * Sys::QP, item & 1, y_t, f_t, mu_t, &h);
+    }
     if constexpr (Sys::SOLO) {
       y[0] = pick_component<N>(y_t, comp);
       K[0][0] = pick_component<N>(f_t, comp);
@@ -1580,6 +1605,40 @@ __global__ void __launch_bounds__(32 * WARPS, TRAJ_MIN_BLOCKS)
     sys.tb = tb;
     auto *ws = reinterpret_cast<WarpSamples<STG, PHYS, Sys::NQ> *>(smem_raw + smem_tables_bytes<PHYS>());
     traj_body<Sys, PHYS, STG, REQ>(sys, P, io, ws);
+  }
+}
+
+
+// Item starts of a launch's items (io.items or 0 .. n_items - 1), one thread per item:
+// item_setup as the trajectory kernel would run it at the item's refill.  CO2-Ar only.
+template <typename PHYS, typename STG>
+__global__ void __launch_bounds__(256) item_start_kernel(TrajParams P, TrajIO io, const Co2arTablesGlobal *gtab,
+                                                        void *out) {
+  using Sys = Co2ArSys<PHYS, STG, false, false>;
+  extern __shared__ __align__(16) unsigned char is_smem[];
+  Co2arTables<PHYS> *tb = reinterpret_cast<Co2arTables<PHYS> *>(is_smem);
+  load_tables<PHYS>(tb, gtab);
+  __syncthreads();
+  Sys sys;
+  sys.inv_mu = 1.0 / P.mu;
+  sys.inv_II = 1.0 / P.II;
+  sys.tb = tb;
+  auto *o = static_cast<ItemStart<Sys::N, PHYS, STG> *>(out);
+  for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < io.n_items; idx += gridDim.x * blockDim.x) {
+    const int item = io.items ? io.items[idx] : idx;
+    double y[Sys::N], h;
+    STG f[Sys::N];
+    PHYS mu[3];
+    item_setup<Sys, PHYS, STG>(sys, P, io.ic + (size_t)(item >> 1) * Sys::QP, item & 1, y, f, mu, &h);
+    ItemStart<Sys::N, PHYS, STG> &st = o[item];
+#pragma unroll
+    for (int i = 0; i < Sys::N; ++i) {
+      st.y0[i] = y[i];
+      st.f0[i] = f[i];
+    }
+#pragma unroll
+    for (int c = 0; c < 3; ++c) st.mu0[c] = mu[c];
+    st.h = h;
   }
 }
 

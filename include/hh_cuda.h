@@ -353,7 +353,8 @@ int hh_cuda_debug_set_defer(int mode, int *previous);
 #define HH_KT_CH4_CORR 4    /* CH4-CO2 per-sample tests and C(t) sums */
 #define HH_KT_MOMENT 5      /* M0 / M2 kernel */
 #define HH_KT_SAMPLES 6     /* deferred samples: dipoles, per-sample tests and C(t) sums */
-#define HH_KT_COUNT 7
+#define HH_KT_ITEM_START 7  /* precomputed item starts of the deferred-sample path */
+#define HH_KT_COUNT 8
 int hh_cuda_debug_kernel_ms(int enable, double *ms, uint64_t *launches, int n);
 /* Tuning knob (no counterpart in the reference): the trajectory launch's block
  * shape (bulk kernel warps per block, 4 or 8) and hand-off threshold (the launch
