@@ -60,14 +60,15 @@ char g_errmsg[512] = "";
 template <typename T> struct DevBuf {
   T *p = nullptr;
   size_t cap = 0;
+  // exactly n elements when it grows (several buffers hold gigabytes; callers that
+  // expect growth ask for their own headroom)
   cudaError_t ensure(size_t n) {
     if (n <= cap) return cudaSuccess;
     if (p) cudaFree(p);
     p = nullptr;
     cap = 0;
-    size_t want = std::max(n, cap * 3 / 2);
-    cudaError_t e = cudaMalloc(&p, want * sizeof(T));
-    if (e == cudaSuccess) cap = want;
+    cudaError_t e = cudaMalloc(&p, n * sizeof(T));
+    if (e == cudaSuccess) cap = n;
     return e;
   }
   void release() {
@@ -1059,8 +1060,17 @@ int run_plain(int precision, const TrajParams &P, const TrajIO &io0, uint64_t n,
       it_launch = std::min<uint64_t>(n_iter, std::max<uint64_t>(1, max_items / (2 * per_iter)));
       items_launch = 2 * std::min<uint64_t>(n, it_launch * per_iter);
       cap = (unsigned long long)(g.defer_est * double(items_launch)) + 4096ull;
-      CK(g.dctx.ensure(cap * sizeof(DeferCtx)));
-      CK(g.dvals.ensure(cap * 2 * sizeof(float)));
+      if (getenv("HH_DEFER_TRACE"))
+        fprintf(stderr, "[defer] attempt %d est %.3f items %llu cap %llu (buffer %llu) launches of %llu iterations, "
+                "budget %.2f GB, free %.2f GB\n", attempt, g.defer_est, (unsigned long long)items_launch, cap,
+                (unsigned long long)(g.dctx.cap / sizeof(DeferCtx)), (unsigned long long)it_launch, budget / 1e9,
+                free_b / 1e9);
+      // 10 % headroom: the estimate moves a little from call to call, and a larger
+      // buffer would otherwise be reallocated (cudaFree and cudaMalloc of gigabytes)
+      // inside a call
+      const size_t alloc = (size_t)(1.1 * double(cap));
+      if (g.dctx.cap < cap * sizeof(DeferCtx)) CK(g.dctx.ensure(alloc * sizeof(DeferCtx)));
+      if (g.dvals.cap < cap * 2 * sizeof(float)) CK(g.dvals.ensure(alloc * 2 * sizeof(float)));
       CK(g.dcount.ensure(2));
       CK(g.item_status.ensure(2 * n));
       CK(g.item_mu0.ensure(2 * n * 4 * sizeof(float)));
