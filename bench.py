@@ -141,6 +141,13 @@ def _ct_errors(c_test, c_ref, floor_ref=None):
     return out
 
 
+def _measured_bf16_tflops():
+    try:
+        return float(json.load(open(os.path.join(ROOT, "MEASURED_PEAKS.json")))["bf16_tflops"])
+    except (OSError, ValueError, KeyError, TypeError):
+        return None
+
+
 def _roof(work, t_s, p32, p64, kernel, note=None):
     achieved = (work["fp32"] + work["fp64"]) / t_s / 1e12
     frac = (work["fp32"] / (p32 * 1e12) + work["fp64"] / (p64 * 1e12)) / t_s
@@ -324,6 +331,21 @@ def bench_ch4co2(args, hh, H, peaks):
     fl = flops.ch4_dipole_flops(4 * nb, ng)
     for name, st in (("mixed", sm), ("fp64", sp)):
         dms = kt[name]["ch4_dipole"]["ms"]
+        if name == "mixed" and s32.value == -1 and dms > 0:
+            # the tensor-core kernel: the MMA work it issues (three TF32 products per
+            # 128-record task and component tile) against the TF32 dense peak, half the
+            # measured bf16 GEMM peak
+            mma = flops.ch4_tc_mma_flops(st["n_samples"])
+            bf16 = _measured_bf16_tflops()
+            out.setdefault("roofline", {})["mixed"] = {
+                "kernel": "ch4_dipole_tc_kernel (tcgen05.mma kind::tf32)", "achieved_tflops": mma / (dms / 1e3) / 1e12,
+                "peak_tflops": 0.5 * bf16 if bf16 else None,
+                "frac": (mma / (dms / 1e3) / 1e12) / (0.5 * bf16) if bf16 else None,
+                "work_flops": {"tf32_mma": mma}, "kernel_ms": dms,
+                "note": "MMA flops issued: 3 TF32 products x 2 x 128 x (2 x 208 + 208) x 368 per 128-record task "
+                        "(records / 128 tasks, padding not counted); peak: half of MEASURED_PEAKS.json bf16 "
+                        "(Blackwell dense TF32 is half its bf16 rate)"}
+            continue
         if dms > 0:
             work = {"fp32": float(fl * st["n_samples"]) if name == "mixed" else 0.0,
                     "fp64": 0.0 if name == "mixed" else float(fl * st["n_samples"])}

@@ -107,6 +107,7 @@ template <typename PHYS, typename STG, bool COMP, bool SOLO_ = false> struct Ch4
   // components a sample reads: r, the quaternion and u
   static constexpr int NQ = 10;
   static constexpr bool RECORDS = true;
+  static constexpr bool EST64 = false;
   static constexpr int MOM2 = 13;  // L and j follow the orientation block
   static __device__ __forceinline__ constexpr int qidx(int i) { return i < 3 ? i : i + 3; }
   double inv_mu, inv_II;      // 1 / mu, 1 / I_CO2

@@ -196,6 +196,7 @@ template <typename PHYS, typename STG, bool COMP, bool SOLO_ = false> struct HeA
   // components the dipole and the R > Rcut test read: r
   static constexpr int NQ = 3;
   static constexpr bool RECORDS = false;
+  static constexpr bool EST64 = true;  // FP64 error-estimate sums (err_terms)
   static constexpr int MOM2 = 6;  // no second momentum block
   static __device__ __forceinline__ constexpr int qidx(int i) { return i; }
   double inv_mu;
@@ -261,6 +262,7 @@ template <typename PHYS, typename STG, bool COMP, bool SOLO_ = false> struct Co2
   // components the dipole and the R > Rcut test read: r and u
   static constexpr int NQ = 6;
   static constexpr bool RECORDS = false;
+  static constexpr bool EST64 = false;
   static constexpr int MOM2 = 9;  // j
   static __device__ __forceinline__ constexpr int qidx(int i) { return i < 3 ? i : i + 3; }
   double inv_mu, inv_II;
@@ -331,6 +333,7 @@ template <typename PHYS, typename STG, bool COMP, bool SOLO_ = false> struct N2A
   static constexpr int QP = 10;
   static constexpr int NQ = 6;
   static constexpr bool RECORDS = false;
+  static constexpr bool EST64 = false;
   static constexpr int MOM2 = 9;  // j
   static __device__ __forceinline__ constexpr int qidx(int i) { return i < 3 ? i : i + 3; }
   double inv_mu, inv_II;
@@ -500,18 +503,23 @@ __device__ __forceinline__ void solution_point(const STG (&K)[16][N], const doub
 // scale.  (Measured on the CO2-Ar workload at rtol 3e-8: FP64 estimate sums let the
 // steps grow, 4 % fewer, past what the FP32 stages resolve, and the C(t) error within
 // the FP64 horizon rose from 1.9e-5 to 1.8e-4 while the kernel ran 12 % slower.)
-template <typename STG, int NK>
+// EST64: the estimate sums in FP64 (He-Ar: with its 6 state components they cost
+// little, and its non-chaotic C(t) follows FP64 to 6e-5 with them against 1.6e-4
+// with stage-precision sums)
+template <typename STG, bool EST64, int NK>
 __device__ __forceinline__ void err_terms(const STG (&K)[16][NK], int i, double y, double y_new, double h,
                                           const TrajParams &P, double &q5, double &q3) {
   double sc = P.atol + fmax(fabs(y), fabs(y_new)) * P.rtol;
-  STG a5s = STG(0), a3s = STG(0), m5s = STG(0);
+  using ET = typename std::conditional<EST64, double, STG>::type;
+  ET a5s = ET(0), a3s = ET(0), m5s = ET(0);
 #pragma unroll
   for (int j = 0; j < 13; ++j) {
     if (hh_dop853_e5[j] != 0.0) {
-      a5s += STG(hh_dop853_e5[j]) * K[j][i];
-      if (sizeof(STG) == 4) m5s += fabs(STG(hh_dop853_e5[j]) * K[j][i]);
+      const ET t = ET(hh_dop853_e5[j]) * ET(K[j][i]);
+      a5s += t;
+      if (sizeof(STG) == 4) m5s += fabs(t);
     }
-    if (hh_dop853_e3[j] != 0.0) a3s += STG(hh_dop853_e3[j]) * K[j][i];
+    if (hh_dop853_e3[j] != 0.0) a3s += ET(hh_dop853_e3[j]) * ET(K[j][i]);
   }
   const double a5 = double(a5s), a3 = double(a3s), m5 = double(m5s);
   if (sizeof(STG) == 4) sc += fabs(h) * P.noise_floor * m5;
@@ -548,7 +556,7 @@ __device__ __forceinline__ double step_attempt(const Sys &sys, const TrajParams 
 #pragma unroll
   for (int i = 0; i < N; ++i) {
     double q5, q3;
-    err_terms<STG>(K, i, y[i], y_new[i], h, P, q5, q3);
+    err_terms<STG, Sys::EST64>(K, i, y[i], y_new[i], h, P, q5, q3);
     e5 += q5 * q5;
     e3 += q3 * q3;
   }
@@ -661,7 +669,7 @@ __device__ __forceinline__ double step_attempt_cp(const Sys &sys, const TrajPara
     K[12][0] = pick_component<N>(f, c);
   }
   double q5, q3;
-  err_terms<STG>(K, 0, y, y_new, h, P, q5, q3);
+  err_terms<STG, Sys::EST64>(K, 0, y, y_new, h, P, q5, q3);
   double e5 = 0.0, e3 = 0.0;
 #pragma unroll
   for (int i = 0; i < N; ++i) {

@@ -49,6 +49,18 @@ def ch4_dipole_flops(n_entries_padded: int, n_groups: int) -> int:
     return 8 * n_entries_padded + 10 * n_groups + 600
 
 
+# CH4-CO2 tensor-core dipole (ch4_dipole_tc_kernel): per 128-record task, pass 0 runs two
+# 208-column component tiles and pass 1 one, over K = 368 in chunks of 16, each MMA of
+# M = 128, N = 208, K = 8 issued three times (A_hi B_hi, A_hi B_lo, A_lo B_hi)
+CH4_TC_MMA_FLOPS_PER_TASK = 3 * 2 * 128 * (2 * 208 + 208) * 368
+
+
+def ch4_tc_mma_flops(n_records: int) -> float:
+    """MMA flops the tensor-core dipole kernel issues for n_records records (whole tasks of
+    128; the per-piece padding of the last task is not counted)."""
+    return float(n_records) / 128.0 * CH4_TC_MMA_FLOPS_PER_TASK
+
+
 def per_event(system: str, mixed: bool = True) -> dict:
     s = dict(SYSTEMS[system])
     if not mixed and "dip_fp64" in s:
