@@ -49,9 +49,11 @@ namespace hh {
 
 constexpr int CH4TC_A_BYTES = CH4TC_M * CH4TC_KC * 4;    // one A image (hi or lo): 8 KB
 constexpr int CH4TC_STAGE_B = 2 * CH4TC_IMG0;            // B_hi | B_lo of the widest pass
-constexpr int CH4TC_STAGES = 3;
-// dynamic shared memory: 3 stages x (A_hi, A_lo, B_hi | B_lo) = 204 KB, 1 KB alignment
-constexpr size_t CH4TC_SMEM = CH4TC_STAGES * (2 * CH4TC_A_BYTES + CH4TC_STAGE_B) + 1024;
+constexpr int CH4TC_STAGES = 2;
+// dynamic shared memory: 2 stages x (A_hi, A_lo, B_hi | B_lo) = 136 KB, Y2 of the task
+// (46.6 KB), 1 KB alignment
+constexpr size_t CH4TC_SMEM =
+    CH4TC_STAGES * (2 * CH4TC_A_BYTES + CH4TC_STAGE_B) + (size_t)CH4_NY2 * CH4TC_M * 4 + 1024;
 constexpr unsigned CH4TC_TMEM_COLS = 512;
 constexpr unsigned CH4TC_COL1 = 256;            // TMEM column of the second accumulator
 constexpr long long CH4TC_WAIT_LIMIT = 1LL << 24;  // polls of an mbarrier before giving up
@@ -159,84 +161,82 @@ __constant__ float c_ch4tc_alpha[CH4_L1 + 1][CH4_L1 + 1];  // [m][l]
 __constant__ float c_ch4tc_beta[CH4_L1 + 1][CH4_L1 + 1];
 __constant__ float c_ch4tc_pm[CH4_L1 + 1];
 
-// Y2 of the CO2 axis (x, y, z) in the CH4 frame, one value per next() in the order of
-// ch4_y2 (m = 0..12, l = m..12 even, cos then sin).  The state is the recurrence's at
-// the position (m, l) to visit next; the caller asks for at most CH4_NY2 values.
-struct Ch4TcY2Gen {
-  float x, y, z, C, Sn, pm, qa, qb, pend;
-  int m, l;
-  bool sin_next;
-  __device__ __forceinline__ void reset(float x_, float y_, float z_) {
-    x = x_;
-    y = y_;
-    z = z_;
-    C = 1.f;
-    Sn = 0.f;
-    pm = c_ch4tc_pm[0];
-    qa = 1.f;
-    qb = 0.f;
-    pend = 0.f;
-    m = 0;
-    l = 0;
-    sin_next = false;
+// first Y2 index of m (order of ch4_y2: m = 0..12, l = m..12 even, cos then sin)
+HH_TC_HD constexpr int ch4tc_y2_off(int m2) {
+  int c = 0;
+  for (int m = 0; m < m2; ++m) c += (m == 0 ? 1 : 2) * (CH4_L2 / 2 + 1 - (m + 1) / 2);  // even l in [m, L2]
+  return c;
+}
+static_assert(ch4tc_y2_off(CH4_L2 + 1) == CH4_NY2, "Y2 count");
+
+// (cos, sin) of m phi as (x + i y)^m (the harmonics' unnormalised azimuthal factor)
+__device__ __forceinline__ void ch4tc_cs_m(float x, float y, int m, float &C, float &Sn) {
+  C = 1.f;
+  Sn = 0.f;
+  for (int i = 0; i < m; ++i) {
+    const float c = C * x - Sn * y;
+    Sn = C * y + Sn * x;
+    C = c;
   }
-  __device__ __forceinline__ void advance() {
-    if (l == CH4_L2) {
-      ++m;
-      l = m;
+}
+
+// Y2 of the CO2 axis (x, y, z) in the CH4 frame for m in [m0, m1), into
+// Y[idx * 128 + t] at their indices of ch4_y2
+__device__ __forceinline__ void ch4tc_y2_range(float x, float y, float z, float *Y, int t, int m0, int m1) {
+  float C, Sn;
+  ch4tc_cs_m(x, y, m0, C, Sn);
+  int idx = ch4tc_y2_off(m0);
+#pragma unroll 1
+  for (int m = m0; m < m1; ++m) {
+    if (m > m0) {
       const float c = C * x - Sn * y;
       Sn = C * y + Sn * x;
       C = c;
-      pm = c_ch4tc_pm[m];
-      qa = 1.f;
-      qb = 0.f;
-    } else {
-      ++l;
-      const float q = c_ch4tc_alpha[m][l] * z * qa - c_ch4tc_beta[m][l] * qb;
-      qb = qa;
-      qa = q;
     }
-  }
-  __device__ __forceinline__ float next() {
-    if (sin_next) {
-      sin_next = false;
-      return pend;
-    }
-    if (l & 1) advance();  // odd l carry no term; the next l is even
-    const float v = pm * C * qa;
-    if (m > 0) {
-      pend = pm * Sn * qa;
-      sin_next = true;
-    }
-    advance();
-    return v;
-  }
-};
-
-// sum_n Y1_n(n1) T[n] over the 196 columns at TMEM address `taddr` (this thread's
-// lane), Y1 generated in column order (m-major, l = m..13, cos then sin)
-__device__ __forceinline__ float ch4tc_y1_dot(uint32_t taddr, const float n1[3]) {
-  float acc = 0.f;
-  float C = 1.f, Sn = 0.f, pm = 1.f, qa = 0.f, qb = 0.f;
-  int m = 0, l = 0;
-  bool sin_next = false;
-  float ys_pending = 0.f;
+    const float pm = c_ch4tc_pm[m];
+    float qa = 1.f, qb = 0.f;
 #pragma unroll 1
-  for (int c0 = 0; c0 < CH4TC_NY1; c0 += 16) {
+    for (int l = m; l <= CH4_L2; ++l) {
+      if (l > m) {
+        const float q = c_ch4tc_alpha[m][l] * z * qa - c_ch4tc_beta[m][l] * qb;
+        qb = qa;
+        qa = q;
+      }
+      if ((l & 1) == 0) {
+        Y[(idx++) * CH4TC_M + t] = pm * C * qa;
+        if (m > 0) Y[(idx++) * CH4TC_M + t] = pm * Sn * qa;
+      }
+    }
+  }
+}
+
+// sum over the Y1 columns of m in [m0, m1) (m-major, l = m..13, cos then sin) of
+// Y1_n(n1) T[n] at TMEM address `taddr` (this thread's lane); m0 and m1 are uniform
+// across the warp (tcgen05.ld is a warp-wide load)
+__device__ __forceinline__ float ch4tc_y1_dot_m(uint32_t taddr, const float n1[3], int m0, int m1) {
+  const int c_begin = ch4tc_y1_col(m0, m0, 0, CH4_L1);
+  const int c_end = (m1 > CH4_L1) ? CH4TC_NY1 : ch4tc_y1_col(m1, m1, 0, CH4_L1);
+  float C, Sn;
+  ch4tc_cs_m(n1[0], n1[1], m0, C, Sn);
+  float pm = c_ch4tc_pm[m0], qa = 1.f, qb = 0.f, ys_pending = 0.f;
+  int m = m0, l = m0;
+  bool first = true, sin_next = false;
+  float acc = 0.f;
+#pragma unroll 1
+  for (int c0 = c_begin & ~15; c0 < c_end; c0 += 16) {
     float v[16];
     tmem_ld16(taddr + (uint32_t)c0, v);
 #pragma unroll
     for (int i = 0; i < 16; ++i) {
       const int c = c0 + i;
-      if (c < CH4TC_NY1) {
+      if (c >= c_begin && c < c_end) {
         float y;
         if (sin_next) {
           y = ys_pending;
           sin_next = false;
         } else {
-          if (c == 0) {
-            qa = 1.f;
-            qb = 0.f;
+          if (first) {
+            first = false;
           } else if (l == CH4_L1) {
             ++m;
             l = m;
@@ -265,26 +265,35 @@ __device__ __forceinline__ float ch4tc_y1_dot(uint32_t taddr, const float n1[3])
   return acc;
 }
 
-// 256 threads: two warps per TMEM lane quadrant.  Thread t works on record row = t % 128;
-// half = t / 128 splits the A rows' K columns (half 0: k = 4c, 4c + 1; half 1: 4c + 2,
-// 4c + 3) and the epilogue (pass 0: half h reads component h; pass 1: half 0).
-constexpr int CH4TC_THREADS = 2 * CH4TC_M;
+// 512 threads: four warps per TMEM lane quadrant.  Thread t works on record row =
+// t % 128; its quarter qt = t / 128 takes
+//   - the Y2 of m in CH4TC_Y2_M[qt] .. CH4TC_Y2_M[qt + 1] (about a quarter of the
+//     recurrence work each) into shared memory,
+//   - column group k = 4 c + qt of every A chunk (its 4 powers of x, hi and lo),
+//   - in pass 0 half of the columns of component qt / 2 (m in [0, 5) or [5, 14)), in
+//     pass 1 a quarter of the columns of component 2 (CH4TC_Y1_M);
+// the partial sums meet in shared memory and quarter 0 finishes the record.
+constexpr int CH4TC_THREADS = 4 * CH4TC_M;
+__constant__ int CH4TC_Y2_M[5] = {0, 2, 4, 7, CH4_L2 + 1};
+__constant__ int CH4TC_Y1_M[5] = {0, 2, 4, 7, CH4_L1 + 1};
+constexpr int CH4TC_Y1_SPLIT = 5;  // pass 0: m < 5 and m >= 5
 
 __global__ void __launch_bounds__(CH4TC_THREADS, 1) ch4_dipole_tc_kernel(Ch4TcArgs a) {
   extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
   unsigned char *smem = reinterpret_cast<unsigned char *>(
       (reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~uintptr_t(1023));
-  // stage s: A_hi, A_lo, B (hi | lo)
+  // stage s: A_hi, A_lo, B (hi | lo); then Y2 of the task
   constexpr size_t STAGE_BYTES = 2 * CH4TC_A_BYTES + CH4TC_STAGE_B;
   auto stA = [&](int s, int lo) { return smem + (size_t)s * STAGE_BYTES + (size_t)lo * CH4TC_A_BYTES; };
   auto stB = [&](int s) { return smem + (size_t)s * STAGE_BYTES + 2 * CH4TC_A_BYTES; };
+  float *Y2s = reinterpret_cast<float *>(smem + CH4TC_STAGES * STAGE_BYTES);
   __shared__ __align__(8) uint64_t bar_load[CH4TC_STAGES], bar_mma[CH4TC_STAGES];
   __shared__ uint32_t tmem_base_s;
   __shared__ int bad_s;
   __shared__ long long w0[CH4_NSEG + 1];
-  __shared__ float acc1_s[CH4TC_M];  // component 1 from half 1 to half 0
+  __shared__ float part_s[4][CH4TC_M];  // the quarters' partial sums of a pass
   const int t = threadIdx.x, warp = t >> 5;
-  const int row = t & (CH4TC_M - 1), half = t / CH4TC_M;
+  const int row = t & (CH4TC_M - 1), qt = t / CH4TC_M;
   for (int i = t; i <= CH4_NSEG; i += blockDim.x) w0[i] = a.warp0[i];
   if (t == 0) {
     for (int s = 0; s < CH4TC_STAGES; ++s) {
@@ -310,10 +319,10 @@ __global__ void __launch_bounds__(CH4TC_THREADS, 1) ch4_dipole_tc_kernel(Ch4TcAr
     while (s < CH4_NSEG - 1 && w0[s + 1] <= task) ++s;
     return s;
   };
-  // chunk sequence: g counts the chunks this CTA has walked; chunk g uses stage g % 3,
-  // and the n-th completion of a stage's barriers belongs to its chunk 3 n + stage.
-  // Thread 0 keeps gl (loads issued), gw (loads seen complete) and gm (chunks whose
-  // MMAs were committed) for the bounded drain after a timeout.
+  // chunk sequence: g counts the chunks this CTA has walked; chunk g uses stage
+  // g % STAGES, and the n-th completion of a stage's barriers belongs to its chunk
+  // STAGES n + stage.  Thread 0 keeps gl (loads issued), gw (loads seen complete) and
+  // gm (chunks whose MMAs were committed) for the bounded drain after a timeout.
   unsigned g = 0, gl = 0, gw = 0, gm = 0;
   // the chunk after (task, q, c) in this CTA's walk, for the B prefetch
   auto next_chunk = [&](long long task, int q, int c, long long &nt, int &nq, int &nc) -> bool {
@@ -341,10 +350,11 @@ __global__ void __launch_bounds__(CH4TC_THREADS, 1) ch4_dipole_tc_kernel(Ch4TcAr
     issue_load(task0, 0, 0, 0);
     gl = 1;
   }
+  const uint32_t lane_addr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
   for (long long task = task0; task < total; task += gridDim.x) {
     const long long w = task * a.task_step;
     const int seg = seg_of(w);
-    // ---- this thread's record: geometry, Y2, powers of x ----
+    // ---- this thread's record: geometry, powers of x ----
     const int first = a.sorted[w * CH4TC_M];
     const int mine = a.sorted[w * CH4TC_M + row];
     const int src = mine >= 0 ? mine : first;
@@ -352,9 +362,9 @@ __global__ void __launch_bounds__(CH4TC_THREADS, 1) ch4_dipole_tc_kernel(Ch4TcAr
     float M[3][3], n1[3], n2[3];
     {
       const float r[3] = {rec[0], rec[1], rec[2]};
-      const float qt[4] = {rec[3], rec[4], rec[5], rec[6]};
+      const float qt4[4] = {rec[3], rec[4], rec[5], rec[6]};
       const float u[3] = {rec[7], rec[8], rec[9]};
-      quat_matrix<float>(qt, M);
+      quat_matrix<float>(qt4, M);
       const float R = sqrtf(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
       const float iR = 1.f / R;
       const float iu = 1.f / sqrtf(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
@@ -367,24 +377,18 @@ __global__ void __launch_bounds__(CH4TC_THREADS, 1) ch4_dipole_tc_kernel(Ch4TcAr
     const float R = sqrtf(rec[0] * rec[0] + rec[1] * rec[1] + rec[2] * rec[2]);
     const float x = R - float(a.centre[seg]);
     const float xp[4] = {1.f, x, x * x, x * x * x};
+    __syncthreads();  // the previous task's last chunk no longer reads Y2s
+    ch4tc_y2_range(n2[0], n2[1], n2[2], Y2s, row, CH4TC_Y2_M[qt], CH4TC_Y2_M[qt + 1]);
+    __syncthreads();
     float acc[3] = {0.f, 0.f, 0.f};
-    Ch4TcY2Gen y2g;
     for (int q = 0; q < 2; ++q) {
       const int ntile = q == 0 ? 2 : 1;
-      y2g.reset(n2[0], n2[1], n2[2]);
       for (int c = 0; c < CH4TC_NCHUNK; ++c, ++g) {
         const int s = g % CH4TC_STAGES;
-        // Y2_k of the chunk's four k (both halves walk the recurrence; each uses two)
-        float y2c[4];
-#pragma unroll
-        for (int kq = 0; kq < 4; ++kq) y2c[kq] = (4 * c + kq < CH4_NY2) ? y2g.next() : 0.f;
-        // ---- A chunk: row t, columns 16 c .. 16 c + 15 (k = 4 c .. 4 c + 3, j = 0..3) ----
-        float *Ah = reinterpret_cast<float *>(stA(s, 0));
-        float *Al = reinterpret_cast<float *>(stA(s, 1));
-#pragma unroll
-        for (int kh = 0; kh < 2; ++kh) {
-          const int kq = 2 * half + kh;
-          const float y2 = half ? y2c[2 + kh] : y2c[kh];
+        // ---- A chunk: row t, columns 4 kq .. 4 kq + 3 (k = 4 c + kq, j = 0..3), kq = qt ----
+        {
+          const int k = 4 * c + qt;
+          const float y2 = (k < CH4_NY2) ? Y2s[k * CH4TC_M + row] : 0.f;
           float4 hi, lo;
           float *ph = &hi.x, *pl = &lo.x;
 #pragma unroll
@@ -394,8 +398,8 @@ __global__ void __launch_bounds__(CH4TC_THREADS, 1) ch4_dipole_tc_kernel(Ch4TcAr
             ph[j] = h;
             pl[j] = v - h;
           }
-          *reinterpret_cast<float4 *>(Ah + ch4tc_img_off(row, 4 * kq)) = hi;
-          *reinterpret_cast<float4 *>(Al + ch4tc_img_off(row, 4 * kq)) = lo;
+          *reinterpret_cast<float4 *>(reinterpret_cast<float *>(stA(s, 0)) + ch4tc_img_off(row, 4 * qt)) = hi;
+          *reinterpret_cast<float4 *>(reinterpret_cast<float *>(stA(s, 1)) + ch4tc_img_off(row, 4 * qt)) = lo;
         }
         asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
         __syncthreads();
@@ -424,13 +428,14 @@ __global__ void __launch_bounds__(CH4TC_THREADS, 1) ch4_dipole_tc_kernel(Ch4TcAr
             }
             ch4tc_commit(&bar_mma[s]);
             gm = g + 1;
-            // prefetch the next chunk's B into stage (g + 1) % 3 once that stage's last
-            // MMAs (chunk g - 2) are done; chunks g - 1 and g stay queued meanwhile
+            // prefetch the next chunk's B into stage (g + 1) % STAGES once that stage's
+            // last MMAs (chunk g + 1 - STAGES) are done
             long long nt_;
             int nq, nc;
             if (next_chunk(task, q, c, nt_, nq, nc)) {
               const int s1 = (g + 1) % CH4TC_STAGES;
-              if (g >= 2 && !mbar_wait(&bar_mma[s1], ((g - 2) / CH4TC_STAGES) & 1)) {
+              if (g + 1 >= (unsigned)CH4TC_STAGES &&
+                  !mbar_wait(&bar_mma[s1], ((g + 1 - CH4TC_STAGES) / CH4TC_STAGES) & 1)) {
                 bad_s = 1;
                 atomicExch(a.err, 1);
               } else {
@@ -440,11 +445,11 @@ __global__ void __launch_bounds__(CH4TC_THREADS, 1) ch4_dipole_tc_kernel(Ch4TcAr
             }
           }
         }
-        // stage (g + 1) % 3 is free for the next chunk's A once thread 0 has seen chunk
-        // g - 2's MMAs complete (above)
+        // stage (g + 1) % STAGES is free for the next chunk's A once thread 0 has seen its
+        // last MMAs complete (above)
         __syncthreads();
       }
-      // ---- all MMAs of this pass done: read the accumulators ----
+      // ---- all MMAs of this pass done: the quarters' partial sums from TMEM ----
       if (t == 0 && !bad_s) {
         if (!mbar_wait(&bar_mma[(g - 1) % CH4TC_STAGES], ((g - 1) / CH4TC_STAGES) & 1)) {
           bad_s = 1;
@@ -454,29 +459,37 @@ __global__ void __launch_bounds__(CH4TC_THREADS, 1) ch4_dipole_tc_kernel(Ch4TcAr
       __syncthreads();
       tc_fence_after();
       if (!bad_s) {
-        const uint32_t lane_addr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+        float v;
         if (q == 0) {
-          const float v = ch4tc_y1_dot(lane_addr + (half ? CH4TC_COL1 : 0u), n1);
-          if (half) acc1_s[row] = v;
-          else acc[0] = v;
-        } else if (half == 0) {
-          acc[2] = ch4tc_y1_dot(lane_addr, n1);
+          const int comp = qt >> 1;
+          v = (qt & 1) ? ch4tc_y1_dot_m(lane_addr + (comp ? CH4TC_COL1 : 0u), n1, CH4TC_Y1_SPLIT, CH4_L1 + 1)
+                       : ch4tc_y1_dot_m(lane_addr + (comp ? CH4TC_COL1 : 0u), n1, 0, CH4TC_Y1_SPLIT);
+        } else {
+          v = ch4tc_y1_dot_m(lane_addr, n1, CH4TC_Y1_M[qt], CH4TC_Y1_M[qt + 1]);
         }
+        part_s[qt][row] = v;
       }
       // the accumulators are rewritten by the next pass's first MMAs
       tc_fence_before();
       __syncthreads();
       tc_fence_after();
+      if (qt == 0) {
+        if (q == 0) {
+          acc[0] = part_s[0][row] + part_s[1][row];
+          acc[1] = part_s[2][row] + part_s[3][row];
+        } else {
+          acc[2] = (part_s[0][row] + part_s[1][row]) + (part_s[2][row] + part_s[3][row]);
+        }
+      }
     }
     if (bad_s) break;
-    acc[1] = acc1_s[row];  // written before the pass-end barrier above
     if (seg == CH4_NSEG - 1) {
       const float i2 = 1.f / (R * R);
       const float i6 = i2 * i2 * i2;
 #pragma unroll
       for (int cc = 0; cc < 3; ++cc) acc[cc] *= i6;
     }
-    if (half == 0 && mine >= 0) {
+    if (qt == 0 && mine >= 0) {
       float *o = a.mu + (size_t)mine * 4;
 #pragma unroll
       for (int i = 0; i < 3; ++i) o[i] = M[i][0] * acc[0] + M[i][1] * acc[1] + M[i][2] * acc[2];
