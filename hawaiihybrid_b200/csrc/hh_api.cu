@@ -653,12 +653,15 @@ int run_deferred_sys(const TrajParams &P, const TrajIO &io, long long traj_base)
   return HH_OK;
 }
 
-// the launch's item starts (CO2-Ar) into buf, which then backs io.setup
+// the launch's item starts (mixed path: CO2-Ar, CH4-CO2) into buf, which then backs
+// io.setup
 using DeferStart = ItemStart<12, float, float>;
+using Ch4Start = ItemStart<19, float, float>;
 int run_item_starts(const TrajParams &P, TrajIO &io, unsigned char *buf) {
-  if (g.sys != SYS_CO2AR) return HH_OK;
-  auto k = item_start_kernel<float, float>;
-  const size_t smem = smem_tables_bytes<float>();
+  if (g.sys != SYS_CO2AR && g.sys != SYS_CH4CO2) return HH_OK;
+  auto k = (g.sys == SYS_CO2AR) ? item_start_kernel<SYS_CO2AR, float, float>
+                                : item_start_kernel<SYS_CH4CO2, float, float>;
+  const size_t smem = (g.sys == SYS_CO2AR) ? smem_tables_bytes<float>() : 0;
   if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 256, smem));
@@ -839,6 +842,12 @@ int run_records_t(const TrajParams &P, const double *d_ic, uint64_t n, uint64_t 
     for (int k = 0; k < 3; ++k) io.inv_I1[k] = 1.0 / g.sx.II1[k];
     io.lj = g.sx.lj;
     io.item_trace = trace ? trace + 2 * base : nullptr;
+    if (precision == HH_PRECISION_MIXED) {
+      // item starts precomputed, one thread per item (the refills then load them)
+      CK(g.istart.ensure(2 * chunk * sizeof(Ch4Start)));
+      int rc1 = run_item_starts(P, io, g.istart.p);
+      if (rc1) return rc1;
+    }
     int rc = (precision == HH_PRECISION_MIXED) ? launch_traj<SYS_CH4CO2, float, float, false>(P, io, nullptr)
                                                : launch_traj<SYS_CH4CO2, double, double, false>(P, io, nullptr);
     if (rc) return rc;

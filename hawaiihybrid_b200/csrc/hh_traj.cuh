@@ -1618,19 +1618,29 @@ __global__ void __launch_bounds__(32 * WARPS, TRAJ_MIN_BLOCKS)
 
 
 // Item starts of a launch's items (io.items or 0 .. n_items - 1), one thread per item:
-// item_setup as the trajectory kernel would run it at the item's refill.  CO2-Ar only.
-template <typename PHYS, typename STG>
+// item_setup as the trajectory kernel would run it at the item's refill (the same
+// out-of-line function of the same system type, so the values are bit-identical).
+// CO2-Ar (surface tables in shared memory) and CH4-CO2.
+template <int SYS, typename PHYS, typename STG>
 __global__ void __launch_bounds__(256) item_start_kernel(TrajParams P, TrajIO io, const Co2arTablesGlobal *gtab,
                                                         void *out) {
-  using Sys = Co2ArSys<PHYS, STG, false, false>;
+  static_assert(SYS == SYS_CO2AR || SYS == SYS_CH4CO2, "item starts of CO2-Ar and CH4-CO2");
+  using Sys = typename std::conditional<SYS == SYS_CO2AR, Co2ArSys<PHYS, STG, false, false>,
+                                        Ch4Co2Sys<PHYS, STG, false, false>>::type;
   extern __shared__ __align__(16) unsigned char is_smem[];
-  Co2arTables<PHYS> *tb = reinterpret_cast<Co2arTables<PHYS> *>(is_smem);
-  load_tables<PHYS>(tb, gtab);
-  __syncthreads();
   Sys sys;
   sys.inv_mu = 1.0 / P.mu;
   sys.inv_II = 1.0 / P.II;
-  sys.tb = tb;
+  if constexpr (SYS == SYS_CO2AR) {
+    Co2arTables<PHYS> *tb = reinterpret_cast<Co2arTables<PHYS> *>(is_smem);
+    load_tables<PHYS>(tb, gtab);
+    __syncthreads();
+    sys.tb = tb;
+  } else {
+#pragma unroll
+    for (int k = 0; k < 3; ++k) sys.inv_I1[k] = io.inv_I1[k];
+    sys.lj = io.lj;
+  }
   auto *o = static_cast<ItemStart<Sys::N, PHYS, STG> *>(out);
   for (int idx = blockIdx.x * blockDim.x + threadIdx.x; idx < io.n_items; idx += gridDim.x * blockDim.x) {
     const int item = io.items ? io.items[idx] : idx;
