@@ -17,7 +17,10 @@ phi is found by the Berlekamp-Massey algorithm on one bit of the untempered
 stream (phi is primitive, so the minimal polynomial of any non-zero bit sequence
 is phi itself).  The script writes the positions of the set bits of x^J mod phi
 for J = HH_MT_SEG_WORDS and J = HH_MT_COARSE * HH_MT_SEG_WORDS, and checks both
-jumps against direct simulation of the stream before it writes the header.
+jumps against direct simulation of the stream before it writes the header.  It also
+writes x^(k J) mod phi for J = HH_MT_SEG_WORDS and k = 1 .. HH_MT_COARSE - 1 (the
+"fine" table), so that every segment of a coarse interval is one jump from the
+interval's start (the products are checked for k = 2 and k = 3 against the stream).
 
 usage: gen_mt_jump.py <output header>
 """
@@ -124,6 +127,18 @@ def x_pow_mod(J: int, phi: int, deg: int) -> int:
     return r
 
 
+def gf2_mulmod(a: int, b: int, phi: int, deg: int) -> int:
+    """a * b mod phi in GF(2)[x]"""
+    r = 0
+    i = 0
+    while a:
+        if a & 1:
+            r ^= b << i
+        a >>= 1
+        i += 1
+    return gf2_mod(r, phi, deg)
+
+
 def jump(words: np.ndarray, m: int, p: int) -> np.ndarray:
     """W(m + J) from the stream words following position m"""
     acc = np.zeros(N, dtype=np.uint32)
@@ -159,6 +174,22 @@ def main():
         mask[0] = 0x80000000     # the low 31 bits of the window's first word are not state
         assert np.array_equal(got & mask, want & mask), name
         print(f"{name}: J = {J} words, {len(tables[name])} set bits, checked against the stream")
+    # the fine table: x^(k SEG) mod phi, k = 1 .. COARSE - 1
+    p1 = x_pow_mod(SEG_WORDS, phi, DEG)
+    fine = [p1]
+    for k in range(2, COARSE):
+        fine.append(gf2_mulmod(fine[-1], p1, phi, DEG))
+    for k in (2, 3):
+        J = k * SEG_WORDS
+        full = stream(st, J // N + 3)
+        got = jump(full, 0, fine[k - 1])
+        mask = np.full(N, 0xFFFFFFFF, dtype=np.uint32)
+        mask[0] = 0x80000000
+        assert np.array_equal(got & mask, full[J:J + N] & mask), k
+        print(f"fine k = {k}: checked against the stream")
+    fine_bits = [[i for i in range(DEG) if (p >> i) & 1] for p in fine]
+    assert fine_bits[0] == tables["seg"]
+    fine_max = max(len(t) for t in fine_bits)
     with open(out, "w") as f:
         f.write("// Generated by gen_mt_jump.py; do not edit.  Jump-ahead tables of the MT19937\n")
         f.write("// stream: the set bits i of x^J mod phi(x), so that the 624-word window J words\n")
@@ -172,6 +203,16 @@ def main():
             for k in range(0, len(t), 16):
                 f.write("  " + ", ".join(str(v) for v in t[k:k + 16]) + ",\n")
             f.write("};\n")
+        f.write(f"#define HH_MT_JUMP_FINE_MAX {fine_max}\n")
+        f.write(f"static const unsigned short hh_mt_jump_fine_n[{COARSE - 1}] = {{"
+                + ", ".join(str(len(t)) for t in fine_bits) + "};\n")
+        f.write(f"static const unsigned short hh_mt_jump_fine[{COARSE - 1}][{fine_max}] = {{\n")
+        for t in fine_bits:
+            f.write("  {\n")
+            for k in range(0, len(t), 16):
+                f.write("    " + ", ".join(str(v) for v in t[k:k + 16]) + ",\n")
+            f.write("  },\n")
+        f.write("};\n")
     print("wrote", out)
 
 

@@ -28,20 +28,34 @@ cudaError_t launch_mt_generate_segments(uint32_t *state, uint32_t *out, int n_se
   e = cudaMemcpyAsync(seg_states, state, MT_N * sizeof(uint32_t), cudaMemcpyDeviceToDevice, st);
   if (e != cudaSuccess) return e;
   const int n_coarse = (n_seg + HH_MT_COARSE - 1) / HH_MT_COARSE;
-  // coarse chain on one CTA: states 0, C, 2C, ...; then the fine chains of each interval
+  // coarse chain on one CTA: states 0, C, 2C, ...; then every other segment state
+  // by one jump from its interval's start (the fine tables follow the segment table
+  // in the same buffer: mt_jump_fine_tables)
   mt_jump_chain_kernel<<<1, MT_JUMP_THREADS, smem, st>>>(seg_states, 0, HH_MT_COARSE, n_coarse - 1, n_seg,
                                                          jump_coarse, HH_MT_JUMP_COARSE_N);
-  mt_jump_chain_kernel<<<n_coarse, MT_JUMP_THREADS, smem, st>>>(seg_states, HH_MT_COARSE, 1, HH_MT_COARSE - 1,
-                                                                n_seg, jump_seg, HH_MT_JUMP_SEG_N);
+  if (n_seg > 1) {
+    e = cudaFuncSetAttribute(mt_jump_fine_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    if (e != cudaSuccess) return e;
+    mt_jump_fine_kernel<<<n_coarse * (HH_MT_COARSE - 1), MT_JUMP_THREADS, smem, st>>>(
+        seg_states, n_seg, jump_seg + MT_FINE_OFFSET, jump_seg + MT_FINE_OFFSET + (HH_MT_COARSE - 1) * HH_MT_JUMP_FINE_MAX);
+  }
   mt_generate_segments_kernel<<<n_seg, 256, 0, st>>>(seg_states, out, n_seg, state);
   return cudaGetLastError();
 }
 
+// *seg holds the segment table, then the fine tables (x^(k J) mod phi, k = 1..31, rows
+// of HH_MT_JUMP_FINE_MAX) and their lengths
 cudaError_t upload_mt_jump_tables(unsigned short **seg, unsigned short **coarse) {
-  cudaError_t e = cudaMalloc(seg, HH_MT_JUMP_SEG_N * sizeof(unsigned short));
+  const size_t n_seg_buf = MT_FINE_OFFSET + (HH_MT_COARSE - 1) * (size_t)HH_MT_JUMP_FINE_MAX + HH_MT_COARSE;
+  cudaError_t e = cudaMalloc(seg, n_seg_buf * sizeof(unsigned short));
   if (e == cudaSuccess) e = cudaMalloc(coarse, HH_MT_JUMP_COARSE_N * sizeof(unsigned short));
   if (e == cudaSuccess)
     e = cudaMemcpy(*seg, hh_mt_jump_seg, sizeof hh_mt_jump_seg, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(*seg + MT_FINE_OFFSET, hh_mt_jump_fine, sizeof hh_mt_jump_fine, cudaMemcpyHostToDevice);
+  if (e == cudaSuccess)
+    e = cudaMemcpy(*seg + MT_FINE_OFFSET + (HH_MT_COARSE - 1) * HH_MT_JUMP_FINE_MAX, hh_mt_jump_fine_n,
+                   sizeof hh_mt_jump_fine_n, cudaMemcpyHostToDevice);
   if (e == cudaSuccess)
     e = cudaMemcpy(*coarse, hh_mt_jump_coarse, sizeof hh_mt_jump_coarse, cudaMemcpyHostToDevice);
   return e;

@@ -175,6 +175,42 @@ __global__ void __launch_bounds__(MT_JUMP_THREADS) mt_jump_chain_kernel(uint32_t
   }
 }
 
+// Fine jumps: CTA b computes segment s = (b / 31) * 32 + b % 31 + 1 (skipping the
+// coarse states, which the chain made) by one jump of k = s % 32 segments from
+// states[s - k] with the table of x^(k J) mod phi, so every segment state of a round
+// is one jump deep instead of a chain of up to 31.
+constexpr size_t MT_FINE_OFFSET = 10240;  // the fine tables' offset in the segment-table buffer
+static_assert(HH_MT_JUMP_FINE_MAX <= 10240, "fine jump table exceeds the buffer");
+__global__ void __launch_bounds__(MT_JUMP_THREADS) mt_jump_fine_kernel(uint32_t *states, int n_seg,
+                                                                      const unsigned short *fine,
+                                                                      const unsigned short *fine_n) {
+  extern __shared__ uint32_t jsm[];
+  uint32_t *win = jsm;                                         // MT_JUMP_WIN words
+  unsigned short *bs = reinterpret_cast<unsigned short *>(jsm + MT_JUMP_WIN);
+  constexpr int PER = HH_MT_COARSE - 1;
+  const long long s = (long long)(blockIdx.x / PER) * HH_MT_COARSE + (blockIdx.x % PER) + 1;
+  if (s >= n_seg) return;  // the whole block
+  const int k = (int)(s % HH_MT_COARSE);
+  const int n_bits = fine_n[k - 1];
+  for (int i = threadIdx.x; i < n_bits; i += blockDim.x) bs[i] = fine[(size_t)(k - 1) * HH_MT_JUMP_FINE_MAX + i];
+  const long long base = s - k;
+  for (int i = threadIdx.x; i < MT_N; i += blockDim.x) win[i] = states[base * MT_N + i];
+  __syncthreads();
+  for (int b = 0; b < 32; ++b) {
+    uint32_t *cur = win + (b + 1) * MT_N;
+    for (int i = threadIdx.x; i < MT_N; i += blockDim.x) cur[i] = win[b * MT_N + i];
+    __syncthreads();
+    mt_refresh_smem(cur);
+  }
+  if (threadIdx.x < MT_N) {
+    const int j = threadIdx.x;
+    uint32_t acc = 0;
+#pragma unroll 4
+    for (int t = 0; t < n_bits; ++t) acc ^= win[bs[t] + j];
+    states[s * MT_N + j] = acc;
+  }
+}
+
 // Segment s: HH_MT_SEG_BLOCKS blocks from states[s], tempered words to
 // out + s * HH_MT_SEG_BLOCKS * 624; the last segment's final block becomes the
 // generator state.
