@@ -93,11 +93,18 @@ __global__ void __launch_bounds__(256) ch4_seg_count_kernel(Ch4SortArgs a) {
   for (int i = threadIdx.x; i < CH4_NSEG; i += blockDim.x) h[i] = 0;
   __syncthreads();
   const long long n = a.n_traj * a.stride;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const long long t = i / a.stride;
-    const int sl = (int)(i - t * a.stride);
-    if (ch4_valid(a.rec_len, t, sl, a.N)) atomicAdd(&h[ch4_seg(a.seg_hi, ch4_rec_R<PHYS>(a.records, i))], 1u);
+  const int lane = threadIdx.x & 31;
+  for (long long b0 = blockIdx.x * (long long)blockDim.x; b0 < n; b0 += (long long)gridDim.x * blockDim.x) {
+    const long long i = b0 + threadIdx.x;
+    int s = -1;
+    if (i < n) {
+      const long long t = i / a.stride;
+      const int sl = (int)(i - t * a.stride);
+      if (ch4_valid(a.rec_len, t, sl, a.N)) s = ch4_seg(a.seg_hi, ch4_rec_R<PHYS>(a.records, i));
+    }
+    // one shared-memory atomic per (warp, piece)
+    const unsigned peers = __match_any_sync(0xffffffffu, s);
+    if (s >= 0 && lane == __ffs(peers) - 1) atomicAdd(&h[s], (unsigned)__popc(peers));
   }
   __syncthreads();
   for (int i = threadIdx.x; i < CH4_NSEG; i += blockDim.x)
@@ -117,17 +124,26 @@ __global__ void ch4_seg_scan_kernel(Ch4SortArgs a) {
   }
 }
 
+// one cursor atomic per (warp, piece): the lanes of a warp that land in the same piece
+// (consecutive slots of a trajectory mostly do) take consecutive positions
 template <typename PHYS>
 __global__ void __launch_bounds__(256) ch4_seg_scatter_kernel(Ch4SortArgs a) {
   const long long n = a.n_traj * a.stride;
-  for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < n;
-       i += (long long)gridDim.x * blockDim.x) {
-    const long long t = i / a.stride;
-    const int sl = (int)(i - t * a.stride);
-    if (!ch4_valid(a.rec_len, t, sl, a.N)) continue;
-    const int s = ch4_seg(a.seg_hi, ch4_rec_R<PHYS>(a.records, i));
-    const unsigned pos = atomicAdd(&a.cursor[s], 1u);
-    a.sorted[a.warp0[s] * a.task + pos] = (int)i;
+  const int lane = threadIdx.x & 31;
+  for (long long b0 = blockIdx.x * (long long)blockDim.x; b0 < n; b0 += (long long)gridDim.x * blockDim.x) {
+    const long long i = b0 + threadIdx.x;
+    int s = -1;
+    if (i < n) {
+      const long long t = i / a.stride;
+      const int sl = (int)(i - t * a.stride);
+      if (ch4_valid(a.rec_len, t, sl, a.N)) s = ch4_seg(a.seg_hi, ch4_rec_R<PHYS>(a.records, i));
+    }
+    const unsigned peers = __match_any_sync(0xffffffffu, s);
+    const int leader = __ffs(peers) - 1;
+    unsigned base = 0;
+    if (s >= 0 && lane == leader) base = atomicAdd(&a.cursor[s], (unsigned)__popc(peers));
+    base = __shfl_sync(0xffffffffu, base, leader);
+    if (s >= 0) a.sorted[a.warp0[s] * a.task + base + __popc(peers & ((1u << lane) - 1u))] = (int)i;
   }
 }
 
