@@ -340,10 +340,17 @@ __global__ void __launch_bounds__(CH4TC_THREADS, 1) ch4_dipole_tc_kernel(Ch4TcAr
     }
     return true;
   };
+  // thread 0's piece of the task whose B it loads: found once per task (seg_of walks
+  // the piece table), not once per chunk
+  long long seg_task = -1;
+  int seg_cached = 0;
   auto issue_load = [&](long long task, int q, int c, int s) {
-    const int seg = seg_of(task * a.task_step);
+    if (task != seg_task) {
+      seg_task = task;
+      seg_cached = seg_of(task * a.task_step);
+    }
     const unsigned bytes = q == 0 ? 2 * CH4TC_IMG0 : 2 * CH4TC_IMG1;
-    ch4tc_load(stB(s), a.blob + ch4tc_blob_off(seg, q, c), bytes, &bar_load[s]);
+    ch4tc_load(stB(s), a.blob + ch4tc_blob_off(seg_cached, q, c), bytes, &bar_load[s]);
   };
   long long task0 = blockIdx.x;
   if (t == 0 && task0 < total) {

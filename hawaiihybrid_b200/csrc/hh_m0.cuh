@@ -132,11 +132,15 @@ __global__ void __launch_bounds__(256) m0_kernel(M0Args a, const Co2arTablesGlob
   if (SYS == SYS_CO2AR) load_tables<PHYS>(tb, gtab);
   if (SYS == SYS_N2AR) load_words(fold, dipnet, sizeof(N2arDipFold));
   __syncthreads();
-  double s[M0_MAXT], c[M0_MAXT], q[M0_MAXT];
+  // per-thread sums of w (compensated) and w^2: FP64 on the FP64 path; on the mixed path
+  // FP32 with compensation (a thread sums a few hundred samples per launch, the block
+  // and launch reductions are FP64)
+  using AT = typename std::conditional<sizeof(PHYS) == 4 && MOMENT == 0, float, double>::type;
+  AT s[M0_MAXT], c[M0_MAXT], q[M0_MAXT];
   PHYS ikT[M0_MAXT];
 #pragma unroll
   for (int t = 0; t < M0_MAXT; ++t) {
-    s[t] = c[t] = q[t] = 0.0;
+    s[t] = c[t] = q[t] = AT(0);
     ikT[t] = PHYS(a.invkT[t]);
   }
   const PHYS Rmin = PHYS(a.Rmin), dR = PHYS(a.Rmax - a.Rmin);
@@ -193,9 +197,8 @@ __global__ void __launch_bounds__(256) m0_kernel(M0Args a, const Co2arTablesGlob
       PHYS sT = sqrt((PHYS(1) - cT) * (PHYS(1) + cT));
       PHYS st = sqrt((PHYS(1) - ct) * (PHYS(1) + ct));
       PHYS x = sT * st * cos(Phi - ph) + cT * ct;
-      PHYS VR, Vx;
       PHYS iR = PHYS(1) / R;
-      co2ar_pes<PHYS, COMP>(tb->pes, tb->fpes, tb->rbound, tb->rlo, R, iR, x, V, VR, Vx, true);
+      V = co2ar_pes_value<PHYS, COMP>(tb->pes, tb->fpes, tb->rbound, tb->rlo, R, iR, x);
       PHYS dz, ax;
       co2ar_dip<PHYS, COMP>(tb->dipx, tb->dipz, tb->fdip, tb->rbound, tb->rlo, R, iR, x, dz, ax);
       mu2 = dz * dz + ax * ax * (PHYS(1) - x) * (PHYS(1) + x);
@@ -214,11 +217,11 @@ __global__ void __launch_bounds__(256) m0_kernel(M0Args a, const Co2arTablesGlob
         bool keep = true;
         if (a.pair_state == 1) keep = (H >= PHYS(0));
         else if (a.pair_state == 2) keep = (H <= PHYS(0));
-        double wv = keep ? double(base * exp(-V * ikT[t])) : 0.0;
-        if constexpr (MOMENT == 2) wv *= double(kappa / ikT[t]);  // (2K/nu) G with K = kappa kT
+        AT wv = keep ? AT(base * exp(-V * ikT[t])) : AT(0);
+        if constexpr (MOMENT == 2) wv *= AT(kappa / ikT[t]);  // (2K/nu) G with K = kappa kT
         // compensated accumulation of w, plain accumulation of w^2
-        double y = wv - c[t];
-        double tt = s[t] + y;
+        AT y = wv - c[t];
+        AT tt = s[t] + y;
         c[t] = (tt - s[t]) - y;
         s[t] = tt;
         q[t] += wv * wv;
@@ -230,7 +233,7 @@ __global__ void __launch_bounds__(256) m0_kernel(M0Args a, const Co2arTablesGlob
   int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
 #pragma unroll
   for (int t = 0; t < M0_MAXT; ++t) {
-    double v = s[t] - c[t], vq = q[t];
+    double v = double(s[t]) - double(c[t]), vq = double(q[t]);
 #pragma unroll
     for (int o = 16; o > 0; o >>= 1) {
       v += __shfl_down_sync(0xffffffffu, v, o);

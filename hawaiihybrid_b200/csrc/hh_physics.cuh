@@ -189,6 +189,22 @@ __device__ __forceinline__ void co2ar_pes(const T *tab, const int *flags, const 
   Vx = ax.get() * s;
 }
 
+// V (Hartree) alone at (R, x): the sums of co2ar_pes without the derivatives
+template <typename T, bool COMP>
+__device__ __forceinline__ T co2ar_pes_value(const T *tab, const int *flags, const T *rbound, const T *rlo, T R,
+                                             T iR, T x) {
+  int i = co2ar_interval<T>(R, rbound);
+  T P[11], dP[11];
+  legendre10(x, P, dP);
+  T t = R - rlo[i];
+  int fl = flags[i];
+  Acc<T> aV;
+  const T *base = tab + i * CO2AR_NL * CO2AR_ROW;
+#pragma unroll
+  for (int li = 0; li < CO2AR_NL; ++li) aV.add(P[2 * li] * radial_value<T>(base + li * CO2AR_ROW, R, t, iR, fl), COMP);
+  return aV.get() * T(1.0 / HH_HTOCM);
+}
+
 // body-frame dipole sums: dz = sum b_l P_l(x), ax = sum a_l P_l'(x)
 template <typename T, bool COMP>
 __device__ __forceinline__ void co2ar_dip(const T *tabx, const T *tabz, const int *flags,

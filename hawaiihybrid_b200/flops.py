@@ -35,11 +35,13 @@ SYSTEMS = {
     "n2ar": dict(n=12, nq=6, rhs=2960, rhs_fp64_kin=15, dip=490, dip_fp64=6500),
 }
 
-# Monte Carlo moment integrand per sample (hh_m0.cuh), surface-precision part and
-# FP64 part (the 16 compensated sums of w and sums of w^2: 6 FP64 operations per
-# temperature).  CO2-Ar: angle transforms (30), surface value and gradient rows
-# (180), dipole sums (170), |mu|^2 (5), per temperature H, exp, weight (5 each).
-M0_PER_SAMPLE = {"co2ar": dict(phys=30 + 180 + 170 + 5, per_T=5, per_T_fp64=6)}
+# Monte Carlo moment integrand per sample (hh_m0.cuh), surface-precision part and the
+# part in the accumulation precision (the compensated sum of w and the sum of w^2: 6
+# operations per temperature, FP64 on the FP64 path, compensated FP32 on the mixed
+# path).  CO2-Ar: angle transforms (30), surface value (Legendre recursion 40, six
+# radial values 60, sums 12: 112), dipole sums (170), |mu|^2 (5), per temperature H,
+# exp, weight (5 each).
+M0_PER_SAMPLE = {"co2ar": dict(phys=30 + 112 + 170 + 5, per_T=5, per_T_acc=6)}
 
 # CH4-CO2 batched dipole (ch4_dipole_kernel) per record: 4 FMA per (padded) entry
 # of the coefficient stream (the per-power sums), Horner and Y1 product per group
@@ -87,10 +89,10 @@ def m0_work(system: str, n_samples: int, nT: int, mixed: bool) -> dict:
     """FP32 and FP64 flops of one M0 call over n_samples samples and nT temperatures."""
     c = M0_PER_SAMPLE[system]
     phys = n_samples * (c["phys"] + nT * c["per_T"])
-    f64 = n_samples * nT * c["per_T_fp64"]
+    acc = n_samples * nT * c["per_T_acc"]
     if mixed:
-        return {"fp32": float(phys), "fp64": float(f64)}
-    return {"fp32": 0.0, "fp64": float(phys + f64)}
+        return {"fp32": float(phys + acc), "fp64": 0.0}
+    return {"fp32": 0.0, "fp64": float(phys + acc)}
 
 
 def sample_work(system: str, stats: dict, mixed: bool) -> dict:

@@ -23,8 +23,12 @@ def test_moment_sums_partition(name, moment, prec):
     sw, sw2 = H.moment_sums(ms, p, T, n, 0, seed=77, moment=moment, precision=prec)
     parts = [H.moment_sums(ms, p, T, n // 3, r * (n // 3), seed=77, moment=moment, precision=prec)
              for r in range(3)]
-    np.testing.assert_allclose(sum(a for a, _ in parts), sw, rtol=1e-12)
-    np.testing.assert_allclose(sum(b for _, b in parts), sw2, rtol=1e-12)
+    # the mixed path sums a thread's samples in compensated FP32 (the block and launch
+    # reductions are FP64), so another split of the samples over threads rounds
+    # differently at the 1e-10 level; the FP64 path agrees to its own rounding
+    rt = 1e-8 if prec == 1 else 1e-12
+    np.testing.assert_allclose(sum(a for a, _ in parts), sw, rtol=rt)
+    np.testing.assert_allclose(sum(b for _, b in parts), sw2, rtol=rt)
     # the moments of the whole range equal the library's own M0 / M2
     m, e = H.moment_from_sums(sw, sw2, n, H.moment_scale(p, moment))
     if moment == 0:
