@@ -92,10 +92,11 @@ def parse():
     ap.add_argument("--ch4co2-per-T", type=int, default=CH4CO2["n_per_T"])
     ap.add_argument("--only", choices=["n2ar", "ch4co2", "hear", "m0"],
                     help="run only this workload and print its block as the JSON line")
-    ap.add_argument("--profile-case", choices=["co2ar", "co2ar_multi", "ch4co2"],
+    ap.add_argument("--profile-case", choices=["co2ar", "co2ar_multi", "ch4co2", "m0"],
                     help="run a small case of a workload twice for an ncu capture (the second "
                          "call is the one to capture) and exit: co2ar one iteration and co2ar_multi "
-                         "8 iterations of 16,384 mixed trajectories; ch4co2 4 x 16,384 mixed")
+                         "8 iterations of 16,384 mixed trajectories; ch4co2 4 x 16,384 mixed; m0 "
+                         "16 temperatures x 2e7 mixed samples")
     return ap.parse_args()
 
 
@@ -109,6 +110,14 @@ def profile_case(args, hh, H):
         K = 1 if args.profile_case == "co2ar" else 8
         for _ in range(2):
             _, _, st = hh.correlation_iterations(ms, p, w["T"], 16384, K, hh.PRECISION_MIXED, seed=w["seed"])
+    elif args.profile_case == "m0":
+        c = M0CFG
+        ms = hh.init_ms(w["mu"], hh.LINEAR_MOLECULE, hh.ATOM, (w["II"], w["II"]), None, 1)
+        p = _params(H, dict(w, Rmin=c["Rmin"], Rmax=c["Rmax"]), w["fp64_tol"], args.mixed_tol, N=64)
+        for _ in range(2):
+            m, _ = hh.calculate_m0(ms, p, np.array(c["Ts"]), 20_000_000, seed=c["seed"], precision=hh.PRECISION_MIXED)
+        print(json.dumps({"profile_case": "m0", "m0": [float(x) for x in m[:2]]}), flush=True)
+        return 0
     else:
         c = CH4CO2
         ms = hh.init_ms(c["mu"], hh.ROTOR, hh.LINEAR_MOLECULE, (c["II1"],) * 3, (c["II2"], c["II2"]), c["seed"])
@@ -205,7 +214,8 @@ def bench_hear(args, hh, H, peaks):
 
 def bench_m0(args, hh, H, peaks):
     """CO2-Ar Monte Carlo zeroth moment: 16 temperatures from 150 to 400 K, 1e8 samples each,
-    all temperatures in one launch; FP32 integrand (FP64 compensated sums) against FP64."""
+    all temperatures in one launch; FP32 integrand and per-thread compensated FP32 sums (FP64
+    block and launch reductions) against FP64."""
     from hawaiihybrid_b200 import _lib, flops
     w, c = WORKLOAD, M0CFG
     ms = hh.init_ms(w["mu"], hh.LINEAR_MOLECULE, hh.ATOM, (w["II"], w["II"]), None, 1)

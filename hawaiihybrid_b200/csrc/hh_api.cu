@@ -658,16 +658,27 @@ int run_deferred_sys(const TrajParams &P, const TrajIO &io, long long traj_base)
 using DeferStart = ItemStart<12, float, float>;
 using Ch4Start = ItemStart<19, float, float>;
 int run_item_starts(const TrajParams &P, TrajIO &io, unsigned char *buf) {
-  if (g.sys != SYS_CO2AR && g.sys != SYS_CH4CO2) return HH_OK;
-  auto k = (g.sys == SYS_CO2AR) ? item_start_kernel<SYS_CO2AR, float, float>
-                                : item_start_kernel<SYS_CH4CO2, float, float>;
-  const size_t smem = (g.sys == SYS_CO2AR) ? smem_tables_bytes<float>() : 0;
+  if (g.sys != SYS_CO2AR && g.sys != SYS_N2AR && g.sys != SYS_CH4CO2) return HH_OK;
+  TrajIO is = io;
+  auto k = item_start_kernel<SYS_CH4CO2, float, float>;
+  size_t smem = 0;
+  if (g.sys == SYS_CO2AR) {
+    k = item_start_kernel<SYS_CO2AR, float, float>;
+    smem = smem_tables_bytes<float>();
+  } else if (g.sys == SYS_N2AR) {
+    // the mixed path's networks, as run_traj_dispatch gives them
+    k = item_start_kernel<SYS_N2AR, float, float>;
+    smem = sizeof(N2arDipFold) + sizeof(N2arPesNet<float>);
+    is.dipnet = g.d_n2ar_fold;
+    is.pesnet = g.d_n2ar_pes_f;
+    is.diptab = g.d_n2ar_tab;
+  }
   if (smem > 48 * 1024) CK(cudaFuncSetAttribute(k, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k, 256, smem));
   const int grid = std::max(1, std::min(per_sm * g.num_sms, (io.n_items + 255) / 256));
   kt_begin();
-  k<<<grid, 256, smem, g.st>>>(P, io, g.d_tab, buf);
+  k<<<grid, 256, smem, g.st>>>(P, is, g.d_tab, buf);
   CK(cudaGetLastError());
   kt_end(HH_KT_ITEM_START);
   g_launches += 1;
@@ -1093,7 +1104,16 @@ int run_plain(int precision, const TrajParams &P, const TrajIO &io0, uint64_t n,
       io.item_status = g.item_status.p;
       io.item_mu0 = g.item_mu0.p;
     }
+    // item starts precomputed for the mixed N2-Ar path (its refill set-up evaluates the
+    // PIP-NN surface twice and the dipole once on one lane)
+    const bool starts = !defer && precision == HH_PRECISION_MIXED && g.sys == SYS_N2AR && io.n_sat == 0 &&
+                        !io.series && !io.records;
     if (!defer) {
+      if (starts) {
+        CK(g.istart.ensure(2 * n * sizeof(DeferStart)));
+        int rc = run_item_starts(P, io, g.istart.p);
+        if (rc) return rc;
+      }
       int rc = run_traj_dispatch(precision, P, io);
       if (rc) return rc;
     } else {
@@ -1156,7 +1176,7 @@ int run_plain(int precision, const TrajParams &P, const TrajIO &io0, uint64_t n,
         if (io2.ctx_cap > g.dvals.cap / (2 * sizeof(float))) io2.ctx_cap = g.dvals.cap / (2 * sizeof(float));
         CK(cudaMemsetAsync(g.dcount.p, 0, 2 * sizeof(unsigned long long), g.st));
       }
-      if (defer) {
+      if (defer || starts) {
         int rc = run_item_starts(P2, io2, g.istart.p);
         if (rc) return rc;
       }

@@ -1620,13 +1620,16 @@ __global__ void __launch_bounds__(32 * WARPS, TRAJ_MIN_BLOCKS)
 // Item starts of a launch's items (io.items or 0 .. n_items - 1), one thread per item:
 // item_setup as the trajectory kernel would run it at the item's refill (the same
 // out-of-line function of the same system type, so the values are bit-identical).
-// CO2-Ar (surface tables in shared memory) and CH4-CO2.
+// CO2-Ar (surface tables in shared memory), N2-Ar (the networks in shared memory) and
+// CH4-CO2.
 template <int SYS, typename PHYS, typename STG>
 __global__ void __launch_bounds__(256) item_start_kernel(TrajParams P, TrajIO io, const Co2arTablesGlobal *gtab,
                                                         void *out) {
-  static_assert(SYS == SYS_CO2AR || SYS == SYS_CH4CO2, "item starts of CO2-Ar and CH4-CO2");
-  using Sys = typename std::conditional<SYS == SYS_CO2AR, Co2ArSys<PHYS, STG, false, false>,
-                                        Ch4Co2Sys<PHYS, STG, false, false>>::type;
+  static_assert(SYS == SYS_CO2AR || SYS == SYS_N2AR || SYS == SYS_CH4CO2, "item starts of a linear or rotor system");
+  using Sys = typename std::conditional<
+      SYS == SYS_CO2AR, Co2ArSys<PHYS, STG, false, false>,
+      typename std::conditional<SYS == SYS_N2AR, N2ArSys<PHYS, STG, false, false>,
+                                Ch4Co2Sys<PHYS, STG, false, false>>::type>::type;
   extern __shared__ __align__(16) unsigned char is_smem[];
   Sys sys;
   sys.inv_mu = 1.0 / P.mu;
@@ -1636,6 +1639,15 @@ __global__ void __launch_bounds__(256) item_start_kernel(TrajParams P, TrajIO io
     load_tables<PHYS>(tb, gtab);
     __syncthreads();
     sys.tb = tb;
+  } else if constexpr (SYS == SYS_N2AR) {
+    N2arDipFold *fold = reinterpret_cast<N2arDipFold *>(is_smem);
+    N2arPesNet<PHYS> *pes = reinterpret_cast<N2arPesNet<PHYS> *>(is_smem + sizeof(N2arDipFold));
+    load_words(fold, io.dipnet, sizeof(N2arDipFold));
+    load_words(pes, io.pesnet, sizeof(N2arPesNet<PHYS>));
+    __syncthreads();
+    sys.fold = fold;
+    sys.pes = pes;
+    sys.dtab = static_cast<const float4 *>(io.diptab);
   } else {
 #pragma unroll
     for (int k = 0; k < 3; ++k) sys.inv_I1[k] = io.inv_I1[k];
