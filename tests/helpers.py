@@ -1,4 +1,4 @@
-"""Shared fixtures: reference workloads as oracle and library parameters."""
+"""Shared fixtures: the benchmark workloads as oracle and library parameters."""
 import numpy as np
 
 from oracle import oracle as O
