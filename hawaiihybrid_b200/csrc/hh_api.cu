@@ -203,6 +203,7 @@ int g_inject_item = -1, g_inject_k = -1, g_inject_status = 0;
 uint32_t *g_trace_host = nullptr;  // registered by hh_cuda_debug_item_trace for the next call
 uint64_t g_trace_cap = 0;
 
+bool g_co2ar_dip_exp = false;  // a CO2-Ar dipole interval with exponential terms
 void build_tables(Co2arTablesGlobal *t) {
   memcpy(t->pes, hh_co2ar_pes, sizeof(t->pes));
   memcpy(t->dipx, hh_co2ar_dipx, sizeof(t->dipx));
@@ -224,6 +225,7 @@ void build_tables(Co2arTablesGlobal *t) {
     }
     t->fpes[i] = fp;
     t->fdip[i] = fd;
+    if (fd & 2) g_co2ar_dip_exp = true;
   }
 }
 
@@ -605,7 +607,8 @@ int g_defer = [] {
   return e ? atoi(e) : 1;
 }();
 bool defer_eligible(int precision, const TrajParams &P, const TrajIO &io) {
-  const bool sys_ok = g.sys == SYS_CO2AR ? g_defer >= 1 : (g.sys == SYS_N2AR && g_defer >= 2);
+  // the CO2-Ar sample kernel evaluates dipole intervals without exponential terms
+  const bool sys_ok = g.sys == SYS_CO2AR ? g_defer >= 1 && !g_co2ar_dip_exp : (g.sys == SYS_N2AR && g_defer >= 2);
   return sys_ok && precision == HH_PRECISION_MIXED && io.n_sat == 0 && !io.series && !io.records && !P.prmu &&
          (P.inject_item < 0 || P.inject_status >= HH_ST_NAN_DIPOLE);
 }
@@ -628,13 +631,14 @@ int run_deferred_sys(const TrajParams &P, const TrajIO &io, long long traj_base)
   a.last_v = g.dvals.p + io.ctx_cap * sizeof(float);
   a.crln = io.crln;
   a.traj_per_iter = io.traj_per_iter;
+  a.inv_traj_per_iter = 1.0 / double(io.traj_per_iter);
   a.status_hist = io.status_hist;
   a.fail_flag = io.fail_flag;
   a.fail_list = io.fail_list;
   a.fail_count = io.fail_count;
   a.traj_base = traj_base;
   a.peak = g.dcount.p + 1;
-  auto eval = defer_eval_kernel<SYS, float, float>;
+  auto eval = SYS == SYS_CO2AR ? defer_eval_co2ar_kernel<float, float> : defer_eval_kernel<SYS_N2AR, float, float>;
   const size_t smem = DeferSys<SYS, float, float>::smem();
   if (smem > 48 * 1024) CK(cudaFuncSetAttribute(eval, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
