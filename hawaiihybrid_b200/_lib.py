@@ -46,7 +46,8 @@ EXPORTS = (
     "hh_cuda_shutdown", "hh_cuda_m0_noalloc", "hh_cuda_correlation_array", "hh_cuda_correlation_temperatures",
     "hh_cuda_prmu", "hh_cuda_debug_n2ar_dipole", "hh_cuda_m2", "hh_cuda_debug_tuning",
     "hh_cuda_debug_kernel_ms", "hh_cuda_debug_ch4co2_fold", "hh_cuda_moment_sums", "hh_cuda_debug_traj_tuning",
-    "hh_cuda_debug_set_ch4_dipole", "hh_cuda_debug_set_defer", "hh_cuda_vegas", "hh_cuda_set_requantization",
+    "hh_cuda_debug_set_ch4_dipole", "hh_cuda_debug_set_defer", "hh_cuda_debug_set_defer_overlap", "hh_cuda_vegas",
+    "hh_cuda_set_requantization",
     "hh_write_correlation_function_ext", "hh_write_spectral_function_ext",
 )
 HH_REQ_NONE, HH_REQ_INTEGER, HH_REQ_HALFINTEGER = 0, 1, 2
@@ -153,6 +154,7 @@ def load(path: str | None = None):
     L.hh_cuda_debug_ch4co2_fold.argtypes = [C.POINTER(C.c_int), C.POINTER(C.c_int)]
     L.hh_cuda_debug_set_ch4_dipole.argtypes = [C.c_int, C.c_int]
     L.hh_cuda_debug_set_defer.argtypes = [C.c_int, C.POINTER(C.c_int)]
+    L.hh_cuda_debug_set_defer_overlap.argtypes = [C.c_int, C.POINTER(C.c_int)]
     L.hh_cuda_set_requantization.argtypes = [C.POINTER(Requantization)]
     L.hh_cuda_vegas.argtypes = [C.POINTER(CalcParamsC), C.c_int, C.c_double, C.c_uint64, C.c_uint64, C.c_uint64,
                                 C.POINTER(C.c_double), C.POINTER(C.c_double)]
@@ -193,6 +195,15 @@ def defer_samples(mode: int = -1) -> int:
     -1 only reads it.  Returns the mode before the call."""
     prev = C.c_int(0)
     check(load().hh_cuda_debug_set_defer(int(mode), C.byref(prev)))
+    return prev.value
+
+
+def defer_overlap(on: int = -1) -> int:
+    """Whether deferred samples of the bulk trajectory launch are evaluated beside the
+    solo launch (hh_cuda_debug_set_defer_overlap): 1 yes, 0 after it, -1 only reads.
+    Returns the setting before the call."""
+    prev = C.c_int(0)
+    check(load().hh_cuda_debug_set_defer_overlap(int(on), C.byref(prev)))
     return prev.value
 
 

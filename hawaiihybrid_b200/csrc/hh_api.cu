@@ -98,6 +98,12 @@ struct Ctx {
   cudaStream_t st2 = nullptr;
   cudaEvent_t ev_sampled = nullptr, ev_pregen = nullptr;
   bool pregen_pending = false;
+  // deferred samples: the contexts the bulk trajectory kernel wrote are evaluated on
+  // st3 (lowest priority; st has the highest) while the solo kernel runs; ev_bulk
+  // follows the snapshot of their count, ev_eval1 the first sample launch
+  cudaStream_t st3 = nullptr;
+  cudaEvent_t ev_bulk = nullptr, ev_eval1 = nullptr;
+  bool bulk_snap = false;  // the last trajectory launch snapshotted its context count
   int num_sms = 0;
   Co2arTablesGlobal *d_tab = nullptr;
   N2arDipFold *d_n2ar_fold = nullptr;  // N2-Ar dipole models, folded (hh_n2ar_fold.h)
@@ -398,6 +404,13 @@ int sample_into(const hh_calc_params *p, double T, uint64_t n, double *d_out, ui
   return HH_OK;
 }
 
+// HH_DEFER_OVERLAP (default 1; 0 off): with deferred samples, the contexts of the bulk
+// trajectory kernel are evaluated while the solo kernel runs
+int g_defer_overlap = [] {
+  const char *e = getenv("HH_DEFER_OVERLAP");
+  return e ? atoi(e) : 1;
+}();
+
 // One trajectory launch: the bulk kernel (WARPS warps per block) until at most
 // cap / handoff_div items are open, then the solo kernel for the rest, where cap is
 // the solo kernel's warp slots.  With ev_split, events ev[4] (start), ev[5] (after the
@@ -435,12 +448,22 @@ int launch_traj_w(const TrajParams &P, const TrajIO &io, int handoff_div, bool e
   io2.done = g.hcount.p + 2;
   io2.handoff_at = std::max(1u, cap / (unsigned)std::max(1, handoff_div));
   if (ev_split) CK(cudaEventRecord(g.ev[4], g.st));
+  g.bulk_snap = false;
   if ((unsigned)io.n_items > cap) {
     kt_begin();
     kern<<<grid, THREADS, smem, g.st>>>(P, io2, g.d_tab);
     CK(cudaGetLastError());
     kt_end(HH_KT_TRAJ_BULK);
     g_launches += 1;
+    // deferred samples: the count of the contexts the bulk kernel wrote, for the first
+    // sample launch beside the solo kernel (not while kernels are timed one by one)
+    if (io.ctx && g_defer_overlap && !g_kt.on) {
+      defer_snapshot_kernel<<<1, 1, 0, g.st>>>(io.ctx_count);
+      CK(cudaGetLastError());
+      CK(cudaEventRecord(g.ev_bulk, g.st));
+      g.bulk_snap = true;
+      g_launches += 1;
+    }
   }
   if (ev_split) CK(cudaEventRecord(g.ev[5], g.st));
   kt_begin();
@@ -637,16 +660,35 @@ int run_deferred_sys(const TrajParams &P, const TrajIO &io, long long traj_base)
   a.fail_list = io.fail_list;
   a.fail_count = io.fail_count;
   a.traj_base = traj_base;
-  a.peak = g.dcount.p + 1;
+  a.peak = g.dcount.p + DEFER_PEAK;
   auto eval = SYS == SYS_CO2AR ? defer_eval_co2ar_kernel<float, float> : defer_eval_kernel<SYS_N2AR, float, float>;
   const size_t smem = DeferSys<SYS, float, float>::smem();
   if (smem > 48 * 1024) CK(cudaFuncSetAttribute(eval, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
   int per_sm = 0;
   CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eval, DEFER_THREADS, smem));
   const int grid = std::max(1, per_sm) * g.num_sms;
+  unsigned long long *cnt = io.ctx_count;
   kt_begin();
-  eval<<<grid, DEFER_THREADS, smem, g.st>>>(a, P, io, g.d_tab);
-  CK(cudaGetLastError());
+  if (g.bulk_snap) {
+    // the bulk kernel's contexts on st3 beside the solo kernel (whose blocks st's
+    // priority places first), the solo kernel's after it on st
+    DeferArgs a1 = a;
+    a1.ctx_hi = cnt + DEFER_SNAP;
+    CK(cudaStreamWaitEvent(g.st3, g.ev_bulk, 0));
+    eval<<<grid, DEFER_THREADS, smem, g.st3>>>(a1, P, io, g.d_tab);
+    CK(cudaGetLastError());
+    CK(cudaEventRecord(g.ev_eval1, g.st3));
+    DeferArgs a2 = a;
+    a2.ctx_lo = cnt + DEFER_SNAP;
+    eval<<<grid, DEFER_THREADS, smem, g.st>>>(a2, P, io, g.d_tab);
+    CK(cudaGetLastError());
+    CK(cudaStreamWaitEvent(g.st, g.ev_eval1, 0));
+    g.bulk_snap = false;
+    g_launches += 1;
+  } else {
+    eval<<<grid, DEFER_THREADS, smem, g.st>>>(a, P, io, g.d_tab);
+    CK(cudaGetLastError());
+  }
   defer_jump_kernel<float, float, 6><<<8 * g.num_sms, DEFER_THREADS, 0, g.st>>>(a, P);
   CK(cudaGetLastError());
   defer_items_kernel<float><<<(unsigned)std::max(1, (io.n_items + DEFER_THREADS - 1) / DEFER_THREADS),
@@ -1095,7 +1137,7 @@ int run_plain(int precision, const TrajParams &P, const TrajIO &io0, uint64_t n,
       const size_t alloc = (size_t)(1.1 * double(cap));
       if (g.dctx.cap < cap * sizeof(DeferCtx)) CK(g.dctx.ensure(alloc * sizeof(DeferCtx)));
       if (g.dvals.cap < cap * 2 * sizeof(float)) CK(g.dvals.ensure(alloc * 2 * sizeof(float)));
-      CK(g.dcount.ensure(2));
+      CK(g.dcount.ensure(DEFER_WORDS));
       CK(g.item_status.ensure(2 * n));
       CK(g.item_mu0.ensure(2 * n * 4 * sizeof(float)));
       CK(g.item_fail.ensure(2 * n));
@@ -1146,7 +1188,7 @@ int run_plain(int precision, const TrajParams &P, const TrajIO &io0, uint64_t n,
     int nfail = 0;
     unsigned long long peak = 0;
     CK(cudaMemcpyAsync(&nfail, g.fail_count.p, sizeof nfail, cudaMemcpyDeviceToHost, g.st));
-    if (defer) CK(cudaMemcpyAsync(&peak, g.dcount.p + 1, sizeof peak, cudaMemcpyDeviceToHost, g.st));
+    if (defer) CK(cudaMemcpyAsync(&peak, g.dcount.p + DEFER_PEAK, sizeof peak, cudaMemcpyDeviceToHost, g.st));
     CK(cudaStreamSynchronize(g.st));
     if (defer) {
       const double per = double(peak) / double(std::max<uint64_t>(1, items_launch));
@@ -1189,7 +1231,7 @@ int run_plain(int precision, const TrajParams &P, const TrajIO &io0, uint64_t n,
       if (defer) {
         rc = run_deferred(P2, io2, 0);
         if (rc) return rc;
-        CK(cudaMemcpyAsync(&peak, g.dcount.p + 1, sizeof peak, cudaMemcpyDeviceToHost, g.st));
+        CK(cudaMemcpyAsync(&peak, g.dcount.p + DEFER_PEAK, sizeof peak, cudaMemcpyDeviceToHost, g.st));
         CK(cudaStreamSynchronize(g.st));
         if (peak > io2.ctx_cap) {
           g.defer_est *= 2.0;
@@ -1513,8 +1555,13 @@ int hh_cuda_init(int device, const hh_system_desc *sys) {
   CK(cudaSetDevice(device));
   if (!g.init) {
     m0_noalloc_forget();
-    CK(cudaStreamCreateWithFlags(&g.st, cudaStreamNonBlocking));
+    int prio_low = 0, prio_high = 0;
+    CK(cudaDeviceGetStreamPriorityRange(&prio_low, &prio_high));
+    CK(cudaStreamCreateWithPriority(&g.st, cudaStreamNonBlocking, prio_high));
     CK(cudaStreamCreateWithFlags(&g.st2, cudaStreamNonBlocking));
+    CK(cudaStreamCreateWithPriority(&g.st3, cudaStreamNonBlocking, prio_low));
+    CK(cudaEventCreateWithFlags(&g.ev_bulk, cudaEventDisableTiming));
+    CK(cudaEventCreateWithFlags(&g.ev_eval1, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&g.ev_sampled, cudaEventDisableTiming));
     CK(cudaEventCreateWithFlags(&g.ev_pregen, cudaEventDisableTiming));
     for (auto &e : g.ev) CK(cudaEventCreate(&e));
@@ -2353,6 +2400,13 @@ int hh_cuda_debug_set_defer(int mode, int *previous) {
   return HH_OK;
 }
 
+int hh_cuda_debug_set_defer_overlap(int on, int *previous) {
+  if (on < -1 || on > 1) return HH_E_INVALID_ARGUMENT;
+  if (previous) *previous = g_defer_overlap;
+  if (on >= 0) g_defer_overlap = on;
+  return HH_OK;
+}
+
 int hh_cuda_debug_ch4co2_fold(int *n_batch, int *n_groups) {
   if (!g.init || !g.d_ch4_cd) return HH_E_NOT_INITIALIZED;
   if (n_batch) *n_batch = g.ch4_B;
@@ -2532,6 +2586,9 @@ void hh_cuda_shutdown(void) {
     if (e) cudaEventDestroy(e);
   if (g.st) cudaStreamDestroy(g.st);
   if (g.st2) cudaStreamDestroy(g.st2);
+  if (g.st3) cudaStreamDestroy(g.st3);
+  if (g.ev_bulk) cudaEventDestroy(g.ev_bulk);
+  if (g.ev_eval1) cudaEventDestroy(g.ev_eval1);
   if (g.ev_sampled) cudaEventDestroy(g.ev_sampled);
   if (g.ev_pregen) cudaEventDestroy(g.ev_pregen);
   g = Ctx();

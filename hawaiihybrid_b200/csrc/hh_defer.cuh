@@ -37,11 +37,19 @@
 namespace hh {
 
 constexpr int DEFER_THREADS = 256;
+// words of the context counter block: the count the trajectory kernels advance, the
+// largest count of a call, and the snapshot of the count after the bulk kernel
+constexpr int DEFER_COUNT = 0, DEFER_PEAK = 1, DEFER_SNAP = 2, DEFER_WORDS = 3;
 
 struct DeferArgs {
   const void *ctx;                      // SampleCtx<STG, NQ>[ctx_cap]
   const unsigned long long *ctx_count;  // contexts written (may exceed ctx_cap)
   unsigned long long ctx_cap;
+  // the sample launch's contexts: [*ctx_lo, *ctx_hi), nullptr standing for 0 and
+  // *ctx_count; warp w of the grid takes the groups of 32 that start at
+  // lo + 32 (w + r W), W warps in the grid (a shared cursor, which balances the end
+  // of a launch better, ran 10 to 30 % slower at a launch of 10^8 contexts)
+  const unsigned long long *ctx_lo, *ctx_hi;
   const int *items;                     // defer_items_kernel: explicit item list or nullptr
   int n_items;
   const int *item_status;               // [item]
@@ -61,6 +69,17 @@ __device__ __forceinline__ unsigned long long defer_count(const DeferArgs &a) {
   const unsigned long long c = *a.ctx_count;
   return c < a.ctx_cap ? c : a.ctx_cap;
 }
+__device__ __forceinline__ unsigned long long defer_hi(const DeferArgs &a) {
+  const unsigned long long c = a.ctx_hi ? *a.ctx_hi : *a.ctx_count;
+  return c < a.ctx_cap ? c : a.ctx_cap;
+}
+__device__ __forceinline__ unsigned long long defer_lo(const DeferArgs &a) {
+  const unsigned long long c = a.ctx_lo ? *a.ctx_lo : 0ull;
+  return c < a.ctx_cap ? c : a.ctx_cap;
+}
+// After the bulk trajectory kernel: the count of the contexts it wrote (all complete
+// at the kernel boundary).
+__global__ void defer_snapshot_kernel(unsigned long long *counts) { counts[DEFER_SNAP] = counts[DEFER_COUNT]; }
 
 // Paired FP32 arithmetic of sm_100: one instruction computes both halves of a float2,
 // each half rounded as the scalar operation would be.  The CO2-Ar sample kernel is
@@ -286,7 +305,7 @@ __global__ void __launch_bounds__(DEFER_THREADS, 1) defer_eval_kernel(DeferArgs 
   DS ds;
   ds.init(df_smem, gtab, io);
   __syncthreads();
-  const unsigned long long count = defer_count(a);
+  const unsigned long long lo = defer_lo(a), count = defer_hi(a);
   const Ctx *ctx = static_cast<const Ctx *>(a.ctx);
   const PHYS *mu0s = static_cast<const PHYS *>(a.item_mu0);
   PHYS *first_v = static_cast<PHYS *>(a.first_v);
@@ -294,7 +313,7 @@ __global__ void __launch_bounds__(DEFER_THREADS, 1) defer_eval_kernel(DeferArgs 
   const int lane = threadIdx.x & 31;
   const unsigned long long gw = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const unsigned long long nw = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
-  for (unsigned long long base = gw * 32; base < count; base += nw * 32) {
+  for (unsigned long long base = lo + gw * 32; base < count; base += nw * 32) {
     const unsigned long long ci = base + lane;
     const int n = ci < count ? ctx[ci].n : 0;
     int off;
@@ -375,7 +394,7 @@ __global__ void __launch_bounds__(DEFER_THREADS, 2) defer_eval_co2ar_kernel(Defe
   DS ds;
   ds.init(df_smem, gtab, io);
   __syncthreads();
-  const unsigned long long count = defer_count(a);
+  const unsigned long long lo = defer_lo(a), count = defer_hi(a);
   const Ctx *ctx = static_cast<const Ctx *>(a.ctx);
   const float *mu0s = static_cast<const float *>(a.item_mu0);
   float *first_v = static_cast<float *>(a.first_v);
@@ -383,7 +402,7 @@ __global__ void __launch_bounds__(DEFER_THREADS, 2) defer_eval_co2ar_kernel(Defe
   const int lane = threadIdx.x & 31;
   const unsigned long long gw = ((unsigned long long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const unsigned long long nw = ((unsigned long long)gridDim.x * blockDim.x) >> 5;
-  for (unsigned long long base = gw * 32; base < count; base += nw * 32) {
+  for (unsigned long long base = lo + gw * 32; base < count; base += nw * 32) {
     const unsigned long long ci = base + lane;
     const int n = ci < count ? ctx[ci].n : 0;
     int off;

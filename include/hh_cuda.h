@@ -339,6 +339,13 @@ int hh_cuda_debug_set_ch4_dipole(int precision, int variant);
  * *previous (if not NULL) receives the mode before the call.  Both placements give the
  * same samples and C(t) up to the order of the FP64 sums. */
 int hh_cuda_debug_set_defer(int mode, int *previous);
+/* Tuning knob (no counterpart in the reference): with deferred samples, whether the
+ * contexts written by the bulk trajectory launch are evaluated while the solo launch
+ * (the last open trajectories) runs, on a second stream.  on 1 (the default, or the
+ * environment variable HH_DEFER_OVERLAP), 0 after the solo launch; -1 leaves it as it
+ * is.  *previous (if not NULL) receives the setting before the call.  Both give the
+ * same C(t) up to the order of the FP64 sums. */
+int hh_cuda_debug_set_defer_overlap(int on, int *previous);
 
 /* Diagnostic (no counterpart in the reference): device time per kernel class.
  * While switched on, every kernel of the classes below is bracketed by CUDA events

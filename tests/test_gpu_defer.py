@@ -6,8 +6,8 @@ statuses, C(t) equal up to the order of the FP64 sums (N2-Ar) or to FP32 roundin
 the sample kernel has its own FP32 interpolation and dipole-surface code, with the sample
 position in FP32, so a sample's dipole may differ by a few ulps), the same failure handling,
 and the same result when the iterations of a call are split over several launches or the
-context buffer overflows.  Also: the bulk kernel's per-round block barrier changes no
-result."""
+context buffer overflows.  Also: the bulk kernel's per-round block barrier and the sample
+launch beside the solo launch change no result."""
 import numpy as np
 import pytest
 
@@ -78,6 +78,35 @@ def test_deferred_failure_matches_in_kernel(lib, status):
         lib.hh_cuda_debug_inject(-1, 0, 0, 0)
     assert sa.n_failed == 1 and sb.n_failed == 1
     assert rel_to_c0(cb, ca) < PLACEMENT_TOL[name]
+
+
+@pytest.mark.parametrize("name", ["co2ar", "n2ar"])
+def test_sample_launch_beside_solo_launch_changes_nothing(lib, name):
+    """The contexts of the bulk trajectory launch evaluated while the solo launch runs (the
+    default) or after it: the same steps, samples and statuses, C(t) equal up to the
+    order of the FP64 sums, a trajectory failed by injection dropped in both."""
+    import hawaiihybrid_b200 as hh
+    from hawaiihybrid_b200 import _lib
+    ms = lib_system(name, 5)
+    N, dt = 4096, 100.0
+    qp, _ = O.sample(5, oracle_system(name), oracle_params(name, N, dt), 300.0, 2048)
+    p = lib_params(name, N, dt, mixed_tol=3e-8)
+    prev_d = _lib.defer_samples(2)
+    prev_o = _lib.defer_overlap(-1)
+    assert lib.hh_cuda_debug_inject(900, 0, 3, 5) == 0
+    try:
+        out = []
+        for on in (0, 1):
+            _lib.defer_overlap(on)
+            out.append(hh.correlation_from_initial_conditions(ms, p, qp, hh.PRECISION_MIXED))
+    finally:
+        lib.hh_cuda_debug_inject(-1, 0, 0, 0)
+        _lib.defer_overlap(prev_o)
+        _lib.defer_samples(prev_d)
+    (ca, sa), (cb, sb) = out
+    assert sa.n_failed == 1
+    assert rel_to_c0(cb, ca) < 1e-12
+    _same_stats(sa, sb)
     assert list(sa.status) == list(sb.status)
 
 
