@@ -664,8 +664,9 @@ int run_deferred_sys(const TrajParams &P, const TrajIO &io, long long traj_base)
   auto eval = SYS == SYS_CO2AR ? defer_eval_co2ar_kernel<float, float> : defer_eval_kernel<SYS_N2AR, float, float>;
   const size_t smem = DeferSys<SYS, float, float>::smem();
   if (smem > 48 * 1024) CK(cudaFuncSetAttribute(eval, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem));
+  constexpr int threads = defer_eval_threads<SYS>();
   int per_sm = 0;
-  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eval, DEFER_THREADS, smem));
+  CK(cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, eval, threads, smem));
   const int grid = std::max(1, per_sm) * g.num_sms;
   unsigned long long *cnt = io.ctx_count;
   kt_begin();
@@ -675,18 +676,18 @@ int run_deferred_sys(const TrajParams &P, const TrajIO &io, long long traj_base)
     DeferArgs a1 = a;
     a1.ctx_hi = cnt + DEFER_SNAP;
     CK(cudaStreamWaitEvent(g.st3, g.ev_bulk, 0));
-    eval<<<grid, DEFER_THREADS, smem, g.st3>>>(a1, P, io, g.d_tab);
+    eval<<<grid, threads, smem, g.st3>>>(a1, P, io, g.d_tab);
     CK(cudaGetLastError());
     CK(cudaEventRecord(g.ev_eval1, g.st3));
     DeferArgs a2 = a;
     a2.ctx_lo = cnt + DEFER_SNAP;
-    eval<<<grid, DEFER_THREADS, smem, g.st>>>(a2, P, io, g.d_tab);
+    eval<<<grid, threads, smem, g.st>>>(a2, P, io, g.d_tab);
     CK(cudaGetLastError());
     CK(cudaStreamWaitEvent(g.st, g.ev_eval1, 0));
     g.bulk_snap = false;
     g_launches += 1;
   } else {
-    eval<<<grid, DEFER_THREADS, smem, g.st>>>(a, P, io, g.d_tab);
+    eval<<<grid, threads, smem, g.st>>>(a, P, io, g.d_tab);
     CK(cudaGetLastError());
   }
   defer_jump_kernel<float, float, 6><<<8 * g.num_sms, DEFER_THREADS, 0, g.st>>>(a, P);

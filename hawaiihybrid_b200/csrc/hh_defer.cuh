@@ -37,6 +37,9 @@
 namespace hh {
 
 constexpr int DEFER_THREADS = 256;
+// block size of the sample kernels: CO2-Ar in blocks of two warps, which fit into the
+// registers that finished solo-kernel warps release while the solo kernel still runs
+template <int SYS> constexpr int defer_eval_threads() { return SYS == SYS_CO2AR ? 64 : DEFER_THREADS; }
 // words of the context counter block: the count the trajectory kernels advance, the
 // largest count of a call, and the snapshot of the count after the bulk kernel
 constexpr int DEFER_COUNT = 0, DEFER_PEAK = 1, DEFER_SNAP = 2, DEFER_WORDS = 3;
@@ -380,11 +383,11 @@ __global__ void __launch_bounds__(DEFER_THREADS, 1) defer_eval_kernel(DeferArgs 
 // (paired FP32, fma2).  The position is formed in FP32, y_old + F0 x + F1 x(1-x) +
 // F2 x^2(1-x) + ... + F6 x^4(1-x)^3 with the basis formed once and one FMA per term.
 // A context with an odd count ends in a single sample: the second half of its last
-// pair is computed but neither tested nor accumulated.  Two blocks per SM (128
-// registers a thread, no spills) ran faster than four (64 registers, with spills).
+// pair is computed but neither tested nor accumulated.  16 warps per SM (128
+// registers a thread, no spills) ran faster than 32 (64 registers, with spills).
 template <typename PHYS, typename STG>
-__global__ void __launch_bounds__(DEFER_THREADS, 2) defer_eval_co2ar_kernel(DeferArgs a, TrajParams P, TrajIO io,
-                                                                            const Co2arTablesGlobal *gtab) {
+__global__ void __launch_bounds__(defer_eval_threads<SYS_CO2AR>(), 16 * 32 / defer_eval_threads<SYS_CO2AR>())
+    defer_eval_co2ar_kernel(DeferArgs a, TrajParams P, TrajIO io, const Co2arTablesGlobal *gtab) {
   using DS = DeferSys<SYS_CO2AR, float, float>;
   constexpr int NQ = DS::NQ;
   using Ctx = SampleCtx<float, NQ>;
