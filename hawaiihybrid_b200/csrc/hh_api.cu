@@ -2077,8 +2077,7 @@ int hh_cuda_moment_sums(const hh_calc_params *p, const double *T, int nT, uint64
     a.Rmin = p->sampler_Rmin;
     a.Rmax = p->sampler_Rmax;
     a.pair_state = p->pair_state;
-    a.nT = std::min(M0_MAXT, nT - t0);
-    for (int t = 0; t < a.nT; ++t) a.invkT[t] = HH_HKT / T[t0 + t];
+    m0_set_temperatures(a, T + t0, std::min(M0_MAXT, nT - t0));
     a.n_samples = n_samples;
     a.offset = sample_offset;
     a.seed = seed;
@@ -2490,8 +2489,7 @@ int hh_cuda_m0_noalloc(const hh_calc_params *p, const double *T, int nT, uint64_
     a.Rmin = p->sampler_Rmin;
     a.Rmax = p->sampler_Rmax;
     a.pair_state = p->pair_state;
-    a.nT = std::min(M0_MAXT, nT - t0);
-    for (int t = 0; t < a.nT; ++t) a.invkT[t] = HH_HKT / T[t0 + t];
+    m0_set_temperatures(a, T + t0, std::min(M0_MAXT, nT - t0));
     a.n_samples = n_samples;
     a.offset = 0;
     a.seed = seed;

@@ -12,6 +12,7 @@
 #define HH_EPSILON0 8.8541878128e-12
 #define HH_HKT (HH_HARTREE / HH_BOLTZMANN)
 #define HH_PI 3.14159265358979323846
+#define HH_LOG2E 1.44269504088896340736  /* log2(e) */
 #define HH_ZEROCOEFF (0.00361479637 / (4.0 * HH_PI))
 #define HH_SECONDCOEFF 13856114.29344114  // src/constants.h:30
 

@@ -84,14 +84,6 @@ __device__ __forceinline__ unsigned long long defer_lo(const DeferArgs &a) {
 // at the kernel boundary).
 __global__ void defer_snapshot_kernel(unsigned long long *counts) { counts[DEFER_SNAP] = counts[DEFER_COUNT]; }
 
-// Paired FP32 arithmetic of sm_100: one instruction computes both halves of a float2,
-// each half rounded as the scalar operation would be.  The CO2-Ar sample kernel is
-// bound by instruction issue, so pairs of independent operations go through as one.
-__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
-__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
-__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
-__device__ __forceinline__ float2 splat2(float v) { return make_float2(v, v); }
-
 // the dipole of the bound system with its surfaces staged in shared memory
 template <int SYS, typename PHYS, typename STG> struct DeferSys;
 

@@ -43,7 +43,15 @@
 
 namespace hh {
 
-constexpr int M0_MAXT = 16;  // temperatures per launch chunk
+constexpr int M0_MAXT = 16;  // temperatures per launch chunk (even: the mixed path pairs them)
+static_assert(M0_MAXT % 2 == 0, "temperature pairs");
+
+// 2^x by the ex2.approx instruction (PTX ISA: maximum relative error about 2^-22)
+__device__ __forceinline__ float ex2_approx(float x) {
+  float y;
+  asm("ex2.approx.ftz.f32 %0, %1;" : "=f"(y) : "f"(x));
+  return y;
+}
 
 struct M0Args {
   int sys;
@@ -53,6 +61,8 @@ struct M0Args {
   int pair_state;
   int nT;
   double invkT[M0_MAXT];   // Hartree^-1
+  float kT[M0_MAXT];       // mixed path: kT (Hartree) and log2(e) / kT, FP32
+  float l2e_kT[M0_MAXT];
   uint64_t n_samples, offset, seed;
 };
 
@@ -122,6 +132,17 @@ __device__ double m2_geometry(const Sys &sys, double R, double x, double inv_mu,
   return (gt * inv_mu + gr * inv_II) / (4.0 * h * h);
 }
 
+// the launch's temperatures T[0 .. nT-1] (K) into a
+inline void m0_set_temperatures(M0Args &a, const double *T, int nT) {
+  a.nT = nT;
+  for (int t = 0; t < M0_MAXT; ++t) {
+    const double ikT = t < nT ? HH_HKT / T[t] : 0.0;
+    a.invkT[t] = ikT;
+    a.kT[t] = t < nT ? float(T[t] / HH_HKT) : 0.f;
+    a.l2e_kT[t] = float(ikT * HH_LOG2E);
+  }
+}
+
 template <int SYS, typename PHYS, bool COMP, int MOMENT = 0>
 __global__ void __launch_bounds__(256) m0_kernel(M0Args a, const Co2arTablesGlobal *gtab,
                                                  const void *dipnet, double *partials) {
@@ -142,6 +163,14 @@ __global__ void __launch_bounds__(256) m0_kernel(M0Args a, const Co2arTablesGlob
   for (int t = 0; t < M0_MAXT; ++t) {
     s[t] = c[t] = q[t] = AT(0);
     ikT[t] = PHYS(a.invkT[t]);
+  }
+  // mixed path: the temperatures in pairs (paired FP32, fma2): the sums, kT and
+  // log2(e) / kT of temperatures (2j, 2j + 1)
+  constexpr bool PAIRED = sizeof(PHYS) == 4 && MOMENT == 0;
+  float2 s2[M0_MAXT / 2], c2[M0_MAXT / 2], q2[M0_MAXT / 2];
+  if constexpr (PAIRED) {
+#pragma unroll
+    for (int j = 0; j < M0_MAXT / 2; ++j) s2[j] = c2[j] = q2[j] = make_float2(0.f, 0.f);
   }
   const PHYS Rmin = PHYS(a.Rmin), dR = PHYS(a.Rmax - a.Rmin);
   const PHYS twopi = PHYS(2.0 * HH_PI);
@@ -210,9 +239,37 @@ __global__ void __launch_bounds__(256) m0_kernel(M0Args a, const Co2arTablesGlob
       kappa = -log(u24<PHYS>(w[5])) - log(u24<PHYS>(w[6])) - log(u24<PHYS>(w[7])) * zc * zc;
     }
     PHYS base = R * R * mu2;
+    if constexpr (PAIRED) {
+      // w = R^2 |mu|^2 2^(-V log2(e) / kT) behind the filter on H = kappa kT + V; the
+      // exponential by ex2.approx (relative error about 2^-22 plus the rounding of the
+      // FP32 argument), the sums compensated as below
+      const float2 kap = splat2(float(kappa)), Vv = splat2(float(V)), nV = splat2(-float(V)), bb = splat2(float(base));
+      const float2 m1 = splat2(-1.f);
+#pragma unroll
+      for (int j = 0; j < M0_MAXT / 2; ++j) {
+        if (2 * j < a.nT) {
+          const float2 H = fma2(kap, make_float2(a.kT[2 * j], a.kT[2 * j + 1]), Vv);
+          const float2 arg = mul2(nV, make_float2(a.l2e_kT[2 * j], a.l2e_kT[2 * j + 1]));
+          float2 e = make_float2(ex2_approx(arg.x), ex2_approx(arg.y));
+          if (a.pair_state == 1) {
+            e.x = H.x >= 0.f ? e.x : 0.f;
+            e.y = H.y >= 0.f ? e.y : 0.f;
+          } else if (a.pair_state == 2) {
+            e.x = H.x <= 0.f ? e.x : 0.f;
+            e.y = H.y <= 0.f ? e.y : 0.f;
+          }
+          const float2 wv = mul2(bb, e);
+          const float2 y = fma2(c2[j], m1, wv);         // wv - c
+          const float2 tt = add2(s2[j], y);
+          c2[j] = fma2(y, m1, fma2(s2[j], m1, tt));    // (tt - s) - y
+          s2[j] = tt;
+          q2[j] = fma2(wv, wv, q2[j]);
+        }
+      }
+    }
 #pragma unroll
     for (int t = 0; t < M0_MAXT; ++t) {
-      if (t < a.nT) {
+      if (!PAIRED && t < a.nT) {
         PHYS H = kappa / ikT[t] + V;
         bool keep = true;
         if (a.pair_state == 1) keep = (H >= PHYS(0));
@@ -226,6 +283,17 @@ __global__ void __launch_bounds__(256) m0_kernel(M0Args a, const Co2arTablesGlob
         s[t] = tt;
         q[t] += wv * wv;
       }
+    }
+  }
+  if constexpr (PAIRED) {
+#pragma unroll
+    for (int j = 0; j < M0_MAXT / 2; ++j) {
+      s[2 * j] = s2[j].x;
+      s[2 * j + 1] = s2[j].y;
+      c[2 * j] = c2[j].x;
+      c[2 * j + 1] = c2[j].y;
+      q[2 * j] = q2[j].x;
+      q[2 * j + 1] = q2[j].y;
     }
   }
   // block reduction in a fixed order

@@ -23,6 +23,14 @@
 
 namespace hh {
 
+// Paired FP32 arithmetic of sm_100: one instruction computes both halves of a float2,
+// each half rounded as the scalar operation would be.  Kernels bound by instruction
+// issue (the sample and M0 kernels) put pairs of independent operations through as one.
+__device__ __forceinline__ float2 fma2(float2 a, float2 b, float2 c) { return __ffma2_rn(a, b, c); }
+__device__ __forceinline__ float2 mul2(float2 a, float2 b) { return __fmul2_rn(a, b); }
+__device__ __forceinline__ float2 add2(float2 a, float2 b) { return __fadd2_rn(a, b); }
+__device__ __forceinline__ float2 splat2(float v) { return make_float2(v, v); }
+
 // ----------------------------------------------------------------------------
 // He-Ar (PES-IDS/HeAr.h:33-107): exponential repulsion + damped dispersion
 // V = A exp(-g1 R - g2 R^2) - sum_{n=3..8} C_2n f_2n(bR) / R^2n,
