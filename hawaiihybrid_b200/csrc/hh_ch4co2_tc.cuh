@@ -16,23 +16,23 @@
 // harmonics' recurrences take their integer-only square roots from constant tables,
 // so neither the split nor the recurrences use the transcendental pipe.
 //
-// Mapping (one CTA of 256 threads per SM, persistent over the 128-record tasks; two
-// warps per TMEM lane quadrant):
-//   - threads t and t + 128 own record t of the task: geometry, x powers, Y2 generated
-//     chunk by chunk from its recurrence (in registers), and its row of A (half the K
-//     columns each) written into shared memory in the canonical no-swizzle K-major
-//     layout (8-row x 16-byte core matrices; K-adjacent cores 128 B apart, 8-row
-//     groups 512 B apart);
+// Mapping (one CTA of 17 warps per SM, persistent over the 128-record tasks):
+//   - 16 producer warps, four per TMEM lane quadrant: the four threads of record t
+//     (one per quarter) compute its geometry and x powers, walk its Y2 with a
+//     generator (in registers) and write their column groups of each A chunk into
+//     shared memory in the canonical no-swizzle K-major layout (8-row x 16-byte core
+//     matrices; K-adjacent cores 128 B apart, 8-row groups 512 B apart);
 //   - K is walked in chunks of 16 (23 chunks for K = 368, the last 4 columns zero);
 //     the chunk's B_hi | B_lo image (built on the host in the same layout) arrives by
 //     one bulk copy (cp.async.bulk, this GPU's memory only, no multicast) into a ring
-//     of three stages tracked by mbarriers: the copy of chunk g + 1 is issued once
-//     chunk g - 2's MMAs are done, so two chunks of MMAs stay queued behind it;
-//   - thread 0 issues the tcgen05.mma instructions of a chunk (M = 128, N = 208, K = 8
-//     each) and commits them to the stage's mbarrier, which frees the stage;
+//     of three stages;
+//   - one issuing warp (one lane) issues the copies two chunks ahead and the
+//     tcgen05.mma instructions of each chunk (M = 128, N = 208, K = 8 each) and
+//     commits them to the stage's mbarrier, which frees the stage; producers and
+//     issuer meet only at mbarriers, so A production, copies and MMAs overlap;
 //   - TMEM holds two 208-column accumulators: pass 0 computes components 0 and 1,
 //     pass 1 component 2 (the three would need 624 of the 512 columns);
-//   - after a pass thread t reads its TMEM lane (tcgen05.ld 32x32b) and forms
+//   - after a pass the producers read their TMEM lanes (tcgen05.ld 32x32b) and form
 //     sum_n Y1_n T[t, n] with Y1 generated by its recurrence in column order (pass 0:
 //     the two halves take one component each).
 // Every mbarrier wait is bounded: on a timeout the CTA records the error in *err,
@@ -49,11 +49,9 @@ namespace hh {
 
 constexpr int CH4TC_A_BYTES = CH4TC_M * CH4TC_KC * 4;    // one A image (hi or lo): 8 KB
 constexpr int CH4TC_STAGE_B = 2 * CH4TC_IMG0;            // B_hi | B_lo of the widest pass
-constexpr int CH4TC_STAGES = 2;
-// dynamic shared memory: 2 stages x (A_hi, A_lo, B_hi | B_lo) = 136 KB, Y2 of the task
-// (46.6 KB), 1 KB alignment
-constexpr size_t CH4TC_SMEM =
-    CH4TC_STAGES * (2 * CH4TC_A_BYTES + CH4TC_STAGE_B) + (size_t)CH4_NY2 * CH4TC_M * 4 + 1024;
+constexpr int CH4TC_STAGES = 3;
+// dynamic shared memory: 3 stages x (A_hi, A_lo, B_hi | B_lo) = 204 KB, 1 KB alignment
+constexpr size_t CH4TC_SMEM = CH4TC_STAGES * (2 * CH4TC_A_BYTES + CH4TC_STAGE_B) + 1024;
 constexpr unsigned CH4TC_TMEM_COLS = 512;
 constexpr unsigned CH4TC_COL1 = 256;            // TMEM column of the second accumulator
 constexpr long long CH4TC_WAIT_LIMIT = 1LL << 24;  // polls of an mbarrier before giving up
@@ -180,36 +178,6 @@ __device__ __forceinline__ void ch4tc_cs_m(float x, float y, int m, float &C, fl
   }
 }
 
-// Y2 of the CO2 axis (x, y, z) in the CH4 frame for m in [m0, m1), into
-// Y[idx * 128 + t] at their indices of ch4_y2
-__device__ __forceinline__ void ch4tc_y2_range(float x, float y, float z, float *Y, int t, int m0, int m1) {
-  float C, Sn;
-  ch4tc_cs_m(x, y, m0, C, Sn);
-  int idx = ch4tc_y2_off(m0);
-#pragma unroll 1
-  for (int m = m0; m < m1; ++m) {
-    if (m > m0) {
-      const float c = C * x - Sn * y;
-      Sn = C * y + Sn * x;
-      C = c;
-    }
-    const float pm = c_ch4tc_pm[m];
-    float qa = 1.f, qb = 0.f;
-#pragma unroll 1
-    for (int l = m; l <= CH4_L2; ++l) {
-      if (l > m) {
-        const float q = c_ch4tc_alpha[m][l] * z * qa - c_ch4tc_beta[m][l] * qb;
-        qb = qa;
-        qa = q;
-      }
-      if ((l & 1) == 0) {
-        Y[(idx++) * CH4TC_M + t] = pm * C * qa;
-        if (m > 0) Y[(idx++) * CH4TC_M + t] = pm * Sn * qa;
-      }
-    }
-  }
-}
-
 // sum over the Y1 columns of m in [m0, m1) (m-major, l = m..13, cos then sin) of
 // Y1_n(n1) T[n] at TMEM address `taddr` (this thread's lane); m0 and m1 are uniform
 // across the warp (tcgen05.ld is a warp-wide load)
@@ -265,41 +233,127 @@ __device__ __forceinline__ float ch4tc_y1_dot_m(uint32_t taddr, const float n1[3
   return acc;
 }
 
-// 512 threads: four warps per TMEM lane quadrant.  Thread t works on record row =
-// t % 128; its quarter qt = t / 128 takes
-//   - the Y2 of m in CH4TC_Y2_M[qt] .. CH4TC_Y2_M[qt + 1] (about a quarter of the
-//     recurrence work each) into shared memory,
-//   - column group k = 4 c + qt of every A chunk (its 4 powers of x, hi and lo),
+// The Y2 of one record in the order of ch4_y2 (m = 0..12, even l = m..12, cos then
+// sin for m > 0), one value per next(): (cos, sin)(m phi) as (x + i y)^m times pm_m,
+// and the normalised three-term recurrence in l, run as a generator so that a thread
+// walks the A columns chunk by chunk without a table.
+struct Ch4TcY2Gen {
+  float x, y, z, C, Sn, pm, qa, qb, pend;
+  int m, l;
+  bool sin_next;
+  __device__ __forceinline__ void reset(float x_, float y_, float z_) {
+    x = x_;
+    y = y_;
+    z = z_;
+    C = 1.f;
+    Sn = 0.f;
+    pm = c_ch4tc_pm[0];
+    qa = 1.f;
+    qb = 0.f;
+    pend = 0.f;
+    m = 0;
+    l = 0;
+    sin_next = false;
+  }
+  // to the next (m, l): l + 1 by the recurrence, or m + 1 with l = m
+  __device__ __forceinline__ void advance() {
+    if (l == CH4_L2) {
+      ++m;
+      l = m;
+      const float c = C * x - Sn * y;
+      Sn = C * y + Sn * x;
+      C = c;
+      pm = c_ch4tc_pm[m];
+      qa = 1.f;
+      qb = 0.f;
+    } else {
+      ++l;
+      const float q = c_ch4tc_alpha[m][l] * z * qa - c_ch4tc_beta[m][l] * qb;
+      qb = qa;
+      qa = q;
+    }
+  }
+  // the next of the 91 values (not called past the last)
+  __device__ __forceinline__ float next() {
+    if (sin_next) {
+      sin_next = false;
+      return pend;
+    }
+    if (l & 1) advance();  // odd l: no value, on to the even l after it
+    const float v = pm * C * qa;
+    if (m > 0) {
+      pend = pm * Sn * qa;
+      sin_next = true;
+    }
+    advance();
+    return v;
+  }
+};
+
+// Warp roles (17 warps): warps 0..15 produce the A chunks and run the epilogue, four
+// per TMEM lane quadrant; thread t < 512 works on record row = t % 128 and its quarter
+// qt = t / 128 takes
+//   - column group k = 4 c + qt of every A chunk (its 4 powers of x, hi and lo), with
+//     the record's Y2 from a generator stepped through every index;
 //   - in pass 0 half of the columns of component qt / 2 (m in [0, 5) or [5, 14)), in
 //     pass 1 a quarter of the columns of component 2 (CH4TC_Y1_M);
-// the partial sums meet in shared memory and quarter 0 finishes the record.
-constexpr int CH4TC_THREADS = 4 * CH4TC_M;
-__constant__ int CH4TC_Y2_M[5] = {0, 2, 4, 7, CH4_L2 + 1};
+// the partial sums meet in shared memory and quarter 0 finishes the record.  Warp 16
+// (one lane) issues the B copies and the MMAs.  The two sides meet only at mbarriers:
+//   full_a[s]  the 16 producer warps wrote stage s's A (after fence.proxy.async);
+//   full_b[s]  stage s's B copy landed (complete_tx);
+//   empty[s]   the MMAs that read stage s are done (tcgen05.commit): A and B of the
+//              chunk three later may be written;
+//   tfree      the producers read the accumulators of a pass: the next pass's MMAs
+//              may overwrite them.
+// Chunk g uses stage g % 3, and the n-th completion of a stage's barriers belongs to
+// its chunk 3 n + stage.  Every wait is bounded; a thread whose wait gives up sets
+// bad_s and skips its work up to the next agreement point (the producers' pass-end
+// barrier, a reduction over bad_s), where all producers leave together.
+constexpr int CH4TC_PRODUCERS = 4 * CH4TC_M;
+constexpr int CH4TC_THREADS = CH4TC_PRODUCERS + 32;
 __constant__ int CH4TC_Y1_M[5] = {0, 2, 4, 7, CH4_L1 + 1};
 constexpr int CH4TC_Y1_SPLIT = 5;  // pass 0: m < 5 and m >= 5
+
+__device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
+  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
+}
+
+// barrier 1 over the 512 producer threads; true if any of them passed `bad`
+__device__ __forceinline__ bool ch4tc_producers_sync_or(bool bad) {
+  uint32_t r;
+  asm volatile(
+      "{\n\t.reg .pred p, q;\n\t"
+      "setp.ne.b32 p, %1, 0;\n\t"
+      "bar.red.or.pred q, 1, %2, p;\n\t"
+      "selp.u32 %0, 1, 0, q;\n\t}"
+      : "=r"(r)
+      : "r"((uint32_t)bad), "n"(CH4TC_PRODUCERS)
+      : "memory");
+  return r != 0;
+}
 
 __global__ void __launch_bounds__(CH4TC_THREADS, 1) ch4_dipole_tc_kernel(Ch4TcArgs a) {
   extern __shared__ __align__(1024) unsigned char tc_smem_raw[];
   unsigned char *smem = reinterpret_cast<unsigned char *>(
       (reinterpret_cast<uintptr_t>(tc_smem_raw) + 1023) & ~uintptr_t(1023));
-  // stage s: A_hi, A_lo, B (hi | lo); then Y2 of the task
+  // stage s: A_hi, A_lo, B (hi | lo)
   constexpr size_t STAGE_BYTES = 2 * CH4TC_A_BYTES + CH4TC_STAGE_B;
   auto stA = [&](int s, int lo) { return smem + (size_t)s * STAGE_BYTES + (size_t)lo * CH4TC_A_BYTES; };
   auto stB = [&](int s) { return smem + (size_t)s * STAGE_BYTES + 2 * CH4TC_A_BYTES; };
-  float *Y2s = reinterpret_cast<float *>(smem + CH4TC_STAGES * STAGE_BYTES);
-  __shared__ __align__(8) uint64_t bar_load[CH4TC_STAGES], bar_mma[CH4TC_STAGES];
+  __shared__ __align__(8) uint64_t bar_fa[CH4TC_STAGES], bar_fb[CH4TC_STAGES], bar_empty[CH4TC_STAGES], bar_tfree;
   __shared__ uint32_t tmem_base_s;
-  __shared__ int bad_s;
+  __shared__ volatile int bad_s;
   __shared__ long long w0[CH4_NSEG + 1];
-  __shared__ float part_s[4][CH4TC_M];  // the quarters' partial sums of a pass
-  const int t = threadIdx.x, warp = t >> 5;
-  const int row = t & (CH4TC_M - 1), qt = t / CH4TC_M;
+  __shared__ float part_s[2][4][CH4TC_M];  // the quarters' partial sums, per pass
+  const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   for (int i = t; i <= CH4_NSEG; i += blockDim.x) w0[i] = a.warp0[i];
   if (t == 0) {
     for (int s = 0; s < CH4TC_STAGES; ++s) {
-      mbar_init(&bar_load[s], 1);
-      mbar_init(&bar_mma[s], 1);
+      mbar_init(&bar_fa[s], CH4TC_PRODUCERS / 32);
+      mbar_init(&bar_fb[s], 1);
+      mbar_init(&bar_empty[s], 1);
     }
+    mbar_init(&bar_tfree, CH4TC_PRODUCERS / 32);
     asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
     bad_s = 0;
   }
@@ -319,103 +373,66 @@ __global__ void __launch_bounds__(CH4TC_THREADS, 1) ch4_dipole_tc_kernel(Ch4TcAr
     while (s < CH4_NSEG - 1 && w0[s + 1] <= task) ++s;
     return s;
   };
-  // chunk sequence: g counts the chunks this CTA has walked; chunk g uses stage
-  // g % STAGES, and the n-th completion of a stage's barriers belongs to its chunk
-  // STAGES n + stage.  Thread 0 keeps gl (loads issued), gw (loads seen complete) and
-  // gm (chunks whose MMAs were committed) for the bounded drain after a timeout.
-  unsigned g = 0, gl = 0, gw = 0, gm = 0;
-  // the chunk after (task, q, c) in this CTA's walk, for the B prefetch
-  auto next_chunk = [&](long long task, int q, int c, long long &nt, int &nq, int &nc) -> bool {
-    nt = task;
-    nq = q;
-    nc = c + 1;
-    if (nc == CH4TC_NCHUNK) {
-      nc = 0;
-      nq = q + 1;
-      if (nq == 2) {
-        nq = 0;
-        nt = task + gridDim.x;
-        if (nt >= total) return false;
-      }
+  auto fail = [&]() {
+    if (!bad_s) {
+      bad_s = 1;
+      atomicExch(a.err, 1);
     }
-    return true;
   };
-  // thread 0's piece of the task whose B it loads: found once per task (seg_of walks
-  // the piece table), not once per chunk
-  long long seg_task = -1;
-  int seg_cached = 0;
-  auto issue_load = [&](long long task, int q, int c, int s) {
-    if (task != seg_task) {
-      seg_task = task;
-      seg_cached = seg_of(task * a.task_step);
-    }
-    const unsigned bytes = q == 0 ? 2 * CH4TC_IMG0 : 2 * CH4TC_IMG1;
-    ch4tc_load(stB(s), a.blob + ch4tc_blob_off(seg_cached, q, c), bytes, &bar_load[s]);
-  };
-  long long task0 = blockIdx.x;
-  if (t == 0 && task0 < total) {
-    issue_load(task0, 0, 0, 0);
-    gl = 1;
-  }
-  const uint32_t lane_addr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
-  for (long long task = task0; task < total; task += gridDim.x) {
-    const long long w = task * a.task_step;
-    const int seg = seg_of(w);
-    // ---- this thread's record: geometry, powers of x ----
-    const int first = a.sorted[w * CH4TC_M];
-    const int mine = a.sorted[w * CH4TC_M + row];
-    const int src = mine >= 0 ? mine : first;
-    const float *rec = a.records + (size_t)src * HH_REC_WORDS;
-    float M[3][3], n1[3], n2[3];
-    {
-      const float r[3] = {rec[0], rec[1], rec[2]};
-      const float qt4[4] = {rec[3], rec[4], rec[5], rec[6]};
-      const float u[3] = {rec[7], rec[8], rec[9]};
-      quat_matrix<float>(qt4, M);
-      const float R = sqrtf(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
-      const float iR = 1.f / R;
-      const float iu = 1.f / sqrtf(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
-#pragma unroll
-      for (int k = 0; k < 3; ++k) {
-        n1[k] = (M[0][k] * r[0] + M[1][k] * r[1] + M[2][k] * r[2]) * iR;
-        n2[k] = (M[0][k] * u[0] + M[1][k] * u[1] + M[2][k] * u[2]) * iu;
-      }
-    }
-    const float R = sqrtf(rec[0] * rec[0] + rec[1] * rec[1] + rec[2] * rec[2]);
-    const float x = R - float(a.centre[seg]);
-    const float xp[4] = {1.f, x, x * x, x * x * x};
-    __syncthreads();  // the previous task's last chunk no longer reads Y2s
-    ch4tc_y2_range(n2[0], n2[1], n2[2], Y2s, row, CH4TC_Y2_M[qt], CH4TC_Y2_M[qt + 1]);
-    __syncthreads();
-    float acc[3] = {0.f, 0.f, 0.f};
-    for (int q = 0; q < 2; ++q) {
-      const int ntile = q == 0 ? 2 : 1;
-      for (int c = 0; c < CH4TC_NCHUNK; ++c, ++g) {
-        const int s = g % CH4TC_STAGES;
-        // ---- A chunk: row t, columns 4 kq .. 4 kq + 3 (k = 4 c + kq, j = 0..3), kq = qt ----
-        {
-          const int k = 4 * c + qt;
-          const float y2 = (k < CH4_NY2) ? Y2s[k * CH4TC_M + row] : 0.f;
-          float4 hi, lo;
-          float *ph = &hi.x, *pl = &lo.x;
-#pragma unroll
-          for (int j = 0; j < 4; ++j) {
-            const float v = y2 * xp[j];
-            const float h = tf32_hi(v);
-            ph[j] = h;
-            pl[j] = v - h;
+
+  if (warp == CH4TC_PRODUCERS / 32) {
+    // ---------------- issuer: B copies and MMAs (one lane) ----------------
+    if (lane == 0) {
+      // the chunk walk (task, pass q, chunk c) of this CTA, for the copies two ahead
+      struct Walk {
+        long long task;
+        int q, c;
+      };
+      auto step = [&](Walk &w) -> bool {
+        if (++w.c == CH4TC_NCHUNK) {
+          w.c = 0;
+          if (++w.q == 2) {
+            w.q = 0;
+            w.task += gridDim.x;
           }
-          *reinterpret_cast<float4 *>(reinterpret_cast<float *>(stA(s, 0)) + ch4tc_img_off(row, 4 * qt)) = hi;
-          *reinterpret_cast<float4 *>(reinterpret_cast<float *>(stA(s, 1)) + ch4tc_img_off(row, 4 * qt)) = lo;
         }
-        asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
-        __syncthreads();
-        if (t == 0 && !bad_s) {
-          if (!mbar_wait(&bar_load[s], (g / CH4TC_STAGES) & 1)) {
-            bad_s = 1;
-            atomicExch(a.err, 1);
-          } else {
-            gw = g + 1;
+        return w.task < total;
+      };
+      long long seg_task = -1;
+      int seg_cached = 0;
+      auto issue_load = [&](const Walk &w, int s) {
+        if (w.task != seg_task) {
+          seg_task = w.task;
+          seg_cached = seg_of(w.task * a.task_step);
+        }
+        const unsigned bytes = w.q == 0 ? 2 * CH4TC_IMG0 : 2 * CH4TC_IMG1;
+        ch4tc_load(stB(s), a.blob + ch4tc_blob_off(seg_cached, w.q, w.c), bytes, &bar_fb[s]);
+      };
+      unsigned gl = 0, gm = 0;  // copies issued, chunks whose MMAs were committed
+      Walk ld{(long long)blockIdx.x, 0, 0};
+      bool more = ld.task < total;
+      for (int i = 0; i < 2 && more; ++i) {
+        issue_load(ld, (int)(gl % CH4TC_STAGES));
+        ++gl;
+        more = step(ld);
+      }
+      unsigned g = 0, np = 0;
+      for (long long task = blockIdx.x; task < total && !bad_s; task += gridDim.x) {
+        for (int q = 0; q < 2 && !bad_s; ++q, ++np) {
+          const int ntile = q == 0 ? 2 : 1;
+          // the previous pass's accumulators have been read
+          if (np > 0 && !mbar_wait(&bar_tfree, (np - 1) & 1)) {
+            fail();
+            break;
+          }
+          tc_fence_after();
+          for (int c = 0; c < CH4TC_NCHUNK; ++c, ++g) {
+            const int s = g % CH4TC_STAGES;
+            const unsigned par = (g / CH4TC_STAGES) & 1;
+            if (!mbar_wait(&bar_fa[s], par) || !mbar_wait(&bar_fb[s], par)) {
+              fail();
+              break;
+            }
             tc_fence_after();
             const uint32_t a_hi = smem_u32(stA(s, 0)), a_lo = smem_u32(stA(s, 1));
             const uint32_t b_hi = smem_u32(stB(s));
@@ -433,79 +450,148 @@ __global__ void __launch_bounds__(CH4TC_THREADS, 1) ch4_dipole_tc_kernel(Ch4TcAr
                 ch4tc_mma(d, ch4tc_desc(a_lo + ko), ch4tc_desc(b_hi + boff + ko), 1u);
               }
             }
-            ch4tc_commit(&bar_mma[s]);
+            ch4tc_commit(&bar_empty[s]);
             gm = g + 1;
-            // prefetch the next chunk's B into stage (g + 1) % STAGES once that stage's
-            // last MMAs (chunk g + 1 - STAGES) are done
-            long long nt_;
-            int nq, nc;
-            if (next_chunk(task, q, c, nt_, nq, nc)) {
-              const int s1 = (g + 1) % CH4TC_STAGES;
-              if (g + 1 >= (unsigned)CH4TC_STAGES &&
-                  !mbar_wait(&bar_mma[s1], ((g + 1 - CH4TC_STAGES) / CH4TC_STAGES) & 1)) {
-                bad_s = 1;
-                atomicExch(a.err, 1);
-              } else {
-                issue_load(nt_, nq, nc, s1);
-                gl = g + 2;
+            // the copy two chunks ahead, into the stage whose MMAs (chunk g - 1) are
+            // queued ahead of this chunk's
+            if (more) {
+              const unsigned h = gl;  // == g + 2
+              const int s2 = h % CH4TC_STAGES;
+              if (h >= (unsigned)CH4TC_STAGES && !mbar_wait(&bar_empty[s2], ((h - CH4TC_STAGES) / CH4TC_STAGES) & 1)) {
+                fail();
+                break;
               }
+              issue_load(ld, s2);
+              ++gl;
+              more = step(ld);
             }
           }
         }
-        // stage (g + 1) % STAGES is free for the next chunk's A once thread 0 has seen its
-        // last MMAs complete (above)
-        __syncthreads();
       }
-      // ---- all MMAs of this pass done: the quarters' partial sums from TMEM ----
-      if (t == 0 && !bad_s) {
-        if (!mbar_wait(&bar_mma[(g - 1) % CH4TC_STAGES], ((g - 1) / CH4TC_STAGES) & 1)) {
-          bad_s = 1;
-          atomicExch(a.err, 1);
-        }
-      }
-      __syncthreads();
-      tc_fence_after();
-      if (!bad_s) {
-        float v;
-        if (q == 0) {
-          const int comp = qt >> 1;
-          v = (qt & 1) ? ch4tc_y1_dot_m(lane_addr + (comp ? CH4TC_COL1 : 0u), n1, CH4TC_Y1_SPLIT, CH4_L1 + 1)
-                       : ch4tc_y1_dot_m(lane_addr + (comp ? CH4TC_COL1 : 0u), n1, 0, CH4TC_Y1_SPLIT);
-        } else {
-          v = ch4tc_y1_dot_m(lane_addr, n1, CH4TC_Y1_M[qt], CH4TC_Y1_M[qt + 1]);
-        }
-        part_s[qt][row] = v;
-      }
-      // the accumulators are rewritten by the next pass's first MMAs
-      tc_fence_before();
-      __syncthreads();
-      tc_fence_after();
-      if (qt == 0) {
-        if (q == 0) {
-          acc[0] = part_s[0][row] + part_s[1][row];
-          acc[1] = part_s[2][row] + part_s[3][row];
-        } else {
-          acc[2] = (part_s[0][row] + part_s[1][row]) + (part_s[2][row] + part_s[3][row]);
-        }
-      }
+      // drain (bounded): the committed MMAs and the copies issued
+      if (gm > 0) mbar_wait(&bar_empty[(gm - 1) % CH4TC_STAGES], ((gm - 1) / CH4TC_STAGES) & 1);
+      for (unsigned h = gm; h < gl; ++h) mbar_wait(&bar_fb[h % CH4TC_STAGES], (h / CH4TC_STAGES) & 1);
     }
-    if (bad_s) break;
-    if (seg == CH4_NSEG - 1) {
-      const float i2 = 1.f / (R * R);
-      const float i6 = i2 * i2 * i2;
+    __syncwarp();
+  } else {
+    // ---------------- producers: A chunks, epilogue ----------------
+    const int row = t & (CH4TC_M - 1), qt = t / CH4TC_M;
+    const uint32_t lane_addr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+    unsigned g = 0;
+    bool stop = false;
+    for (long long task = blockIdx.x; task < total && !stop; task += gridDim.x) {
+      const long long w = task * a.task_step;
+      const int seg = seg_of(w);
+      // ---- this thread's record: geometry, powers of x ----
+      const int first = a.sorted[w * CH4TC_M];
+      const int mine = a.sorted[w * CH4TC_M + row];
+      const int src = mine >= 0 ? mine : first;
+      const float *rec = a.records + (size_t)src * HH_REC_WORDS;
+      float M[3][3], n1[3], n2[3];
+      {
+        const float r[3] = {rec[0], rec[1], rec[2]};
+        const float qt4[4] = {rec[3], rec[4], rec[5], rec[6]};
+        const float u[3] = {rec[7], rec[8], rec[9]};
+        quat_matrix<float>(qt4, M);
+        const float R = sqrtf(r[0] * r[0] + r[1] * r[1] + r[2] * r[2]);
+        const float iR = 1.f / R;
+        const float iu = 1.f / sqrtf(u[0] * u[0] + u[1] * u[1] + u[2] * u[2]);
 #pragma unroll
-      for (int cc = 0; cc < 3; ++cc) acc[cc] *= i6;
-    }
-    if (qt == 0 && mine >= 0) {
-      float *o = a.mu + (size_t)mine * 4;
+        for (int k = 0; k < 3; ++k) {
+          n1[k] = (M[0][k] * r[0] + M[1][k] * r[1] + M[2][k] * r[2]) * iR;
+          n2[k] = (M[0][k] * u[0] + M[1][k] * u[1] + M[2][k] * u[2]) * iu;
+        }
+      }
+      const float R = sqrtf(rec[0] * rec[0] + rec[1] * rec[1] + rec[2] * rec[2]);
+      const float x = R - float(a.centre[seg]);
+      const float xp[4] = {1.f, x, x * x, x * x * x};
+      float acc[3] = {0.f, 0.f, 0.f};
+      for (int q = 0; q < 2; ++q) {
+        Ch4TcY2Gen y2g;
+        y2g.reset(n2[0], n2[1], n2[2]);
+        bool bad = bad_s != 0;
+        for (int c = 0; c < CH4TC_NCHUNK; ++c, ++g) {
+          const int s = g % CH4TC_STAGES;
+          // this thread's Y2 of the chunk: index 4 c + qt (the generator visits all four)
+          float y2 = 0.f;
 #pragma unroll
-      for (int i = 0; i < 3; ++i) o[i] = M[i][0] * acc[0] + M[i][1] * acc[1] + M[i][2] * acc[2];
+          for (int i = 0; i < 4; ++i) {
+            const float v = (4 * c + i < CH4_NY2) ? y2g.next() : 0.f;
+            if (i == qt) y2 = v;
+          }
+          // stage s is free once the MMAs of chunk g - 3 are done
+          if (!bad && g >= (unsigned)CH4TC_STAGES &&
+              !mbar_wait(&bar_empty[s], ((g - CH4TC_STAGES) / CH4TC_STAGES) & 1)) {
+            bad = true;
+            fail();
+          }
+          if (!bad) {
+            float4 hi, lo;
+            float *ph = &hi.x, *pl = &lo.x;
+#pragma unroll
+            for (int j = 0; j < 4; ++j) {
+              const float v = y2 * xp[j];
+              const float h = tf32_hi(v);
+              ph[j] = h;
+              pl[j] = v - h;
+            }
+            *reinterpret_cast<float4 *>(reinterpret_cast<float *>(stA(s, 0)) + ch4tc_img_off(row, 4 * qt)) = hi;
+            *reinterpret_cast<float4 *>(reinterpret_cast<float *>(stA(s, 1)) + ch4tc_img_off(row, 4 * qt)) = lo;
+            asm volatile("fence.proxy.async.shared::cta;" ::: "memory");
+          }
+          __syncwarp();
+          if (lane == 0 && !bad) mbar_arrive(&bar_fa[s]);
+          if (!bad && bad_s) bad = true;
+        }
+        // ---- all MMAs of this pass done: the quarters' partial sums from TMEM ----
+        if (!bad && !mbar_wait(&bar_empty[(g - 1) % CH4TC_STAGES], ((g - 1) / CH4TC_STAGES) & 1)) {
+          bad = true;
+          fail();
+        }
+        // tcgen05.ld is a warp-wide instruction: the warp reads TMEM or skips it as one
+        bad = __any_sync(0xffffffffu, bad);
+        tc_fence_after();
+        if (!bad) {
+          float v;
+          if (q == 0) {
+            const int comp = qt >> 1;
+            v = (qt & 1) ? ch4tc_y1_dot_m(lane_addr + (comp ? CH4TC_COL1 : 0u), n1, CH4TC_Y1_SPLIT, CH4_L1 + 1)
+                         : ch4tc_y1_dot_m(lane_addr + (comp ? CH4TC_COL1 : 0u), n1, 0, CH4TC_Y1_SPLIT);
+          } else {
+            v = ch4tc_y1_dot_m(lane_addr, n1, CH4TC_Y1_M[qt], CH4TC_Y1_M[qt + 1]);
+          }
+          part_s[q][qt][row] = v;
+        }
+        // the accumulators may be rewritten by the next pass's MMAs
+        tc_fence_before();
+        __syncwarp();
+        if (lane == 0 && !bad) mbar_arrive(&bar_tfree);
+        if (ch4tc_producers_sync_or(bad || bad_s)) {
+          stop = true;
+          break;
+        }
+        if (qt == 0) {
+          if (q == 0) {
+            acc[0] = part_s[0][0][row] + part_s[0][1][row];
+            acc[1] = part_s[0][2][row] + part_s[0][3][row];
+          } else {
+            acc[2] = (part_s[1][0][row] + part_s[1][1][row]) + (part_s[1][2][row] + part_s[1][3][row]);
+          }
+        }
+      }
+      if (stop) break;
+      if (seg == CH4_NSEG - 1) {
+        const float i2 = 1.f / (R * R);
+        const float i6 = i2 * i2 * i2;
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc) acc[cc] *= i6;
+      }
+      if (qt == 0 && mine >= 0) {
+        float *o = a.mu + (size_t)mine * 4;
+#pragma unroll
+        for (int i = 0; i < 3; ++i) o[i] = M[i][0] * acc[0] + M[i][1] * acc[1] + M[i][2] * acc[2];
+      }
     }
-  }
-  // a CTA that gave up waits (bounded) for the work it issued before freeing TMEM
-  if (bad_s && t == 0) {
-    if (gm > 0) mbar_wait(&bar_mma[(gm - 1) % CH4TC_STAGES], ((gm - 1) / CH4TC_STAGES) & 1);
-    for (unsigned h = gw; h < gl; ++h) mbar_wait(&bar_load[h % CH4TC_STAGES], (h / CH4TC_STAGES) & 1);
   }
   tc_fence_before();
   __syncthreads();
