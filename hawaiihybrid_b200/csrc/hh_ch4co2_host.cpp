@@ -162,7 +162,9 @@ int ch4co2_build_tc_blob(const Ch4Co2FoldHost &f, std::vector<float> *blob) {
           const int comp = q == 0 ? cc : 2;
           for (int n = 0; n < CH4TC_N; ++n)
             for (int kk = 0; kk < CH4TC_KC; ++kk) {
-              const double v = B[((size_t)s * 3 + comp) * per_comp + (size_t)n * CH4TC_K + CH4TC_KC * c + kk];
+              // the chunk's column kk: power kk % 4 of the Y2 its group holds
+              const int k = ch4tc_k_of(c, kk / 4);
+              const double v = k < 0 ? 0.0 : B[((size_t)s * 3 + comp) * per_comp + (size_t)n * CH4TC_K + 4 * k + kk % 4];
               const float h = tf32_rna((float)v);
               const int off = ch4tc_img_off(cc * CH4TC_N + n, kk);
               hi[off] = h;

@@ -179,9 +179,12 @@ __device__ __forceinline__ void ch4tc_cs_m(float x, float y, int m, float &C, fl
 }
 
 // sum over the Y1 columns of m in [m0, m1) (m-major, l = m..13, cos then sin) of
-// Y1_n(n1) T[n] at TMEM address `taddr` (this thread's lane); m0 and m1 are uniform
-// across the warp (tcgen05.ld is a warp-wide load)
-__device__ __forceinline__ float ch4tc_y1_dot_m(uint32_t taddr, const float n1[3], int m0, int m1) {
+// Y1_n(n1) T_i[n] for NA accumulators at TMEM addresses taddr[i] (this thread's lane),
+// the recurrence of Y1 shared between them; m0 and m1 are uniform across the warp
+// (tcgen05.ld is a warp-wide load)
+template <int NA>
+__device__ __forceinline__ void ch4tc_y1_dot(const uint32_t (&taddr)[NA], const float n1[3], int m0, int m1,
+                                             float (&acc)[NA]) {
   const int c_begin = ch4tc_y1_col(m0, m0, 0, CH4_L1);
   const int c_end = (m1 > CH4_L1) ? CH4TC_NY1 : ch4tc_y1_col(m1, m1, 0, CH4_L1);
   float C, Sn;
@@ -189,14 +192,16 @@ __device__ __forceinline__ float ch4tc_y1_dot_m(uint32_t taddr, const float n1[3
   float pm = c_ch4tc_pm[m0], qa = 1.f, qb = 0.f, ys_pending = 0.f;
   int m = m0, l = m0;
   bool first = true, sin_next = false;
-  float acc = 0.f;
+#pragma unroll
+  for (int i = 0; i < NA; ++i) acc[i] = 0.f;
 #pragma unroll 1
   for (int c0 = c_begin & ~15; c0 < c_end; c0 += 16) {
-    float v[16];
-    tmem_ld16(taddr + (uint32_t)c0, v);
+    float v[NA][16];
 #pragma unroll
-    for (int i = 0; i < 16; ++i) {
-      const int c = c0 + i;
+    for (int i = 0; i < NA; ++i) tmem_ld16(taddr[i] + (uint32_t)c0, v[i]);
+#pragma unroll
+    for (int k = 0; k < 16; ++k) {
+      const int c = c0 + k;
       if (c >= c_begin && c < c_end) {
         float y;
         if (sin_next) {
@@ -226,11 +231,11 @@ __device__ __forceinline__ float ch4tc_y1_dot_m(uint32_t taddr, const float n1[3
             sin_next = true;
           }
         }
-        acc = fmaf(y, v[i], acc);
+#pragma unroll
+        for (int i = 0; i < NA; ++i) acc[i] = fmaf(y, v[i][k], acc[i]);
       }
     }
   }
-  return acc;
 }
 
 // The Y2 of one record in the order of ch4_y2 (m = 0..12, even l = m..12, cos then
@@ -254,6 +259,15 @@ struct Ch4TcY2Gen {
     m = 0;
     l = 0;
     sin_next = false;
+  }
+  // the first value of m = m0 next: (cos, sin)(m0 phi) by ch4tc_cs_m, whose products are
+  // those of the rotations a walk from m = 0 makes, so the values are the same
+  __device__ __forceinline__ void start(float x_, float y_, float z_, int m0) {
+    reset(x_, y_, z_);
+    ch4tc_cs_m(x, y, m0, C, Sn);
+    m = m0;
+    l = m0;
+    pm = c_ch4tc_pm[m0];
   }
   // to the next (m, l): l + 1 by the recurrence, or m + 1 with l = m
   __device__ __forceinline__ void advance() {
@@ -293,10 +307,11 @@ struct Ch4TcY2Gen {
 // Warp roles (17 warps): warps 0..15 produce the A chunks and run the epilogue, four
 // per TMEM lane quadrant; thread t < 512 works on record row = t % 128 and its quarter
 // qt = t / 128 takes
-//   - column group k = 4 c + qt of every A chunk (its 4 powers of x, hi and lo), with
-//     the record's Y2 from a generator stepped through every index;
-//   - in pass 0 half of the columns of component qt / 2 (m in [0, 5) or [5, 14)), in
-//     pass 1 a quarter of the columns of component 2 (CH4TC_Y1_M);
+//   - column group qt of every A chunk (its 4 powers of x, hi and lo): chunk c's group qt
+//     holds Y2 index 23 qt + c (ch4tc_k_of), so the thread's generator walks only its
+//     quarter of the Y2 sequence, one value per chunk;
+//   - the Y1 columns of m in its quarter's range (CH4TC_Y1_M) of components 0 and 1 in
+//     pass 0, with one Y1 recurrence for both, and of component 2 in pass 1;
 // the partial sums meet in shared memory and quarter 0 finishes the record.  Warp 16
 // (one lane) issues the B copies and the MMAs.  The two sides meet only at mbarriers:
 //   full_a[s]  the 16 producer warps wrote stage s's A (after fence.proxy.async);
@@ -311,8 +326,8 @@ struct Ch4TcY2Gen {
 // barrier, a reduction over bad_s), where all producers leave together.
 constexpr int CH4TC_PRODUCERS = 4 * CH4TC_M;
 constexpr int CH4TC_THREADS = CH4TC_PRODUCERS + 32;
-__constant__ int CH4TC_Y1_M[5] = {0, 2, 4, 7, CH4_L1 + 1};
-constexpr int CH4TC_Y1_SPLIT = 5;  // pass 0: m < 5 and m >= 5
+__constant__ int CH4TC_Y1_M[5] = {0, 2, 4, 7, CH4_L1 + 1};  // the quarters' m ranges of Y1
+static_assert(CH4TC_QLEN == CH4TC_NCHUNK && 4 * CH4TC_QLEN >= CH4_NY2, "one Y2 per quarter and chunk");
 
 __device__ __forceinline__ void mbar_arrive(uint64_t *bar) {
   asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];" ::"r"(smem_u32(bar)) : "memory");
@@ -344,7 +359,7 @@ __global__ void __launch_bounds__(CH4TC_THREADS, 1) ch4_dipole_tc_kernel(Ch4TcAr
   __shared__ uint32_t tmem_base_s;
   __shared__ volatile int bad_s;
   __shared__ long long w0[CH4_NSEG + 1];
-  __shared__ float part_s[2][4][CH4TC_M];  // the quarters' partial sums, per pass
+  __shared__ float part_s[3][4][CH4TC_M];  // the quarters' partial sums, per component
   const int t = threadIdx.x, warp = t >> 5, lane = t & 31;
   for (int i = t; i <= CH4_NSEG; i += blockDim.x) w0[i] = a.warp0[i];
   if (t == 0) {
@@ -477,6 +492,11 @@ __global__ void __launch_bounds__(CH4TC_THREADS, 1) ch4_dipole_tc_kernel(Ch4TcAr
     // ---------------- producers: A chunks, epilogue ----------------
     const int row = t & (CH4TC_M - 1), qt = t / CH4TC_M;
     const uint32_t lane_addr = tmem + ((uint32_t)((warp & 3) * 32) << 16);
+    // this quarter's Y2 values, indices CH4TC_QLEN qt .., start in the run of m = m_q,
+    // d_q values into it
+    int m_q = 0;
+    while (m_q < CH4_L2 && ch4tc_y2_off(m_q + 1) <= CH4TC_QLEN * qt) ++m_q;
+    const int d_q = CH4TC_QLEN * qt - ch4tc_y2_off(m_q);
     unsigned g = 0;
     bool stop = false;
     for (long long task = blockIdx.x; task < total && !stop; task += gridDim.x) {
@@ -508,17 +528,13 @@ __global__ void __launch_bounds__(CH4TC_THREADS, 1) ch4_dipole_tc_kernel(Ch4TcAr
       float acc[3] = {0.f, 0.f, 0.f};
       for (int q = 0; q < 2; ++q) {
         Ch4TcY2Gen y2g;
-        y2g.reset(n2[0], n2[1], n2[2]);
+        y2g.start(n2[0], n2[1], n2[2], m_q);
+        for (int i = 0; i < d_q; ++i) (void)y2g.next();
         bool bad = bad_s != 0;
         for (int c = 0; c < CH4TC_NCHUNK; ++c, ++g) {
           const int s = g % CH4TC_STAGES;
-          // this thread's Y2 of the chunk: index 4 c + qt (the generator visits all four)
-          float y2 = 0.f;
-#pragma unroll
-          for (int i = 0; i < 4; ++i) {
-            const float v = (4 * c + i < CH4_NY2) ? y2g.next() : 0.f;
-            if (i == qt) y2 = v;
-          }
+          // this thread's Y2 of the chunk (column group qt): the quarter's next value
+          const float y2 = ch4tc_k_of(c, qt) >= 0 ? y2g.next() : 0.f;
           // stage s is free once the MMAs of chunk g - 3 are done
           if (!bad && g >= (unsigned)CH4TC_STAGES &&
               !mbar_wait(&bar_empty[s], ((g - CH4TC_STAGES) / CH4TC_STAGES) & 1)) {
@@ -552,15 +568,20 @@ __global__ void __launch_bounds__(CH4TC_THREADS, 1) ch4_dipole_tc_kernel(Ch4TcAr
         bad = __any_sync(0xffffffffu, bad);
         tc_fence_after();
         if (!bad) {
-          float v;
+          // the quarter's m range of the Y1 columns: components 0 and 1 in pass 0 (one
+          // Y1 recurrence for both), component 2 in pass 1
           if (q == 0) {
-            const int comp = qt >> 1;
-            v = (qt & 1) ? ch4tc_y1_dot_m(lane_addr + (comp ? CH4TC_COL1 : 0u), n1, CH4TC_Y1_SPLIT, CH4_L1 + 1)
-                         : ch4tc_y1_dot_m(lane_addr + (comp ? CH4TC_COL1 : 0u), n1, 0, CH4TC_Y1_SPLIT);
+            const uint32_t ta[2] = {lane_addr, lane_addr + CH4TC_COL1};
+            float v[2];
+            ch4tc_y1_dot<2>(ta, n1, CH4TC_Y1_M[qt], CH4TC_Y1_M[qt + 1], v);
+            part_s[0][qt][row] = v[0];
+            part_s[1][qt][row] = v[1];
           } else {
-            v = ch4tc_y1_dot_m(lane_addr, n1, CH4TC_Y1_M[qt], CH4TC_Y1_M[qt + 1]);
+            const uint32_t ta[1] = {lane_addr};
+            float v[1];
+            ch4tc_y1_dot<1>(ta, n1, CH4TC_Y1_M[qt], CH4TC_Y1_M[qt + 1], v);
+            part_s[2][qt][row] = v[0];
           }
-          part_s[q][qt][row] = v;
         }
         // the accumulators may be rewritten by the next pass's MMAs
         tc_fence_before();
@@ -571,12 +592,9 @@ __global__ void __launch_bounds__(CH4TC_THREADS, 1) ch4_dipole_tc_kernel(Ch4TcAr
           break;
         }
         if (qt == 0) {
-          if (q == 0) {
-            acc[0] = part_s[0][0][row] + part_s[0][1][row];
-            acc[1] = part_s[0][2][row] + part_s[0][3][row];
-          } else {
-            acc[2] = (part_s[1][0][row] + part_s[1][1][row]) + (part_s[1][2][row] + part_s[1][3][row]);
-          }
+#pragma unroll
+          for (int cc = (q == 0 ? 0 : 2); cc < (q == 0 ? 2 : 3); ++cc)
+            acc[cc] = (part_s[cc][0][row] + part_s[cc][1][row]) + (part_s[cc][2][row] + part_s[cc][3][row]);
         }
       }
       if (stop) break;

@@ -30,6 +30,15 @@ HH_TC_HD constexpr int ch4tc_img_off(int row, int kk) {
   return (row >> 3) * 128 + (kk >> 2) * 32 + (row & 7) * 4 + (kk & 3);
 }
 
+// K order of the A and B images: column group i (columns 4 i .. 4 i + 3 of a chunk,
+// the powers x^0..x^3) of chunk c holds Y2 index CH4TC_QLEN i + c, so the four quarters
+// of the Y2 sequence sit side by side and a thread that writes group i walks only its
+// quarter, one value per chunk; -1 past the sequence's end (a zero group)
+constexpr int CH4TC_QLEN = 23;  // Y2 values per quarter: 23 x 4 >= 91, and 23 chunks
+HH_TC_HD constexpr int ch4tc_k_of(int c, int i) {
+  return (c < CH4TC_QLEN && CH4TC_QLEN * i + c < 91) ? CH4TC_QLEN * i + c : -1;
+}
+
 // byte offset of the (hi, lo) image pair of piece p, pass q, chunk c in the blob
 HH_TC_HD constexpr size_t ch4tc_blob_off(int p, int q, int c) {
   return (size_t)p * CH4TC_PIECE_BYTES + (q == 0 ? (size_t)c * 2 * CH4TC_IMG0
