@@ -375,10 +375,10 @@ __global__ void __launch_bounds__(DEFER_THREADS, 1) defer_eval_kernel(DeferArgs 
 // (paired FP32, fma2).  The position is formed in FP32, y_old + F0 x + F1 x(1-x) +
 // F2 x^2(1-x) + ... + F6 x^4(1-x)^3 with the basis formed once and one FMA per term.
 // A context with an odd count ends in a single sample: the second half of its last
-// pair is computed but neither tested nor accumulated.  16 warps per SM (128
-// registers a thread, no spills) ran faster than 32 (64 registers, with spills).
+// pair is computed but neither tested nor accumulated.  20 warps per SM (96 registers a
+// thread, no spills) ran faster than 16 (128) and than 24 or 32 (80 or 64, with spills).
 template <typename PHYS, typename STG>
-__global__ void __launch_bounds__(defer_eval_threads<SYS_CO2AR>(), 16 * 32 / defer_eval_threads<SYS_CO2AR>())
+__global__ void __launch_bounds__(defer_eval_threads<SYS_CO2AR>(), 20 * 32 / defer_eval_threads<SYS_CO2AR>())
     defer_eval_co2ar_kernel(DeferArgs a, TrajParams P, TrajIO io, const Co2arTablesGlobal *gtab) {
   using DS = DeferSys<SYS_CO2AR, float, float>;
   constexpr int NQ = DS::NQ;
