@@ -152,6 +152,12 @@ __device__ __forceinline__ unsigned long long globaltimer_ns() {
 }
 
 // ---- coefficient tables for CO2-Ar, staged in shared memory ----
+// FP32 surface rows for the paired evaluation of the value c and the derivative dc of a
+// radial function (co2ar_pes_grad_f2): 20 words per (interval, l),
+//   (a3, 0 | a2, 3 a3), (a1, 2 a2 | a0, a1)       Horner of the (c, dc) pair in t
+//   (b4, -4 b4 | b5, -5 b5), (b6, -6 b6 | b7, -7 b7)   against (R^-k, R^-(k+1))
+//   (A, A k, k, 0)                                  the exponential A e^(k R)
+constexpr int CO2AR_PAIR_WORDS = 20;
 template <typename T> struct Co2arTables {
   T pes[CO2AR_TABLE];
   T dipx[CO2AR_TABLE];
@@ -160,6 +166,7 @@ template <typename T> struct Co2arTables {
   T rlo[CO2AR_NINT];
   int fpes[CO2AR_NINT];
   int fdip[CO2AR_NINT];
+  float4 pes2[sizeof(T) == 4 ? CO2AR_NINT * CO2AR_NL * CO2AR_PAIR_WORDS / 4 : 1];  // FP32 tables only
 };
 
 struct Co2arTablesGlobal {  // FP64 master copy in global memory
@@ -184,6 +191,36 @@ __device__ void load_tables(Co2arTables<T> *s, const Co2arTablesGlobal *g) {
     s->rlo[i] = T(g->rlo[i]);
     s->fpes[i] = g->fpes[i];
     s->fdip[i] = g->fdip[i];
+  }
+  if constexpr (sizeof(T) == 4) {
+    float *w = reinterpret_cast<float *>(s->pes2);
+    for (int e = threadIdx.x; e < CO2AR_NINT * CO2AR_NL * CO2AR_PAIR_WORDS; e += blockDim.x) {
+      const double *r = g->pes + (e / CO2AR_PAIR_WORDS) * CO2AR_ROW;
+      const int k = e % CO2AR_PAIR_WORDS;
+      double v = 0.0;
+      switch (k) {
+        case 0: v = r[3]; break;
+        case 2: v = r[2]; break;
+        case 3: v = 3.0 * r[3]; break;
+        case 4: v = r[1]; break;
+        case 5: v = 2.0 * r[2]; break;
+        case 6: v = r[0]; break;
+        case 7: v = r[1]; break;
+        case 8: v = r[4]; break;
+        case 9: v = -4.0 * r[4]; break;
+        case 10: v = r[5]; break;
+        case 11: v = -5.0 * r[5]; break;
+        case 12: v = r[6]; break;
+        case 13: v = -6.0 * r[6]; break;
+        case 14: v = r[7]; break;
+        case 15: v = -7.0 * r[7]; break;
+        case 16: v = r[8]; break;
+        case 17: v = r[8] * r[9]; break;
+        case 18: v = r[9]; break;
+        default: v = 0.0;  // words 1 and 19
+      }
+      w[e] = float(v);
+    }
   }
 }
 
@@ -235,11 +272,60 @@ template <typename PHYS, typename STG, bool COMP, bool SOLO_ = false> struct HeA
 template <typename T> struct PesGrad {
   T VR, Vx;
 };
+// FP32 without compensation: the value c and derivative dc of each radial function as
+// one (c, dc) pair through the paired FP32 instructions (fma2), from the pes2 rows; the
+// sums over l as co2ar_pes forms them
+__device__ __forceinline__ PesGrad<float> co2ar_pes_grad_f2(const Co2arTables<float> *tb, float R, float iR,
+                                                           float x) {
+  const int i = co2ar_interval<float>(R, tb->rbound);
+  float P[11], dP[11];
+  legendre10(x, P, dP);
+  const float2 t = splat2(R - tb->rlo[i]);
+  const int fl = tb->fpes[i];
+  float2 q4 = make_float2(0.f, 0.f), q5 = q4, q6 = q4, q7 = q4;
+  if (fl & 1) {
+    const float iR2 = iR * iR, iR4 = iR2 * iR2;
+    q4 = make_float2(iR4, iR4 * iR);   // (R^-4, R^-5)
+    q5 = mul2(q4, splat2(iR));         // (R^-5, R^-6)
+    q6 = mul2(q5, splat2(iR));
+    q7 = mul2(q6, splat2(iR));
+  }
+  float aR = 0.f, ax = 0.f;
+  const float4 *rows = tb->pes2 + (size_t)i * CO2AR_NL * (CO2AR_PAIR_WORDS / 4);
+#pragma unroll
+  for (int li = 0; li < CO2AR_NL; ++li) {
+    const float4 *rw = rows + li * (CO2AR_PAIR_WORDS / 4);
+    const float4 a = rw[0], b = rw[1];
+    float2 c = fma2(make_float2(a.x, a.y), t, make_float2(a.z, a.w));
+    c = fma2(c, t, make_float2(b.x, b.y));
+    c = fma2(c, t, make_float2(b.z, b.w));
+    if (fl & 1) {
+      const float4 p = rw[2], q = rw[3];
+      c = fma2(make_float2(p.x, p.y), q4, c);
+      c = fma2(make_float2(p.z, p.w), q5, c);
+      c = fma2(make_float2(q.x, q.y), q6, c);
+      c = fma2(make_float2(q.z, q.w), q7, c);
+    }
+    if (fl & 2) {
+      const float4 e = rw[4];
+      c = fma2(make_float2(e.x, e.y), splat2(expf(e.z * R)), c);
+    }
+    aR = fmaf(P[2 * li], c.y, aR);
+    ax = fmaf(dP[2 * li], c.x, ax);
+  }
+  const float sc = float(1.0 / HH_HTOCM);
+  return {aR * sc, ax * sc};
+}
+
 template <typename T, bool COMP>
 __device__ __noinline__ PesGrad<T> co2ar_pes_grad(const Co2arTables<T> *tb, T R, T iR, T x) {
-  T V, VR, Vx;
-  co2ar_pes<T, COMP>(tb->pes, tb->fpes, tb->rbound, tb->rlo, R, iR, x, V, VR, Vx, false);
-  return {VR, Vx};
+  if constexpr (sizeof(T) == 4 && !COMP) {
+    return co2ar_pes_grad_f2(tb, R, iR, x);
+  } else {
+    T V, VR, Vx;
+    co2ar_pes<T, COMP>(tb->pes, tb->fpes, tb->rbound, tb->rlo, R, iR, x, V, VR, Vx, false);
+    return {VR, Vx};
+  }
 }
 
 // Body-frame dipole sums (d_z, a_x) of CO2-Ar, out of line for the same reason:
