@@ -220,22 +220,48 @@ template <typename T> __device__ __forceinline__ T n2ar_unit_grad(T h, T w1) {
 // PIPs and their Jacobian are unrolled over the monomial table; the network is a
 // runtime loop over the 32 hidden units (forward and backward in one pass) with
 // the weights of `net` (shared memory in the kernels), so the code stays small.
+// FP32: two hidden units per iteration with the paired FP32 instructions of sm_100,
+// each half the scalar loop's fma chain in the same order (h_j over i, a_i over j), so
+// the values are bit for bit those of the scalar loop and of n2ar_pes_grad_coop.
 template <typename T>
 __device__ __noinline__ N2arGrad<T> n2ar_pes_grad(const N2arPesNet<T> *net, T d1, T d2) {
   constexpr int NP = N2AR_PES_NP;
-  T ptr[NP], j1[NP], j2[NP], a[NP], dy1, dy2;
+  T ptr[NP], j1[NP], j2[NP], a[NP + 1], dy1, dy2;
   n2ar_grad_inputs(net, d1, d2, ptr, j1, j2, dy1, dy2);
 #pragma unroll
-  for (int i = 0; i < NP; ++i) a[i] = T(0);
+  for (int i = 0; i <= NP; ++i) a[i] = T(0);
+  if constexpr (sizeof(T) == 4) {
+    static_assert(N2AR_PES_NH % 2 == 0 && NP + 1 <= N2AR_PES_ROW, "unit pairs, input pairs within a row");
 #pragma unroll 1
-  for (int j = 0; j < N2AR_PES_NH; ++j) {
-    const T *w = net->w0t[j];
-    T h = net->b0[j];
+    for (int jp = 0; jp < N2AR_PES_NH / 2; ++jp) {
+      const float2 *wp = reinterpret_cast<const float2 *>(net->w0p[jp]);
+      float2 h = make_float2(net->b0[2 * jp], net->b0[2 * jp + 1]);
 #pragma unroll
-    for (int i = 0; i < NP; ++i) h = n2_fma(ptr[i], w[i], h);
-    const T g = n2ar_unit_grad(h, net->w1[j]);
+      for (int i = 0; i < NP; ++i) h = __ffma2_rn(make_float2(ptr[i], ptr[i]), wp[i], h);
 #pragma unroll
-    for (int i = 0; i < NP; ++i) a[i] = n2_fma(w[i], g, a[i]);
+      for (int b = 0; b < 2; ++b) {
+        const int j = 2 * jp + b;
+        const T g = n2ar_unit_grad(b == 0 ? h.x : h.y, net->w1[j]);
+        const float2 *w = reinterpret_cast<const float2 *>(net->w0t[j]);
+#pragma unroll
+        for (int i = 0; i < NP; i += 2) {  // w0t[j][NP] is zero: a[NP] is never read
+          const float2 r = __ffma2_rn(w[i / 2], make_float2(g, g), make_float2(a[i], a[i + 1]));
+          a[i] = r.x;
+          a[i + 1] = r.y;
+        }
+      }
+    }
+  } else {
+#pragma unroll 1
+    for (int j = 0; j < N2AR_PES_NH; ++j) {
+      const T *w = net->w0t[j];
+      T h = net->b0[j];
+#pragma unroll
+      for (int i = 0; i < NP; ++i) h = n2_fma(ptr[i], w[i], h);
+      const T g = n2ar_unit_grad(h, net->w1[j]);
+#pragma unroll
+      for (int i = 0; i < NP; ++i) a[i] = n2_fma(w[i], g, a[i]);
+    }
   }
   T a1 = T(0), a2 = T(0);
 #pragma unroll

@@ -62,6 +62,9 @@ constexpr int N2AR_PES_NH = 32;
 constexpr int N2AR_PES_ROW = 20;
 template <typename T> struct N2arPesNet {
   T w0t[N2AR_PES_NH][N2AR_PES_ROW];  // w0t[j][i] = W0[i][j]
+  // the hidden units in pairs: w0p[p][2 i + b] = W0[i][2 p + b], so that (W0[i][2p],
+  // W0[i][2p + 1]) is one 8-byte word
+  T w0p[N2AR_PES_NH / 2][2 * N2AR_PES_ROW];
   T b0[N2AR_PES_NH];
   T w1[N2AR_PES_NH];
   T xmean[N2AR_PES_ROW];

@@ -36,7 +36,10 @@ void n2ar_build_pes(N2arPesNet<double> *d, N2arPesNet<float> *f) {
   std::memset(d, 0, sizeof *d);
   std::memset(f, 0, sizeof *f);
   for (int j = 0; j < N2AR_PES_NH; ++j) {
-    for (int i = 0; i < N2AR_PES_NP; ++i) d->w0t[j][i] = hh_n2ar_pes_w0[i][j];
+    for (int i = 0; i < N2AR_PES_NP; ++i) {
+      d->w0t[j][i] = hh_n2ar_pes_w0[i][j];
+      d->w0p[j / 2][2 * i + (j & 1)] = hh_n2ar_pes_w0[i][j];
+    }
     d->b0[j] = hh_n2ar_pes_b0[j];
     d->w1[j] = hh_n2ar_pes_w1[j];
   }
